@@ -1,0 +1,872 @@
+/*
+ * CPU oracle for the PyroclastMPM update-stress-last step.
+ * TEST INFRASTRUCTURE ONLY (see oracle.h): used by tests/, smoke() and the
+ * bench's CPU baseline as the checker; never part of the product path.
+ *
+ * Every function names the reference code it restates.  Paths are relative to
+ * the PyroclastMPM project root.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef REAL real;
+
+/* ------------------------------------------------------------------------ */
+/* Grid and stencil windows                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Grid ctor: include/pyroclastmpm/common/types_common.h:260-272.
+ * inv = 1/h and N_axis = (int)((end - origin)/h) + 1, all in REAL. */
+void or_grid_init(or_grid *g, int dim, const REAL *origin, const REAL *end, REAL cell_size) {
+  memset(g, 0, sizeof(*g));
+  g->dim = dim;
+  g->cell_size = cell_size;
+  g->inv_cell_size = (real)1.0 / cell_size;
+  g->num_cells_total = 1;
+  for (int a = 0; a < 3; a++) {
+    g->num_cells[a] = 1;
+    if (a < dim) {
+      g->origin[a] = origin[a];
+      g->end[a] = end[a];
+      real span = (real)(end[a] - origin[a]);
+      g->num_cells[a] = (int)(span / cell_size) + 1;
+    }
+    g->num_cells_total *= g->num_cells[a];
+  }
+}
+
+/* set_global_shapefunction: nsn = window^DIM, window 2 (linear) or 4
+ * (src/common/global_settings.cpp:232-268).  Quadratic (absent from the
+ * reference) uses the same 4-wide window as cubic; its fourth slot per axis
+ * always carries a zero weight. */
+int or_num_surround_nodes(int dim, int sf) {
+  int w = (sf == OR_LINEAR) ? 2 : 4;
+  int n = 1;
+  for (int a = 0; a < dim; a++) n *= w;
+  return n;
+}
+
+/* Window offsets of slot `sid`, in the reference's slot order
+ * (src/common/global_settings.cpp:108-150): 2D is x-fastest then y; 3D is
+ * z-fastest, then x, then y.  Linear offsets are {0,1}, the 4-wide ones
+ * {-1,0,1,2}.  The P2G window is the negation (p2g = -g2p). */
+static void window_offset(int dim, int sf, int sid, int w[3]) {
+  int width = (sf == OR_LINEAR) ? 2 : 4;
+  int lo = (sf == OR_LINEAR) ? 0 : -1;
+  w[0] = w[1] = w[2] = 0;
+  if (dim == 1) {
+    w[0] = lo + sid;
+  } else if (dim == 2) {
+    w[0] = lo + sid % width;
+    w[1] = lo + sid / width;
+  } else {
+    w[2] = lo + sid % width;
+    w[0] = lo + (sid / width) % width;
+    w[1] = lo + sid / (width * width);
+  }
+}
+
+static inline int flat3(const or_grid *g, const int b[3]) {
+  /* NODE_MEM_INDEX: include/pyroclastmpm/common/types_common.h:98-99,110 */
+  return b[0] + b[1] * g->num_cells[0] + b[2] * g->num_cells[0] * g->num_cells[1];
+}
+
+/* NodesContainer::calculate_bin_ids (src/nodes/nodes.cpp:89-129): x-fastest. */
+void or_node_ids(const or_grid *g, int *node_ids) {
+  for (int z = 0; z < g->num_cells[2]; z++)
+    for (int y = 0; y < g->num_cells[1]; y++)
+      for (int x = 0; x < g->num_cells[0]; x++) {
+        int idx = x + y * g->num_cells[0] + z * g->num_cells[0] * g->num_cells[1];
+        node_ids[3 * idx + 0] = x;
+        node_ids[3 * idx + 1] = y;
+        node_ids[3 * idx + 2] = z;
+      }
+}
+
+/* NodesContainer::calculate_bin_types (src/nodes/nodes.cpp:135-173), cubic
+ * only: 1 at either end, 2 at index 1, 3 otherwise.  The reference's "left of
+ * boundary" test can never be true, so type 4 is never assigned; that is kept. */
+void or_node_types(const or_grid *g, int sf, const int *node_ids, int *node_types) {
+  for (int i = 0; i < g->num_cells_total; i++)
+    for (int a = 0; a < 3; a++) node_types[3 * i + a] = 0;
+  if (sf != OR_CUBIC) return;
+  for (int i = 0; i < g->num_cells_total; i++)
+    for (int a = 0; a < g->dim; a++) {
+      int id = node_ids[3 * i + a];
+      int t;
+      if (id == 0 || id == g->num_cells[a] - 1) t = 1;
+      else if (id == 1) t = 2;
+      else t = 3;
+      node_types[3 * i + a] = t;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Spatial partition                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* calculate_hashes (src/spatialpartition/spatialpartition_inline.h:49-62):
+ * bin = (int)((x - origin) * inv_h) (truncation), hash = NODE_MEM_INDEX as
+ * unsigned; then SpatialPartition::calculate_hash copies the hashes into the
+ * to-be-sorted array (src/spatialpartition/spatialpartition.cpp:90-110). */
+void or_calculate_hash(const or_grid *g, int n, const REAL *x, int *bins,
+                       unsigned int *hash_unsorted, unsigned int *hash_sorted) {
+  int d = g->dim;
+  for (int i = 0; i < n; i++) {
+    int b[3] = {0, 0, 0};
+    for (int a = 0; a < d; a++) {
+      real rel = (real)(x[i * d + a] - g->origin[a]);
+      rel = (real)(rel * g->inv_cell_size);
+      b[a] = (int)rel;
+    }
+    for (int a = 0; a < d; a++) bins[i * d + a] = b[a];
+    unsigned int h = (unsigned int)flat3(g, b);
+    hash_unsorted[i] = h;
+    hash_sorted[i] = h;
+  }
+}
+
+/* SpatialPartition::sort_hashes (src/spatialpartition/spatialpartition.cpp:113-117):
+ * stable sort of (hash, index) with index = 0..n-1 (reset, :80).  Stable LSD
+ * radix sort on the 32-bit key. */
+void or_sort_hashes(int n, unsigned int *hash_sorted, int *sorted_index) {
+  unsigned int *kbuf = (unsigned int *)malloc(sizeof(unsigned int) * (size_t)(n > 0 ? n : 1));
+  int *vbuf = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; i++) sorted_index[i] = i;
+  unsigned int *ks = hash_sorted, *kd = kbuf;
+  int *vs = sorted_index, *vd = vbuf;
+  for (int shift = 0; shift < 32; shift += 8) {
+    size_t count[257];
+    memset(count, 0, sizeof(count));
+    for (int i = 0; i < n; i++) count[((ks[i] >> shift) & 255u) + 1]++;
+    for (int k = 0; k < 256; k++) count[k + 1] += count[k];
+    for (int i = 0; i < n; i++) {
+      size_t pos = count[(ks[i] >> shift) & 255u]++;
+      kd[pos] = ks[i];
+      vd[pos] = vs[i];
+    }
+    unsigned int *tk = ks; ks = kd; kd = tk;
+    int *tv = vs; vs = vd; vd = tv;
+  }
+  /* four passes: the result is back in the caller's arrays */
+  free(kbuf);
+  free(vbuf);
+}
+
+/* bin_particles_kernel (src/spatialpartition/spatialpartition_inline.h:85-115):
+ * start/end from adjacent-hash changes; empty cells keep 0/0 (reset fills 0).
+ * Hashes >= num_cells_total (particles outside the grid) would write out of
+ * bounds in the reference; they are skipped here. */
+void or_bin_particles(const or_grid *g, int n, const unsigned int *hs, int *cell_start, int *cell_end) {
+  unsigned int nt = (unsigned int)g->num_cells_total;
+  for (int i = 0; i < g->num_cells_total; i++) cell_start[i] = cell_end[i] = 0;
+  for (int t = 0; t < n; t++) {
+    unsigned int h = hs[t];
+    if (t < n - 1) {
+      unsigned int nh = hs[t + 1];
+      if (t == 0 && h < nt) cell_start[h] = t;
+      if (h != nh) {
+        if (h < nt) cell_end[h] = t + 1;
+        if (nh < nt) cell_start[nh] = t + 1;
+      }
+    }
+    if (t == n - 1 && h < nt) cell_end[h] = t + 1;
+  }
+}
+
+/* ParticlesContainer::partition (src/particles/particles.cpp:332-339). */
+void or_partition(or_sim *s) {
+  or_calculate_hash(&s->grid, s->num_particles, s->positions, s->bins, s->hash_unsorted, s->hash_sorted);
+  or_sort_hashes(s->num_particles, s->hash_sorted, s->sorted_index);
+  or_bin_particles(&s->grid, s->num_particles, s->hash_sorted, s->cell_start, s->cell_end);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Shape functions                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* linear / derivative_linear (src/shapefunction/linear.cuh:28-52): the weight
+ * is evaluated in double and rounded; the derivative is 0 at r == 0 exactly. */
+static real sf_linear(real r) {
+  double ar = fabs((double)r);
+  if (ar >= 1.0) return (real)0.0;
+  return (real)(1.0 - ar);
+}
+static real sf_dlinear(real r, real inv_h) {
+  if (r > (real)1.0 || r < (real)-1.0 || r == (real)0.0) return (real)0.0;
+  if (r > (real)0.0) return -inv_h;
+  return inv_h;
+}
+
+/* Boundary-modified cubic B-spline (src/shapefunction/cubic.cuh:28-197),
+ * restated as Horner coefficient tables per node type and unit interval
+ * [-2,-1), [-1,0), [0,1), [1,2).  Weight: ((c3 r + c2) r + c1) r + c0;
+ * derivative: inv_h * ((d2 r + d1) r + d0).  Type 3 is the uniform cubic
+ * B-spline; types 1 (grid end) and 2 (next to the end) are the boundary
+ * variants; type 4 exists in the reference but is never assigned.  Evaluated
+ * in double, then rounded, as in the reference. */
+static const double CUBIC_W[5][4][4] = {
+    /* type 0: zero everywhere (node types are only set for cubic grids) */
+    {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},
+    /* type 1 */
+    {{1.0 / 6.0, 1.0, 2.0, 4.0 / 3.0}, {-1.0 / 6.0, 0.0, 1.0, 1.0},
+     {1.0 / 6.0, 0.0, -1.0, 1.0}, {-1.0 / 6.0, 1.0, -2.0, 4.0 / 3.0}},
+    /* type 2 */
+    {{0, 0, 0, 0}, {-1.0 / 3.0, -1.0, 0.0, 2.0 / 3.0},
+     {0.5, -1.0, 0.0, 2.0 / 3.0}, {-1.0 / 6.0, 1.0, -2.0, 4.0 / 3.0}},
+    /* type 3 */
+    {{1.0 / 6.0, 1.0, 2.0, 4.0 / 3.0}, {-0.5, -1.0, 0.0, 2.0 / 3.0},
+     {0.5, -1.0, 0.0, 2.0 / 3.0}, {-1.0 / 6.0, 1.0, -2.0, 4.0 / 3.0}},
+    /* type 4 */
+    {{1.0 / 6.0, 1.0, 2.0, 4.0 / 3.0}, {-0.5, -1.0, 0.0, 2.0 / 3.0},
+     {1.0 / 3.0, -1.0, 0.0, 2.0 / 3.0}, {0, 0, 0, 0}},
+};
+static const double CUBIC_D[5][4][3] = {
+    {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},
+    {{0.5, 2.0, 2.0}, {-0.5, 0.0, 1.0}, {0.5, 0.0, -1.0}, {-0.5, 2.0, -2.0}},
+    {{0, 0, 0}, {-1.0, -2.0, 0.0}, {1.5, -2.0, 0.0}, {-0.5, 2.0, -2.0}},
+    {{0.5, 2.0, 2.0}, {-1.5, -2.0, 0.0}, {1.5, -2.0, 0.0}, {-0.5, 2.0, -2.0}},
+    {{0.5, 2.0, 2.0}, {-1.5, -2.0, 0.0}, {1.0, -2.0, 0.0}, {0, 0, 0}},
+};
+static int cubic_interval(real r) {
+  if (r >= (real)-2.0 && r < (real)-1.0) return 0;
+  if (r >= (real)-1.0 && r < (real)0.0) return 1;
+  if (r >= (real)0.0 && r < (real)1.0) return 2;
+  if (r >= (real)1.0 && r < (real)2.0) return 3;
+  return -1;
+}
+static real sf_cubic(real r, int type) {
+  int k = cubic_interval(r);
+  if (k < 0 || type < 0 || type > 4) return (real)0.0;
+  const double *c = CUBIC_W[type][k];
+  double rd = (double)r;
+  return (real)(((c[0] * rd + c[1]) * rd + c[2]) * rd + c[3]);
+}
+static real sf_dcubic(real r, real inv_h, int type) {
+  int k = cubic_interval(r);
+  if (k < 0 || type < 0 || type > 4) return (real)0.0;
+  const double *c = CUBIC_D[type][k];
+  double rd = (double)r;
+  return (real)((double)inv_h * ((c[0] * rd + c[1]) * rd + c[2]));
+}
+
+/* Quadratic B-spline (no reference implementation: quadratic.cuh is a TODO).
+ * Uniform C1 quadratic B-spline of support 3h:
+ *   |r| < 1/2:        3/4 - r^2            d = -2 r
+ *   1/2 <= |r| < 3/2: (3/2 - |r|)^2 / 2    d = -sign(r) (3/2 - |r|)
+ * Boundary handling: a stencil node that falls outside the grid on an axis is
+ * folded onto the nearest grid node of that axis, so the weights of any
+ * particle inside the grid sum to one. */
+static real sf_quadratic(real r) {
+  real ar = (real)fabs((double)r);
+  if (ar < (real)0.5) return (real)((real)0.75 - r * r);
+  if (ar < (real)1.5) {
+    real t = (real)((real)1.5 - ar);
+    return (real)((real)0.5 * t * t);
+  }
+  return (real)0.0;
+}
+static real sf_dquadratic(real r, real inv_h) {
+  real ar = (real)fabs((double)r);
+  if (ar < (real)0.5) return (real)(inv_h * ((real)-2.0 * r));
+  if (ar < (real)1.5) {
+    real t = (real)((real)1.5 - ar);
+    return (real)(inv_h * (r > (real)0.0 ? -t : t));
+  }
+  return (real)0.0;
+}
+
+/* Target node of a particle slot.  Linear/cubic follow the reference exactly:
+ * node = flat(bin + w) as an unsigned index, valid iff < num_cells_total (so a
+ * slot that leaves the grid on one axis may alias into a neighbouring row, as
+ * in src/shapefunction/shapefunction.cpp:84-91 and
+ * src/solver/usl/usl_inline.h:114-126).  Quadratic clamps each axis (fold). */
+static int slot_target(const or_sim *s, const int b[3], const int w[3], int sel[3]) {
+  const or_grid *g = &s->grid;
+  int t[3];
+  for (int a = 0; a < 3; a++) {
+    sel[a] = b[a] + w[a];
+    t[a] = sel[a];
+    if (s->shape_function == OR_QUADRATIC && a < g->dim) {
+      if (t[a] < 0) t[a] = 0;
+      if (t[a] > g->num_cells[a] - 1) t[a] = g->num_cells[a] - 1;
+    }
+  }
+  unsigned int h = (unsigned int)flat3(g, t);
+  if (h >= (unsigned int)g->num_cells_total) return -1;
+  return (int)h;
+}
+
+/* shape_function_kernel (src/shapefunction/shapefunction.cpp:70-142):
+ * psi/dpsi per (particle, slot); relative coordinate
+ * (x - origin)*inv_h - selected_bin; products N0*N1[*N2]. */
+void or_shape_functions(or_sim *s) {
+  const or_grid *g = &s->grid;
+  int d = g->dim, nsn = s->nsn;
+  for (int i = 0; i < s->num_particles; i++) {
+    int b[3] = {0, 0, 0};
+    for (int a = 0; a < d; a++) b[a] = s->bins[i * d + a];
+    for (int sid = 0; sid < nsn; sid++) {
+      int w[3], sel[3];
+      window_offset(d, s->shape_function, sid, w);
+      int node = slot_target(s, b, w, sel);
+      if (node < 0) continue;
+      real N[3] = {1, 1, 1}, dN[3] = {0, 0, 0};
+      for (int a = 0; a < d; a++) {
+        real rel = (real)(s->positions[i * d + a] - g->origin[a]);
+        rel = (real)(rel * g->inv_cell_size);
+        rel = (real)(rel - (real)sel[a]);
+        if (s->shape_function == OR_LINEAR) {
+          N[a] = sf_linear(rel);
+          dN[a] = sf_dlinear(rel, g->inv_cell_size);
+        } else if (s->shape_function == OR_CUBIC) {
+          int type = s->node_types[3 * node + a];
+          N[a] = sf_cubic(rel, type);
+          dN[a] = sf_dcubic(rel, g->inv_cell_size, type);
+        } else {
+          N[a] = sf_quadratic(rel);
+          dN[a] = sf_dquadratic(rel, g->inv_cell_size);
+        }
+      }
+      real psi;
+      real dpsi[3] = {0, 0, 0};
+      if (d == 1) {
+        psi = N[0];
+        dpsi[0] = dN[0];
+      } else if (d == 2) {
+        psi = (real)(N[0] * N[1]);
+        dpsi[0] = (real)(dN[0] * N[1]);
+        dpsi[1] = (real)(dN[1] * N[0]);
+      } else {
+        psi = (real)((real)(N[0] * N[1]) * N[2]);
+        dpsi[0] = (real)((real)(dN[0] * N[1]) * N[2]);
+        dpsi[1] = (real)((real)(dN[1] * N[0]) * N[2]);
+        dpsi[2] = (real)((real)(dN[2] * N[0]) * N[1]);
+      }
+      s->psi[(size_t)i * nsn + sid] = psi;
+      for (int a = 0; a < d; a++) s->dpsi[((size_t)i * nsn + sid) * d + a] = dpsi[a];
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Particle set-up                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* calculate_initial_volumes (src/particles/particles.cpp:345-365):
+ * V = (REAL)pow(h, DIM) / ppc for particles whose volume is not set (> 0). */
+void or_initial_volumes(or_sim *s) {
+  int d = s->grid.dim;
+  for (int i = 0; i < s->num_particles; i++) {
+    if (s->volumes[i] > (real)0.0) continue;
+    real v = (real)pow((double)s->grid.cell_size, (double)d);
+    v = (real)(v / (real)s->particles_per_cell);
+    s->volumes[i] = v;
+  }
+  memcpy(s->volumes_original, s->volumes, sizeof(real) * (size_t)s->num_particles);
+}
+
+/* calculate_initial_masses (src/particles/particles.cpp:372-393). */
+void or_initial_masses(or_sim *s, int mat_id, REAL density) {
+  for (int i = 0; i < s->num_particles; i++) {
+    if ((int)s->colors[i] != mat_id || s->masses[i] > (real)0.0) continue;
+    s->masses[i] = (real)(density * s->volumes[i]);
+  }
+}
+
+/* USL::reset (src/solver/usl/usl.cpp:61-66) with NodesContainer::reset
+ * (src/nodes/nodes.cpp:183-188), ParticlesContainer::reset
+ * (src/particles/particles.cpp:162-175) and SpatialPartition::reset
+ * (src/spatialpartition/spatialpartition.cpp:77-86). */
+void or_reset(or_sim *s) {
+  int d = s->grid.dim;
+  size_t nn = (size_t)s->grid.num_cells_total, np = (size_t)s->num_particles;
+  memset(s->node_masses, 0, sizeof(real) * nn);
+  memset(s->node_moments, 0, sizeof(real) * nn * d);
+  memset(s->node_moments_nt, 0, sizeof(real) * nn * d);
+  memset(s->psi, 0, sizeof(real) * np * s->nsn);
+  memset(s->dpsi, 0, sizeof(real) * np * s->nsn * d);
+  memset(s->velocity_gradient, 0, sizeof(real) * np * d * d);
+  memset(s->forces_external, 0, sizeof(real) * np * d);
+  for (size_t i = 0; i < np; i++) s->sorted_index[i] = (int)i;
+  memset(s->cell_start, 0, sizeof(int) * nn);
+  memset(s->cell_end, 0, sizeof(int) * nn);
+  memset(s->bins, 0, sizeof(int) * np * d);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Boundary conditions                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* apply_planardomain (src/boundaryconditions/planardomain_inline.h:56-138):
+ * radius = 0.5 V^(1/D); overlap with each face -> f_ext += (m/dt^2) *
+ * overlap * (n - mu (v - (n.v) n)).  Friction is stored in radians and used
+ * as the coefficient directly, as in the reference. */
+static void planardomain(or_sim *s, const or_bc *bc) {
+  const or_grid *g = &s->grid;
+  int d = g->dim;
+  real inv_dim = (real)((real)1.0 / (real)d);
+  for (int i = 0; i < s->num_particles; i++) {
+    const real *x = s->positions + (size_t)i * d;
+    const real *v = s->velocities + (size_t)i * d;
+#ifdef OR_DOUBLE
+    double pv = pow((double)s->volumes[i], (double)inv_dim);
+#else
+    double pv = (double)powf((float)s->volumes[i], (float)inv_dim);
+#endif
+    real radius = (real)((real)0.5 * (real)pv);
+    real mass = s->masses[i];
+    real scale = (real)((double)mass / pow((double)s->dt, 2.0));
+    for (int face = 0; face < 2; face++) {
+      for (int a = 0; a < d; a++) {
+        real overlap = face == 0 ? (real)(radius - (real)(x[a] - g->origin[a]))
+                                 : (real)(radius - (real)(g->end[a] - x[a]));
+        if (!(overlap > (real)0.0)) continue;
+        real nrm[3] = {0, 0, 0};
+        nrm[a] = face == 0 ? (real)1.0 : (real)-1.0;
+        real mu = bc->r[3 * face + a];
+        real ndotv = 0;
+        for (int b = 0; b < d; b++) ndotv = (real)(ndotv + nrm[b] * v[b]);
+        for (int b = 0; b < d; b++) {
+          real tang = (real)(v[b] - (real)(ndotv * nrm[b]));
+          real fric = (real)(nrm[b] - (real)(mu * tang));
+          s->forces_external[(size_t)i * d + b] =
+              (real)(s->forces_external[(size_t)i * d + b] + (real)((real)(scale * overlap) * fric));
+        }
+      }
+    }
+  }
+}
+
+/* USL::solve step 5: BoundaryCondition::apply_on_particles over the list. */
+void or_apply_on_particles(or_sim *s) {
+  for (int k = 0; k < s->num_bcs; k++)
+    if (s->bcs[k].type == OR_BC_PLANARDOMAIN) planardomain(s, &s->bcs[k]);
+}
+
+/* Gravity::apply_on_nodes_moments (src/boundaryconditions/gravity.cpp:65-88)
+ * and apply_gravity (src/boundaryconditions/gravity_inline.h:46-63).  The ramp
+ * overwrites the stored gravity while step < ramp_step, so after the ramp the
+ * last ramp value stays in force (reproduced). */
+static void gravity(or_sim *s, or_bc *bc) {
+  int d = s->grid.dim;
+  int is_ramp = bc->i[0], ramp_step = bc->i[1];
+  real ramp_factor = (real)((real)s->global_step / (real)ramp_step);
+  if (is_ramp && s->global_step < ramp_step)
+    for (int a = 0; a < d; a++) bc->r[a] = (real)(bc->r[3 + a] * ramp_factor);
+  for (int n = 0; n < s->grid.num_cells_total; n++) {
+    real m = s->node_masses[n];
+    if (m <= (real)0.000000001) continue;
+    for (int a = 0; a < d; a++) {
+      real inc = (real)((real)(bc->r[a] * m) * s->dt);
+      s->node_moments_nt[(size_t)n * d + a] = (real)(s->node_moments_nt[(size_t)n * d + a] + inc);
+    }
+  }
+}
+
+/* apply_nodedomain (src/boundaryconditions/nodedomain_inline.h:40-87). */
+static void nodedomain(or_sim *s, const or_bc *bc) {
+  int d = s->grid.dim;
+  for (int n = 0; n < s->grid.num_cells_total; n++) {
+    if (s->node_masses[n] <= (real)0.00001) continue;
+    real *p = s->node_moments + (size_t)n * d;
+    real *q = s->node_moments_nt + (size_t)n * d;
+    for (int a = 0; a < d; a++) {
+      int id = s->node_ids[3 * n + a];
+      if (id < 1) {
+        if (bc->i[a] == 0) {
+          for (int b = 0; b < d; b++) p[b] = q[b] = (real)0.0;
+        } else if (bc->i[a] == 1) {
+          p[a] = (real)fmax(0.0, (double)p[a]);
+          q[a] = (real)fmax(0.0, (double)q[a]);
+        }
+      } else if (id >= s->grid.num_cells[a] - 1) {
+        if (bc->i[3 + a] == 0) {
+          for (int b = 0; b < d; b++) p[b] = q[b] = (real)0.0;
+        } else if (bc->i[3 + a] == 1) {
+          p[a] = (real)fmin(0.0, (double)p[a]);
+          q[a] = (real)fmin(0.0, (double)q[a]);
+        }
+      }
+    }
+  }
+}
+
+/* BodyForce::apply_on_nodes_moments (src/boundaryconditions/bodyforce.cpp:72-100)
+ * and apply_bodymoments (src/boundaryconditions/bodyforce_inline.h:41-59):
+ * "fixed" sets moments_nt, the other modes add to moments. */
+static void bodyforce(or_sim *s, const or_bc *bc) {
+  int d = s->grid.dim;
+  if (!bc->i[1]) return;
+  int fixed = bc->i[0] == 2;
+  for (int n = 0; n < s->grid.num_cells_total; n++) {
+    if (!bc->mask[n]) continue;
+    for (int a = 0; a < d; a++) {
+      if (fixed) s->node_moments_nt[(size_t)n * d + a] = bc->values[(size_t)n * d + a];
+      else s->node_moments[(size_t)n * d + a] = (real)(s->node_moments[(size_t)n * d + a] + bc->values[(size_t)n * d + a]);
+    }
+  }
+}
+
+/* USL::solve step 8 (src/solver/usl/usl.cpp:97-103): list order. */
+void or_apply_on_nodes_moments(or_sim *s) {
+  for (int k = 0; k < s->num_bcs; k++) {
+    or_bc *bc = &s->bcs[k];
+    if (bc->type == OR_BC_GRAVITY) gravity(s, bc);
+    else if (bc->type == OR_BC_NODEDOMAIN) nodedomain(s, bc);
+    else if (bc->type == OR_BC_BODYFORCE) bodyforce(s, bc);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* P2G / G2P                                                                */
+/* ------------------------------------------------------------------------ */
+
+/* usl_p2g_kernel (src/solver/usl/usl_inline.h:82-180).  The reference is a
+ * node-centric gather: for each node, for slot sid in order, for the particles
+ * of cell (node + p2g_window[sid]) in sorted order.  The same per-node
+ * summation order is produced here by a scatter with sid outermost and the
+ * sorted particle order inside; the target node is flat(bin) + flat(window)
+ * with the reference's single unsigned range check.  Per pair:
+ *   m += psi m_p;  p += (psi m_p) v_p;  f += psi f_ext - V_p (sigma_p [dpsi;0]) */
+void or_p2g(or_sim *s) {
+  const or_grid *g = &s->grid;
+  int d = g->dim, nsn = s->nsn;
+  size_t nn = (size_t)g->num_cells_total;
+  real *mass = (real *)calloc(nn, sizeof(real));
+  real *mom = (real *)calloc(nn * d, sizeof(real));
+  real *force = (real *)calloc(nn * d, sizeof(real));
+  for (int sid = 0; sid < nsn; sid++) {
+    int w[3];
+    window_offset(d, s->shape_function, sid, w);
+    for (int k = 0; k < s->num_particles; k++) {
+      int j = s->sorted_index[k];
+      if (s->hash_sorted[k] >= (unsigned int)g->num_cells_total) continue;
+      int b[3] = {0, 0, 0}, sel[3];
+      for (int a = 0; a < d; a++) b[a] = s->bins[j * d + a];
+      if (s->shape_function == OR_QUADRATIC) {
+        /* quadratic only: a particle binned outside the grid on any axis
+         * takes no part in P2G (no folding of whole particles) */
+        int out = 0;
+        for (int a = 0; a < d; a++)
+          if (b[a] < 0 || b[a] >= g->num_cells[a]) out = 1;
+        if (out) continue;
+      }
+      int node = slot_target(s, b, w, sel);
+      if (node < 0) continue;
+      real psi = s->psi[(size_t)j * nsn + sid];
+      const real *dpsi = s->dpsi + ((size_t)j * nsn + sid) * d;
+      real sm = (real)(psi * s->masses[j]);
+      mass[node] = (real)(mass[node] + sm);
+      for (int a = 0; a < d; a++)
+        mom[node * d + a] = (real)(mom[node * d + a] + (real)(sm * s->velocities[(size_t)j * d + a]));
+      for (int a = 0; a < d; a++)
+        force[node * d + a] = (real)(force[node * d + a] + (real)(psi * s->forces_external[(size_t)j * d + a]));
+      real mv = (real)(-1.0 * (double)s->volumes[j]);
+      const real *sig = s->stresses + (size_t)j * 9;
+      real dp3[3] = {0, 0, 0};
+      for (int a = 0; a < d; a++) dp3[a] = dpsi[a];
+      for (int a = 0; a < d; a++) {
+        real acc = (real)((real)(mv * sig[3 * a + 0]) * dp3[0]);
+        acc = (real)(acc + (real)((real)(mv * sig[3 * a + 1]) * dp3[1]));
+        acc = (real)(acc + (real)((real)(mv * sig[3 * a + 2]) * dp3[2]));
+        force[node * d + a] = (real)(force[node * d + a] + acc);
+      }
+    }
+  }
+  for (size_t n = 0; n < nn; n++) {
+    if (mass[n] <= s->small_mass_cutoff) continue;
+    s->node_masses[n] = mass[n];
+    for (int a = 0; a < d; a++) {
+      s->node_moments[n * d + a] = mom[n * d + a];
+      s->node_moments_nt[n * d + a] = (real)(mom[n * d + a] + (real)(force[n * d + a] * s->dt));
+    }
+  }
+  free(mass);
+  free(mom);
+  free(force);
+}
+
+/* Determinant: 2x2 as m00 m11 - m10 m01; 3x3 by cofactors of the first row. */
+static real det(int d, const real *A) {
+  if (d == 1) return A[0];
+  if (d == 2) return (real)((real)(A[0] * A[3]) - (real)(A[2] * A[1]));
+  real c0 = (real)((real)(A[4] * A[8]) - (real)(A[5] * A[7]));
+  real c1 = (real)((real)(A[3] * A[8]) - (real)(A[5] * A[6]));
+  real c2 = (real)((real)(A[3] * A[7]) - (real)(A[4] * A[6]));
+  return (real)((real)((real)(A[0] * c0) - (real)(A[1] * c1)) + (real)(A[2] * c2));
+}
+
+/* usl_g2p_kernel (src/solver/usl/usl_inline.h:245-332): slots leaving the grid
+ * on any axis, or hitting a node with m <= cutoff, are skipped.
+ *   dv += psi (v_nt - v_n);  v_pic += psi v_nt;  L += dpsi v_nt^T
+ *   v <- (1 - alpha) v_pic + alpha (v + dv);  x += dt v_pic;
+ *   F <- (I + L dt) F;  V = det(F) V0 */
+void or_g2p(or_sim *s) {
+  const or_grid *g = &s->grid;
+  int d = g->dim, nsn = s->nsn;
+  real one_minus_alpha = (real)(1.0 - (double)s->alpha);
+  for (int i = 0; i < s->num_particles; i++) {
+    int b[3] = {0, 0, 0};
+    for (int a = 0; a < d; a++) b[a] = s->bins[i * d + a];
+    real vinc[3] = {0, 0, 0}, dvinc[3] = {0, 0, 0}, L[9] = {0};
+    for (int sid = 0; sid < nsn; sid++) {
+      int w[3], sel[3];
+      window_offset(d, s->shape_function, sid, w);
+      int node = slot_target(s, b, w, sel);
+      if (s->shape_function != OR_QUADRATIC) {
+        int invalid = 0;
+        for (int a = 0; a < d; a++)
+          if (sel[a] < 0 || sel[a] >= g->num_cells[a]) invalid = 1;
+        if (invalid) continue;
+      }
+      if (node < 0) continue;
+      real m = s->node_masses[node];
+      if (m <= s->small_mass_cutoff) continue;
+      real psi = s->psi[(size_t)i * nsn + sid];
+      const real *dpsi = s->dpsi + ((size_t)i * nsn + sid) * d;
+      real vn[3], vnt[3];
+      for (int a = 0; a < d; a++) {
+        vn[a] = (real)(s->node_moments[(size_t)node * d + a] / m);
+        vnt[a] = (real)(s->node_moments_nt[(size_t)node * d + a] / m);
+      }
+      for (int a = 0; a < d; a++) {
+        dvinc[a] = (real)(dvinc[a] + (real)(psi * (real)(vnt[a] - vn[a])));
+        vinc[a] = (real)(vinc[a] + (real)(psi * vnt[a]));
+      }
+      for (int a = 0; a < d; a++)
+        for (int c = 0; c < d; c++) L[a * d + c] = (real)(L[a * d + c] + (real)(dpsi[a] * vnt[c]));
+    }
+    real *v = s->velocities + (size_t)i * d;
+    real *x = s->positions + (size_t)i * d;
+    for (int a = 0; a < d; a++) {
+      v[a] = (real)((real)(one_minus_alpha * vinc[a]) + (real)(s->alpha * (real)(v[a] + dvinc[a])));
+    }
+    memcpy(s->velocity_gradient + (size_t)i * d * d, L, sizeof(real) * d * d);
+    for (int a = 0; a < d; a++) x[a] = (real)(x[a] + (real)(s->dt * vinc[a]));
+    real A[9], Fn[9];
+    real *F = s->F + (size_t)i * d * d;
+    for (int a = 0; a < d; a++)
+      for (int c = 0; c < d; c++) A[a * d + c] = (real)((a == c ? (real)1.0 : (real)0.0) + (real)(L[a * d + c] * s->dt));
+    for (int a = 0; a < d; a++)
+      for (int c = 0; c < d; c++) {
+        real acc = (real)(A[a * d + 0] * F[0 * d + c]);
+        for (int k = 1; k < d; k++) acc = (real)(acc + (real)(A[a * d + k] * F[k * d + c]));
+        Fn[a * d + c] = acc;
+      }
+    memcpy(F, Fn, sizeof(real) * d * d);
+    s->volumes[i] = (real)(det(d, F) * s->volumes_original[i]);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Materials                                                                */
+/* ------------------------------------------------------------------------ */
+
+/* update_linearelastic (src/materials/linearelastic_inline.h:40-107):
+ * deps = 0.5 (L + L^T) dt; sigma_DIM += lame*deps*I + 2G*deps.  "lame * deps *
+ * I" is a matrix product, so the reference adds (lame + 2G) deps (kept by
+ * default).  corrected=1 gives the textbook lame tr(deps) I + 2G deps, with
+ * sigma_zz += lame tr(deps) in 2D (plane strain). */
+static void le_point(int d, const real *L, real *sig, real dt, const or_material *m) {
+  real lame = m->p[2], shear = m->p[3];
+  int corrected = m->p[5] != (real)0.0;
+  real two_g = (real)(2.0 * (double)shear);
+  real deps[9];
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++)
+      deps[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] + L[b * d + a])) * dt);
+  real tr = 0;
+  for (int a = 0; a < d; a++) tr = (real)(tr + deps[a * d + a]);
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real inc;
+      if (corrected)
+        inc = (real)((a == b ? (real)(lame * tr) : (real)0.0) + (real)(two_g * deps[a * d + b]));
+      else
+        inc = (real)((real)(lame * deps[a * d + b]) + (real)(two_g * deps[a * d + b]));
+      sig[3 * a + b] = (real)(sig[3 * a + b] + inc);
+    }
+  if (corrected && d == 2) sig[8] = (real)(sig[8] + (real)(lame * tr));
+}
+
+/* stress_update_newtonfluid (src/materials/newtonfluid_inline.h:49-96):
+ * rho = m/V, rho0 = m/V0, p = -K((rho/rho0)^gamma - 1); sigma = p I_DIM +
+ * (2 mu / 3) dev(D) on the DIM x DIM block only (other entries 0). */
+static void nf_point(int d, const real *L, real *sig, real mass, real vol, real vol0, const or_material *m) {
+  real visc = m->p[0], bulk = m->p[1], gamma = m->p[2];
+  real rho = (real)(mass / vol), rho0 = (real)(mass / vol0);
+#ifdef OR_DOUBLE
+  real pw = (real)pow(rho / rho0, gamma);
+#else
+  real pw = (real)powf((float)(rho / rho0), (float)gamma);
+#endif
+  real pressure = (real)(-bulk * (real)(pw - (real)1.0));
+  real D[9];
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) D[a * d + b] = (real)((real)0.5 * (real)(L[a * d + b] + L[b * d + a]));
+  real tr = 0;
+  for (int a = 0; a < d; a++) tr = (real)(tr + D[a * d + a]);
+  real third = (real)(1.0 / 3.0);
+  real coef = (real)(2.0 * (double)visc / 3.0);
+  for (int k = 0; k < 9; k++) sig[k] = (real)0.0;
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real dev = (real)(D[a * d + b] - (a == b ? (real)((real)(third * tr)) : (real)0.0));
+      real iso = a == b ? pressure : (real)0.0;
+      sig[3 * a + b] = (real)(iso + (real)(dev * coef));
+    }
+}
+
+/* Drucker-Prager cone + apex return mapping, restating update_dp_rheo
+ * (src/materials/dp_rheo_inline.h:123-246) with return_mapping_cone (:50-65),
+ * return_mapping_apex (:67-78) and update_plasticity (:80-96):
+ *   deps = sym(L) dt - W eps_e + eps_e W,  W = skew(L) dt
+ *   eps_tr = eps_e + deps;  p_tr = p_ref + K tr(eps_tr)
+ *   s_tr = s_ref + 2G dev(eps_tr)  (zz deviator zeroed in 2D)
+ *   Phi = sqrt(J2) + eta p_tr - kc;  elastic if Phi <= 0
+ *   cone: dgamma = Phi/(K eta eta_bar + G); p = p_tr - K eta_bar dgamma;
+ *         s = (1 - G dgamma / sqrt(J2)) s_tr
+ *   apex (sqrt(J2) - G dgamma < 0): s = 0, p = p_apex
+ *   eps_e = (s - s_ref)/2G + (p - p_ref)/(3K) I  (DIM x DIM block)
+ * The reference writes eta (p - Pt); with kc = eta*Pt and p_apex = Pt the two
+ * agree.  For eta_bar > 0 the reference's apex formula yields p = Pt, which is
+ * p_apex here; for eta_bar = 0 (no dilatancy) the reference divides by zero,
+ * while this step keeps the limit p = p_apex.
+ * p = {K, G, eta, eta_bar, kc, p_apex, has_apex}. */
+void or_dp_point(int d, const REAL *L, REAL *sig, REAL *eps_e, const REAL *sref, REAL dt,
+                 const REAL *p, int velgrad_is_strain_increment) {
+  real K = p[0], G = p[1], eta = p[2], eta_bar = p[3], kc = p[4], p_apex = p[5];
+  int has_apex = p[6] != (real)0.0;
+  real deps[9];
+  if (velgrad_is_strain_increment) {
+    for (int k = 0; k < d * d; k++) deps[k] = L[k];
+  } else {
+    real W[9];
+    for (int a = 0; a < d; a++)
+      for (int b = 0; b < d; b++) {
+        deps[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] + L[b * d + a])) * dt);
+        W[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] - L[b * d + a])) * dt);
+      }
+    for (int a = 0; a < d; a++)
+      for (int b = 0; b < d; b++) {
+        real we = 0, ew = 0;
+        for (int k = 0; k < d; k++) {
+          we = (real)(we + (real)(W[a * d + k] * eps_e[k * d + b]));
+          ew = (real)(ew + (real)(eps_e[a * d + k] * W[k * d + b]));
+        }
+        deps[a * d + b] = (real)(deps[a * d + b] + (real)(-we + ew));
+      }
+  }
+  real p_ref = (real)((real)(1.0 / 3.0) * (real)((real)(sref[0] + sref[4]) + sref[8]));
+  real s_ref[9];
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] = (real)(s_ref[0] - p_ref);
+  s_ref[4] = (real)(s_ref[4] - p_ref);
+  s_ref[8] = (real)(s_ref[8] - p_ref);
+  real eps_tr[9];
+  for (int k = 0; k < d * d; k++) eps_tr[k] = (real)(eps_e[k] + deps[k]);
+  real ev = 0;
+  for (int a = 0; a < d; a++) ev = (real)(ev + eps_tr[a * d + a]);
+  real p_tr = (real)(p_ref + (real)(K * ev));
+  real edev[9] = {0};
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) edev[3 * a + b] = eps_tr[a * d + b];
+  real third_ev = (real)((real)(1.0 / 3.0) * ev);
+  for (int a = 0; a < 3; a++) edev[3 * a + a] = (real)(edev[3 * a + a] - third_ev);
+  if (d < 3) edev[8] = (real)0.0;
+  real two_g = (real)(2.0 * (double)G);
+  real s_tr[9];
+  for (int k = 0; k < 9; k++) s_tr[k] = (real)(s_ref[k] + (real)(two_g * edev[k]));
+  real ss = 0;
+  for (int k = 0; k < 9; k++) ss = (real)(ss + (real)(s_tr[k] * s_tr[k]));
+  real J2 = (real)((real)0.5 * ss);
+  real sqrtJ2 = (real)sqrt((double)J2);
+  real Phi = (real)((real)(sqrtJ2 + (real)(eta * p_tr)) - kc);
+  if (Phi <= (real)0.0) {
+    for (int k = 0; k < 9; k++) sig[k] = s_tr[k];
+    sig[0] = (real)(sig[0] + p_tr);
+    sig[4] = (real)(sig[4] + p_tr);
+    sig[8] = (real)(sig[8] + p_tr);
+    for (int k = 0; k < d * d; k++) eps_e[k] = eps_tr[k];
+    return;
+  }
+  double dgamma = (double)Phi / ((double)K * (double)eta * (double)eta_bar + (double)G);
+  double p_next = (double)p_tr - (double)K * (double)eta_bar * dgamma;
+  real s_next[9];
+  int apex = has_apex && ((double)sqrtJ2 - (double)G * dgamma < 0.0);
+  if (apex) {
+    p_next = (double)p_apex;
+    for (int k = 0; k < 9; k++) s_next[k] = (real)0.0;
+  } else {
+    double scale = 1.0 - ((double)G * dgamma) / (double)sqrtJ2;
+    for (int k = 0; k < 9; k++) s_next[k] = (real)(scale * (double)s_tr[k]);
+  }
+  real pn = (real)p_next;
+  for (int k = 0; k < 9; k++) sig[k] = s_next[k];
+  sig[0] = (real)(sig[0] + pn);
+  sig[4] = (real)(sig[4] + pn);
+  sig[8] = (real)(sig[8] + pn);
+  double inv2g = 1.0 / (2.0 * (double)G);
+  real dpk = (real)(((double)pn - (double)p_ref) / (3.0 * (double)K));
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real e = (real)((double)(real)(s_next[3 * a + b] - s_ref[3 * a + b]) * inv2g);
+      if (a == b) e = (real)(e + dpk);
+      eps_e[a * d + b] = e;
+    }
+}
+
+/* Solver::stress_update (src/solver/solver.cpp:110-121): materials in list
+ * order, each over all particles of its colour (LE and NF skip inactive
+ * particles; the reference DP kernel does not check the flag). */
+void or_stress_update(or_sim *s) {
+  int d = s->grid.dim;
+  for (int mid = 0; mid < s->num_materials; mid++) {
+    const or_material *m = &s->materials[mid];
+    for (int i = 0; i < s->num_particles; i++) {
+      if ((int)s->colors[i] != mid) continue;
+      const real *L = s->velocity_gradient + (size_t)i * d * d;
+      real *sig = s->stresses + (size_t)i * 9;
+      if (m->type == OR_MAT_LINEAR_ELASTIC) {
+        if (!s->is_active[i]) continue;
+        le_point(d, L, sig, s->dt, m);
+      } else if (m->type == OR_MAT_NEWTON_FLUID) {
+        if (!s->is_active[i]) continue;
+        nf_point(d, L, sig, s->masses[i], s->volumes[i], s->volumes_original[i], m);
+      } else if (m->type == OR_MAT_DRUCKER_PRAGER) {
+        or_dp_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->dt, m->p, 0);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* One USL step                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* USL::solve (src/solver/usl/usl.cpp:69-115).  apply_on_nodes_f_ext has no
+ * override in any boundary condition on this path, and the second
+ * apply_on_particles call only writes f_ext, which the next reset clears. */
+void or_solve(or_sim *s) {
+  or_reset(s);
+  or_partition(s);
+  or_shape_functions(s);
+  or_apply_on_particles(s);
+  or_p2g(s);
+  or_apply_on_nodes_moments(s);
+  or_g2p(s);
+  or_stress_update(s);
+}
+
+/* Solver::solve_nsteps (src/solver/solver.cpp:125-134): solve, then
+ * increment_global (src/common/global_settings.cpp:220-227). */
+void or_solve_nsteps(or_sim *s, int nsteps) {
+  for (int k = 0; k < nsteps; k++) {
+    or_solve(s);
+    s->global_step += 1;
+  }
+}
