@@ -1,0 +1,338 @@
+"""Benchmark of the USL MPM step: particle-steps/s on B200.
+
+Default workload: the 3D granular column collapse (1,331,712 particles,
+Drucker-Prager, quadratic B-splines, gravity, slip walls, 257x65x129 nodes,
+dt 1e-5), the configuration the headline metric is quoted on.  Synthetic,
+seeded particle set (numpy PCG64 seed 0).  The particle state (~154 MB) is
+larger than the 126 MB L2, so no flush is needed between timed steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs one independent replica per GPU (the path does not shard at this
+size; no collective on the data path), launched by torch.distributed.run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1xB200: plain vs batched vs fwd+adjoint, <=1e-4 rel err vs FP64"
+# algorithmic bytes per particle-step of the whole step (FP32 SoA state read
+# and written once; symmetric tensors 6 floats in 3D)
+STEP_BYTES = {("3d", "dp"): 224, ("2d", "le"): 96, ("2d", "dp"): 120}
+
+
+def load_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def scene_for(config, scale=1.0):
+    from pyroclastmpm_b200 import scenes
+
+    if config == "column":
+        return scenes.granular_column(scale=scale)
+    if config == "discs":
+        return scenes.two_discs()
+    if config == "bed":
+        return scenes.granular_bed(scale=scale)
+    raise ValueError(config)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, value):
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_reference(config, steps, warmup, sample_scale):
+    """The oracle (C restatement of the reference step, one thread) on a
+    bounded sample of the workload: the same grid, the particle region scaled
+    by sample_scale per axis."""
+    import oracle
+    from pyroclastmpm_b200 import scenes
+
+    scene = scene_for(config, scale=sample_scale)
+    ref = oracle.OracleSim(**scenes.sim_kwargs(scene), positions=scene["positions"],
+                           velocities=scene["velocities"]).initialize()
+    for _ in range(warmup):
+        ref.solve(1)
+    t0 = time.perf_counter()
+    ref.solve(steps)
+    dt = time.perf_counter() - t0
+    n = len(scene["positions"])
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{n} particles ({config} particle region scaled {sample_scale:g} per axis, same grid), "
+                      f"{steps} steps after {warmup} warm-up, serial C oracle (FP32)",
+            "seconds": dt}
+
+
+def run_reference(args, world, rank, pg):
+    line = None
+    if rank == 0:
+        cb = cpu_reference(args.config, args.steps, args.warmup, args.ref_sample_scale)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "particle-steps/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * cb["seconds"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": workload_name(args.config), "sample": cb["sample"]},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def workload_name(config):
+    return {"column": "granular column collapse 3D, Drucker-Prager, quadratic B-spline, 1,331,712 particles, "
+                      "257x65x129 nodes, gravity + slip walls, dt 1e-5",
+            "discs": "two-disc elastic impact 2D, linear, 2,528 particles, 51x51 nodes, dt 1e-3",
+            "bed": "granular bed 3D, Drucker-Prager, cubic B-spline, 4,915,200 particles, 241x97x129 nodes, dt 8e-6"
+            }[config]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="column", choices=["column", "discs", "bed"])
+    ap.add_argument("--resort-interval", type=int, default=32)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--ref-sample-scale", type=float, default=0.45)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import torch
+
+    from pyroclastmpm_b200 import Simulation, scenes
+
+    torch.cuda.set_device(local)
+    scene = scene_for(args.config)
+    kw = scenes.sim_kwargs(scene)
+    sim = Simulation(**kw, device=local, resort_interval=args.resort_interval)
+    sim.set_particles(scene["positions"], scene["velocities"])
+    sim.initialize()
+    n = sim.n
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+
+    for _ in range(args.warmup):
+        sim.solve(1)
+    status = sim.synchronize()
+    if status != 0:
+        raise RuntimeError(f"device fault during warm-up: {status}")
+
+    # ---- timed region: K steps, device time on the simulation's stream ----
+    barrier(pg)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = sim.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sim.solve(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(pg)
+    launches = sim.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_max = allreduce_max(pg, ms)
+    status = sim.synchronize()
+    if status != 0:
+        raise RuntimeError(f"device fault in the timed region: {status}")
+    value = world * n * args.steps / (ms_max / 1000.0)
+
+    # ---- per-phase times (CUDA events inside the library, same stream) ----
+    phases = np.zeros(3)
+    nprof = 5
+    for _ in range(nprof):
+        p, _nl = sim.profile_step()
+        phases += np.array(p)
+    phases /= nprof
+    active = sim.active_nodes()
+    dim = scene["dim"]
+    peak, peak_kind = load_peak()
+    step_bytes = STEP_BYTES[("3d", "dp")] if dim == 3 else STEP_BYTES[("2d", "le")]
+    grid_bytes = 16 * dim * active
+    # algorithmic bytes per launch of each phase
+    phase_names = ["partition", "p2g", "g2p_stress"]
+    st = 4
+    if dim == 3:
+        p2g_bytes = n * st * (3 + 3 + 1 + 1 + 6) + active * st * 2 * dim
+        g2p_bytes = n * st * (3 + 3 + 9 + 6 + 1 + (3 + 3 + 9 + 6 + 6 + 1)) + n * 1 + active * st * 2 * dim
+    else:
+        p2g_bytes = n * st * (2 + 2 + 1 + 1 + 4) + active * st * 2 * dim
+        g2p_bytes = n * st * (2 + 2 + 4 + 4 + 1 + (2 + 2 + 4 + 4 + 1)) + n * 1 + active * st * 2 * dim
+    part_bytes = n * st * (dim + 1 + 1) + sim.num_nodes * st * 2
+    algo = {"partition": part_bytes, "p2g": p2g_bytes, "g2p_stress": g2p_bytes}
+    dom = int(np.argmax(phases))
+    dom_name = phase_names[dom]
+    achieved = algo[dom_name] / (phases[dom] / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.config, {}).get(dom_name)
+        except Exception:
+            traffic = None
+    step_ms = ms_max / args.steps
+    step_achieved = (step_bytes * n + grid_bytes) / (step_ms / 1000.0) / 1e9
+
+    # ---- end to end through the C ABI with host buffers ----
+    pin_x = torch.empty((n, dim), dtype=torch.float32, pin_memory=True)
+    pin_v = torch.empty((n, dim), dtype=torch.float32, pin_memory=True)
+    pin_x.copy_(torch.from_numpy(sim.get("positions")))
+    pin_v.copy_(torch.from_numpy(sim.get("velocities")))
+    nbytes = n * dim * 4
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        sim.set_ptr("positions", pin_x.data_ptr(), nbytes)
+        sim.set_ptr("velocities", pin_v.data_ptr(), nbytes)
+        sim.solve(1)
+        sim.get_ptr("positions", pin_x.data_ptr(), nbytes)
+        sim.get_ptr("velocities", pin_v.data_ptr(), nbytes)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = allreduce_max(pg, e0.elapsed_time(e1) / args.e2e_steps)
+    e2e_value = world * n / (e2e_ms / 1000.0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference(args.config, args.cpu_steps, 0, 1.0)
+        cpu.pop("seconds", None)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, numpy PCG64)",
+            "config": {"workload": workload_name(args.config), "particles_per_gpu": n, "grid_nodes": sim.num_nodes,
+                       "active_nodes": active, "resort_interval": args.resort_interval,
+                       "l2": "state larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": traffic, "algorithmic_bytes_per_launch": algo[dom_name],
+                         "ms_per_launch": float(phases[dom])},
+            "step_roofline": {"achieved": step_achieved, "peak": peak, "unit": "GB/s",
+                              "frac": step_achieved / peak,
+                              "bytes_per_particle_step": step_bytes, "grid_bytes_per_step": grid_bytes},
+            "phases_ms": dict(zip(phase_names, [float(x) for x in phases])),
+            "clocks": clocks, "gpu_launches": int(launches),
+            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 2 * nbytes,
+                    "d2h_bytes_per_step": 2 * nbytes,
+                    "note": "per step: positions + velocities uploaded from pinned host memory, one step, "
+                            "positions + velocities read back"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,306 @@
+/*
+ * pmpm.h - C ABI of the B200-native update-stress-last (USL) MPM step.
+ *
+ * Drop-in replacement for the hot path of PyroclastMPM's USL solver.  Every
+ * entry point names the reference interface it stands in for (paths relative
+ * to the PyroclastMPM project root).  All state lives in one opaque handle
+ * (no process globals), so several simulations may coexist in one process;
+ * one handle must not be used from two host threads at once.
+ *
+ * Conventions
+ *  - Every call returns an int status (pmpm_status); nothing calls exit().
+ *  - Host arrays use the reference container layouts, particles in the order
+ *    they were given (the "id" order), row-major:
+ *      vectors [n][dim], stresses [n][3][3], F / velocity_gradient [n][dim][dim],
+ *      node vectors [num_nodes][dim], node ids [num_nodes][3].
+ *  - Kernels run on the handle's stream; calls that return data synchronise.
+ *    Device faults of the step (a particle outside the grid, non-finite
+ *    state) are accumulated on the device and reported by pmpm_synchronize.
+ *  - Arithmetic is FP32, as the reference's DOUBLE_PRECISION=OFF build.
+ */
+#ifndef PMPM_H
+#define PMPM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMPM_MAX_MATERIALS 16
+#define PMPM_MAX_BCS 16
+
+typedef enum {
+  PMPM_OK = 0,
+  PMPM_ERR_INVALID_ARGUMENT = 1,
+  PMPM_ERR_CUDA = 2,
+  PMPM_ERR_OUT_OF_MEMORY = 3,
+  PMPM_ERR_NOT_SUPPORTED = 4,
+  PMPM_ERR_STATE = 5,          /* call order: e.g. a step before particles exist */
+  PMPM_ERR_OUT_OF_DOMAIN = 16, /* a particle's cell lies outside the grid        */
+  PMPM_ERR_NONFINITE = 17,     /* NaN or Inf appeared in particle positions      */
+  PMPM_ERR_CELL_OVERFLOW = 18  /* more particles in one cell than the sort holds */
+} pmpm_status;
+
+/* Shape functions: numbering of the reference SFType
+ * (include/pyroclastmpm/common/types_common.h:151-156).  Quadratic has no
+ * reference implementation (src/shapefunction/quadratic.cuh is empty). */
+enum { PMPM_SHAPE_LINEAR = 0, PMPM_SHAPE_QUADRATIC = 1, PMPM_SHAPE_CUBIC = 2 };
+
+/* Materials: the reference MaterialType variant
+ * (include/pyroclastmpm/solver/solver.h:76-78) members on this path, plus
+ * Drucker-Prager (cone + apex return mapping). */
+enum {
+  PMPM_MAT_NONE = 0,            /* Material base: stress untouched            */
+  PMPM_MAT_LINEAR_ELASTIC = 1,  /* src/materials/linearelastic_inline.h:40-107 */
+  PMPM_MAT_NEWTON_FLUID = 2,    /* src/materials/newtonfluid_inline.h:49-96    */
+  PMPM_MAT_DRUCKER_PRAGER = 3   /* src/materials/dp_rheo_inline.h:123-246      */
+};
+
+/* Boundary conditions: the reference BoundaryConditionType members on this
+ * path (include/pyroclastmpm/solver/solver.h:80-82). */
+enum {
+  PMPM_BC_GRAVITY = 1,      /* src/boundaryconditions/gravity.cpp:65-88            */
+  PMPM_BC_NODEDOMAIN = 2,   /* src/boundaryconditions/nodedomain_inline.h:40-87    */
+  PMPM_BC_BODYFORCE = 3,    /* src/boundaryconditions/bodyforce_inline.h:41-59     */
+  PMPM_BC_PLANARDOMAIN = 4  /* src/boundaryconditions/planardomain_inline.h:56-138 */
+};
+
+/* Step flags. */
+enum {
+  /* keep the velocity gradient L of the last step in device memory (needed
+   * for the velocity_gradient getter; the step itself does not need it) */
+  PMPM_FLAG_KEEP_VELOCITY_GRADIENT = 1u << 0
+};
+
+/* Material parameters; fill with the pmpm_material_* helpers.
+ *   LINEAR_ELASTIC: {E, pois, lame, shear, bulk, corrected}
+ *   NEWTON_FLUID:   {viscosity, bulk_modulus, gamma}
+ *   DRUCKER_PRAGER: {K, G, eta, eta_bar, kc, p_apex, has_apex}
+ *                   yield sqrt(J2) + eta p - kc (p = tr(sigma)/3) */
+typedef struct {
+  int type;
+  float density;
+  float params[8];
+} pmpm_material;
+
+/* Boundary-condition parameters; fill with the pmpm_bc_* helpers.
+ *   GRAVITY:      reals[0..2] gravity, reals[3..5] gravity_end,
+ *                 ints[0] is_ramp, ints[1] ramp_step
+ *   NODEDOMAIN:   ints[0..2] face0_mode, ints[3..5] face1_mode (0 stick, 1 slip)
+ *   BODYFORCE:    ints[0] mode (0 forces, 1 moments, 2 fixed), ints[1] active,
+ *                 values [num_nodes][dim] and mask [num_nodes] (host, copied)
+ *   PLANARDOMAIN: reals[0..2] face0 friction, reals[3..5] face1 friction
+ *                 (radians; the pmpm_bc_planardomain helper converts degrees) */
+typedef struct {
+  int type;
+  int ints[8];
+  float reals[12];
+  const float *values;
+  const unsigned char *mask;
+} pmpm_bc;
+
+/* Everything the reference keeps in NodesContainer/Grid, the process-global
+ * settings (set_globals, src/common/global_settings.cpp:161-176) and the
+ * Solver's material/BC lists (src/solver/solver.cpp:69-104). */
+typedef struct {
+  int dim;                 /* 2 or 3 */
+  float origin[3];
+  float end[3];
+  float cell_size;
+  int shape_function;      /* PMPM_SHAPE_* */
+  float dt;
+  int particles_per_cell;
+  float alpha;             /* FLIP/PIC blend, reference default 0.99 */
+  int num_materials;
+  const pmpm_material *materials;
+  int num_bcs;
+  const pmpm_bc *bcs;      /* applied in list order, as the reference */
+  unsigned flags;          /* PMPM_FLAG_* */
+  int device;              /* CUDA device ordinal */
+  void *stream;            /* cudaStream_t; NULL: the handle creates its own */
+  int resort_interval;     /* steps between physical re-sorts of particle
+                              storage by cell (0: never); default 32 */
+} pmpm_desc;
+
+typedef struct pmpm_sim pmpm_sim;
+
+/* Field ids for pmpm_get_field / pmpm_set_field (reference member names). */
+typedef enum {
+  PMPM_FIELD_POSITIONS = 0,          /* float [n][dim]    ParticlesContainer::positions_gpu        */
+  PMPM_FIELD_VELOCITIES = 1,         /* float [n][dim]    ::velocities_gpu                         */
+  PMPM_FIELD_STRESSES = 2,           /* float [n][3][3]   ::stresses_gpu                           */
+  PMPM_FIELD_F = 3,                  /* float [n][dim][dim] ::F_gpu                                */
+  PMPM_FIELD_VELOCITY_GRADIENT = 4,  /* float [n][dim][dim] ::velocity_gradient_gpu                */
+  PMPM_FIELD_MASSES = 5,             /* float [n]         ::masses_gpu                             */
+  PMPM_FIELD_VOLUMES = 6,            /* float [n]         ::volumes_gpu                            */
+  PMPM_FIELD_VOLUMES_ORIGINAL = 7,   /* float [n]         ::volumes_original_gpu                   */
+  PMPM_FIELD_COLORS = 8,             /* uint8 [n]         ::colors_gpu                             */
+  PMPM_FIELD_IS_RIGID = 9,           /* uint8 [n]         ::is_rigid_gpu                           */
+  PMPM_FIELD_IS_ACTIVE = 10,         /* uint8 [n]         ::is_active_gpu                          */
+  PMPM_FIELD_FORCES_EXTERNAL = 11,   /* float [n][dim]    ::forces_external_gpu                    */
+  PMPM_FIELD_EPS_E = 12,             /* float [n][dim][dim] Drucker-Prager elastic strain          */
+  PMPM_FIELD_STRESS_REF = 13,        /* float [n][3][3]   Drucker-Prager reference stress          */
+  PMPM_FIELD_NODE_MASSES = 20,       /* float [nodes]     NodesContainer::masses_gpu               */
+  PMPM_FIELD_NODE_MOMENTS = 21,      /* float [nodes][dim] ::moments_gpu                           */
+  PMPM_FIELD_NODE_MOMENTS_NT = 22,   /* float [nodes][dim] ::moments_nt_gpu                        */
+  PMPM_FIELD_NODE_IDS = 23,          /* int   [nodes][3]  ::node_ids_gpu (unused axes 0)           */
+  PMPM_FIELD_NODE_TYPES = 24,        /* int   [nodes][3]  ::node_types_gpu                         */
+  PMPM_FIELD_BINS = 30,              /* int   [n][dim]    SpatialPartition::bins_gpu               */
+  PMPM_FIELD_HASH_UNSORTED = 31,     /* uint32 [n]        ::hash_unsorted_gpu                      */
+  PMPM_FIELD_HASH_SORTED = 32,       /* uint32 [n]        ::hash_sorted_gpu                        */
+  PMPM_FIELD_SORTED_INDEX = 33,      /* int   [n]         ::sorted_index_gpu                       */
+  PMPM_FIELD_CELL_START = 34,        /* int   [nodes]     ::cell_start_gpu (0 for empty cells)     */
+  PMPM_FIELD_CELL_END = 35           /* int   [nodes]     ::cell_end_gpu (0 for empty cells)       */
+} pmpm_field;
+
+/* Human-readable status text. */
+const char *pmpm_status_string(int status);
+
+/* Material helpers: derived constants computed exactly as the reference
+ * constructors do, in FP32.
+ * LinearElastic::LinearElastic (src/materials/linearelastic.cpp:47-58);
+ * corrected != 0 selects lame*tr(deps)*I + 2G*deps instead of the
+ * reference's (lame + 2G)*deps (src/materials/linearelastic_inline.h:74-75). */
+int pmpm_material_linear_elastic(float density, float E, float pois, int corrected, pmpm_material *out);
+/* NewtonFluid::NewtonFluid (src/materials/newtonfluid.cpp:44-52). */
+int pmpm_material_newton_fluid(float density, float viscosity, float bulk_modulus, float gamma,
+                               pmpm_material *out);
+/* Drucker-Prager with friction angle, dilatancy angle (degrees) and cohesion,
+ * fitted to Mohr-Coulomb's outer cone: eta = 6 sin(phi)/(sqrt3 (3 - sin(phi))),
+ * kc = 6 c cos(phi)/(sqrt3 (3 - sin(phi))), eta_bar likewise from psi.  The
+ * cone and apex return follow update_dp_rheo (src/materials/dp_rheo_inline.h:
+ * 123-246); there is no reference class with these parameters (the reference's
+ * DP classes are not reachable from its USL solver). */
+int pmpm_material_drucker_prager(float density, float E, float pois, float friction_deg,
+                                 float dilatancy_deg, float cohesion, pmpm_material *out);
+/* The reference DP_rheo parameters M (CSL slope), Pt (tensile pressure) and
+ * dilatancy angle (degrees): DP_rheo::DP_rheo (src/materials/dp_rheo.cpp:45-70). */
+int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
+                          pmpm_material *out);
+
+/* Boundary-condition helpers (reference constructors). */
+/* Gravity::Gravity (src/boundaryconditions/gravity.cpp:52-60) */
+int pmpm_bc_gravity(const float *gravity, int is_ramp, int ramp_step, const float *gravity_end,
+                    int dim, pmpm_bc *out);
+/* NodeDomain::NodeDomain (src/boundaryconditions/nodedomain.cpp:33-37) */
+int pmpm_bc_nodedomain(const int *face0_mode, const int *face1_mode, int dim, pmpm_bc *out);
+/* BodyForce::BodyForce (src/boundaryconditions/bodyforce.cpp:44-61): mode
+ * "forces" 0, "moments" 1, "fixed" 2 */
+int pmpm_bc_bodyforce(int mode, const float *values, const unsigned char *mask, pmpm_bc *out);
+/* PlanarDomain::PlanarDomain (src/boundaryconditions/planardomain.cpp:33-40):
+ * friction angles in degrees, stored in radians */
+int pmpm_bc_planardomain(const float *face0_friction_deg, const float *face1_friction_deg, int dim,
+                         pmpm_bc *out);
+
+/* Create a simulation: the Grid and NodesContainer constructors
+ * (include/pyroclastmpm/common/types_common.h:260-272, src/nodes/nodes.cpp:
+ * 55-83) and set_globals (src/common/global_settings.cpp:161-176), held per
+ * handle instead of in process globals. */
+int pmpm_create(const pmpm_desc *desc, pmpm_sim **out);
+
+/* Release all device memory of the handle. */
+int pmpm_destroy(pmpm_sim *sim);
+
+/* Grid sizes: Grid::num_cells / num_cells_total. */
+int pmpm_get_grid(const pmpm_sim *sim, int num_cells[3], int *num_cells_total, float *inv_cell_size);
+
+/* Upload particles: ParticlesContainer::ParticlesContainer
+ * (src/particles/particles.cpp:51-149).  Rigid particles are appended after
+ * the others, as in the reference.  velocities/colors/rigid arrays may be NULL.
+ * Masses and volumes start at -1 (unset), F at identity, stresses at zero. */
+int pmpm_set_particles(pmpm_sim *sim, int num_particles, const float *positions, const float *velocities,
+                       const unsigned char *colors, int num_rigid, const float *rigid_positions,
+                       const float *rigid_velocities, const unsigned char *rigid_colors);
+
+/* Solver::Solver set-up (src/solver/solver.cpp:69-104): partition, initial
+ * volumes (src/particles/particles.cpp:345-365), initial masses per material
+ * (:372-393); Drucker-Prager history starts from the current stresses. */
+int pmpm_initialize(pmpm_sim *sim);
+
+/* Copy a field out (reference layout, id order).  dst is host memory unless
+ * on_device != 0.  bytes must equal the field's size. */
+int pmpm_get_field(pmpm_sim *sim, int field, void *dst, size_t bytes, int on_device);
+
+/* Copy a field in (the pybind property setters,
+ * python/pybind/particles/particles_bind.cpp:179-301).  Stresses are stored
+ * as symmetric tensors (upper triangle); 2D keeps xx, yy, xy and zz. */
+int pmpm_set_field(pmpm_sim *sim, int field, const void *src, size_t bytes, int on_device);
+
+/* Number of particles / nodes, bytes of one field. */
+int pmpm_num_particles(const pmpm_sim *sim);
+int pmpm_num_nodes(const pmpm_sim *sim);
+size_t pmpm_field_bytes(const pmpm_sim *sim, int field);
+
+/* ParticlesContainer::partition (src/particles/particles.cpp:332-339):
+ * cell hash, stable sort by hash, cell start/end; bit-exact with the
+ * reference (SpatialPartition, src/spatialpartition/spatialpartition.cpp:90-136). */
+int pmpm_partition(pmpm_sim *sim);
+
+/* calculate_shape_function (src/shapefunction/shapefunction.cpp:167-190):
+ * psi [n][nsn] and dpsi [n][nsn][dim] in the reference slot order.  The step
+ * never stores these (weights live in registers); this call materialises them
+ * for inspection.  Requires a prior pmpm_partition. */
+int pmpm_shape_functions(pmpm_sim *sim, float *psi, float *dpsi, int on_device);
+int pmpm_num_surround_nodes(const pmpm_sim *sim);
+
+/* USL::P2G (src/solver/usl/usl.cpp:118-161).  apply_bcs != 0 also applies the
+ * node boundary conditions in list order (USL::solve :97-103), fused into the
+ * P2G epilogue.  Requires a prior pmpm_partition. */
+int pmpm_p2g(pmpm_sim *sim, int apply_bcs);
+
+/* USL::G2P (src/solver/usl/usl.cpp:164-199); stress_update != 0 also runs
+ * Solver::stress_update (src/solver/solver.cpp:110-121) fused per particle. */
+int pmpm_g2p(pmpm_sim *sim, int stress_update);
+
+/* Solver::stress_update alone, from the stored velocity gradient. */
+int pmpm_stress_update(pmpm_sim *sim);
+
+/* USL::solve (src/solver/usl/usl.cpp:69-115) followed by increment_global
+ * (src/common/global_settings.cpp:220-227), nsteps times: Solver::solve_nsteps
+ * (src/solver/solver.cpp:125-134).  Asynchronous. */
+int pmpm_solve(pmpm_sim *sim, int nsteps);
+
+/* Diagnostic: one USL step (as pmpm_solve(sim, 1)) with CUDA events between
+ * its phases on the handle's stream; returns the phase durations in ms:
+ * ms[0] partition (hash, scan, scatter, in-cell sort, re-sort when due),
+ * ms[1] P2G with the node epilogue, ms[2] G2P with the stress update.
+ * launches (may be NULL) receives the number of kernels the step launched.
+ * No reference counterpart (the reference logs only wall time,
+ * src/solver/solver.cpp:153-169). */
+int pmpm_profile_step(pmpm_sim *sim, float ms[3], int *launches);
+
+/* Number of kernels the handle has launched since it was created. */
+int pmpm_launch_count(const pmpm_sim *sim, long long *count);
+
+/* Number of grid nodes with mass above the cutoff after the last P2G
+ * (the nodes the step actually updates). */
+int pmpm_active_nodes(pmpm_sim *sim, int *count);
+
+/* The global step counter (set_global_step / global_step_cpu). */
+int pmpm_get_step(const pmpm_sim *sim, int *step);
+int pmpm_set_step(pmpm_sim *sim, int step);
+
+/* Wait for the handle's stream; returns the first device fault seen since
+ * the last call (PMPM_ERR_OUT_OF_DOMAIN, ...) or PMPM_OK, and clears it. */
+int pmpm_synchronize(pmpm_sim *sim);
+
+/* The handle's CUDA stream (cudaStream_t) and device. */
+void *pmpm_stream(const pmpm_sim *sim);
+
+/* Single-point material update on host arrays of n points: the standalone
+ * stress_update binding of the reference DP material
+ * (python/pybind/materials/dp_rheo.cpp:57) generalised to any material here.
+ * L [n][dim][dim] (or the strain increment itself when
+ * velgrad_is_strain_increment != 0), stress [n][3][3] in/out, eps_e
+ * [n][dim][dim] in/out, stress_ref [n][3][3], masses/volumes/volumes_original
+ * [n] (Newtonian fluid only; may be NULL otherwise). */
+int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float dt, const float *L,
+                               float *stress, float *eps_e, const float *stress_ref, const float *masses,
+                               const float *volumes, const float *volumes_original,
+                               int velgrad_is_strain_increment, int device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMPM_H */

@@ -1,0 +1,1329 @@
+// Host side of the C ABI (include/pmpm.h): handle lifetime, device memory,
+// field conversion between the reference layouts and the SoA device layout,
+// and the launch sequence of one USL step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "pmpm.h"
+#include "pmpm_kernels.cuh"
+
+using namespace pmpm;
+
+namespace {
+
+constexpr int kTPB = 256;
+
+inline int blocks_for(long long n, int tpb = kTPB) { return (int)((n + tpb - 1) / tpb); }
+
+#define PMPM_CUDA(call)                                                                   \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      fprintf(stderr, "pmpm: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+              __LINE__);                                                                  \
+      return PMPM_ERR_CUDA;                                                               \
+    }                                                                                     \
+  } while (0)
+
+#define PMPM_LAUNCHED()                                                                   \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) {                                                              \
+      fprintf(stderr, "pmpm: launch error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+              __LINE__);                                                                  \
+      return PMPM_ERR_CUDA;                                                               \
+    }                                                                                     \
+  } while (0)
+
+#define PMPM_TRY(expr)        \
+  do {                        \
+    int st_ = (expr);         \
+    if (st_ != PMPM_OK) return st_; \
+  } while (0)
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return PMPM_OK;
+  cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+  if (e == cudaErrorMemoryAllocation) return PMPM_ERR_OUT_OF_MEMORY;
+  PMPM_CUDA(e);
+  return PMPM_OK;
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+struct GravityState {
+  int bc_index;
+  float current[3];
+};
+
+}  // namespace
+
+struct pmpm_sim {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int dim = 2, shape = 0;
+  DevGrid g{};
+  float dt = 0, alpha = 0.99f;
+  int ppc = 1;
+  unsigned flags = 0;
+  int resort_interval = 32;
+  std::vector<DevMaterial> mats;
+  std::vector<DevBC> bcs;
+  std::vector<float *> bc_values;
+  std::vector<uint8_t *> bc_masks;
+  std::vector<GravityState> gravity;
+  bool has_planar = false, has_dp = false, has_sref = false;
+
+  // particles (two storage sets, swapped by the physical re-sort)
+  int n = 0, stride = 0;
+  DevParticles P[2]{};
+  int cur = 0;
+  int *slot = nullptr;
+  // nodes
+  DevNodes N{};
+  int *node_epoch = nullptr;  // epoch of the P2G that last wrote each tile
+  // bins
+  DevBins B{};
+  int nscan_blocks = 0;
+  int *fault = nullptr;
+  // staging for field conversion
+  void *staging = nullptr;
+  size_t staging_bytes = 0;
+
+  long long launches = 0;
+  int step = 0;
+  int epoch = -1;
+  int p2g_epoch = -2;
+  int steps_since_sort = 0;
+  bool partitioned = false;
+};
+
+namespace {
+
+int ensure_staging(pmpm_sim *s, size_t bytes) {
+  if (s->staging_bytes >= bytes) return PMPM_OK;
+  if (s->staging) cudaFree(s->staging);
+  s->staging = nullptr;
+  s->staging_bytes = 0;
+  cudaError_t e = cudaMalloc(&s->staging, bytes);
+  if (e == cudaErrorMemoryAllocation) return PMPM_ERR_OUT_OF_MEMORY;
+  PMPM_CUDA(e);
+  s->staging_bytes = bytes;
+  return PMPM_OK;
+}
+
+void free_particles(pmpm_sim *s) {
+  for (int k = 0; k < 2; k++) {
+    DevParticles &P = s->P[k];
+    dfree(P.x);
+    dfree(P.v);
+    dfree(P.F);
+    dfree(P.sig);
+    dfree(P.L);
+    dfree(P.m);
+    dfree(P.V);
+    dfree(P.V0);
+    dfree(P.fext);
+    dfree(P.eps);
+    dfree(P.sref);
+    dfree(P.color);
+    dfree(P.active);
+    dfree(P.rigid);
+    dfree(P.id);
+    dfree(P.hash);
+    P = DevParticles{};
+  }
+  dfree(s->slot);
+  dfree(s->B.order);
+  s->n = 0;
+  s->stride = 0;
+}
+
+int alloc_particle_set(pmpm_sim *s, DevParticles &P) {
+  const int D = s->dim, st = s->stride;
+  const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6;
+  P.n = s->n;
+  P.stride = st;
+  PMPM_TRY(dalloc(&P.x, (size_t)D * st));
+  PMPM_TRY(dalloc(&P.v, (size_t)D * st));
+  PMPM_TRY(dalloc(&P.F, (size_t)D * D * st));
+  PMPM_TRY(dalloc(&P.sig, (size_t)S * st));
+  PMPM_TRY(dalloc(&P.L, (size_t)D * D * st));
+  PMPM_TRY(dalloc(&P.m, (size_t)st));
+  PMPM_TRY(dalloc(&P.V, (size_t)st));
+  PMPM_TRY(dalloc(&P.V0, (size_t)st));
+  if (s->has_planar) PMPM_TRY(dalloc(&P.fext, (size_t)D * st));
+  if (s->has_dp) {
+    PMPM_TRY(dalloc(&P.eps, (size_t)E * st));
+    PMPM_TRY(dalloc(&P.sref, (size_t)S * st));
+  }
+  PMPM_TRY(dalloc(&P.color, (size_t)st));
+  PMPM_TRY(dalloc(&P.active, (size_t)st));
+  PMPM_TRY(dalloc(&P.rigid, (size_t)st));
+  PMPM_TRY(dalloc(&P.id, (size_t)st));
+  PMPM_TRY(dalloc(&P.hash, (size_t)st));
+  return PMPM_OK;
+}
+
+StepArgs make_args(pmpm_sim *s) {
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = s->g;
+  a.P = s->P[s->cur];
+  a.P.slot = s->slot;
+  a.N = s->N;
+  a.B = s->B;
+  a.dt = s->dt;
+  a.alpha = s->alpha;
+  a.one_minus_alpha = (float)(1.0 - (double)s->alpha);
+  a.cutoff = 0.000000001f;
+  a.epoch = s->epoch;
+  a.flags = s->flags;
+  a.fault = s->fault;
+  a.nmat = (int)s->mats.size();
+  a.nbc = (int)s->bcs.size();
+  a.has_planar = s->has_planar ? 1 : 0;
+  a.has_sref = s->has_sref ? 1 : 0;
+  for (int k = 0; k < a.nmat; k++) a.mat[k] = s->mats[k];
+  for (int k = 0; k < a.nbc; k++) a.bc[k] = s->bcs[k];
+  for (const GravityState &gs : s->gravity)
+    for (int c = 0; c < 3; c++) a.bc[gs.bc_index].r[c] = gs.current[c];
+  return a;
+}
+
+// Gravity::apply_on_nodes_moments (src/boundaryconditions/gravity.cpp:68-73):
+// while step < ramp_step the stored gravity becomes gravity_end * step/ramp_step.
+void update_gravity(pmpm_sim *s) {
+  for (GravityState &gs : s->gravity) {
+    const DevBC &bc = s->bcs[gs.bc_index];
+    const int is_ramp = bc.i[0], ramp_step = bc.i[1];
+    const float ramp_factor = (float)s->step / (float)ramp_step;
+    if (is_ramp && s->step < ramp_step)
+      for (int c = 0; c < 3; c++) gs.current[c] = bc.r[3 + c] * ramp_factor;
+  }
+}
+
+template <int D, int SF>
+int launch_partition(pmpm_sim *s) {
+  s->epoch += 1;
+  StepArgs a = make_args(s);
+  cudaStream_t st = s->stream;
+  k_hash_count<D, SF><<<blocks_for(s->n), kTPB, 0, st>>>(a);
+  PMPM_LAUNCHED();
+  s->launches += 7;
+  k_scan_reduce<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->g.ntotal, s->B.block_sums);
+  PMPM_LAUNCHED();
+  k_scan_top<<<1, kScanThreads, 0, st>>>(s->B.block_sums, s->nscan_blocks, s->B.scalars);
+  PMPM_LAUNCHED();
+  k_scan_apply<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->g.ntotal, s->B.block_sums, s->B.offset);
+  PMPM_LAUNCHED();
+  k_scatter<<<blocks_for(s->n), kTPB, 0, st>>>(a);
+  PMPM_LAUNCHED();
+  k_sort_cells<<<blocks_for(s->g.ntotal), kTPB, 0, st>>>(a);
+  PMPM_LAUNCHED();
+  k_sort_big<<<148, 1024, 0, st>>>(a);
+  PMPM_LAUNCHED();
+  s->partitioned = true;
+  return PMPM_OK;
+}
+
+template <int D>
+int launch_reorder(pmpm_sim *s) {
+  StepArgs a = make_args(s);
+  DevParticles dst = s->P[1 - s->cur];
+  const bool move_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) != 0;
+  k_reorder<D><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, dst, move_L ? 1 : 0, s->has_planar ? 1 : 0);
+  PMPM_LAUNCHED();
+  s->launches += 1;
+  s->cur = 1 - s->cur;
+  s->steps_since_sort = 0;
+  return PMPM_OK;
+}
+
+template <int D, int SF>
+int launch_p2g(pmpm_sim *s, int apply_bcs) {
+  if (apply_bcs) update_gravity(s);
+  StepArgs a = make_args(s);
+  k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
+  PMPM_LAUNCHED();
+  s->launches += 1;
+  s->p2g_epoch = s->epoch;
+  return PMPM_OK;
+}
+
+template <int D, int SF>
+int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
+  StepArgs a = make_args(s);
+  k_g2p<D, SF><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
+  PMPM_LAUNCHED();
+  s->launches += 1;
+  return PMPM_OK;
+}
+
+template <int D, int SF>
+int step_once(pmpm_sim *s) {
+  PMPM_TRY((launch_partition<D, SF>(s)));
+  if (s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
+    PMPM_TRY(launch_reorder<D>(s));
+  } else {
+    s->steps_since_sort += 1;
+  }
+  PMPM_TRY((launch_p2g<D, SF>(s, 1)));
+  const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
+  PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
+  s->step += 1;
+  return PMPM_OK;
+}
+
+// Runtime (dim, shape function) -> template instantiation.
+#define PMPM_DISPATCH(s, FN, ...)                                                   \
+  ((s)->dim == 2                                                                    \
+       ? ((s)->shape == PMPM_SHAPE_LINEAR      ? FN<2, PMPM_SHAPE_LINEAR>(__VA_ARGS__) \
+          : (s)->shape == PMPM_SHAPE_QUADRATIC ? FN<2, PMPM_SHAPE_QUADRATIC>(__VA_ARGS__) \
+                                               : FN<2, PMPM_SHAPE_CUBIC>(__VA_ARGS__))  \
+       : ((s)->shape == PMPM_SHAPE_LINEAR      ? FN<3, PMPM_SHAPE_LINEAR>(__VA_ARGS__) \
+          : (s)->shape == PMPM_SHAPE_QUADRATIC ? FN<3, PMPM_SHAPE_QUADRATIC>(__VA_ARGS__) \
+                                               : FN<3, PMPM_SHAPE_CUBIC>(__VA_ARGS__)))
+
+// ---------------------------------------------------------------------------
+// field conversion kernels: reference AoS layout (id order) <-> SoA storage
+// ---------------------------------------------------------------------------
+
+// kind: 0 vector [dim], 1 full matrix [dim][dim], 2 stress/ref 3x3 from the
+// symmetric storage, 3 eps [dim][dim] from symmetric, 4 scalar float,
+// 5 uint8, 6 uint32 hash, 7 bins from positions
+__global__ void k_get_particles(DevParticles P, int D, int kind, const void *src, void *dst, int extra) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  const int i = P.id[s], st = P.stride;
+  if (kind == 0 || kind == 1) {
+    const int nc = kind == 0 ? D : D * D;
+    const float *f = (const float *)src;
+    for (int c = 0; c < nc; c++) ((float *)dst)[(size_t)i * nc + c] = f[c * st + s];
+  } else if (kind == 2) {
+    const float *f = (const float *)src;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) {
+        int k;
+        if (D == 2) {
+          k = (a == b) ? (a == 2 ? 3 : a) : (a + b == 1 ? 2 : -1);
+        } else {
+          k = (a == b) ? a : 2 + a + b;
+        }
+        ((float *)dst)[(size_t)i * 9 + 3 * a + b] = k < 0 ? 0.0f : f[k * st + s];
+      }
+  } else if (kind == 3) {
+    const float *f = (const float *)src;
+    for (int a = 0; a < D; a++)
+      for (int b = 0; b < D; b++) {
+        int k = (a == b) ? a : (D == 2 ? 2 : 2 + a + b);
+        ((float *)dst)[(size_t)i * D * D + a * D + b] = f[k * st + s];
+      }
+  } else if (kind == 4) {
+    ((float *)dst)[i] = ((const float *)src)[s];
+  } else if (kind == 5) {
+    ((uint8_t *)dst)[i] = ((const uint8_t *)src)[s];
+  } else if (kind == 6) {
+    ((unsigned *)dst)[i] = ((const unsigned *)src)[s];
+  } else if (kind == 7) {
+    const DevGrid *g = (const DevGrid *)src;
+    for (int c = 0; c < D; c++)
+      ((int *)dst)[(size_t)i * D + c] = (int)scaled_coord(P.x[c * st + s], g->origin[c], g->inv_h);
+  }
+  (void)extra;
+}
+
+__global__ void k_set_particles(DevParticles P, int D, int kind, const void *src, void *dst) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  const int i = P.id[s], st = P.stride;
+  if (kind == 0 || kind == 1) {
+    const int nc = kind == 0 ? D : D * D;
+    for (int c = 0; c < nc; c++) ((float *)dst)[c * st + s] = ((const float *)src)[(size_t)i * nc + c];
+  } else if (kind == 2) {
+    const float *M = (const float *)src + (size_t)i * 9;
+    float *f = (float *)dst;
+    if (D == 2) {
+      f[0 * st + s] = M[0];
+      f[1 * st + s] = M[4];
+      f[2 * st + s] = M[1];
+      f[3 * st + s] = M[8];
+    } else {
+      f[0 * st + s] = M[0];
+      f[1 * st + s] = M[4];
+      f[2 * st + s] = M[8];
+      f[3 * st + s] = M[1];
+      f[4 * st + s] = M[2];
+      f[5 * st + s] = M[5];
+    }
+  } else if (kind == 3) {
+    const float *M = (const float *)src + (size_t)i * D * D;
+    float *f = (float *)dst;
+    if (D == 2) {
+      f[0 * st + s] = M[0];
+      f[1 * st + s] = M[3];
+      f[2 * st + s] = M[1];
+    } else {
+      f[0 * st + s] = M[0];
+      f[1 * st + s] = M[4];
+      f[2 * st + s] = M[8];
+      f[3 * st + s] = M[1];
+      f[4 * st + s] = M[2];
+      f[5 * st + s] = M[5];
+    }
+  } else if (kind == 4) {
+    ((float *)dst)[s] = ((const float *)src)[i];
+  } else if (kind == 5) {
+    ((uint8_t *)dst)[s] = ((const uint8_t *)src)[i];
+  }
+}
+
+// Node field out: nodes of tiles the last P2G did not write read as 0.
+__global__ void k_get_nodes(DevGrid g, int D, int ncomp, const float *src, const int *node_epoch, int p2g_epoch,
+                            float *dst) {
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= g.ntotal) return;
+  const int c[3] = {node % g.n[0], (node / g.n[0]) % g.n[1], node / (g.n[0] * g.n[1])};
+  int t = D == 2 ? tile_of<2>(g, c) : tile_of<3>(g, c);
+  const bool valid = node_epoch[t] == p2g_epoch;
+  for (int k = 0; k < ncomp; k++) dst[(size_t)node * ncomp + k] = valid ? src[(size_t)k * g.ntotal + node] : 0.0f;
+}
+
+// Solver::Solver set-up kernels.
+__global__ void k_initial_volumes(DevParticles P, float vol) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  if (!(P.V[s] > 0.0f)) P.V[s] = vol;
+  P.V0[s] = P.V[s];
+}
+
+__global__ void k_initial_masses(DevParticles P, int mat_id, float density) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  if ((int)P.color[s] != mat_id || P.m[s] > 0.0f) return;
+  P.m[s] = density * P.V[s];
+}
+
+__global__ void k_dp_init(DevParticles P, int D, int *nonzero_ref) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6, st = P.stride;
+  bool nz = false;
+  for (int k = 0; k < S; k++) {
+    float v = P.sig[k * st + s];
+    P.sref[k * st + s] = v;
+    nz = nz || v != 0.0f;
+  }
+  for (int k = 0; k < E; k++) P.eps[k * st + s] = 0.0f;
+  if (nz) atomicOr(nonzero_ref, 1);
+}
+
+int field_info(const pmpm_sim *s, int field, size_t *bytes) {
+  const size_t n = (size_t)s->n, D = (size_t)s->dim, nn = (size_t)s->g.ntotal;
+  switch (field) {
+    case PMPM_FIELD_POSITIONS:
+    case PMPM_FIELD_VELOCITIES:
+    case PMPM_FIELD_FORCES_EXTERNAL:
+      *bytes = n * D * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_STRESSES:
+    case PMPM_FIELD_STRESS_REF:
+      *bytes = n * 9 * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_F:
+    case PMPM_FIELD_VELOCITY_GRADIENT:
+    case PMPM_FIELD_EPS_E:
+      *bytes = n * D * D * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_MASSES:
+    case PMPM_FIELD_VOLUMES:
+    case PMPM_FIELD_VOLUMES_ORIGINAL:
+    case PMPM_FIELD_HASH_UNSORTED:
+    case PMPM_FIELD_HASH_SORTED:
+    case PMPM_FIELD_SORTED_INDEX:
+      *bytes = n * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_COLORS:
+    case PMPM_FIELD_IS_RIGID:
+    case PMPM_FIELD_IS_ACTIVE:
+      *bytes = n;
+      return PMPM_OK;
+    case PMPM_FIELD_NODE_MASSES:
+    case PMPM_FIELD_CELL_START:
+    case PMPM_FIELD_CELL_END:
+      *bytes = nn * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_NODE_MOMENTS:
+    case PMPM_FIELD_NODE_MOMENTS_NT:
+      *bytes = nn * D * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_NODE_IDS:
+    case PMPM_FIELD_NODE_TYPES:
+      *bytes = nn * 3 * 4;
+      return PMPM_OK;
+    case PMPM_FIELD_BINS:
+      *bytes = n * D * 4;
+      return PMPM_OK;
+    default:
+      return PMPM_ERR_INVALID_ARGUMENT;
+  }
+}
+
+int copy_out(pmpm_sim *s, const void *dev_src, void *dst, size_t bytes, int on_device) {
+  PMPM_CUDA(cudaMemcpyAsync(dst, dev_src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                            s->stream));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMPM_OK;
+}
+
+// Sorted index and sorted hashes in the reference's layout: binned particles
+// in cell order (ids ascending inside a cell), then the unbinned ones (hash
+// >= num_cells_total) by (hash, id), as a stable sort of all hashes gives.
+int sorted_views(pmpm_sim *s, std::vector<int> &sorted_index, std::vector<unsigned> &hash_sorted) {
+  const int n = s->n;
+  std::vector<int> order(n), id(n);
+  std::vector<unsigned> hash(n);
+  int nb = 0;
+  const DevParticles &P = s->P[s->cur];
+  PMPM_CUDA(cudaMemcpyAsync(order.data(), s->B.order, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  PMPM_CUDA(cudaMemcpyAsync(id.data(), P.id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+  PMPM_CUDA(cudaMemcpyAsync(hash.data(), P.hash, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s->stream));
+  PMPM_CUDA(cudaMemcpyAsync(&nb, s->B.scalars, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  sorted_index.resize(n);
+  hash_sorted.resize(n);
+  for (int k = 0; k < n; k++) {
+    sorted_index[k] = id[order[k]];
+    hash_sorted[k] = hash[order[k]];
+  }
+  std::vector<std::pair<unsigned, int>> tail;
+  for (int k = nb; k < n; k++) tail.emplace_back(hash_sorted[k], sorted_index[k]);
+  std::sort(tail.begin(), tail.end());
+  for (int k = nb; k < n; k++) {
+    hash_sorted[k] = tail[k - nb].first;
+    sorted_index[k] = tail[k - nb].second;
+  }
+  return PMPM_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char *pmpm_status_string(int status) {
+  switch (status) {
+    case PMPM_OK: return "ok";
+    case PMPM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case PMPM_ERR_CUDA: return "CUDA error";
+    case PMPM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case PMPM_ERR_NOT_SUPPORTED: return "not supported";
+    case PMPM_ERR_STATE: return "call out of order (particles not set or not initialised)";
+    case PMPM_ERR_OUT_OF_DOMAIN: return "a particle left the background grid";
+    case PMPM_ERR_NONFINITE: return "non-finite particle position";
+    case PMPM_ERR_CELL_OVERFLOW: return "too many particles in one cell";
+    default: return "unknown status";
+  }
+}
+
+int pmpm_material_linear_elastic(float density, float E, float pois, int corrected, pmpm_material *out) {
+  if (!out) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_MAT_LINEAR_ELASTIC;
+  out->density = density;
+  const float bulk = E / (3.0f * (1.0f - 2.0f * pois));
+  const float shear = E / (2.0f * (1.0f + pois));
+  const float lame = E * pois / ((1.0f + pois) * (1.0f - 2.0f * pois));
+  float p[8] = {E, pois, lame, shear, bulk, corrected ? 1.0f : 0.0f, 0.0f, 0.0f};
+  memcpy(out->params, p, sizeof(p));
+  return PMPM_OK;
+}
+
+int pmpm_material_newton_fluid(float density, float viscosity, float bulk_modulus, float gamma,
+                               pmpm_material *out) {
+  if (!out) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_MAT_NEWTON_FLUID;
+  out->density = density;
+  out->params[0] = viscosity;
+  out->params[1] = bulk_modulus;
+  out->params[2] = gamma;
+  return PMPM_OK;
+}
+
+int pmpm_material_drucker_prager(float density, float E, float pois, float friction_deg, float dilatancy_deg,
+                                 float cohesion, pmpm_material *out) {
+  if (!out) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_MAT_DRUCKER_PRAGER;
+  out->density = density;
+  const float bulk = E / (3.0f * (1.0f - 2.0f * pois));
+  const float shear = E / (2.0f * (1.0f + pois));
+  const double deg = 3.14159265358979323846 / 180.0;
+  const double phi = (double)friction_deg * deg, psi = (double)dilatancy_deg * deg;
+  const double s3 = std::sqrt(3.0);
+  const double eta = 6.0 * std::sin(phi) / (s3 * (3.0 - std::sin(phi)));
+  const double xi = 6.0 * std::cos(phi) / (s3 * (3.0 - std::sin(phi)));
+  const double eta_bar = 6.0 * std::sin(psi) / (s3 * (3.0 - std::sin(psi)));
+  const double kc = xi * (double)cohesion;
+  out->params[0] = bulk;
+  out->params[1] = shear;
+  out->params[2] = (float)eta;
+  out->params[3] = (float)eta_bar;
+  out->params[4] = (float)kc;
+  out->params[5] = eta > 0.0 ? (float)(kc / eta) : 0.0f;
+  out->params[6] = eta > 0.0 ? 1.0f : 0.0f;
+  return PMPM_OK;
+}
+
+int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
+                          pmpm_material *out) {
+  if (!out) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_MAT_DRUCKER_PRAGER;
+  out->density = density;
+  const float bulk = E / (3.0f * (1.0f - 2.0f * pois));
+  const float shear = E / (2.0f * (1.0f + pois));
+  const float psi = dilatancy_deg * (float)(3.14159265358979323846 / 180.0);
+  const float eta_bar = (float)(6.0 * std::sin((double)psi) / (std::sqrt(3.0) * (3.0 + std::sin((double)psi))));
+  const float eta = (float)(std::sqrt(1.0 / 3.0) * (double)M);
+  out->params[0] = bulk;
+  out->params[1] = shear;
+  out->params[2] = eta;
+  out->params[3] = eta_bar;
+  out->params[4] = eta * Pt;
+  out->params[5] = Pt;
+  out->params[6] = 1.0f;
+  return PMPM_OK;
+}
+
+int pmpm_bc_gravity(const float *gravity, int is_ramp, int ramp_step, const float *gravity_end, int dim,
+                    pmpm_bc *out) {
+  if (!out || !gravity || dim < 2 || dim > 3) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_BC_GRAVITY;
+  for (int c = 0; c < dim; c++) {
+    out->reals[c] = gravity[c];
+    out->reals[3 + c] = gravity_end ? gravity_end[c] : 0.0f;
+  }
+  out->ints[0] = is_ramp ? 1 : 0;
+  out->ints[1] = ramp_step;
+  return PMPM_OK;
+}
+
+int pmpm_bc_nodedomain(const int *face0_mode, const int *face1_mode, int dim, pmpm_bc *out) {
+  if (!out || dim < 2 || dim > 3) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_BC_NODEDOMAIN;
+  for (int c = 0; c < dim; c++) {
+    out->ints[c] = face0_mode ? face0_mode[c] : 0;
+    out->ints[3 + c] = face1_mode ? face1_mode[c] : 0;
+  }
+  return PMPM_OK;
+}
+
+int pmpm_bc_bodyforce(int mode, const float *values, const unsigned char *mask, pmpm_bc *out) {
+  if (!out || !values || !mask || mode < 0 || mode > 2) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_BC_BODYFORCE;
+  out->ints[0] = mode;
+  out->ints[1] = 1;
+  out->values = values;
+  out->mask = mask;
+  return PMPM_OK;
+}
+
+int pmpm_bc_planardomain(const float *face0_friction_deg, const float *face1_friction_deg, int dim,
+                         pmpm_bc *out) {
+  if (!out || dim < 2 || dim > 3) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_BC_PLANARDOMAIN;
+  const float deg = (float)(3.14159265358979323846 / 180.0);
+  for (int c = 0; c < dim; c++) {
+    out->reals[c] = (face0_friction_deg ? face0_friction_deg[c] : 0.0f) * deg;
+    out->reals[3 + c] = (face1_friction_deg ? face1_friction_deg[c] : 0.0f) * deg;
+  }
+  return PMPM_OK;
+}
+
+int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
+  if (!desc || !out) return PMPM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (desc->dim != 2 && desc->dim != 3) return PMPM_ERR_NOT_SUPPORTED;
+  if (desc->shape_function < 0 || desc->shape_function > 2) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!(desc->cell_size > 0.0f) || desc->num_materials < 0 || desc->num_materials > PMPM_MAX_MATERIALS ||
+      desc->num_bcs < 0 || desc->num_bcs > PMPM_MAX_BCS || desc->particles_per_cell <= 0)
+    return PMPM_ERR_INVALID_ARGUMENT;
+  if ((desc->num_materials > 0 && !desc->materials) || (desc->num_bcs > 0 && !desc->bcs))
+    return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(desc->device));
+  pmpm_sim *s = new pmpm_sim();
+  s->device = desc->device;
+  s->dim = desc->dim;
+  s->shape = desc->shape_function;
+  s->dt = desc->dt;
+  s->alpha = desc->alpha;
+  s->ppc = desc->particles_per_cell;
+  s->flags = desc->flags;
+  s->resort_interval = desc->resort_interval < 0 ? 0 : desc->resort_interval;
+  if (desc->stream) {
+    s->stream = (cudaStream_t)desc->stream;
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete s;
+      return PMPM_ERR_CUDA;
+    }
+    s->own_stream = true;
+  }
+  // Grid (include/pyroclastmpm/common/types_common.h:260-272), FP32 as the reference
+  DevGrid &g = s->g;
+  g.h = desc->cell_size;
+  g.inv_h = 1.0f / desc->cell_size;
+  g.ntotal = 1;
+  for (int c = 0; c < 3; c++) {
+    g.n[c] = 1;
+    g.origin[c] = 0.0f;
+    g.end[c] = 0.0f;
+    if (c < s->dim) {
+      g.origin[c] = desc->origin[c];
+      g.end[c] = desc->end[c];
+      const float span = desc->end[c] - desc->origin[c];
+      g.n[c] = (int)(span / desc->cell_size) + 1;
+      if (g.n[c] < 1) {
+        delete s;
+        return PMPM_ERR_INVALID_ARGUMENT;
+      }
+    }
+    g.ntotal *= g.n[c];
+  }
+  const int tsz[3] = {s->dim == 2 ? TileDims<2>::X : TileDims<3>::X, s->dim == 2 ? TileDims<2>::Y : TileDims<3>::Y,
+                      s->dim == 2 ? 1 : TileDims<3>::Z};
+  g.ntiles = 1;
+  for (int c = 0; c < 3; c++) {
+    g.tdim[c] = (g.n[c] + tsz[c] - 1) / tsz[c];
+    g.ntiles *= g.tdim[c];
+  }
+  // materials
+  for (int k = 0; k < desc->num_materials; k++) {
+    const pmpm_material &m = desc->materials[k];
+    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_DRUCKER_PRAGER) {
+      delete s;
+      return PMPM_ERR_INVALID_ARGUMENT;
+    }
+    DevMaterial dm;
+    dm.type = m.type;
+    dm.density = m.density;
+    memcpy(dm.p, m.params, sizeof(dm.p));
+    if (m.type == PMPM_MAT_NEWTON_FLUID) dm.p[3] = (float)(2.0 * (double)m.params[0] / 3.0);
+    if (m.type == PMPM_MAT_DRUCKER_PRAGER) s->has_dp = true;
+    s->mats.push_back(dm);
+  }
+  int st = PMPM_OK;
+  // boundary conditions
+  for (int k = 0; k < desc->num_bcs && st == PMPM_OK; k++) {
+    const pmpm_bc &b = desc->bcs[k];
+    DevBC db;
+    memset(&db, 0, sizeof(db));
+    db.type = b.type;
+    memcpy(db.i, b.ints, sizeof(db.i));
+    memcpy(db.r, b.reals, sizeof(db.r));
+    if (b.type == PMPM_BC_GRAVITY) {
+      GravityState gs;
+      gs.bc_index = k;
+      for (int c = 0; c < 3; c++) gs.current[c] = b.reals[c];
+      s->gravity.push_back(gs);
+    } else if (b.type == PMPM_BC_BODYFORCE) {
+      if (!b.values || !b.mask) {
+        st = PMPM_ERR_INVALID_ARGUMENT;
+        break;
+      }
+      float *vals = nullptr;
+      uint8_t *mask = nullptr;
+      st = dalloc(&vals, (size_t)g.ntotal * s->dim);
+      if (st == PMPM_OK) st = dalloc(&mask, (size_t)g.ntotal);
+      if (st == PMPM_OK &&
+          (cudaMemcpy(vals, b.values, sizeof(float) * g.ntotal * s->dim, cudaMemcpyHostToDevice) != cudaSuccess ||
+           cudaMemcpy(mask, b.mask, g.ntotal, cudaMemcpyHostToDevice) != cudaSuccess))
+        st = PMPM_ERR_CUDA;
+      s->bc_values.push_back(vals);
+      s->bc_masks.push_back(mask);
+      db.values = vals;
+      db.mask = mask;
+    } else if (b.type == PMPM_BC_PLANARDOMAIN) {
+      s->has_planar = true;
+    } else if (b.type != PMPM_BC_NODEDOMAIN) {
+      st = PMPM_ERR_INVALID_ARGUMENT;
+    }
+    s->bcs.push_back(db);
+  }
+  // nodes and bins
+  const size_t nn = (size_t)g.ntotal, D = (size_t)s->dim;
+  if (st == PMPM_OK) st = dalloc(&s->N.m, nn);
+  if (st == PMPM_OK) st = dalloc(&s->N.p, nn * D);
+  if (st == PMPM_OK) st = dalloc(&s->N.pnt, nn * D);
+  if (st == PMPM_OK) st = dalloc(&s->N.v, nn * D);
+  if (st == PMPM_OK) st = dalloc(&s->N.vnt, nn * D);
+  if (st == PMPM_OK) st = dalloc(&s->N.tile_epoch, (size_t)g.ntiles);
+  if (st == PMPM_OK) st = dalloc(&s->node_epoch, (size_t)g.ntiles);
+  s->nscan_blocks = (g.ntotal + kScanChunk - 1) / kScanChunk;
+  if (st == PMPM_OK) st = dalloc(&s->B.count, nn);
+  if (st == PMPM_OK) st = dalloc(&s->B.offset, nn + 1);
+  if (st == PMPM_OK) st = dalloc(&s->B.block_sums, (size_t)s->nscan_blocks);
+  if (st == PMPM_OK) st = dalloc(&s->B.scalars, 4);
+  if (st == PMPM_OK) st = dalloc(&s->B.big_cells, nn);
+  if (st == PMPM_OK) st = dalloc(&s->fault, 1);
+  if (st == PMPM_OK) {
+    if (cudaMemset(s->B.count, 0, nn * sizeof(int)) != cudaSuccess ||
+        cudaMemset(s->B.scalars, 0, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(s->fault, 0, sizeof(int)) != cudaSuccess ||
+        cudaMemset(s->N.tile_epoch, 0xff, g.ntiles * sizeof(int)) != cudaSuccess ||
+        cudaMemset(s->node_epoch, 0xff, g.ntiles * sizeof(int)) != cudaSuccess ||
+        cudaMemset(s->N.m, 0, nn * sizeof(float)) != cudaSuccess)
+      st = PMPM_ERR_CUDA;
+  }
+  if (st != PMPM_OK) {
+    pmpm_destroy(s);
+    return st;
+  }
+  *out = s;
+  return PMPM_OK;
+}
+
+int pmpm_destroy(pmpm_sim *s) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_particles(s);
+  dfree(s->N.m);
+  dfree(s->N.p);
+  dfree(s->N.pnt);
+  dfree(s->N.v);
+  dfree(s->N.vnt);
+  dfree(s->N.tile_epoch);
+  dfree(s->node_epoch);
+  dfree(s->B.count);
+  dfree(s->B.offset);
+  dfree(s->B.block_sums);
+  dfree(s->B.scalars);
+  dfree(s->B.big_cells);
+  dfree(s->fault);
+  for (float *p : s->bc_values) dfree(p);
+  for (uint8_t *p : s->bc_masks) dfree(p);
+  if (s->staging) cudaFree(s->staging);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return PMPM_OK;
+}
+
+int pmpm_get_grid(const pmpm_sim *s, int num_cells[3], int *num_cells_total, float *inv_cell_size) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (num_cells)
+    for (int c = 0; c < 3; c++) num_cells[c] = s->g.n[c];
+  if (num_cells_total) *num_cells_total = s->g.ntotal;
+  if (inv_cell_size) *inv_cell_size = s->g.inv_h;
+  return PMPM_OK;
+}
+
+int pmpm_num_particles(const pmpm_sim *s) { return s ? s->n : -1; }
+int pmpm_num_nodes(const pmpm_sim *s) { return s ? s->g.ntotal : -1; }
+void *pmpm_stream(const pmpm_sim *s) { return s ? (void *)s->stream : nullptr; }
+
+int pmpm_num_surround_nodes(const pmpm_sim *s) {
+  if (!s) return -1;
+  const int w = s->shape == PMPM_SHAPE_LINEAR ? 2 : 4;
+  return s->dim == 2 ? w * w : w * w * w;
+}
+
+size_t pmpm_field_bytes(const pmpm_sim *s, int field) {
+  size_t b = 0;
+  if (!s || field_info(s, field, &b) != PMPM_OK) return 0;
+  return b;
+}
+
+int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, const float *velocities,
+                       const unsigned char *colors, int num_rigid, const float *rigid_positions,
+                       const float *rigid_velocities, const unsigned char *rigid_colors) {
+  if (!s || num_particles < 0 || num_rigid < 0 || (num_particles > 0 && !positions) ||
+      (num_rigid > 0 && !rigid_positions) || num_particles + num_rigid < 1)
+    return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  free_particles(s);
+  const int D = s->dim;
+  const int n = num_particles + num_rigid;
+  s->n = n;
+  s->stride = (n + 63) / 64 * 64;
+  s->cur = 0;
+  PMPM_TRY(alloc_particle_set(s, s->P[0]));
+  PMPM_TRY(alloc_particle_set(s, s->P[1]));
+  PMPM_TRY(dalloc(&s->slot, (size_t)s->stride));
+  PMPM_TRY(dalloc(&s->B.order, (size_t)s->stride));
+  const int st = s->stride;
+  const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6;
+  // ParticlesContainer ctor (src/particles/particles.cpp:51-149): rigid particles appended
+  std::vector<float> x((size_t)D * st, 0.0f), v((size_t)D * st, 0.0f), F((size_t)D * D * st, 0.0f);
+  std::vector<float> m(st, -1.0f), V(st, -1.0f);
+  std::vector<uint8_t> color(st, 0), rigid(st, 0), active(st, 1);
+  std::vector<int> id(st, 0);
+  for (int i = 0; i < n; i++) {
+    const bool r = i >= num_particles;
+    const int j = r ? i - num_particles : i;
+    const float *px = r ? rigid_positions : positions;
+    const float *pv = r ? rigid_velocities : velocities;
+    const unsigned char *pc = r ? rigid_colors : colors;
+    for (int c = 0; c < D; c++) {
+      x[(size_t)c * st + i] = px[(size_t)j * D + c];
+      v[(size_t)c * st + i] = pv ? pv[(size_t)j * D + c] : 0.0f;
+    }
+    for (int c = 0; c < D; c++) F[(size_t)(c * D + c) * st + i] = 1.0f;
+    color[i] = pc ? pc[j] : 0;
+    rigid[i] = r ? 1 : 0;
+    id[i] = i;
+  }
+  DevParticles &P = s->P[0];
+  PMPM_CUDA(cudaMemcpy(P.x, x.data(), sizeof(float) * x.size(), cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.v, v.data(), sizeof(float) * v.size(), cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.F, F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemset(P.sig, 0, sizeof(float) * S * st));
+  PMPM_CUDA(cudaMemset(P.L, 0, sizeof(float) * D * D * st));
+  PMPM_CUDA(cudaMemcpy(P.m, m.data(), sizeof(float) * st, cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.V, V.data(), sizeof(float) * st, cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.V0, V.data(), sizeof(float) * st, cudaMemcpyHostToDevice));
+  if (P.fext) PMPM_CUDA(cudaMemset(P.fext, 0, sizeof(float) * D * st));
+  if (P.eps) PMPM_CUDA(cudaMemset(P.eps, 0, sizeof(float) * E * st));
+  if (P.sref) PMPM_CUDA(cudaMemset(P.sref, 0, sizeof(float) * S * st));
+  PMPM_CUDA(cudaMemcpy(P.color, color.data(), st, cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.rigid, rigid.data(), st, cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.active, active.data(), st, cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemcpy(P.id, id.data(), sizeof(int) * st, cudaMemcpyHostToDevice));
+  PMPM_CUDA(cudaMemset(P.hash, 0, sizeof(unsigned) * st));
+  PMPM_CUDA(cudaMemset(s->B.order, 0, sizeof(int) * st));
+  s->partitioned = false;
+  s->steps_since_sort = 0;
+  return PMPM_OK;
+}
+
+int pmpm_partition(pmpm_sim *s) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  return PMPM_DISPATCH(s, launch_partition, s);
+}
+
+int pmpm_initialize(pmpm_sim *s) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  PMPM_TRY(pmpm_partition(s));
+  DevParticles &P = s->P[s->cur];
+  // calculate_initial_volumes: (REAL)pow(h, DIM) / ppc
+  float vol = (float)std::pow((double)s->g.h, (double)s->dim);
+  vol = vol / (float)s->ppc;
+  k_initial_volumes<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, vol);
+  PMPM_LAUNCHED();
+  for (int k = 0; k < (int)s->mats.size(); k++) {
+    k_initial_masses<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, k, s->mats[k].density);
+    PMPM_LAUNCHED();
+  }
+  if (s->has_dp) {
+    int *flag = s->B.scalars + 3;
+    PMPM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+    k_dp_init<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, s->dim, flag);
+    PMPM_LAUNCHED();
+    int h = 0;
+    PMPM_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    PMPM_CUDA(cudaStreamSynchronize(s->stream));
+    s->has_sref = h != 0;
+  }
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMPM_OK;
+}
+
+int pmpm_get_field(pmpm_sim *s, int field, void *dst, size_t bytes, int on_device) {
+  if (!s || !dst) return PMPM_ERR_INVALID_ARGUMENT;
+  size_t need = 0;
+  PMPM_TRY(field_info(s, field, &need));
+  if (bytes != need) return PMPM_ERR_INVALID_ARGUMENT;
+  const bool particle_field = field < PMPM_FIELD_NODE_MASSES || field == PMPM_FIELD_BINS ||
+                              (field >= PMPM_FIELD_HASH_UNSORTED && field <= PMPM_FIELD_SORTED_INDEX);
+  if (particle_field && s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  const int D = s->dim;
+  const DevParticles &P = s->P[s->cur];
+  // host-computed fields
+  if (field == PMPM_FIELD_NODE_IDS || field == PMPM_FIELD_NODE_TYPES || field == PMPM_FIELD_SORTED_INDEX ||
+      field == PMPM_FIELD_HASH_SORTED || field == PMPM_FIELD_CELL_START || field == PMPM_FIELD_CELL_END) {
+    std::vector<int> host(need / 4, 0);
+    const DevGrid &g = s->g;
+    if (field == PMPM_FIELD_NODE_IDS || field == PMPM_FIELD_NODE_TYPES) {
+      for (int node = 0; node < g.ntotal; node++) {
+        const int c[3] = {node % g.n[0], (node / g.n[0]) % g.n[1], node / (g.n[0] * g.n[1])};
+        for (int a = 0; a < 3; a++) {
+          int val = c[a];
+          if (field == PMPM_FIELD_NODE_TYPES) {
+            // calculate_bin_types (src/nodes/nodes.cpp:135-173): cubic grids only
+            if (s->shape != PMPM_SHAPE_CUBIC || a >= D)
+              val = 0;
+            else
+              val = (c[a] == 0 || c[a] == g.n[a] - 1) ? 1 : (c[a] == 1 ? 2 : 3);
+          }
+          host[(size_t)node * 3 + a] = val;
+        }
+      }
+    } else if (field == PMPM_FIELD_SORTED_INDEX || field == PMPM_FIELD_HASH_SORTED) {
+      std::vector<int> si;
+      std::vector<unsigned> hs;
+      PMPM_TRY(sorted_views(s, si, hs));
+      if (field == PMPM_FIELD_SORTED_INDEX)
+        memcpy(host.data(), si.data(), need);
+      else
+        memcpy(host.data(), hs.data(), need);
+    } else {
+      // cell_start / cell_end: 0 for empty cells (SpatialPartition::reset fills 0)
+      std::vector<int> off(g.ntotal + 1);
+      PMPM_CUDA(cudaMemcpyAsync(off.data(), s->B.offset, sizeof(int) * (g.ntotal + 1), cudaMemcpyDeviceToHost,
+                                s->stream));
+      PMPM_CUDA(cudaStreamSynchronize(s->stream));
+      for (int c = 0; c < g.ntotal; c++) {
+        const bool occupied = off[c + 1] > off[c];
+        host[c] = occupied ? (field == PMPM_FIELD_CELL_START ? off[c] : off[c + 1]) : 0;
+      }
+    }
+    if (on_device) {
+      PMPM_CUDA(cudaMemcpy(dst, host.data(), need, cudaMemcpyHostToDevice));
+    } else {
+      memcpy(dst, host.data(), need);
+    }
+    return PMPM_OK;
+  }
+  PMPM_TRY(ensure_staging(s, need));
+  if (field >= PMPM_FIELD_NODE_MASSES && field <= PMPM_FIELD_NODE_MOMENTS_NT) {
+    const float *src = field == PMPM_FIELD_NODE_MASSES ? s->N.m : (field == PMPM_FIELD_NODE_MOMENTS ? s->N.p : s->N.pnt);
+    const int ncomp = field == PMPM_FIELD_NODE_MASSES ? 1 : D;
+    k_get_nodes<<<blocks_for(s->g.ntotal), kTPB, 0, s->stream>>>(s->g, D, ncomp, src, s->node_epoch, s->p2g_epoch,
+                                                                  (float *)s->staging);
+    PMPM_LAUNCHED();
+    return copy_out(s, s->staging, dst, need, on_device);
+  }
+  int kind = -1;
+  const void *src = nullptr;
+  DevGrid *gdev = nullptr;
+  switch (field) {
+    case PMPM_FIELD_POSITIONS: kind = 0; src = P.x; break;
+    case PMPM_FIELD_VELOCITIES: kind = 0; src = P.v; break;
+    case PMPM_FIELD_FORCES_EXTERNAL:
+      if (!P.fext) {
+        PMPM_CUDA(cudaMemsetAsync(s->staging, 0, need, s->stream));
+        return copy_out(s, s->staging, dst, need, on_device);
+      }
+      kind = 0;
+      src = P.fext;
+      break;
+    case PMPM_FIELD_STRESSES: kind = 2; src = P.sig; break;
+    case PMPM_FIELD_STRESS_REF:
+      if (!P.sref) {
+        PMPM_CUDA(cudaMemsetAsync(s->staging, 0, need, s->stream));
+        return copy_out(s, s->staging, dst, need, on_device);
+      }
+      kind = 2;
+      src = P.sref;
+      break;
+    case PMPM_FIELD_F: kind = 1; src = P.F; break;
+    case PMPM_FIELD_VELOCITY_GRADIENT: kind = 1; src = P.L; break;
+    case PMPM_FIELD_EPS_E:
+      if (!P.eps) {
+        PMPM_CUDA(cudaMemsetAsync(s->staging, 0, need, s->stream));
+        return copy_out(s, s->staging, dst, need, on_device);
+      }
+      kind = 3;
+      src = P.eps;
+      break;
+    case PMPM_FIELD_MASSES: kind = 4; src = P.m; break;
+    case PMPM_FIELD_VOLUMES: kind = 4; src = P.V; break;
+    case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; src = P.V0; break;
+    case PMPM_FIELD_COLORS: kind = 5; src = P.color; break;
+    case PMPM_FIELD_IS_RIGID: kind = 5; src = P.rigid; break;
+    case PMPM_FIELD_IS_ACTIVE: kind = 5; src = P.active; break;
+    case PMPM_FIELD_HASH_UNSORTED: kind = 6; src = P.hash; break;
+    case PMPM_FIELD_BINS: {
+      kind = 7;
+      PMPM_TRY(ensure_staging(s, need + sizeof(DevGrid) + 256));
+      gdev = (DevGrid *)((char *)s->staging + ((need + 255) / 256) * 256);
+      PMPM_CUDA(cudaMemcpyAsync(gdev, &s->g, sizeof(DevGrid), cudaMemcpyHostToDevice, s->stream));
+      src = gdev;
+      break;
+    }
+    default: return PMPM_ERR_INVALID_ARGUMENT;
+  }
+  k_get_particles<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, D, kind, src, s->staging, 0);
+  PMPM_LAUNCHED();
+  return copy_out(s, s->staging, dst, need, on_device);
+}
+
+int pmpm_set_field(pmpm_sim *s, int field, const void *src, size_t bytes, int on_device) {
+  if (!s || !src) return PMPM_ERR_INVALID_ARGUMENT;
+  size_t need = 0;
+  PMPM_TRY(field_info(s, field, &need));
+  if (bytes != need) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  const DevParticles &P = s->P[s->cur];
+  int kind = -1;
+  void *dstp = nullptr;
+  switch (field) {
+    case PMPM_FIELD_POSITIONS: kind = 0; dstp = P.x; break;
+    case PMPM_FIELD_VELOCITIES: kind = 0; dstp = P.v; break;
+    case PMPM_FIELD_STRESSES: kind = 2; dstp = P.sig; break;
+    case PMPM_FIELD_STRESS_REF: kind = 2; dstp = P.sref; break;
+    case PMPM_FIELD_F: kind = 1; dstp = P.F; break;
+    case PMPM_FIELD_VELOCITY_GRADIENT: kind = 1; dstp = P.L; break;
+    case PMPM_FIELD_EPS_E: kind = 3; dstp = P.eps; break;
+    case PMPM_FIELD_MASSES: kind = 4; dstp = P.m; break;
+    case PMPM_FIELD_VOLUMES: kind = 4; dstp = P.V; break;
+    case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; dstp = P.V0; break;
+    case PMPM_FIELD_COLORS: kind = 5; dstp = P.color; break;
+    case PMPM_FIELD_IS_RIGID: kind = 5; dstp = P.rigid; break;
+    case PMPM_FIELD_IS_ACTIVE: kind = 5; dstp = P.active; break;
+    case PMPM_FIELD_FORCES_EXTERNAL: kind = 0; dstp = P.fext; break;
+    default: return PMPM_ERR_NOT_SUPPORTED;
+  }
+  if (!dstp) return PMPM_ERR_NOT_SUPPORTED;  // field not held by this configuration
+  const void *dsrc = src;
+  if (!on_device) {
+    PMPM_TRY(ensure_staging(s, need));
+    PMPM_CUDA(cudaMemcpyAsync(s->staging, src, need, cudaMemcpyHostToDevice, s->stream));
+    dsrc = s->staging;
+  }
+  k_set_particles<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, s->dim, kind, dsrc, dstp);
+  PMPM_LAUNCHED();
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMPM_OK;
+}
+
+int pmpm_shape_functions(pmpm_sim *s, float *psi, float *dpsi, int on_device) {
+  if (!s || !psi || !dpsi) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  const size_t nsn = (size_t)pmpm_num_surround_nodes(s);
+  const size_t bpsi = (size_t)s->n * nsn * 4, bdpsi = bpsi * s->dim;
+  PMPM_TRY(ensure_staging(s, bpsi + bdpsi));
+  float *dp = (float *)s->staging;
+  float *dd = dp + (size_t)s->n * nsn;
+  StepArgs a = make_args(s);
+#define PMPM_SHAPE_LAUNCH(D, SF) k_shape_dump<D, SF><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, dp, dd)
+  if (s->dim == 2) {
+    if (s->shape == PMPM_SHAPE_LINEAR) PMPM_SHAPE_LAUNCH(2, PMPM_SHAPE_LINEAR);
+    else if (s->shape == PMPM_SHAPE_QUADRATIC) PMPM_SHAPE_LAUNCH(2, PMPM_SHAPE_QUADRATIC);
+    else PMPM_SHAPE_LAUNCH(2, PMPM_SHAPE_CUBIC);
+  } else {
+    if (s->shape == PMPM_SHAPE_LINEAR) PMPM_SHAPE_LAUNCH(3, PMPM_SHAPE_LINEAR);
+    else if (s->shape == PMPM_SHAPE_QUADRATIC) PMPM_SHAPE_LAUNCH(3, PMPM_SHAPE_QUADRATIC);
+    else PMPM_SHAPE_LAUNCH(3, PMPM_SHAPE_CUBIC);
+  }
+#undef PMPM_SHAPE_LAUNCH
+  PMPM_LAUNCHED();
+  const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  PMPM_CUDA(cudaMemcpyAsync(psi, dp, bpsi, kd, s->stream));
+  PMPM_CUDA(cudaMemcpyAsync(dpsi, dd, bdpsi, kd, s->stream));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMPM_OK;
+}
+
+int pmpm_p2g(pmpm_sim *s, int apply_bcs) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0 || !s->partitioned) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  return PMPM_DISPATCH(s, launch_p2g, s, apply_bcs ? 1 : 0);
+}
+
+int pmpm_g2p(pmpm_sim *s, int stress_update) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0 || !s->partitioned) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  return PMPM_DISPATCH(s, launch_g2p, s, stress_update ? 1 : 0, 1);
+}
+
+int pmpm_stress_update(pmpm_sim *s) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  StepArgs a = make_args(s);
+  if (s->dim == 2)
+    k_stress_update<2><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a);
+  else
+    k_stress_update<3><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a);
+  PMPM_LAUNCHED();
+  return PMPM_OK;
+}
+
+int pmpm_solve(pmpm_sim *s, int nsteps) {
+  if (!s || nsteps < 0) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  for (int k = 0; k < nsteps; k++) PMPM_TRY(PMPM_DISPATCH(s, step_once, s));
+  return PMPM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+template <int D, int SF>
+int profile_step(pmpm_sim *s, float *ms, int *launches) {
+  cudaEvent_t ev[4];
+  for (int k = 0; k < 4; k++) PMPM_CUDA(cudaEventCreate(&ev[k]));
+  int n_launch = 0;
+  PMPM_CUDA(cudaEventRecord(ev[0], s->stream));
+  PMPM_TRY((launch_partition<D, SF>(s)));
+  n_launch += 7;
+  if (s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
+    PMPM_TRY(launch_reorder<D>(s));
+    n_launch += 1;
+  } else {
+    s->steps_since_sort += 1;
+  }
+  PMPM_CUDA(cudaEventRecord(ev[1], s->stream));
+  PMPM_TRY((launch_p2g<D, SF>(s, 1)));
+  n_launch += 1;
+  PMPM_CUDA(cudaEventRecord(ev[2], s->stream));
+  const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
+  PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
+  n_launch += 1;
+  PMPM_CUDA(cudaEventRecord(ev[3], s->stream));
+  s->step += 1;
+  PMPM_CUDA(cudaEventSynchronize(ev[3]));
+  for (int k = 0; k < 3; k++) PMPM_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+  for (int k = 0; k < 4; k++) cudaEventDestroy(ev[k]);
+  if (launches) *launches = n_launch;
+  return PMPM_OK;
+}
+
+__global__ void k_count_active(const float *m, int n, float cutoff, int *count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool a = i < n && m[i] > cutoff;
+  unsigned b = __ballot_sync(0xffffffffu, a);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
+}
+}  // namespace
+
+extern "C" {
+
+int pmpm_profile_step(pmpm_sim *s, float ms[3], int *launches) {
+  if (!s || !ms) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  return PMPM_DISPATCH(s, profile_step, s, ms, launches);
+}
+
+int pmpm_launch_count(const pmpm_sim *s, long long *count) {
+  if (!s || !count) return PMPM_ERR_INVALID_ARGUMENT;
+  *count = s->launches;
+  return PMPM_OK;
+}
+
+int pmpm_active_nodes(pmpm_sim *s, int *count) {
+  if (!s || !count) return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  const int nn = s->g.ntotal;
+  PMPM_TRY(ensure_staging(s, (size_t)nn * 4 + 256));
+  float *m = (float *)s->staging;
+  k_get_nodes<<<blocks_for(nn), kTPB, 0, s->stream>>>(s->g, s->dim, 1, s->N.m, s->node_epoch, s->p2g_epoch, m);
+  PMPM_LAUNCHED();
+  int *cnt = (int *)((char *)s->staging + (size_t)nn * 4 + 128 - ((size_t)nn * 4) % 128);
+  PMPM_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), s->stream));
+  k_count_active<<<blocks_for(nn), kTPB, 0, s->stream>>>(m, nn, 0.000000001f, cnt);
+  PMPM_LAUNCHED();
+  PMPM_CUDA(cudaMemcpyAsync(count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMPM_OK;
+}
+
+int pmpm_get_step(const pmpm_sim *s, int *step) {
+  if (!s || !step) return PMPM_ERR_INVALID_ARGUMENT;
+  *step = s->step;
+  return PMPM_OK;
+}
+
+int pmpm_set_step(pmpm_sim *s, int step) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  s->step = step;
+  return PMPM_OK;
+}
+
+int pmpm_synchronize(pmpm_sim *s) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  int f = 0;
+  PMPM_CUDA(cudaMemcpyAsync(&f, s->fault, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  if (f) PMPM_CUDA(cudaMemset(s->fault, 0, sizeof(int)));
+  if (f & kFaultNonFinite) return PMPM_ERR_NONFINITE;
+  if (f & kFaultOutOfDomain) return PMPM_ERR_OUT_OF_DOMAIN;
+  if (f & kFaultCellOverflow) return PMPM_ERR_CELL_OVERFLOW;
+  return PMPM_OK;
+}
+
+int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float dt, const float *L, float *stress,
+                               float *eps_e, const float *stress_ref, const float *masses, const float *volumes,
+                               const float *volumes_original, int velgrad_is_strain_increment, int device) {
+  if (!mat || (dim != 2 && dim != 3) || n < 0 || !L || !stress) return PMPM_ERR_INVALID_ARGUMENT;
+  if (mat->type == PMPM_MAT_DRUCKER_PRAGER && (!eps_e || !stress_ref)) return PMPM_ERR_INVALID_ARGUMENT;
+  if (mat->type == PMPM_MAT_NEWTON_FLUID && (!masses || !volumes || !volumes_original))
+    return PMPM_ERR_INVALID_ARGUMENT;
+  if (n == 0) return PMPM_OK;
+  PMPM_CUDA(cudaSetDevice(device));
+  DevMaterial dm;
+  dm.type = mat->type;
+  dm.density = mat->density;
+  memcpy(dm.p, mat->params, sizeof(dm.p));
+  if (mat->type == PMPM_MAT_NEWTON_FLUID) dm.p[3] = (float)(2.0 * (double)mat->params[0] / 3.0);
+  const size_t dd = (size_t)dim * dim;
+  std::vector<void *> bufs;
+  auto up = [&](const float *h, size_t count, float **d) -> int {
+    *d = nullptr;
+    if (!h) return PMPM_OK;
+    PMPM_TRY(dalloc(d, count));
+    bufs.push_back(*d);
+    PMPM_CUDA(cudaMemcpy(*d, h, count * 4, cudaMemcpyHostToDevice));
+    return PMPM_OK;
+  };
+  float *dL, *dS, *dE, *dR, *dm_, *dV, *dV0;
+  int st = up(L, n * dd, &dL);
+  if (st == PMPM_OK) st = up(stress, (size_t)n * 9, &dS);
+  if (st == PMPM_OK) st = up(eps_e, n * dd, &dE);
+  if (st == PMPM_OK) st = up(stress_ref, (size_t)n * 9, &dR);
+  if (st == PMPM_OK) st = up(masses, (size_t)n, &dm_);
+  if (st == PMPM_OK) st = up(volumes, (size_t)n, &dV);
+  if (st == PMPM_OK) st = up(volumes_original, (size_t)n, &dV0);
+  if (st == PMPM_OK) {
+    if (dim == 2)
+      k_point_update<2><<<blocks_for(n), kTPB>>>(dm, n, dt, dL, dS, dE, dR, dm_, dV, dV0, velgrad_is_strain_increment);
+    else
+      k_point_update<3><<<blocks_for(n), kTPB>>>(dm, n, dt, dL, dS, dE, dR, dm_, dV, dV0, velgrad_is_strain_increment);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = PMPM_ERR_CUDA;
+  }
+  if (st == PMPM_OK && cudaMemcpy(stress, dS, (size_t)n * 9 * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = PMPM_ERR_CUDA;
+  if (st == PMPM_OK && eps_e && cudaMemcpy(eps_e, dE, n * dd * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = PMPM_ERR_CUDA;
+  for (void *p : bufs) cudaFree(p);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,539 @@
+// Device-side data layout and per-point math of the USL step (sm_100a).
+//
+// Layout in HBM (all FP32 unless noted), structure-of-arrays with one
+// contiguous array per tensor component ("component-major"):
+//   particle field f, component c, storage slot s  ->  f[c * stride + s]
+// stride is the particle count rounded up to 64 so every component array
+// starts 256-byte aligned.  Symmetric tensors keep only their independent
+// components:
+//   stress  2D: xx yy xy zz           3D: xx yy zz xy xz yz
+//   eps_e   2D: xx yy xy              3D: xx yy zz xy xz yz
+// F and the velocity gradient L are full dim x dim, row-major components.
+// Grid nodes are dense, x-fastest (the reference NODE_MEM_INDEX order), one
+// array per component: m, p (moments), pnt (moments_nt), v = p/m, vnt = pnt/m.
+#pragma once
+
+#include <cstdint>
+
+#include "pmpm.h"
+
+namespace pmpm {
+
+constexpr int kMaxMat = PMPM_MAX_MATERIALS;
+constexpr int kMaxBC = PMPM_MAX_BCS;
+
+// fault word bits (first fault wins the status)
+enum : int { kFaultOutOfDomain = 1, kFaultNonFinite = 2, kFaultCellOverflow = 4 };
+
+struct DevGrid {
+  float origin[3];
+  float end[3];
+  float h, inv_h;
+  int n[3];
+  int ntotal;
+  int tdim[3];  // tiles per axis
+  int ntiles;
+};
+
+// Node tiles: the unit of P2G work and of grid activity tracking.
+template <int D>
+struct TileDims;
+template <>
+struct TileDims<2> {
+  static constexpr int X = 16, Y = 16, Z = 1, N = 256;
+};
+template <>
+struct TileDims<3> {
+  static constexpr int X = 8, Y = 8, Z = 8, N = 512;
+};
+
+template <int D>
+struct Sym {
+  static constexpr int S = (D == 2) ? 4 : 6;  // stress components
+  static constexpr int E = (D == 2) ? 3 : 6;  // elastic strain components
+};
+
+struct DevParticles {
+  int n;
+  int stride;
+  float *x, *v, *F, *sig, *L, *m, *V, *V0, *fext, *eps, *sref;
+  uint8_t *color, *active, *rigid;
+  int *id;             // original particle id of each storage slot
+  unsigned int *hash;  // cell hash of the last partition
+  int *slot;           // rank inside the cell from the counting pass (-1: not binned)
+};
+
+struct DevNodes {
+  float *m, *p, *pnt, *v, *vnt;
+  int *tile_epoch;  // tile active in the partition whose epoch it holds
+};
+
+struct DevBins {
+  int *count;       // per cell, zero between steps
+  int *offset;      // exclusive prefix, ntotal + 1 entries
+  int *order;       // sorted position -> storage slot
+  int *block_sums;  // scan scratch
+  int *scalars;     // [0] binned count, [1] unbinned counter, [2] big-cell count
+  int *big_cells;   // cells too large for the in-register sort
+};
+
+struct DevMaterial {
+  int type;
+  float density;
+  float p[8];
+};
+
+struct DevBC {
+  int type;
+  int i[8];
+  float r[12];  // gravity: r[0..2] is the gravity in force this step
+  const float *values;
+  const uint8_t *mask;
+};
+
+struct StepArgs {
+  DevGrid g;
+  DevParticles P;
+  DevNodes N;
+  DevBins B;
+  float dt, alpha, one_minus_alpha, cutoff;
+  int epoch;
+  unsigned flags;
+  int *fault;
+  int nmat;
+  int nbc;
+  int has_planar;
+  int has_sref;
+  DevMaterial mat[kMaxMat];
+  DevBC bc[kMaxBC];
+};
+
+// --------------------------------------------------------------------------
+// index helpers
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ int flat_index(const DevGrid &g, int x, int y, int z) {
+  return x + y * g.n[0] + z * g.n[0] * g.n[1];
+}
+
+// Cell coordinate of a position: (int)((x - origin) * inv_h), truncation
+// toward zero, FP32 subtract then multiply (no contraction possible), as
+// calculate_hashes (src/spatialpartition/spatialpartition_inline.h:49-62).
+__device__ __forceinline__ float scaled_coord(float x, float o, float inv_h) {
+  return __fmul_rn(__fsub_rn(x, o), inv_h);
+}
+
+// Boundary-modified cubic B-spline node type of a node index (one axis):
+// NodesContainer::calculate_bin_types (src/nodes/nodes.cpp:135-173).
+__device__ __forceinline__ int cubic_node_type(int i, int n) {
+  if (i == 0 || i == n - 1) return 1;
+  if (i == 1) return 2;
+  return 3;
+}
+
+// --------------------------------------------------------------------------
+// shape functions, one axis
+// --------------------------------------------------------------------------
+
+// Horner coefficients of the boundary-modified cubic B-spline by node type
+// (0..4) and unit interval [-2,-1), [-1,0), [0,1), [1,2): weight
+// ((c3 r + c2) r + c1) r + c0, derivative (d2 r + d1) r + d0 (times 1/h).
+// Same piecewise polynomials as src/shapefunction/cubic.cuh:28-197.
+__constant__ float kCubicW[5][4][4] = {
+    {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},
+    {{1.0f / 6.0f, 1.0f, 2.0f, 4.0f / 3.0f},
+     {-1.0f / 6.0f, 0.0f, 1.0f, 1.0f},
+     {1.0f / 6.0f, 0.0f, -1.0f, 1.0f},
+     {-1.0f / 6.0f, 1.0f, -2.0f, 4.0f / 3.0f}},
+    {{0, 0, 0, 0},
+     {-1.0f / 3.0f, -1.0f, 0.0f, 2.0f / 3.0f},
+     {0.5f, -1.0f, 0.0f, 2.0f / 3.0f},
+     {-1.0f / 6.0f, 1.0f, -2.0f, 4.0f / 3.0f}},
+    {{1.0f / 6.0f, 1.0f, 2.0f, 4.0f / 3.0f},
+     {-0.5f, -1.0f, 0.0f, 2.0f / 3.0f},
+     {0.5f, -1.0f, 0.0f, 2.0f / 3.0f},
+     {-1.0f / 6.0f, 1.0f, -2.0f, 4.0f / 3.0f}},
+    {{1.0f / 6.0f, 1.0f, 2.0f, 4.0f / 3.0f},
+     {-0.5f, -1.0f, 0.0f, 2.0f / 3.0f},
+     {1.0f / 3.0f, -1.0f, 0.0f, 2.0f / 3.0f},
+     {0, 0, 0, 0}},
+};
+__constant__ float kCubicD[5][4][3] = {
+    {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}},
+    {{0.5f, 2.0f, 2.0f}, {-0.5f, 0.0f, 1.0f}, {0.5f, 0.0f, -1.0f}, {-0.5f, 2.0f, -2.0f}},
+    {{0, 0, 0}, {-1.0f, -2.0f, 0.0f}, {1.5f, -2.0f, 0.0f}, {-0.5f, 2.0f, -2.0f}},
+    {{0.5f, 2.0f, 2.0f}, {-1.5f, -2.0f, 0.0f}, {1.5f, -2.0f, 0.0f}, {-0.5f, 2.0f, -2.0f}},
+    {{0.5f, 2.0f, 2.0f}, {-1.5f, -2.0f, 0.0f}, {1.0f, -2.0f, 0.0f}, {0, 0, 0}},
+};
+
+// Weight and derivative of one axis for relative coordinate r (in cells).
+// linear: src/shapefunction/linear.cuh:28-52 (derivative 0 at r == 0);
+// quadratic: uniform C1 quadratic B-spline of support 3h;
+// cubic: table above, node type `type`.
+template <int SF>
+__device__ __forceinline__ void axis_weight(float r, float inv_h, int type, float &N, float &dN) {
+  if (SF == PMPM_SHAPE_LINEAR) {
+    float ar = fabsf(r);
+    N = ar >= 1.0f ? 0.0f : 1.0f - ar;
+    if (r > 1.0f || r < -1.0f || r == 0.0f)
+      dN = 0.0f;
+    else
+      dN = r > 0.0f ? -inv_h : inv_h;
+  } else if (SF == PMPM_SHAPE_QUADRATIC) {
+    float ar = fabsf(r);
+    if (ar < 0.5f) {
+      N = 0.75f - r * r;
+      dN = inv_h * (-2.0f * r);
+    } else if (ar < 1.5f) {
+      float t = 1.5f - ar;
+      N = 0.5f * t * t;
+      dN = inv_h * (r > 0.0f ? -t : t);
+    } else {
+      N = 0.0f;
+      dN = 0.0f;
+    }
+  } else {
+    int k = -1;
+    if (r >= -2.0f && r < -1.0f)
+      k = 0;
+    else if (r >= -1.0f && r < 0.0f)
+      k = 1;
+    else if (r >= 0.0f && r < 1.0f)
+      k = 2;
+    else if (r >= 1.0f && r < 2.0f)
+      k = 3;
+    if (k < 0) {
+      N = 0.0f;
+      dN = 0.0f;
+    } else {
+      const float *c = kCubicW[type][k];
+      const float *d = kCubicD[type][k];
+      N = ((c[0] * r + c[1]) * r + c[2]) * r + c[3];
+      dN = inv_h * ((d[0] * r + d[1]) * r + d[2]);
+    }
+  }
+}
+
+// Stencil geometry per shape function: window width and first offset in the
+// reference slot tables (src/common/global_settings.cpp:108-150); the
+// quadratic B-spline has three non-zero nodes per axis inside that window.
+template <int SF>
+struct Stencil;
+template <>
+struct Stencil<PMPM_SHAPE_LINEAR> {
+  static constexpr int WIN = 2, WLO = 0, K = 2;
+};
+template <>
+struct Stencil<PMPM_SHAPE_QUADRATIC> {
+  static constexpr int WIN = 4, WLO = -1, K = 3;
+};
+template <>
+struct Stencil<PMPM_SHAPE_CUBIC> {
+  static constexpr int WIN = 4, WLO = -1, K = 4;
+};
+
+// Window offset of reference slot `sid` (2D x-fastest; 3D z-fastest, then x,
+// then y).
+template <int D, int SF>
+__device__ __forceinline__ void window_offset(int sid, int w[3]) {
+  constexpr int W = Stencil<SF>::WIN, LO = Stencil<SF>::WLO;
+  w[0] = w[1] = w[2] = 0;
+  if (D == 2) {
+    w[0] = LO + sid % W;
+    w[1] = LO + sid / W;
+  } else {
+    w[2] = LO + sid % W;
+    w[0] = LO + (sid / W) % W;
+    w[1] = LO + sid / (W * W);
+  }
+}
+
+// --------------------------------------------------------------------------
+// symmetric tensor helpers
+// --------------------------------------------------------------------------
+
+// index of (a,b) in the symmetric stress storage
+template <int D>
+__device__ __forceinline__ int sig_index(int a, int b) {
+  if (D == 2) {
+    if (a == b) return a == 2 ? 3 : a;
+    if (a + b == 1) return 2;  // xy
+    return -1;                 // xz / yz are not stored in 2D
+  } else {
+    if (a == b) return a;
+    int s = a + b;  // 1: xy, 2: xz, 3: yz
+    return 2 + s;
+  }
+}
+template <int D>
+__device__ __forceinline__ int eps_index(int a, int b) {
+  if (D == 2) {
+    if (a == b) return a;
+    return 2;
+  } else {
+    if (a == b) return a;
+    return 2 + a + b;
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void load_sig3(const DevParticles &P, int s, float S[9]) {
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      int k = sig_index<D>(a, b);
+      S[3 * a + b] = k < 0 ? 0.0f : P.sig[k * P.stride + s];
+    }
+}
+template <int D>
+__device__ __forceinline__ void store_sig3(const DevParticles &P, int s, const float S[9]) {
+  if (D == 2) {
+    P.sig[0 * P.stride + s] = S[0];
+    P.sig[1 * P.stride + s] = S[4];
+    P.sig[2 * P.stride + s] = S[1];
+    P.sig[3 * P.stride + s] = S[8];
+  } else {
+    P.sig[0 * P.stride + s] = S[0];
+    P.sig[1 * P.stride + s] = S[4];
+    P.sig[2 * P.stride + s] = S[8];
+    P.sig[3 * P.stride + s] = S[1];
+    P.sig[4 * P.stride + s] = S[2];
+    P.sig[5 * P.stride + s] = S[5];
+  }
+}
+
+// --------------------------------------------------------------------------
+// materials (per point)
+// --------------------------------------------------------------------------
+
+// update_linearelastic (src/materials/linearelastic_inline.h:40-107):
+// deps = sym(L) dt; sigma_DIM += lame*deps + 2G*deps (the reference's matrix
+// product lame*deps*I); corrected: lame tr(deps) I + 2G deps (+ plane strain zz).
+template <int D>
+__device__ __forceinline__ void le_update(const DevMaterial &mt, const float *L, float dt, float S[9]) {
+  float lame = mt.p[2], two_g = 2.0f * mt.p[3];
+  bool corrected = mt.p[5] != 0.0f;
+  float deps[9];
+  float tr = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) deps[a * D + b] = (0.5f * (L[a * D + b] + L[b * D + a])) * dt;
+#pragma unroll
+  for (int a = 0; a < D; a++) tr += deps[a * D + a];
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      float e = deps[a * D + b];
+      float inc = corrected ? ((a == b ? lame * tr : 0.0f) + two_g * e) : (lame * e + two_g * e);
+      S[3 * a + b] += inc;
+    }
+  if (corrected && D == 2) S[8] += lame * tr;
+}
+
+// stress_update_newtonfluid (src/materials/newtonfluid_inline.h:49-96):
+// pressure from the Tait law on rho/rho0 = V0/V; deviator (2 mu / 3) dev(D).
+template <int D>
+__device__ __forceinline__ void nf_update(const DevMaterial &mt, const float *L, float mass, float vol,
+                                          float vol0, float S[9]) {
+  float visc = mt.p[0], bulk = mt.p[1], gamma = mt.p[2];
+  float rho = mass / vol, rho0 = mass / vol0;
+  float pressure = -bulk * (powf(rho / rho0, gamma) - 1.0f);
+  float Dm[9];
+  float tr = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) Dm[a * D + b] = 0.5f * (L[a * D + b] + L[b * D + a]);
+#pragma unroll
+  for (int a = 0; a < D; a++) tr += Dm[a * D + a];
+  const float third = 1.0f / 3.0f;
+  (void)visc;
+  const float c2 = mt.p[3];  // 2 mu / 3, computed on the host in FP64 and rounded
+#pragma unroll
+  for (int k = 0; k < 9; k++) S[k] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      float dev = Dm[a * D + b] - (a == b ? third * tr : 0.0f);
+      S[3 * a + b] = (a == b ? pressure : 0.0f) + dev * c2;
+    }
+}
+
+// Drucker-Prager cone/apex return mapping: update_dp_rheo
+// (src/materials/dp_rheo_inline.h:123-246), return_mapping_cone (:50-65),
+// return_mapping_apex (:67-78), update_plasticity (:80-96).  eps (D x D,
+// full) and sref (3 x 3) are local copies; the yield function is
+// sqrt(J2) + eta p - kc, the apex return sets s = 0 and p = p_apex.
+// Scalars of the return are evaluated in FP64 as in the reference.
+template <int D>
+__device__ __forceinline__ void dp_update(const float *prm, const float *L, float dt, float eps[9],
+                                          const float sref[9], float S[9], bool velgrad_is_increment) {
+  const float K = prm[0], G = prm[1], eta = prm[2], eta_bar = prm[3], kc = prm[4], p_apex = prm[5];
+  const bool has_apex = prm[6] != 0.0f;
+  float deps[9];
+  if (velgrad_is_increment) {
+#pragma unroll
+    for (int k = 0; k < D * D; k++) deps[k] = L[k];
+  } else {
+    float W[9];
+#pragma unroll
+    for (int a = 0; a < D; a++)
+#pragma unroll
+      for (int b = 0; b < D; b++) {
+        deps[a * D + b] = (0.5f * (L[a * D + b] + L[b * D + a])) * dt;
+        W[a * D + b] = (0.5f * (L[a * D + b] - L[b * D + a])) * dt;
+      }
+#pragma unroll
+    for (int a = 0; a < D; a++)
+#pragma unroll
+      for (int b = 0; b < D; b++) {
+        float we = 0.0f, ew = 0.0f;
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+          we += W[a * D + k] * eps[k * D + b];
+          ew += eps[a * D + k] * W[k * D + b];
+        }
+        deps[a * D + b] += -we + ew;
+      }
+  }
+  const float p_ref = (1.0f / 3.0f) * ((sref[0] + sref[4]) + sref[8]);
+  float s_ref[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] -= p_ref;
+  s_ref[4] -= p_ref;
+  s_ref[8] -= p_ref;
+  float eps_tr[9];
+#pragma unroll
+  for (int k = 0; k < D * D; k++) eps_tr[k] = eps[k] + deps[k];
+  float ev = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++) ev += eps_tr[a * D + a];
+  const float p_tr = p_ref + K * ev;
+  float edev[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) edev[k] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) edev[3 * a + b] = eps_tr[a * D + b];
+  const float third_ev = (1.0f / 3.0f) * ev;
+#pragma unroll
+  for (int a = 0; a < 3; a++) edev[3 * a + a] -= third_ev;
+  if (D < 3) edev[8] = 0.0f;
+  const float two_g = 2.0f * G;
+  float s_tr[9];
+  float ss = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    s_tr[k] = s_ref[k] + two_g * edev[k];
+    ss += s_tr[k] * s_tr[k];
+  }
+  const float J2 = 0.5f * ss;
+  const float sqrtJ2 = sqrtf(J2);
+  const float Phi = (sqrtJ2 + eta * p_tr) - kc;
+  if (Phi <= 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) S[k] = s_tr[k];
+    S[0] += p_tr;
+    S[4] += p_tr;
+    S[8] += p_tr;
+#pragma unroll
+    for (int k = 0; k < D * D; k++) eps[k] = eps_tr[k];
+    return;
+  }
+  const double dgamma = (double)Phi / ((double)K * (double)eta * (double)eta_bar + (double)G);
+  double p_next = (double)p_tr - (double)K * (double)eta_bar * dgamma;
+  float s_next[9];
+  const bool apex = has_apex && ((double)sqrtJ2 - (double)G * dgamma < 0.0);
+  if (apex) {
+    p_next = (double)p_apex;
+#pragma unroll
+    for (int k = 0; k < 9; k++) s_next[k] = 0.0f;
+  } else {
+    const double scale = 1.0 - ((double)G * dgamma) / (double)sqrtJ2;
+#pragma unroll
+    for (int k = 0; k < 9; k++) s_next[k] = (float)(scale * (double)s_tr[k]);
+  }
+  const float pn = (float)p_next;
+#pragma unroll
+  for (int k = 0; k < 9; k++) S[k] = s_next[k];
+  S[0] += pn;
+  S[4] += pn;
+  S[8] += pn;
+  const double inv2g = 1.0 / (2.0 * (double)G);
+  const float dpk = (float)(((double)pn - (double)p_ref) / (3.0 * (double)K));
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      float e = (float)((double)(s_next[3 * a + b] - s_ref[3 * a + b]) * inv2g);
+      if (a == b) e += dpk;
+      eps[a * D + b] = e;
+    }
+}
+
+// --------------------------------------------------------------------------
+// node epilogue: P2G result -> boundary conditions -> velocities
+// --------------------------------------------------------------------------
+
+// Applies the node boundary conditions in list order to (p, pnt) of node
+// `node` with coordinates nc and mass m:
+//   Gravity    (src/boundaryconditions/gravity_inline.h:46-63): pnt += g m dt, m > 1e-9
+//   NodeDomain (src/boundaryconditions/nodedomain_inline.h:40-87): m > 1e-5;
+//              face0 where id < 1, face1 where id >= n-1; mode 0 zeroes both
+//              vectors, mode 1 clamps the normal component
+//   BodyForce  (src/boundaryconditions/bodyforce_inline.h:41-59): masked nodes;
+//              "fixed" sets pnt, other modes add to p
+template <int D>
+__device__ __forceinline__ void node_bcs(const StepArgs &a, int node, const int nc[3], float m, float p[3],
+                                         float pnt[3]) {
+  for (int k = 0; k < a.nbc; k++) {
+    const DevBC &bc = a.bc[k];
+    if (bc.type == PMPM_BC_GRAVITY) {
+      if (m > 0.000000001f) {
+#pragma unroll
+        for (int c = 0; c < D; c++) pnt[c] += (bc.r[c] * m) * a.dt;
+      }
+    } else if (bc.type == PMPM_BC_NODEDOMAIN) {
+      if (m > 0.00001f) {
+#pragma unroll
+        for (int c = 0; c < D; c++) {
+          if (nc[c] < 1) {
+            if (bc.i[c] == 0) {
+#pragma unroll
+              for (int e = 0; e < D; e++) p[e] = pnt[e] = 0.0f;
+            } else if (bc.i[c] == 1) {
+              p[c] = fmaxf(0.0f, p[c]);
+              pnt[c] = fmaxf(0.0f, pnt[c]);
+            }
+          } else if (nc[c] >= a.g.n[c] - 1) {
+            if (bc.i[3 + c] == 0) {
+#pragma unroll
+              for (int e = 0; e < D; e++) p[e] = pnt[e] = 0.0f;
+            } else if (bc.i[3 + c] == 1) {
+              p[c] = fminf(0.0f, p[c]);
+              pnt[c] = fminf(0.0f, pnt[c]);
+            }
+          }
+        }
+      }
+    } else if (bc.type == PMPM_BC_BODYFORCE) {
+      if (bc.i[1] && bc.mask[node]) {
+        if (bc.i[0] == 2) {
+#pragma unroll
+          for (int c = 0; c < D; c++) pnt[c] = bc.values[(size_t)node * D + c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < D; c++) p[c] += bc.values[(size_t)node * D + c];
+        }
+      }
+    }
+  }
+}
+
+}  // namespace pmpm

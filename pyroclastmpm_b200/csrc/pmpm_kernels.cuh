@@ -1,0 +1,796 @@
+// sm_100a kernels of the USL step.
+//
+// One step (USL::solve, src/solver/usl/usl.cpp:69-115) runs as:
+//   k_hash_count   cell hash per particle, per-cell counts (atomics), grid
+//                  tile activity, PlanarDomain external force
+//   k_scan_*       exclusive prefix over cells -> CSR offsets
+//   k_scatter      particles into cell order
+//   k_sort_cells / k_sort_big
+//                  order inside each cell by particle id, which makes the
+//                  permutation identical to the reference's stable sort and
+//                  the P2G summation order deterministic
+//   k_reorder      (every resort_interval steps) physical re-sort of particle
+//                  storage into cell order
+//   k_p2g_gather   one CTA per active node tile, one thread per node: P2G in
+//                  the reference's per-node order with shape functions
+//                  evaluated in registers, fused node epilogue (BCs, v = p/m)
+//   k_g2p          one thread per particle: G2P, F, V and the material
+//                  stress update fused
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pmpm_device.cuh"
+
+namespace pmpm {
+
+template <int B, int E>
+struct IPow {
+  static constexpr int value = B * IPow<B, E - 1>::value;
+};
+template <int B>
+struct IPow<B, 0> {
+  static constexpr int value = 1;
+};
+
+template <int D>
+__device__ __forceinline__ int tile_of(const DevGrid &g, const int c[3]) {
+  using T = TileDims<D>;
+  int tx = c[0] / T::X, ty = c[1] / T::Y, tz = (D == 3) ? c[2] / T::Z : 0;
+  return tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
+}
+
+// --------------------------------------------------------------------------
+// binning
+// --------------------------------------------------------------------------
+
+// Marks every node tile the particle's P2G contributions or G2P reads touch.
+template <int D, int SF>
+__device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], unsigned hu, bool binned,
+                                           bool in_axes) {
+  using T = TileDims<D>;
+  constexpr int LO = Stencil<SF>::WLO, HI = Stencil<SF>::WLO + Stencil<SF>::WIN - 1;
+  const DevGrid &g = a.g;
+  if (SF == PMPM_SHAPE_QUADRATIC && !in_axes) return;  // takes no part in the step
+  int tlo[3] = {0, 0, 0}, thi[3] = {0, 0, 0};
+  bool empty = false, clipped = false;
+  const int tsz[3] = {T::X, T::Y, T::Z};
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    int lo = b[c] + LO, hi = b[c] + HI;
+    if (lo < 0) {
+      lo = 0;
+      clipped = true;
+    }
+    if (hi > g.n[c] - 1) {
+      hi = g.n[c] - 1;
+      clipped = true;
+    }
+    if (lo > hi) empty = true;
+    tlo[c] = lo / tsz[c];
+    thi[c] = hi / tsz[c];
+  }
+  if (!empty) {
+    for (int tz = tlo[2]; tz <= thi[2]; tz++)
+      for (int ty = tlo[1]; ty <= thi[1]; ty++)
+        for (int tx = tlo[0]; tx <= thi[0]; tx++) {
+          int t = tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
+          if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+        }
+  }
+  if (SF != PMPM_SHAPE_QUADRATIC && clipped && binned) {
+    // slots leaving the grid on an axis: the reference's flat index check lets
+    // them land on a node of a neighbouring row (src/solver/usl/usl_inline.h:114-126)
+    constexpr int NS = IPow<Stencil<SF>::WIN, D>::value;
+    for (int sid = 0; sid < NS; sid++) {
+      int w[3];
+      window_offset<D, SF>(sid, w);
+      int f = (int)hu + w[0] + w[1] * g.n[0] + w[2] * g.n[0] * g.n[1];
+      if ((unsigned)f >= (unsigned)g.ntotal) continue;
+      int c[3] = {f % g.n[0], (f / g.n[0]) % g.n[1], f / (g.n[0] * g.n[1])};
+      int t = tile_of<D>(g, c);
+      if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+    }
+  }
+}
+
+// apply_planardomain (src/boundaryconditions/planardomain_inline.h:56-138).
+template <int D>
+__device__ __forceinline__ void planar_force(const StepArgs &a, int s, const float x[3]) {
+  const DevParticles &P = a.P;
+  float f[3] = {0.0f, 0.0f, 0.0f};
+  float v[3];
+#pragma unroll
+  for (int c = 0; c < D; c++) v[c] = P.v[c * P.stride + s];
+  const float vol = P.V[s], mass = P.m[s];
+  const float radius = 0.5f * powf(vol, 1.0f / (float)D);
+  const float scale = (float)((double)mass / ((double)a.dt * (double)a.dt));
+  for (int k = 0; k < a.nbc; k++) {
+    const DevBC &bc = a.bc[k];
+    if (bc.type != PMPM_BC_PLANARDOMAIN) continue;
+    for (int face = 0; face < 2; face++) {
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        float overlap = face == 0 ? radius - (x[c] - a.g.origin[c]) : radius - (a.g.end[c] - x[c]);
+        if (!(overlap > 0.0f)) continue;
+        float nrm = face == 0 ? 1.0f : -1.0f;
+        float mu = bc.r[3 * face + c];
+        float ndotv = nrm * v[c];
+#pragma unroll
+        for (int e = 0; e < D; e++) {
+          float ne = (e == c) ? nrm : 0.0f;
+          float tang = v[e] - ndotv * ne;
+          f[e] += (scale * overlap) * (ne - mu * tang);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < D; c++) P.fext[c * P.stride + s] = f[c];
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.P.n) return;
+  const DevGrid &g = a.g;
+  float x[3] = {0.0f, 0.0f, 0.0f};
+  int b[3] = {0, 0, 0};
+  bool in_axes = true;
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    x[c] = a.P.x[c * a.P.stride + s];
+    b[c] = (int)scaled_coord(x[c], g.origin[c], g.inv_h);
+    in_axes = in_axes && b[c] >= 0 && b[c] < g.n[c];
+  }
+  const unsigned hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
+  a.P.hash[s] = hu;
+  const bool binned = hu < (unsigned)g.ntotal;
+  a.P.slot[s] = binned ? atomicAdd(&a.B.count[hu], 1) : -1;
+  if (!binned || (SF == PMPM_SHAPE_QUADRATIC && !in_axes)) atomicOr(a.fault, kFaultOutOfDomain);
+  mark_tiles<D, SF>(a, b, hu, binned, in_axes);
+  if (a.has_planar) planar_force<D>(a, s, x);
+}
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kScanChunk = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *smem_warp, int &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) smem_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int wv = lane < (blockDim.x >> 5) ? smem_warp[lane] : 0;
+    int wi = wv;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    smem_warp[lane] = wi - wv;
+    if (lane == 31) smem_warp[32] = wi;
+  }
+  __syncthreads();
+  total = smem_warp[32];
+  int r = smem_warp[warp] + incl - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int *count, int n, int *block_sums) {
+  __shared__ int sw[33];
+  const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; k++)
+    if (base + k < n) sum += count[base + k];
+  int total;
+  block_exclusive_scan(sum, sw, total);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+// Scans the block sums in place (single CTA) and resets the per-step counters.
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(int *block_sums, int nblocks, int *scalars) {
+  __shared__ int sw[33];
+  int carry = 0;
+  for (int base = 0; base < nblocks; base += kScanThreads) {
+    int i = base + threadIdx.x;
+    int v = i < nblocks ? block_sums[i] : 0;
+    int total;
+    int ex = block_exclusive_scan(v, sw, total);
+    if (i < nblocks) block_sums[i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) {
+    scalars[0] = carry;  // binned particles
+    scalars[1] = 0;      // unbinned counter
+    scalars[2] = 0;      // big-cell counter
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(int *count, int n, const int *block_sums,
+                                                               int *offset) {
+  __shared__ int sw[33];
+  const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
+  int v[kScanPer];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; k++) {
+    v[k] = base + k < n ? count[base + k] : 0;
+    sum += v[k];
+  }
+  int total;
+  int ex = block_exclusive_scan(sum, sw, total) + block_sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanPer; k++) {
+    if (base + k < n) {
+      offset[base + k] = ex;
+      count[base + k] = 0;
+    }
+    ex += v[k];
+  }
+  if (base <= n - 1 && n - 1 < base + kScanPer) offset[n] = ex;
+}
+
+__global__ void __launch_bounds__(256) k_scatter(StepArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.P.n) return;
+  const int slot = a.P.slot[s];
+  if (slot >= 0) {
+    a.B.order[a.B.offset[a.P.hash[s]] + slot] = s;
+  } else {
+    int k = atomicAdd(&a.B.scalars[1], 1);
+    a.B.order[a.B.scalars[0] + k] = s;
+  }
+}
+
+constexpr int kSmallCell = 32;
+constexpr int kBigCell = 2048;
+
+// Orders each cell's particles by id; cells above kSmallCell go to k_sort_big.
+__global__ void __launch_bounds__(256) k_sort_cells(StepArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.g.ntotal) return;
+  const int lo = a.B.offset[c], hi = a.B.offset[c + 1];
+  const int cnt = hi - lo;
+  if (cnt < 2) return;
+  if (cnt > kSmallCell) {
+    int k = atomicAdd(&a.B.scalars[2], 1);
+    a.B.big_cells[k] = c;
+    return;
+  }
+  int key[kSmallCell], val[kSmallCell];
+  for (int i = 0; i < cnt; i++) {
+    val[i] = a.B.order[lo + i];
+    key[i] = a.P.id[val[i]];
+  }
+  for (int i = 1; i < cnt; i++) {
+    int kk = key[i], vv = val[i];
+    int j = i - 1;
+    while (j >= 0 && key[j] > kk) {
+      key[j + 1] = key[j];
+      val[j + 1] = val[j];
+      j--;
+    }
+    key[j + 1] = kk;
+    val[j + 1] = vv;
+  }
+  for (int i = 0; i < cnt; i++) a.B.order[lo + i] = val[i];
+}
+
+// Bitonic sort in shared memory of each large cell (up to kBigCell entries).
+__global__ void __launch_bounds__(1024) k_sort_big(StepArgs a) {
+  __shared__ int key[kBigCell], val[kBigCell];
+  const int nbig = a.B.scalars[2];
+  for (int bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+    const int c = a.B.big_cells[bi];
+    const int lo = a.B.offset[c], cnt = a.B.offset[c + 1] - lo;
+    if (cnt > kBigCell) {
+      if (threadIdx.x == 0) atomicOr(a.fault, kFaultCellOverflow);
+      continue;
+    }
+    int p2 = 1;
+    while (p2 < cnt) p2 <<= 1;
+    for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+      if (i < cnt) {
+        val[i] = a.B.order[lo + i];
+        key[i] = a.P.id[val[i]];
+      } else {
+        key[i] = 0x7fffffff;
+        val[i] = -1;
+      }
+    }
+    __syncthreads();
+    for (int k = 2; k <= p2; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+          int ixj = i ^ j;
+          if (ixj > i) {
+            bool up = (i & k) == 0;
+            if ((key[i] > key[ixj]) == up) {
+              int tk = key[i];
+              key[i] = key[ixj];
+              key[ixj] = tk;
+              int tv = val[i];
+              val[i] = val[ixj];
+              val[ixj] = tv;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) a.B.order[lo + i] = val[i];
+    __syncthreads();
+  }
+}
+
+// --------------------------------------------------------------------------
+// physical re-sort of particle storage into cell order
+// --------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ void move_comps(const T *src, T *dst, int ncomp, int stride, int from, int to) {
+  if (!src) return;
+  for (int c = 0; c < ncomp; c++) dst[c * stride + to] = src[c * stride + from];
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_reorder(StepArgs a, DevParticles dst, int move_L, int move_fext) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.P.n) return;
+  const DevParticles &S = a.P;
+  const int s = a.B.order[k];
+  const int st = S.stride;
+  move_comps(S.x, dst.x, D, st, s, k);
+  move_comps(S.v, dst.v, D, st, s, k);
+  move_comps(S.F, dst.F, D * D, st, s, k);
+  move_comps(S.sig, dst.sig, Sym<D>::S, st, s, k);
+  if (move_L) move_comps(S.L, dst.L, D * D, st, s, k);
+  move_comps(S.m, dst.m, 1, st, s, k);
+  move_comps(S.V, dst.V, 1, st, s, k);
+  move_comps(S.V0, dst.V0, 1, st, s, k);
+  if (move_fext) move_comps(S.fext, dst.fext, D, st, s, k);
+  move_comps(S.eps, dst.eps, Sym<D>::E, st, s, k);
+  move_comps(S.sref, dst.sref, Sym<D>::S, st, s, k);
+  move_comps(S.color, dst.color, 1, st, s, k);
+  move_comps(S.active, dst.active, 1, st, s, k);
+  move_comps(S.rigid, dst.rigid, 1, st, s, k);
+  move_comps(S.id, dst.id, 1, st, s, k);
+  move_comps(S.hash, dst.hash, 1, st, s, k);
+  a.B.order[k] = k;  // storage is now in cell order
+}
+
+__global__ void __launch_bounds__(256) k_identity_order(int *order, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) order[k] = k;
+}
+
+// --------------------------------------------------------------------------
+// P2G: node-tile gather with fused node epilogue
+// --------------------------------------------------------------------------
+
+// Adds the contributions of the particles at sorted positions [k0, k1) for
+// window slot w to node nc (usl_p2g_kernel, src/solver/usl/usl_inline.h:
+// 136-161): m += psi m_p; p += (psi m_p) v_p; f += psi f_ext - V_p sigma_p dpsi.
+template <int D, int SF>
+__device__ __forceinline__ void p2g_range(const StepArgs &a, int k0, int k1, const int w[3], const int nc[3],
+                                          float &mass, float mom[3], float force[3]) {
+  const DevParticles &P = a.P;
+  const DevGrid &g = a.g;
+  const int st = P.stride;
+  for (int k = k0; k < k1; k++) {
+    const int s = a.B.order[k];
+    float u[3];
+    int b[3];
+    bool inside = true;
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+      b[c] = (int)u[c];
+      inside = inside && b[c] >= 0 && b[c] < g.n[c];
+    }
+    if (SF == PMPM_SHAPE_QUADRATIC && !inside) continue;
+    float N[3], dN[3];
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      const float rel = u[c] - (float)(b[c] + w[c]);
+      const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(nc[c], g.n[c]) : 0;
+      axis_weight<SF>(rel, g.inv_h, type, N[c], dN[c]);
+    }
+    float psi, dpsi[3];
+    if (D == 2) {
+      psi = N[0] * N[1];
+      dpsi[0] = dN[0] * N[1];
+      dpsi[1] = dN[1] * N[0];
+      dpsi[2] = 0.0f;
+    } else {
+      psi = N[0] * N[1] * N[2];
+      dpsi[0] = dN[0] * N[1] * N[2];
+      dpsi[1] = dN[1] * N[0] * N[2];
+      dpsi[2] = dN[2] * N[0] * N[1];
+    }
+    const float sm = psi * P.m[s];
+    mass += sm;
+#pragma unroll
+    for (int c = 0; c < D; c++) mom[c] += sm * P.v[c * st + s];
+    if (a.has_planar) {
+#pragma unroll
+      for (int c = 0; c < D; c++) force[c] += psi * P.fext[c * st + s];
+    }
+    const float mv = -P.V[s];
+    float S[9];
+    load_sig3<D>(P, s, S);
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      float acc = (mv * S[3 * c + 0]) * dpsi[0];
+      acc += (mv * S[3 * c + 1]) * dpsi[1];
+      if (D == 3) acc += (mv * S[3 * c + 2]) * dpsi[2];
+      force[c] += acc;
+    }
+  }
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int apply_bcs, int *node_epoch) {
+  using T = TileDims<D>;
+  const DevGrid &g = a.g;
+  const int tile = blockIdx.x;
+  if (a.N.tile_epoch[tile] != a.epoch) return;
+  if (threadIdx.x == 0) node_epoch[tile] = a.epoch;
+  const int tx = tile % g.tdim[0], ty = (tile / g.tdim[0]) % g.tdim[1], tz = tile / (g.tdim[0] * g.tdim[1]);
+  const int lx = threadIdx.x % T::X, ly = (threadIdx.x / T::X) % T::Y, lz = threadIdx.x / (T::X * T::Y);
+  const int nc[3] = {tx * T::X + lx, ty * T::Y + ly, D == 3 ? tz * T::Z + lz : 0};
+  if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) return;
+  const int node = flat_index(g, nc[0], nc[1], nc[2]);
+  float mass = 0.0f, mom[3] = {0.0f, 0.0f, 0.0f}, force[3] = {0.0f, 0.0f, 0.0f};
+  constexpr int NS = IPow<Stencil<SF>::WIN, D>::value;
+  const int *off = a.B.offset;
+  for (int sid = 0; sid < NS; sid++) {
+    int w[3];
+    window_offset<D, SF>(sid, w);
+    if (SF == PMPM_SHAPE_QUADRATIC) {
+      // cells whose slot w folds onto this node (axis-wise clamp preimage)
+      int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+      bool empty = false;
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        int l = nc[c] == 0 ? 0 : nc[c] - w[c];
+        int h = nc[c] == g.n[c] - 1 ? g.n[c] - 1 : nc[c] - w[c];
+        l = max(l, 0);
+        h = min(h, g.n[c] - 1);
+        if (l > h) empty = true;
+        lo[c] = l;
+        hi[c] = h;
+      }
+      if (empty) continue;
+      for (int cz = lo[2]; cz <= hi[2]; cz++)
+        for (int cy = lo[1]; cy <= hi[1]; cy++) {
+          const int c0 = flat_index(g, lo[0], cy, cz), c1 = flat_index(g, hi[0], cy, cz);
+          p2g_range<D, SF>(a, off[c0], off[c1 + 1], w, nc, mass, mom, force);
+        }
+    } else {
+      const int cell = node - (w[0] + w[1] * g.n[0] + w[2] * g.n[0] * g.n[1]);
+      if ((unsigned)cell >= (unsigned)g.ntotal) continue;
+      p2g_range<D, SF>(a, off[cell], off[cell + 1], w, nc, mass, mom, force);
+    }
+  }
+  // epilogue: the reference leaves nodes with m <= cutoff at their reset value (0)
+  float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+  const bool live = mass > a.cutoff;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      p[c] = mom[c];
+      pnt[c] = mom[c] + force[c] * a.dt;
+    }
+  } else {
+    mass = 0.0f;
+  }
+  if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
+  const int nt = g.ntotal;
+  a.N.m[node] = mass;
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    a.N.p[c * nt + node] = p[c];
+    a.N.pnt[c * nt + node] = pnt[c];
+    a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
+    a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
+  }
+}
+
+// --------------------------------------------------------------------------
+// G2P + deformation update + stress update
+// --------------------------------------------------------------------------
+
+template <int D>
+__device__ __forceinline__ float det_rows(const float *A) {
+  if (D == 2) return A[0] * A[3] - A[2] * A[1];
+  const float c0 = A[4] * A[8] - A[5] * A[7];
+  const float c1 = A[3] * A[8] - A[5] * A[6];
+  const float c2 = A[3] * A[7] - A[4] * A[6];
+  return (A[0] * c0 - A[1] * c1) + A[2] * c2;
+}
+
+// Material update of storage slot s from velocity gradient L
+// (Solver::stress_update, src/solver/solver.cpp:110-121; materials by colour).
+template <int D>
+__device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, const float *L) {
+  const DevParticles &P = a.P;
+  const int color = P.color[s];
+  if (color >= a.nmat) return;
+  const DevMaterial &mt = a.mat[color];
+  if (mt.type == PMPM_MAT_NONE) return;
+  if ((mt.type == PMPM_MAT_LINEAR_ELASTIC || mt.type == PMPM_MAT_NEWTON_FLUID) && !P.active[s]) return;
+  const int st = P.stride;
+  float S[9];
+  if (mt.type == PMPM_MAT_LINEAR_ELASTIC) {
+    load_sig3<D>(P, s, S);
+    le_update<D>(mt, L, a.dt, S);
+  } else if (mt.type == PMPM_MAT_NEWTON_FLUID) {
+    nf_update<D>(mt, L, P.m[s], P.V[s], P.V0[s], S);
+  } else {
+    float eps[9], sref[9];
+#pragma unroll
+    for (int x = 0; x < D; x++)
+#pragma unroll
+      for (int y = 0; y < D; y++) eps[x * D + y] = P.eps[eps_index<D>(x, y) * st + s];
+    if (a.has_sref) {
+      // the reference stress uses the stress's symmetric layout
+#pragma unroll
+      for (int x = 0; x < 3; x++)
+#pragma unroll
+        for (int y = 0; y < 3; y++) {
+          int k = sig_index<D>(x, y);
+          sref[3 * x + y] = k < 0 ? 0.0f : P.sref[k * st + s];
+        }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; k++) sref[k] = 0.0f;
+    }
+    dp_update<D>(mt.p, L, a.dt, eps, sref, S, false);
+#pragma unroll
+    for (int x = 0; x < D; x++)
+#pragma unroll
+      for (int y = x; y < D; y++) P.eps[eps_index<D>(x, y) * st + s] = eps[x * D + y];
+  }
+  store_sig3<D>(P, s, S);
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int store_L) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.P.n) return;
+  const DevParticles &P = a.P;
+  const DevGrid &g = a.g;
+  const int st = P.stride, nt = g.ntotal;
+  constexpr int K = Stencil<SF>::K;
+  float x[3] = {0, 0, 0}, v[3] = {0, 0, 0}, u[3] = {0, 0, 0};
+  int b[3] = {0, 0, 0};
+  bool inside = true;
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    x[c] = P.x[c * st + s];
+    v[c] = P.v[c * st + s];
+    u[c] = scaled_coord(x[c], g.origin[c], g.inv_h);
+    b[c] = (int)u[c];
+    inside = inside && b[c] >= 0 && b[c] < g.n[c];
+  }
+  float L[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) L[k] = 0.0f;
+  if (SF != PMPM_SHAPE_QUADRATIC || inside) {
+    // per-axis weights, node indices and validity
+    float N[3][K], dN[3][K];
+    int idx[3][K];
+    bool ok[3][K];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        N[c][k] = 1.0f;
+        dN[c][k] = 0.0f;
+        idx[c][k] = 0;
+        ok[c][k] = true;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      int w0 = Stencil<SF>::WLO;
+      if (SF == PMPM_SHAPE_QUADRATIC) w0 = (u[c] - (float)(b[c] - 1)) < 1.5f ? -1 : 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const int sel = b[c] + w0 + k;
+        const float rel = u[c] - (float)sel;
+        const bool in = sel >= 0 && sel < g.n[c];
+        const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(sel, g.n[c]) : 0;
+        axis_weight<SF>(rel, g.inv_h, in ? type : 0, N[c][k], dN[c][k]);
+        if (SF == PMPM_SHAPE_QUADRATIC) {
+          idx[c][k] = min(max(sel, 0), g.n[c] - 1);
+          ok[c][k] = true;
+        } else {
+          idx[c][k] = sel;
+          ok[c][k] = in;
+        }
+      }
+    }
+    float vinc[3] = {0, 0, 0}, dvinc[3] = {0, 0, 0};
+    constexpr int KZ = D == 3 ? K : 1;
+#pragma unroll
+    for (int ky = 0; ky < K; ky++) {
+#pragma unroll
+      for (int kx = 0; kx < K; kx++) {
+#pragma unroll
+        for (int kz = 0; kz < KZ; kz++) {
+          if (!ok[0][kx] || !ok[1][ky] || (D == 3 && !ok[2][kz])) continue;
+          const int node = idx[0][kx] + idx[1][ky] * g.n[0] + (D == 3 ? idx[2][kz] * g.n[0] * g.n[1] : 0);
+          float psi, dpsi[3];
+          if (D == 2) {
+            psi = N[0][kx] * N[1][ky];
+            dpsi[0] = dN[0][kx] * N[1][ky];
+            dpsi[1] = dN[1][ky] * N[0][kx];
+          } else {
+            psi = N[0][kx] * N[1][ky] * N[2][kz];
+            dpsi[0] = dN[0][kx] * N[1][ky] * N[2][kz];
+            dpsi[1] = dN[1][ky] * N[0][kx] * N[2][kz];
+            dpsi[2] = dN[2][kz] * N[0][kx] * N[1][ky];
+          }
+          float vn[3], vnt[3];
+#pragma unroll
+          for (int c = 0; c < D; c++) {
+            vn[c] = a.N.v[c * nt + node];
+            vnt[c] = a.N.vnt[c * nt + node];
+          }
+#pragma unroll
+          for (int c = 0; c < D; c++) {
+            dvinc[c] += psi * (vnt[c] - vn[c]);
+            vinc[c] += psi * vnt[c];
+          }
+#pragma unroll
+          for (int r = 0; r < D; r++)
+#pragma unroll
+            for (int c = 0; c < D; c++) L[r * D + c] += dpsi[r] * vnt[c];
+        }
+      }
+    }
+    // v <- (1 - alpha) v_pic + alpha (v + dv); x += dt v_pic; F <- (I + L dt) F; V = det(F) V0
+    float F[9], A[9], Fn[9];
+#pragma unroll
+    for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
+#pragma unroll
+    for (int r = 0; r < D; r++)
+#pragma unroll
+      for (int c = 0; c < D; c++) A[r * D + c] = (r == c ? 1.0f : 0.0f) + L[r * D + c] * a.dt;
+#pragma unroll
+    for (int r = 0; r < D; r++)
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        float acc = A[r * D + 0] * F[0 * D + c];
+#pragma unroll
+        for (int k = 1; k < D; k++) acc += A[r * D + k] * F[k * D + c];
+        Fn[r * D + c] = acc;
+      }
+    bool finite = true;
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      const float vnew = a.one_minus_alpha * vinc[c] + a.alpha * (v[c] + dvinc[c]);
+      const float xnew = x[c] + a.dt * vinc[c];
+      P.v[c * st + s] = vnew;
+      P.x[c * st + s] = xnew;
+      finite = finite && isfinite(xnew);
+    }
+#pragma unroll
+    for (int k = 0; k < D * D; k++) P.F[k * st + s] = Fn[k];
+    P.V[s] = det_rows<D>(Fn) * P.V0[s];
+    if (!finite) atomicOr(a.fault, kFaultNonFinite);
+  }
+  if (store_L) {
+#pragma unroll
+    for (int k = 0; k < D * D; k++) P.L[k * st + s] = L[k];
+  }
+  if (do_stress) stress_update_point<D>(a, s, L);
+}
+
+// Stress update alone from the stored velocity gradient.
+template <int D>
+__global__ void __launch_bounds__(256) k_stress_update(StepArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.P.n) return;
+  float L[9];
+#pragma unroll
+  for (int k = 0; k < D * D; k++) L[k] = a.P.L[k * a.P.stride + s];
+  stress_update_point<D>(a, s, L);
+}
+
+// --------------------------------------------------------------------------
+// shape-function dump (reference psi / dpsi layout, for inspection)
+// --------------------------------------------------------------------------
+
+template <int D, int SF>
+__global__ void __launch_bounds__(256) k_shape_dump(StepArgs a, float *psi, float *dpsi) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.P.n) return;
+  const DevParticles &P = a.P;
+  const DevGrid &g = a.g;
+  constexpr int NS = IPow<Stencil<SF>::WIN, D>::value;
+  const int i = P.id[s];
+  float u[3];
+  int b[3] = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    u[c] = scaled_coord(P.x[c * P.stride + s], g.origin[c], g.inv_h);
+    b[c] = (int)u[c];
+  }
+  for (int sid = 0; sid < NS; sid++) {
+    int w[3];
+    window_offset<D, SF>(sid, w);
+    int t[3] = {b[0] + w[0], b[1] + w[1], D == 3 ? b[2] + w[2] : 0};
+    if (SF == PMPM_SHAPE_QUADRATIC)
+      for (int c = 0; c < D; c++) t[c] = min(max(t[c], 0), g.n[c] - 1);
+    const int f = t[0] + t[1] * g.n[0] + t[2] * g.n[0] * g.n[1];
+    float ps = 0.0f, dp[3] = {0.0f, 0.0f, 0.0f};
+    if ((unsigned)f < (unsigned)g.ntotal) {
+      const int nc[3] = {f % g.n[0], (f / g.n[0]) % g.n[1], f / (g.n[0] * g.n[1])};
+      float N[3], dN[3];
+      for (int c = 0; c < D; c++) {
+        const float rel = u[c] - (float)(b[c] + w[c]);
+        const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(nc[c], g.n[c]) : 0;
+        axis_weight<SF>(rel, g.inv_h, type, N[c], dN[c]);
+      }
+      if (D == 2) {
+        ps = N[0] * N[1];
+        dp[0] = dN[0] * N[1];
+        dp[1] = dN[1] * N[0];
+      } else {
+        ps = N[0] * N[1] * N[2];
+        dp[0] = dN[0] * N[1] * N[2];
+        dp[1] = dN[1] * N[0] * N[2];
+        dp[2] = dN[2] * N[0] * N[1];
+      }
+    }
+    psi[(size_t)i * NS + sid] = ps;
+    for (int c = 0; c < D; c++) dpsi[((size_t)i * NS + sid) * D + c] = dp[c];
+  }
+}
+
+// --------------------------------------------------------------------------
+// single-point material update (standalone material binding)
+// --------------------------------------------------------------------------
+
+template <int D>
+__global__ void __launch_bounds__(256) k_point_update(DevMaterial mt, int n, float dt, const float *L, float *S,
+                                                      float *eps, const float *sref, const float *m, const float *V,
+                                                      const float *V0, int velgrad_is_increment) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float Li[9], Si[9];
+#pragma unroll
+  for (int k = 0; k < D * D; k++) Li[k] = L[(size_t)i * D * D + k];
+#pragma unroll
+  for (int k = 0; k < 9; k++) Si[k] = S[(size_t)i * 9 + k];
+  if (mt.type == PMPM_MAT_LINEAR_ELASTIC) {
+    le_update<D>(mt, Li, dt, Si);
+  } else if (mt.type == PMPM_MAT_NEWTON_FLUID) {
+    nf_update<D>(mt, Li, m[i], V[i], V0[i], Si);
+  } else if (mt.type == PMPM_MAT_DRUCKER_PRAGER) {
+    float e[9], r[9];
+#pragma unroll
+    for (int k = 0; k < D * D; k++) e[k] = eps[(size_t)i * D * D + k];
+#pragma unroll
+    for (int k = 0; k < 9; k++) r[k] = sref[(size_t)i * 9 + k];
+    dp_update<D>(mt.p, Li, dt, e, r, Si, velgrad_is_increment != 0);
+#pragma unroll
+    for (int k = 0; k < D * D; k++) eps[(size_t)i * D * D + k] = e[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 9; k++) S[(size_t)i * 9 + k] = Si[k];
+}
+
+}  // namespace pmpm

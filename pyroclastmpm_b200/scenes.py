@@ -1,0 +1,83 @@
+"""Synthetic particle sets of the benchmark configurations (seeded, no data files).
+
+Each builder returns a dict with the grid, the particles and the solver
+settings, in the form both the C ABI ``Simulation`` and the oracle take.
+Sizes follow the configuration descriptions; ``scale`` shrinks the particle
+region (same cell size, same particle spacing) for quick parity runs.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _lattice(lo, hi, spacing):
+    """Points at (i + 1/2) * spacing inside [lo, hi) per axis (x fastest)."""
+    axes = []
+    for a in range(len(lo)):
+        n = int(np.floor((hi[a] - lo[a]) / spacing + 1e-9))
+        axes.append(lo[a] + (np.arange(n) + 0.5) * spacing)
+    mesh = np.meshgrid(*axes[::-1], indexing="ij")
+    pts = np.stack([m.ravel() for m in mesh[::-1]], axis=1)
+    return pts
+
+
+def two_discs(cell_size=0.02, radius=0.2, centers=((0.25, 0.25), (0.75, 0.75)), ppc_1d=2, speed=0.1,
+              E=1000.0, pois=0.3, density=1000.0, dt=1e-3, alpha=0.99):
+    """Two elastic discs moving toward each other on [0,1]^2 (linear shape
+    functions): 2x2 particles per cell on the sub-cell lattice."""
+    spacing = cell_size / ppc_1d
+    pos, vel = [], []
+    for k, c in enumerate(centers):
+        c = np.asarray(c, np.float64)
+        lo = np.floor((c - radius) / spacing) * spacing
+        hi = np.ceil((c + radius) / spacing) * spacing
+        pts = _lattice(lo, hi, spacing)
+        inside = ((pts - c) ** 2).sum(axis=1) < radius ** 2
+        pts = pts[inside]
+        pos.append(pts)
+        vel.append(np.full_like(pts, speed if k == 0 else -speed))
+    return dict(dim=2, origin=[0.0, 0.0], end=[1.0, 1.0], cell_size=cell_size, shape_function="linear",
+                dt=dt, particles_per_cell=ppc_1d ** 2, alpha=alpha,
+                materials=[{"type": "LinearElastic", "density": density, "E": E, "pois": pois}], bcs=[],
+                positions=np.concatenate(pos), velocities=np.concatenate(vel))
+
+
+def granular_column(domain=(1.0, 0.25, 0.5), cell_size=1.0 / 256, column=(0.2, 0.25, 0.2), ppc_1d=2,
+                    jitter=0.25, seed=0, shape_function="quadratic", dt=1e-5, scale=1.0,
+                    density=1500.0, E=1.0e7, pois=0.3, friction_angle=30.0, dilatancy_angle=0.0, cohesion=0.0):
+    """3D granular column against the x = 0 wall, Drucker-Prager, gravity,
+    slip walls on all faces.  Particles on a (ppc_1d)^3 lattice per cell,
+    each coordinate jittered uniformly by +-jitter * spacing (numpy PCG64)."""
+    spacing = cell_size / ppc_1d
+    col = np.asarray(column, np.float64) * scale
+    pts = _lattice(np.zeros(3), col, spacing)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = pts + rng.uniform(-jitter * spacing, jitter * spacing, size=pts.shape)
+    return dict(dim=3, origin=[0.0, 0.0, 0.0], end=list(domain), cell_size=cell_size,
+                shape_function=shape_function, dt=dt, particles_per_cell=ppc_1d ** 3, alpha=0.99,
+                materials=[{"type": "DruckerPrager", "density": density, "E": E, "pois": pois,
+                            "friction_angle": friction_angle, "dilatancy_angle": dilatancy_angle,
+                            "cohesion": cohesion}],
+                bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]},
+                     {"type": "NodeDomain", "face0_mode": [1, 1, 1], "face1_mode": [1, 1, 1]}],
+                positions=pts, velocities=np.zeros_like(pts))
+
+
+def granular_bed(domain=(1.5, 0.6, 0.8), cell_size=1.0 / 160, bed=(1.0, 0.5, 0.3), ppc_1d=2, jitter=0.25,
+                 seed=1, shape_function="cubic", dt=8e-6, scale=1.0, **kw):
+    """3D granular bed (the scoop configuration's particle set)."""
+    spacing = cell_size / ppc_1d
+    b = np.asarray(bed, np.float64) * scale
+    pts = _lattice(np.zeros(3), b, spacing)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = pts + rng.uniform(-jitter * spacing, jitter * spacing, size=pts.shape)
+    d = granular_column(domain=domain, cell_size=cell_size, shape_function=shape_function, dt=dt, **kw)
+    d.update(positions=pts, velocities=np.zeros_like(pts))
+    return d
+
+
+def sim_kwargs(scene):
+    """Keyword arguments of Simulation / OracleSim from a scene dict."""
+    keys = ["dim", "origin", "end", "cell_size", "shape_function", "dt", "particles_per_cell", "alpha",
+            "materials", "bcs"]
+    return {k: scene[k] for k in keys}

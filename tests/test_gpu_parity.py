@@ -1,0 +1,324 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle.
+
+Tolerances: binning is bit-exact; one FP32 step must agree with the FP32
+oracle within 1e-5 relative (max |a - b| / max |b| per field); multi-step drift
+against the FP64 oracle is reported with the bound stated per test.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from pyroclastmpm_b200 import Simulation, scenes
+
+pytestmark = pytest.mark.gpu
+
+G = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_unit_vectors.json")))
+STEP_TOL = 1e-5
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def make_pair(scene, precision="f32", **extra):
+    kw = scenes.sim_kwargs(scene)
+    sim = Simulation(**kw, **extra)
+    sim.set_particles(scene["positions"], scene["velocities"], scene.get("colors"))
+    ref = oracle.OracleSim(**kw, positions=scene["positions"], velocities=scene["velocities"],
+                           colors=scene.get("colors"), precision=precision)
+    return sim, ref
+
+
+def random_scene(dim, n, shape_function, seed, margin=0.0, lo=0.0, hi=1.0, cell=0.1, mats=None, bcs=None):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(lo + margin, hi - margin, size=(n, dim))
+    v = rng.normal(0.0, 0.1, size=(n, dim))
+    return dict(dim=dim, origin=[0.0] * dim, end=[1.0] * dim, cell_size=cell, shape_function=shape_function,
+                dt=1e-3, particles_per_cell=4 if dim == 2 else 8, alpha=0.99,
+                materials=mats or [{"type": "LinearElastic", "density": 1000.0, "E": 1e4, "pois": 0.3}],
+                bcs=bcs or [], positions=x, velocities=v)
+
+
+# ----------------------------------------------------------------------------
+# known-answer vectors of the reference's unit tests, through the GPU path
+# ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reference_vectors_spatialpartition(dim):
+    v = G["spatialpartition"]
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, v["cell_size"])
+    sim.set_particles(np.array(v["positions"][str(dim)]))
+    sim.partition()
+    assert sim.num_cells == v["num_cells"][str(dim)]
+    assert sim.get("bins").tolist() == v["bins"][str(dim)]
+    assert sim.get("hash_unsorted").tolist() == v["hash_unsorted"]
+    assert sim.get("hash_sorted").tolist() == v["hash_sorted"]
+    assert sim.get("sorted_index").tolist() == v["sorted_index"]
+    cs, ce = sim.get("cell_start"), sim.get("cell_end")
+    for c in range(sim.num_nodes):
+        assert [cs[c], ce[c]] == v["cell_ranges"].get(str(c), [0, 0])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("sf", ["linear", "cubic"])
+def test_reference_vectors_shapefunctions(dim, sf):
+    v = G["shapefunctions"]
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, v["cell_size"], shape_function=sf)
+    sim.set_particles(np.array([v["position"][str(dim)]]))
+    sim.partition()
+    psi, dpsi = sim.shape_functions()
+    exp = v[sf][str(dim)]
+    np.testing.assert_allclose(psi[0, : len(exp["psi"])], exp["psi"], atol=v["tol"])
+    np.testing.assert_allclose(dpsi[0, : len(exp["dpsi"])], exp["dpsi"], atol=v["tol"])
+    assert abs(psi.sum() - 1.0) < v["tol"]
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reference_vectors_usl_stepwise(dim):
+    v = G["usl_stepwise"]
+    k = str(dim)
+    pos = np.array(v["positions"][k])
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, 1.0, shape_function="linear", dt=v["dt"],
+                     particles_per_cell=1)
+    sim.set_particles(pos, np.ones_like(pos))
+    sim.initialize()
+    stresses = np.zeros((2, 3, 3))
+    stresses[0] = 1.0
+    sim.set("masses", v["masses"])
+    sim.set("volumes", v["volumes"])
+    sim.set("volumes_original", v["volumes"])
+    sim.set("stresses", stresses)
+    sim.partition()
+    sim.p2g()
+    tol = v["tol"]
+    np.testing.assert_allclose(sim.get("node_masses")[:2], v["node_masses"][k], atol=tol)
+    np.testing.assert_allclose(sim.get("node_moments")[:2], v["node_moments"][k], atol=tol)
+    sim.g2p()
+    np.testing.assert_allclose(sim.get("volumes")[0], v["particle0_volume"][k], atol=tol)
+    np.testing.assert_allclose(sim.get("positions")[0], v["particle0_position"][k], atol=tol)
+    np.testing.assert_allclose(sim.get("velocities")[0], v["particle0_velocity"][k], atol=tol)
+    np.testing.assert_allclose(np.diag(sim.get("F")[0]), v["particle0_F_diag"][k], atol=tol)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reference_vectors_particles(dim):
+    v = G["particles"]
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, v["cell_size"], particles_per_cell=v["ppc"],
+                     materials=[{"type": "Material", "density": v["density"]}])
+    sim.set_particles(np.array(v["positions"][str(dim)]))
+    sim.initialize()
+    np.testing.assert_allclose(sim.get("volumes"), v["volume"][str(dim)], atol=v["tol"])
+    np.testing.assert_allclose(sim.get("masses"), v["mass"][str(dim)], atol=v["tol"])
+
+
+# ----------------------------------------------------------------------------
+# binning: bit-exact against the oracle (reference semantics)
+# ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("seed", [0, 1])
+def test_binning_bit_exact(dim, seed):
+    rng = np.random.default_rng(seed)
+    n = 20000 if dim == 3 else 5000
+    x = rng.uniform(0.0, 1.0, size=(n, dim))
+    # edge cases: exact node lines, the far boundary, slightly outside (aliasing
+    # rows and hashes past the grid), duplicates, dense clusters
+    x[:50] = np.round(x[:50] * 10) / 10
+    x[50:60] = 1.0
+    x[60:70, 0] = 1.05
+    x[70:80, 0] = -0.05
+    x[80:90] = 5.0
+    x[90:200] = x[90]
+    x[200:1000] = rng.uniform(0.3, 0.31, size=(800, dim))
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, 0.05)
+    sim.set_particles(x)
+    sim.partition()
+    ref = oracle.OracleSim(dim, [0.0] * dim, [1.0] * dim, 0.05, x)
+    ref.call("or_partition")
+    for name in ("bins", "hash_unsorted", "hash_sorted", "sorted_index", "cell_start", "cell_end"):
+        np.testing.assert_array_equal(sim.get(name), ref[name], err_msg=name)
+    assert sim.synchronize() == 16  # particles past the grid are reported
+
+
+def test_binning_big_cells_and_resort():
+    """More than 32 particles in a cell (bitonic path), and physical re-sorts
+    keep the reference permutation."""
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.uniform(0.5, 0.52, size=(1500, 2)), rng.uniform(0, 1, size=(3000, 2))])
+    sc = random_scene(2, 10, "linear", 0)
+    sc["positions"], sc["velocities"] = x, np.zeros_like(x)
+    sim, ref = make_pair(sc, resort_interval=1)
+    sim.initialize()
+    ref.initialize()
+    for name in ("hash_sorted", "sorted_index", "cell_start", "cell_end"):
+        np.testing.assert_array_equal(sim.get(name), ref[name], err_msg=name)
+    sim.solve(2)
+    ref.solve(2)
+    np.testing.assert_array_equal(sim.get("sorted_index"), ref["sorted_index"])
+    assert rel(sim.get("positions"), ref["positions"]) < STEP_TOL
+
+
+# ----------------------------------------------------------------------------
+# shape functions against the oracle
+# ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("sf", ["linear", "quadratic", "cubic"])
+def test_shape_functions_match_oracle(dim, sf):
+    rng = np.random.default_rng(7)
+    x = rng.uniform(0.0, 1.0, size=(2000, dim))
+    x[:10] = 0.0
+    x[10:20] = 1.0
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, 0.1, shape_function=sf)
+    sim.set_particles(x)
+    sim.partition()
+    psi, dpsi = sim.shape_functions()
+    ref = oracle.OracleSim(dim, [0.0] * dim, [1.0] * dim, 0.1, x, shape_function=sf)
+    ref.call("or_partition")
+    ref.call("or_shape_functions")
+    np.testing.assert_allclose(psi.ravel(), ref["psi"], atol=2e-6)
+    np.testing.assert_allclose(dpsi.ravel(), ref["dpsi"], atol=2e-5 * 10)
+    inside = np.all((x > 0.0) & (x < 0.9), axis=1)
+    np.testing.assert_allclose(psi[inside].sum(axis=1), 1.0, atol=1e-5)   # partition of unity
+    np.testing.assert_allclose(dpsi[inside].sum(axis=1), 0.0, atol=1e-3)  # sum of gradients
+
+
+# ----------------------------------------------------------------------------
+# one step and several steps against the oracle
+# ----------------------------------------------------------------------------
+
+STEP_CASES = {
+    "discs_2d_linear_le": lambda: scenes.two_discs(),
+    "random_2d_cubic_le": lambda: random_scene(2, 3000, "cubic", 1, margin=0.05),
+    "random_2d_quadratic_nf": lambda: random_scene(
+        2, 3000, "quadratic", 2, margin=0.0,
+        mats=[{"type": "NewtonFluid", "density": 1000.0, "viscosity": 1e-3, "bulk_modulus": 2e6, "gamma": 7.0}],
+        bcs=[{"type": "Gravity", "gravity": [0.0, -9.81]},
+             {"type": "NodeDomain", "face0_mode": [1, 1], "face1_mode": [1, 1]}]),
+    "random_2d_linear_dp_mixed": lambda: dict(
+        random_scene(2, 3000, "linear", 3, margin=0.02,
+                     mats=[{"type": "DruckerPrager", "density": 1500.0, "E": 1e6, "pois": 0.3, "friction_angle": 30.0,
+                            "cohesion": 10.0},
+                           {"type": "LinearElastic", "density": 1000.0, "E": 1e5, "pois": 0.2}],
+                     bcs=[{"type": "NodeDomain", "face0_mode": [0, 1], "face1_mode": [1, 0]}]),
+        colors=np.random.default_rng(3).integers(0, 2, 3000)),
+    "column_3d_quadratic_dp": lambda: scenes.granular_column(cell_size=1.0 / 64),
+    "random_3d_cubic_le_gravity": lambda: random_scene(
+        3, 4000, "cubic", 4, margin=0.05, cell=0.1,
+        bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]},
+             {"type": "NodeDomain", "face0_mode": [1, 1, 1], "face1_mode": [1, 1, 1]}]),
+    "random_3d_linear_nf_planar": lambda: random_scene(
+        3, 4000, "linear", 5, margin=0.0, cell=0.1,
+        mats=[{"type": "NewtonFluid", "density": 1000.0, "viscosity": 1e-2, "bulk_modulus": 1e4, "gamma": 7.0}],
+        bcs=[{"type": "PlanarDomain", "face0_friction": [10.0, 0.0, 5.0], "face1_friction": [0.0, 20.0, 0.0]}]),
+}
+
+FIELDS = ("positions", "velocities", "stresses", "F", "volumes")
+
+
+@pytest.mark.parametrize("case", sorted(STEP_CASES))
+def test_one_step_matches_oracle(case):
+    scene = STEP_CASES[case]()
+    sim, ref = make_pair(scene, flags=1)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(1)
+    ref.solve(1)
+    for name in FIELDS + ("velocity_gradient",):
+        err = rel(sim.get(name), ref[name])
+        assert err <= STEP_TOL, f"{case} {name}: {err:.3e}"
+    for name in ("node_masses", "node_moments", "node_moments_nt"):
+        err = rel(sim.get(name), ref[name])
+        assert err <= STEP_TOL, f"{case} {name}: {err:.3e}"
+
+
+@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "random_2d_quadratic_nf"])
+def test_multi_step_drift_vs_fp64(case):
+    """20 steps: FP32 GPU against the FP64 oracle (drift bound 1e-4)."""
+    scene = STEP_CASES[case]()
+    sim, ref = make_pair(scene, precision="f64")
+    sim.initialize()
+    ref.initialize()
+    sim.solve(20)
+    ref.solve(20)
+    assert sim.synchronize() == 0
+    for name in ("positions", "velocities", "stresses"):
+        err = rel(sim.get(name), ref[name])
+        assert err <= 1e-4, f"{case} {name}: {err:.3e}"
+
+
+def test_deterministic_bitwise():
+    scene = scenes.granular_column(cell_size=1.0 / 64)
+    outs = []
+    for _ in range(2):
+        sim, _ref = make_pair(scene, resort_interval=4)
+        sim.initialize()
+        sim.solve(10)
+        outs.append([sim.get(n) for n in FIELDS])
+        sim.close()
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_drucker_prager_points_match_reference_dp_rheo():
+    """Per-point cone / apex return (reference DP_rheo parameters) on random
+    strain histories, against the oracle's restatement of update_dp_rheo."""
+    from pyroclastmpm_b200 import material_point_update
+
+    rng = np.random.default_rng(11)
+    for dim in (2, 3):
+        n = 4000
+        mat = {"type": "DP_rheo", "density": 1500.0, "E": 1e7, "pois": 0.3, "M": 1.2, "Pt": 20.0,
+               "dilatancy_angle": 6.0}
+        L = rng.normal(0, 0.5, size=(n, dim, dim))
+        sref = rng.normal(0, 1e4, size=(n, 3, 3))
+        sref = 0.5 * (sref + sref.transpose(0, 2, 1))
+        sref[:, np.arange(3), np.arange(3)] -= 3e4
+        eps = rng.normal(0, 1e-4, size=(n, dim, dim))
+        eps = 0.5 * (eps + eps.transpose(0, 2, 1))
+        S0 = np.zeros((n, 3, 3))
+        S, E = material_point_update(mat, dim, L, S0, eps_e=eps, stress_ref=sref, dt=1e-3)
+        for i in range(0, n, 97):
+            s_ref, e_ref = oracle.dp_point(dim, L[i], S0[i], eps[i], sref[i], 1e-3, mat)
+            assert rel(S[i], s_ref) < 2e-5
+            assert rel(E[i], e_ref) < 2e-5
+
+
+def test_two_disc_kinetic_energy():
+    """tests/examples/two_disc_impact/test_two_disks.py: KE(0) ~ 2.51 (+-10 %)
+    and |KE(end) - KE(0)| / KE(0) < 0.2 over 3600 steps."""
+    v = G["two_disc_impact"]
+    scene = scenes.two_discs(cell_size=1.0 / 20, centers=((0.2, 0.2), (0.8, 0.8)), ppc_1d=2)
+    scene["materials"] = scene["materials"] * 2
+    n = len(scene["positions"])
+    scene["colors"] = (np.arange(n) >= n // 2).astype(np.uint8)
+    sim, _ = make_pair(scene)
+    sim.initialize()
+
+    def ke():
+        m = sim.get("masses")
+        vel = sim.get("velocities")
+        return 0.5 * float((m[:, None] * vel ** 2).sum())
+
+    ke0 = ke()
+    assert abs(ke0 - v["ke0"]) / v["ke0"] < v["ke0_rel_tol"]
+    sim.solve(v["steps"])
+    assert sim.synchronize() == 0
+    assert abs(ke() - ke0) / ke0 < v["ke_drift_max"]
+
+
+def test_out_of_domain_is_reported_not_fatal():
+    sc = random_scene(2, 500, "linear", 9, margin=0.1)
+    sc["positions"][0] = [3.0, 3.0]
+    sim, _ = make_pair(sc)
+    sim.initialize()
+    sim.solve(2)
+    assert sim.synchronize() == 16
+    sim.solve(1)
+    assert sim.synchronize() == 16
+    assert np.isfinite(sim.get("positions")[1:]).all()
