@@ -70,7 +70,12 @@ enum {
 enum {
   /* keep the velocity gradient L of the last step in device memory (needed
    * for the velocity_gradient getter; the step itself does not need it) */
-  PMPM_FLAG_KEEP_VELOCITY_GRADIENT = 1u << 0
+  PMPM_FLAG_KEEP_VELOCITY_GRADIENT = 1u << 0,
+  /* deterministic reduction: P2G gathers each node's contributions in the
+   * reference's fixed order (slot, then cell-sorted particle), so repeated
+   * runs are bitwise identical; the default P2G accumulates in shared memory
+   * in whatever order the threads arrive */
+  PMPM_FLAG_DETERMINISTIC = 1u << 1
 };
 
 /* Material parameters; fill with the pmpm_material_* helpers.

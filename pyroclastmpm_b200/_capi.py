@@ -23,6 +23,7 @@ SHAPE = {"linear": 0, "quadratic": 1, "cubic": 2}
 MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER = 0, 1, 2, 3
 BC_GRAVITY, BC_NODEDOMAIN, BC_BODYFORCE, BC_PLANARDOMAIN = 1, 2, 3, 4
 FLAG_KEEP_VELOCITY_GRADIENT = 1
+FLAG_DETERMINISTIC = 2
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not supported",

@@ -257,7 +257,10 @@ template <int D, int SF>
 int launch_p2g(pmpm_sim *s, int apply_bcs) {
   if (apply_bcs) update_gravity(s);
   StepArgs a = make_args(s);
-  k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
+  if (s->flags & PMPM_FLAG_DETERMINISTIC)
+    k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
+  else
+    k_p2g_tile<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
   PMPM_LAUNCHED();
   s->launches += 1;
   s->p2g_epoch = s->epoch;

@@ -507,6 +507,300 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int a
 }
 
 // --------------------------------------------------------------------------
+// P2G, fast path: tile scatter into shared memory
+// --------------------------------------------------------------------------
+//
+// One CTA per active node tile owns the tile's nodes.  It streams every
+// particle of the cells that can reach those nodes (the tile plus a halo of
+// the stencil width), evaluates the particle's per-axis weights once, and
+// adds the contributions that land inside the tile to shared-memory
+// accumulators (float atomics).  After a barrier each thread finishes one
+// node: the same epilogue as the gather path.  Each (particle, node) pair is
+// added by exactly one CTA, so no global atomics are needed; the summation
+// order inside a node is not fixed (use the gather path for bitwise
+// reproducibility).
+//
+// The halo is walked as rows of cells along x; a row is one contiguous range
+// of the cell-sorted order.  Rows use the reference's flat cell arithmetic,
+// so a row that runs past the grid's x extent continues into the next row of
+// cells, exactly where the reference's gather (usl_inline.h:114-126) finds
+// its aliased neighbours; overlapping row ranges are merged so each
+// particle is visited once per tile.
+
+template <int D, int SF>
+struct P2GTileShape {
+  using T = TileDims<D>;
+  static constexpr int LO = Stencil<SF>::WLO;
+  static constexpr int HI = Stencil<SF>::WLO + Stencil<SF>::WIN - 1;
+  static constexpr int HX = T::X + HI - LO;
+  static constexpr int HY = T::Y + HI - LO;
+  static constexpr int HZ = D == 3 ? T::Z + HI - LO : 1;
+  static constexpr int ROWS = HY * HZ;
+  static constexpr int NACC = 1 + 2 * D;
+};
+
+template <int D, int SF>
+__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int apply_bcs, int *node_epoch) {
+  using T = TileDims<D>;
+  using Sh = P2GTileShape<D, SF>;
+  constexpr int NT = T::N;
+  constexpr int K = Stencil<SF>::K;
+  const DevGrid &g = a.g;
+  const int tile = blockIdx.x;
+  if (a.N.tile_epoch[tile] != a.epoch) return;
+
+  __shared__ float acc[Sh::NACC * NT];
+  __shared__ int row_k0[Sh::ROWS];
+  __shared__ int row_lo[Sh::ROWS], row_hi[Sh::ROWS];
+  __shared__ int row_pref[Sh::ROWS + 1];
+  __shared__ int warp_tmp[33];
+
+  const int tid = threadIdx.x;
+  const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
+                     D == 3 ? (tile / (g.tdim[0] * g.tdim[1])) * T::Z : 0};
+#pragma unroll
+  for (int k = 0; k < Sh::NACC; k++) acc[k * NT + tid] = 0.0f;
+  if (tid == 0) node_epoch[tile] = a.epoch;
+
+  // ---- halo rows -> flat cell intervals -> sorted-order ranges ----
+  // Interior tiles (halo inside the grid) have disjoint, increasing row
+  // intervals.  Near the grid boundary the reference's flat arithmetic can
+  // make virtual rows overlap, so there the intervals are sorted and merged
+  // (each particle must be visited once).
+  bool interior = true;
+  {
+    const int tsz[3] = {T::X, T::Y, T::Z};
+#pragma unroll
+    for (int c = 0; c < D; c++)
+      interior = interior && t0[c] - Sh::HI >= 0 && t0[c] + tsz[c] - 1 - Sh::LO <= g.n[c] - 1;
+  }
+  const bool merge = SF != PMPM_SHAPE_QUADRATIC && !interior;
+  for (int r = tid; r < Sh::ROWS; r += NT) {
+    const int cy = t0[1] - Sh::HI + r % Sh::HY;
+    const int cz = D == 3 ? t0[2] - Sh::HI + r / Sh::HY : 0;
+    int x0 = t0[0] - Sh::HI, x1 = t0[0] + T::X - 1 - Sh::LO;
+    long long lo, hi;
+    if (SF == PMPM_SHAPE_QUADRATIC) {
+      const bool row_in = cy >= 0 && cy < g.n[1] && cz >= 0 && cz < g.n[2];
+      x0 = max(x0, 0);
+      x1 = min(x1, g.n[0] - 1);
+      lo = flat_index(g, x0, cy, cz);
+      hi = row_in ? (long long)flat_index(g, x1, cy, cz) : lo - 1;
+    } else {
+      const long long base = (long long)cy * g.n[0] + (long long)cz * g.n[0] * g.n[1];
+      lo = max(base + x0, 0ll);
+      hi = min(base + x1, (long long)g.ntotal - 1);
+    }
+    row_lo[r] = (int)max(min(lo, (long long)g.ntotal), -1ll);
+    row_hi[r] = (int)max(min(hi, (long long)g.ntotal), -2ll);
+  }
+  __syncthreads();
+  if (merge && tid == 0) {
+    // insertion sort by interval start, then clip each start past the
+    // furthest end seen so far
+    for (int i = 1; i < Sh::ROWS; i++) {
+      const int l = row_lo[i], h = row_hi[i];
+      int j = i - 1;
+      while (j >= 0 && row_lo[j] > l) {
+        row_lo[j + 1] = row_lo[j];
+        row_hi[j + 1] = row_hi[j];
+        j--;
+      }
+      row_lo[j + 1] = l;
+      row_hi[j + 1] = h;
+    }
+    int maxend = -1;
+    for (int i = 0; i < Sh::ROWS; i++) {
+      if (row_lo[i] > row_hi[i]) continue;
+      if (row_lo[i] <= maxend) row_lo[i] = maxend + 1;
+      if (row_hi[i] > maxend) maxend = row_hi[i];
+    }
+  }
+  __syncthreads();
+  const int nrow_iter = (Sh::ROWS + NT - 1) / NT;
+  int carry = 0;
+  for (int it = 0; it < nrow_iter; it++) {
+    const int r = it * NT + tid;
+    int cnt = 0, k0 = 0;
+    if (r < Sh::ROWS) {
+      const int lo = row_lo[r], hi = row_hi[r];
+      if (lo <= hi) {
+        k0 = a.B.offset[lo];
+        cnt = a.B.offset[hi + 1] - k0;
+      }
+    }
+    int total;
+    const int ex = block_exclusive_scan(cnt, warp_tmp, total);
+    if (r < Sh::ROWS) {
+      row_k0[r] = k0;
+      row_pref[r] = carry + ex;
+    }
+    carry += total;
+  }
+  if (tid == 0) row_pref[Sh::ROWS] = carry;
+  __syncthreads();
+  const int ntot = row_pref[Sh::ROWS];
+
+  // ---- particles: each thread takes one contiguous chunk of the list ----
+  const int chunk = (ntot + NT - 1) / NT;
+  const int j0 = tid * chunk, j1 = min(j0 + chunk, ntot);
+  int row = 0;
+  if (j0 < j1) {
+    int lo = 0, hi = Sh::ROWS;  // last row with row_pref <= j0
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (row_pref[mid] <= j0) lo = mid; else hi = mid;
+    }
+    row = lo;
+  }
+  const DevParticles &P = a.P;
+  const int st = P.stride;
+  for (int j = j0; j < j1; j++) {
+    while (row_pref[row + 1] <= j) row++;
+    const int s = a.B.order[row_k0[row] + (j - row_pref[row])];
+    float u[3] = {0, 0, 0};
+    int b[3] = {0, 0, 0};
+    bool inside = true;
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+      b[c] = (int)u[c];
+      inside = inside && b[c] >= 0 && b[c] < g.n[c];
+    }
+    if (SF == PMPM_SHAPE_QUADRATIC && !inside) continue;
+    // per-axis weights, target node coordinates and tile-local coordinates
+    float N[3][K], dN[3][K];
+    int loc[3][K];   // tile-local coordinate, or -1 outside the tile
+    bool inrange[3][K];
+    int woff[3] = {Stencil<SF>::WLO, Stencil<SF>::WLO, Stencil<SF>::WLO};
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        N[c][k] = 1.0f;
+        dN[c][k] = 0.0f;
+        loc[c][k] = 0;
+        inrange[c][k] = true;
+      }
+    const int tsz[3] = {T::X, T::Y, T::Z};
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      if (SF == PMPM_SHAPE_QUADRATIC) woff[c] = (u[c] - (float)(b[c] - 1)) < 1.5f ? -1 : 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const int sel = b[c] + woff[c] + k;
+        const bool in = sel >= 0 && sel < g.n[c];
+        const int node_c = SF == PMPM_SHAPE_QUADRATIC ? min(max(sel, 0), g.n[c] - 1) : sel;
+        const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(in ? sel : 0, g.n[c]) : 0;
+        axis_weight<SF>(u[c] - (float)sel, g.inv_h, type, N[c][k], dN[c][k]);
+        inrange[c][k] = SF == PMPM_SHAPE_QUADRATIC ? true : in;
+        const int l = node_c - t0[c];
+        loc[c][k] = (l >= 0 && l < tsz[c]) ? l : -1;
+      }
+    }
+    const float m = P.m[s];
+    float mv[3], fx[3] = {0, 0, 0}, S[9];
+#pragma unroll
+    for (int c = 0; c < D; c++) mv[c] = m * P.v[c * st + s];
+    if (a.has_planar) {
+#pragma unroll
+      for (int c = 0; c < D; c++) fx[c] = P.fext[c * st + s];
+    }
+    load_sig3<D>(P, s, S);
+    const float nvol = -P.V[s];
+#pragma unroll
+    for (int k = 0; k < 9; k++) S[k] *= nvol;
+    const unsigned hu = P.hash[s];
+    constexpr int KZ = D == 3 ? K : 1;
+#pragma unroll
+    for (int ky = 0; ky < K; ky++) {
+#pragma unroll
+      for (int kx = 0; kx < K; kx++) {
+#pragma unroll
+        for (int kz = 0; kz < KZ; kz++) {
+          int lx = loc[0][kx], ly = loc[1][ky], lz = D == 3 ? loc[2][kz] : 0;
+          const bool all_in = inrange[0][kx] && inrange[1][ky] && (D == 2 || inrange[2][kz]);
+          float tN[3] = {N[0][kx], N[1][ky], D == 3 ? N[2][kz] : 1.0f};
+          float tdN[3] = {dN[0][kx], dN[1][ky], D == 3 ? dN[2][kz] : 0.0f};
+          if (!all_in) {
+            // reference aliasing: the slot leaves the grid on an axis; its
+            // node is the flat index hash + flat(window offset)
+            const int w[3] = {woff[0] + kx, woff[1] + ky, D == 3 ? woff[2] + kz : 0};
+            const long long f = (long long)hu + w[0] + (long long)w[1] * g.n[0] +
+                                (long long)w[2] * g.n[0] * g.n[1];
+            if (f < 0 || f >= g.ntotal) continue;
+            const int fc[3] = {(int)(f % g.n[0]), (int)((f / g.n[0]) % g.n[1]),
+                               (int)(f / ((long long)g.n[0] * g.n[1]))};
+            lx = fc[0] - t0[0];
+            ly = fc[1] - t0[1];
+            lz = D == 3 ? fc[2] - t0[2] : 0;
+            if (lx < 0 || lx >= T::X || ly < 0 || ly >= T::Y || lz < 0 || lz >= T::Z) continue;
+            if (SF == PMPM_SHAPE_CUBIC) {
+              // node types of the aliased node (src/shapefunction/shapefunction.cpp:104-110)
+#pragma unroll
+              for (int c = 0; c < D; c++)
+                axis_weight<SF>(u[c] - (float)(b[c] + w[c]), g.inv_h, cubic_node_type(fc[c], g.n[c]), tN[c], tdN[c]);
+            }
+          } else if (lx < 0 || ly < 0 || lz < 0) {
+            continue;
+          }
+          float psi, dpsi[3];
+          if (D == 2) {
+            psi = tN[0] * tN[1];
+            dpsi[0] = tdN[0] * tN[1];
+            dpsi[1] = tdN[1] * tN[0];
+            dpsi[2] = 0.0f;
+          } else {
+            psi = tN[0] * tN[1] * tN[2];
+            dpsi[0] = tdN[0] * tN[1] * tN[2];
+            dpsi[1] = tdN[1] * tN[0] * tN[2];
+            dpsi[2] = tdN[2] * tN[0] * tN[1];
+          }
+          const int ln = lx + T::X * (ly + T::Y * lz);
+          atomicAdd(&acc[ln], psi * m);
+#pragma unroll
+          for (int c = 0; c < D; c++) {
+            float f = psi * fx[c] + S[3 * c + 0] * dpsi[0] + S[3 * c + 1] * dpsi[1];
+            if (D == 3) f += S[3 * c + 2] * dpsi[2];
+            atomicAdd(&acc[(1 + c) * NT + ln], psi * mv[c]);
+            atomicAdd(&acc[(1 + D + c) * NT + ln], f);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- node epilogue (one node per thread) ----
+  const int lx = tid % T::X, ly = (tid / T::X) % T::Y, lz = tid / (T::X * T::Y);
+  const int nc[3] = {t0[0] + lx, t0[1] + ly, D == 3 ? t0[2] + lz : 0};
+  if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) return;
+  const int node = flat_index(g, nc[0], nc[1], nc[2]);
+  float mass = acc[tid];
+  float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+  const bool live = mass > a.cutoff;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      p[c] = acc[(1 + c) * NT + tid];
+      pnt[c] = p[c] + acc[(1 + D + c) * NT + tid] * a.dt;
+    }
+  } else {
+    mass = 0.0f;
+  }
+  if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
+  const int nt = g.ntotal;
+  a.N.m[node] = mass;
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    a.N.p[c * nt + node] = p[c];
+    a.N.pnt[c * nt + node] = pnt[c];
+    a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
+    a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
+  }
+}
+
+// --------------------------------------------------------------------------
 // G2P + deformation update + stress update
 // --------------------------------------------------------------------------
 

@@ -42,6 +42,21 @@ def two_discs(cell_size=0.02, radius=0.2, centers=((0.25, 0.25), (0.75, 0.75)), 
                 positions=np.concatenate(pos), velocities=np.concatenate(vel))
 
 
+def water_column(cell_size=0.02, block=(0.4, 0.6), domain=(1.0, 1.0), ppc_1d=2, dt=1e-4, viscosity=1e-3,
+                 bulk_modulus=2e6, gamma=7.0, density=1000.0, shape_function="quadratic"):
+    """2D water block in the corner of a box (Newtonian fluid, gravity, slip
+    walls), as the reference's water example sets it up."""
+    spacing = cell_size / ppc_1d
+    pts = _lattice(np.zeros(2), np.asarray(block, np.float64), spacing)
+    return dict(dim=2, origin=[0.0, 0.0], end=list(domain), cell_size=cell_size, shape_function=shape_function,
+                dt=dt, particles_per_cell=ppc_1d ** 2, alpha=0.99,
+                materials=[{"type": "NewtonFluid", "density": density, "viscosity": viscosity,
+                            "bulk_modulus": bulk_modulus, "gamma": gamma}],
+                bcs=[{"type": "Gravity", "gravity": [0.0, -9.81]},
+                     {"type": "NodeDomain", "face0_mode": [1, 1], "face1_mode": [1, 1]}],
+                positions=pts, velocities=np.zeros_like(pts))
+
+
 def granular_column(domain=(1.0, 0.25, 0.5), cell_size=1.0 / 256, column=(0.2, 0.25, 0.2), ppc_1d=2,
                     jitter=0.25, seed=0, shape_function="quadratic", dt=1e-5, scale=1.0,
                     density=1500.0, E=1.0e7, pois=0.3, friction_angle=30.0, dilatancy_angle=0.0, cohesion=0.0):

