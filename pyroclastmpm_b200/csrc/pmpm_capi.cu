@@ -906,6 +906,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   PMPM_CUDA(cudaMemcpy(P.F, F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemset(P.sig, 0, sizeof(float) * S * st));
   PMPM_CUDA(cudaMemset(P.L, 0, sizeof(float) * D * D * st));
+  PMPM_CUDA(cudaMemset(s->P[1].L, 0, sizeof(float) * D * D * st));
   PMPM_CUDA(cudaMemcpy(P.m, m.data(), sizeof(float) * st, cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemcpy(P.V, V.data(), sizeof(float) * st, cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemcpy(P.V0, V.data(), sizeof(float) * st, cudaMemcpyHostToDevice));

@@ -591,8 +591,9 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int app
       lo = max(base + x0, 0ll);
       hi = min(base + x1, (long long)g.ntotal - 1);
     }
-    row_lo[r] = (int)max(min(lo, (long long)g.ntotal), -1ll);
-    row_hi[r] = (int)max(min(hi, (long long)g.ntotal), -2ll);
+    // keep 0 <= lo and hi <= ntotal - 1; lo > hi marks an empty row
+    row_lo[r] = (int)min(max(lo, 0ll), (long long)g.ntotal);
+    row_hi[r] = (int)max(min(hi, (long long)g.ntotal - 1), -1ll);
   }
   __syncthreads();
   if (merge && tid == 0) {
