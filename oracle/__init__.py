@@ -158,7 +158,8 @@ class OracleSim:
         self.npr = npr
         self.dim = d = dim
         self.sf = SHAPE_FUNCTIONS[shape_function] if isinstance(shape_function, str) else int(shape_function)
-        x = np.ascontiguousarray(np.asarray(positions, dtype=npr).reshape(-1, d))
+        # inputs are always copied: the simulation advances its arrays in place
+        x = np.array(positions, dtype=npr, copy=True).reshape(-1, d)
         n = x.shape[0]
         self.n = n
         g = Grid()
@@ -172,8 +173,8 @@ class OracleSim:
         z = lambda *shape: np.zeros(shape, dtype=npr)
         self.a = a = {}
         a["positions"] = x
-        a["velocities"] = z(n, d) if velocities is None else np.ascontiguousarray(np.asarray(velocities, npr).reshape(n, d))
-        a["stresses"] = z(n, 3, 3) if stresses is None else np.ascontiguousarray(np.asarray(stresses, npr).reshape(n, 3, 3))
+        a["velocities"] = z(n, d) if velocities is None else np.array(velocities, npr, copy=True).reshape(n, d)
+        a["stresses"] = z(n, 3, 3) if stresses is None else np.array(stresses, npr, copy=True).reshape(n, 3, 3)
         a["F"] = np.ascontiguousarray(np.broadcast_to(np.eye(d, dtype=npr), (n, d, d)))
         a["velocity_gradient"] = z(n, d, d)
         a["masses"] = np.full(n, -1.0, npr) if masses is None else np.asarray(masses, npr).copy()
