@@ -257,10 +257,20 @@ template <int D, int SF>
 int launch_p2g(pmpm_sim *s, int apply_bcs) {
   if (apply_bcs) update_gravity(s);
   StepArgs a = make_args(s);
-  if (s->flags & PMPM_FLAG_DETERMINISTIC)
+  if (s->flags & PMPM_FLAG_DETERMINISTIC) {
     k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
-  else
+  } else if (D == 3) {
+    constexpr int bytes = sweep3_smem_bytes<SF>();
+    static bool attr_set[64] = {false};  // per device
+    const int dev = s->device < 64 ? s->device : 63;
+    if (!attr_set[dev]) {
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      attr_set[dev] = true;
+    }
+    k_p2g_sweep3<SF><<<s->g.ntiles, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+  } else {
     k_p2g_tile<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
+  }
   PMPM_LAUNCHED();
   s->launches += 1;
   s->p2g_epoch = s->epoch;

@@ -802,6 +802,329 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int app
 }
 
 // --------------------------------------------------------------------------
+// P2G, 3D fast path: z-sweep with register windows
+// --------------------------------------------------------------------------
+//
+// One CTA per active 8x8x8 node tile.  Work item = (x pair, y pair), a pair
+// being (source cell column, stencil offset) whose target node column lies in
+// the tile.  Each item sweeps the source cell layers along z.  For every
+// layer the CTA stages the particles of the layer's halo cells in shared
+// memory (with their z weights, which every item needs), then each item adds
+// its source cell's particles into a register window of the WIN z nodes
+// that layer can reach.  The lowest window node is complete after the layer
+// (later layers only reach higher nodes), so it is added to the shared tile
+// accumulator and the window shifts: 7 shared-memory atomics per item and
+// tile node instead of 7 per particle and node.
+//
+// Sources are virtual cells: node n takes slot w from cell flat(n) - flat(w),
+// the reference gather's flat arithmetic (usl_inline.h:114-126), so cells
+// past a grid face alias onto neighbouring rows exactly as there; the weight
+// uses the particle's own bin (the reference psi), the cubic node type the
+// target node's.  Quadratic sources are real cells and targets are clamped.
+
+template <int SF>
+struct Sweep3 {
+  using T = TileDims<3>;
+  static constexpr int WIN = Stencil<SF>::WIN;
+  static constexpr int LO = Stencil<SF>::WLO;
+  static constexpr int HI = Stencil<SF>::WLO + Stencil<SF>::WIN - 1;
+  static constexpr int NS = T::X + WIN - 1;          // source cells per axis
+  static constexpr int MAXPAIR = NS * WIN;           // (source, offset) pairs per axis
+  static constexpr int NCELL = NS * NS;              // source cells per layer
+  static constexpr int CAP = 1024;                   // staged particles per chunk
+  static constexpr int NT = T::N;
+  static constexpr int IPT = 2;                      // items per thread per round
+};
+
+template <int SF>
+constexpr int sweep3_smem_bytes() {
+  return (7 * Sweep3<SF>::NT + Sweep3<SF>::CAP * (2 + 2 + 1 + 3 + 6 + 2 * Sweep3<SF>::WIN)) * 4;
+}
+
+// pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
+// stencil offset in bits 8..9, target local coordinate in bits 12..15
+__device__ __forceinline__ int pair_src(int p) { return p & 0xff; }
+__device__ __forceinline__ int pair_off(int p) { return (p >> 8) & 0x3; }
+__device__ __forceinline__ int pair_tgt(int p) { return (p >> 12) & 0xf; }
+
+template <int SF>
+__device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
+  using W = Sweep3<SF>;
+  constexpr int TS = W::T::X;
+  int cnt = 0;
+  for (int si = 0; si < W::NS; si++) {
+    const int src = t0 - W::HI + si;
+    if (SF == PMPM_SHAPE_QUADRATIC && (src < 0 || src >= n)) continue;
+    for (int i = 0; i < W::WIN; i++) {
+      int t = src + i + W::LO;
+      if (SF == PMPM_SHAPE_QUADRATIC) t = min(max(t, 0), n - 1);
+      const int l = t - t0;
+      if (l < 0 || l >= TS || t >= n || t < 0) continue;
+      pairs[cnt++] = si | (i << 8) | (l << 12);
+    }
+  }
+  return cnt;
+}
+
+template <int SF>
+__global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
+  using W = Sweep3<SF>;
+  using T = TileDims<3>;
+  constexpr int NT = W::NT;
+  constexpr int WIN = W::WIN;
+  const DevGrid &g = a.g;
+  const int tile = blockIdx.x;
+  if (a.N.tile_epoch[tile] != a.epoch) return;
+
+  __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
+  __shared__ int npair[2];
+  __shared__ int cell_k0[W::NCELL], cell_pref[W::NCELL + 1];
+  __shared__ int warp_tmp[33];
+  // dynamic shared memory: tile accumulators, then the staged particles
+  // (structure of arrays, W::CAP entries each); size sweep3_smem_bytes<SF>()
+  extern __shared__ __align__(16) float dyn_smem[];
+  float *acc = dyn_smem;                                   // [7][NT]
+  float(*st_u)[W::CAP] = (float(*)[W::CAP])(acc + 7 * NT);  // [2] scaled x, y
+  int(*st_b)[W::CAP] = (int(*)[W::CAP])(st_u + 2);          // [2] bins x, y
+  float *st_m = (float *)(st_b + 2);                        // [CAP]
+  float(*st_mv)[W::CAP] = (float(*)[W::CAP])(st_m + W::CAP); // [3]
+  float(*st_S)[W::CAP] = st_mv + 3;                          // [6] -V sigma
+  float(*st_nz)[W::CAP] = st_S + 6;                          // [WIN]
+  float(*st_dnz)[W::CAP] = st_nz + WIN;                      // [WIN]
+
+  const int tid = threadIdx.x;
+  const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
+                     (tile / (g.tdim[0] * g.tdim[1])) * T::Z};
+#pragma unroll
+  for (int k = 0; k < 7; k++) acc[k * NT + tid] = 0.0f;
+  if (tid == 0) {
+    node_epoch[tile] = a.epoch;
+    npair[0] = build_pairs<SF>(t0[0], g.n[0], pairs_x);
+  } else if (tid == 32) {
+    npair[1] = build_pairs<SF>(t0[1], g.n[1], pairs_y);
+  }
+  __syncthreads();
+  const int nx = npair[0], ny = npair[1];
+  const int nitems = nx * ny;
+  const int nrounds = (nitems + NT * W::IPT - 1) / (NT * W::IPT);
+
+  // z range of source layers
+  int cz_lo = t0[2] - W::HI, cz_hi = t0[2] + T::Z - 1 - W::LO;
+  if (SF == PMPM_SHAPE_QUADRATIC) {
+    cz_lo = max(cz_lo, 0);
+    cz_hi = min(cz_hi, g.n[2] - 1);
+  }
+  const DevParticles &P = a.P;
+  const int st = P.stride;
+  const long long nxny = (long long)g.n[0] * g.n[1];
+
+  for (int round = 0; round < nrounds; round++) {
+    // this thread's items
+    int item_cell[W::IPT], item_ix[W::IPT], item_iy[W::IPT], item_tl[W::IPT];
+    int item_tx[W::IPT], item_ty[W::IPT];
+    bool item_ok[W::IPT];
+    float win[W::IPT][WIN][7];
+#pragma unroll
+    for (int q = 0; q < W::IPT; q++) {
+      const int it = (round * W::IPT + q) * NT + tid;
+      item_ok[q] = it < nitems;
+      const int px = item_ok[q] ? pairs_x[it % nx] : 0;
+      const int py = item_ok[q] ? pairs_y[it / nx] : 0;
+      item_cell[q] = pair_src(py) * W::NS + pair_src(px);
+      item_ix[q] = pair_off(px);
+      item_iy[q] = pair_off(py);
+      item_tx[q] = pair_tgt(px);
+      item_ty[q] = pair_tgt(py);
+      item_tl[q] = item_tx[q] + T::X * item_ty[q];
+#pragma unroll
+      for (int k = 0; k < WIN; k++)
+#pragma unroll
+        for (int c = 0; c < 7; c++) win[q][k][c] = 0.0f;
+    }
+    for (int cz = cz_lo; cz <= cz_hi; cz++) {
+      // ---- the layer's source cells -> sorted ranges, prefix ----
+      int carry = 0;
+      for (int it = 0; it < (W::NCELL + NT - 1) / NT; it++) {
+        const int vc = it * NT + tid;
+        int cnt = 0, k0 = 0;
+        if (vc < W::NCELL) {
+          const int sx = t0[0] - W::HI + vc % W::NS, sy = t0[1] - W::HI + vc / W::NS;
+          bool valid;
+          long long f;
+          if (SF == PMPM_SHAPE_QUADRATIC) {
+            valid = sx >= 0 && sx < g.n[0] && sy >= 0 && sy < g.n[1];
+            f = sx + (long long)sy * g.n[0] + (long long)cz * nxny;
+          } else {
+            f = sx + (long long)sy * g.n[0] + (long long)cz * nxny;
+            valid = f >= 0 && f < g.ntotal;
+          }
+          if (valid) {
+            k0 = a.B.offset[f];
+            cnt = a.B.offset[f + 1] - k0;
+          }
+          cell_k0[vc] = k0;
+        }
+        int total;
+        const int ex = block_exclusive_scan(cnt, warp_tmp, total);
+        if (vc < W::NCELL) cell_pref[vc] = carry + ex;
+        carry += total;
+      }
+      if (tid == 0) cell_pref[W::NCELL] = carry;
+      __syncthreads();
+      const int layer_n = cell_pref[W::NCELL];
+      // cubic z node types of this layer's targets cz + LO .. cz + HI
+      for (int c0 = 0; c0 < layer_n; c0 += W::CAP) {
+        const int c1 = min(c0 + W::CAP, layer_n);
+        // ---- stage particles [c0, c1) ----
+        for (int j = c0 + tid; j < c1; j += NT) {
+          int lo = 0, hi = W::NCELL;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (cell_pref[mid] <= j) lo = mid; else hi = mid;
+          }
+          const int s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+          const int jj = j - c0;
+          float u[3];
+          int b[3];
+          bool inside = true;
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+            b[c] = (int)u[c];
+            inside = inside && b[c] >= 0 && b[c] < g.n[c];
+          }
+          float m = P.m[s];
+          if (SF == PMPM_SHAPE_QUADRATIC && !inside) m = 0.0f;  // takes no part in P2G
+          const float nv = (SF == PMPM_SHAPE_QUADRATIC && !inside) ? 0.0f : -P.V[s];
+          st_u[0][jj] = u[0];
+          st_u[1][jj] = u[1];
+          st_b[0][jj] = b[0];
+          st_b[1][jj] = b[1];
+          st_m[jj] = m;
+#pragma unroll
+          for (int c = 0; c < 3; c++) st_mv[c][jj] = m * P.v[c * st + s];
+          // -V sigma, symmetric: xx yy zz xy xz yz
+#pragma unroll
+          for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
+#pragma unroll
+          for (int k = 0; k < WIN; k++) {
+            const int tz = cz + k + W::LO;
+            const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(min(max(tz, 0), g.n[2] - 1), g.n[2]) : 0;
+            float N, dN;
+            axis_weight<SF>(u[2] - (float)(b[2] + k + W::LO), g.inv_h, type, N, dN);
+            st_nz[k][jj] = N;
+            st_dnz[k][jj] = dN;
+          }
+        }
+        __syncthreads();
+        // ---- items: add their source cell's staged particles ----
+#pragma unroll
+        for (int q = 0; q < W::IPT; q++) {
+          if (!item_ok[q]) continue;
+          const int vc = item_cell[q];
+          const int j0 = max(cell_pref[vc], c0) - c0, j1 = min(cell_pref[vc + 1], c1) - c0;
+          const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
+          const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
+          const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
+          for (int j = j0; j < j1; j++) {
+            float Nx, dNx, Ny, dNy;
+            axis_weight<SF>(st_u[0][j] - (float)(st_b[0][j] + wx), g.inv_h, typex, Nx, dNx);
+            axis_weight<SF>(st_u[1][j] - (float)(st_b[1][j] + wy), g.inv_h, typey, Ny, dNy);
+            const float m = st_m[j];
+            const float mvx = st_mv[0][j], mvy = st_mv[1][j], mvz = st_mv[2][j];
+            const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
+            const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
+            const float nn = Nx * Ny;
+            const float gx = dNx * Ny, gy = Nx * dNy;
+            // f_c = Nz (S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
+            const float Ax = Sxx * gx + Sxy * gy, Ay = Sxy * gx + Syy * gy, Az = Sxz * gx + Syz * gy;
+            const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
+            const float mn = m * nn, mvxn = mvx * nn, mvyn = mvy * nn, mvzn = mvz * nn;
+#pragma unroll
+            for (int k = 0; k < WIN; k++) {
+              const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
+              win[q][k][0] += mn * Nz;
+              win[q][k][1] += mvxn * Nz;
+              win[q][k][2] += mvyn * Nz;
+              win[q][k][3] += mvzn * Nz;
+              win[q][k][4] += Ax * Nz + Bx * dNz;
+              win[q][k][5] += Ay * Nz + By * dNz;
+              win[q][k][6] += Az * Nz + Bz * dNz;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      // ---- the lowest window node is complete: flush and shift ----
+#pragma unroll
+      for (int q = 0; q < W::IPT; q++) {
+        if (item_ok[q]) {
+          int tz = cz + W::LO;
+          if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
+          const int lz = tz - t0[2];
+          if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
+            const int ln = item_tl[q] + T::X * T::Y * lz;
+#pragma unroll
+            for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NT + ln], win[q][0][c]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < WIN - 1; k++)
+#pragma unroll
+          for (int c = 0; c < 7; c++) win[q][k][c] = win[q][k + 1][c];
+#pragma unroll
+        for (int c = 0; c < 7; c++) win[q][WIN - 1][c] = 0.0f;
+      }
+    }
+    // ---- remaining window nodes after the last layer ----
+#pragma unroll
+    for (int q = 0; q < W::IPT; q++) {
+      if (!item_ok[q]) continue;
+#pragma unroll
+      for (int k = 0; k < WIN - 1; k++) {
+        int tz = cz_hi + 1 + k + W::LO;
+        if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
+        const int lz = tz - t0[2];
+        if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
+          const int ln = item_tl[q] + T::X * T::Y * lz;
+#pragma unroll
+          for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NT + ln], win[q][k][c]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- node epilogue (one node per thread) ----
+  const int lx = tid % T::X, ly = (tid / T::X) % T::Y, lz = tid / (T::X * T::Y);
+  const int nc[3] = {t0[0] + lx, t0[1] + ly, t0[2] + lz};
+  if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) return;
+  const int node = flat_index(g, nc[0], nc[1], nc[2]);
+  float mass = acc[tid];
+  float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+  const bool live = mass > a.cutoff;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      p[c] = acc[(1 + c) * NT + tid];
+      pnt[c] = p[c] + acc[(4 + c) * NT + tid] * a.dt;
+    }
+  } else {
+    mass = 0.0f;
+  }
+  if (apply_bcs) node_bcs<3>(a, node, nc, mass, p, pnt);
+  const int nt = g.ntotal;
+  a.N.m[node] = mass;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    a.N.p[c * nt + node] = p[c];
+    a.N.pnt[c * nt + node] = pnt[c];
+    a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
+    a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
+  }
+}
+
+// --------------------------------------------------------------------------
 // G2P + deformation update + stress update
 // --------------------------------------------------------------------------
 

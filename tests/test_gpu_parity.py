@@ -239,6 +239,10 @@ STEP_CASES = {
         3, 4000, "cubic", 4, margin=0.05, cell=0.1,
         bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]},
              {"type": "NodeDomain", "face0_mode": [1, 1, 1], "face1_mode": [1, 1, 1]}]),
+    "random_3d_quadratic_le_walls": lambda: random_scene(
+        3, 4000, "quadratic", 6, margin=0.0, cell=0.1,
+        bcs=[{"type": "Gravity", "gravity": [0.0, -9.81, 0.0]},
+             {"type": "NodeDomain", "face0_mode": [1, 0, 1], "face1_mode": [1, 1, 0]}]),
     "random_3d_linear_nf_planar": lambda: random_scene(
         3, 4000, "linear", 5, margin=0.0, cell=0.1,
         mats=[{"type": "NewtonFluid", "density": 1000.0, "viscosity": 1e-2, "bulk_modulus": 1e4, "gamma": 7.0}],
