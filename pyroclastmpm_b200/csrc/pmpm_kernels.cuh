@@ -832,13 +832,17 @@ struct Sweep3 {
   static constexpr int MAXPAIR = NS * WIN;           // (source, offset) pairs per axis
   static constexpr int NCELL = NS * NS;              // source cells per layer
   static constexpr int CAP = 1024;                   // staged particles per chunk
+  // each cell's staged run starts one slot later than packing would put it,
+  // so runs of neighbouring cells (read by neighbouring lanes) start in
+  // different shared-memory banks
+  static constexpr int SLOTS = CAP + NS * NS;
   static constexpr int NT = T::N;
   static constexpr int IPT = 2;                      // items per thread per round
 };
 
 template <int SF>
 constexpr int sweep3_smem_bytes() {
-  return (7 * Sweep3<SF>::NT + Sweep3<SF>::CAP * (2 + 2 + 1 + 3 + 6 + 2 * Sweep3<SF>::WIN)) * 4;
+  return (7 * Sweep3<SF>::NT + Sweep3<SF>::SLOTS * (2 + 2 + 1 + 3 + 3 + 6 + 2 * Sweep3<SF>::WIN)) * 4;
 }
 
 // pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
@@ -884,13 +888,15 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
   // (structure of arrays, W::CAP entries each); size sweep3_smem_bytes<SF>()
   extern __shared__ __align__(16) float dyn_smem[];
   float *acc = dyn_smem;                                   // [7][NT]
-  float(*st_u)[W::CAP] = (float(*)[W::CAP])(acc + 7 * NT);  // [2] scaled x, y
-  int(*st_b)[W::CAP] = (int(*)[W::CAP])(st_u + 2);          // [2] bins x, y
-  float *st_m = (float *)(st_b + 2);                        // [CAP]
-  float(*st_mv)[W::CAP] = (float(*)[W::CAP])(st_m + W::CAP); // [3]
-  float(*st_S)[W::CAP] = st_mv + 3;                          // [6] -V sigma
-  float(*st_nz)[W::CAP] = st_S + 6;                          // [WIN]
-  float(*st_dnz)[W::CAP] = st_nz + WIN;                      // [WIN]
+  constexpr int SL = W::SLOTS;
+  float(*st_u)[SL] = (float(*)[SL])(acc + 7 * NT);  // [2] scaled x, y
+  int(*st_b)[SL] = (int(*)[SL])(st_u + 2);          // [2] bins x, y
+  float *st_m = (float *)(st_b + 2);                // [SL]
+  float(*st_mv)[SL] = (float(*)[SL])(st_m + SL);    // [3] m v
+  float(*st_f)[SL] = st_mv + 3;                     // [3] external force
+  float(*st_S)[SL] = st_f + 3;                      // [6] -V sigma
+  float(*st_nz)[SL] = st_S + 6;                     // [WIN]
+  float(*st_dnz)[SL] = st_nz + WIN;                 // [WIN]
 
   const int tid = threadIdx.x;
   const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
@@ -983,7 +989,7 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
             if (cell_pref[mid] <= j) lo = mid; else hi = mid;
           }
           const int s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
-          const int jj = j - c0;
+          const int jj = j - c0 + lo;  // skewed slot
           float u[3];
           int b[3];
           bool inside = true;
@@ -1002,7 +1008,10 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
           st_b[1][jj] = b[1];
           st_m[jj] = m;
 #pragma unroll
-          for (int c = 0; c < 3; c++) st_mv[c][jj] = m * P.v[c * st + s];
+          for (int c = 0; c < 3; c++) {
+            st_mv[c][jj] = m * P.v[c * st + s];
+            st_f[c][jj] = (a.has_planar && m != 0.0f) ? P.fext[c * st + s] : 0.0f;
+          }
           // -V sigma, symmetric: xx yy zz xy xz yz
 #pragma unroll
           for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
@@ -1022,7 +1031,7 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
         for (int q = 0; q < W::IPT; q++) {
           if (!item_ok[q]) continue;
           const int vc = item_cell[q];
-          const int j0 = max(cell_pref[vc], c0) - c0, j1 = min(cell_pref[vc + 1], c1) - c0;
+          const int j0 = max(cell_pref[vc], c0) - c0 + vc, j1 = min(cell_pref[vc + 1], c1) - c0 + vc;
           const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
           const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
           const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
@@ -1036,8 +1045,10 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
             const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
             const float nn = Nx * Ny;
             const float gx = dNx * Ny, gy = Nx * dNy;
-            // f_c = Nz (S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
-            const float Ax = Sxx * gx + Sxy * gy, Ay = Sxy * gx + Syy * gy, Az = Sxz * gx + Syz * gy;
+            // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
+            const float Ax = st_f[0][j] * nn + Sxx * gx + Sxy * gy;
+            const float Ay = st_f[1][j] * nn + Sxy * gx + Syy * gy;
+            const float Az = st_f[2][j] * nn + Sxz * gx + Syz * gy;
             const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
             const float mn = m * nn, mvxn = mvx * nn, mvyn = mvy * nn, mvzn = mvz * nn;
 #pragma unroll
