@@ -98,6 +98,10 @@ struct pmpm_sim {
   // bins
   DevBins B{};
   int nscan_blocks = 0;
+  bool dual = false;  // quadratic 3D fast path bins by dual cell
+  int kd[3] = {1, 1, 1};
+  int nkeys = 0;
+  int *key = nullptr;  // binning key scratch
   int *fault = nullptr;
   // staging for field conversion
   void *staging = nullptr;
@@ -147,6 +151,7 @@ void free_particles(pmpm_sim *s) {
     P = DevParticles{};
   }
   dfree(s->slot);
+  dfree(s->key);
   dfree(s->B.order);
   s->n = 0;
   s->stride = 0;
@@ -184,8 +189,12 @@ StepArgs make_args(pmpm_sim *s) {
   a.g = s->g;
   a.P = s->P[s->cur];
   a.P.slot = s->slot;
+  a.P.key = (unsigned *)s->key;
   a.N = s->N;
   a.B = s->B;
+  a.B.dual = s->dual ? 1 : 0;
+  for (int c = 0; c < 3; c++) a.B.kd[c] = s->kd[c];
+  a.B.nkeys = s->nkeys;
   a.dt = s->dt;
   a.alpha = s->alpha;
   a.one_minus_alpha = (float)(1.0 - (double)s->alpha);
@@ -224,15 +233,15 @@ int launch_partition(pmpm_sim *s) {
   k_hash_count<D, SF><<<blocks_for(s->n), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
   s->launches += 7;
-  k_scan_reduce<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->g.ntotal, s->B.block_sums);
+  k_scan_reduce<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->nkeys, s->B.block_sums);
   PMPM_LAUNCHED();
   k_scan_top<<<1, kScanThreads, 0, st>>>(s->B.block_sums, s->nscan_blocks, s->B.scalars);
   PMPM_LAUNCHED();
-  k_scan_apply<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->g.ntotal, s->B.block_sums, s->B.offset);
+  k_scan_apply<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->nkeys, s->B.block_sums, s->B.offset);
   PMPM_LAUNCHED();
   k_scatter<<<blocks_for(s->n), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
-  k_sort_cells<<<blocks_for(s->g.ntotal), kTPB, 0, st>>>(a);
+  k_sort_cells<<<blocks_for(s->nkeys), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
   k_sort_big<<<148, 1024, 0, st>>>(a);
   PMPM_LAUNCHED();
@@ -259,6 +268,15 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   StepArgs a = make_args(s);
   if (s->flags & PMPM_FLAG_DETERMINISTIC) {
     k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
+  } else if (s->dual) {
+    constexpr int bytes = dual3_smem_bytes();
+    static bool attr_set[64] = {false};  // per device
+    const int dev = s->device < 64 ? s->device : 63;
+    if (!attr_set[dev]) {
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      attr_set[dev] = true;
+    }
+    k_p2g_dual3<<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
   } else if (D == 3) {
     constexpr int bytes = sweep3_smem_bytes<SF>();
     static bool attr_set[64] = {false};  // per device
@@ -511,6 +529,22 @@ int sorted_views(pmpm_sim *s, std::vector<int> &sorted_index, std::vector<unsign
   std::vector<unsigned> hash(n);
   int nb = 0;
   const DevParticles &P = s->P[s->cur];
+  if (s->dual) {
+    // the step bins by dual cell; the reference permutation is the stable
+    // sort of the stored reference hashes
+    PMPM_CUDA(cudaMemcpyAsync(id.data(), P.id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+    PMPM_CUDA(cudaMemcpyAsync(hash.data(), P.hash, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s->stream));
+    PMPM_CUDA(cudaStreamSynchronize(s->stream));
+    std::vector<unsigned> by_id(n);
+    for (int k = 0; k < n; k++) by_id[id[k]] = hash[k];
+    sorted_index.resize(n);
+    hash_sorted.resize(n);
+    std::iota(sorted_index.begin(), sorted_index.end(), 0);
+    std::stable_sort(sorted_index.begin(), sorted_index.end(),
+                     [&](int x, int y) { return by_id[x] < by_id[y]; });
+    for (int k = 0; k < n; k++) hash_sorted[k] = by_id[sorted_index[k]];
+    return PMPM_OK;
+  }
   PMPM_CUDA(cudaMemcpyAsync(order.data(), s->B.order, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
   PMPM_CUDA(cudaMemcpyAsync(id.data(), P.id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
   PMPM_CUDA(cudaMemcpyAsync(hash.data(), P.hash, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s->stream));
@@ -795,15 +829,23 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK) st = dalloc(&s->N.vnt, nn * D);
   if (st == PMPM_OK) st = dalloc(&s->N.tile_epoch, (size_t)g.ntiles);
   if (st == PMPM_OK) st = dalloc(&s->node_epoch, (size_t)g.ntiles);
-  s->nscan_blocks = (g.ntotal + kScanChunk - 1) / kScanChunk;
-  if (st == PMPM_OK) st = dalloc(&s->B.count, nn);
-  if (st == PMPM_OK) st = dalloc(&s->B.offset, nn + 1);
+  // binning key space (reference cells, or dual cells for the 3D quadratic fast path)
+  s->dual = s->dim == 3 && s->shape == PMPM_SHAPE_QUADRATIC && !(s->flags & PMPM_FLAG_DETERMINISTIC);
+  s->nkeys = 1;
+  for (int c = 0; c < 3; c++) {
+    s->kd[c] = (s->dual && c < s->dim) ? g.n[c] + 1 : g.n[c];
+    s->nkeys *= s->kd[c];
+  }
+  const size_t nk = (size_t)s->nkeys;
+  s->nscan_blocks = (s->nkeys + kScanChunk - 1) / kScanChunk;
+  if (st == PMPM_OK) st = dalloc(&s->B.count, nk);
+  if (st == PMPM_OK) st = dalloc(&s->B.offset, nk + 1);
   if (st == PMPM_OK) st = dalloc(&s->B.block_sums, (size_t)s->nscan_blocks);
   if (st == PMPM_OK) st = dalloc(&s->B.scalars, 4);
-  if (st == PMPM_OK) st = dalloc(&s->B.big_cells, nn);
+  if (st == PMPM_OK) st = dalloc(&s->B.big_cells, nk);
   if (st == PMPM_OK) st = dalloc(&s->fault, 1);
   if (st == PMPM_OK) {
-    if (cudaMemset(s->B.count, 0, nn * sizeof(int)) != cudaSuccess ||
+    if (cudaMemset(s->B.count, 0, nk * sizeof(int)) != cudaSuccess ||
         cudaMemset(s->B.scalars, 0, 4 * sizeof(int)) != cudaSuccess ||
         cudaMemset(s->fault, 0, sizeof(int)) != cudaSuccess ||
         cudaMemset(s->N.tile_epoch, 0xff, g.ntiles * sizeof(int)) != cudaSuccess ||
@@ -887,6 +929,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   PMPM_TRY(alloc_particle_set(s, s->P[0]));
   PMPM_TRY(alloc_particle_set(s, s->P[1]));
   PMPM_TRY(dalloc(&s->slot, (size_t)s->stride));
+  PMPM_TRY(dalloc(&s->key, (size_t)s->stride));
   PMPM_TRY(dalloc(&s->B.order, (size_t)s->stride));
   const int st = s->stride;
   const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6;
@@ -1011,10 +1054,19 @@ int pmpm_get_field(pmpm_sim *s, int field, void *dst, size_t bytes, int on_devic
         memcpy(host.data(), hs.data(), need);
     } else {
       // cell_start / cell_end: 0 for empty cells (SpatialPartition::reset fills 0)
-      std::vector<int> off(g.ntotal + 1);
-      PMPM_CUDA(cudaMemcpyAsync(off.data(), s->B.offset, sizeof(int) * (g.ntotal + 1), cudaMemcpyDeviceToHost,
-                                s->stream));
-      PMPM_CUDA(cudaStreamSynchronize(s->stream));
+      std::vector<int> off(g.ntotal + 1, 0);
+      if (s->dual) {
+        std::vector<unsigned> hash(s->n);
+        PMPM_CUDA(cudaMemcpyAsync(hash.data(), P.hash, sizeof(unsigned) * s->n, cudaMemcpyDeviceToHost, s->stream));
+        PMPM_CUDA(cudaStreamSynchronize(s->stream));
+        for (unsigned h : hash)
+          if (h < (unsigned)g.ntotal) off[h + 1] += 1;
+        for (int c = 0; c < g.ntotal; c++) off[c + 1] += off[c];
+      } else {
+        PMPM_CUDA(cudaMemcpyAsync(off.data(), s->B.offset, sizeof(int) * (g.ntotal + 1), cudaMemcpyDeviceToHost,
+                                  s->stream));
+        PMPM_CUDA(cudaStreamSynchronize(s->stream));
+      }
       for (int c = 0; c < g.ntotal; c++) {
         const bool occupied = off[c + 1] > off[c];
         host[c] = occupied ? (field == PMPM_FIELD_CELL_START ? off[c] : off[c + 1]) : 0;

@@ -59,8 +59,9 @@ struct DevParticles {
   float *x, *v, *F, *sig, *L, *m, *V, *V0, *fext, *eps, *sref;
   uint8_t *color, *active, *rigid;
   int *id;             // original particle id of each storage slot
-  unsigned int *hash;  // cell hash of the last partition
-  int *slot;           // rank inside the cell from the counting pass (-1: not binned)
+  unsigned int *hash;  // reference cell hash of the last partition
+  int *slot;           // rank inside the key bin from the counting pass (-1: not binned)
+  unsigned int *key;   // binning key of the last partition (scratch)
 };
 
 struct DevNodes {
@@ -69,8 +70,15 @@ struct DevNodes {
 };
 
 struct DevBins {
-  int *count;       // per cell, zero between steps
-  int *offset;      // exclusive prefix, ntotal + 1 entries
+  // Binning key space.  Reference mode: the reference cell hash (key grid =
+  // node grid).  Dual mode (quadratic fast path): the dual cell
+  // floor(x/h + 1/2), whose particles share one 3x3x3 node window; key grid =
+  // node grid + 1 per axis.
+  int dual;
+  int kd[3];
+  int nkeys;
+  int *count;       // per key, zero between steps
+  int *offset;      // exclusive prefix, nkeys + 1 entries
   int *order;       // sorted position -> storage slot
   int *block_sums;  // scan scratch
   int *scalars;     // [0] binned count, [1] unbinned counter, [2] big-cell count

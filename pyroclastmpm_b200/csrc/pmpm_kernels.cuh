@@ -94,6 +94,26 @@ __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], un
   }
 }
 
+// Dual binning: the particle's nodes are d - 1 .. d + 1 (clamped) per axis.
+template <int D>
+__device__ __forceinline__ void mark_tiles_dual(const StepArgs &a, const int d[3]) {
+  using T = TileDims<D>;
+  const DevGrid &g = a.g;
+  const int tsz[3] = {T::X, T::Y, T::Z};
+  int tlo[3] = {0, 0, 0}, thi[3] = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    tlo[c] = max(d[c] - 1, 0) / tsz[c];
+    thi[c] = min(d[c] + 1, g.n[c] - 1) / tsz[c];
+  }
+  for (int tz = tlo[2]; tz <= thi[2]; tz++)
+    for (int ty = tlo[1]; ty <= thi[1]; ty++)
+      for (int tx = tlo[0]; tx <= thi[0]; tx++) {
+        const int t = tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
+        if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+      }
+}
+
 // apply_planardomain (src/boundaryconditions/planardomain_inline.h:56-138).
 template <int D>
 __device__ __forceinline__ void planar_force(const StepArgs &a, int s, const float x[3]) {
@@ -129,26 +149,44 @@ __device__ __forceinline__ void planar_force(const StepArgs &a, int s, const flo
   for (int c = 0; c < D; c++) P.fext[c * P.stride + s] = f[c];
 }
 
+// Dual cell of a quadratic particle: the first of its three nodes plus one,
+// chosen with the same comparison as the G2P window (frac < 1/2 -> b - 1).
+__device__ __forceinline__ int dual_coord(float u, int b) { return (u - (float)(b - 1)) < 1.5f ? b : b + 1; }
+
 template <int D, int SF>
 __global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.P.n) return;
   const DevGrid &g = a.g;
-  float x[3] = {0.0f, 0.0f, 0.0f};
+  float x[3] = {0.0f, 0.0f, 0.0f}, u[3] = {0.0f, 0.0f, 0.0f};
   int b[3] = {0, 0, 0};
   bool in_axes = true;
 #pragma unroll
   for (int c = 0; c < D; c++) {
     x[c] = a.P.x[c * a.P.stride + s];
-    b[c] = (int)scaled_coord(x[c], g.origin[c], g.inv_h);
+    u[c] = scaled_coord(x[c], g.origin[c], g.inv_h);
+    b[c] = (int)u[c];
     in_axes = in_axes && b[c] >= 0 && b[c] < g.n[c];
   }
   const unsigned hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
   a.P.hash[s] = hu;
-  const bool binned = hu < (unsigned)g.ntotal;
-  a.P.slot[s] = binned ? atomicAdd(&a.B.count[hu], 1) : -1;
+  bool binned;
+  unsigned key;
+  if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual) {
+    int d[3] = {0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < D; c++) d[c] = dual_coord(u[c], b[c]);
+    key = (unsigned)(d[0] + d[1] * a.B.kd[0] + d[2] * a.B.kd[0] * a.B.kd[1]);
+    binned = in_axes;
+    if (in_axes) mark_tiles_dual<D>(a, d);
+  } else {
+    key = hu;
+    binned = hu < (unsigned)g.ntotal;
+    mark_tiles<D, SF>(a, b, hu, binned, in_axes);
+  }
+  a.P.key[s] = key;
+  a.P.slot[s] = binned ? atomicAdd(&a.B.count[key], 1) : -1;
   if (!binned || (SF == PMPM_SHAPE_QUADRATIC && !in_axes)) atomicOr(a.fault, kFaultOutOfDomain);
-  mark_tiles<D, SF>(a, b, hu, binned, in_axes);
   if (a.has_planar) planar_force<D>(a, s, x);
 }
 
@@ -244,7 +282,7 @@ __global__ void __launch_bounds__(256) k_scatter(StepArgs a) {
   if (s >= a.P.n) return;
   const int slot = a.P.slot[s];
   if (slot >= 0) {
-    a.B.order[a.B.offset[a.P.hash[s]] + slot] = s;
+    a.B.order[a.B.offset[a.P.key[s]] + slot] = s;
   } else {
     int k = atomicAdd(&a.B.scalars[1], 1);
     a.B.order[a.B.scalars[0] + k] = s;
@@ -257,7 +295,7 @@ constexpr int kBigCell = 2048;
 // Orders each cell's particles by id; cells above kSmallCell go to k_sort_big.
 __global__ void __launch_bounds__(256) k_sort_cells(StepArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.g.ntotal) return;
+  if (c >= a.B.nkeys) return;
   const int lo = a.B.offset[c], hi = a.B.offset[c + 1];
   const int cnt = hi - lo;
   if (cnt < 2) return;
@@ -1133,6 +1171,279 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
     a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
     a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
   }
+}
+
+// --------------------------------------------------------------------------
+// P2G, 3D quadratic fast path: dual-cell z-sweep
+// --------------------------------------------------------------------------
+//
+// Particles are binned by dual cell d = floor(x/h + 1/2), so every particle
+// of a dual cell has the same three nodes d - 1 .. d + 1 per axis (clamped
+// onto the grid: the boundary fold of the quadratic spline) and every
+// (particle, node) pair the sweep visits carries weight.  Work item = (x
+// pair, y pair), a pair being (dual source column, node offset 0..2) whose
+// target lies in the tile; items sweep the dual layers along z with a
+// three-node register window, as k_p2g_sweep3.
+
+struct Dual3 {
+  using T = TileDims<3>;
+  static constexpr int NS = T::X + 2;   // dual sources per axis
+  static constexpr int MAXPAIR = NS * 3;
+  static constexpr int NCELL = NS * NS;
+  static constexpr int CAP = 1024;
+  static constexpr int SLOTS = CAP + NCELL;
+  static constexpr int NT = 320;        // threads (10 warps)
+  static constexpr int IPT = 2;         // items per thread per round
+};
+
+constexpr int dual3_smem_bytes() { return (7 * TileDims<3>::N + Dual3::SLOTS * (2 + 1 + 3 + 3 + 6 + 6)) * 4; }
+
+__device__ __forceinline__ int build_dual_pairs(int t0, int n, int *pairs) {
+  int cnt = 0;
+  for (int si = 0; si < Dual3::NS; si++) {
+    const int src = t0 - 1 + si;
+    if (src < 0 || src > n) continue;  // dual coordinates run 0 .. n
+    for (int i = 0; i < 3; i++) {
+      const int t = min(max(src - 1 + i, 0), n - 1);
+      const int l = t - t0;
+      if (l < 0 || l >= TileDims<3>::X) continue;
+      pairs[cnt++] = si | (i << 8) | (l << 12);
+    }
+  }
+  return cnt;
+}
+
+// Node epilogue for the nodes of a tile from shared accumulators acc[7][512]:
+// the reference leaves nodes with m <= cutoff at their reset value (0).
+__device__ __forceinline__ void tile_epilogue3(const StepArgs &a, int apply_bcs, const int t0[3], const float *acc,
+                                               int tid, int nthreads) {
+  using T = TileDims<3>;
+  const DevGrid &g = a.g;
+  for (int ln = tid; ln < T::N; ln += nthreads) {
+    const int lx = ln % T::X, ly = (ln / T::X) % T::Y, lz = ln / (T::X * T::Y);
+    const int nc[3] = {t0[0] + lx, t0[1] + ly, t0[2] + lz};
+    if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) continue;
+    const int node = flat_index(g, nc[0], nc[1], nc[2]);
+    float mass = acc[ln];
+    float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+    const bool live = mass > a.cutoff;
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        p[c] = acc[(1 + c) * T::N + ln];
+        pnt[c] = p[c] + acc[(4 + c) * T::N + ln] * a.dt;
+      }
+    } else {
+      mass = 0.0f;
+    }
+    if (apply_bcs) node_bcs<3>(a, node, nc, mass, p, pnt);
+    const int nt = g.ntotal;
+    a.N.m[node] = mass;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      a.N.p[c * nt + node] = p[c];
+      a.N.pnt[c * nt + node] = pnt[c];
+      a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
+      a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
+  using W = Dual3;
+  using T = TileDims<3>;
+  constexpr int NT = W::NT;
+  constexpr int NN = T::N;  // nodes per tile
+  const DevGrid &g = a.g;
+  const int tile = blockIdx.x;
+  if (a.N.tile_epoch[tile] != a.epoch) return;
+
+  __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
+  __shared__ int npair[2];
+  __shared__ int cell_k0[W::NCELL], cell_pref[W::NCELL + 1];
+  __shared__ int warp_tmp[33];
+  extern __shared__ __align__(16) float dyn_smem[];
+  constexpr int SL = W::SLOTS;
+  float *acc = dyn_smem;                            // [7][NN]
+  float(*st_u)[SL] = (float(*)[SL])(acc + 7 * NN);  // [2] scaled x, y
+  float *st_m = (float *)(st_u + 2);                // [SL]
+  float(*st_mv)[SL] = (float(*)[SL])(st_m + SL);    // [3] m v
+  float(*st_f)[SL] = st_mv + 3;                     // [3] external force
+  float(*st_S)[SL] = st_f + 3;                      // [6] -V sigma
+  float(*st_nz)[SL] = st_S + 6;                     // [3] z weights of the layer's nodes
+  float(*st_dnz)[SL] = st_nz + 3;                   // [3]
+
+  const int tid = threadIdx.x;
+  const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
+                     (tile / (g.tdim[0] * g.tdim[1])) * T::Z};
+  for (int k = tid; k < 7 * NN; k += NT) acc[k] = 0.0f;
+  if (tid == 0) {
+    node_epoch[tile] = a.epoch;
+    npair[0] = build_dual_pairs(t0[0], g.n[0], pairs_x);
+  } else if (tid == 32) {
+    npair[1] = build_dual_pairs(t0[1], g.n[1], pairs_y);
+  }
+  __syncthreads();
+  const int nx = npair[0], ny = npair[1];
+  const int nitems = nx * ny;
+  const int nrounds = (nitems + NT * W::IPT - 1) / (NT * W::IPT);
+  const int dz_lo = max(t0[2] - 1, 0), dz_hi = min(t0[2] + T::Z, g.n[2]);
+  const DevParticles &P = a.P;
+  const int st = P.stride;
+  const int kd0 = a.B.kd[0];
+  const long long kd01 = (long long)a.B.kd[0] * a.B.kd[1];
+
+  for (int round = 0; round < nrounds; round++) {
+    int item_cell[W::IPT], item_tl[W::IPT];
+    float item_xn[W::IPT], item_yn[W::IPT];  // virtual target node coordinates
+    bool item_ok[W::IPT];
+    float win[W::IPT][3][7];
+#pragma unroll
+    for (int q = 0; q < W::IPT; q++) {
+      const int it = (round * W::IPT + q) * NT + tid;
+      item_ok[q] = it < nitems;
+      const int px = item_ok[q] ? pairs_x[it % nx] : 0;
+      const int py = item_ok[q] ? pairs_y[it / nx] : 0;
+      item_cell[q] = pair_src(py) * W::NS + pair_src(px);
+      item_tl[q] = pair_tgt(px) + T::X * pair_tgt(py);
+      item_xn[q] = (float)(t0[0] - 1 + pair_src(px) - 1 + pair_off(px));
+      item_yn[q] = (float)(t0[1] - 1 + pair_src(py) - 1 + pair_off(py));
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int c = 0; c < 7; c++) win[q][k][c] = 0.0f;
+    }
+    for (int dz = dz_lo; dz <= dz_hi; dz++) {
+      // ---- the layer's dual source cells -> sorted ranges, prefix ----
+      {
+        const int vc = tid;
+        int cnt = 0, k0 = 0;
+        if (vc < W::NCELL) {
+          const int sx = t0[0] - 1 + vc % W::NS, sy = t0[1] - 1 + vc / W::NS;
+          if (sx >= 0 && sx <= g.n[0] && sy >= 0 && sy <= g.n[1]) {
+            const long long f = sx + (long long)sy * kd0 + (long long)dz * kd01;
+            k0 = a.B.offset[f];
+            cnt = a.B.offset[f + 1] - k0;
+          }
+          cell_k0[vc] = k0;
+        }
+        int total;
+        const int ex = block_exclusive_scan(cnt, warp_tmp, total);
+        if (vc < W::NCELL) cell_pref[vc] = ex;
+        if (tid == 0) cell_pref[W::NCELL] = total;
+      }
+      __syncthreads();
+      const int layer_n = cell_pref[W::NCELL];
+      for (int c0 = 0; c0 < layer_n; c0 += W::CAP) {
+        const int c1 = min(c0 + W::CAP, layer_n);
+        // ---- stage particles [c0, c1) ----
+        for (int j = c0 + tid; j < c1; j += NT) {
+          int lo = 0, hi = W::NCELL;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (cell_pref[mid] <= j) lo = mid; else hi = mid;
+          }
+          const int s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+          const int jj = j - c0 + lo;  // skewed slot: neighbouring cells start in different banks
+          const float ux = scaled_coord(P.x[s], g.origin[0], g.inv_h);
+          const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
+          const float uz = scaled_coord(P.x[2 * st + s], g.origin[2], g.inv_h);
+          const float m = P.m[s];
+          const float nv = -P.V[s];
+          st_u[0][jj] = ux;
+          st_u[1][jj] = uy;
+          st_m[jj] = m;
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            st_mv[c][jj] = m * P.v[c * st + s];
+            st_f[c][jj] = a.has_planar ? P.fext[c * st + s] : 0.0f;
+          }
+#pragma unroll
+          for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            float N, dN;
+            axis_weight<PMPM_SHAPE_QUADRATIC>(uz - (float)(dz - 1 + k), g.inv_h, 0, N, dN);
+            st_nz[k][jj] = N;
+            st_dnz[k][jj] = dN;
+          }
+        }
+        __syncthreads();
+        // ---- items: add their source cell's staged particles ----
+#pragma unroll
+        for (int q = 0; q < W::IPT; q++) {
+          if (!item_ok[q]) continue;
+          const int vc = item_cell[q];
+          const int j0 = max(cell_pref[vc], c0) - c0 + vc, j1 = min(cell_pref[vc + 1], c1) - c0 + vc;
+          const float xn = item_xn[q], yn = item_yn[q];
+          for (int j = j0; j < j1; j++) {
+            float Nx, dNx, Ny, dNy;
+            axis_weight<PMPM_SHAPE_QUADRATIC>(st_u[0][j] - xn, g.inv_h, 0, Nx, dNx);
+            axis_weight<PMPM_SHAPE_QUADRATIC>(st_u[1][j] - yn, g.inv_h, 0, Ny, dNy);
+            const float m = st_m[j];
+            const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
+            const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
+            const float nn = Nx * Ny;
+            const float gx = dNx * Ny, gy = Nx * dNy;
+            // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
+            const float Ax = st_f[0][j] * nn + Sxx * gx + Sxy * gy;
+            const float Ay = st_f[1][j] * nn + Sxy * gx + Syy * gy;
+            const float Az = st_f[2][j] * nn + Sxz * gx + Syz * gy;
+            const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
+            const float mn = m * nn, mvxn = st_mv[0][j] * nn, mvyn = st_mv[1][j] * nn, mvzn = st_mv[2][j] * nn;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
+              win[q][k][0] += mn * Nz;
+              win[q][k][1] += mvxn * Nz;
+              win[q][k][2] += mvyn * Nz;
+              win[q][k][3] += mvzn * Nz;
+              win[q][k][4] += Ax * Nz + Bx * dNz;
+              win[q][k][5] += Ay * Nz + By * dNz;
+              win[q][k][6] += Az * Nz + Bz * dNz;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      // ---- node dz - 1 gets nothing from later layers: flush, shift ----
+#pragma unroll
+      for (int q = 0; q < W::IPT; q++) {
+        if (item_ok[q]) {
+          const int tz = max(dz - 1, 0);
+          const int lz = tz - t0[2];
+          if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
+            const int ln = item_tl[q] + T::X * T::Y * lz;
+#pragma unroll
+            for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NN + ln], win[q][0][c]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 7; c++) {
+          win[q][0][c] = win[q][1][c];
+          win[q][1][c] = win[q][2][c];
+          win[q][2][c] = 0.0f;
+        }
+      }
+      __syncthreads();  // cell tables are rebuilt for the next layer
+    }
+#pragma unroll
+    for (int q = 0; q < W::IPT; q++) {
+      if (!item_ok[q]) continue;
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const int tz = min(dz_hi + k, g.n[2] - 1);
+        const int lz = tz - t0[2];
+        if (lz >= 0 && lz < T::Z) {
+          const int ln = item_tl[q] + T::X * T::Y * lz;
+#pragma unroll
+          for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NN + ln], win[q][k][c]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  tile_epilogue3(a, apply_bcs, t0, acc, tid, NT);
 }
 
 // --------------------------------------------------------------------------

@@ -141,9 +141,12 @@ def test_reference_vectors_particles(dim):
 # binning: bit-exact against the oracle (reference semantics)
 # ----------------------------------------------------------------------------
 
-@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("dim,sf", [(2, "linear"), (3, "linear"), (3, "quadratic")])
 @pytest.mark.parametrize("seed", [0, 1])
-def test_binning_bit_exact(dim, seed):
+def test_binning_bit_exact(dim, sf, seed):
+    """The reference partition views are bit-exact; with the 3D quadratic
+    fast path the step bins by dual cell and the views come from the stored
+    reference hashes."""
     rng = np.random.default_rng(seed)
     n = 20000 if dim == 3 else 5000
     x = rng.uniform(0.0, 1.0, size=(n, dim))
@@ -156,10 +159,10 @@ def test_binning_bit_exact(dim, seed):
     x[80:90] = 5.0
     x[90:200] = x[90]
     x[200:1000] = rng.uniform(0.3, 0.31, size=(800, dim))
-    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, 0.05)
+    sim = Simulation(dim, [0.0] * dim, [1.0] * dim, 0.05, shape_function=sf)
     sim.set_particles(x)
     sim.partition()
-    ref = oracle.OracleSim(dim, [0.0] * dim, [1.0] * dim, 0.05, x)
+    ref = oracle.OracleSim(dim, [0.0] * dim, [1.0] * dim, 0.05, x, shape_function=sf)
     ref.call("or_partition")
     for name in ("bins", "hash_unsorted", "hash_sorted", "sorted_index", "cell_start", "cell_end"):
         np.testing.assert_array_equal(sim.get(name), ref[name], err_msg=name)
