@@ -305,6 +305,27 @@ int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float d
                                const float *volumes, const float *volumes_original,
                                int velgrad_is_strain_increment, int device);
 
+/* Spatial partition that allocates no device memory.  No counterpart in the
+ * reference; it gives the results of pmpm_partition (reference hashing,
+ * stable sort, cell ranges) to callers that cannot allocate device memory at
+ * the point they need them, for example code running while a CUDA graph is
+ * being captured, code inside an allocator callback, or plug-ins held to a
+ * fixed memory budget.  The caller passes device pointers: positions
+ * [n][dim] (the particles in index order) in, and hash_unsorted [n],
+ * sorted_index [n] (binned particles), cell_start and cell_end [cells] out,
+ * with cells = num_cells[0] * num_cells[1] (* num_cells[2]).  Temporaries
+ * live in one fixed device array inside the library: at most 131072
+ * particles and 131072 cells (larger inputs return
+ * PMPM_ERR_INVALID_ARGUMENT).  The first call on a device looks up that
+ * array's address; make it before any stream capture.  Calls share the array,
+ * so calls that overlap on the GPU race: serialise them.  Waits for `stream`
+ * (cudaStream_t, may be NULL) before returning.  Returns
+ * PMPM_ERR_OUT_OF_DOMAIN when a particle lies outside the grid (the outputs
+ * then cover the particles inside it). */
+int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const int *num_cells,
+                           const float *positions, int num_particles, unsigned *hash_unsorted,
+                           int *sorted_index, int *cell_start, int *cell_end, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,7 +75,7 @@ EXPORTS = [
     "pmpm_num_nodes", "pmpm_field_bytes", "pmpm_partition", "pmpm_shape_functions",
     "pmpm_num_surround_nodes", "pmpm_p2g", "pmpm_g2p", "pmpm_stress_update", "pmpm_solve",
     "pmpm_get_step", "pmpm_set_step", "pmpm_synchronize", "pmpm_stream", "pmpm_material_point_update",
-    "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count",
+    "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
 ]
 
 _lib = None
@@ -129,6 +129,7 @@ def lib():
     L.pmpm_profile_step.argtypes = [vp, fp, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_active_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.pmpm_partition_noalloc.argtypes = [i, fp, f, ctypes.POINTER(ctypes.c_int), vp, i, vp, vp, vp, vp, vp]
     L.pmpm_material_point_update.argtypes = [ctypes.POINTER(Material), i, i, f, vp, vp, vp, vp, vp, vp, vp, i, i]
     _lib = L
     return L
