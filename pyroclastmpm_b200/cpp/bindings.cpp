@@ -1,0 +1,185 @@
+// pybind11 module with the reference's Python API (python/pybind/**): module
+// MPM2D or MPM3D (-DDIM), classes and argument names as the reference binds
+// them.  Arrays cross as numpy arrays (the reference returns lists of Eigen
+// vectors; np.asarray of either gives the same [n, dim] array).
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include "pyroclastmpm.hpp"
+
+namespace py = pybind11;
+using namespace pyroclastmpm;
+
+#if DIM == 2
+#define PMPM_MODULE MPM2D
+#else
+#define PMPM_MODULE MPM3D
+#endif
+
+namespace {
+
+using farr = py::array_t<float, py::array::c_style | py::array::forcecast>;
+using iarr = py::array_t<int, py::array::c_style | py::array::forcecast>;
+
+std::vector<float> flat(const py::object &o, size_t per) {
+  if (o.is_none()) return {};
+  farr a = farr::ensure(o);
+  if (!a) throw std::invalid_argument("expected an array of numbers");
+  if (a.size() == 0) return {};
+  if ((size_t)a.size() % per) throw std::invalid_argument("array size is not a multiple of the dimension");
+  return std::vector<float>(a.data(), a.data() + a.size());
+}
+std::vector<int> flati(const py::object &o) {
+  if (o.is_none()) return {};
+  iarr a = iarr::ensure(o);
+  if (!a || a.size() == 0) return {};
+  return std::vector<int>(a.data(), a.data() + a.size());
+}
+template <typename V>
+V vec(const py::object &o) {
+  V v{};
+  auto f = flat(o, 1);
+  for (size_t k = 0; k < v.size() && k < f.size(); k++) v[k] = (typename V::value_type)f[k];
+  return v;
+}
+template <typename T>
+py::array_t<T> to_array(const std::vector<T> &v, std::vector<py::ssize_t> shape) {
+  py::array_t<T> out(shape);
+  std::copy(v.begin(), v.end(), out.mutable_data());
+  return out;
+}
+
+}  // namespace
+
+PYBIND11_MODULE(PMPM_MODULE, m) {
+  m.doc() = "B200-native USL MPM step with the PyroclastMPM Python API";
+  m.attr("global_dimension") = DIM;
+
+  m.def("set_globals", &set_globals, py::arg("time_step"), py::arg("particles_per_cell"),
+        py::arg("shape_function") = "linear", py::arg("output_directory") = "./output/");
+  m.def("set_global_shapefunction", &set_global_shapefunction, py::arg("shapefunction") = "linear");
+  m.def("set_global_timestep", &set_global_timestep, py::arg("timestep"));
+  m.def("set_global_step", &set_global_step, py::arg("step"));
+  m.def("set_global_output_directory", &set_global_output_directory, py::arg("directory"));
+
+  py::class_<NodesContainer>(m, "NodesContainer")
+      .def(py::init([](py::object o, py::object e, float h) {
+             return NodesContainer(vec<Vectorr>(o), vec<Vectorr>(e), h);
+           }),
+           py::arg("origin"), py::arg("end"), py::arg("cell_size"))
+      .def("give_coords", [](const NodesContainer &n) {
+        return to_array(n.give_coords(), {n.num_cells_total, DIM});
+      })
+      .def_property_readonly("num_cells", [](const NodesContainer &n) { return n.num_cells; })
+      .def_property_readonly("num_cells_total", [](const NodesContainer &n) { return n.num_cells_total; })
+      .def_property_readonly("masses", [](const NodesContainer &n) { return to_array(n.masses(), {n.num_cells_total}); })
+      .def_property_readonly("moments",
+                             [](const NodesContainer &n) { return to_array(n.moments(), {n.num_cells_total, DIM}); })
+      .def_property_readonly("moments_nt", [](const NodesContainer &n) {
+        return to_array(n.moments_nt(), {n.num_cells_total, DIM});
+      })
+      .def("set_output_formats", [](NodesContainer &, const std::vector<std::string> &) {}, py::arg("output_formats"));
+
+  auto P = py::class_<ParticlesContainer>(m, "ParticlesContainer", py::dynamic_attr());
+  P.def(py::init([](py::object pos, py::object vel, py::object col, py::object rpos, py::object rvel, py::object rcol) {
+          return ParticlesContainer(flat(pos, DIM), flat(vel, DIM), flati(col), flat(rpos, DIM), flat(rvel, DIM),
+                                    flati(rcol));
+        }),
+        py::arg("positions"), py::arg("velocities") = py::none(), py::arg("colors") = py::none(),
+        py::arg("rigid_positions") = py::none(), py::arg("rigid_velocities") = py::none(),
+        py::arg("rigid_colors") = py::none());
+  P.def_readonly("num_particles", &ParticlesContainer::num_particles);
+  P.def("set_output_formats", [](ParticlesContainer &, const std::vector<std::string> &) {}, py::arg("output_formats"));
+#define PMPM_PROP(NAME, ID, NCOMP, ...)                                                              \
+  P.def_property(                                                                                   \
+      NAME,                                                                                         \
+      [](ParticlesContainer &p) { return to_array(p.get<float>(ID, NCOMP), {__VA_ARGS__}); },       \
+      [](ParticlesContainer &p, py::object v) { p.set<float>(ID, flat(v, 1), NCOMP); })
+  PMPM_PROP("positions", PMPM_FIELD_POSITIONS, DIM, p.num_particles, DIM);
+  PMPM_PROP("velocities", PMPM_FIELD_VELOCITIES, DIM, p.num_particles, DIM);
+  PMPM_PROP("stresses", PMPM_FIELD_STRESSES, 9, p.num_particles, 3, 3);
+  PMPM_PROP("F", PMPM_FIELD_F, DIM * DIM, p.num_particles, DIM, DIM);
+  PMPM_PROP("velocity_gradient", PMPM_FIELD_VELOCITY_GRADIENT, DIM * DIM, p.num_particles, DIM, DIM);
+  PMPM_PROP("masses", PMPM_FIELD_MASSES, 1, p.num_particles);
+  PMPM_PROP("volumes", PMPM_FIELD_VOLUMES, 1, p.num_particles);
+  PMPM_PROP("volumes_original", PMPM_FIELD_VOLUMES_ORIGINAL, 1, p.num_particles);
+#undef PMPM_PROP
+  P.def_property(
+      "colors",
+      [](ParticlesContainer &p) {
+        auto c = p.get<unsigned char>(PMPM_FIELD_COLORS, 1);
+        return to_array(std::vector<int>(c.begin(), c.end()), {p.num_particles});
+      },
+      [](ParticlesContainer &p, py::object v) {
+        auto c = flati(v);
+        p.set<unsigned char>(PMPM_FIELD_COLORS, std::vector<unsigned char>(c.begin(), c.end()), 1);
+      });
+
+  py::class_<Material>(m, "Material", py::dynamic_attr()).def(py::init<>()).def_readwrite("density", &Material::density);
+  py::class_<LinearElastic>(m, "LinearElastic", py::dynamic_attr())
+      .def(py::init<float, float, float>(), py::arg("density"), py::arg("E"), py::arg("pois") = 0.0f)
+      .def_readonly("E", &LinearElastic::E)
+      .def_readonly("pois", &LinearElastic::pois)
+      .def_readonly("shear_modulus", &LinearElastic::shear_modulus)
+      .def_readonly("lame_modulus", &LinearElastic::lame_modulus)
+      .def_readonly("bulk_modulus", &LinearElastic::bulk_modulus)
+      .def_readwrite("density", &LinearElastic::density)
+      .def_readwrite("corrected", &LinearElastic::corrected);
+  py::class_<NewtonFluid>(m, "NewtonFluid", py::dynamic_attr())
+      .def(py::init<float, float, float, float>(), py::arg("density"), py::arg("viscosity"),
+           py::arg("bulk_modulus") = 0.0f, py::arg("gamma") = 7.0f)
+      .def_readwrite("density", &NewtonFluid::density)
+      .def_readwrite("viscosity", &NewtonFluid::viscosity)
+      .def_readwrite("bulk_modulus", &NewtonFluid::bulk_modulus)
+      .def_readwrite("gamma", &NewtonFluid::gamma);
+  py::class_<DruckerPrager>(m, "DruckerPrager", py::dynamic_attr())
+      .def(py::init<float, float, float, float, float, float>(), py::arg("density"), py::arg("E"),
+           py::arg("pois") = 0.0f, py::arg("friction_angle") = 30.0f, py::arg("dilatancy_angle") = 0.0f,
+           py::arg("cohesion") = 0.0f)
+      .def_readwrite("density", &DruckerPrager::density);
+
+  py::class_<BoundaryCondition>(m, "BoundaryCondition").def(py::init<>());
+  py::class_<Gravity>(m, "Gravity", py::dynamic_attr())
+      .def(py::init([](py::object g, bool is_ramp, int ramp_step, py::object ge) {
+             return Gravity(vec<Vectorr>(g), is_ramp, ramp_step, vec<Vectorr>(ge));
+           }),
+           py::arg("gravity"), py::arg("is_ramp") = false, py::arg("ramp_step") = 0,
+           py::arg("gravity_end") = py::none())
+      .def_readwrite("gravity", &Gravity::gravity);
+  py::class_<NodeDomain>(m, "NodeDomain", py::dynamic_attr())
+      .def(py::init([](py::object f0, py::object f1) { return NodeDomain(vec<Vectori>(f0), vec<Vectori>(f1)); }),
+           py::arg("face0_mode") = py::none(), py::arg("face1_mode") = py::none());
+  py::class_<BodyForce>(m, "BodyForce", py::dynamic_attr())
+      .def(py::init([](const std::string &mode, py::object values, py::object mask) {
+             auto mk = flati(mask);
+             return BodyForce(mode, flat(values, DIM), std::vector<bool>(mk.begin(), mk.end()));
+           }),
+           py::arg("mode"), py::arg("values"), py::arg("mask"))
+      .def_readwrite("isActive", &BodyForce::isActive);
+  py::class_<PlanarDomain>(m, "PlanarDomain", py::dynamic_attr())
+      .def(py::init([](py::object f0, py::object f1) { return PlanarDomain(vec<Vectorr>(f0), vec<Vectorr>(f1)); }),
+           py::arg("face0_friction") = py::none(), py::arg("face1_friction") = py::none());
+
+  py::class_<Solver>(m, "Solver")
+      .def(py::init<ParticlesContainer, NodesContainer, std::vector<MaterialType>, std::vector<BoundaryConditionType>>(),
+           py::arg("particles"), py::arg("nodes"), py::arg("materials") = std::vector<MaterialType>(),
+           py::arg("boundaryconditions") = std::vector<BoundaryConditionType>())
+      .def("run", &Solver::run, py::arg("total_steps"), py::arg("output_frequency"))
+      .def("solve", &Solver::solve)
+      .def("solve_nsteps", &Solver::solve_nsteps, py::arg("n_steps"))
+      .def("stress_update", &Solver::stress_update)
+      .def_property_readonly("current_step", &Solver::current_step)
+      .def_readwrite("particles", &Solver::particles)
+      .def_readwrite("nodes", &Solver::nodes);
+  py::class_<USL, Solver>(m, "USL")
+      .def(py::init<ParticlesContainer, NodesContainer, std::vector<MaterialType>, std::vector<BoundaryConditionType>,
+                    float, unsigned>(),
+           py::arg("particles"), py::arg("nodes"), py::arg("materials") = std::vector<MaterialType>(),
+           py::arg("boundaryconditions") = std::vector<BoundaryConditionType>(), py::arg("alpha") = 0.99f,
+           py::arg("flags") = 0u)
+      .def("partition", &USL::partition)
+      .def("P2G", &USL::P2G)
+      .def("G2P", &USL::G2P)
+      .def_readonly("alpha", &USL::alpha);
+}

@@ -1,0 +1,397 @@
+// Drop-in C++ classes with the reference's names and interfaces (one
+// dimension per build, -DDIM=2 or 3, as the reference builds MPM2D / MPM3D).
+// They are host views over the C ABI in pmpm.h: containers hold host arrays
+// until a solver binds them, after which their fields read and write the
+// device state of the solver's simulation handle.
+//
+//   set_globals            src/common/global_settings.cpp:161-176
+//   NodesContainer         include/pyroclastmpm/nodes/nodes.h:73-144
+//   ParticlesContainer     include/pyroclastmpm/particles/particles.h:94-271
+//   LinearElastic, NewtonFluid, Material    include/pyroclastmpm/materials/*.h
+//   Gravity, NodeDomain, BodyForce, PlanarDomain  include/pyroclastmpm/boundaryconditions/*.h
+//   Solver, USL            include/pyroclastmpm/solver/{solver.h,usl/usl.h}
+//
+// Vectors are std::array (the reference uses Eigen fixed-size matrices).
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <variant>
+#include <vector>
+
+#include "pmpm.h"
+
+#ifndef DIM
+#define DIM 3
+#endif
+
+namespace pyroclastmpm {
+// the 2D and 3D builds are distinct C++ types (both modules may be loaded in
+// one process), as the reference's per-DIM libraries are
+#if DIM == 2
+inline namespace dim2 {
+#else
+inline namespace dim3 {
+#endif
+
+using Real = float;
+using Vectorr = std::array<Real, DIM>;
+using Vectori = std::array<int, DIM>;
+using Matrixr = std::array<Real, DIM * DIM>;
+using Matrix3r = std::array<Real, 9>;
+
+inline void check(int status, const char *what) {
+  if (status != PMPM_OK) throw std::runtime_error(std::string(what) + ": " + pmpm_status_string(status));
+}
+
+// ---------------------------------------------------------------------------
+// globals (per process, read when a solver is constructed, as the reference)
+// ---------------------------------------------------------------------------
+struct Globals {
+  Real dt = 0.0f;
+  int particles_per_cell = 1;
+  int shape_function = PMPM_SHAPE_LINEAR;
+  int step = 0;
+  std::string output_directory = "./output/";
+};
+inline Globals &globals() {
+  static Globals g;
+  return g;
+}
+inline int shape_function_id(const std::string &name) {
+  if (name == "linear") return PMPM_SHAPE_LINEAR;
+  if (name == "quadratic") return PMPM_SHAPE_QUADRATIC;
+  if (name == "cubic") return PMPM_SHAPE_CUBIC;
+  throw std::invalid_argument("shape function must be \"linear\", \"quadratic\" or \"cubic\"");
+}
+inline void set_global_shapefunction(const std::string &name) { globals().shape_function = shape_function_id(name); }
+inline void set_global_timestep(Real dt) { globals().dt = dt; }
+inline void set_global_step(int step) { globals().step = step; }
+inline void set_global_particles_per_cell(int ppc) { globals().particles_per_cell = ppc; }
+inline void set_global_output_directory(const std::string &dir) { globals().output_directory = dir; }
+inline void set_globals(Real dt, int ppc, const std::string &shape, const std::string &dir) {
+  set_global_timestep(dt);
+  set_global_shapefunction(shape);
+  set_global_output_directory(dir);
+  set_global_particles_per_cell(ppc);
+}
+
+// the simulation handle shared by a solver and the containers bound to it
+struct SimHandle {
+  pmpm_sim *sim = nullptr;
+  ~SimHandle() {
+    if (sim) pmpm_destroy(sim);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// nodes
+// ---------------------------------------------------------------------------
+class NodesContainer {
+ public:
+  NodesContainer() = default;
+  NodesContainer(const Vectorr &origin, const Vectorr &end, Real cell_size)
+      : origin(origin), end(end), cell_size(cell_size) {
+    // Grid ctor (include/pyroclastmpm/common/types_common.h:260-272)
+    num_cells_total = 1;
+    for (int a = 0; a < DIM; a++) {
+      num_cells[a] = (int)((end[a] - origin[a]) / cell_size) + 1;
+      num_cells_total *= num_cells[a];
+    }
+  }
+  Vectorr origin{}, end{};
+  Real cell_size = 1.0f;
+  Vectori num_cells{};
+  int num_cells_total = 0;
+  std::shared_ptr<SimHandle> handle;
+
+  std::vector<Real> field(int id, int ncomp) const {
+    std::vector<Real> out((size_t)num_cells_total * ncomp, 0.0f);
+    if (handle) check(pmpm_get_field(handle->sim, id, out.data(), out.size() * sizeof(Real), 0), "nodes field");
+    return out;
+  }
+  std::vector<Real> masses() const { return field(PMPM_FIELD_NODE_MASSES, 1); }
+  std::vector<Real> moments() const { return field(PMPM_FIELD_NODE_MOMENTS, DIM); }
+  std::vector<Real> moments_nt() const { return field(PMPM_FIELD_NODE_MOMENTS_NT, DIM); }
+  // give_node_coords (src/nodes/nodes.cpp:190-205): x-fastest
+  std::vector<Real> give_coords() const {
+    std::vector<Real> out((size_t)num_cells_total * DIM);
+    for (int i = 0; i < num_cells_total; i++) {
+      int rem = i;
+      for (int a = 0; a < DIM; a++) {
+        const int id = rem % num_cells[a];
+        rem /= num_cells[a];
+        out[(size_t)i * DIM + a] = origin[a] + (Real)id * cell_size;
+      }
+    }
+    return out;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// particles
+// ---------------------------------------------------------------------------
+class ParticlesContainer {
+ public:
+  ParticlesContainer() = default;
+  ParticlesContainer(const std::vector<Real> &positions, const std::vector<Real> &velocities,
+                     const std::vector<int> &colors, const std::vector<Real> &rigid_positions,
+                     const std::vector<Real> &rigid_velocities, const std::vector<int> &rigid_colors)
+      : positions_(positions), velocities_(velocities), rigid_positions_(rigid_positions),
+        rigid_velocities_(rigid_velocities) {
+    for (int c : colors) colors_.push_back((unsigned char)c);
+    for (int c : rigid_colors) rigid_colors_.push_back((unsigned char)c);
+    num_particles = (int)((positions.size() + rigid_positions.size()) / DIM);
+  }
+  int num_particles = 0;
+  std::shared_ptr<SimHandle> handle;
+  // host values set before a solver exists (applied when it binds)
+  std::vector<std::pair<int, std::vector<unsigned char>>> pending;
+
+  std::vector<Real> positions_, velocities_, rigid_positions_, rigid_velocities_;
+  std::vector<unsigned char> colors_, rigid_colors_;
+
+  template <typename T>
+  std::vector<T> get(int id, size_t ncomp) const {
+    std::vector<T> out((size_t)num_particles * ncomp);
+    if (!handle) throw std::runtime_error("the container is not bound to a solver yet");
+    check(pmpm_get_field(handle->sim, id, out.data(), out.size() * sizeof(T), 0), "particles field");
+    return out;
+  }
+  template <typename T>
+  void set(int id, const std::vector<T> &v, size_t ncomp) {
+    if (v.size() != (size_t)num_particles * ncomp) throw std::invalid_argument("wrong number of values");
+    if (!handle) {
+      std::vector<unsigned char> raw((const unsigned char *)v.data(), (const unsigned char *)(v.data() + v.size()));
+      pending.emplace_back(id, raw);
+      return;
+    }
+    check(pmpm_set_field(handle->sim, id, v.data(), v.size() * sizeof(T), 0), "particles field");
+  }
+  void apply_pending() {
+    for (auto &kv : pending) check(pmpm_set_field(handle->sim, kv.first, kv.second.data(), kv.second.size(), 0), "set");
+    pending.clear();
+  }
+};
+
+// ---------------------------------------------------------------------------
+// materials and boundary conditions
+// ---------------------------------------------------------------------------
+struct Material {
+  Real density = 0.0f;
+  pmpm_material desc() const {
+    pmpm_material m{};
+    m.type = PMPM_MAT_NONE;
+    m.density = density;
+    return m;
+  }
+};
+struct LinearElastic {
+  LinearElastic(Real density, Real E, Real pois) : density(density), E(E), pois(pois) {
+    // LinearElastic::LinearElastic (src/materials/linearelastic.cpp:47-58)
+    bulk_modulus = E / (3.0f * (1.0f - 2.0f * pois));
+    shear_modulus = E / (2.0f * (1.0f + pois));
+    lame_modulus = E * pois / ((1.0f + pois) * (1.0f - 2.0f * pois));
+  }
+  Real density, E, pois, bulk_modulus, shear_modulus, lame_modulus;
+  bool corrected = false;
+  pmpm_material desc() const {
+    pmpm_material m;
+    check(pmpm_material_linear_elastic(density, E, pois, corrected ? 1 : 0, &m), "LinearElastic");
+    return m;
+  }
+};
+struct NewtonFluid {
+  NewtonFluid(Real density, Real viscosity, Real bulk_modulus, Real gamma)
+      : density(density), viscosity(viscosity), bulk_modulus(bulk_modulus), gamma(gamma) {}
+  Real density, viscosity, bulk_modulus, gamma;
+  pmpm_material desc() const {
+    pmpm_material m;
+    check(pmpm_material_newton_fluid(density, viscosity, bulk_modulus, gamma, &m), "NewtonFluid");
+    return m;
+  }
+};
+struct DruckerPrager {
+  DruckerPrager(Real density, Real E, Real pois, Real friction_angle, Real dilatancy_angle, Real cohesion)
+      : density(density), E(E), pois(pois), friction_angle(friction_angle), dilatancy_angle(dilatancy_angle),
+        cohesion(cohesion) {}
+  Real density, E, pois, friction_angle, dilatancy_angle, cohesion;
+  pmpm_material desc() const {
+    pmpm_material m;
+    check(pmpm_material_drucker_prager(density, E, pois, friction_angle, dilatancy_angle, cohesion, &m),
+          "DruckerPrager");
+    return m;
+  }
+};
+using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager>;
+
+struct BoundaryCondition {
+  bool isActive = true;
+  pmpm_bc desc(int) const {
+    pmpm_bc b{};
+    b.type = PMPM_BC_NODEDOMAIN;  // a NodeDomain with no constrained faces is inert
+    for (int k = 0; k < 6; k++) b.ints[k] = -1;
+    return b;
+  }
+};
+struct Gravity {
+  Gravity(const Vectorr &gravity, bool is_ramp, int ramp_step, const Vectorr &gravity_end)
+      : gravity(gravity), is_ramp(is_ramp), ramp_step(ramp_step), gravity_end(gravity_end) {}
+  Vectorr gravity;
+  bool is_ramp;
+  int ramp_step;
+  Vectorr gravity_end;
+  pmpm_bc desc(int) const {
+    pmpm_bc b;
+    check(pmpm_bc_gravity(gravity.data(), is_ramp ? 1 : 0, ramp_step, gravity_end.data(), DIM, &b), "Gravity");
+    return b;
+  }
+};
+struct NodeDomain {
+  NodeDomain(const Vectori &face0_mode, const Vectori &face1_mode) : face0_mode(face0_mode), face1_mode(face1_mode) {}
+  Vectori face0_mode, face1_mode;
+  pmpm_bc desc(int) const {
+    pmpm_bc b;
+    check(pmpm_bc_nodedomain(face0_mode.data(), face1_mode.data(), DIM, &b), "NodeDomain");
+    return b;
+  }
+};
+struct BodyForce {
+  BodyForce(const std::string &mode, const std::vector<Real> &values, const std::vector<bool> &mask)
+      : values(values) {
+    // BodyForce::BodyForce (src/boundaryconditions/bodyforce.cpp:44-61)
+    mode_id = mode == "forces" ? 0 : (mode == "moments" ? 1 : (mode == "fixed" ? 2 : -1));
+    if (mode_id < 0) throw std::invalid_argument("mode must be \"forces\", \"moments\" or \"fixed\"");
+    for (bool m : mask) this->mask.push_back(m ? 1 : 0);
+  }
+  int mode_id;
+  bool isActive = true;
+  std::vector<Real> values;
+  std::vector<unsigned char> mask;
+  pmpm_bc desc(int num_nodes) const {
+    if (values.size() != (size_t)num_nodes * DIM || mask.size() != (size_t)num_nodes)
+      throw std::invalid_argument("BodyForce values/mask do not match the node count");
+    pmpm_bc b;
+    check(pmpm_bc_bodyforce(mode_id, values.data(), mask.data(), &b), "BodyForce");
+    b.ints[1] = isActive ? 1 : 0;
+    return b;
+  }
+};
+struct PlanarDomain {
+  PlanarDomain(const Vectorr &face0_friction, const Vectorr &face1_friction)
+      : face0_friction(face0_friction), face1_friction(face1_friction) {}
+  Vectorr face0_friction, face1_friction;  // degrees
+  pmpm_bc desc(int) const {
+    pmpm_bc b;
+    check(pmpm_bc_planardomain(face0_friction.data(), face1_friction.data(), DIM, &b), "PlanarDomain");
+    return b;
+  }
+};
+using BoundaryConditionType = std::variant<BoundaryCondition, Gravity, NodeDomain, BodyForce, PlanarDomain>;
+
+// ---------------------------------------------------------------------------
+// solvers
+// ---------------------------------------------------------------------------
+class Solver {
+ public:
+  Solver(const ParticlesContainer &p, const NodesContainer &n, const std::vector<MaterialType> &mats,
+         const std::vector<BoundaryConditionType> &bcs, Real alpha = 0.99f, unsigned flags = 0)
+      : nodes(n), particles(p), materials(mats), boundaryconditions(bcs) {
+    // Solver::Solver (src/solver/solver.cpp:69-104): copies, partition,
+    // initial volumes and masses
+    pmpm_desc d{};
+    d.dim = DIM;
+    for (int a = 0; a < DIM; a++) {
+      d.origin[a] = nodes.origin[a];
+      d.end[a] = nodes.end[a];
+    }
+    d.cell_size = nodes.cell_size;
+    d.shape_function = globals().shape_function;
+    d.dt = globals().dt;
+    d.particles_per_cell = globals().particles_per_cell;
+    d.alpha = alpha;
+    d.flags = flags | PMPM_FLAG_KEEP_VELOCITY_GRADIENT;
+    d.resort_interval = 32;
+    std::vector<pmpm_material> md;
+    for (auto &m : materials) md.push_back(std::visit([](auto &x) { return x.desc(); }, m));
+    std::vector<pmpm_bc> bd;
+    for (auto &b : boundaryconditions) bd.push_back(std::visit([&](auto &x) { return x.desc(nodes.num_cells_total); }, b));
+    d.num_materials = (int)md.size();
+    d.materials = md.data();
+    d.num_bcs = (int)bd.size();
+    d.bcs = bd.data();
+    handle = std::make_shared<SimHandle>();
+    check(pmpm_create(&d, &handle->sim), "pmpm_create");
+    const int D = DIM;
+    const int nrig = (int)(particles.rigid_positions_.size() / D);
+    const int nnon = (int)(particles.positions_.size() / D);
+    check(pmpm_set_particles(handle->sim, nnon, particles.positions_.empty() ? nullptr : particles.positions_.data(),
+                             particles.velocities_.empty() ? nullptr : particles.velocities_.data(),
+                             particles.colors_.empty() ? nullptr : particles.colors_.data(), nrig,
+                             particles.rigid_positions_.empty() ? nullptr : particles.rigid_positions_.data(),
+                             particles.rigid_velocities_.empty() ? nullptr : particles.rigid_velocities_.data(),
+                             particles.rigid_colors_.empty() ? nullptr : particles.rigid_colors_.data()),
+          "pmpm_set_particles");
+    particles.handle = handle;
+    nodes.handle = handle;
+    particles.apply_pending();
+    check(pmpm_set_step(handle->sim, globals().step), "pmpm_set_step");
+    check(pmpm_initialize(handle->sim), "pmpm_initialize");
+  }
+  virtual ~Solver() = default;
+
+  // USL::solve + increment_global
+  virtual void solve() {
+    check(pmpm_solve(handle->sim, 1), "solve");
+    sync_step();
+  }
+  // Solver::solve_nsteps (src/solver/solver.cpp:125-134)
+  void solve_nsteps(int n) {
+    check(pmpm_solve(handle->sim, n), "solve_nsteps");
+    sync_step();
+  }
+  // Solver::run (src/solver/solver.cpp:140-174): total_steps + 1 solves
+  void run(int total_steps, int output_frequency) {
+    (void)output_frequency;  // output writers are outside this path
+    check(pmpm_solve(handle->sim, total_steps + 1), "run");
+    sync_step();
+  }
+  void stress_update() { check(pmpm_stress_update(handle->sim), "stress_update"); }
+  int status() { return pmpm_synchronize(handle->sim); }
+  int current_step() const {
+    int s = 0;
+    check(pmpm_get_step(handle->sim, &s), "step");
+    return s;
+  }
+
+  NodesContainer nodes;
+  ParticlesContainer particles;
+  std::vector<MaterialType> materials;
+  std::vector<BoundaryConditionType> boundaryconditions;
+  std::shared_ptr<SimHandle> handle;
+
+ protected:
+  void sync_step() {
+    globals().step = current_step();
+    const int st = pmpm_synchronize(handle->sim);
+    if (st != PMPM_OK && st != PMPM_ERR_OUT_OF_DOMAIN) check(st, "step");
+  }
+};
+
+class USL : public Solver {
+ public:
+  USL(const ParticlesContainer &p, const NodesContainer &n, const std::vector<MaterialType> &mats,
+      const std::vector<BoundaryConditionType> &bcs, Real alpha = 0.99f, unsigned flags = 0)
+      : Solver(p, n, mats, bcs, alpha, flags), alpha(alpha) {}
+  // USL::P2G / USL::G2P (src/solver/usl/usl.cpp:118-199), after a partition
+  void partition() { check(pmpm_partition(handle->sim), "partition"); }
+  void P2G() { check(pmpm_p2g(handle->sim, 0), "P2G"); }
+  void G2P() { check(pmpm_g2p(handle->sim, 0), "G2P"); }
+  Real alpha;
+};
+
+}  // namespace dim2 / dim3
+}  // namespace pyroclastmpm

@@ -1,0 +1,91 @@
+"""The reference's Python workflows, run through MPM2D / MPM3D on the GPU."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from pyroclastmpm_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+G = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_unit_vectors.json")))
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def test_two_disc_example_through_module():
+    """examples/two_disc_impact/run.py, shortened, vs the FP32 oracle."""
+    import pyroclastmpm_b200.MPM2D as pm
+
+    sc = scenes.two_discs()
+    rng = np.random.default_rng(5)
+    sc["velocities"] = sc["velocities"] * (1.0 + 0.01 * rng.uniform(-1, 1, sc["velocities"].shape))
+    pm.set_globals(sc["dt"], sc["particles_per_cell"], "linear", "output")
+    pm.set_global_step(0)
+    nodes = pm.NodesContainer([0.0, 0.0], [1.0, 1.0], sc["cell_size"])
+    particles = pm.ParticlesContainer(sc["positions"], sc["velocities"])
+    mpm = pm.USL(particles, nodes, [pm.LinearElastic(1000.0, 1000.0, 0.3)], alpha=0.99)
+    mpm.run(9, 100)  # 10 solves
+    assert mpm.current_step == 10
+    ref = oracle.OracleSim(**scenes.sim_kwargs(sc), positions=sc["positions"], velocities=sc["velocities"])
+    ref.initialize()
+    ref.run(9)
+    assert rel(mpm.particles.positions, ref["positions"]) < 1e-5
+    assert rel(mpm.particles.velocities, ref["velocities"]) < 1e-5
+    assert rel(mpm.particles.stresses, ref["stresses"]) < 2e-4
+    assert mpm.particles.positions.shape == (len(sc["positions"]), 2)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_usl_stepwise_through_module(dim):
+    """tests/unit/test_usl.h:32-176 written against the module API."""
+    import importlib
+
+    pm = importlib.import_module(f"pyroclastmpm_b200.MPM{dim}D")
+    v = G["usl_stepwise"]
+    k = str(dim)
+    pm.set_globals(v["dt"], 1, "linear", "output")
+    pm.set_global_step(0)
+    pos = np.array(v["positions"][k])
+    particles = pm.ParticlesContainer(pos, np.ones_like(pos))
+    nodes = pm.NodesContainer([0.0] * dim, [1.0] * dim, 1.0)
+    usl = pm.USL(particles, nodes)
+    stresses = np.zeros((2, 3, 3))
+    stresses[0] = 1.0
+    usl.particles.masses = v["masses"]
+    usl.particles.volumes = v["volumes"]
+    usl.particles.volumes_original = v["volumes"]
+    usl.particles.stresses = stresses
+    usl.partition()
+    usl.P2G()
+    tol = v["tol"]
+    np.testing.assert_allclose(usl.nodes.masses[:2], v["node_masses"][k], atol=tol)
+    np.testing.assert_allclose(usl.nodes.moments[:2], v["node_moments"][k], atol=tol)
+    usl.G2P()
+    np.testing.assert_allclose(usl.particles.volumes[0], v["particle0_volume"][k], atol=tol)
+    np.testing.assert_allclose(usl.particles.positions[0], v["particle0_position"][k], atol=tol)
+    np.testing.assert_allclose(np.diag(usl.particles.F[0]), v["particle0_F_diag"][k], atol=tol)
+
+
+def test_granular_column_through_module():
+    import pyroclastmpm_b200.MPM3D as pm
+
+    sc = scenes.granular_column(cell_size=1.0 / 64)
+    pm.set_globals(sc["dt"], sc["particles_per_cell"], "quadratic", "output")
+    pm.set_global_step(0)
+    nodes = pm.NodesContainer(sc["origin"], sc["end"], sc["cell_size"])
+    particles = pm.ParticlesContainer(sc["positions"], sc["velocities"])
+    mat = pm.DruckerPrager(1500.0, 1.0e7, 0.3, 30.0, 0.0, 0.0)
+    bcs = [pm.Gravity([0.0, 0.0, -9.81]), pm.NodeDomain([1, 1, 1], [1, 1, 1])]
+    mpm = pm.USL(particles, nodes, [mat], bcs)
+    mpm.solve_nsteps(5)
+    ref = oracle.OracleSim(**scenes.sim_kwargs(sc), positions=sc["positions"], velocities=sc["velocities"])
+    ref.initialize()
+    ref.solve(5)
+    for name in ("positions", "velocities", "stresses", "F"):
+        assert rel(getattr(mpm.particles, name), ref[name]) < 1e-5, name

@@ -1,0 +1,54 @@
+"""The MPM2D / MPM3D modules expose the reference's Python API (CPU checks)."""
+import numpy as np
+import pytest
+
+NAMES = ["set_globals", "set_global_shapefunction", "set_global_timestep", "set_global_step",
+         "set_global_output_directory", "NodesContainer", "ParticlesContainer", "Solver", "USL",
+         "Material", "LinearElastic", "NewtonFluid", "DruckerPrager", "BoundaryCondition", "Gravity",
+         "NodeDomain", "BodyForce", "PlanarDomain", "global_dimension"]
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_module_names(dim):
+    import importlib
+
+    pm = importlib.import_module(f"pyroclastmpm_b200.MPM{dim}D")
+    for n in NAMES:
+        assert hasattr(pm, n), n
+    assert pm.global_dimension == dim
+
+
+def test_nodes_container_grid_and_coords():
+    import oracle
+    import pyroclastmpm_b200.MPM3D as pm
+
+    nodes = pm.NodesContainer([0.0, 0.0, 0.0], [1.0, 0.25, 0.5], 1.0 / 64)
+    assert nodes.num_cells == oracle.grid_dims(3, [0, 0, 0], [1.0, 0.25, 0.5], 1.0 / 64)
+    xyz = nodes.give_coords()
+    assert xyz.shape == (nodes.num_cells_total, 3)
+    np.testing.assert_allclose(xyz[1], [1.0 / 64, 0.0, 0.0], rtol=1e-6)
+    np.testing.assert_allclose(xyz[nodes.num_cells[0]], [0.0, 1.0 / 64, 0.0], rtol=1e-6)
+
+
+def test_material_constants_and_unknown_shape_function():
+    import pyroclastmpm_b200.MPM2D as pm
+
+    le = pm.LinearElastic(1000.0, 1000.0, 0.3)
+    E, nu = np.float32(1000.0), np.float32(0.3)
+    assert le.shear_modulus == pytest.approx(float(E / (np.float32(2) * (np.float32(1) + nu))))
+    with pytest.raises(ValueError):
+        pm.set_global_shapefunction("quartic")  # the reference calls exit(1) here
+
+
+def test_solver_without_gpu_raises():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    import pyroclastmpm_b200.MPM2D as pm
+
+    pm.set_globals(1e-3, 4, "linear", "./output/")
+    p = pm.ParticlesContainer(np.array([[0.5, 0.5]]))
+    n = pm.NodesContainer([0.0, 0.0], [1.0, 1.0], 0.1)
+    with pytest.raises(RuntimeError):
+        pm.USL(p, n, [pm.LinearElastic(1000.0, 1000.0, 0.3)])
