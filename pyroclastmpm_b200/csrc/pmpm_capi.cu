@@ -825,8 +825,7 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK) st = dalloc(&s->N.m, nn);
   if (st == PMPM_OK) st = dalloc(&s->N.p, nn * D);
   if (st == PMPM_OK) st = dalloc(&s->N.pnt, nn * D);
-  if (st == PMPM_OK) st = dalloc(&s->N.v, nn * D);
-  if (st == PMPM_OK) st = dalloc(&s->N.vnt, nn * D);
+  if (st == PMPM_OK) st = dalloc(&s->N.vel, nn * (s->dim == 3 ? NodeVel<3>::F : NodeVel<2>::F));
   if (st == PMPM_OK) st = dalloc(&s->N.tile_epoch, (size_t)g.ntiles);
   if (st == PMPM_OK) st = dalloc(&s->node_epoch, (size_t)g.ntiles);
   // binning key space (reference cells, or dual cells for the 3D quadratic fast path)
@@ -869,8 +868,7 @@ int pmpm_destroy(pmpm_sim *s) {
   dfree(s->N.m);
   dfree(s->N.p);
   dfree(s->N.pnt);
-  dfree(s->N.v);
-  dfree(s->N.vnt);
+  dfree(s->N.vel);
   dfree(s->N.tile_epoch);
   dfree(s->node_epoch);
   dfree(s->B.count);

@@ -65,8 +65,16 @@ struct DevParticles {
 };
 
 struct DevNodes {
-  float *m, *p, *pnt, *v, *vnt;
+  float *m, *p, *pnt;
+  // v = p/m and v_nt = p_nt/m packed per node for the G2P gather:
+  // 3D: vx vy vz - | vntx vnty vntz -  (two float4), 2D: vx vy vntx vnty
+  float *vel;
   int *tile_epoch;  // tile active in the partition whose epoch it holds
+};
+
+template <int D>
+struct NodeVel {
+  static constexpr int F = D == 3 ? 8 : 4;  // floats per node in DevNodes::vel
 };
 
 struct DevBins {
@@ -488,6 +496,31 @@ __device__ __forceinline__ void dp_update(const float *prm, const float *L, floa
 // --------------------------------------------------------------------------
 // node epilogue: P2G result -> boundary conditions -> velocities
 // --------------------------------------------------------------------------
+
+// Writes one node's final values: mass, moments, forward moments and the
+// packed velocities (0 where the mass is at or below the cutoff, which G2P
+// then adds as zero, as the reference skips those nodes).
+template <int D>
+__device__ __forceinline__ void write_node(const StepArgs &a, int node, float mass, const float p[3],
+                                           const float pnt[3], bool live) {
+  const int nt = a.g.ntotal;
+  a.N.m[node] = mass;
+  float v[3] = {0.0f, 0.0f, 0.0f}, vn[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    a.N.p[c * nt + node] = p[c];
+    a.N.pnt[c * nt + node] = pnt[c];
+    v[c] = live ? p[c] / mass : 0.0f;
+    vn[c] = live ? pnt[c] / mass : 0.0f;
+  }
+  float4 *vel = reinterpret_cast<float4 *>(a.N.vel);
+  if (D == 3) {
+    vel[2 * (size_t)node] = make_float4(v[0], v[1], v[2], 0.0f);
+    vel[2 * (size_t)node + 1] = make_float4(vn[0], vn[1], vn[2], 0.0f);
+  } else {
+    vel[node] = make_float4(v[0], v[1], vn[0], vn[1]);
+  }
+}
 
 // Applies the node boundary conditions in list order to (p, pnt) of node
 // `node` with coordinates nc and mass m:

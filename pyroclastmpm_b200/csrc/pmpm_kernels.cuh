@@ -533,15 +533,7 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int a
     mass = 0.0f;
   }
   if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
-  const int nt = g.ntotal;
-  a.N.m[node] = mass;
-#pragma unroll
-  for (int c = 0; c < D; c++) {
-    a.N.p[c * nt + node] = p[c];
-    a.N.pnt[c * nt + node] = pnt[c];
-    a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
-    a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
-  }
+  write_node<D>(a, node, mass, p, pnt, live);
 }
 
 // --------------------------------------------------------------------------
@@ -828,15 +820,7 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int app
     mass = 0.0f;
   }
   if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
-  const int nt = g.ntotal;
-  a.N.m[node] = mass;
-#pragma unroll
-  for (int c = 0; c < D; c++) {
-    a.N.p[c * nt + node] = p[c];
-    a.N.pnt[c * nt + node] = pnt[c];
-    a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
-    a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
-  }
+  write_node<D>(a, node, mass, p, pnt, live);
 }
 
 // --------------------------------------------------------------------------
@@ -1162,15 +1146,7 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
     mass = 0.0f;
   }
   if (apply_bcs) node_bcs<3>(a, node, nc, mass, p, pnt);
-  const int nt = g.ntotal;
-  a.N.m[node] = mass;
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    a.N.p[c * nt + node] = p[c];
-    a.N.pnt[c * nt + node] = pnt[c];
-    a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
-    a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
-  }
+  write_node<3>(a, node, mass, p, pnt, live);
 }
 
 // --------------------------------------------------------------------------
@@ -1237,15 +1213,7 @@ __device__ __forceinline__ void tile_epilogue3(const StepArgs &a, int apply_bcs,
       mass = 0.0f;
     }
     if (apply_bcs) node_bcs<3>(a, node, nc, mass, p, pnt);
-    const int nt = g.ntotal;
-    a.N.m[node] = mass;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      a.N.p[c * nt + node] = p[c];
-      a.N.pnt[c * nt + node] = pnt[c];
-      a.N.v[c * nt + node] = live ? p[c] / mass : 0.0f;
-      a.N.vnt[c * nt + node] = live ? pnt[c] / mass : 0.0f;
-    }
+    write_node<3>(a, node, mass, p, pnt, live);
   }
 }
 
@@ -1510,7 +1478,7 @@ __global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int stor
   if (s >= a.P.n) return;
   const DevParticles &P = a.P;
   const DevGrid &g = a.g;
-  const int st = P.stride, nt = g.ntotal;
+  const int st = P.stride;
   constexpr int K = Stencil<SF>::K;
   float x[3] = {0, 0, 0}, v[3] = {0, 0, 0}, u[3] = {0, 0, 0};
   int b[3] = {0, 0, 0};
@@ -1583,10 +1551,15 @@ __global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int stor
             dpsi[2] = dN[2][kz] * N[0][kx] * N[1][ky];
           }
           float vn[3], vnt[3];
-#pragma unroll
-          for (int c = 0; c < D; c++) {
-            vn[c] = a.N.v[c * nt + node];
-            vnt[c] = a.N.vnt[c * nt + node];
+          const float4 *vel = reinterpret_cast<const float4 *>(a.N.vel);
+          if (D == 3) {
+            const float4 q0 = __ldg(vel + 2 * (size_t)node), q1 = __ldg(vel + 2 * (size_t)node + 1);
+            vn[0] = q0.x; vn[1] = q0.y; vn[2] = q0.z;
+            vnt[0] = q1.x; vnt[1] = q1.y; vnt[2] = q1.z;
+          } else {
+            const float4 q = __ldg(vel + node);
+            vn[0] = q.x; vn[1] = q.y; vn[2] = 0.0f;
+            vnt[0] = q.z; vnt[1] = q.w; vnt[2] = 0.0f;
           }
 #pragma unroll
           for (int c = 0; c < D; c++) {
