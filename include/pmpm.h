@@ -63,8 +63,21 @@ enum {
   PMPM_BC_GRAVITY = 1,      /* src/boundaryconditions/gravity.cpp:65-88            */
   PMPM_BC_NODEDOMAIN = 2,   /* src/boundaryconditions/nodedomain_inline.h:40-87    */
   PMPM_BC_BODYFORCE = 3,    /* src/boundaryconditions/bodyforce_inline.h:41-59     */
-  PMPM_BC_PLANARDOMAIN = 4  /* src/boundaryconditions/planardomain_inline.h:56-138 */
+  PMPM_BC_PLANARDOMAIN = 4, /* src/boundaryconditions/planardomain_inline.h:56-138 */
+  /* RigidBodyLevelSet as the reference computes it: stick contact of nodes
+   * with the nearest rigid particle (rigidbodylevelset_inline.h:65-199, 240-343,
+   * rigidbodylevelset.cpp:92-275); linear shape functions only */
+  PMPM_BC_RIGIDBODY_LEVELSET = 5,
+  /* RigidBodyLevelSet with an analytic signed-distance body (sphere or
+   * half-cylinder shell) in translation and rotation and Coulomb friction;
+   * no reference counterpart (the reference's level set is the mode above) */
+  PMPM_BC_RIGID_SDF = 6
 };
+
+/* Rigid-body modes (RigidBodyMode, include/pyroclastmpm/boundaryconditions/
+ * rigidbodylevelset.h:33) and analytic shapes. */
+enum { PMPM_RIGID_STATIC = 0, PMPM_RIGID_LOOP_ROTATE = 1 };
+enum { PMPM_SDF_SPHERE = 0, PMPM_SDF_HALF_CYLINDER_SHELL = 1 };
 
 /* Step flags. */
 enum {
@@ -96,11 +109,23 @@ typedef struct {
  *   BODYFORCE:    ints[0] mode (0 forces, 1 moments, 2 fixed), ints[1] active,
  *                 values [num_nodes][dim] and mask [num_nodes] (host, copied)
  *   PLANARDOMAIN: reals[0..2] face0 friction, reals[3..5] face1 friction
- *                 (radians; the pmpm_bc_planardomain helper converts degrees) */
+ *                 (radians; the pmpm_bc_planardomain helper converts degrees)
+ *   RIGIDBODY_LEVELSET: ints[0] mode (PMPM_RIGID_*), ints[1] corrected rotation
+ *                 (0: the reference's matrices, 1: proper Rz Ry Rx),
+ *                 reals[0..2] euler angles per second, reals[3..5] COM
+ *   RIGID_SDF:    ints[0] shape (PMPM_SDF_*), ints[1] axis (3D: 0, 1, 2; the
+ *                 cross-section plane is (axis+1, axis+2) cyclic; 2D: the
+ *                 plane is (x, y)), reals[0..2] centre at step 0,
+ *                 reals[3..5] translational velocity, reals[6] angular
+ *                 velocity about the axis (rad/s), reals[7] Coulomb friction
+ *                 coefficient, reals[8..10] dimensions (sphere: radius;
+ *                 shell: mid-surface radius, thickness, length along the
+ *                 axis), reals[11] contact distance (nodes with signed
+ *                 distance below it are in contact), reals[12] angle at step 0 */
 typedef struct {
   int type;
   int ints[8];
-  float reals[12];
+  float reals[16];
   const float *values;
   const unsigned char *mask;
 } pmpm_bc;
@@ -197,6 +222,32 @@ int pmpm_bc_bodyforce(int mode, const float *values, const unsigned char *mask, 
  * friction angles in degrees, stored in radians */
 int pmpm_bc_planardomain(const float *face0_friction_deg, const float *face1_friction_deg, int dim,
                          pmpm_bc *out);
+/* RigidBodyLevelSet::RigidBodyLevelSet and ::set_mode_loop_rotate
+ * (src/boundaryconditions/rigidbodylevelset.cpp:32-60).  mode STATIC keeps
+ * the rigid particles' velocity at zero (the reference leaves its rotation
+ * matrix unset in that mode; the identity is used).  euler_angles_per_second
+ * and com may be NULL (zero). */
+int pmpm_bc_rigidbodylevelset(int mode, const float *euler_angles_per_second, const float *com,
+                              int corrected_rotation, int dim, pmpm_bc *out);
+/* Analytic rigid body (no reference counterpart): shape PMPM_SDF_*, centre,
+ * velocity (may be NULL), angular velocity about the axis, angle at step 0,
+ * dims[3], Coulomb friction, contact distance.  Applied to the forward
+ * moments of every node with mass whose position has signed distance below
+ * the contact distance: the relative velocity's inward normal part is
+ * removed and its tangential part reduced by friction (stick if the
+ * tangential speed is below friction x the normal speed). */
+int pmpm_bc_rigid_sdf(int shape, int axis, const float *center, const float *velocity, float angular_velocity,
+                      float angle0, const float *dims, float friction, float contact_distance, int dim,
+                      pmpm_bc *out);
+
+/* Critical time step from the p-wave speed (src/common/tools.cpp:373-380,
+ * LinearElastic::calculate_timestep, src/materials/linearelastic.cpp:96-105):
+ * dt = factor * cell_size / sqrt((K + 4G/3) / density). */
+int pmpm_calculate_timestep(float cell_size, float factor, float bulk_modulus, float shear_modulus,
+                            float density, float *dt);
+/* The same for a filled pmpm_material: LINEAR_ELASTIC and DRUCKER_PRAGER use
+ * their K and G; NEWTON_FLUID uses K and G = 0 (sound speed sqrt(K/rho)). */
+int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float factor, float *dt);
 
 /* Create a simulation: the Grid and NodesContainer constructors
  * (include/pyroclastmpm/common/types_common.h:260-272, src/nodes/nodes.cpp:

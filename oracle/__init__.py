@@ -30,6 +30,9 @@ SHAPE_FUNCTIONS = {"linear": LINEAR, "quadratic": QUADRATIC, "cubic": CUBIC}
 
 MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER = 0, 1, 2, 3
 BC_GRAVITY, BC_NODEDOMAIN, BC_BODYFORCE, BC_PLANARDOMAIN = 1, 2, 3, 4
+BC_RIGIDBODY_LEVELSET, BC_RIGID_SDF = 5, 6
+RIGID_MODES = {"static": 0, "loop_rotate": 1}
+SDF_SHAPES = {"sphere": 0, "half_cylinder_shell": 1}
 
 
 def build() -> None:
@@ -62,7 +65,7 @@ def _structs(precision):
         _fields_ = [("type", ctypes.c_int), ("density", creal), ("p", creal * 8)]
 
     class BC(ctypes.Structure):
-        _fields_ = [("type", ctypes.c_int), ("i", ctypes.c_int * 8), ("r", creal * 12),
+        _fields_ = [("type", ctypes.c_int), ("i", ctypes.c_int * 8), ("r", creal * 16),
                     ("values", ctypes.c_void_p), ("mask", ctypes.c_void_p)]
 
     P = ctypes.c_void_p
@@ -150,7 +153,8 @@ class OracleSim:
     def __init__(self, dim, origin, end, cell_size, positions, velocities=None, colors=None,
                  shape_function="linear", dt=1e-3, particles_per_cell=1, alpha=0.99,
                  materials=(), bcs=(), precision="f32", global_step=0,
-                 stresses=None, volumes=None, masses=None, volumes_original=None):
+                 stresses=None, volumes=None, masses=None, volumes_original=None,
+                 rigid_positions=None, rigid_velocities=None, rigid_colors=None):
         self.precision = precision
         self.lib = _lib(precision)
         Grid, Material, BC, Sim = _structs(precision)
@@ -158,8 +162,20 @@ class OracleSim:
         self.npr = npr
         self.dim = d = dim
         self.sf = SHAPE_FUNCTIONS[shape_function] if isinstance(shape_function, str) else int(shape_function)
-        # inputs are always copied: the simulation advances its arrays in place
+        # inputs are always copied: the simulation advances its arrays in place.
+        # Rigid particles follow the others (ParticlesContainer ctor,
+        # src/particles/particles.cpp:51-149).
         x = np.array(positions, dtype=npr, copy=True).reshape(-1, d)
+        nr = 0 if rigid_positions is None else len(np.asarray(rigid_positions).reshape(-1, d))
+        n0 = x.shape[0]
+        if nr:
+            x = np.concatenate([x, np.asarray(rigid_positions, npr).reshape(nr, d)])
+            rv = np.zeros((nr, d), npr) if rigid_velocities is None else np.asarray(rigid_velocities, npr)
+            v0 = np.zeros((n0, d), npr) if velocities is None else np.asarray(velocities, npr).reshape(n0, d)
+            velocities = np.concatenate([v0, rv.reshape(nr, d)])
+            c0 = np.zeros(n0, np.uint8) if colors is None else np.asarray(colors).astype(np.uint8)
+            rc = np.zeros(nr, np.uint8) if rigid_colors is None else np.asarray(rigid_colors).astype(np.uint8)
+            colors = np.concatenate([c0, rc])
         n = x.shape[0]
         self.n = n
         g = Grid()
@@ -184,6 +200,7 @@ class OracleSim:
         a["forces_external"] = z(n, d)
         a["colors"] = (np.zeros(n, np.uint8) if colors is None else np.asarray(colors).astype(np.uint8))
         a["is_rigid"] = np.zeros(n, np.uint8)
+        a["is_rigid"][n0:] = 1
         a["is_active"] = np.ones(n, np.uint8)
         a["psi"] = z(n * self.nsn)
         a["dpsi"] = z(n * self.nsn * d)
@@ -273,6 +290,30 @@ class OracleSim:
             for a in range(3):
                 c.r[a] = float(npr(npr(f0[a]) * deg))
                 c.r[3 + a] = float(npr(npr(f1[a]) * deg))
+        elif t == "RigidBodyLevelSet" and "shape" not in bc:
+            c.type = BC_RIGIDBODY_LEVELSET
+            c.i[0] = RIGID_MODES[bc.get("mode", "static")]
+            c.i[1] = 1 if bc.get("corrected_rotation", False) else 0
+            rate = list(bc.get("euler_angles_per_second", [0.0] * d)) + [0.0] * 3
+            com = list(bc.get("COM", [0.0] * d)) + [0.0] * 3
+            for a in range(3):
+                c.r[a] = float(npr(rate[a])) if a < d else 0.0
+                c.r[3 + a] = float(npr(com[a])) if a < d else 0.0
+        elif t == "RigidBodyLevelSet":
+            c.type = BC_RIGID_SDF
+            c.i[0] = SDF_SHAPES[bc["shape"]]
+            c.i[1] = int(bc.get("axis", 2)) if d == 3 else 2
+            cen = list(bc["center"]) + [0.0] * 3
+            vel = list(bc.get("velocity", [0.0] * d)) + [0.0] * 3
+            dims = list(bc["dims"]) + [0.0] * 3
+            for a in range(3):
+                c.r[a] = float(npr(cen[a])) if a < d else 0.0
+                c.r[3 + a] = float(npr(vel[a])) if a < d else 0.0
+                c.r[8 + a] = float(npr(dims[a])) if (c.i[0] == 1 or a == 0) else 0.0
+            c.r[6] = float(npr(bc.get("angular_velocity", 0.0)))
+            c.r[7] = float(npr(bc.get("friction", 0.0)))
+            c.r[11] = float(npr(bc.get("contact_distance", 0.0)))
+            c.r[12] = float(npr(bc.get("angle", 0.0)))
         else:
             raise ValueError(f"unknown boundary condition {t}")
 

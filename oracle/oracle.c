@@ -511,6 +511,267 @@ static void bodyforce(or_sim *s, const or_bc *bc) {
   }
 }
 
+#ifdef OR_DOUBLE
+#define RCOS cos
+#define RSIN sin
+#define RSQRT sqrt
+#else
+#define RCOS cosf
+#define RSIN sinf
+#define RSQRT sqrtf
+#endif
+
+/* 3x3 product, coefficients summed ((a0 b0 + a1 b1) + a2 b2). */
+static void mat3_mul(const real *A, const real *B, real *C) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      real acc = (real)(A[3 * i] * B[j]);
+      acc = (real)(acc + (real)(A[3 * i + 1] * B[3 + j]));
+      C[3 * i + j] = (real)(acc + (real)(A[3 * i + 2] * B[6 + j]));
+    }
+}
+
+/* RigidBodyLevelSet::update_animation (src/boundaryconditions/rigidbodylevelset.cpp:
+ * 127-206).  LOOP_ROTATE: euler += rate dt; delta = previous - new.  2D:
+ * R = [[cos d0, -sin d0], [sin d0, cos d0]].  3D as the reference assigns it:
+ * Rx keeps (0,1) = -sin d0 and (1,0) = sin d0 of the 2D assignment under its
+ * 3D entries, Rz is never assigned (zero), so R = Rz Ry Rx = 0; i[1] = 1 gives
+ * the proper Rz(d2) Ry(d1) Rx(d0).  STATIC leaves the reference's matrix
+ * unset; the identity is taken. */
+static void rigid_rotation(or_sim *s, or_bc *bc, real *R) {
+  int d = s->grid.dim;
+  real R3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (bc->i[0] == 1) {
+    real dl[3];
+    for (int a = 0; a < 3; a++) {
+      real prev = bc->r[6 + a];
+      bc->r[6 + a] = (real)(bc->r[6 + a] + (real)(bc->r[a] * s->dt));
+      dl[a] = (real)(prev - bc->r[6 + a]);
+    }
+    real c0 = (real)RCOS(dl[0]), s0 = (real)RSIN(dl[0]);
+    real c1 = (real)RCOS(dl[1]), s1 = (real)RSIN(dl[1]);
+    real c2 = (real)RCOS(dl[2]), s2 = (real)RSIN(dl[2]);
+    if (d == 2) {
+      real M[9] = {c0, -s0, 0, s0, c0, 0, 0, 0, 1};
+      memcpy(R3, M, sizeof(R3));
+    } else {
+      real Rx[9], Ry[9] = {c1, 0, s1, 0, 1, 0, -s1, 0, c1}, Rz[9], T[9];
+      if (!bc->i[1]) {
+        real X[9] = {1, -s0, 0, s0, c2, -s2, 0, s2, c2};
+        memcpy(Rx, X, sizeof(X));
+        memset(Rz, 0, sizeof(Rz));
+      } else {
+        real X[9] = {1, 0, 0, 0, c0, -s0, 0, s0, c0};
+        real Z[9] = {c2, -s2, 0, s2, c2, 0, 0, 0, 1};
+        memcpy(Rx, X, sizeof(X));
+        memcpy(Rz, Z, sizeof(Z));
+      }
+      mat3_mul(Rz, Ry, T);
+      mat3_mul(T, Rx, R3);
+    }
+  }
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) R[a * d + b] = R3[3 * a + b];
+}
+
+/* RigidBodyLevelSet::apply_on_nodes_moments (src/boundaryconditions/
+ * rigidbodylevelset.cpp:92-105): update_animation; set_velocities (CPU
+ * branch, :245-275, update_rigid_velocity rigidbodylevelset_inline.h:240-299);
+ * calculate_grid_normals_nn_rigid (rigidbodylevelset_inline.h:65-199) per
+ * node; set_position (update_rigid_position, :329-343). */
+static void rigid_nn(or_sim *s, or_bc *bc) {
+  const or_grid *g = &s->grid;
+  int d = g->dim;
+  real R[9];
+  rigid_rotation(s, bc, R);
+  for (int i = 0; i < s->num_particles; i++) {
+    if (!s->is_rigid[i]) continue;
+    real r[3], u[3];
+    for (int a = 0; a < d; a++) r[a] = (real)(s->positions[i * d + a] - bc->r[3 + a]);
+    for (int a = 0; a < d; a++) {
+      real acc = (real)(R[a * d] * r[0]);
+      for (int b = 1; b < d; b++) acc = (real)(acc + (real)(R[a * d + b] * r[b]));
+      u[a] = acc;
+    }
+    for (int a = 0; a < d; a++) s->velocities[i * d + a] = (real)((real)(u[a] - r[a]) / s->dt);
+  }
+  static const int W3[8][3] = {{0, 0, 0}, {0, 0, -1}, {-1, 0, 0}, {-1, 0, -1},
+                               {0, -1, 0}, {0, -1, -1}, {-1, -1, 0}, {-1, -1, -1}};
+  static const int W2[4][3] = {{0, 0, 0}, {-1, 0, 0}, {0, -1, 0}, {-1, -1, 0}};
+  int nw = d == 3 ? 8 : 4;
+  for (int n = 0; n < g->num_cells_total; n++) {
+    real m = s->node_masses[n];
+    if (m <= (real)0.000000001) continue;
+    real normal[3] = {0, 0, 0};
+    real min_dist = (real)999999999999999.;
+    int min_id = -1;
+    for (int sid = 0; sid < nw; sid++) {
+      const int *w = d == 3 ? W3[sid] : W2[sid];
+      int sb[3] = {0, 0, 0};
+      for (int a = 0; a < d; a++) sb[a] = s->node_ids[3 * n + a] + w[a];
+      unsigned int h = (unsigned int)flat3(g, sb);
+      if (h >= (unsigned int)g->num_cells_total) continue;
+      int cs = s->cell_start[h], ce = s->cell_end[h];
+      for (int j = cs; j < ce; j++) {
+        int pid = s->sorted_index[j];
+        if (s->is_rigid[pid]) {
+          real dist = 0;
+          for (int a = 0; a < d; a++) {
+            real rel = (real)((real)(s->positions[pid * d + a] - g->origin[a]) * g->inv_cell_size);
+            rel = (real)(rel - (real)sb[a]);
+            dist = a == 0 ? (real)(rel * rel) : (real)(dist + (real)(rel * rel));
+          }
+          if (dist < min_dist) {
+            min_dist = dist;
+            min_id = pid;
+          }
+        } else {
+          const real *dp = s->dpsi + ((size_t)pid * s->nsn + sid) * d;
+          for (int a = 0; a < d; a++) normal[a] = (real)(normal[a] + (real)(dp[a] * s->masses[pid]));
+        }
+      }
+    }
+    if (min_id < 0) continue;
+    real sq = (real)(normal[0] * normal[0]);
+    for (int a = 1; a < d; a++) sq = (real)(sq + (real)(normal[a] * normal[a]));
+    if (sq > (real)0.0) {
+      real len = (real)RSQRT(sq);
+      for (int a = 0; a < d; a++) normal[a] = (real)(normal[a] / len);
+    }
+    real *p = s->node_moments + (size_t)n * d;
+    real *q = s->node_moments_nt + (size_t)n * d;
+    real v[3], vt[3], cv[3], cvt[3], rel = 0, rel_nt = 0;
+    for (int a = 0; a < d; a++) {
+      real vb = s->velocities[min_id * d + a];
+      v[a] = (real)(p[a] / m);
+      vt[a] = (real)(q[a] / m);
+      cv[a] = (real)(v[a] - vb);
+      cvt[a] = (real)(vt[a] - vb);
+      rel = a == 0 ? (real)(cv[a] * normal[a]) : (real)(rel + (real)(cv[a] * normal[a]));
+      rel_nt = a == 0 ? (real)(cvt[a] * normal[a]) : (real)(rel_nt + (real)(cvt[a] * normal[a]));
+    }
+    if (rel >= (real)0.0)
+      for (int a = 0; a < d; a++) p[a] = (real)((real)(v[a] - cv[a]) * m);
+    if (rel_nt >= (real)0.0)
+      for (int a = 0; a < d; a++) q[a] = (real)((real)(vt[a] - cvt[a]) * m);
+  }
+  for (int i = 0; i < s->num_particles; i++) {
+    if (!s->is_rigid[i]) continue;
+    for (int a = 0; a < d; a++)
+      s->positions[i * d + a] = (real)(s->positions[i * d + a] + (real)(s->velocities[i * d + a] * s->dt));
+  }
+}
+
+/* Analytic rigid body (no reference counterpart).  Pose at time step*dt:
+ * centre c0 + v t, angle angle0 + omega t about the axis.  Cross-section
+ * plane (P, Q) = (axis+1, axis+2) cyclic in 3D, (x, y) in 2D.  Shell: the
+ * half q <= 0 (local) of the annulus |rho - R| <= t/2, ends rounded with
+ * radius t/2, extruded to length L along the axis (3D).  Returns the signed
+ * distance of x and the outward unit normal. */
+static real sdf_eval(int d, const or_bc *bc, const real *c, real cs, real sn, const real *x, real *nrm) {
+  int A = d == 3 ? bc->i[1] : 2;
+  int P = d == 3 ? (A + 1) % 3 : 0, Q = d == 3 ? (A + 2) % 3 : 1;
+  real dd[3] = {0, 0, 0};
+  for (int a = 0; a < d; a++) dd[a] = (real)(x[a] - c[a]);
+  nrm[0] = nrm[1] = nrm[2] = 0;
+  if (bc->i[0] == 0) {
+    real r2 = 0;
+    for (int a = 0; a < d; a++) r2 = (real)(r2 + (real)(dd[a] * dd[a]));
+    real r = (real)RSQRT(r2);
+    if (r > 0) {
+      for (int a = 0; a < d; a++) nrm[a] = (real)(dd[a] / r);
+    } else {
+      nrm[Q] = 1;
+    }
+    return (real)(r - bc->r[8]);
+  }
+  real lp = (real)((real)(cs * dd[P]) + (real)(sn * dd[Q]));
+  real lq = (real)((real)(cs * dd[Q]) - (real)(sn * dd[P]));
+  real R = bc->r[8], ht = (real)((real)0.5 * bc->r[9]);
+  real phi2, gp = 0, gq = 1;
+  if (lq <= 0) {
+    real rho = (real)RSQRT((real)((real)(lp * lp) + (real)(lq * lq)));
+    phi2 = (real)((real)fabs((double)(rho - R)) - ht);
+    if (rho > 0) {
+      real sg = rho >= R ? (real)1 : (real)-1;
+      gp = (real)((real)(sg * lp) / rho);
+      gq = (real)((real)(sg * lq) / rho);
+    }
+  } else {
+    real wp = (real)(lp - (lp >= 0 ? R : -R)), wq = lq;
+    real w = (real)RSQRT((real)((real)(wp * wp) + (real)(wq * wq)));
+    phi2 = (real)(w - ht);
+    if (w > 0) {
+      gp = (real)(wp / w);
+      gq = (real)(wq / w);
+    }
+  }
+  real phi = phi2, ga = 0;
+  if (d == 3) {
+    real la = dd[A];
+    real hA = (real)((real)fabs((double)la) - (real)((real)0.5 * bc->r[10]));
+    real sa = la >= 0 ? (real)1 : (real)-1;
+    if (phi2 > 0 && hA > 0) {
+      phi = (real)RSQRT((real)((real)(phi2 * phi2) + (real)(hA * hA)));
+      gp = (real)((real)(phi2 * gp) / phi);
+      gq = (real)((real)(phi2 * gq) / phi);
+      ga = (real)((real)(hA * sa) / phi);
+    } else if (hA > phi2) {
+      phi = hA;
+      gp = gq = 0;
+      ga = sa;
+    }
+  }
+  nrm[P] = (real)((real)(cs * gp) - (real)(sn * gq));
+  nrm[Q] = (real)((real)(sn * gp) + (real)(cs * gq));
+  if (d == 3) nrm[A] = ga;
+  return phi;
+}
+
+/* Coulomb contact of the forward moments of every node with m > 1e-9 whose
+ * signed distance is below the contact distance: relative velocity
+ * v_rel = p_nt/m - v_body(x); if its normal part vn < 0, the normal part is
+ * removed and the tangential part vt scaled by max(0, 1 + mu vn / |vt|). */
+static void rigid_sdf(or_sim *s, const or_bc *bc) {
+  const or_grid *g = &s->grid;
+  int d = g->dim;
+  int A = d == 3 ? bc->i[1] : 2;
+  int P = d == 3 ? (A + 1) % 3 : 0, Q = d == 3 ? (A + 2) % 3 : 1;
+  double t = (double)s->global_step * (double)s->dt;
+  real c[3] = {0, 0, 0};
+  for (int a = 0; a < d; a++) c[a] = (real)((double)bc->r[a] + (double)bc->r[3 + a] * t);
+  double ang = (double)bc->r[12] + (double)bc->r[6] * t;
+  real cs = (real)cos(ang), sn = (real)sin(ang);
+  real mu = bc->r[7], omega = bc->r[6];
+  for (int n = 0; n < g->num_cells_total; n++) {
+    real m = s->node_masses[n];
+    if (m <= (real)0.000000001) continue;
+    real x[3] = {0, 0, 0}, nrm[3];
+    for (int a = 0; a < d; a++)
+      x[a] = (real)(g->origin[a] + (real)((real)s->node_ids[3 * n + a] * g->cell_size));
+    real phi = sdf_eval(d, bc, c, cs, sn, x, nrm);
+    if (!(phi < bc->r[11])) continue;
+    real vb[3] = {bc->r[3], bc->r[4], bc->r[5]};
+    vb[P] = (real)(vb[P] - (real)(omega * (real)(x[Q] - c[Q])));
+    vb[Q] = (real)(vb[Q] + (real)(omega * (real)(x[P] - c[P])));
+    real *q = s->node_moments_nt + (size_t)n * d;
+    real vr[3] = {0, 0, 0}, vn = 0;
+    for (int a = 0; a < d; a++) {
+      vr[a] = (real)((real)(q[a] / m) - vb[a]);
+      vn = (real)(vn + (real)(vr[a] * nrm[a]));
+    }
+    if (!(vn < 0)) continue;
+    real vt2 = 0;
+    for (int a = 0; a < d; a++) {
+      vr[a] = (real)(vr[a] - (real)(vn * nrm[a]));
+      vt2 = (real)(vt2 + (real)(vr[a] * vr[a]));
+    }
+    real vt = (real)RSQRT(vt2);
+    real scale = vt <= (real)(-mu * vn) ? (real)0 : (real)((real)1 + (real)((real)(mu * vn) / vt));
+    for (int a = 0; a < d; a++) q[a] = (real)((real)(vb[a] + (real)(vr[a] * scale)) * m);
+  }
+}
+
 /* USL::solve step 8 (src/solver/usl/usl.cpp:97-103): list order. */
 void or_apply_on_nodes_moments(or_sim *s) {
   for (int k = 0; k < s->num_bcs; k++) {
@@ -518,6 +779,8 @@ void or_apply_on_nodes_moments(or_sim *s) {
     if (bc->type == OR_BC_GRAVITY) gravity(s, bc);
     else if (bc->type == OR_BC_NODEDOMAIN) nodedomain(s, bc);
     else if (bc->type == OR_BC_BODYFORCE) bodyforce(s, bc);
+    else if (bc->type == OR_BC_RIGIDBODY_LEVELSET) rigid_nn(s, bc);
+    else if (bc->type == OR_BC_RIGID_SDF) rigid_sdf(s, bc);
   }
 }
 

@@ -46,7 +46,9 @@ enum {
   OR_BC_GRAVITY = 1,
   OR_BC_NODEDOMAIN = 2,
   OR_BC_BODYFORCE = 3,
-  OR_BC_PLANARDOMAIN = 4
+  OR_BC_PLANARDOMAIN = 4,
+  OR_BC_RIGIDBODY_LEVELSET = 5, /* reference mode: nearest rigid particle */
+  OR_BC_RIGID_SDF = 6           /* analytic body, Coulomb contact (no reference) */
 };
 
 /* Mirrors the reference Grid (include/pyroclastmpm/common/types_common.h:250-291). */
@@ -79,11 +81,18 @@ typedef struct {
  *   BODYFORCE:    i[0] mode_id (0 forces, 1 moments, 2 fixed), i[1] is_active,
  *                 values [nodes][dim], mask [nodes]
  *   PLANARDOMAIN: r[0..2] face0 friction (radians), r[3..5] face1 friction
+ *   RIGIDBODY_LEVELSET: i[0] mode (0 STATIC, 1 LOOP_ROTATE), i[1] corrected
+ *                 rotation, r[0..2] euler angles per second, r[3..5] COM,
+ *                 r[6..8] accumulated euler angles (state)
+ *   RIGID_SDF:    i[0] shape (0 sphere, 1 half-cylinder shell), i[1] axis,
+ *                 r[0..2] centre at step 0, r[3..5] velocity, r[6] angular
+ *                 velocity, r[7] friction, r[8..10] dims, r[11] contact
+ *                 distance, r[12] angle at step 0
  */
 typedef struct {
   int type;
   int i[8];
-  REAL r[12];
+  REAL r[16];
   const REAL *values;
   const unsigned char *mask;
 } or_bc;

@@ -54,7 +54,7 @@ class Material(ctypes.Structure):
 
 
 class BC(ctypes.Structure):
-    _fields_ = [("type", ctypes.c_int), ("ints", ctypes.c_int * 8), ("reals", ctypes.c_float * 12),
+    _fields_ = [("type", ctypes.c_int), ("ints", ctypes.c_int * 8), ("reals", ctypes.c_float * 16),
                 ("values", ctypes.c_void_p), ("mask", ctypes.c_void_p)]
 
 
@@ -76,7 +76,11 @@ EXPORTS = [
     "pmpm_num_surround_nodes", "pmpm_p2g", "pmpm_g2p", "pmpm_stress_update", "pmpm_solve",
     "pmpm_get_step", "pmpm_set_step", "pmpm_synchronize", "pmpm_stream", "pmpm_material_point_update",
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
+    "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
 ]
+
+RIGID_MODES = {"static": 0, "loop_rotate": 1}
+SDF_SHAPES = {"sphere": 0, "half_cylinder_shell": 1}
 
 _lib = None
 
@@ -103,6 +107,10 @@ def lib():
                                      ctypes.POINTER(BC)]
     L.pmpm_bc_bodyforce.argtypes = [i, fp, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(BC)]
     L.pmpm_bc_planardomain.argtypes = [fp, fp, i, ctypes.POINTER(BC)]
+    L.pmpm_bc_rigidbodylevelset.argtypes = [i, fp, fp, i, i, ctypes.POINTER(BC)]
+    L.pmpm_bc_rigid_sdf.argtypes = [i, i, fp, fp, f, f, fp, f, f, i, ctypes.POINTER(BC)]
+    L.pmpm_calculate_timestep.argtypes = [f, f, f, f, f, fp]
+    L.pmpm_material_timestep.argtypes = [ctypes.POINTER(Material), f, f, fp]
     L.pmpm_create.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(vp)]
     L.pmpm_destroy.argtypes = [vp]
     L.pmpm_get_grid.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), fp]
@@ -198,9 +206,38 @@ def make_bc(b: dict, dim: int, num_nodes: int, keep: list) -> BC:
     elif t == "PlanarDomain":
         check(L.pmpm_bc_planardomain(_f3(b.get("face0_friction", [0.0] * dim)),
                                      _f3(b.get("face1_friction", [0.0] * dim)), dim, ctypes.byref(out)), "bc")
+    elif t == "RigidBodyLevelSet" and "shape" not in b:
+        check(L.pmpm_bc_rigidbodylevelset(RIGID_MODES[b.get("mode", "static")],
+                                          _f3(b.get("euler_angles_per_second", [0.0] * dim)),
+                                          _f3(b.get("COM", [0.0] * dim)),
+                                          1 if b.get("corrected_rotation", False) else 0, dim,
+                                          ctypes.byref(out)), "bc")
+    elif t == "RigidBodyLevelSet":
+        check(L.pmpm_bc_rigid_sdf(SDF_SHAPES[b["shape"]], int(b.get("axis", 2)), _f3(b["center"]),
+                                  _f3(b.get("velocity", [0.0] * dim)), float(b.get("angular_velocity", 0.0)),
+                                  float(b.get("angle", 0.0)), _f3(b["dims"]), float(b.get("friction", 0.0)),
+                                  float(b.get("contact_distance", 0.0)), dim, ctypes.byref(out)), "bc")
     else:
         raise ValueError(f"unknown boundary condition {t}")
     return out
+
+
+def calculate_timestep(cell_size, factor, bulk_modulus, shear_modulus, density):
+    """tools::calculate_timestep (src/common/tools.cpp:373-380)."""
+    out = ctypes.c_float()
+    check(lib().pmpm_calculate_timestep(float(cell_size), float(factor), float(bulk_modulus),
+                                        float(shear_modulus), float(density), ctypes.byref(out)),
+          "pmpm_calculate_timestep")
+    return out.value
+
+
+def material_timestep(material: dict, cell_size, factor):
+    """<Material>::calculate_timestep (src/materials/linearelastic.cpp:96-105) for a material dict."""
+    out = ctypes.c_float()
+    m = make_material(material)
+    check(lib().pmpm_material_timestep(ctypes.byref(m), float(cell_size), float(factor), ctypes.byref(out)),
+          "pmpm_material_timestep")
+    return out.value
 
 
 def field_shape(name, dim, n, num_nodes, nsn=None):

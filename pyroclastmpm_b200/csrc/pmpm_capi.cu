@@ -68,6 +68,21 @@ struct GravityState {
   float current[3];
 };
 
+// RigidBodyLevelSet in the reference's mode: animation state of
+// RigidBodyLevelSet::update_animation (src/boundaryconditions/rigidbodylevelset.cpp:127-206).
+struct RigidState {
+  int mode = PMPM_RIGID_STATIC, corrected = 0;
+  float rate[3] = {0, 0, 0};   // euler_angles_per_second
+  float com[3] = {0, 0, 0};
+  float euler[3] = {0, 0, 0};  // accumulated euler angles
+};
+
+// Analytic rigid body: pose at step 0 and its motion.
+struct SdfState {
+  int bc_index;
+  double c0[3], v[3], omega, angle0;
+};
+
 }  // namespace
 
 struct pmpm_sim {
@@ -85,6 +100,10 @@ struct pmpm_sim {
   std::vector<float *> bc_values;
   std::vector<uint8_t *> bc_masks;
   std::vector<GravityState> gravity;
+  int rbls_index = -1;  // the nearest-rigid-particle RigidBodyLevelSet in the BC list
+  RigidState rigid;
+  std::vector<SdfState> sdf;
+  bool rigid_shift_pending = false;  // the next G2P moves rigid particles by their set velocity
   bool has_planar = false, has_dp = false, has_sref = false;
 
   // particles (two storage sets, swapped by the physical re-sort)
@@ -204,6 +223,8 @@ StepArgs make_args(pmpm_sim *s) {
   a.fault = s->fault;
   a.nmat = (int)s->mats.size();
   a.nbc = (int)s->bcs.size();
+  a.nbc_epi = s->rbls_index >= 0 ? s->rbls_index : a.nbc;
+  a.rigid_shift = s->rigid_shift_pending ? 1 : 0;
   a.has_planar = s->has_planar ? 1 : 0;
   a.has_sref = s->has_sref ? 1 : 0;
   for (int k = 0; k < a.nmat; k++) a.mat[k] = s->mats[k];
@@ -223,6 +244,87 @@ void update_gravity(pmpm_sim *s) {
     if (is_ramp && s->step < ramp_step)
       for (int c = 0; c < 3; c++) gs.current[c] = bc.r[3 + c] * ramp_factor;
   }
+}
+
+// Pose of the analytic rigid bodies at the current step (time step * dt).
+void update_bodies(pmpm_sim *s) {
+  const double t = (double)s->step * (double)s->dt;
+  for (const SdfState &b : s->sdf) {
+    DevBC &bc = s->bcs[b.bc_index];
+    for (int c = 0; c < 3; c++) bc.r[c] = (float)(b.c0[c] + b.v[c] * t);
+    const double ang = b.angle0 + b.omega * t;
+    bc.r[12] = (float)std::cos(ang);
+    bc.r[13] = (float)std::sin(ang);
+  }
+}
+
+// 3x3 product in Eigen's coefficient order: ((a0 b0 + a1 b1) + a2 b2).
+void matmul3(const float *A, const float *B, float *C) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) C[3 * i + j] = (A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j]) + A[3 * i + 2] * B[6 + j];
+}
+
+// RigidBodyLevelSet::update_animation (src/boundaryconditions/rigidbodylevelset.cpp:
+// 127-206): LOOP_ROTATE advances the euler angles by rate * dt and rotates by
+// delta = previous - new.  The reference's 3D matrices are kept by default:
+// Rx carries both the 2D and the 3D entries and Rz stays zero, so R = Rz Ry Rx
+// is zero; `corrected` builds the proper Rz(d2) Ry(d1) Rx(d0).  STATIC: the
+// reference leaves R unset; the identity is used (rigid velocity zero).
+void rigid_rotation(pmpm_sim *s, float *R) {
+  const int D = s->dim;
+  RigidState &r = s->rigid;
+  float R3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (r.mode == PMPM_RIGID_LOOP_ROTATE) {
+    float d[3];
+    for (int c = 0; c < 3; c++) {
+      const float prev = r.euler[c];
+      r.euler[c] = r.euler[c] + r.rate[c] * s->dt;
+      d[c] = prev - r.euler[c];
+    }
+    const float c0 = std::cos(d[0]), s0 = std::sin(d[0]);
+    const float c1 = std::cos(d[1]), s1 = std::sin(d[1]);
+    const float c2 = std::cos(d[2]), s2 = std::sin(d[2]);
+    if (D == 2) {
+      const float M[9] = {c0, -s0, 0, s0, c0, 0, 0, 0, 1};
+      memcpy(R3, M, sizeof(R3));
+    } else if (!r.corrected) {
+      const float Rx[9] = {1, -s0, 0, s0, c2, -s2, 0, s2, c2};
+      const float Ry[9] = {c1, 0, s1, 0, 1, 0, -s1, 0, c1};
+      const float Rz[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      float T[9];
+      matmul3(Rz, Ry, T);
+      matmul3(T, Rx, R3);
+    } else {
+      const float Rx[9] = {1, 0, 0, 0, c0, -s0, 0, s0, c0};
+      const float Ry[9] = {c1, 0, s1, 0, 1, 0, -s1, 0, c1};
+      const float Rz[9] = {c2, -s2, 0, s2, c2, 0, 0, 0, 1};
+      float T[9];
+      matmul3(Rz, Ry, T);
+      matmul3(T, Rx, R3);
+    }
+  }
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) R[i * D + j] = R3[3 * i + j];
+}
+
+// The nearest-rigid-particle RigidBodyLevelSet after P2G: rigid velocities,
+// then node contact and the node BCs listed after it; G2P then also moves
+// the rigid particles by their set velocity.
+template <int D>
+int launch_rigid(pmpm_sim *s) {
+  if (s->rbls_index < 0) return PMPM_OK;
+  RigidMotion rm;
+  memset(&rm, 0, sizeof(rm));
+  rigid_rotation(s, rm.R);
+  for (int c = 0; c < 3; c++) rm.com[c] = s->rigid.com[c];
+  StepArgs a = make_args(s);
+  k_rigid_velocity<D><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, rm);
+  PMPM_LAUNCHED();
+  k_rigid_nodes<D><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, s->rbls_index);
+  PMPM_LAUNCHED();
+  s->launches += 2;
+  s->rigid_shift_pending = true;
+  return PMPM_OK;
 }
 
 template <int D, int SF>
@@ -264,7 +366,10 @@ int launch_reorder(pmpm_sim *s) {
 
 template <int D, int SF>
 int launch_p2g(pmpm_sim *s, int apply_bcs) {
-  if (apply_bcs) update_gravity(s);
+  if (apply_bcs) {
+    update_gravity(s);
+    update_bodies(s);
+  }
   StepArgs a = make_args(s);
   if (s->flags & PMPM_FLAG_DETERMINISTIC) {
     k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
@@ -292,6 +397,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   PMPM_LAUNCHED();
   s->launches += 1;
   s->p2g_epoch = s->epoch;
+  if (apply_bcs) PMPM_TRY(launch_rigid<D>(s));
   return PMPM_OK;
 }
 
@@ -301,6 +407,7 @@ int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
   k_g2p<D, SF><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
   PMPM_LAUNCHED();
   s->launches += 1;
+  s->rigid_shift_pending = false;
   return PMPM_OK;
 }
 
@@ -709,6 +816,68 @@ int pmpm_bc_planardomain(const float *face0_friction_deg, const float *face1_fri
   return PMPM_OK;
 }
 
+int pmpm_bc_rigidbodylevelset(int mode, const float *euler_angles_per_second, const float *com,
+                              int corrected_rotation, int dim, pmpm_bc *out) {
+  if (!out || dim < 2 || dim > 3 || (mode != PMPM_RIGID_STATIC && mode != PMPM_RIGID_LOOP_ROTATE))
+    return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_BC_RIGIDBODY_LEVELSET;
+  out->ints[0] = mode;
+  out->ints[1] = corrected_rotation ? 1 : 0;
+  for (int c = 0; c < dim; c++) {
+    out->reals[c] = euler_angles_per_second ? euler_angles_per_second[c] : 0.0f;
+    out->reals[3 + c] = com ? com[c] : 0.0f;
+  }
+  return PMPM_OK;
+}
+
+int pmpm_bc_rigid_sdf(int shape, int axis, const float *center, const float *velocity, float angular_velocity,
+                      float angle0, const float *dims, float friction, float contact_distance, int dim,
+                      pmpm_bc *out) {
+  if (!out || !center || !dims || dim < 2 || dim > 3 || axis < 0 || axis > 2 ||
+      (shape != PMPM_SDF_SPHERE && shape != PMPM_SDF_HALF_CYLINDER_SHELL) || !(friction >= 0.0f))
+    return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_BC_RIGID_SDF;
+  out->ints[0] = shape;
+  out->ints[1] = dim == 2 ? 2 : axis;
+  for (int c = 0; c < dim; c++) {
+    out->reals[c] = center[c];
+    out->reals[3 + c] = velocity ? velocity[c] : 0.0f;
+  }
+  out->reals[6] = angular_velocity;
+  out->reals[7] = friction;
+  for (int c = 0; c < 3; c++) out->reals[8 + c] = dims[c];
+  if (shape == PMPM_SDF_SPHERE) out->reals[9] = out->reals[10] = 0.0f;
+  out->reals[11] = contact_distance;
+  out->reals[12] = angle0;
+  return PMPM_OK;
+}
+
+int pmpm_calculate_timestep(float cell_size, float factor, float bulk_modulus, float shear_modulus,
+                            float density, float *dt) {
+  if (!dt || !(density > 0.0f) || !(cell_size > 0.0f)) return PMPM_ERR_INVALID_ARGUMENT;
+  // c = (Real)sqrt((K + 4. G / 3.) / rho) in double, as the reference
+  const float c = (float)std::sqrt(((double)bulk_modulus + 4.0 * (double)shear_modulus / 3.0) / (double)density);
+  if (!(c > 0.0f)) return PMPM_ERR_INVALID_ARGUMENT;
+  *dt = factor * (cell_size / c);
+  return PMPM_OK;
+}
+
+int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float factor, float *dt) {
+  if (!mat) return PMPM_ERR_INVALID_ARGUMENT;
+  switch (mat->type) {
+    case PMPM_MAT_LINEAR_ELASTIC:
+      return pmpm_calculate_timestep(cell_size, factor, mat->params[4], mat->params[3], mat->density, dt);
+    case PMPM_MAT_NEWTON_FLUID:
+      return pmpm_calculate_timestep(cell_size, factor, mat->params[1], 0.0f, mat->density, dt);
+    case PMPM_MAT_DRUCKER_PRAGER:
+      return pmpm_calculate_timestep(cell_size, factor, mat->params[0], mat->params[1], mat->density, dt);
+    default:
+      return PMPM_ERR_NOT_SUPPORTED;
+  }
+}
+
 int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (!desc || !out) return PMPM_ERR_INVALID_ARGUMENT;
   *out = nullptr;
@@ -815,6 +984,41 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
       db.mask = mask;
     } else if (b.type == PMPM_BC_PLANARDOMAIN) {
       s->has_planar = true;
+    } else if (b.type == PMPM_BC_RIGIDBODY_LEVELSET) {
+      // the reference hard-codes the linear window (rigidbodylevelset_inline.h:88-101)
+      if (s->rbls_index >= 0 || s->shape != PMPM_SHAPE_LINEAR) {
+        st = PMPM_ERR_NOT_SUPPORTED;
+        break;
+      }
+      if (b.ints[0] != PMPM_RIGID_STATIC && b.ints[0] != PMPM_RIGID_LOOP_ROTATE) {
+        st = PMPM_ERR_INVALID_ARGUMENT;
+        break;
+      }
+      s->rbls_index = k;
+      s->rigid.mode = b.ints[0];
+      s->rigid.corrected = b.ints[1] ? 1 : 0;
+      for (int c = 0; c < 3; c++) {
+        s->rigid.rate[c] = b.reals[c];
+        s->rigid.com[c] = b.reals[3 + c];
+      }
+    } else if (b.type == PMPM_BC_RIGID_SDF) {
+      const int shape = b.ints[0], axis = b.ints[1];
+      const bool dims_ok = b.reals[8] > 0.0f && (shape == PMPM_SDF_SPHERE || (b.reals[9] > 0.0f && b.reals[10] > 0.0f));
+      if ((shape != PMPM_SDF_SPHERE && shape != PMPM_SDF_HALF_CYLINDER_SHELL) || axis < 0 || axis > 2 || !dims_ok ||
+          !(b.reals[7] >= 0.0f)) {
+        st = PMPM_ERR_INVALID_ARGUMENT;
+        break;
+      }
+      SdfState sd;
+      sd.bc_index = k;
+      for (int c = 0; c < 3; c++) {
+        sd.c0[c] = c < s->dim ? b.reals[c] : 0.0;
+        sd.v[c] = c < s->dim ? b.reals[3 + c] : 0.0;
+        db.r[3 + c] = (float)sd.v[c];
+      }
+      sd.omega = b.reals[6];
+      sd.angle0 = b.reals[12];
+      s->sdf.push_back(sd);
     } else if (b.type != PMPM_BC_NODEDOMAIN) {
       st = PMPM_ERR_INVALID_ARGUMENT;
     }
@@ -1264,7 +1468,7 @@ int profile_step(pmpm_sim *s, float *ms, int *launches) {
   }
   PMPM_CUDA(cudaEventRecord(ev[1], s->stream));
   PMPM_TRY((launch_p2g<D, SF>(s, 1)));
-  n_launch += 1;
+  n_launch += s->rbls_index >= 0 ? 3 : 1;
   PMPM_CUDA(cudaEventRecord(ev[2], s->stream));
   const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
   PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));

@@ -102,7 +102,9 @@ struct DevMaterial {
 struct DevBC {
   int type;
   int i[8];
-  float r[12];  // gravity: r[0..2] is the gravity in force this step
+  // gravity: r[0..2] is the gravity in force this step; rigid SDF body:
+  // r[0..2] centre this step, r[12..13] cos and sin of its angle this step
+  float r[16];
   const float *values;
   const uint8_t *mask;
 };
@@ -118,6 +120,8 @@ struct StepArgs {
   int *fault;
   int nmat;
   int nbc;
+  int nbc_epi;      // node BCs [0, nbc_epi) run in the P2G epilogue, the rest after the rigid pass
+  int rigid_shift;  // G2P also moves rigid particles by their set velocity (RigidBodyLevelSet)
   int has_planar;
   int has_sref;
   DevMaterial mat[kMaxMat];
@@ -522,6 +526,113 @@ __device__ __forceinline__ void write_node(const StepArgs &a, int node, float ma
   }
 }
 
+// Analytic rigid body of a PMPM_BC_RIGID_SDF condition: signed distance of
+// world point x and the outward unit normal there.  The cross-section plane
+// is (P, Q) with P = axis+1, Q = axis+2 (cyclic) in 3D and (x, y) in 2D; the
+// body's local frame is turned by its angle about the axis.  Shell: the half
+// q <= 0 of the annulus |rho - R| <= t/2 in local coordinates, ends rounded
+// with radius t/2, extruded to length L along the axis in 3D.
+template <int D>
+__device__ __forceinline__ float rigid_sdf(const DevBC &bc, const float x[3], float nrm[3]) {
+  const int A = D == 3 ? bc.i[1] : 2;
+  const int P = D == 3 ? (A + 1) % 3 : 0, Q = D == 3 ? (A + 2) % 3 : 1;
+  float d[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int c = 0; c < D; c++) d[c] = x[c] - bc.r[c];
+  nrm[0] = nrm[1] = nrm[2] = 0.0f;
+  if (bc.i[0] == PMPM_SDF_SPHERE) {
+    float r2 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < D; c++) r2 += d[c] * d[c];
+    const float r = sqrtf(r2);
+    if (r > 0.0f) {
+#pragma unroll
+      for (int c = 0; c < D; c++) nrm[c] = d[c] / r;
+    } else {
+      nrm[Q] = 1.0f;
+    }
+    return r - bc.r[8];
+  }
+  const float cs = bc.r[12], sn = bc.r[13];
+  const float lp = cs * d[P] + sn * d[Q], lq = cs * d[Q] - sn * d[P];
+  const float R = bc.r[8], ht = 0.5f * bc.r[9];
+  float phi2, gp = 0.0f, gq = 1.0f;
+  if (lq <= 0.0f) {
+    const float rho = sqrtf(lp * lp + lq * lq);
+    phi2 = fabsf(rho - R) - ht;
+    if (rho > 0.0f) {
+      const float sg = rho >= R ? 1.0f : -1.0f;
+      gp = sg * lp / rho;
+      gq = sg * lq / rho;
+    }
+  } else {
+    const float wp = lp - (lp >= 0.0f ? R : -R), wq = lq;
+    const float w = sqrtf(wp * wp + wq * wq);
+    phi2 = w - ht;
+    if (w > 0.0f) {
+      gp = wp / w;
+      gq = wq / w;
+    }
+  }
+  float phi = phi2, ga = 0.0f;
+  if (D == 3) {
+    const float la = d[A];
+    const float hA = fabsf(la) - 0.5f * bc.r[10];
+    const float sa = la >= 0.0f ? 1.0f : -1.0f;
+    if (phi2 > 0.0f && hA > 0.0f) {
+      phi = sqrtf(phi2 * phi2 + hA * hA);
+      gp = phi2 * gp / phi;
+      gq = phi2 * gq / phi;
+      ga = hA * sa / phi;
+    } else if (hA > phi2) {
+      phi = hA;
+      gp = gq = 0.0f;
+      ga = sa;
+    }
+  }
+  nrm[P] = cs * gp - sn * gq;
+  nrm[Q] = sn * gp + cs * gq;
+  if (D == 3) nrm[A] = ga;
+  return phi;
+}
+
+// Coulomb contact of a node's forward moments with an analytic rigid body.
+template <int D>
+__device__ __forceinline__ void rigid_sdf_contact(const StepArgs &a, const DevBC &bc, const int nc[3], float m,
+                                                  float pnt[3]) {
+  float x[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int c = 0; c < D; c++) x[c] = __fadd_rn(a.g.origin[c], __fmul_rn((float)nc[c], a.g.h));
+  float nrm[3];
+  const float phi = rigid_sdf<D>(bc, x, nrm);
+  if (!(phi < bc.r[11])) return;
+  const int A = D == 3 ? bc.i[1] : 2;
+  const int P = D == 3 ? (A + 1) % 3 : 0, Q = D == 3 ? (A + 2) % 3 : 1;
+  float vb[3] = {bc.r[3], bc.r[4], bc.r[5]};
+  const float w = bc.r[6];
+  vb[P] -= w * (x[Q] - bc.r[Q]);
+  vb[Q] += w * (x[P] - bc.r[P]);
+  float vr[3] = {0.0f, 0.0f, 0.0f};
+  float vn = 0.0f;
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    vr[c] = pnt[c] / m - vb[c];
+    vn += vr[c] * nrm[c];
+  }
+  if (!(vn < 0.0f)) return;
+  float vt2 = 0.0f;
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    vr[c] -= vn * nrm[c];
+    vt2 += vr[c] * vr[c];
+  }
+  const float vt = sqrtf(vt2);
+  const float mu = bc.r[7];
+  const float scale = vt <= -mu * vn ? 0.0f : 1.0f + mu * vn / vt;
+#pragma unroll
+  for (int c = 0; c < D; c++) pnt[c] = (vb[c] + vr[c] * scale) * m;
+}
+
 // Applies the node boundary conditions in list order to (p, pnt) of node
 // `node` with coordinates nc and mass m:
 //   Gravity    (src/boundaryconditions/gravity_inline.h:46-63): pnt += g m dt, m > 1e-9
@@ -530,10 +641,11 @@ __device__ __forceinline__ void write_node(const StepArgs &a, int node, float ma
 //              vectors, mode 1 clamps the normal component
 //   BodyForce  (src/boundaryconditions/bodyforce_inline.h:41-59): masked nodes;
 //              "fixed" sets pnt, other modes add to p
+//   rigid SDF  m > 1e-9: Coulomb contact of pnt with the analytic body
 template <int D>
-__device__ __forceinline__ void node_bcs(const StepArgs &a, int node, const int nc[3], float m, float p[3],
-                                         float pnt[3]) {
-  for (int k = 0; k < a.nbc; k++) {
+__device__ __forceinline__ void node_bcs_range(const StepArgs &a, int node, const int nc[3], float m, float p[3],
+                                               float pnt[3], int k0, int k1) {
+  for (int k = k0; k < k1; k++) {
     const DevBC &bc = a.bc[k];
     if (bc.type == PMPM_BC_GRAVITY) {
       if (m > 0.000000001f) {
@@ -573,8 +685,18 @@ __device__ __forceinline__ void node_bcs(const StepArgs &a, int node, const int 
           for (int c = 0; c < D; c++) p[c] += bc.values[(size_t)node * D + c];
         }
       }
+    } else if (bc.type == PMPM_BC_RIGID_SDF) {
+      if (m > 0.000000001f) rigid_sdf_contact<D>(a, bc, nc, m, pnt);
     }
   }
+}
+
+// The node boundary conditions of the P2G epilogue: the list up to the first
+// nearest-rigid-particle RigidBodyLevelSet, which needs the finished grid.
+template <int D>
+__device__ __forceinline__ void node_bcs(const StepArgs &a, int node, const int nc[3], float m, float p[3],
+                                         float pnt[3]) {
+  node_bcs_range<D>(a, node, nc, m, p, pnt, 0, a.nbc_epi);
 }
 
 }  // namespace pmpm

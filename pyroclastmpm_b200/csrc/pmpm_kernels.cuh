@@ -537,6 +537,152 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int a
 }
 
 // --------------------------------------------------------------------------
+// RigidBodyLevelSet, reference mode: nearest rigid particle stick contact
+// --------------------------------------------------------------------------
+
+struct RigidMotion {
+  float R[9];  // row-major D x D rotation of this step
+  float com[3];
+};
+
+// RigidBodyLevelSet::set_velocities, CPU branch, and update_rigid_velocity
+// (src/boundaryconditions/rigidbodylevelset.cpp:245-275, rigidbodylevelset_inline.h:
+// 240-299): v = (R (x - COM) - (x - COM)) / dt for rigid particles.
+template <int D>
+__global__ void __launch_bounds__(256) k_rigid_velocity(StepArgs a, RigidMotion rm) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const DevParticles &P = a.P;
+  if (s >= P.n || !P.rigid[s]) return;
+  const int st = P.stride;
+  float r[3];
+#pragma unroll
+  for (int c = 0; c < D; c++) r[c] = __fsub_rn(P.x[c * st + s], rm.com[c]);
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    float u = __fmul_rn(rm.R[i * D], r[0]);
+#pragma unroll
+    for (int j = 1; j < D; j++) u = __fadd_rn(u, __fmul_rn(rm.R[i * D + j], r[j]));
+    P.v[i * st + s] = __fdiv_rn(__fsub_rn(u, r[i]), a.dt);
+  }
+}
+
+// calculate_grid_normals_nn_rigid (src/boundaryconditions/rigidbodylevelset_inline.h:
+// 65-199) for the nodes of the active tiles, then the node BCs listed after
+// it.  Per node with m > 1e-9: over the linear P2G window cells (slot order,
+// flattened index with the reference's single unsigned range check), the
+// rigid particle nearest to its cell's corner (first strict minimum) gives
+// the body velocity; the mass-weighted sum of the non-rigid particles' shape
+// function gradients, normalised, the normal; p and p_nt each stick to the
+// body velocity when (v - v_body) . n >= 0.  Linear shape functions only.
+template <int D>
+__global__ void __launch_bounds__(TileDims<D>::N) k_rigid_nodes(StepArgs a, int rb) {
+  using T = TileDims<D>;
+  const DevGrid &g = a.g;
+  const DevParticles &P = a.P;
+  const int tile = blockIdx.x;
+  if (a.N.tile_epoch[tile] != a.epoch) return;
+  const int tx = tile % g.tdim[0], ty = (tile / g.tdim[0]) % g.tdim[1], tz = tile / (g.tdim[0] * g.tdim[1]);
+  const int lx = threadIdx.x % T::X, ly = (threadIdx.x / T::X) % T::Y, lz = threadIdx.x / (T::X * T::Y);
+  const int nc[3] = {tx * T::X + lx, ty * T::Y + ly, D == 3 ? tz * T::Z + lz : 0};
+  if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) return;
+  const int node = flat_index(g, nc[0], nc[1], nc[2]);
+  const int nt = g.ntotal, st = P.stride;
+  float m = a.N.m[node];
+  float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    p[c] = a.N.p[c * nt + node];
+    pnt[c] = a.N.pnt[c * nt + node];
+  }
+  if (m > 0.000000001f) {
+    float min_dist = 999999999999999.0f;
+    int min_s = -1;
+    float nrm[3] = {0.0f, 0.0f, 0.0f};
+    constexpr int NS = D == 3 ? 8 : 4;
+    for (int sid = 0; sid < NS; sid++) {
+      int w[3];
+      window_offset<D, PMPM_SHAPE_LINEAR>(sid, w);  // g2p offset; the cell is node - w
+      const int cell = node - (w[0] + w[1] * g.n[0] + w[2] * g.n[0] * g.n[1]);
+      if ((unsigned)cell >= (unsigned)nt) continue;
+      for (int k = a.B.offset[cell]; k < a.B.offset[cell + 1]; k++) {
+        const int s = a.B.order[k];
+        float u[3];
+#pragma unroll
+        for (int c = 0; c < D; c++) u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+        if (P.rigid[s]) {
+          float dist = 0.0f;
+#pragma unroll
+          for (int c = 0; c < D; c++) {
+            const float rel = __fsub_rn(u[c], (float)(nc[c] - w[c]));
+            dist = c == 0 ? __fmul_rn(rel, rel) : __fadd_rn(dist, __fmul_rn(rel, rel));
+          }
+          if (dist < min_dist) {
+            min_dist = dist;
+            min_s = s;
+          }
+        } else {
+          // the particle's gradient for slot sid: node (own bin + w), zero
+          // where that node is outside the flattened range
+          int b[3];
+#pragma unroll
+          for (int c = 0; c < D; c++) b[c] = (int)u[c];
+          const int tgt = flat_index(g, b[0] + w[0], b[1] + w[1], D == 3 ? b[2] + w[2] : 0);
+          if ((unsigned)tgt >= (unsigned)nt) continue;
+          float N[3], dN[3];
+#pragma unroll
+          for (int c = 0; c < D; c++)
+            axis_weight<PMPM_SHAPE_LINEAR>(__fsub_rn(u[c], (float)(b[c] + w[c])), g.inv_h, 0, N[c], dN[c]);
+          float dpsi[3];
+          if (D == 2) {
+            dpsi[0] = __fmul_rn(dN[0], N[1]);
+            dpsi[1] = __fmul_rn(dN[1], N[0]);
+          } else {
+            dpsi[0] = __fmul_rn(__fmul_rn(dN[0], N[1]), N[2]);
+            dpsi[1] = __fmul_rn(__fmul_rn(dN[1], N[0]), N[2]);
+            dpsi[2] = __fmul_rn(__fmul_rn(dN[2], N[0]), N[1]);
+          }
+          const float mp = P.m[s];
+#pragma unroll
+          for (int c = 0; c < D; c++) nrm[c] = __fadd_rn(nrm[c], __fmul_rn(dpsi[c], mp));
+        }
+      }
+    }
+    if (min_s >= 0) {
+      float sq = __fmul_rn(nrm[0], nrm[0]);
+#pragma unroll
+      for (int c = 1; c < D; c++) sq = __fadd_rn(sq, __fmul_rn(nrm[c], nrm[c]));
+      if (sq > 0.0f) {
+        const float len = __fsqrt_rn(sq);
+#pragma unroll
+        for (int c = 0; c < D; c++) nrm[c] = __fdiv_rn(nrm[c], len);
+      }
+      float vn[3], vnt[3], cv[3], cvt[3];
+      float rel = 0.0f, rel_nt = 0.0f;
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        const float vb = P.v[c * st + min_s];
+        vn[c] = __fdiv_rn(p[c], m);
+        vnt[c] = __fdiv_rn(pnt[c], m);
+        cv[c] = __fsub_rn(vn[c], vb);
+        cvt[c] = __fsub_rn(vnt[c], vb);
+        rel = c == 0 ? __fmul_rn(cv[c], nrm[c]) : __fadd_rn(rel, __fmul_rn(cv[c], nrm[c]));
+        rel_nt = c == 0 ? __fmul_rn(cvt[c], nrm[c]) : __fadd_rn(rel_nt, __fmul_rn(cvt[c], nrm[c]));
+      }
+      if (rel >= 0.0f) {
+#pragma unroll
+        for (int c = 0; c < D; c++) p[c] = __fmul_rn(__fsub_rn(vn[c], cv[c]), m);
+      }
+      if (rel_nt >= 0.0f) {
+#pragma unroll
+        for (int c = 0; c < D; c++) pnt[c] = __fmul_rn(__fsub_rn(vnt[c], cvt[c]), m);
+      }
+    }
+  }
+  node_bcs_range<D>(a, node, nc, m, p, pnt, rb + 1, a.nbc);
+  write_node<D>(a, node, m, p, pnt, m > a.cutoff);
+}
+
+// --------------------------------------------------------------------------
 // P2G, fast path: tile scatter into shared memory
 // --------------------------------------------------------------------------
 //
@@ -1591,10 +1737,15 @@ __global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int stor
         Fn[r * D + c] = acc;
       }
     bool finite = true;
+    // RigidBodyLevelSet::set_position (rigidbodylevelset.cpp:222-243) moved
+    // rigid particles by their set velocity before G2P; their weights above
+    // are those of the unmoved position, as the reference's stored psi
+    const bool shift = a.rigid_shift && P.rigid[s];
 #pragma unroll
     for (int c = 0; c < D; c++) {
       const float vnew = a.one_minus_alpha * vinc[c] + a.alpha * (v[c] + dvinc[c]);
-      const float xnew = x[c] + a.dt * vinc[c];
+      const float x0 = shift ? __fadd_rn(x[c], __fmul_rn(v[c], a.dt)) : x[c];
+      const float xnew = x0 + a.dt * vinc[c];
       P.v[c * st + s] = vnew;
       P.x[c * st + s] = xnew;
       finite = finite && isfinite(xnew);

@@ -78,9 +78,21 @@ def granular_column(domain=(1.0, 0.25, 0.5), cell_size=1.0 / 256, column=(0.2, 0
                 positions=pts, velocities=np.zeros_like(pts))
 
 
+def scoop(center=(0.15, 0.25, 0.3), radius=0.15, thickness=0.01, length=0.4, velocity=(0.5, 0.0, 0.0),
+          angular_velocity=1.0, friction=0.3, angle=0.0, axis=1):
+    """Half-cylinder shell rigid body (RigidBodyLevelSet with an analytic
+    signed distance): axis along y, the shell on the -x side of its axis at
+    angle 0 (open towards +x), translating and turning about its axis."""
+    return {"type": "RigidBodyLevelSet", "shape": "half_cylinder_shell", "axis": axis, "center": list(center),
+            "velocity": list(velocity), "angular_velocity": angular_velocity, "angle": angle,
+            "dims": [radius, thickness, length], "friction": friction, "contact_distance": 0.0}
+
+
 def granular_bed(domain=(1.5, 0.6, 0.8), cell_size=1.0 / 160, bed=(1.0, 0.5, 0.3), ppc_1d=2, jitter=0.25,
-                 seed=1, shape_function="cubic", dt=8e-6, scale=1.0, **kw):
-    """3D granular bed (the scoop configuration's particle set)."""
+                 seed=1, shape_function="cubic", dt=8e-6, scale=1.0, with_scoop=True, **kw):
+    """3D granular bed dug by a translating, turning half-cylinder scoop
+    (R 0.15, t 0.01, L 0.4, 0.5 m/s in x, 1 rad/s, Coulomb 0.3); Drucker-Prager,
+    gravity, slip walls."""
     spacing = cell_size / ppc_1d
     b = np.asarray(bed, np.float64) * scale
     pts = _lattice(np.zeros(3), b, spacing)
@@ -88,6 +100,11 @@ def granular_bed(domain=(1.5, 0.6, 0.8), cell_size=1.0 / 160, bed=(1.0, 0.5, 0.3
     pts = pts + rng.uniform(-jitter * spacing, jitter * spacing, size=pts.shape)
     d = granular_column(domain=domain, cell_size=cell_size, shape_function=shape_function, dt=dt, **kw)
     d.update(positions=pts, velocities=np.zeros_like(pts))
+    if with_scoop:
+        top = float(b[2])
+        body = scoop(center=(0.15 * scale, 0.5 * float(b[1]), top), radius=0.15 * scale,
+                     thickness=max(0.01 * scale, 1.5 * cell_size), length=0.8 * float(b[1]))
+        d["bcs"] = [d["bcs"][0], body, d["bcs"][1]]
     return d
 
 

@@ -29,11 +29,17 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
 
 
+def particle_kwargs(scene):
+    """Particle arrays of a scene (rigid particles follow the others)."""
+    return dict(positions=scene["positions"], velocities=scene["velocities"], colors=scene.get("colors"),
+                rigid_positions=scene.get("rigid_positions"), rigid_velocities=scene.get("rigid_velocities"),
+                rigid_colors=scene.get("rigid_colors"))
+
+
 def cond_tol(scene, steps, names, base):
     """Per-field tolerance: base, or 3x the FP32-vs-FP64 oracle distance."""
     kw = scenes.sim_kwargs(scene)
-    o = [oracle.OracleSim(**kw, positions=scene["positions"], velocities=scene["velocities"],
-                          colors=scene.get("colors"), precision=p).initialize() for p in ("f32", "f64")]
+    o = [oracle.OracleSim(**kw, **particle_kwargs(scene), precision=p).initialize() for p in ("f32", "f64")]
     for x in o:
         x.solve(steps)
     return {n: max(base, 3.0 * rel(o[0][n], o[1][n])) for n in names}
@@ -49,9 +55,8 @@ def perturbed(scene, amount=0.01, seed=5):
 def make_pair(scene, precision="f32", **extra):
     kw = scenes.sim_kwargs(scene)
     sim = Simulation(**kw, **extra)
-    sim.set_particles(scene["positions"], scene["velocities"], scene.get("colors"))
-    ref = oracle.OracleSim(**kw, positions=scene["positions"], velocities=scene["velocities"],
-                           colors=scene.get("colors"), precision=precision)
+    sim.set_particles(**particle_kwargs(scene))
+    ref = oracle.OracleSim(**kw, **particle_kwargs(scene), precision=precision)
     return sim, ref
 
 
@@ -252,6 +257,78 @@ STEP_CASES = {
         bcs=[{"type": "PlanarDomain", "face0_friction": [10.0, 0.0, 5.0], "face1_friction": [0.0, 20.0, 0.0]}]),
 }
 
+def rigid_block_scene(dim, mode="static", rate=None, corrected=False, seed=7):
+    """A linear-elastic block driven into a block of rigid particles
+    (RigidBodyLevelSet in the reference's nearest-rigid-particle mode)."""
+    rng = np.random.default_rng(seed)
+    h = 0.05
+    sp = h / 2
+    lo, hi = np.full(dim, 0.3), np.full(dim, 0.5)
+    soft = scenes._lattice(lo, hi, sp)
+    soft = soft + rng.uniform(-0.2 * sp, 0.2 * sp, soft.shape)
+    rlo = lo.copy()
+    rlo[0] = 0.5
+    rhi = hi.copy()
+    rhi[0] = 0.6
+    rigid = scenes._lattice(rlo, rhi, sp)
+    v = np.zeros_like(soft)
+    v[:, 0] = 0.5
+    v += rng.normal(0, 0.02, v.shape)
+    com = list(0.5 * (rlo + rhi))
+    bc = {"type": "RigidBodyLevelSet", "mode": mode, "COM": com, "corrected_rotation": corrected,
+          "euler_angles_per_second": rate or [0.0] * dim}
+    return dict(dim=dim, origin=[0.0] * dim, end=[1.0] * dim, cell_size=h, shape_function="linear", dt=1e-3,
+                particles_per_cell=2 ** dim, alpha=0.99,
+                materials=[{"type": "LinearElastic", "density": 1000.0, "E": 1e4, "pois": 0.3},
+                           {"type": "Material", "density": 2000.0}],
+                bcs=[{"type": "Gravity", "gravity": [0.0, -9.81] + [0.0] * (dim - 2)}, bc,
+                     {"type": "NodeDomain", "face0_mode": [1] * dim, "face1_mode": [1] * dim}],
+                positions=soft, velocities=v, rigid_positions=rigid, rigid_colors=np.ones(len(rigid), np.uint8))
+
+
+def scoop_scene(dim, shape_function, shape="half_cylinder_shell", friction=0.3, seed=8, n_side=None):
+    """A Drucker-Prager bed with an analytic rigid body cutting into it,
+    translating and turning (RigidBodyLevelSet with a signed distance)."""
+    rng = np.random.default_rng(seed)
+    h = 0.05 if dim == 2 else 0.1
+    sp = h / 2
+    lo = np.zeros(dim)
+    hi = np.full(dim, 0.6)
+    hi[0] = 0.9
+    pts = scenes._lattice(lo, hi, sp) + 0.05
+    pts = pts + rng.uniform(-0.2 * sp, 0.2 * sp, pts.shape)
+    up = dim - 1
+    # geometry off the node lattice, so no node sits on the body's surface
+    c = [0.3137, 0.4871, 0.5][:dim]
+    c[up] = 0.6071
+    dims = [0.2513, 0.0617, 0.5129] if shape == "half_cylinder_shell" else [0.2213, 0.0, 0.0]
+    body = {"type": "RigidBodyLevelSet", "shape": shape, "axis": 1, "center": c,
+            "velocity": [0.5, 0.0, 0.0][:dim], "angular_velocity": 1.0, "angle": -0.3, "dims": dims,
+            "friction": friction, "contact_distance": 0.0}
+    g = [0.0] * dim
+    g[up] = -9.81
+    return dict(dim=dim, origin=[0.0] * dim, end=[1.0] * dim, cell_size=h, shape_function=shape_function,
+                dt=1e-4, particles_per_cell=2 ** dim, alpha=0.99,
+                materials=[{"type": "DruckerPrager", "density": 1500.0, "E": 1e6, "pois": 0.3,
+                            "friction_angle": 30.0, "cohesion": 100.0}],
+                bcs=[{"type": "Gravity", "gravity": g}, body,
+                     {"type": "NodeDomain", "face0_mode": [1] * dim, "face1_mode": [1] * dim}],
+                positions=pts, velocities=rng.normal(0, 0.05, pts.shape))
+
+
+STEP_CASES.update({
+    "rigid_nn_2d_static": lambda: rigid_block_scene(2),
+    "rigid_nn_2d_rotate": lambda: rigid_block_scene(2, "loop_rotate", [2.0, 0.0]),
+    "rigid_nn_3d_static": lambda: rigid_block_scene(3),
+    "rigid_nn_3d_rotate_reference": lambda: rigid_block_scene(3, "loop_rotate", [1e-4, 2e-4, 3e-4]),
+    "rigid_nn_3d_rotate_corrected": lambda: rigid_block_scene(3, "loop_rotate", [1.0, 2.0, 3.0], True),
+    "sdf_2d_quadratic_shell": lambda: scoop_scene(2, "quadratic"),
+    "sdf_2d_linear_sphere_frictionless": lambda: scoop_scene(2, "linear", "sphere", 0.0),
+    "sdf_3d_quadratic_shell": lambda: scoop_scene(3, "quadratic"),
+    "sdf_3d_cubic_sphere": lambda: scoop_scene(3, "cubic", "sphere", 0.5),
+    "sdf_3d_linear_shell_stick": lambda: scoop_scene(3, "linear", friction=100.0),
+})
+
 FIELDS = ("positions", "velocities", "stresses", "F", "volumes")
 
 
@@ -270,7 +347,8 @@ def test_one_step_matches_oracle(case):
         assert err <= tol[name], f"{case} {name}: {err:.3e} > {tol[name]:.1e}"
 
 
-@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "water_2d_quadratic_nf"])
+@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "water_2d_quadratic_nf",
+                                  "sdf_3d_quadratic_shell", "sdf_2d_quadratic_shell", "rigid_nn_2d_rotate"])
 def test_multi_step_drift_vs_fp64(case):
     """20 steps: FP32 GPU against the FP64 oracle (drift bound 1e-4)."""
     scene = STEP_CASES[case]()
@@ -287,7 +365,8 @@ def test_multi_step_drift_vs_fp64(case):
         assert err <= tol[name], f"{case} {name}: {err:.3e} > {tol[name]:.1e}"
 
 
-@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "random_3d_cubic_le_gravity"])
+@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "random_3d_cubic_le_gravity",
+                                  "rigid_nn_3d_static", "sdf_3d_quadratic_shell"])
 def test_deterministic_path_matches_oracle(case):
     """The deterministic (gather) P2G against the FP32 oracle, one step."""
     scene = STEP_CASES[case]()
