@@ -125,7 +125,8 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def_readonly("lame_modulus", &LinearElastic::lame_modulus)
       .def_readonly("bulk_modulus", &LinearElastic::bulk_modulus)
       .def_readwrite("density", &LinearElastic::density)
-      .def_readwrite("corrected", &LinearElastic::corrected);
+      .def_readwrite("corrected", &LinearElastic::corrected)
+      .def("calculate_timestep", &LinearElastic::calculate_timestep, py::arg("cell_size"), py::arg("factor"));
   py::class_<NewtonFluid>(m, "NewtonFluid", py::dynamic_attr())
       .def(py::init<float, float, float, float>(), py::arg("density"), py::arg("viscosity"),
            py::arg("bulk_modulus") = 0.0f, py::arg("gamma") = 7.0f)
@@ -137,7 +138,8 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def(py::init<float, float, float, float, float, float>(), py::arg("density"), py::arg("E"),
            py::arg("pois") = 0.0f, py::arg("friction_angle") = 30.0f, py::arg("dilatancy_angle") = 0.0f,
            py::arg("cohesion") = 0.0f)
-      .def_readwrite("density", &DruckerPrager::density);
+      .def_readwrite("density", &DruckerPrager::density)
+      .def("calculate_timestep", &DruckerPrager::calculate_timestep, py::arg("cell_size"), py::arg("factor"));
 
   py::class_<BoundaryCondition>(m, "BoundaryCondition").def(py::init<>());
   py::class_<Gravity>(m, "Gravity", py::dynamic_attr())
@@ -160,6 +162,42 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
   py::class_<PlanarDomain>(m, "PlanarDomain", py::dynamic_attr())
       .def(py::init([](py::object f0, py::object f1) { return PlanarDomain(vec<Vectorr>(f0), vec<Vectorr>(f1)); }),
            py::arg("face0_friction") = py::none(), py::arg("face1_friction") = py::none());
+
+  py::class_<RigidBodyLevelSet>(m, "RigidBodyLevelSet", py::dynamic_attr())
+      .def(py::init<>())
+      .def(
+          "set_mode_loop_rotate",
+          [](RigidBodyLevelSet &r, py::object rate, py::object com) {
+            r.set_mode_loop_rotate(vec<Vectorr>(rate), vec<Vectorr>(com));
+          },
+          py::arg("euler_angles_per_second"), py::arg("COM") = py::none())
+      .def(
+          "set_shape_sphere", [](RigidBodyLevelSet &r, py::object c, float radius) { r.set_shape_sphere(vec<Vectorr>(c), radius); },
+          py::arg("center"), py::arg("radius"))
+      .def(
+          "set_shape_half_cylinder_shell",
+          [](RigidBodyLevelSet &r, py::object c, int axis, float radius, float thickness, float length, float angle) {
+            r.set_shape_half_cylinder_shell(vec<Vectorr>(c), axis, radius, thickness, length, angle);
+          },
+          py::arg("center"), py::arg("axis"), py::arg("radius"), py::arg("thickness"), py::arg("length"),
+          py::arg("angle") = 0.0f)
+      .def(
+          "set_motion", [](RigidBodyLevelSet &r, py::object v, float w) { r.set_motion(vec<Vectorr>(v), w); },
+          py::arg("velocity"), py::arg("angular_velocity") = 0.0f)
+      .def_readwrite("friction", &RigidBodyLevelSet::friction)
+      .def_readwrite("contact_distance", &RigidBodyLevelSet::contact_distance)
+      .def_readwrite("corrected_rotation", &RigidBodyLevelSet::corrected_rotation)
+      .def("set_output_formats", [](RigidBodyLevelSet &, const std::vector<std::string> &) {},
+           py::arg("output_formats"));
+
+  m.def("calculate_timestep",
+        [](float cell_size, float factor, float bulk, float shear, float density) {
+          float dt;
+          check(pmpm_calculate_timestep(cell_size, factor, bulk, shear, density, &dt), "calculate_timestep");
+          return dt;
+        },
+        py::arg("cell_size"), py::arg("factor"), py::arg("bulk_modulus"), py::arg("shear_modulus"),
+        py::arg("density"));
 
   py::class_<Solver>(m, "Solver")
       .def(py::init<ParticlesContainer, NodesContainer, std::vector<MaterialType>, std::vector<BoundaryConditionType>>(),

@@ -203,6 +203,13 @@ struct LinearElastic {
     check(pmpm_material_linear_elastic(density, E, pois, corrected ? 1 : 0, &m), "LinearElastic");
     return m;
   }
+  // LinearElastic::calculate_timestep (src/materials/linearelastic.cpp:96-105)
+  Real calculate_timestep(Real cell_size, Real factor) const {
+    Real dt;
+    check(pmpm_calculate_timestep(cell_size, factor, bulk_modulus, shear_modulus, density, &dt),
+          "calculate_timestep");
+    return dt;
+  }
 };
 struct NewtonFluid {
   NewtonFluid(Real density, Real viscosity, Real bulk_modulus, Real gamma)
@@ -224,6 +231,14 @@ struct DruckerPrager {
     check(pmpm_material_drucker_prager(density, E, pois, friction_angle, dilatancy_angle, cohesion, &m),
           "DruckerPrager");
     return m;
+  }
+  // DP_rheo::calculate_timestep (src/materials/dp_rheo.cpp:165-175): the
+  // moduli are arguments there; these default to the material's own
+  Real calculate_timestep(Real cell_size, Real factor) const {
+    pmpm_material m = desc();
+    Real dt;
+    check(pmpm_material_timestep(&m, cell_size, factor, &dt), "calculate_timestep");
+    return dt;
   }
 };
 using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager>;
@@ -290,7 +305,57 @@ struct PlanarDomain {
     return b;
   }
 };
-using BoundaryConditionType = std::variant<BoundaryCondition, Gravity, NodeDomain, BodyForce, PlanarDomain>;
+// RigidBodyLevelSet (include/pyroclastmpm/boundaryconditions/rigidbodylevelset.h:
+// 85-170): the reference's nearest-rigid-particle contact (STATIC, or
+// set_mode_loop_rotate), or, once a shape is set, an analytic body with
+// Coulomb friction (set_shape_sphere / set_shape_half_cylinder_shell,
+// set_motion, set_friction).
+struct RigidBodyLevelSet {
+  RigidBodyLevelSet() { COM.fill(0.0f), euler_angles_per_second.fill(0.0f), center.fill(0.0f), velocity.fill(0.0f); }
+  void set_mode_loop_rotate(const Vectorr &rate, const Vectorr &com) {
+    mode = PMPM_RIGID_LOOP_ROTATE;
+    euler_angles_per_second = rate;
+    COM = com;
+  }
+  void set_shape_sphere(const Vectorr &c, Real radius) {
+    shape = PMPM_SDF_SPHERE;
+    center = c;
+    dims = {radius, 0.0f, 0.0f};
+  }
+  void set_shape_half_cylinder_shell(const Vectorr &c, int ax, Real radius, Real thickness, Real length,
+                                     Real angle0) {
+    shape = PMPM_SDF_HALF_CYLINDER_SHELL;
+    center = c;
+    axis = ax;
+    dims = {radius, thickness, length};
+    angle = angle0;
+  }
+  void set_motion(const Vectorr &v, Real w) {
+    velocity = v;
+    angular_velocity = w;
+  }
+  int mode = PMPM_RIGID_STATIC;
+  bool corrected_rotation = false;
+  Vectorr euler_angles_per_second, COM;
+  int shape = -1, axis = 1;
+  Vectorr center, velocity;
+  std::array<Real, 3> dims{0.0f, 0.0f, 0.0f};
+  Real angle = 0.0f, angular_velocity = 0.0f, friction = 0.0f, contact_distance = 0.0f;
+  pmpm_bc desc(int) const {
+    pmpm_bc b;
+    if (shape < 0)
+      check(pmpm_bc_rigidbodylevelset(mode, euler_angles_per_second.data(), COM.data(), corrected_rotation ? 1 : 0,
+                                      DIM, &b),
+            "RigidBodyLevelSet");
+    else
+      check(pmpm_bc_rigid_sdf(shape, axis, center.data(), velocity.data(), angular_velocity, angle, dims.data(),
+                              friction, contact_distance, DIM, &b),
+            "RigidBodyLevelSet");
+    return b;
+  }
+};
+using BoundaryConditionType =
+    std::variant<BoundaryCondition, Gravity, NodeDomain, BodyForce, PlanarDomain, RigidBodyLevelSet>;
 
 // ---------------------------------------------------------------------------
 // solvers

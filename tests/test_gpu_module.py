@@ -89,3 +89,29 @@ def test_granular_column_through_module():
     ref.solve(5)
     for name in ("positions", "velocities", "stresses", "F"):
         assert rel(getattr(mpm.particles, name), ref[name]) < 1e-5, name
+
+
+def test_scoop_through_module_matches_capi():
+    """RigidBodyLevelSet with an analytic half-cylinder shell, set up through
+    the module API, gives the C ABI Simulation's result for the same scene."""
+    import pyroclastmpm_b200.MPM3D as pm
+    from pyroclastmpm_b200 import Simulation
+
+    sc = scenes.granular_bed(cell_size=1.0 / 40, scale=0.25, shape_function="cubic", dt=1e-5)
+    body = sc["bcs"][1]
+    pm.set_globals(sc["dt"], sc["particles_per_cell"], "cubic", "output")
+    pm.set_global_step(0)
+    nodes = pm.NodesContainer(sc["origin"], sc["end"], sc["cell_size"])
+    particles = pm.ParticlesContainer(sc["positions"], sc["velocities"])
+    mat = pm.DruckerPrager(1500.0, 1.0e7, 0.3, 30.0, 0.0, 0.0)
+    rb = pm.RigidBodyLevelSet()
+    rb.set_shape_half_cylinder_shell(body["center"], body["axis"], *body["dims"], body["angle"])
+    rb.set_motion(body["velocity"], body["angular_velocity"])
+    rb.friction = body["friction"]
+    mpm = pm.USL(particles, nodes, [mat], [pm.Gravity([0.0, 0.0, -9.81]), rb, pm.NodeDomain([1, 1, 1], [1, 1, 1])])
+    mpm.solve_nsteps(5)
+    sim = Simulation(**scenes.sim_kwargs(sc))
+    sim.set_particles(sc["positions"], sc["velocities"]).initialize()
+    sim.solve(5)
+    for name in ("positions", "velocities", "stresses"):
+        assert rel(getattr(mpm.particles, name), sim.get(name)) < 1e-6, name

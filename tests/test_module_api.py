@@ -5,7 +5,7 @@ import pytest
 NAMES = ["set_globals", "set_global_shapefunction", "set_global_timestep", "set_global_step",
          "set_global_output_directory", "NodesContainer", "ParticlesContainer", "Solver", "USL",
          "Material", "LinearElastic", "NewtonFluid", "DruckerPrager", "BoundaryCondition", "Gravity",
-         "NodeDomain", "BodyForce", "PlanarDomain", "global_dimension"]
+         "NodeDomain", "BodyForce", "PlanarDomain", "RigidBodyLevelSet", "calculate_timestep", "global_dimension"]
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -52,3 +52,22 @@ def test_solver_without_gpu_raises():
     n = pm.NodesContainer([0.0, 0.0], [1.0, 1.0], 0.1)
     with pytest.raises(RuntimeError):
         pm.USL(p, n, [pm.LinearElastic(1000.0, 1000.0, 0.3)])
+
+
+def test_calculate_timestep_and_rigid_body_api():
+    import pyroclastmpm_b200.MPM3D as pm
+    from pyroclastmpm_b200 import _capi
+
+    le = pm.LinearElastic(1500.0, 1e7, 0.3)
+    dt = le.calculate_timestep(1.0 / 160, 0.3)
+    assert dt == _capi.calculate_timestep(1.0 / 160, 0.3, le.bulk_modulus, le.shear_modulus, 1500.0)
+    assert pm.calculate_timestep(1.0 / 160, 0.3, le.bulk_modulus, le.shear_modulus, 1500.0) == dt
+    dp = pm.DruckerPrager(1500.0, 1e7, 0.3, 30.0, 0.0, 0.0)
+    assert dp.calculate_timestep(1.0 / 160, 0.3) == dt
+    rb = pm.RigidBodyLevelSet()
+    rb.set_mode_loop_rotate([0.0, 0.0, 1.0], [0.5, 0.5, 0.5])
+    scoop = pm.RigidBodyLevelSet()
+    scoop.set_shape_half_cylinder_shell([0.15, 0.25, 0.3], 1, 0.15, 0.01, 0.4)
+    scoop.set_motion([0.5, 0.0, 0.0], 1.0)
+    scoop.friction = 0.3
+    assert scoop.friction == pytest.approx(0.3)
