@@ -377,6 +377,46 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
                            const float *positions, int num_particles, unsigned *hash_unsorted,
                            int *sorted_index, int *cell_start, int *cell_end, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched ensembles.  No counterpart in the reference (its settings are
+ * process globals: one simulation per process).  Many independent
+ * simulations are stepped together with one kernel launch per phase for
+ * all of them; each instance gives the results of a pmpm_sim created from
+ * the same descriptor and particles.  Instances share the dimension, shape
+ * function and flags; the grid, dt, materials and boundary conditions are
+ * per instance (RIGIDBODY_LEVELSET's nearest-rigid-particle mode is not
+ * supported).  The descriptors' device, stream and resort_interval are
+ * replaced by the batch's.
+ * ------------------------------------------------------------------------- */
+typedef struct pmpm_batch pmpm_batch;
+
+typedef struct {
+  const pmpm_desc *desc;
+  int num_particles;
+  const float *positions;      /* [n][dim], host */
+  const float *velocities;     /* [n][dim] or NULL */
+  const unsigned char *colors; /* [n] or NULL */
+} pmpm_instance;
+
+int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int device, void *stream,
+                      int resort_interval, pmpm_batch **out);
+int pmpm_batch_destroy(pmpm_batch *b);
+/* Solver::Solver set-up for every instance (volumes, masses, partition). */
+int pmpm_batch_initialize(pmpm_batch *b);
+/* nsteps USL steps of every instance (Solver::solve_nsteps per instance). */
+int pmpm_batch_solve(pmpm_batch *b, int nsteps);
+int pmpm_batch_num_instances(const pmpm_batch *b);
+int pmpm_batch_num_particles(const pmpm_batch *b, int instance);
+/* Particle fields, node masses/moments/ids/types and bins of one instance,
+ * as pmpm_get_field / pmpm_set_field (setters: particle fields only). */
+int pmpm_batch_get_field(pmpm_batch *b, int instance, int field, void *dst, size_t bytes, int on_device);
+int pmpm_batch_set_field(pmpm_batch *b, int instance, int field, const void *src, size_t bytes, int on_device);
+/* Waits for the batch's work; returns the first device fault of any instance. */
+int pmpm_batch_synchronize(pmpm_batch *b);
+/* One step with CUDA-event times: ms[0] partition, ms[1] P2G, ms[2] G2P. */
+int pmpm_batch_profile_step(pmpm_batch *b, float *ms, int *launches);
+int pmpm_batch_launch_count(const pmpm_batch *b, long long *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,6 @@
 - ``pyroclastmpm_b200._capi.Simulation``: direct binding of the C ABI
   (include/pmpm.h).
 """
-from ._capi import PmpmError, Simulation, lib, material_point_update  # noqa: F401
+from ._capi import Batch, PmpmError, Simulation, lib, material_point_update  # noqa: F401
 
-__all__ = ["Simulation", "PmpmError", "lib", "material_point_update"]
+__all__ = ["Simulation", "Batch", "PmpmError", "lib", "material_point_update"]

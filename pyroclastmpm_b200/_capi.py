@@ -67,6 +67,11 @@ class Desc(ctypes.Structure):
                 ("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("resort_interval", ctypes.c_int)]
 
 
+class Instance(ctypes.Structure):
+    _fields_ = [("desc", ctypes.POINTER(Desc)), ("num_particles", ctypes.c_int), ("positions", ctypes.c_void_p),
+                ("velocities", ctypes.c_void_p), ("colors", ctypes.c_void_p)]
+
+
 EXPORTS = [
     "pmpm_status_string", "pmpm_material_linear_elastic", "pmpm_material_newton_fluid",
     "pmpm_material_drucker_prager", "pmpm_material_dp_rheo", "pmpm_bc_gravity", "pmpm_bc_nodedomain",
@@ -77,6 +82,12 @@ EXPORTS = [
     "pmpm_get_step", "pmpm_set_step", "pmpm_synchronize", "pmpm_stream", "pmpm_material_point_update",
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
+]
+
+EXPORTS += [
+    "pmpm_batch_create", "pmpm_batch_destroy", "pmpm_batch_initialize", "pmpm_batch_solve",
+    "pmpm_batch_num_instances", "pmpm_batch_num_particles", "pmpm_batch_get_field", "pmpm_batch_set_field",
+    "pmpm_batch_synchronize", "pmpm_batch_profile_step", "pmpm_batch_launch_count",
 ]
 
 RIGID_MODES = {"static": 0, "loop_rotate": 1}
@@ -110,6 +121,17 @@ def lib():
     L.pmpm_bc_rigidbodylevelset.argtypes = [i, fp, fp, i, i, ctypes.POINTER(BC)]
     L.pmpm_bc_rigid_sdf.argtypes = [i, i, fp, fp, f, f, fp, f, f, i, ctypes.POINTER(BC)]
     L.pmpm_calculate_timestep.argtypes = [f, f, f, f, f, fp]
+    L.pmpm_batch_create.argtypes = [i, ctypes.POINTER(Instance), i, vp, i, ctypes.POINTER(vp)]
+    L.pmpm_batch_destroy.argtypes = [vp]
+    L.pmpm_batch_initialize.argtypes = [vp]
+    L.pmpm_batch_solve.argtypes = [vp, i]
+    L.pmpm_batch_num_instances.argtypes = [vp]
+    L.pmpm_batch_num_particles.argtypes = [vp, i]
+    L.pmpm_batch_get_field.argtypes = [vp, i, i, vp, sz, i]
+    L.pmpm_batch_set_field.argtypes = [vp, i, i, vp, sz, i]
+    L.pmpm_batch_synchronize.argtypes = [vp]
+    L.pmpm_batch_profile_step.argtypes = [vp, fp, ctypes.POINTER(ctypes.c_int)]
+    L.pmpm_batch_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.pmpm_material_timestep.argtypes = [ctypes.POINTER(Material), f, f, fp]
     L.pmpm_create.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(vp)]
     L.pmpm_destroy.argtypes = [vp]
@@ -263,6 +285,41 @@ def field_dtype(name):
     return np.float32
 
 
+def make_desc(dim, origin, end, cell_size, shape_function="linear", dt=1e-3, particles_per_cell=1, alpha=0.99,
+              materials=(), bcs=(), flags=0, device=0, stream=None, resort_interval=32, keep=None):
+    """pmpm_desc of a simulation; the arrays it points to are appended to `keep`."""
+    keep = [] if keep is None else keep
+    mats = list(materials)
+    bcl = list(bcs)
+    if len(mats) > MAX_MATERIALS or len(bcl) > MAX_BCS:
+        raise ValueError("too many materials or boundary conditions")
+    marr = (Material * max(1, len(mats)))(*[make_material(m) for m in mats]) if mats else (Material * 1)()
+    # node count is needed for BodyForce arrays; compute it the reference way
+    num_nodes = 1
+    for a in range(dim):
+        num_nodes *= int(np.float32(np.float32(end[a]) - np.float32(origin[a])) / np.float32(cell_size)) + 1
+    barr = (BC * max(1, len(bcl)))(*[make_bc(b, dim, num_nodes, keep) for b in bcl]) if bcl else (BC * 1)()
+    keep += [marr, barr]
+    d = Desc()
+    d.dim = dim
+    d.origin = _f3(list(origin) + [0.0] * 3)
+    d.end = _f3(list(end) + [0.0] * 3)
+    d.cell_size = float(cell_size)
+    d.shape_function = SHAPE[shape_function] if isinstance(shape_function, str) else int(shape_function)
+    d.dt = float(dt)
+    d.particles_per_cell = int(particles_per_cell)
+    d.alpha = float(alpha)
+    d.num_materials = len(mats)
+    d.materials = ctypes.cast(marr, ctypes.POINTER(Material))
+    d.num_bcs = len(bcl)
+    d.bcs = ctypes.cast(barr, ctypes.POINTER(BC))
+    d.flags = int(flags)
+    d.device = int(device)
+    d.stream = stream
+    d.resort_interval = int(resort_interval)
+    return d
+
+
 class Simulation:
     """One simulation handle (pmpm_sim) of the C ABI."""
 
@@ -271,37 +328,12 @@ class Simulation:
         L = lib()
         self.dim = dim
         self._keep = []
-        mats = list(materials)
-        bcl = list(bcs)
-        if len(mats) > MAX_MATERIALS or len(bcl) > MAX_BCS:
-            raise ValueError("too many materials or boundary conditions")
-        marr = (Material * max(1, len(mats)))(*[make_material(m) for m in mats]) if mats else (Material * 1)()
-        # node count is needed for BodyForce arrays; compute it the reference way
-        num_nodes = 1
-        for a in range(dim):
-            num_nodes *= int(np.float32(np.float32(end[a]) - np.float32(origin[a])) / np.float32(cell_size)) + 1
-        barr = (BC * max(1, len(bcl)))(*[make_bc(b, dim, num_nodes, self._keep) for b in bcl]) if bcl else (BC * 1)()
-        d = Desc()
-        d.dim = dim
-        d.origin = _f3(list(origin) + [0.0] * 3)
-        d.end = _f3(list(end) + [0.0] * 3)
-        d.cell_size = float(cell_size)
-        d.shape_function = SHAPE[shape_function] if isinstance(shape_function, str) else int(shape_function)
-        d.dt = float(dt)
-        d.particles_per_cell = int(particles_per_cell)
-        d.alpha = float(alpha)
-        d.num_materials = len(mats)
-        d.materials = ctypes.cast(marr, ctypes.POINTER(Material))
-        d.num_bcs = len(bcl)
-        d.bcs = ctypes.cast(barr, ctypes.POINTER(BC))
-        d.flags = int(flags)
-        d.device = int(device)
-        d.stream = stream
-        d.resort_interval = int(resort_interval)
+        d = make_desc(dim, origin, end, cell_size, shape_function, dt, particles_per_cell, alpha, materials, bcs,
+                      flags, device, stream, resort_interval, self._keep)
         h = ctypes.c_void_p()
         check(L.pmpm_create(ctypes.byref(d), ctypes.byref(h)), "pmpm_create")
         self._h = h
-        self._marr, self._barr = marr, barr
+        self._desc = d
         nc = (ctypes.c_int * 3)()
         nt = ctypes.c_int()
         inv = ctypes.c_float()
@@ -461,3 +493,107 @@ def material_point_update(mat: dict, dim, L, stress, eps_e=None, stress_ref=None
                                            p(vv), p(v0), 1 if velgrad_is_strain_increment else 0, device),
           "pmpm_material_point_update")
     return S, E
+
+
+class Batch:
+    """A batched ensemble (pmpm_batch): independent simulations stepped with
+    one launch per phase.  `instances` are dicts with the Simulation keyword
+    arguments (dim, origin, end, cell_size, shape_function, dt,
+    particles_per_cell, alpha, materials, bcs) plus positions, velocities and
+    colors."""
+
+    KEYS = ("dim", "origin", "end", "cell_size", "shape_function", "dt", "particles_per_cell", "alpha",
+            "materials", "bcs")
+
+    def __init__(self, instances, flags=0, device=0, stream=None, resort_interval=32):
+        L = lib()
+        self._keep = []
+        insts = list(instances)
+        arr = (Instance * len(insts))()
+        self.dims, self.n, self.num_nodes = [], [], []
+        for k, sc in enumerate(insts):
+            kw = {key: sc[key] for key in self.KEYS if key in sc}
+            d = make_desc(**kw, flags=flags, device=device, keep=self._keep)
+            self._keep.append(d)
+            dim = kw["dim"]
+            x = np.ascontiguousarray(np.asarray(sc["positions"], np.float32).reshape(-1, dim))
+            v = sc.get("velocities")
+            v = None if v is None else np.ascontiguousarray(np.asarray(v, np.float32).reshape(-1, dim))
+            c = sc.get("colors")
+            c = None if c is None else np.ascontiguousarray(np.asarray(c).astype(np.uint8))
+            self._keep += [x, v, c]
+            arr[k].desc = ctypes.pointer(d)
+            arr[k].num_particles = x.shape[0]
+            arr[k].positions = x.ctypes.data_as(ctypes.c_void_p)
+            arr[k].velocities = None if v is None else v.ctypes.data_as(ctypes.c_void_p)
+            arr[k].colors = None if c is None else c.ctypes.data_as(ctypes.c_void_p)
+            nn = 1
+            for a in range(dim):
+                nn *= int(np.float32(np.float32(kw["end"][a]) - np.float32(kw["origin"][a]))
+                          / np.float32(kw["cell_size"])) + 1
+            self.dims.append(dim)
+            self.n.append(x.shape[0])
+            self.num_nodes.append(nn)
+        h = ctypes.c_void_p()
+        check(L.pmpm_batch_create(len(insts), arr, int(device), stream, int(resort_interval), ctypes.byref(h)),
+              "pmpm_batch_create")
+        self._h = h
+        self._keep = None  # the batch copied everything it needs
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pmpm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.n)
+
+    def initialize(self):
+        check(lib().pmpm_batch_initialize(self._h), "pmpm_batch_initialize")
+        return self
+
+    def solve(self, nsteps=1):
+        check(lib().pmpm_batch_solve(self._h, int(nsteps)), "pmpm_batch_solve")
+        return self
+
+    def synchronize(self):
+        return lib().pmpm_batch_synchronize(self._h)
+
+    def get(self, instance, name, out=None):
+        shape = field_shape(name, self.dims[instance], self.n[instance], self.num_nodes[instance])
+        if out is None:
+            out = np.empty(shape, field_dtype(name))
+        check(lib().pmpm_batch_get_field(self._h, int(instance), FIELDS[name], out.ctypes.data_as(ctypes.c_void_p),
+                                         out.nbytes, 0), f"get {name}")
+        return out
+
+    def set(self, instance, name, values):
+        shape = field_shape(name, self.dims[instance], self.n[instance], self.num_nodes[instance])
+        a = np.ascontiguousarray(np.asarray(values, field_dtype(name)).reshape(shape))
+        check(lib().pmpm_batch_set_field(self._h, int(instance), FIELDS[name], a.ctypes.data_as(ctypes.c_void_p),
+                                         a.nbytes, 0), f"set {name}")
+
+    def get_ptr(self, instance, name, ptr, nbytes, on_device=False):
+        check(lib().pmpm_batch_get_field(self._h, int(instance), FIELDS[name], ctypes.c_void_p(ptr), nbytes,
+                                         1 if on_device else 0), f"get {name}")
+
+    def set_ptr(self, instance, name, ptr, nbytes, on_device=False):
+        check(lib().pmpm_batch_set_field(self._h, int(instance), FIELDS[name], ctypes.c_void_p(ptr), nbytes,
+                                         1 if on_device else 0), f"set {name}")
+
+    def profile_step(self):
+        ms = (ctypes.c_float * 3)()
+        nl = ctypes.c_int()
+        check(lib().pmpm_batch_profile_step(self._h, ms, ctypes.byref(nl)), "pmpm_batch_profile_step")
+        return [ms[0], ms[1], ms[2]], nl.value
+
+    def launch_count(self):
+        c = ctypes.c_longlong()
+        check(lib().pmpm_batch_launch_count(self._h, ctypes.byref(c)), "pmpm_batch_launch_count")
+        return c.value

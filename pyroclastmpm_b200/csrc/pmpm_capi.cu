@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -878,9 +879,9 @@ int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float fact
   }
 }
 
-int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
-  if (!desc || !out) return PMPM_ERR_INVALID_ARGUMENT;
-  *out = nullptr;
+// Descriptor -> handle parameters: grid, materials and boundary conditions
+// (BodyForce arrays are copied to the device; nothing else is allocated).
+static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
   if (desc->dim != 2 && desc->dim != 3) return PMPM_ERR_NOT_SUPPORTED;
   if (desc->shape_function < 0 || desc->shape_function > 2) return PMPM_ERR_INVALID_ARGUMENT;
   if (!(desc->cell_size > 0.0f) || desc->num_materials < 0 || desc->num_materials > PMPM_MAX_MATERIALS ||
@@ -888,8 +889,6 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
     return PMPM_ERR_INVALID_ARGUMENT;
   if ((desc->num_materials > 0 && !desc->materials) || (desc->num_bcs > 0 && !desc->bcs))
     return PMPM_ERR_INVALID_ARGUMENT;
-  PMPM_CUDA(cudaSetDevice(desc->device));
-  pmpm_sim *s = new pmpm_sim();
   s->device = desc->device;
   s->dim = desc->dim;
   s->shape = desc->shape_function;
@@ -898,16 +897,6 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   s->ppc = desc->particles_per_cell;
   s->flags = desc->flags;
   s->resort_interval = desc->resort_interval < 0 ? 0 : desc->resort_interval;
-  if (desc->stream) {
-    s->stream = (cudaStream_t)desc->stream;
-  } else {
-    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-      delete s;
-      return PMPM_ERR_CUDA;
-    }
-    s->own_stream = true;
-  }
   // Grid (include/pyroclastmpm/common/types_common.h:260-272), FP32 as the reference
   DevGrid &g = s->g;
   g.h = desc->cell_size;
@@ -922,10 +911,7 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
       g.end[c] = desc->end[c];
       const float span = desc->end[c] - desc->origin[c];
       g.n[c] = (int)(span / desc->cell_size) + 1;
-      if (g.n[c] < 1) {
-        delete s;
-        return PMPM_ERR_INVALID_ARGUMENT;
-      }
+      if (g.n[c] < 1) return PMPM_ERR_INVALID_ARGUMENT;
     }
     g.ntotal *= g.n[c];
   }
@@ -939,10 +925,7 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   // materials
   for (int k = 0; k < desc->num_materials; k++) {
     const pmpm_material &m = desc->materials[k];
-    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_DRUCKER_PRAGER) {
-      delete s;
-      return PMPM_ERR_INVALID_ARGUMENT;
-    }
+    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_DRUCKER_PRAGER) return PMPM_ERR_INVALID_ARGUMENT;
     DevMaterial dm;
     dm.type = m.type;
     dm.density = m.density;
@@ -1024,6 +1007,32 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
     }
     s->bcs.push_back(db);
   }
+  return st;
+}
+
+int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
+  if (!desc || !out) return PMPM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (desc->dim != 2 && desc->dim != 3) return PMPM_ERR_NOT_SUPPORTED;
+  if (desc->shape_function < 0 || desc->shape_function > 2) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!(desc->cell_size > 0.0f) || desc->num_materials < 0 || desc->num_materials > PMPM_MAX_MATERIALS ||
+      desc->num_bcs < 0 || desc->num_bcs > PMPM_MAX_BCS || desc->particles_per_cell <= 0)
+    return PMPM_ERR_INVALID_ARGUMENT;
+  if ((desc->num_materials > 0 && !desc->materials) || (desc->num_bcs > 0 && !desc->bcs))
+    return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(desc->device));
+  pmpm_sim *s = new pmpm_sim();
+  int st = setup_handle(desc, s);
+  if (st == PMPM_OK) {
+    if (desc->stream) {
+      s->stream = (cudaStream_t)desc->stream;
+    } else if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess) {
+      s->own_stream = true;
+    } else {
+      st = PMPM_ERR_CUDA;
+    }
+  }
+  const DevGrid &g = s->g;
   // nodes and bins
   const size_t nn = (size_t)g.ntotal, D = (size_t)s->dim;
   if (st == PMPM_OK) st = dalloc(&s->N.m, nn);
@@ -1592,6 +1601,583 @@ int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float d
     st = PMPM_ERR_CUDA;
   for (void *p : bufs) cudaFree(p);
   return st;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched ensembles
+// ===========================================================================
+//
+// Many independent simulations stepped together: one launch per phase for
+// all instances.  Instance i owns storage slots [first_i, first_i + n_i) of
+// shared particle arrays, node sub-arrays at noff_i (component-major inside
+// the instance), node tiles at toff_i and binning keys at koff_i (its cells
+// plus one sentinel key for particles outside its grid).  The key space is
+// instance-major, so the counting sort and the physical re-sort keep every
+// instance inside its slot range, and one scan serves all instances.  Each
+// instance's StepArgs view (grid, node and key sub-arrays, materials, BCs,
+// dt) lives in device memory; the batched kernels copy it to shared memory
+// and run the single-instance bodies.
+
+struct pmpm_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int dim = 2, shape = 0;
+  unsigned flags = 0;
+  int resort_interval = 32;
+  std::vector<pmpm_sim *> inst;  // per-instance parameters (grid, materials, BCs, dt)
+  std::vector<int> np, first, noff, toff, koff;
+  int n = 0, stride = 0, nn = 0, ntiles = 0, nkeys = 0;
+  DevParticles P[2]{};
+  int cur = 0;
+  int *slot = nullptr, *key = nullptr;
+  DevNodes N{};
+  int *node_epoch = nullptr;
+  DevBins B{};
+  int nscan_blocks = 0;
+  int *fault = nullptr;
+  std::vector<StepArgs> views;
+  StepArgs *d_views = nullptr;
+  std::vector<int> dynamic_bcs;  // instances whose BC state changes per step (gravity ramp, moving bodies)
+  BatchBlock *d_blocks = nullptr;
+  int nblocks = 0;
+  BatchTile *d_tiles = nullptr;
+  bool has_dp = false, has_sref = false, has_planar = false;
+  void *staging = nullptr;
+  size_t staging_bytes = 0;
+  long long launches = 0;
+  int step = 0, epoch = -1, p2g_epoch = -2, steps_since_sort = 0;
+  bool initialized = false;
+};
+
+namespace {
+
+// The per-instance view a batched kernel runs on (P and epoch are set per launch).
+StepArgs batch_view(pmpm_batch *b, int i) {
+  pmpm_sim *h = b->inst[i];
+  h->step = b->step;
+  StepArgs a = make_args(h);
+  const int D = b->dim;
+  const int F = D == 3 ? NodeVel<3>::F : NodeVel<2>::F;
+  a.N.m = b->N.m + b->noff[i];
+  a.N.p = b->N.p + (size_t)D * b->noff[i];
+  a.N.pnt = b->N.pnt + (size_t)D * b->noff[i];
+  a.N.vel = b->N.vel + (size_t)F * b->noff[i];
+  a.N.tile_epoch = b->N.tile_epoch + b->toff[i];
+  a.B = b->B;
+  a.B.dual = 0;
+  a.B.nkeys = h->g.ntotal + 1;
+  a.B.key_base = b->koff[i];
+  a.B.sentinel = 1;
+  a.B.count = b->B.count + b->koff[i];
+  a.B.offset = b->B.offset + b->koff[i];
+  a.fault = b->fault;
+  a.has_planar = h->has_planar ? 1 : 0;
+  a.has_sref = b->has_sref ? 1 : 0;
+  a.rigid_shift = 0;
+  return a;
+}
+
+// The whole-batch arguments of the global phases (scatter, sorts, re-sort).
+StepArgs batch_global_args(pmpm_batch *b) {
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.P = b->P[b->cur];
+  a.P.slot = b->slot;
+  a.P.key = (unsigned *)b->key;
+  a.B = b->B;
+  a.B.nkeys = b->nkeys;
+  a.fault = b->fault;
+  return a;
+}
+
+DevParticles batch_particles(pmpm_batch *b) {
+  DevParticles P = b->P[b->cur];
+  P.slot = b->slot;
+  P.key = (unsigned *)b->key;
+  return P;
+}
+
+// Non-owning single-instance handle over instance i's part of the batch
+// (for the field getters and setters and the set-up kernels).
+void batch_instance_handle(pmpm_batch *b, int i, pmpm_sim &v) {
+  pmpm_sim *h = b->inst[i];
+  v.device = b->device;
+  v.stream = b->stream;
+  v.dim = b->dim;
+  v.shape = b->shape;
+  v.g = h->g;
+  v.dt = h->dt;
+  v.alpha = h->alpha;
+  v.ppc = h->ppc;
+  v.flags = b->flags;
+  v.mats = h->mats;
+  v.has_dp = h->has_dp;
+  v.has_planar = h->has_planar;
+  v.has_sref = b->has_sref;
+  v.n = b->np[i];
+  v.stride = b->stride;
+  v.cur = 0;
+  DevParticles P = b->P[b->cur];
+  const int o = b->first[i];
+  auto off = [o](auto *p) { return p ? p + o : p; };
+  P.n = v.n;
+  P.x = off(P.x);
+  P.v = off(P.v);
+  P.F = off(P.F);
+  P.sig = off(P.sig);
+  P.L = off(P.L);
+  P.m = off(P.m);
+  P.V = off(P.V);
+  P.V0 = off(P.V0);
+  P.fext = off(P.fext);
+  P.eps = off(P.eps);
+  P.sref = off(P.sref);
+  P.color = off(P.color);
+  P.active = off(P.active);
+  P.rigid = off(P.rigid);
+  P.id = off(P.id);
+  P.hash = off(P.hash);
+  v.P[0] = P;
+  const StepArgs a = batch_view(b, i);
+  v.N = a.N;
+  v.node_epoch = b->node_epoch + b->toff[i];
+  v.B = a.B;
+  v.fault = b->fault;
+  v.staging = b->staging;
+  v.staging_bytes = b->staging_bytes;
+  v.epoch = b->epoch;
+  v.p2g_epoch = b->p2g_epoch;
+  v.partitioned = true;
+}
+
+void release_instance_handle(pmpm_batch *b, pmpm_sim &v) {
+  b->staging = v.staging;
+  b->staging_bytes = v.staging_bytes;
+  v.staging = nullptr;
+  v.stream = nullptr;
+}
+
+int upload_views(pmpm_batch *b, bool only_dynamic) {
+  if (!only_dynamic) {
+    for (int i = 0; i < (int)b->inst.size(); i++) b->views[i] = batch_view(b, i);
+    PMPM_CUDA(cudaMemcpyAsync(b->d_views, b->views.data(), sizeof(StepArgs) * b->views.size(),
+                              cudaMemcpyHostToDevice, b->stream));
+    return PMPM_OK;
+  }
+  for (int i : b->dynamic_bcs) {
+    pmpm_sim *h = b->inst[i];
+    h->step = b->step;
+    update_gravity(h);
+    update_bodies(h);
+    b->views[i] = batch_view(b, i);
+    // pageable source: the call returns once the bytes are staged, so the
+    // host copy may change for the next step
+    PMPM_CUDA(cudaMemcpyAsync(b->d_views + i, &b->views[i], sizeof(StepArgs), cudaMemcpyHostToDevice, b->stream));
+  }
+  return PMPM_OK;
+}
+
+template <int D, int SF>
+int batch_partition(pmpm_batch *b) {
+  b->epoch += 1;
+  const DevParticles P = batch_particles(b);
+  cudaStream_t st = b->stream;
+  kb_hash_count<D, SF><<<b->nblocks, kTPB, 0, st>>>(b->d_views, b->d_blocks, P, b->epoch);
+  PMPM_LAUNCHED();
+  const StepArgs ga = batch_global_args(b);
+  k_scan_reduce<<<b->nscan_blocks, kScanThreads, 0, st>>>(b->B.count, b->nkeys, b->B.block_sums);
+  PMPM_LAUNCHED();
+  k_scan_top<<<1, kScanThreads, 0, st>>>(b->B.block_sums, b->nscan_blocks, b->B.scalars);
+  PMPM_LAUNCHED();
+  k_scan_apply<<<b->nscan_blocks, kScanThreads, 0, st>>>(b->B.count, b->nkeys, b->B.block_sums, b->B.offset);
+  PMPM_LAUNCHED();
+  k_scatter<<<blocks_for(b->n), kTPB, 0, st>>>(ga);
+  PMPM_LAUNCHED();
+  k_sort_cells<<<blocks_for(b->nkeys), kTPB, 0, st>>>(ga);
+  PMPM_LAUNCHED();
+  k_sort_big<<<148, 1024, 0, st>>>(ga);
+  PMPM_LAUNCHED();
+  b->launches += 7;
+  return PMPM_OK;
+}
+
+template <int D>
+int batch_reorder(pmpm_batch *b) {
+  const StepArgs ga = batch_global_args(b);
+  DevParticles dst = b->P[1 - b->cur];
+  const bool move_L = (b->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) != 0;
+  k_reorder<D><<<blocks_for(b->n), kTPB, 0, b->stream>>>(ga, dst, move_L ? 1 : 0, b->has_planar ? 1 : 0);
+  PMPM_LAUNCHED();
+  b->launches += 1;
+  b->cur = 1 - b->cur;
+  b->steps_since_sort = 0;
+  return PMPM_OK;
+}
+
+template <int D, int SF>
+int batch_step(pmpm_batch *b, float *ms) {
+  cudaEvent_t ev[4];
+  if (ms)
+    for (int k = 0; k < 4; k++) PMPM_CUDA(cudaEventCreate(&ev[k]));
+  if (ms) PMPM_CUDA(cudaEventRecord(ev[0], b->stream));
+  PMPM_TRY((batch_partition<D, SF>(b)));
+  if (b->resort_interval > 0 && b->steps_since_sort + 1 >= b->resort_interval) {
+    PMPM_TRY(batch_reorder<D>(b));
+  } else {
+    b->steps_since_sort += 1;
+  }
+  if (ms) PMPM_CUDA(cudaEventRecord(ev[1], b->stream));
+  if (!b->dynamic_bcs.empty()) PMPM_TRY(upload_views(b, true));
+  const DevParticles P = batch_particles(b);
+  const int gather = (b->flags & PMPM_FLAG_DETERMINISTIC) ? 1 : 0;
+  kb_p2g<D, SF><<<b->ntiles, TileDims<D>::N, 0, b->stream>>>(b->d_views, b->d_tiles, b->N.tile_epoch, P, b->epoch,
+                                                              1, b->node_epoch, gather);
+  PMPM_LAUNCHED();
+  b->p2g_epoch = b->epoch;
+  if (ms) PMPM_CUDA(cudaEventRecord(ev[2], b->stream));
+  const int store_L = (b->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
+  kb_g2p<D, SF><<<b->nblocks, kTPB, 0, b->stream>>>(b->d_views, b->d_blocks, P, b->epoch, 1, store_L);
+  PMPM_LAUNCHED();
+  b->launches += 2;
+  b->step += 1;
+  if (ms) {
+    PMPM_CUDA(cudaEventRecord(ev[3], b->stream));
+    PMPM_CUDA(cudaEventSynchronize(ev[3]));
+    for (int k = 0; k < 3; k++) PMPM_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+    for (int k = 0; k < 4; k++) cudaEventDestroy(ev[k]);
+  }
+  return PMPM_OK;
+}
+
+int batch_step_dispatch(pmpm_batch *b, float *ms) {
+  if (b->dim == 2) {
+    if (b->shape == PMPM_SHAPE_LINEAR) return batch_step<2, PMPM_SHAPE_LINEAR>(b, ms);
+    if (b->shape == PMPM_SHAPE_QUADRATIC) return batch_step<2, PMPM_SHAPE_QUADRATIC>(b, ms);
+    return batch_step<2, PMPM_SHAPE_CUBIC>(b, ms);
+  }
+  if (b->shape == PMPM_SHAPE_LINEAR) return batch_step<3, PMPM_SHAPE_LINEAR>(b, ms);
+  if (b->shape == PMPM_SHAPE_QUADRATIC) return batch_step<3, PMPM_SHAPE_QUADRATIC>(b, ms);
+  return batch_step<3, PMPM_SHAPE_CUBIC>(b, ms);
+}
+
+int batch_partition_dispatch(pmpm_batch *b) {
+  if (b->dim == 2) {
+    if (b->shape == PMPM_SHAPE_LINEAR) return batch_partition<2, PMPM_SHAPE_LINEAR>(b);
+    if (b->shape == PMPM_SHAPE_QUADRATIC) return batch_partition<2, PMPM_SHAPE_QUADRATIC>(b);
+    return batch_partition<2, PMPM_SHAPE_CUBIC>(b);
+  }
+  if (b->shape == PMPM_SHAPE_LINEAR) return batch_partition<3, PMPM_SHAPE_LINEAR>(b);
+  if (b->shape == PMPM_SHAPE_QUADRATIC) return batch_partition<3, PMPM_SHAPE_QUADRATIC>(b);
+  return batch_partition<3, PMPM_SHAPE_CUBIC>(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmpm_batch_destroy(pmpm_batch *b) {
+  if (!b) return PMPM_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (pmpm_sim *h : b->inst) pmpm_destroy(h);
+  for (int k = 0; k < 2; k++) {
+    DevParticles &P = b->P[k];
+    for (void *p : {(void *)P.x, (void *)P.v, (void *)P.F, (void *)P.sig, (void *)P.L, (void *)P.m, (void *)P.V,
+                    (void *)P.V0, (void *)P.fext, (void *)P.eps, (void *)P.sref, (void *)P.color, (void *)P.active,
+                    (void *)P.rigid, (void *)P.id, (void *)P.hash})
+      if (p) cudaFree(p);
+  }
+  for (void *p : {(void *)b->slot, (void *)b->key, (void *)b->N.m, (void *)b->N.p, (void *)b->N.pnt, (void *)b->N.vel,
+                  (void *)b->N.tile_epoch, (void *)b->node_epoch, (void *)b->B.count, (void *)b->B.offset,
+                  (void *)b->B.order, (void *)b->B.block_sums, (void *)b->B.scalars, (void *)b->B.big_cells,
+                  (void *)b->fault, (void *)b->d_views, (void *)b->d_blocks, (void *)b->d_tiles, b->staging})
+    if (p) cudaFree(p);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return PMPM_OK;
+}
+
+int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int device, void *stream,
+                      int resort_interval, pmpm_batch **out) {
+  if (!out || num_instances < 1 || !instances) return PMPM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  PMPM_CUDA(cudaSetDevice(device));
+  pmpm_batch *b = new pmpm_batch();
+  b->device = device;
+  b->resort_interval = resort_interval < 0 ? 0 : resort_interval;
+  int st = PMPM_OK;
+  long long n = 0, nn = 0, nt = 0, nk = 0;
+  for (int i = 0; i < num_instances && st == PMPM_OK; i++) {
+    const pmpm_instance &in = instances[i];
+    if (!in.desc || in.num_particles < 1 || !in.positions) {
+      st = PMPM_ERR_INVALID_ARGUMENT;
+      break;
+    }
+    pmpm_sim *h = new pmpm_sim();
+    b->inst.push_back(h);
+    st = setup_handle(in.desc, h);
+    if (st != PMPM_OK) break;
+    h->device = device;
+    if (i == 0) {
+      b->dim = h->dim;
+      b->shape = h->shape;
+      b->flags = h->flags;
+    } else if (h->dim != b->dim || h->shape != b->shape || h->flags != b->flags) {
+      st = PMPM_ERR_INVALID_ARGUMENT;  // one kernel instantiation serves the batch
+      break;
+    }
+    if (h->rbls_index >= 0) {
+      st = PMPM_ERR_NOT_SUPPORTED;
+      break;
+    }
+    bool dyn = !h->sdf.empty();
+    for (const GravityState &gs : h->gravity) dyn = dyn || h->bcs[gs.bc_index].i[0] != 0;
+    if (dyn) b->dynamic_bcs.push_back(i);
+    b->has_dp = b->has_dp || h->has_dp;
+    b->has_planar = b->has_planar || h->has_planar;
+    b->np.push_back(in.num_particles);
+    b->first.push_back((int)n);
+    b->noff.push_back((int)nn);
+    b->toff.push_back((int)nt);
+    b->koff.push_back((int)nk);
+    n += in.num_particles;
+    nn += h->g.ntotal;
+    nt += h->g.ntiles;
+    nk += h->g.ntotal + 1;
+  }
+  if (st == PMPM_OK && (n > INT32_MAX / 2 || nn > INT32_MAX / 8 || nk > INT32_MAX / 2)) st = PMPM_ERR_NOT_SUPPORTED;
+  if (st != PMPM_OK) {
+    pmpm_batch_destroy(b);
+    return st;
+  }
+  b->n = (int)n;
+  b->nn = (int)nn;
+  b->ntiles = (int)nt;
+  b->nkeys = (int)nk;
+  b->stride = (b->n + 63) / 64 * 64;
+  if (stream) {
+    b->stream = (cudaStream_t)stream;
+  } else if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess) {
+    b->own_stream = true;
+  } else {
+    pmpm_batch_destroy(b);
+    return PMPM_ERR_CUDA;
+  }
+  for (pmpm_sim *h : b->inst) h->stream = b->stream;
+  const int D = b->dim;
+  // particle storage: instance-major, local ids
+  pmpm_sim shape_of;
+  shape_of.dim = D;
+  shape_of.n = b->n;
+  shape_of.stride = b->stride;
+  shape_of.has_dp = b->has_dp;
+  shape_of.has_planar = b->has_planar;
+  st = alloc_particle_set(&shape_of, b->P[0]);
+  if (st == PMPM_OK) st = alloc_particle_set(&shape_of, b->P[1]);
+  const size_t stv = (size_t)b->stride;
+  if (st == PMPM_OK) st = dalloc(&b->slot, stv);
+  if (st == PMPM_OK) st = dalloc(&b->key, stv);
+  if (st == PMPM_OK) st = dalloc(&b->B.order, stv);
+  const int F = D == 3 ? NodeVel<3>::F : NodeVel<2>::F;
+  if (st == PMPM_OK) st = dalloc(&b->N.m, (size_t)b->nn);
+  if (st == PMPM_OK) st = dalloc(&b->N.p, (size_t)b->nn * D);
+  if (st == PMPM_OK) st = dalloc(&b->N.pnt, (size_t)b->nn * D);
+  if (st == PMPM_OK) st = dalloc(&b->N.vel, (size_t)b->nn * F);
+  if (st == PMPM_OK) st = dalloc(&b->N.tile_epoch, (size_t)b->ntiles);
+  if (st == PMPM_OK) st = dalloc(&b->node_epoch, (size_t)b->ntiles);
+  b->nscan_blocks = (b->nkeys + kScanChunk - 1) / kScanChunk;
+  if (st == PMPM_OK) st = dalloc(&b->B.count, (size_t)b->nkeys);
+  if (st == PMPM_OK) st = dalloc(&b->B.offset, (size_t)b->nkeys + 1);
+  if (st == PMPM_OK) st = dalloc(&b->B.block_sums, (size_t)b->nscan_blocks);
+  if (st == PMPM_OK) st = dalloc(&b->B.scalars, 4);
+  if (st == PMPM_OK) st = dalloc(&b->B.big_cells, (size_t)b->nkeys);
+  if (st == PMPM_OK) st = dalloc(&b->fault, 1);
+  if (st == PMPM_OK && cudaMalloc(&b->d_views, sizeof(StepArgs) * num_instances) != cudaSuccess) st = PMPM_ERR_OUT_OF_MEMORY;
+  // block and tile tables
+  std::vector<BatchBlock> blocks;
+  std::vector<BatchTile> tiles;
+  for (int i = 0; i < num_instances && st == PMPM_OK; i++) {
+    for (int s0 = 0; s0 < b->np[i]; s0 += kTPB)
+      blocks.push_back({i, b->first[i] + s0, b->first[i] + std::min(s0 + kTPB, b->np[i])});
+    for (int t = 0; t < b->inst[i]->g.ntiles; t++) tiles.push_back({i, t, b->toff[i] + t});
+  }
+  b->nblocks = (int)blocks.size();
+  if (st == PMPM_OK && cudaMalloc(&b->d_blocks, sizeof(BatchBlock) * blocks.size()) != cudaSuccess)
+    st = PMPM_ERR_OUT_OF_MEMORY;
+  if (st == PMPM_OK && cudaMalloc(&b->d_tiles, sizeof(BatchTile) * tiles.size()) != cudaSuccess)
+    st = PMPM_ERR_OUT_OF_MEMORY;
+  if (st == PMPM_OK &&
+      (cudaMemcpy(b->d_blocks, blocks.data(), sizeof(BatchBlock) * blocks.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemset(b->B.count, 0, sizeof(int) * b->nkeys) != cudaSuccess ||
+       cudaMemset(b->B.scalars, 0, 4 * sizeof(int)) != cudaSuccess || cudaMemset(b->fault, 0, sizeof(int)) != cudaSuccess ||
+       cudaMemset(b->N.tile_epoch, 0xff, sizeof(int) * b->ntiles) != cudaSuccess ||
+       cudaMemset(b->node_epoch, 0xff, sizeof(int) * b->ntiles) != cudaSuccess ||
+       cudaMemset(b->N.m, 0, sizeof(float) * b->nn) != cudaSuccess))
+    st = PMPM_ERR_CUDA;
+  // particles (ParticlesContainer ctor per instance; ids local to the instance)
+  if (st == PMPM_OK) {
+    const size_t sv = (size_t)b->stride;
+    const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6;
+    std::vector<float> x((size_t)D * sv, 0.0f), v((size_t)D * sv, 0.0f), Fm((size_t)D * D * sv, 0.0f);
+    std::vector<float> m(sv, -1.0f), V(sv, -1.0f);
+    std::vector<uint8_t> color(sv, 0), zero(sv, 0), active(sv, 1);
+    std::vector<int> id(sv, 0);
+    for (int i = 0; i < num_instances; i++) {
+      const pmpm_instance &in = instances[i];
+      for (int j = 0; j < in.num_particles; j++) {
+        const size_t s = (size_t)b->first[i] + j;
+        for (int c = 0; c < D; c++) {
+          x[c * sv + s] = in.positions[(size_t)j * D + c];
+          v[c * sv + s] = in.velocities ? in.velocities[(size_t)j * D + c] : 0.0f;
+          Fm[(c * D + c) * sv + s] = 1.0f;
+        }
+        color[s] = in.colors ? in.colors[j] : 0;
+        id[s] = j;
+      }
+    }
+    DevParticles &P = b->P[0];
+    if (cudaMemcpy(P.x, x.data(), sizeof(float) * x.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.v, v.data(), sizeof(float) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.F, Fm.data(), sizeof(float) * Fm.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(P.sig, 0, sizeof(float) * S * sv) != cudaSuccess ||
+        cudaMemset(P.L, 0, sizeof(float) * D * D * sv) != cudaSuccess ||
+        cudaMemset(b->P[1].L, 0, sizeof(float) * D * D * sv) != cudaSuccess ||
+        cudaMemcpy(P.m, m.data(), sizeof(float) * sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.V, V.data(), sizeof(float) * sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.V0, V.data(), sizeof(float) * sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (P.fext && cudaMemset(P.fext, 0, sizeof(float) * D * sv) != cudaSuccess) ||
+        (P.eps && cudaMemset(P.eps, 0, sizeof(float) * E * sv) != cudaSuccess) ||
+        (P.sref && cudaMemset(P.sref, 0, sizeof(float) * S * sv) != cudaSuccess) ||
+        cudaMemcpy(P.color, color.data(), sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.rigid, zero.data(), sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.active, active.data(), sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P.id, id.data(), sizeof(int) * sv, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(P.hash, 0, sizeof(unsigned) * sv) != cudaSuccess ||
+        cudaMemset(b->B.order, 0, sizeof(int) * sv) != cudaSuccess)
+      st = PMPM_ERR_CUDA;
+  }
+  if (st == PMPM_OK) {
+    b->views.resize(num_instances);
+    st = upload_views(b, false);
+  }
+  if (st == PMPM_OK && cudaStreamSynchronize(b->stream) != cudaSuccess) st = PMPM_ERR_CUDA;
+  if (st != PMPM_OK) {
+    pmpm_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return PMPM_OK;
+}
+
+int pmpm_batch_num_instances(const pmpm_batch *b) { return b ? (int)b->inst.size() : -1; }
+
+int pmpm_batch_num_particles(const pmpm_batch *b, int instance) {
+  if (!b || instance < 0 || instance >= (int)b->inst.size()) return -1;
+  return b->np[instance];
+}
+
+int pmpm_batch_initialize(pmpm_batch *b) {
+  if (!b) return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(b->device));
+  PMPM_TRY(batch_partition_dispatch(b));
+  // calculate_initial_volumes / calculate_initial_masses per instance
+  for (int i = 0; i < (int)b->inst.size(); i++) {
+    pmpm_sim v;
+    batch_instance_handle(b, i, v);
+    float vol = (float)std::pow((double)v.g.h, (double)v.dim);
+    vol = vol / (float)v.ppc;
+    int st = PMPM_OK;
+    k_initial_volumes<<<blocks_for(v.n), kTPB, 0, b->stream>>>(v.P[0], vol);
+    if (cudaGetLastError() != cudaSuccess) st = PMPM_ERR_CUDA;
+    for (int k = 0; k < (int)v.mats.size() && st == PMPM_OK; k++) {
+      k_initial_masses<<<blocks_for(v.n), kTPB, 0, b->stream>>>(v.P[0], k, v.mats[k].density);
+      if (cudaGetLastError() != cudaSuccess) st = PMPM_ERR_CUDA;
+    }
+    release_instance_handle(b, v);
+    PMPM_TRY(st);
+  }
+  if (b->has_dp) {
+    DevParticles P = b->P[b->cur];
+    P.n = b->n;
+    int *flag = b->B.scalars + 3;
+    PMPM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), b->stream));
+    k_dp_init<<<blocks_for(b->n), kTPB, 0, b->stream>>>(P, b->dim, flag);
+    PMPM_LAUNCHED();
+    int hflag = 0;
+    PMPM_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    PMPM_CUDA(cudaStreamSynchronize(b->stream));
+    b->has_sref = hflag != 0;
+  }
+  PMPM_TRY(upload_views(b, false));
+  PMPM_CUDA(cudaStreamSynchronize(b->stream));
+  b->initialized = true;
+  return PMPM_OK;
+}
+
+int pmpm_batch_solve(pmpm_batch *b, int nsteps) {
+  if (!b || nsteps < 0) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!b->initialized) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(b->device));
+  for (int k = 0; k < nsteps; k++) PMPM_TRY(batch_step_dispatch(b, nullptr));
+  return PMPM_OK;
+}
+
+int pmpm_batch_profile_step(pmpm_batch *b, float *ms, int *launches) {
+  if (!b || !ms) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!b->initialized) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(b->device));
+  const long long l0 = b->launches;
+  PMPM_TRY(batch_step_dispatch(b, ms));
+  if (launches) *launches = (int)(b->launches - l0);
+  return PMPM_OK;
+}
+
+static bool batch_field_ok(int field) {
+  return field < PMPM_FIELD_NODE_MASSES || (field >= PMPM_FIELD_NODE_MASSES && field <= PMPM_FIELD_NODE_TYPES) ||
+         field == PMPM_FIELD_BINS;
+}
+
+int pmpm_batch_get_field(pmpm_batch *b, int instance, int field, void *dst, size_t bytes, int on_device) {
+  if (!b || instance < 0 || instance >= (int)b->inst.size()) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!batch_field_ok(field)) return PMPM_ERR_NOT_SUPPORTED;
+  pmpm_sim v;
+  batch_instance_handle(b, instance, v);
+  const int st = pmpm_get_field(&v, field, dst, bytes, on_device);
+  release_instance_handle(b, v);
+  return st;
+}
+
+int pmpm_batch_set_field(pmpm_batch *b, int instance, int field, const void *src, size_t bytes, int on_device) {
+  if (!b || instance < 0 || instance >= (int)b->inst.size()) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!batch_field_ok(field) || field >= PMPM_FIELD_NODE_MASSES) return PMPM_ERR_NOT_SUPPORTED;
+  pmpm_sim v;
+  batch_instance_handle(b, instance, v);
+  const int st = pmpm_set_field(&v, field, src, bytes, on_device);
+  release_instance_handle(b, v);
+  return st;
+}
+
+int pmpm_batch_synchronize(pmpm_batch *b) {
+  if (!b) return PMPM_ERR_INVALID_ARGUMENT;
+  PMPM_CUDA(cudaSetDevice(b->device));
+  int f = 0;
+  PMPM_CUDA(cudaMemcpyAsync(&f, b->fault, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  PMPM_CUDA(cudaStreamSynchronize(b->stream));
+  if (f) PMPM_CUDA(cudaMemset(b->fault, 0, sizeof(int)));
+  if (f & kFaultNonFinite) return PMPM_ERR_NONFINITE;
+  if (f & kFaultOutOfDomain) return PMPM_ERR_OUT_OF_DOMAIN;
+  if (f & kFaultCellOverflow) return PMPM_ERR_CELL_OVERFLOW;
+  return PMPM_OK;
+}
+
+int pmpm_batch_launch_count(const pmpm_batch *b, long long *count) {
+  if (!b || !count) return PMPM_ERR_INVALID_ARGUMENT;
+  *count = b->launches;
+  return PMPM_OK;
 }
 
 }  // extern "C"

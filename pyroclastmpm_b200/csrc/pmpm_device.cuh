@@ -85,6 +85,8 @@ struct DevBins {
   int dual;
   int kd[3];
   int nkeys;
+  int key_base;     // added to the stored particle keys (an instance's first key in a batch)
+  int sentinel;     // particles outside the grid take key ntotal (batched ensembles)
   int *count;       // per key, zero between steps
   int *offset;      // exclusive prefix, nkeys + 1 entries
   int *order;       // sorted position -> storage slot

@@ -154,9 +154,7 @@ __device__ __forceinline__ void planar_force(const StepArgs &a, int s, const flo
 __device__ __forceinline__ int dual_coord(float u, int b) { return (u - (float)(b - 1)) < 1.5f ? b : b + 1; }
 
 template <int D, int SF>
-__global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.P.n) return;
+__device__ __forceinline__ void hash_count_body(const StepArgs &a, int s) {
   const DevGrid &g = a.g;
   float x[3] = {0.0f, 0.0f, 0.0f}, u[3] = {0.0f, 0.0f, 0.0f};
   int b[3] = {0, 0, 0};
@@ -184,10 +182,24 @@ __global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
     binned = hu < (unsigned)g.ntotal;
     mark_tiles<D, SF>(a, b, hu, binned, in_axes);
   }
-  a.P.key[s] = key;
-  a.P.slot[s] = binned ? atomicAdd(&a.B.count[key], 1) : -1;
+  // with a sentinel key (batched ensembles) a particle outside the grid is
+  // sorted into its instance's extra last key, so instances keep their
+  // storage ranges; it is reported as a fault either way
+  bool sorted = binned;
+  if (!binned && a.B.sentinel) {
+    key = (unsigned)g.ntotal;
+    sorted = true;
+  }
+  a.P.key[s] = (unsigned)a.B.key_base + key;
+  a.P.slot[s] = sorted ? atomicAdd(&a.B.count[key], 1) : -1;
   if (!binned || (SF == PMPM_SHAPE_QUADRATIC && !in_axes)) atomicOr(a.fault, kFaultOutOfDomain);
   if (a.has_planar) planar_force<D>(a, s, x);
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < a.P.n) hash_count_body<D, SF>(a, s);
 }
 
 constexpr int kScanThreads = 1024;
@@ -477,10 +489,9 @@ __device__ __forceinline__ void p2g_range(const StepArgs &a, int k0, int k1, con
 }
 
 template <int D, int SF>
-__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int apply_bcs, int *node_epoch) {
+__device__ __forceinline__ void p2g_gather_body(const StepArgs &a, int tile, int apply_bcs, int *node_epoch) {
   using T = TileDims<D>;
   const DevGrid &g = a.g;
-  const int tile = blockIdx.x;
   if (a.N.tile_epoch[tile] != a.epoch) return;
   if (threadIdx.x == 0) node_epoch[tile] = a.epoch;
   const int tx = tile % g.tdim[0], ty = (tile / g.tdim[0]) % g.tdim[1], tz = tile / (g.tdim[0] * g.tdim[1]);
@@ -534,6 +545,11 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int a
   }
   if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
   write_node<D>(a, node, mass, p, pnt, live);
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int apply_bcs, int *node_epoch) {
+  p2g_gather_body<D, SF>(a, blockIdx.x, apply_bcs, node_epoch);
 }
 
 // --------------------------------------------------------------------------
@@ -716,13 +732,12 @@ struct P2GTileShape {
 };
 
 template <int D, int SF>
-__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int apply_bcs, int *node_epoch) {
+__device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int apply_bcs, int *node_epoch) {
   using T = TileDims<D>;
   using Sh = P2GTileShape<D, SF>;
   constexpr int NT = T::N;
   constexpr int K = Stencil<SF>::K;
   const DevGrid &g = a.g;
-  const int tile = blockIdx.x;
   if (a.N.tile_epoch[tile] != a.epoch) return;
 
   __shared__ float acc[Sh::NACC * NT];
@@ -967,6 +982,11 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int app
   }
   if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
   write_node<D>(a, node, mass, p, pnt, live);
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int apply_bcs, int *node_epoch) {
+  p2g_tile_body<D, SF>(a, blockIdx.x, apply_bcs, node_epoch);
 }
 
 // --------------------------------------------------------------------------
@@ -1619,9 +1639,7 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
 }
 
 template <int D, int SF>
-__global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int store_L) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.P.n) return;
+__device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress, int store_L) {
   const DevParticles &P = a.P;
   const DevGrid &g = a.g;
   const int st = P.stride;
@@ -1762,6 +1780,12 @@ __global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int stor
   if (do_stress) stress_update_point<D>(a, s, L);
 }
 
+template <int D, int SF>
+__global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int store_L) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < a.P.n) g2p_body<D, SF>(a, s, do_stress, store_L);
+}
+
 // Stress update alone from the stored velocity gradient.
 template <int D>
 __global__ void __launch_bounds__(256) k_stress_update(StepArgs a) {
@@ -1855,6 +1879,74 @@ __global__ void __launch_bounds__(256) k_point_update(DevMaterial mt, int n, flo
   }
 #pragma unroll
   for (int k = 0; k < 9; k++) S[(size_t)i * 9 + k] = Si[k];
+}
+
+// --------------------------------------------------------------------------
+// batched ensembles: one launch per phase for all instances
+// --------------------------------------------------------------------------
+//
+// Each CTA works inside one instance.  The instance's StepArgs view (grid,
+// node and key sub-arrays, materials, boundary conditions, dt) is copied
+// from device memory into shared memory, and the single-instance bodies run
+// on it unchanged.  Particle arrays are shared: instance i owns storage
+// slots [first_i, first_i + n_i), an invariant of the instance-major key
+// space (instance i's keys precede instance i+1's, and a particle outside
+// its grid takes its instance's sentinel key).
+
+struct BatchBlock {
+  int inst, first, end;  // particle block: storage slots [first, end) of instance inst
+};
+struct BatchTile {
+  int inst, tile, global_tile;  // node tile `tile` of instance inst
+};
+
+__device__ __forceinline__ void load_view(StepArgs &sa, const StepArgs *views, int inst, const DevParticles &P,
+                                          int epoch) {
+  const int *src = reinterpret_cast<const int *>(views + inst);
+  int *dst = reinterpret_cast<int *>(&sa);
+  constexpr int W = (int)(sizeof(StepArgs) / sizeof(int));
+  for (int k = threadIdx.x; k < W; k += blockDim.x) dst[k] = __ldg(src + k);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sa.P = P;
+    sa.epoch = epoch;
+  }
+  __syncthreads();
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(256) kb_hash_count(const StepArgs *views, const BatchBlock *blocks, DevParticles P,
+                                                     int epoch) {
+  __shared__ StepArgs sa;
+  const BatchBlock b = blocks[blockIdx.x];
+  load_view(sa, views, b.inst, P, epoch);
+  const int s = b.first + (int)threadIdx.x;
+  if (s < b.end) hash_count_body<D, SF>(sa, s);
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(TileDims<D>::N) kb_p2g(const StepArgs *views, const BatchTile *tiles,
+                                                         const int *tile_epoch, DevParticles P, int epoch,
+                                                         int apply_bcs, int *node_epoch, int gather) {
+  __shared__ StepArgs sa;
+  const BatchTile t = tiles[blockIdx.x];
+  if (tile_epoch[t.global_tile] != epoch) return;  // inactive: skip the view copy
+  load_view(sa, views, t.inst, P, epoch);
+  int *ne = node_epoch + (t.global_tile - t.tile);
+  if (gather)
+    p2g_gather_body<D, SF>(sa, t.tile, apply_bcs, ne);
+  else
+    p2g_tile_body<D, SF>(sa, t.tile, apply_bcs, ne);
+}
+
+template <int D, int SF>
+__global__ void __launch_bounds__(256) kb_g2p(const StepArgs *views, const BatchBlock *blocks, DevParticles P,
+                                              int epoch, int do_stress, int store_L) {
+  __shared__ StepArgs sa;
+  const BatchBlock b = blocks[blockIdx.x];
+  load_view(sa, views, b.inst, P, epoch);
+  const int s = b.first + (int)threadIdx.x;
+  if (s < b.end) g2p_body<D, SF>(sa, s, do_stress, store_L);
 }
 
 }  // namespace pmpm

@@ -108,6 +108,79 @@ def granular_bed(domain=(1.5, 0.6, 0.8), cell_size=1.0 / 160, bed=(1.0, 0.5, 0.3
     return d
 
 
+def _wave_timestep(mat, h, cfl):
+    """cfl * h / c with the p-wave speed c = sqrt((K + 4G/3) / rho), K and G in
+    FP32 as the material constructors, the root in double (tools.cpp:373-380);
+    a Newtonian fluid has G = 0."""
+    f = np.float32
+    rho = float(mat["density"])
+    if mat["type"] == "NewtonFluid":
+        K, G = f(mat["bulk_modulus"]), f(0.0)
+    else:
+        E, nu = f(mat["E"]), f(mat.get("pois", 0.0))
+        K = E / (f(3) * (f(1) - f(2) * nu))
+        G = E / (f(2) * (f(1) + nu))
+    c = f(np.sqrt((float(K) + 4.0 * float(G) / 3.0) / rho))
+    return float(f(cfl) * (f(h) / c))
+
+
+def ensemble(num=256, seed=3, shape_function="quadratic", np_range=(2000, 64000), grid_range=(64, 512), cfl=0.3):
+    """Batched-ensemble instances: 2D column collapses (even instances) and
+    disc impacts (odd), particle counts log-uniform in np_range, grids of
+    G x G nodes on [0,1]^2 with G log-uniform in grid_range, materials cycled
+    linear elastic (E ~ U[1, 20] MPa, nu 0.3) / Newtonian fluid (mu 1e-3,
+    K 2e6) / Drucker-Prager (E ~ U[1, 20] MPa, phi ~ U[20, 40] deg), dt from
+    each instance's CFL number.  Particles sit on a regular sub-cell lattice
+    of 2x2 to 4x4 per cell; where the grid cannot hold the drawn count with
+    at most 4x4 per cell over the scene's region, the count is the most it
+    holds."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(num):
+        target = float(np.exp(rng.uniform(np.log(np_range[0]), np.log(np_range[1]))))
+        G = int(round(np.exp(rng.uniform(np.log(grid_range[0]), np.log(grid_range[1])))))
+        h = 1.0 / (G - 1)
+        E = float(rng.uniform(1e6, 20e6))
+        phi = float(rng.uniform(20.0, 40.0))
+        kind = i % 3
+        if kind == 0:
+            mat = {"type": "LinearElastic", "density": 1000.0, "E": E, "pois": 0.3}
+        elif kind == 1:
+            mat = {"type": "NewtonFluid", "density": 1000.0, "viscosity": 1e-3, "bulk_modulus": 2e6, "gamma": 7.0}
+        else:
+            mat = {"type": "DruckerPrager", "density": 1500.0, "E": E, "pois": 0.3, "friction_angle": phi,
+                   "dilatancy_angle": 0.0, "cohesion": 0.0}
+        column = i % 2 == 0
+        region = 0.18 if column else 0.2  # area the scene's bodies may cover
+        ppc_1d = 2
+        while ppc_1d < 4 and target * (h / ppc_1d) ** 2 > region:
+            ppc_1d += 1
+        sp = h / ppc_1d
+        area = min(target * sp * sp, region)
+        if column:
+            w = float(np.sqrt(area / 2.0))
+            pts = _lattice(np.array([h, h]), np.array([h + w, h + 2.0 * w]), sp)
+            vel = np.zeros_like(pts)
+            bcs = [{"type": "Gravity", "gravity": [0.0, -9.81]},
+                   {"type": "NodeDomain", "face0_mode": [1, 1], "face1_mode": [1, 1]}]
+        else:
+            r = float(np.sqrt(area / (2.0 * np.pi)))
+            pts, vel = [], []
+            for k, c in enumerate(((0.3, 0.3), (0.7, 0.7))):
+                c = np.asarray(c)
+                lo = np.floor((c - r) / sp) * sp
+                p = _lattice(lo, lo + 2 * r + 2 * sp, sp)
+                p = p[((p - c) ** 2).sum(axis=1) < r * r]
+                pts.append(p)
+                vel.append(np.full_like(p, 0.5 if k == 0 else -0.5))
+            pts, vel = np.concatenate(pts), np.concatenate(vel)
+            bcs = [{"type": "NodeDomain", "face0_mode": [1, 1], "face1_mode": [1, 1]}]
+        out.append(dict(dim=2, origin=[0.0, 0.0], end=[1.0, 1.0], cell_size=h, shape_function=shape_function,
+                        dt=_wave_timestep(mat, h, cfl), particles_per_cell=ppc_1d * ppc_1d, alpha=0.99,
+                        materials=[mat], bcs=bcs, positions=pts, velocities=vel))
+    return out
+
+
 def sim_kwargs(scene):
     """Keyword arguments of Simulation / OracleSim from a scene dict."""
     keys = ["dim", "origin", "end", "cell_size", "shape_function", "dt", "particles_per_cell", "alpha",
