@@ -132,6 +132,24 @@ def barrier(pg):
         pg.barrier()
 
 
+def cpu_reference_ensemble(steps, num):
+    """The oracle on the first `num` instances of the ensemble, `steps` each."""
+    import oracle
+    from pyroclastmpm_b200 import scenes
+
+    insts = scenes.ensemble()[:num]
+    refs = [oracle.OracleSim(**scenes.sim_kwargs(sc), positions=sc["positions"],
+                             velocities=sc["velocities"]).initialize() for sc in insts]
+    t0 = time.perf_counter()
+    for r in refs:
+        r.solve(steps)
+    dt = time.perf_counter() - t0
+    n = sum(len(sc["positions"]) for sc in insts)
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+            "sample": f"first {num} ensemble instances ({n} particles), {steps} steps each, serial C oracle (FP32)",
+            "seconds": dt}
+
+
 def cpu_reference(config, steps, warmup, sample_scale):
     """The oracle (C restatement of the reference step, one thread) on a
     bounded sample of the workload: the same grid, the particle region scaled
@@ -139,6 +157,8 @@ def cpu_reference(config, steps, warmup, sample_scale):
     import oracle
     from pyroclastmpm_b200 import scenes
 
+    if config == "ensemble":
+        return cpu_reference_ensemble(max(steps, 1), 16)
     scene = scene_for(config, scale=sample_scale)
     ref = oracle.OracleSim(**scenes.sim_kwargs(scene), positions=scene["positions"],
                            velocities=scene["velocities"]).initialize()
@@ -174,8 +194,140 @@ def workload_name(config):
     return {"column": "granular column collapse 3D, Drucker-Prager, quadratic B-spline, 1,331,712 particles, "
                       "257x65x129 nodes, gravity + slip walls, dt 1e-5",
             "discs": "two-disc elastic impact 2D, linear, 2,528 particles, 51x51 nodes, dt 1e-3",
-            "bed": "granular bed 3D, Drucker-Prager, cubic B-spline, 4,915,200 particles, 241x97x129 nodes, dt 8e-6"
+            "bed": "granular bed 3D with a translating, turning half-cylinder scoop (SDF contact, Coulomb 0.3), "
+                   "Drucker-Prager, cubic B-spline, 4,915,200 particles, 241x97x129 nodes, dt 8e-6",
+            "ensemble": "batched ensemble of 256 2D instances (column collapses and disc impacts, 2k-64k particles, "
+                        "64^2-512^2 grids, LE / NF / DP cycled, per-instance CFL 0.3 dt), quadratic B-spline"
             }[config]
+
+
+def run_ensemble(args, world, rank, local, pg):
+    """Batched ensemble: all instances stepped by one launch per phase, timed
+    against one simulation handle per instance stepped one after another."""
+    import torch
+
+    from pyroclastmpm_b200 import Batch, Simulation, scenes
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    insts = scenes.ensemble()
+    n = sum(len(sc["positions"]) for sc in insts)
+    b = Batch(insts, device=local, stream=stream.cuda_stream, resort_interval=args.resort_interval).initialize()
+    b.solve(args.warmup)
+    if b.synchronize() != 0:
+        raise RuntimeError("device fault during warm-up")
+    barrier(pg)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = b.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    b.solve(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    clocks = sampler.stop()
+    barrier(pg)
+    launches = b.launch_count() - l0
+    ms = allreduce_max(pg, ev0.elapsed_time(ev1))
+    if b.synchronize() != 0:
+        raise RuntimeError("device fault in the timed region")
+    value = world * n * args.steps / (ms / 1000.0)
+    phases = np.zeros(3)
+    for _ in range(5):
+        p, _nl = b.profile_step()
+        phases += np.array(p)
+    phases /= 5
+
+    # one handle per instance, launched one after another on one stream
+    sims = []
+    for sc in insts:
+        sim = Simulation(**scenes.sim_kwargs(sc), device=local, stream=stream.cuda_stream,
+                         resort_interval=args.resort_interval)
+        sim.set_particles(sc["positions"], sc["velocities"]).initialize()
+        sims.append(sim)
+    for sim in sims:
+        sim.solve(args.warmup)
+    base_steps = max(3, args.steps // 4)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(base_steps):
+        for sim in sims:
+            sim.solve(1)
+    e1.record(stream)
+    e1.synchronize()
+    single_value = n * base_steps / (e0.elapsed_time(e1) / 1000.0)
+    for sim in sims:
+        sim.close()
+
+    # end to end: every instance's positions and velocities up from pinned
+    # host memory, one step, back again
+    pins = [(torch.empty((len(sc["positions"]), 2), dtype=torch.float32, pin_memory=True),
+             torch.empty((len(sc["positions"]), 2), dtype=torch.float32, pin_memory=True)) for sc in insts]
+    for i, (px, pv) in enumerate(pins):
+        px.copy_(torch.from_numpy(b.get(i, "positions")))
+        pv.copy_(torch.from_numpy(b.get(i, "velocities")))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, args.e2e_steps // 2)
+    for _ in range(e2e_steps):
+        for i, (px, pv) in enumerate(pins):
+            b.set_ptr(i, "positions", px.data_ptr(), px.numel() * 4)
+            b.set_ptr(i, "velocities", pv.data_ptr(), pv.numel() * 4)
+        b.solve(1)
+        for i, (px, pv) in enumerate(pins):
+            b.get_ptr(i, "positions", px.data_ptr(), px.numel() * 4)
+            b.get_ptr(i, "velocities", pv.data_ptr(), pv.numel() * 4)
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(pg, (time.perf_counter() - t0) / e2e_steps)
+    nbytes = n * 2 * 4 * 2
+
+    peak, peak_kind = load_peak()
+    st = 4
+    algo = {"partition": n * st * 4 + sum(sc_nodes(sc) for sc in insts) * st * 2,
+            "p2g": n * st * (2 + 2 + 1 + 1 + 4),
+            "g2p_stress": n * st * (2 + 2 + 4 + 4 + 1 + (2 + 2 + 4 + 4 + 1)) + n}
+    names = ["partition", "p2g", "g2p_stress"]
+    dom = int(np.argmax(phases))
+    achieved = algo[names[dom]] / (phases[dom] / 1000.0) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_ensemble(1, 16)
+        cpu.pop("seconds", None)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, numpy PCG64 seed 3)",
+            "config": {"workload": workload_name("ensemble"), "instances": len(insts), "particles_per_gpu": n,
+                       "grid_nodes": int(sum(sc_nodes(sc) for sc in insts)), "resort_interval": args.resort_interval,
+                       "l2": "state larger than L2 (no flush)", "parallelism": f"replicas x{world}",
+                       "one_sim_per_launch": {"value": single_value, "unit": "particle-steps/s",
+                                              "steps": base_steps,
+                                              "note": "one pmpm_sim per instance, stepped in turn on one stream"},
+                       "batched_over_one_sim_per_launch": value / single_value},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                         "algorithmic_bytes_per_launch": algo[names[dom]], "ms_per_launch": float(phases[dom])},
+            "phases_ms": dict(zip(names, [float(x) for x in phases])),
+            "clocks": clocks, "gpu_launches": int(launches),
+            "e2e": {"value": world * n / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": nbytes // 2,
+                    "d2h_bytes_per_step": nbytes // 2,
+                    "note": "per step: every instance's positions + velocities uploaded from pinned host memory, "
+                            "one batched step, read back (host wall clock around synchronised calls)"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
+def sc_nodes(sc):
+    n = 1
+    for a in range(sc["dim"]):
+        n *= int(np.float32(np.float32(sc["end"][a]) - np.float32(sc["origin"][a])) / np.float32(sc["cell_size"])) + 1
+    return n
 
 
 def main():
@@ -184,7 +336,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="column", choices=["column", "discs", "bed"])
+    ap.add_argument("--config", default="column", choices=["column", "discs", "bed", "ensemble"])
     ap.add_argument("--resort-interval", type=int, default=32)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=1)
@@ -196,6 +348,12 @@ def main():
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    if args.config == "ensemble":
+        run_ensemble(args, world, rank, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return
