@@ -94,7 +94,9 @@ enum {
 /* Material parameters; fill with the pmpm_material_* helpers.
  *   LINEAR_ELASTIC: {E, pois, lame, shear, bulk, corrected}
  *   NEWTON_FLUID:   {viscosity, bulk_modulus, gamma}
- *   DRUCKER_PRAGER: {K, G, eta, eta_bar, kc, p_apex, has_apex}
+ *   DRUCKER_PRAGER: {K, G, eta, eta_bar, kc, p_apex, has_apex, pois}
+ *                   (pois = -1 for the dp_rheo form, which takes no
+ *                   per-particle E / friction angle)
  *                   yield sqrt(J2) + eta p - kc (p = tr(sigma)/3) */
 typedef struct {
   int type;
@@ -171,6 +173,9 @@ typedef enum {
   PMPM_FIELD_FORCES_EXTERNAL = 11,   /* float [n][dim]    ::forces_external_gpu                    */
   PMPM_FIELD_EPS_E = 12,             /* float [n][dim][dim] Drucker-Prager elastic strain          */
   PMPM_FIELD_STRESS_REF = 13,        /* float [n][3][3]   Drucker-Prager reference stress          */
+  PMPM_FIELD_YOUNGS_MODULUS = 14,    /* float [n]  per-particle Drucker-Prager E (no reference
+                                        counterpart); first use fills it from the materials    */
+  PMPM_FIELD_FRICTION_ANGLE = 15,    /* float [n]  per-particle Drucker-Prager friction angle (deg) */
   PMPM_FIELD_NODE_MASSES = 20,       /* float [nodes]     NodesContainer::masses_gpu               */
   PMPM_FIELD_NODE_MOMENTS = 21,      /* float [nodes][dim] ::moments_gpu                           */
   PMPM_FIELD_NODE_MOMENTS_NT = 22,   /* float [nodes][dim] ::moments_nt_gpu                        */
@@ -376,6 +381,28 @@ int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float d
 int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const int *num_cells,
                            const float *positions, int num_particles, unsigned *hash_unsorted,
                            int *sorted_index, int *cell_start, int *cell_end, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Differentiable rollouts (no counterpart in the reference).  A rollout of
+ * nsteps USL steps from the current state keeps the particle state every
+ * checkpoint_every steps; the backward pass recomputes each segment from its
+ * checkpoint and runs the adjoint kernels step by step, giving the gradient
+ * of a loss on the final positions with respect to the per-particle
+ * Drucker-Prager Young's modulus and friction angle (PMPM_FIELD_YOUNGS_MODULUS
+ * / _FRICTION_ANGLE, filled from the materials if not set) and the initial
+ * positions and velocities.  Quadratic shape functions; Drucker-Prager and
+ * inert materials; Gravity and NodeDomain conditions.  The physical re-sort
+ * is off while a rollout is held.
+ * ------------------------------------------------------------------------- */
+int pmpm_rollout_forward(pmpm_sim *s, int nsteps, int checkpoint_every);
+/* Back to the state the last rollout started from (step counter included). */
+int pmpm_rollout_reset(pmpm_sim *s);
+/* grad_positions: dLoss/dx of the final positions [n][dim] (id order).
+ * Outputs (each may be NULL): [n] dLoss/dE, [n] dLoss/dphi (per degree),
+ * [n][dim] dLoss/dx0, [n][dim] dLoss/dv0.  All host or all device memory
+ * (on_device).  Leaves the simulation at the rollout's initial state. */
+int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_device, float *grad_youngs,
+                          float *grad_friction, float *grad_positions0, float *grad_velocities0);
 
 /* ---------------------------------------------------------------------------
  * Batched ensembles.  No counterpart in the reference (its settings are

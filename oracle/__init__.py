@@ -85,7 +85,7 @@ def _structs(precision):
                     ("node_ids", P), ("node_types", P),
                     ("num_materials", ctypes.c_int), ("materials", P),
                     ("num_bcs", ctypes.c_int), ("bcs", P),
-                    ("eps_e", P), ("stress_ref", P)]
+                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P)]
 
     return Grid, Material, BC, Sim
 
@@ -132,7 +132,8 @@ def material_params(mat: dict, precision: str = "f32"):
         kc = xi * c
         has_apex = 1.0 if eta > 0 else 0.0
         p_apex = kc / eta if eta > 0 else 0.0
-        return MAT_DRUCKER_PRAGER, dens, [bulk, shear, npr(eta), npr(eta_bar), npr(kc), npr(p_apex), has_apex, 0]
+        return MAT_DRUCKER_PRAGER, dens, [bulk, shear, npr(eta), npr(eta_bar), npr(kc), npr(p_apex), has_apex,
+                                          float(nu)]
     if t == "DP_rheo":
         # the reference's DP_rheo parameters (src/materials/dp_rheo.cpp:45-70)
         E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
@@ -143,7 +144,7 @@ def material_params(mat: dict, precision: str = "f32"):
         psi = npr(npr(mat.get("dilatancy_angle", 0.0)) * npr(math.pi / 180.0))
         eta_bar = npr(6.0 * math.sin(float(psi)) / (math.sqrt(3.0) * (3.0 + math.sin(float(psi)))))
         eta = npr(math.sqrt(1.0 / 3.0) * float(M))
-        return MAT_DRUCKER_PRAGER, dens, [bulk, shear, eta, eta_bar, npr(eta * Pt), Pt, 1.0, 0]
+        return MAT_DRUCKER_PRAGER, dens, [bulk, shear, eta, eta_bar, npr(eta * Pt), Pt, 1.0, -1.0]
     raise ValueError(f"unknown material {t}")
 
 
@@ -154,7 +155,8 @@ class OracleSim:
                  shape_function="linear", dt=1e-3, particles_per_cell=1, alpha=0.99,
                  materials=(), bcs=(), precision="f32", global_step=0,
                  stresses=None, volumes=None, masses=None, volumes_original=None,
-                 rigid_positions=None, rigid_velocities=None, rigid_colors=None):
+                 rigid_positions=None, rigid_velocities=None, rigid_colors=None,
+                 youngs_modulus=None, friction_angle=None):
         self.precision = precision
         self.lib = _lib(precision)
         Grid, Material, BC, Sim = _structs(precision)
@@ -217,6 +219,9 @@ class OracleSim:
         a["node_types"] = np.zeros((nn, 3), np.int32)
         a["eps_e"] = z(n, d, d)
         a["stress_ref"] = z(n, 3, 3)
+        if youngs_modulus is not None:
+            a["youngs"] = np.array(youngs_modulus, npr, copy=True).reshape(n)
+            a["friction"] = np.array(friction_angle, npr, copy=True).reshape(n)
         self.lib.or_node_ids(ctypes.byref(g), a["node_ids"].ctypes.data_as(ctypes.c_void_p))
         self.lib.or_node_types(ctypes.byref(g), self.sf, a["node_ids"].ctypes.data_as(ctypes.c_void_p),
                                a["node_types"].ctypes.data_as(ctypes.c_void_p))

@@ -1086,6 +1086,30 @@ void or_dp_point(int d, const REAL *L, REAL *sig, REAL *eps_e, const REAL *sref,
 /* Solver::stress_update (src/solver/solver.cpp:110-121): materials in list
  * order, each over all particles of its colour (LE and NF skip inactive
  * particles; the reference DP kernel does not check the flag). */
+/* Drucker-Prager parameters of one particle from its Young's modulus and
+ * friction angle (degrees): K = E / (3 (1 - 2 nu)), G = E / (2 (1 + nu)),
+ * eta = 6 sin(phi) / (sqrt(3) (3 - sin(phi))), xi = 6 cos(phi) / (same),
+ * kc = xi c, with nu = p[7], eta_bar = p[3] and the cohesion c recovered
+ * from the material's kc and eta. */
+static void dp_particle_params(const REAL *mp, REAL E, REAL phi_deg, REAL *out) {
+  double nu = mp[7], s3 = sqrt(3.0);
+  double eta_m = mp[2];
+  double sn_m = 3.0 * s3 * eta_m / (6.0 + s3 * eta_m);
+  double xi_m = 6.0 * sqrt(fmax(0.0, 1.0 - sn_m * sn_m)) / (s3 * (3.0 - sn_m));
+  double c = xi_m > 0 ? (double)mp[4] / xi_m : 0.0;
+  double phi = (double)phi_deg * 3.14159265358979323846 / 180.0;
+  double sn = sin(phi), cs = cos(phi);
+  double eta = 6.0 * sn / (s3 * (3.0 - sn)), xi = 6.0 * cs / (s3 * (3.0 - sn));
+  out[0] = (REAL)((double)E / (3.0 * (1.0 - 2.0 * nu)));
+  out[1] = (REAL)((double)E / (2.0 * (1.0 + nu)));
+  out[2] = (REAL)eta;
+  out[3] = mp[3];
+  out[4] = (REAL)(xi * c);
+  out[5] = eta > 0 ? (REAL)(xi * c / eta) : (REAL)0;
+  out[6] = eta > 0 ? (REAL)1 : (REAL)0;
+  out[7] = (REAL)nu;
+}
+
 void or_stress_update(or_sim *s) {
   int d = s->grid.dim;
   for (int mid = 0; mid < s->num_materials; mid++) {
@@ -1101,7 +1125,13 @@ void or_stress_update(or_sim *s) {
         if (!s->is_active[i]) continue;
         nf_point(d, L, sig, s->masses[i], s->volumes[i], s->volumes_original[i], m);
       } else if (m->type == OR_MAT_DRUCKER_PRAGER) {
-        or_dp_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->dt, m->p, 0);
+        const REAL *prm = m->p;
+        REAL pp[8];
+        if (s->youngs && m->p[7] >= 0) {
+          dp_particle_params(m->p, s->youngs[i], s->friction[i], pp);
+          prm = pp;
+        }
+        or_dp_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->dt, prm, 0);
       }
     }
   }

@@ -65,7 +65,8 @@ typedef struct {
 /* Material parameters.
  *   LINEAR_ELASTIC: p = {E, pois, lame, shear, bulk, corrected(0/1)}
  *   NEWTON_FLUID:   p = {viscosity, bulk_modulus, gamma}
- *   DRUCKER_PRAGER: p = {bulk K, shear G, eta, eta_bar, kc, p_apex, has_apex}
+ *   DRUCKER_PRAGER: p = {bulk K, shear G, eta, eta_bar, kc, p_apex, has_apex, pois}
+ *     (pois < 0: dp_rheo form, no per-particle parameters)
  *     yield  Phi = sqrt(J2) + eta*p - kc   (p = tr(sigma)/3, tension positive)
  */
 typedef struct {
@@ -131,6 +132,11 @@ typedef struct {
 
   /* Drucker-Prager history: elastic strain [n][dim][dim], reference stress [n][3][3] */
   REAL *eps_e, *stress_ref;
+
+  /* optional per-particle Drucker-Prager Young's modulus and friction angle
+   * (degrees) [n], or NULL: replace the material's K, G, eta, kc (friction
+   * form of the material only, p[7] = Poisson ratio >= 0) */
+  REAL *youngs, *friction;
 } or_sim;
 
 void or_grid_init(or_grid *g, int dim, const REAL *origin, const REAL *end, REAL cell_size);

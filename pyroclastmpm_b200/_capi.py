@@ -34,7 +34,7 @@ STATUS = {
 FIELDS = {
     "positions": 0, "velocities": 1, "stresses": 2, "F": 3, "velocity_gradient": 4, "masses": 5,
     "volumes": 6, "volumes_original": 7, "colors": 8, "is_rigid": 9, "is_active": 10,
-    "forces_external": 11, "eps_e": 12, "stress_ref": 13,
+    "forces_external": 11, "eps_e": 12, "stress_ref": 13, "youngs_modulus": 14, "friction_angle": 15,
     "node_masses": 20, "node_moments": 21, "node_moments_nt": 22, "node_ids": 23, "node_types": 24,
     "bins": 30, "hash_unsorted": 31, "hash_sorted": 32, "sorted_index": 33, "cell_start": 34, "cell_end": 35,
 }
@@ -82,6 +82,7 @@ EXPORTS = [
     "pmpm_get_step", "pmpm_set_step", "pmpm_synchronize", "pmpm_stream", "pmpm_material_point_update",
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
+    "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward",
 ]
 
 EXPORTS += [
@@ -121,6 +122,9 @@ def lib():
     L.pmpm_bc_rigidbodylevelset.argtypes = [i, fp, fp, i, i, ctypes.POINTER(BC)]
     L.pmpm_bc_rigid_sdf.argtypes = [i, i, fp, fp, f, f, fp, f, f, i, ctypes.POINTER(BC)]
     L.pmpm_calculate_timestep.argtypes = [f, f, f, f, f, fp]
+    L.pmpm_rollout_forward.argtypes = [vp, i, i]
+    L.pmpm_rollout_reset.argtypes = [vp]
+    L.pmpm_rollout_backward.argtypes = [vp, vp, i, vp, vp, vp, vp]
     L.pmpm_batch_create.argtypes = [i, ctypes.POINTER(Instance), i, vp, i, ctypes.POINTER(vp)]
     L.pmpm_batch_destroy.argtypes = [vp]
     L.pmpm_batch_initialize.argtypes = [vp]
@@ -267,6 +271,7 @@ def field_shape(name, dim, n, num_nodes, nsn=None):
         "positions": (n, dim), "velocities": (n, dim), "forces_external": (n, dim),
         "stresses": (n, 3, 3), "stress_ref": (n, 3, 3), "F": (n, dim, dim), "velocity_gradient": (n, dim, dim),
         "eps_e": (n, dim, dim), "masses": (n,), "volumes": (n,), "volumes_original": (n,),
+        "youngs_modulus": (n,), "friction_angle": (n,),
         "colors": (n,), "is_rigid": (n,), "is_active": (n,),
         "node_masses": (num_nodes,), "node_moments": (num_nodes, dim), "node_moments_nt": (num_nodes, dim),
         "node_ids": (num_nodes, 3), "node_types": (num_nodes, 3), "bins": (n, dim),
@@ -465,6 +470,35 @@ class Simulation:
         c = ctypes.c_longlong()
         check(lib().pmpm_launch_count(self._h, ctypes.byref(c)), "pmpm_launch_count")
         return c.value
+
+    # ---- differentiable rollouts ----
+    def rollout_forward(self, nsteps, checkpoint_every=25):
+        check(lib().pmpm_rollout_forward(self._h, int(nsteps), int(checkpoint_every)), "pmpm_rollout_forward")
+        return self
+
+    def rollout_reset(self):
+        check(lib().pmpm_rollout_reset(self._h), "pmpm_rollout_reset")
+        return self
+
+    def rollout_backward(self, grad_positions):
+        """Host arrays: returns (dL/dE, dL/dphi, dL/dx0, dL/dv0) for a loss
+        gradient dL/dx of the final positions."""
+        g = np.ascontiguousarray(np.asarray(grad_positions, np.float32).reshape(self.n, self.dim))
+        gE = np.empty(self.n, np.float32)
+        gp = np.empty(self.n, np.float32)
+        gx = np.empty((self.n, self.dim), np.float32)
+        gv = np.empty((self.n, self.dim), np.float32)
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        check(lib().pmpm_rollout_backward(self._h, ptr(g), 0, ptr(gE), ptr(gp), ptr(gx), ptr(gv)),
+              "pmpm_rollout_backward")
+        return gE, gp, gx, gv
+
+    def rollout_backward_ptr(self, grad_positions, grad_youngs, grad_friction, grad_positions0=0,
+                             grad_velocities0=0):
+        """Device pointers (integers; 0 for an output not wanted)."""
+        vp = lambda p: ctypes.c_void_p(p) if p else None
+        check(lib().pmpm_rollout_backward(self._h, vp(grad_positions), 1, vp(grad_youngs), vp(grad_friction),
+                                          vp(grad_positions0), vp(grad_velocities0)), "pmpm_rollout_backward")
 
     def active_nodes(self):
         c = ctypes.c_int()

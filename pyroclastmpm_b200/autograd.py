@@ -1,0 +1,65 @@
+"""torch.autograd wrapper of the differentiable USL rollout.
+
+``rollout(sim, youngs, friction, nsteps, checkpoint_every)`` runs `nsteps`
+steps of `sim` from its current state with per-particle Drucker-Prager
+Young's modulus and friction angle (CUDA float32 tensors [n], particle id
+order) and returns the final positions [n, dim] as a CUDA tensor.  Its
+backward runs the checkpointed adjoint in the native library and returns the
+gradients of the two parameter tensors, so a calibration loop is plain torch:
+
+    E = torch.full((n,), 5e6, device="cuda", requires_grad=True)
+    phi = torch.full((n,), 25.0, device="cuda", requires_grad=True)
+    x = rollout(sim, E, phi, 500, 25)
+    loss = ((x - target) ** 2).mean()
+    loss.backward()                  # E.grad, phi.grad
+
+Each forward starts from the state the first rollout started from (the
+simulation is reset to it), so repeated calls evaluate the same map.
+PyTorch is plumbing here: no torch operator runs on the step.
+"""
+from __future__ import annotations
+
+import torch
+
+from ._capi import Simulation
+
+
+class _Rollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, youngs, friction, sim: Simulation, nsteps: int, checkpoint_every: int):
+        if not (youngs.is_cuda and friction.is_cuda):
+            raise ValueError("parameters must be CUDA tensors")
+        n, d = sim.n, sim.dim
+        E = youngs.detach().to(torch.float32).contiguous()
+        phi = friction.detach().to(torch.float32).contiguous()
+        if E.numel() != n or phi.numel() != n:
+            raise ValueError("one parameter per particle expected")
+        if getattr(sim, "_rollout_started", False):
+            sim.rollout_reset()
+        torch.cuda.current_stream().synchronize()
+        sim.set_ptr("youngs_modulus", E.data_ptr(), 4 * n, on_device=True)
+        sim.set_ptr("friction_angle", phi.data_ptr(), 4 * n, on_device=True)
+        sim.rollout_forward(nsteps, checkpoint_every)
+        sim._rollout_started = True
+        x = torch.empty((n, d), dtype=torch.float32, device=youngs.device)
+        sim.get_ptr("positions", x.data_ptr(), 4 * n * d, on_device=True)
+        ctx.sim = sim
+        return x
+
+    @staticmethod
+    def backward(ctx, grad_x):
+        sim = ctx.sim
+        n = sim.n
+        g = grad_x.detach().to(torch.float32).contiguous()
+        gE = torch.empty(n, dtype=torch.float32, device=g.device)
+        gphi = torch.empty(n, dtype=torch.float32, device=g.device)
+        torch.cuda.current_stream().synchronize()
+        sim.rollout_backward_ptr(g.data_ptr(), gE.data_ptr(), gphi.data_ptr())
+        return gE, gphi, None, None, None
+
+
+def rollout(sim: Simulation, youngs: torch.Tensor, friction: torch.Tensor, nsteps: int,
+            checkpoint_every: int = 25) -> torch.Tensor:
+    """Final positions after `nsteps` steps, differentiable in the per-particle
+    Young's modulus and friction angle (degrees)."""
+    return _Rollout.apply(youngs, friction, sim, int(nsteps), int(checkpoint_every))

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "pmpm.h"
+#include "pmpm_adjoint.cuh"
 #include "pmpm_kernels.cuh"
 
 using namespace pmpm;
@@ -105,6 +106,16 @@ struct pmpm_sim {
   RigidState rigid;
   std::vector<SdfState> sdf;
   bool rigid_shift_pending = false;  // the next G2P moves rigid particles by their set velocity
+  // differentiable rollout: checkpoints of the particle state (storage-slot
+  // order, so the physical re-sort is off while a rollout is held)
+  struct Rollout {
+    int every = 0, nsteps = 0, start_step = 0;
+    std::vector<float *> ckpt;
+    float *seg = nullptr;
+    int seg_states = 0;
+    AdjState A{};
+    bool held = false;
+  } ro;
   bool has_planar = false, has_dp = false, has_sref = false;
 
   // particles (two storage sets, swapped by the physical re-sort)
@@ -149,7 +160,10 @@ int ensure_staging(pmpm_sim *s, size_t bytes) {
   return PMPM_OK;
 }
 
+void free_rollout(pmpm_sim *s);
+
 void free_particles(pmpm_sim *s) {
+  free_rollout(s);
   for (int k = 0; k < 2; k++) {
     DevParticles &P = s->P[k];
     dfree(P.x);
@@ -168,6 +182,8 @@ void free_particles(pmpm_sim *s) {
     dfree(P.rigid);
     dfree(P.id);
     dfree(P.hash);
+    dfree(P.pE);
+    dfree(P.pphi);
     P = DevParticles{};
   }
   dfree(s->slot);
@@ -415,7 +431,7 @@ int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
 template <int D, int SF>
 int step_once(pmpm_sim *s) {
   PMPM_TRY((launch_partition<D, SF>(s)));
-  if (s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
+  if (!s->ro.held && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
     PMPM_TRY(launch_reorder<D>(s));
   } else {
     s->steps_since_sort += 1;
@@ -556,6 +572,21 @@ __global__ void k_initial_masses(DevParticles P, int mat_id, float density) {
   P.m[s] = density * P.V[s];
 }
 
+// Per-particle Drucker-Prager parameters from the particles' materials:
+// E = 3 K (1 - 2 nu), friction angle of the material (0 elsewhere).
+__global__ void k_fill_particle_params(DevParticles P, const DevMaterial *mats, int nmat) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  float E = 0.0f, phi = 0.0f;
+  const int c = P.color[s];
+  if (c < nmat && mats[c].type == PMPM_MAT_DRUCKER_PRAGER && mats[c].p[7] >= 0.0f) {
+    E = 3.0f * mats[c].p[0] * (1.0f - 2.0f * mats[c].p[7]);
+    phi = mats[c].p[9];
+  }
+  P.pE[s] = E;
+  P.pphi[s] = phi;
+}
+
 __global__ void k_dp_init(DevParticles P, int D, int *nonzero_ref) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.n) return;
@@ -590,6 +621,8 @@ int field_info(const pmpm_sim *s, int field, size_t *bytes) {
     case PMPM_FIELD_MASSES:
     case PMPM_FIELD_VOLUMES:
     case PMPM_FIELD_VOLUMES_ORIGINAL:
+    case PMPM_FIELD_YOUNGS_MODULUS:
+    case PMPM_FIELD_FRICTION_ANGLE:
     case PMPM_FIELD_HASH_UNSORTED:
     case PMPM_FIELD_HASH_SORTED:
     case PMPM_FIELD_SORTED_INDEX:
@@ -619,6 +652,30 @@ int field_info(const pmpm_sim *s, int field, size_t *bytes) {
     default:
       return PMPM_ERR_INVALID_ARGUMENT;
   }
+}
+
+// Allocates the per-particle Drucker-Prager parameters on first use (both
+// storage sets) and fills them from the materials.
+int ensure_particle_params(pmpm_sim *s) {
+  if (s->P[0].pE) return PMPM_OK;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  for (int k = 0; k < 2; k++) {
+    PMPM_TRY(dalloc(&s->P[k].pE, (size_t)s->stride));
+    PMPM_TRY(dalloc(&s->P[k].pphi, (size_t)s->stride));
+  }
+  DevMaterial *dm = nullptr;
+  const int nmat = (int)s->mats.size();
+  if (nmat > 0) {
+    PMPM_CUDA(cudaMalloc(&dm, sizeof(DevMaterial) * nmat));
+    PMPM_CUDA(cudaMemcpy(dm, s->mats.data(), sizeof(DevMaterial) * nmat, cudaMemcpyHostToDevice));
+  }
+  DevParticles P = s->P[s->cur];
+  k_fill_particle_params<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, dm, nmat);
+  const cudaError_t e = cudaGetLastError();
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  if (dm) cudaFree(dm);
+  PMPM_CUDA(e);
+  return PMPM_OK;
 }
 
 int copy_out(pmpm_sim *s, const void *dev_src, void *dst, size_t bytes, int on_device) {
@@ -744,6 +801,7 @@ int pmpm_material_drucker_prager(float density, float E, float pois, float frict
   out->params[4] = (float)kc;
   out->params[5] = eta > 0.0 ? (float)(kc / eta) : 0.0f;
   out->params[6] = eta > 0.0 ? 1.0f : 0.0f;
+  out->params[7] = pois;
   return PMPM_OK;
 }
 
@@ -765,6 +823,7 @@ int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt,
   out->params[4] = eta * Pt;
   out->params[5] = Pt;
   out->params[6] = 1.0f;
+  out->params[7] = -1.0f;
   return PMPM_OK;
 }
 
@@ -931,7 +990,15 @@ static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
     dm.density = m.density;
     memcpy(dm.p, m.params, sizeof(dm.p));
     if (m.type == PMPM_MAT_NEWTON_FLUID) dm.p[3] = (float)(2.0 * (double)m.params[0] / 3.0);
-    if (m.type == PMPM_MAT_DRUCKER_PRAGER) s->has_dp = true;
+    if (m.type == PMPM_MAT_DRUCKER_PRAGER) {
+      s->has_dp = true;
+      // cohesion from kc = xi(phi) c, phi from eta = 6 sin(phi) / (sqrt(3) (3 - sin(phi)))
+      const double eta = m.params[2], s3 = std::sqrt(3.0);
+      const double sn = 3.0 * s3 * eta / (6.0 + s3 * eta);
+      const double xi = 6.0 * std::sqrt(std::max(0.0, 1.0 - sn * sn)) / (s3 * (3.0 - sn));
+      dm.p[8] = xi > 0.0 ? (float)((double)m.params[4] / xi) : 0.0f;
+      dm.p[9] = (float)(std::asin(std::min(1.0, sn)) * 180.0 / 3.14159265358979323846);
+    }
     s->mats.push_back(dm);
   }
   int st = PMPM_OK;
@@ -1335,6 +1402,12 @@ int pmpm_get_field(pmpm_sim *s, int field, void *dst, size_t bytes, int on_devic
     case PMPM_FIELD_MASSES: kind = 4; src = P.m; break;
     case PMPM_FIELD_VOLUMES: kind = 4; src = P.V; break;
     case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; src = P.V0; break;
+    case PMPM_FIELD_YOUNGS_MODULUS:
+    case PMPM_FIELD_FRICTION_ANGLE:
+      PMPM_TRY(ensure_particle_params(s));
+      kind = 4;
+      src = field == PMPM_FIELD_YOUNGS_MODULUS ? s->P[s->cur].pE : s->P[s->cur].pphi;
+      break;
     case PMPM_FIELD_COLORS: kind = 5; src = P.color; break;
     case PMPM_FIELD_IS_RIGID: kind = 5; src = P.rigid; break;
     case PMPM_FIELD_IS_ACTIVE: kind = 5; src = P.active; break;
@@ -1375,6 +1448,12 @@ int pmpm_set_field(pmpm_sim *s, int field, const void *src, size_t bytes, int on
     case PMPM_FIELD_MASSES: kind = 4; dstp = P.m; break;
     case PMPM_FIELD_VOLUMES: kind = 4; dstp = P.V; break;
     case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; dstp = P.V0; break;
+    case PMPM_FIELD_YOUNGS_MODULUS:
+    case PMPM_FIELD_FRICTION_ANGLE:
+      PMPM_TRY(ensure_particle_params(s));
+      kind = 4;
+      dstp = field == PMPM_FIELD_YOUNGS_MODULUS ? s->P[s->cur].pE : s->P[s->cur].pphi;
+      break;
     case PMPM_FIELD_COLORS: kind = 5; dstp = P.color; break;
     case PMPM_FIELD_IS_RIGID: kind = 5; dstp = P.rigid; break;
     case PMPM_FIELD_IS_ACTIVE: kind = 5; dstp = P.active; break;
@@ -1469,7 +1548,7 @@ int profile_step(pmpm_sim *s, float *ms, int *launches) {
   PMPM_CUDA(cudaEventRecord(ev[0], s->stream));
   PMPM_TRY((launch_partition<D, SF>(s)));
   n_launch += 7;
-  if (s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
+  if (!s->ro.held && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
     PMPM_TRY(launch_reorder<D>(s));
     n_launch += 1;
   } else {
@@ -2137,6 +2216,7 @@ int pmpm_batch_profile_step(pmpm_batch *b, float *ms, int *launches) {
 }
 
 static bool batch_field_ok(int field) {
+  if (field == PMPM_FIELD_YOUNGS_MODULUS || field == PMPM_FIELD_FRICTION_ANGLE) return false;
   return field < PMPM_FIELD_NODE_MASSES || (field >= PMPM_FIELD_NODE_MASSES && field <= PMPM_FIELD_NODE_TYPES) ||
          field == PMPM_FIELD_BINS;
 }
@@ -2177,6 +2257,203 @@ int pmpm_batch_synchronize(pmpm_batch *b) {
 int pmpm_batch_launch_count(const pmpm_batch *b, long long *count) {
   if (!b || !count) return PMPM_ERR_INVALID_ARGUMENT;
   *count = b->launches;
+  return PMPM_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Differentiable rollouts
+// ===========================================================================
+
+namespace {
+
+// Floats per storage slot of one saved particle state: x, v, F, stress,
+// elastic strain, volume.
+int state_floats(const pmpm_sim *s) {
+  const int D = s->dim;
+  return D + D + D * D + (D == 2 ? 4 : 6) + (D == 2 ? 3 : 6) + 1;
+}
+
+int copy_state(pmpm_sim *s, float *buf, bool save) {
+  const int D = s->dim, st = s->stride;
+  const DevParticles &P = s->P[s->cur];
+  float *arrays[6] = {P.x, P.v, P.F, P.sig, P.eps, P.V};
+  const int ncomp[6] = {D, D, D * D, D == 2 ? 4 : 6, D == 2 ? 3 : 6, 1};
+  size_t off = 0;
+  for (int k = 0; k < 6; k++) {
+    const size_t bytes = sizeof(float) * (size_t)ncomp[k] * st;
+    if (arrays[k]) {
+      if (save)
+        PMPM_CUDA(cudaMemcpyAsync(buf + off, arrays[k], bytes, cudaMemcpyDeviceToDevice, s->stream));
+      else
+        PMPM_CUDA(cudaMemcpyAsync(arrays[k], buf + off, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    off += (size_t)ncomp[k] * st;
+  }
+  return PMPM_OK;
+}
+
+void free_rollout(pmpm_sim *s) {
+  for (float *p : s->ro.ckpt) cudaFree(p);
+  s->ro.ckpt.clear();
+  for (float *p : {s->ro.seg, s->ro.A.x, s->ro.A.v, s->ro.A.F, s->ro.A.sig, s->ro.A.eps, s->ro.A.gE, s->ro.A.gphi,
+                   s->ro.A.node})
+    if (p) cudaFree(p);
+  s->ro.seg = nullptr;
+  s->ro.seg_states = 0;
+  s->ro.A = AdjState{};
+  s->ro.held = false;
+}
+
+int rollout_supported(const pmpm_sim *s) {
+  if (s->shape != PMPM_SHAPE_QUADRATIC || s->has_planar || s->rbls_index >= 0) return PMPM_ERR_NOT_SUPPORTED;
+  for (const DevMaterial &m : s->mats)
+    if (m.type != PMPM_MAT_DRUCKER_PRAGER && m.type != PMPM_MAT_NONE) return PMPM_ERR_NOT_SUPPORTED;
+  for (const DevBC &b : s->bcs)
+    if (b.type != PMPM_BC_GRAVITY && b.type != PMPM_BC_NODEDOMAIN) return PMPM_ERR_NOT_SUPPORTED;
+  return PMPM_OK;
+}
+
+template <int D, int SF>
+int adjoint_step(pmpm_sim *s) {
+  PMPM_TRY((launch_partition<D, SF>(s)));
+  PMPM_TRY((launch_p2g<D, SF>(s, 1)));
+  AdjState &A = s->ro.A;
+  PMPM_CUDA(cudaMemsetAsync(A.node, 0, sizeof(float) * 8 * (size_t)s->g.ntotal, s->stream));
+  StepArgs a = make_args(s);
+  kadj_g2p<D><<<blocks_for(s->n, 128), 128, 0, s->stream>>>(a, A);
+  PMPM_LAUNCHED();
+  kadj_grid<D><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, A);
+  PMPM_LAUNCHED();
+  kadj_p2g<D><<<blocks_for(s->n, 128), 128, 0, s->stream>>>(a, A);
+  PMPM_LAUNCHED();
+  s->launches += 3;
+  return PMPM_OK;
+}
+
+int adjoint_step_dispatch(pmpm_sim *s) {
+  return s->dim == 2 ? adjoint_step<2, PMPM_SHAPE_QUADRATIC>(s) : adjoint_step<3, PMPM_SHAPE_QUADRATIC>(s);
+}
+
+int to_id_order(pmpm_sim *s, int kind, const float *src, void *dst, size_t bytes, int on_device) {
+  PMPM_TRY(ensure_staging(s, bytes));
+  k_get_particles<<<blocks_for(s->n), kTPB, 0, s->stream>>>(s->P[s->cur], s->dim, kind, src, s->staging, 0);
+  PMPM_LAUNCHED();
+  return copy_out(s, s->staging, dst, bytes, on_device);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmpm_rollout_forward(pmpm_sim *s, int nsteps, int checkpoint_every) {
+  if (!s || nsteps < 1 || checkpoint_every < 1) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_TRY(rollout_supported(s));
+  PMPM_CUDA(cudaSetDevice(s->device));
+  free_rollout(s);
+  PMPM_TRY(ensure_particle_params(s));
+  const size_t per = (size_t)state_floats(s) * s->stride;
+  const int ncp = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  for (int c = 0; c < ncp; c++) {
+    float *buf = nullptr;
+    if (cudaMalloc(&buf, per * sizeof(float)) != cudaSuccess) {
+      free_rollout(s);
+      return PMPM_ERR_OUT_OF_MEMORY;
+    }
+    s->ro.ckpt.push_back(buf);
+  }
+  s->ro.every = checkpoint_every;
+  s->ro.nsteps = nsteps;
+  s->ro.start_step = s->step;
+  s->ro.held = true;
+  for (int k = 0; k < nsteps; k++) {
+    if (k % checkpoint_every == 0) PMPM_TRY(copy_state(s, s->ro.ckpt[k / checkpoint_every], true));
+    PMPM_TRY(PMPM_DISPATCH(s, step_once, s));
+  }
+  return PMPM_OK;
+}
+
+int pmpm_rollout_reset(pmpm_sim *s) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!s->ro.held || s->ro.ckpt.empty()) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  PMPM_TRY(copy_state(s, s->ro.ckpt[0], false));
+  s->step = s->ro.start_step;
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMPM_OK;
+}
+
+int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_device, float *grad_youngs,
+                          float *grad_friction, float *grad_positions0, float *grad_velocities0) {
+  if (!s || !grad_positions) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!s->ro.held) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  const int D = s->dim, st = s->stride;
+  const int NS = D == 2 ? 4 : 6, NE = D == 2 ? 3 : 6;
+  AdjState &A = s->ro.A;
+  const int every = s->ro.every, nsteps = s->ro.nsteps;
+  const size_t per = (size_t)state_floats(s) * st;
+  if (!A.x) {
+    PMPM_TRY(dalloc(&A.x, (size_t)D * st));
+    PMPM_TRY(dalloc(&A.v, (size_t)D * st));
+    PMPM_TRY(dalloc(&A.F, (size_t)D * D * st));
+    PMPM_TRY(dalloc(&A.sig, (size_t)NS * st));
+    PMPM_TRY(dalloc(&A.eps, (size_t)NE * st));
+    PMPM_TRY(dalloc(&A.gE, (size_t)st));
+    PMPM_TRY(dalloc(&A.gphi, (size_t)st));
+    PMPM_TRY(dalloc(&A.node, (size_t)8 * s->g.ntotal));
+  }
+  if (s->ro.seg_states < every) {
+    if (s->ro.seg) cudaFree(s->ro.seg);
+    s->ro.seg = nullptr;
+    s->ro.seg_states = 0;
+    if (cudaMalloc(&s->ro.seg, per * every * sizeof(float)) != cudaSuccess) return PMPM_ERR_OUT_OF_MEMORY;
+    s->ro.seg_states = every;
+  }
+  PMPM_CUDA(cudaMemsetAsync(A.v, 0, sizeof(float) * D * st, s->stream));
+  PMPM_CUDA(cudaMemsetAsync(A.F, 0, sizeof(float) * D * D * st, s->stream));
+  PMPM_CUDA(cudaMemsetAsync(A.sig, 0, sizeof(float) * NS * st, s->stream));
+  PMPM_CUDA(cudaMemsetAsync(A.eps, 0, sizeof(float) * NE * st, s->stream));
+  PMPM_CUDA(cudaMemsetAsync(A.gE, 0, sizeof(float) * st, s->stream));
+  PMPM_CUDA(cudaMemsetAsync(A.gphi, 0, sizeof(float) * st, s->stream));
+  PMPM_CUDA(cudaMemsetAsync(A.x, 0, sizeof(float) * D * st, s->stream));
+  // loss gradient of the final positions (id order) into storage order
+  {
+    const size_t bytes = sizeof(float) * (size_t)s->n * D;
+    const void *src = grad_positions;
+    if (!on_device) {
+      PMPM_TRY(ensure_staging(s, bytes));
+      PMPM_CUDA(cudaMemcpyAsync(s->staging, grad_positions, bytes, cudaMemcpyHostToDevice, s->stream));
+      src = s->staging;
+    }
+    DevParticles P = s->P[s->cur];
+    k_set_particles<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, D, 0, src, A.x);
+    PMPM_LAUNCHED();
+  }
+  const int ncp = (int)s->ro.ckpt.size();
+  for (int c = ncp - 1; c >= 0; c--) {
+    const int k0 = c * every, k1 = std::min(k0 + every, nsteps);
+    PMPM_TRY(copy_state(s, s->ro.ckpt[c], false));
+    s->step = s->ro.start_step + k0;
+    for (int j = k0; j < k1; j++) {
+      PMPM_TRY(copy_state(s, s->ro.seg + per * (j - k0), true));
+      if (j + 1 < k1) PMPM_TRY(PMPM_DISPATCH(s, step_once, s));
+    }
+    for (int j = k1 - 1; j >= k0; j--) {
+      PMPM_TRY(copy_state(s, s->ro.seg + per * (j - k0), false));
+      s->step = s->ro.start_step + j;
+      PMPM_TRY(adjoint_step_dispatch(s));
+    }
+  }
+  s->step = s->ro.start_step;
+  const size_t nb = sizeof(float) * (size_t)s->n;
+  if (grad_youngs) PMPM_TRY(to_id_order(s, 4, A.gE, grad_youngs, nb, on_device));
+  if (grad_friction) PMPM_TRY(to_id_order(s, 4, A.gphi, grad_friction, nb, on_device));
+  if (grad_positions0) PMPM_TRY(to_id_order(s, 0, A.x, grad_positions0, nb * D, on_device));
+  if (grad_velocities0) PMPM_TRY(to_id_order(s, 0, A.v, grad_velocities0, nb * D, on_device));
+  PMPM_CUDA(cudaStreamSynchronize(s->stream));
   return PMPM_OK;
 }
 

@@ -57,6 +57,7 @@ struct DevParticles {
   int n;
   int stride;
   float *x, *v, *F, *sig, *L, *m, *V, *V0, *fext, *eps, *sref;
+  float *pE, *pphi;  // per-particle Young's modulus and friction angle (deg) of Drucker-Prager, or null
   uint8_t *color, *active, *rigid;
   int *id;             // original particle id of each storage slot
   unsigned int *hash;  // reference cell hash of the last partition
@@ -98,7 +99,9 @@ struct DevBins {
 struct DevMaterial {
   int type;
   float density;
-  float p[8];
+  // p[0..7]: the pmpm_material parameters; Drucker-Prager (friction-angle
+  // form) also p[8] = cohesion, for per-particle parameters
+  float p[10];
 };
 
 struct DevBC {
@@ -497,6 +500,26 @@ __device__ __forceinline__ void dp_update(const float *prm, const float *L, floa
       if (a == b) e += dpk;
       eps[a * D + b] = e;
     }
+}
+
+// Drucker-Prager parameters {K, G, eta, eta_bar, kc, p_apex, has_apex} of one
+// particle from its Young's modulus E and friction angle phi (degrees), with
+// the material's Poisson ratio (p[7]), dilatancy (eta_bar, p[3]) and
+// cohesion (p[8]): the outer-cone fit of pmpm_material_drucker_prager.
+__device__ __forceinline__ void dp_particle_params(const DevMaterial &mt, float E, float phi_deg, float prm[8]) {
+  const float nu = mt.p[7], c = mt.p[8];
+  const float phi = phi_deg * 0.017453292519943295f;
+  const float sn = sinf(phi), cs = cosf(phi);
+  const float den = 1.7320508075688772f * (3.0f - sn);
+  const float eta = 6.0f * sn / den, xi = 6.0f * cs / den;
+  prm[0] = E / (3.0f * (1.0f - 2.0f * nu));
+  prm[1] = E / (2.0f * (1.0f + nu));
+  prm[2] = eta;
+  prm[3] = mt.p[3];
+  prm[4] = xi * c;
+  prm[5] = eta > 0.0f ? prm[4] / eta : 0.0f;
+  prm[6] = eta > 0.0f ? 1.0f : 0.0f;
+  prm[7] = nu;
 }
 
 // --------------------------------------------------------------------------

@@ -414,6 +414,10 @@ __global__ void __launch_bounds__(256) k_reorder(StepArgs a, DevParticles dst, i
   move_comps(S.active, dst.active, 1, st, s, k);
   move_comps(S.rigid, dst.rigid, 1, st, s, k);
   move_comps(S.id, dst.id, 1, st, s, k);
+  if (S.pE) {
+    move_comps(S.pE, dst.pE, 1, st, s, k);
+    move_comps(S.pphi, dst.pphi, 1, st, s, k);
+  }
   move_comps(S.hash, dst.hash, 1, st, s, k);
   a.B.order[k] = k;  // storage is now in cell order
 }
@@ -1629,7 +1633,13 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
 #pragma unroll
       for (int k = 0; k < 9; k++) sref[k] = 0.0f;
     }
-    dp_update<D>(mt.p, L, a.dt, eps, sref, S, false);
+    float prm[8];
+    const float *pp = mt.p;
+    if (P.pE && mt.p[7] >= 0.0f) {
+      dp_particle_params(mt, P.pE[s], P.pphi[s], prm);
+      pp = prm;
+    }
+    dp_update<D>(pp, L, a.dt, eps, sref, S, false);
 #pragma unroll
     for (int x = 0; x < D; x++)
 #pragma unroll

@@ -181,6 +181,31 @@ def ensemble(num=256, seed=3, shape_function="quadratic", np_range=(2000, 64000)
     return out
 
 
+def calibration_cube(n_side=64, cell_size=1.0 / 128, domain=0.5, seed=2, dt=2e-5, E_median=5e6, E_sigma=0.2,
+                     phi_mean=25.0, phi_std=3.0, target_E=1e7, target_phi=30.0):
+    """Differentiable-calibration cube: n_side^3 particles on a 2x2x2 lattice
+    per cell (side n_side/2 cells) standing on the floor of a domain^3 box,
+    Drucker-Prager (rho 1500, nu 0.3, psi 0, c 0), quadratic B-splines,
+    gravity, slip walls.  Returns the scene with the initial per-particle
+    parameters (E log-normal around E_median, phi normal, numpy PCG64 `seed`)
+    and the target parameters."""
+    spacing = cell_size / 2
+    side = n_side * spacing
+    lo = np.array([0.5 * (domain - side), 0.5 * (domain - side), 0.0])
+    pts = _lattice(lo, lo + side, spacing)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    E = E_median * np.exp(rng.normal(0.0, E_sigma, len(pts)))
+    phi = rng.normal(phi_mean, phi_std, len(pts))
+    scene = dict(dim=3, origin=[0.0, 0.0, 0.0], end=[domain] * 3, cell_size=cell_size,
+                 shape_function="quadratic", dt=dt, particles_per_cell=8, alpha=0.99,
+                 materials=[{"type": "DruckerPrager", "density": 1500.0, "E": target_E, "pois": 0.3,
+                             "friction_angle": target_phi, "dilatancy_angle": 0.0, "cohesion": 0.0}],
+                 bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]},
+                      {"type": "NodeDomain", "face0_mode": [1, 1, 1], "face1_mode": [1, 1, 1]}],
+                 positions=pts, velocities=np.zeros_like(pts))
+    return scene, E.astype(np.float32), phi.astype(np.float32), (target_E, target_phi)
+
+
 def sim_kwargs(scene):
     """Keyword arguments of Simulation / OracleSim from a scene dict."""
     keys = ["dim", "origin", "end", "cell_size", "shape_function", "dt", "particles_per_cell", "alpha",

@@ -1,0 +1,123 @@
+"""Differentiable rollouts: per-particle Drucker-Prager parameters in the
+forward step, and the checkpointed adjoint against finite differences of
+the FP64 oracle (directional derivatives, central differences).
+
+The loss is the mean squared distance of the final positions from a target
+rollout made with other parameters, as in the calibration configuration.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from pyroclastmpm_b200 import Simulation, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def small_cube(steps_dt=1e-4):
+    scene, E, phi, target = scenes.calibration_cube(n_side=16, cell_size=1.0 / 32, domain=0.5, dt=steps_dt)
+    return scene, E, phi, target
+
+
+def oracle_final(scene, E, phi, steps, precision="f64", x0=None, v0=None):
+    o = oracle.OracleSim(**scenes.sim_kwargs(scene), positions=scene["positions"] if x0 is None else x0,
+                         velocities=scene["velocities"] if v0 is None else v0, youngs_modulus=E,
+                         friction_angle=phi, precision=precision).initialize()
+    o.solve(steps)
+    return np.array(o["positions"], np.float64)
+
+
+def make_sim(scene, E, phi):
+    sim = Simulation(**scenes.sim_kwargs(scene))
+    sim.set_particles(scene["positions"], scene["velocities"]).initialize()
+    sim.set("youngs_modulus", E)
+    sim.set("friction_angle", phi)
+    return sim
+
+
+def test_per_particle_parameters_forward_matches_oracle():
+    scene, E, phi, _ = small_cube()
+    sim = make_sim(scene, E, phi)
+    np.testing.assert_array_equal(sim.get("youngs_modulus"), E)
+    sim.solve(10)
+    assert sim.synchronize() == 0
+    ref = [oracle.OracleSim(**scenes.sim_kwargs(scene), positions=scene["positions"],
+                            velocities=scene["velocities"], youngs_modulus=E, friction_angle=phi,
+                            precision=p).initialize() for p in ("f32", "f64")]
+    for r in ref:
+        r.solve(10)
+    for name in ("positions", "velocities", "stresses"):
+        tol = max(1e-5, 3 * rel(ref[0][name], ref[1][name]))
+        assert rel(sim.get(name), ref[0][name]) <= tol, name
+    # the material's own values reproduce the material path
+    sim2 = Simulation(**scenes.sim_kwargs(scene))
+    sim2.set_particles(scene["positions"], scene["velocities"]).initialize()
+    filled = sim2.get("youngs_modulus")
+    np.testing.assert_allclose(filled, 1e7, rtol=1e-6)
+    np.testing.assert_allclose(sim2.get("friction_angle"), 30.0, rtol=1e-5)
+
+
+@pytest.mark.parametrize("steps,every", [(3, 1), (12, 5)])
+def test_adjoint_matches_fp64_finite_differences(steps, every):
+    scene, E, phi, (tE, tphi) = small_cube()
+    n = len(scene["positions"])
+    target = oracle_final(scene, np.full(n, tE), np.full(n, tphi), steps)
+
+    def loss(x):
+        return float(((x - target) ** 2).sum() / n)
+
+    sim = make_sim(scene, E, phi)
+    sim.rollout_forward(steps, every)
+    x = sim.get("positions").astype(np.float64)
+    gE, gphi, gx0, gv0 = sim.rollout_backward(2.0 * (x - target) / n)
+    # the backward leaves the simulation at the initial state
+    np.testing.assert_array_equal(sim.get("positions"), scene["positions"].astype(np.float32))
+
+    rng = np.random.default_rng(0)
+    dE = E * rng.normal(0, 1, n)
+    dphi = rng.normal(0, 1, n)
+    dx = rng.normal(0, 1e-3 * scene["cell_size"], (n, 3))
+    dv = rng.normal(0, 1e-2, (n, 3))
+    cases = [
+        ("E", np.dot(gE.astype(np.float64), dE), lambda e: oracle_final(scene, E + e * dE, phi, steps)),
+        ("phi", np.dot(gphi.astype(np.float64), dphi), lambda e: oracle_final(scene, E, phi + e * dphi, steps)),
+        ("x0", (gx0.astype(np.float64) * dx).sum(),
+         lambda e: oracle_final(scene, E, phi, steps, x0=scene["positions"] + e * dx)),
+        ("v0", (gv0.astype(np.float64) * dv).sum(),
+         lambda e: oracle_final(scene, E, phi, steps, v0=scene["velocities"] + e * dv)),
+    ]
+    eps = 1e-3
+    for name, adj, run in cases:
+        fd = (loss(run(eps)) - loss(run(-eps))) / (2 * eps)
+        assert abs(adj - fd) <= 2e-2 * abs(fd) + 1e-12, f"{name}: adjoint {adj:.6e} vs FD {fd:.6e}"
+
+
+def test_autograd_function_matches_direct_backward():
+    torch = pytest.importorskip("torch")
+    from pyroclastmpm_b200.autograd import rollout
+
+    scene, E, phi, _ = small_cube()
+    n = len(scene["positions"])
+    sim = make_sim(scene, E, phi)
+    target = torch.tensor(scene["positions"], dtype=torch.float32, device="cuda") + 0.001
+    Et = torch.tensor(E, device="cuda", requires_grad=True)
+    pt = torch.tensor(phi, device="cuda", requires_grad=True)
+    for _ in range(2):  # a second evaluation starts from the same state
+        x = rollout(sim, Et, pt, 6, 3)
+        loss = ((x - target) ** 2).sum() / n
+        Et.grad = None
+        pt.grad = None
+        loss.backward()
+    sim2 = make_sim(scene, E, phi)
+    sim2.rollout_forward(6, 3)
+    x2 = sim2.get("positions")
+    np.testing.assert_allclose(x.detach().cpu().numpy(), x2, rtol=0, atol=1e-6)
+    gE, gphi, _, _ = sim2.rollout_backward(2.0 * (x2 - target.cpu().numpy()) / n)
+    np.testing.assert_allclose(Et.grad.cpu().numpy(), gE, rtol=1e-3, atol=1e-3 * np.abs(gE).max())
+    np.testing.assert_allclose(pt.grad.cpu().numpy(), gphi, rtol=1e-3, atol=1e-3 * np.abs(gphi).max())
