@@ -196,6 +196,9 @@ def workload_name(config):
             "discs": "two-disc elastic impact 2D, linear, 2,528 particles, 51x51 nodes, dt 1e-3",
             "bed": "granular bed 3D with a translating, turning half-cylinder scoop (SDF contact, Coulomb 0.3), "
                    "Drucker-Prager, cubic B-spline, 4,915,200 particles, 241x97x129 nodes, dt 8e-6",
+            "calibration": "differentiable calibration rollout: 3D Drucker-Prager cube, 262,144 particles "
+                           "(64^3 lattice, h 1/128), quadratic, per-particle E and friction angle, 500 steps of "
+                           "dt 2e-5, checkpoints every 25, forward + adjoint",
             "ensemble": "batched ensemble of 256 2D instances (column collapses and disc impacts, 2k-64k particles, "
                         "64^2-512^2 grids, LE / NF / DP cycled, per-instance CFL 0.3 dt), quadratic B-spline"
             }[config]
@@ -323,6 +326,109 @@ def run_ensemble(args, world, rank, local, pg):
     b.close()
 
 
+def run_calibration(args, world, rank, local, pg):
+    """Differentiable calibration rollout: forward with checkpoints plus the
+    adjoint, against the plain forward of the same rollout."""
+    import torch
+
+    from pyroclastmpm_b200 import Simulation, scenes
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    nsteps, every = args.rollout_steps, 25
+    scene, E, phi, (tE, tphi) = scenes.calibration_cube()
+    n = len(scene["positions"])
+    kw = scenes.sim_kwargs(scene)
+    # target rollout with the target parameters (the material's own)
+    tgt = Simulation(**kw, device=local, stream=stream.cuda_stream)
+    tgt.set_particles(scene["positions"], scene["velocities"]).initialize()
+    tgt.solve(nsteps)
+    target = tgt.get("positions").astype(np.float64)
+    tgt.close()
+    sim = Simulation(**kw, device=local, stream=stream.cuda_stream)
+    sim.set_particles(scene["positions"], scene["velocities"]).initialize()
+    sim.set("youngs_modulus", E)
+    sim.set("friction_angle", phi)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    # warm-up: a short rollout and its adjoint
+    for _ in range(max(1, args.warmup // 3)):
+        sim.rollout_forward(2 * every, every)
+        x = sim.get("positions")
+        sim.rollout_backward(np.zeros_like(x))
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    # the plain forward of the same rollout (normal stepping, re-sorts on)
+    plain = Simulation(**kw, device=local, stream=stream.cuda_stream)
+    plain.set_particles(scene["positions"], scene["velocities"]).initialize()
+    plain.set("youngs_modulus", E)
+    plain.set("friction_angle", phi)
+    plain.solve(args.warmup)
+    ms_plain, _ = timed(lambda: plain.solve(nsteps))
+    plain.close()
+    # the warm-up's backward left `sim` at the initial state
+    l0 = sim.launch_count()
+    ms_fwd, _ = timed(lambda: sim.rollout_forward(nsteps, every))
+    x = sim.get("positions").astype(np.float64)
+    loss = float(((x - target) ** 2).sum() / n)
+    grad = (2.0 * (x - target) / n).astype(np.float32)
+    ms_bwd, out = timed(lambda: sim.rollout_backward(grad))
+    clocks = sampler.stop()
+    launches = sim.launch_count() - l0
+    if sim.synchronize() != 0:
+        raise RuntimeError("device fault in the timed region")
+    gE, gphi = out[0], out[1]
+    ms_total = allreduce_max(pg, ms_fwd + ms_bwd)
+    value = world * n * nsteps / (ms_total / 1000.0)
+    # G2P-side adjoint traffic per particle-step: state in, adjoints in and out
+    peak, peak_kind = load_peak()
+    ms_adj_step = ms_bwd / nsteps
+    adj_bytes = n * 4 * (28 + 2 * 27 + 2 * 27)
+    achieved = adj_bytes / (ms_adj_step / 1000.0) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference("column", 1, 0, 0.3)
+        cpu.pop("seconds", None)
+        cpu["sample"] += " (forward only: the reference has no adjoint)"
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": nsteps,
+            "warmup": args.warmup, "ms_per_step": ms_total / nsteps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (64^3 lattice cube, numpy PCG64 seed 2)",
+            "config": {"workload": workload_name("calibration"), "particles_per_gpu": n,
+                       "checkpoint_every": every, "parallelism": f"replicas x{world}",
+                       "l2": "state larger than L2 (no flush)",
+                       "plain_forward_ms_per_step": ms_plain / nsteps,
+                       "rollout_forward_ms_per_step": ms_fwd / nsteps,
+                       "adjoint_ms_per_step": ms_bwd / nsteps,
+                       "fwd_plus_adjoint_over_plain_forward": (ms_fwd + ms_bwd) / ms_plain,
+                       "loss": loss, "grad_norm_E": float(np.linalg.norm(gE)),
+                       "grad_norm_phi": float(np.linalg.norm(gphi))},
+            "roofline": {"bound": "hbm", "kernel": "adjoint step (3 kernels + recomputed P2G)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                         "algorithmic_bytes_per_launch": adj_bytes, "ms_per_launch": ms_adj_step},
+            "clocks": clocks, "gpu_launches": int(launches),
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(grad.nbytes // nsteps),
+                    "d2h_bytes_per_step": int((gE.nbytes + gphi.nbytes + 4 * 3 * n) // nsteps),
+                    "note": "rollout through the C ABI: loss gradient uploaded from host, parameter gradients "
+                            "and final positions read back; per-step share of those bytes"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+
+
 def sc_nodes(sc):
     n = 1
     for a in range(sc["dim"]):
@@ -336,7 +442,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="column", choices=["column", "discs", "bed", "ensemble"])
+    ap.add_argument("--config", default="column", choices=["column", "discs", "bed", "ensemble", "calibration"])
+    ap.add_argument("--rollout-steps", type=int, default=500)
     ap.add_argument("--resort-interval", type=int, default=32)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=1)
@@ -352,8 +459,8 @@ def main():
             pg.destroy_process_group()
         return
 
-    if args.config == "ensemble":
-        run_ensemble(args, world, rank, local, pg)
+    if args.config in ("ensemble", "calibration"):
+        (run_ensemble if args.config == "ensemble" else run_calibration)(args, world, rank, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return
