@@ -20,6 +20,8 @@
 // NodeDomain as node conditions; Drucker-Prager and inert materials.
 #pragma once
 
+#include <climits>
+
 #include "pmpm_kernels.cuh"
 
 namespace pmpm {
@@ -421,11 +423,21 @@ __device__ __forceinline__ void load_node_vel(const StepArgs &a, int node, float
 }
 
 // Backward of G2P, the F update and the stress update of one particle.
+//
+// The node adjoints are first summed in shared memory over the node box the
+// CTA's particles touch (consecutive storage slots are spatially close: cell
+// order after a re-sort, input order otherwise), then added to global
+// memory once per node; a CTA whose box exceeds kAdjBoxNodes adds directly.
+constexpr int kAdjBoxNodes = 1536;
+
 template <int D>
 __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ int box[6];
+  __shared__ float acc[kAdjBoxNodes * 6];
+  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
   const DevParticles &P = a.P;
-  if (s >= P.n) return;
+  const bool valid = s0 < P.n;
+  const int s = valid ? s0 : P.n - 1;
   const DevGrid &g = a.g;
   const int st = P.stride;
   constexpr int NE = Sym<D>::E, NS = Sym<D>::S;
@@ -437,6 +449,36 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
   }
   QuadStencil<D> Q;
   Q.build(g, x);
+  // ---- node box of the CTA ----
+  if (threadIdx.x < 3) {
+    box[threadIdx.x] = INT_MAX;
+    box[3 + threadIdx.x] = -1;
+  }
+  __syncthreads();
+  const bool contributes = valid && Q.inside;
+  if (contributes) {
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      atomicMin(&box[c], Q.idx[c][0]);
+      atomicMax(&box[3 + c], Q.idx[c][2]);
+    }
+  }
+  __syncthreads();
+  int bx = 1, by = 1, bz = 1, b0x = 0, b0y = 0, b0z = 0;
+  if (box[3] >= 0) {
+    b0x = box[0];
+    b0y = box[1];
+    bx = box[3] - box[0] + 1;
+    by = box[4] - box[1] + 1;
+    if (D == 3) {
+      b0z = box[2];
+      bz = box[5] - box[2] + 1;
+    }
+  }
+  const bool use_smem = box[3] >= 0 && bx * by * bz <= kAdjBoxNodes;
+  const int nbox = use_smem ? bx * by * bz : 0;
+  for (int k = threadIdx.x; k < nbox * 6; k += blockDim.x) acc[k] = 0.0f;
+  __syncthreads();
   // incoming adjoints (of the step's outputs)
   float xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, Fb[9], sb[6] = {0, 0, 0, 0, 0, 0}, eb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -454,7 +496,7 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
   float vo[3] = {0, 0, 0}, Fo[9], eo[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int k = 0; k < 9; k++) Fo[k] = 0.0f;
-  if (Q.inside) {
+  if (contributes) {
     // recompute L
     float L[9];
 #pragma unroll
@@ -543,7 +585,13 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
           const float w = Q.eval(kx, ky, kz, gw, H);
           const int node = Q.node(g, kx, ky, kz);
           load_node_vel<D>(a, node, vn, vnt);
-          float* na = A.node + (size_t)node * 8;
+          float *na;
+          if (use_smem) {
+            const int lx = Q.idx[0][kx] - b0x, ly = Q.idx[1][ky] - b0y, lz = D == 3 ? Q.idx[2][kz] - b0z : 0;
+            na = acc + 6 * (lx + bx * (ly + by * lz));
+          } else {
+            na = A.node + (size_t)node * 8;
+          }
           float coef = 0.0f;  // d/dw of (pic . vnt + dv . (vnt - vn))
 #pragma unroll
           for (int c = 0; c < D; c++) {
@@ -577,6 +625,17 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
 #pragma unroll
     for (int k = 0; k < NE; k++) eo[k] = eb[k];
   }
+  // ---- box sums -> global node adjoints ----
+  __syncthreads();
+  for (int k = threadIdx.x; k < nbox; k += blockDim.x) {
+    const int lx = k % bx, ly = (k / bx) % by, lz = k / (bx * by);
+    const int node = (b0x + lx) + (b0y + ly) * g.n[0] + (D == 3 ? (b0z + lz) * g.n[0] * g.n[1] : 0);
+    const float *src = acc + 6 * k;
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      if (src[c] != 0.0f) atomicAdd(A.node + (size_t)node * 8 + c, src[c]);
+  }
+  if (!valid) return;
 #pragma unroll
   for (int c = 0; c < D; c++) {
     A.x[c * st + s] = xo[c];

@@ -113,6 +113,8 @@ struct pmpm_sim {
     std::vector<float *> ckpt;
     float *seg = nullptr;
     int seg_states = 0;
+    char *seg_nodes = nullptr;  // node data of each segment step's P2G
+    std::vector<int> seg_epoch;
     AdjState A{};
     bool held = false;
   } ro;
@@ -2300,6 +2302,8 @@ void free_rollout(pmpm_sim *s) {
   for (float *p : {s->ro.seg, s->ro.A.x, s->ro.A.v, s->ro.A.F, s->ro.A.sig, s->ro.A.eps, s->ro.A.gE, s->ro.A.gphi,
                    s->ro.A.node})
     if (p) cudaFree(p);
+  if (s->ro.seg_nodes) cudaFree(s->ro.seg_nodes);
+  s->ro.seg_nodes = nullptr;
   s->ro.seg = nullptr;
   s->ro.seg_states = 0;
   s->ro.A = AdjState{};
@@ -2315,13 +2319,45 @@ int rollout_supported(const pmpm_sim *s) {
   return PMPM_OK;
 }
 
+// Bytes of one node snapshot: mass, moments, forward moments, packed
+// velocities and the tile activity marks of one step's P2G.
+size_t node_snapshot_bytes(const pmpm_sim *s) {
+  const size_t nn = (size_t)s->g.ntotal, D = (size_t)s->dim;
+  const size_t F = s->dim == 3 ? NodeVel<3>::F : NodeVel<2>::F;
+  return sizeof(float) * nn * (1 + 2 * D + F) + sizeof(int) * (size_t)s->g.ntiles;
+}
+
+int copy_nodes(pmpm_sim *s, char *buf, bool save) {
+  const size_t nn = (size_t)s->g.ntotal, D = (size_t)s->dim;
+  const size_t F = s->dim == 3 ? NodeVel<3>::F : NodeVel<2>::F;
+  void *arrays[5] = {s->N.m, s->N.p, s->N.pnt, s->N.vel, s->N.tile_epoch};
+  const size_t bytes[5] = {4 * nn, 4 * D * nn, 4 * D * nn, 4 * F * nn, 4 * (size_t)s->g.ntiles};
+  size_t off = 0;
+  for (int k = 0; k < 5; k++) {
+    if (save)
+      PMPM_CUDA(cudaMemcpyAsync(buf + off, arrays[k], bytes[k], cudaMemcpyDeviceToDevice, s->stream));
+    else
+      PMPM_CUDA(cudaMemcpyAsync(arrays[k], buf + off, bytes[k], cudaMemcpyDeviceToDevice, s->stream));
+    off += bytes[k];
+  }
+  return PMPM_OK;
+}
+
+// The step's P2G alone (partition and P2G with the node conditions).
 template <int D, int SF>
-int adjoint_step(pmpm_sim *s) {
+int p2g_only(pmpm_sim *s) {
   PMPM_TRY((launch_partition<D, SF>(s)));
   PMPM_TRY((launch_p2g<D, SF>(s, 1)));
+  return PMPM_OK;
+}
+
+// Backward of one step whose state and P2G node data are in place.
+template <int D, int SF>
+int adjoint_step(pmpm_sim *s, int epoch) {
   AdjState &A = s->ro.A;
   PMPM_CUDA(cudaMemsetAsync(A.node, 0, sizeof(float) * 8 * (size_t)s->g.ntotal, s->stream));
   StepArgs a = make_args(s);
+  a.epoch = epoch;  // the epoch the restored tile marks carry
   kadj_g2p<D><<<blocks_for(s->n, 128), 128, 0, s->stream>>>(a, A);
   PMPM_LAUNCHED();
   kadj_grid<D><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, A);
@@ -2332,8 +2368,9 @@ int adjoint_step(pmpm_sim *s) {
   return PMPM_OK;
 }
 
-int adjoint_step_dispatch(pmpm_sim *s) {
-  return s->dim == 2 ? adjoint_step<2, PMPM_SHAPE_QUADRATIC>(s) : adjoint_step<3, PMPM_SHAPE_QUADRATIC>(s);
+int adjoint_step_dispatch(pmpm_sim *s, int epoch) {
+  return s->dim == 2 ? adjoint_step<2, PMPM_SHAPE_QUADRATIC>(s, epoch)
+                     : adjoint_step<3, PMPM_SHAPE_QUADRATIC>(s, epoch);
 }
 
 int to_id_order(pmpm_sim *s, int kind, const float *src, void *dst, size_t bytes, int on_device) {
@@ -2405,13 +2442,18 @@ int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_devic
     PMPM_TRY(dalloc(&A.gphi, (size_t)st));
     PMPM_TRY(dalloc(&A.node, (size_t)8 * s->g.ntotal));
   }
+  const size_t nodeb = node_snapshot_bytes(s);
   if (s->ro.seg_states < every) {
     if (s->ro.seg) cudaFree(s->ro.seg);
+    if (s->ro.seg_nodes) cudaFree(s->ro.seg_nodes);
     s->ro.seg = nullptr;
+    s->ro.seg_nodes = nullptr;
     s->ro.seg_states = 0;
     if (cudaMalloc(&s->ro.seg, per * every * sizeof(float)) != cudaSuccess) return PMPM_ERR_OUT_OF_MEMORY;
+    if (cudaMalloc(&s->ro.seg_nodes, nodeb * every) != cudaSuccess) return PMPM_ERR_OUT_OF_MEMORY;
     s->ro.seg_states = every;
   }
+  s->ro.seg_epoch.assign(every, 0);
   PMPM_CUDA(cudaMemsetAsync(A.v, 0, sizeof(float) * D * st, s->stream));
   PMPM_CUDA(cudaMemsetAsync(A.F, 0, sizeof(float) * D * D * st, s->stream));
   PMPM_CUDA(cudaMemsetAsync(A.sig, 0, sizeof(float) * NS * st, s->stream));
@@ -2437,14 +2479,21 @@ int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_devic
     const int k0 = c * every, k1 = std::min(k0 + every, nsteps);
     PMPM_TRY(copy_state(s, s->ro.ckpt[c], false));
     s->step = s->ro.start_step + k0;
+    // forward over the segment, keeping each step's state and P2G node data
     for (int j = k0; j < k1; j++) {
       PMPM_TRY(copy_state(s, s->ro.seg + per * (j - k0), true));
-      if (j + 1 < k1) PMPM_TRY(PMPM_DISPATCH(s, step_once, s));
+      if (j + 1 < k1)
+        PMPM_TRY(PMPM_DISPATCH(s, step_once, s));
+      else
+        PMPM_TRY(s->dim == 2 ? (p2g_only<2, PMPM_SHAPE_QUADRATIC>(s)) : (p2g_only<3, PMPM_SHAPE_QUADRATIC>(s)));
+      PMPM_TRY(copy_nodes(s, s->ro.seg_nodes + nodeb * (j - k0), true));
+      s->ro.seg_epoch[j - k0] = s->epoch;
     }
     for (int j = k1 - 1; j >= k0; j--) {
       PMPM_TRY(copy_state(s, s->ro.seg + per * (j - k0), false));
+      PMPM_TRY(copy_nodes(s, s->ro.seg_nodes + nodeb * (j - k0), false));
       s->step = s->ro.start_step + j;
-      PMPM_TRY(adjoint_step_dispatch(s));
+      PMPM_TRY(adjoint_step_dispatch(s, s->ro.seg_epoch[j - k0]));
     }
   }
   s->step = s->ro.start_step;

@@ -63,39 +63,73 @@ def test_per_particle_parameters_forward_matches_oracle():
     np.testing.assert_allclose(sim2.get("friction_angle"), 30.0, rtol=1e-5)
 
 
-@pytest.mark.parametrize("steps,every", [(3, 1), (12, 5)])
-def test_adjoint_matches_fp64_finite_differences(steps, every):
-    scene, E, phi, (tE, tphi) = small_cube()
+def impact_cube():
+    """The small cube thrown at the floor and sideways (2 m/s): within a few
+    steps it is compressed against the wall and yields, so the parameters
+    shape the final positions well above FP32 resolution."""
+    scene, E, phi, target = small_cube()
+    v = np.zeros_like(scene["positions"])
+    v[:, 0] = 0.7
+    v[:, 2] = -2.0
+    scene["velocities"] = v
+    return scene, E, phi, target
+
+
+def flight_cube():
+    """A cohesive cube in free flight with a random velocity field: it stays
+    elastic and away from the walls, so the rollout is a smooth map and
+    central differences converge in every direction."""
+    scene, E, phi, target = small_cube()
+    scene["positions"] = scene["positions"] + np.array([0.0, 0.0, 0.15])
+    scene["materials"][0]["cohesion"] = 2e4
+    rng = np.random.default_rng(3)
+    scene["velocities"] = np.array([0.7, 0.0, -2.0]) + rng.normal(0, 0.05, scene["positions"].shape)
+    return scene, E, phi, target
+
+
+def directional_checks(scene, E, phi, steps, every, names, tol, eps=1e-4):
+    """Loss w . x_final with fixed random weights w (its gradient is O(1) in
+    every direction, so FP32 roundoff of the positions does not mask it):
+    the adjoint's directional derivatives against FP64 central differences."""
     n = len(scene["positions"])
-    target = oracle_final(scene, np.full(n, tE), np.full(n, tphi), steps)
-
-    def loss(x):
-        return float(((x - target) ** 2).sum() / n)
-
+    w = np.random.default_rng(7).normal(0, 1, (n, 3))
     sim = make_sim(scene, E, phi)
     sim.rollout_forward(steps, every)
-    x = sim.get("positions").astype(np.float64)
-    gE, gphi, gx0, gv0 = sim.rollout_backward(2.0 * (x - target) / n)
+    gE, gphi, gx0, gv0 = sim.rollout_backward(w)
     # the backward leaves the simulation at the initial state
     np.testing.assert_array_equal(sim.get("positions"), scene["positions"].astype(np.float32))
-
     rng = np.random.default_rng(0)
     dE = E * rng.normal(0, 1, n)
     dphi = rng.normal(0, 1, n)
     dx = rng.normal(0, 1e-3 * scene["cell_size"], (n, 3))
     dv = rng.normal(0, 1e-2, (n, 3))
-    cases = [
-        ("E", np.dot(gE.astype(np.float64), dE), lambda e: oracle_final(scene, E + e * dE, phi, steps)),
-        ("phi", np.dot(gphi.astype(np.float64), dphi), lambda e: oracle_final(scene, E, phi + e * dphi, steps)),
-        ("x0", (gx0.astype(np.float64) * dx).sum(),
-         lambda e: oracle_final(scene, E, phi, steps, x0=scene["positions"] + e * dx)),
-        ("v0", (gv0.astype(np.float64) * dv).sum(),
-         lambda e: oracle_final(scene, E, phi, steps, v0=scene["velocities"] + e * dv)),
-    ]
-    eps = 1e-3
-    for name, adj, run in cases:
-        fd = (loss(run(eps)) - loss(run(-eps))) / (2 * eps)
-        assert abs(adj - fd) <= 2e-2 * abs(fd) + 1e-12, f"{name}: adjoint {adj:.6e} vs FD {fd:.6e}"
+    cases = {
+        "E": (np.dot(gE.astype(np.float64), dE), lambda e: oracle_final(scene, E + e * dE, phi, steps)),
+        "phi": (np.dot(gphi.astype(np.float64), dphi), lambda e: oracle_final(scene, E, phi + e * dphi, steps)),
+        "x0": ((gx0.astype(np.float64) * dx).sum(),
+               lambda e: oracle_final(scene, E, phi, steps, x0=scene["positions"] + e * dx)),
+        "v0": ((gv0.astype(np.float64) * dv).sum(),
+               lambda e: oracle_final(scene, E, phi, steps, v0=scene["velocities"] + e * dv)),
+    }
+    for name in names:
+        adj, run = cases[name]
+        fd = (float((w * run(eps)).sum()) - float((w * run(-eps)).sum())) / (2 * eps)
+        assert fd != 0.0
+        assert abs(adj - fd) <= tol * abs(fd), f"{name}: adjoint {adj:.6e} vs FD {fd:.6e}"
+
+
+def test_adjoint_smooth_rollout_matches_fp64_finite_differences():
+    scene, E, phi, _ = flight_cube()
+    directional_checks(scene, E, phi, 16, 5, ("E", "x0", "v0"), 1e-3)
+
+
+@pytest.mark.parametrize("steps,every", [(4, 1), (16, 5)])
+def test_adjoint_plastic_impact_matches_fp64_finite_differences(steps, every):
+    """Yielding against the floor.  The slip-wall clamps and the yield
+    surface put kinks in the map; along the velocity direction central
+    differences do not converge there, so v0 is checked in the smooth case."""
+    scene, E, phi, _ = impact_cube()
+    directional_checks(scene, E, phi, steps, every, ("E", "phi", "x0"), 2e-2)
 
 
 def test_autograd_function_matches_direct_backward():
