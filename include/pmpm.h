@@ -404,6 +404,20 @@ int pmpm_rollout_reset(pmpm_sim *s);
 int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_device, float *grad_youngs,
                           float *grad_friction, float *grad_positions0, float *grad_velocities0);
 
+/* Vector-Jacobian product of the single-point Drucker-Prager update
+ * (pmpm_material_point_update's material law; no reference counterpart):
+ * given adjoints of the new stress [n][3][3] and elastic strain [n][dim][dim],
+ * the adjoints of the velocity gradient [n][dim][dim], of the old elastic
+ * strain [n][dim][dim] (one value per independent component, on both of its
+ * entries) and, with per-particle youngs / friction (else NULL, and the
+ * gradients are 0), of E and the friction angle (per degree).  method 0:
+ * reverse mode (what the rollout adjoint uses); 1: forward-mode dual
+ * numbers, an independent evaluation for cross-checks.  Host arrays. */
+int pmpm_material_point_vjp(const pmpm_material *mat, int dim, int n, float dt, const float *L, const float *eps_e,
+                            const float *stress_ref, const float *youngs, const float *friction,
+                            const float *grad_stress, const float *grad_eps_e, float *grad_L, float *grad_eps_e_in,
+                            float *grad_youngs, float *grad_friction, int method, int device);
+
 /* ---------------------------------------------------------------------------
  * Batched ensembles.  No counterpart in the reference (its settings are
  * process globals: one simulation per process).  Many independent

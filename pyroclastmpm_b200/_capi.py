@@ -82,7 +82,7 @@ EXPORTS = [
     "pmpm_get_step", "pmpm_set_step", "pmpm_synchronize", "pmpm_stream", "pmpm_material_point_update",
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
-    "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward",
+    "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
 ]
 
 EXPORTS += [
@@ -123,6 +123,7 @@ def lib():
     L.pmpm_bc_rigid_sdf.argtypes = [i, i, fp, fp, f, f, fp, f, f, i, ctypes.POINTER(BC)]
     L.pmpm_calculate_timestep.argtypes = [f, f, f, f, f, fp]
     L.pmpm_rollout_forward.argtypes = [vp, i, i]
+    L.pmpm_material_point_vjp.argtypes = [ctypes.POINTER(Material), i, i, f] + [vp] * 11 + [i, i]
     L.pmpm_rollout_reset.argtypes = [vp]
     L.pmpm_rollout_backward.argtypes = [vp, vp, i, vp, vp, vp, vp]
     L.pmpm_batch_create.argtypes = [i, ctypes.POINTER(Instance), i, vp, i, ctypes.POINTER(vp)]
@@ -246,6 +247,32 @@ def make_bc(b: dict, dim: int, num_nodes: int, keep: list) -> BC:
     else:
         raise ValueError(f"unknown boundary condition {t}")
     return out
+
+
+def material_point_vjp(material: dict, dim, dt, L, eps_e, stress_ref, grad_stress, grad_eps_e, youngs=None,
+                       friction=None, method=0, device=0):
+    """Vector-Jacobian product of the single-point Drucker-Prager update:
+    returns (dL, d eps_e, dE, dphi) for the adjoints of the new stress and
+    elastic strain.  method 0 reverse mode, 1 forward-mode dual numbers."""
+    m = make_material(material)
+    a = lambda x, shape: np.ascontiguousarray(np.asarray(x, np.float32).reshape(shape))
+    L = a(L, (-1, dim, dim))
+    n = L.shape[0]
+    eps = a(eps_e, (n, dim, dim))
+    sref = a(stress_ref, (n, 3, 3))
+    gS = a(grad_stress, (n, 3, 3))
+    gEo = a(grad_eps_e, (n, dim, dim))
+    Y = None if youngs is None else a(youngs, (n,))
+    Fr = None if friction is None else a(friction, (n,))
+    oL = np.empty((n, dim, dim), np.float32)
+    oE = np.empty((n, dim, dim), np.float32)
+    oY = np.empty(n, np.float32)
+    oF = np.empty(n, np.float32)
+    p = lambda x: None if x is None else x.ctypes.data_as(ctypes.c_void_p)
+    check(lib().pmpm_material_point_vjp(ctypes.byref(m), dim, n, float(dt), p(L), p(eps), p(sref), p(Y), p(Fr),
+                                        p(gS), p(gEo), p(oL), p(oE), p(oY), p(oF), int(method), int(device)),
+          "pmpm_material_point_vjp")
+    return oL, oE, oY, oF
 
 
 def calculate_timestep(cell_size, factor, bulk_modulus, shear_modulus, density):

@@ -318,6 +318,263 @@ __device__ void dp_vjp(const DevMaterial &mt, bool per_particle, float Ep, float
   phibar = gin[D * D + NE + 1];
 }
 
+// Reverse-mode vector-Jacobian product of the Drucker-Prager update (same
+// contract as dp_vjp: Lbar accumulates, epsbar / Ebar / phibar are set).
+// The primal is recomputed in FP32 with the branch tests of dp_update;
+// adjoints follow the forward's expressions in reverse:
+//   deps = sym(L) dt - W eps + eps W,  W = skew(L) dt;  eps_tr = eps + deps
+//   p_tr = p_ref + K tr(eps_tr);  s_tr = s_ref + 2G dev(eps_tr)  (2D: zz 0)
+//   q = sqrt(J2(s_tr));  Phi = q + eta p_tr - kc
+//   elastic: S = s_tr + p_tr I, eps' = eps_tr
+//   plastic: dgamma = Phi / (K eta eta_bar + G); p = p_tr - K eta_bar dgamma;
+//            cone s = (1 - G dgamma / q) s_tr, apex s = 0, p = p_apex;
+//            S = s + p I, eps' = (s - s_ref) / 2G + (p - p_ref) / 3K I
+template <int D>
+__device__ void dp_vjp_rev(const DevMaterial &mt, bool per_particle, float Ep, float phip, const float L[9],
+                           float dt, const float eps_s[6], const float sref[9], const float sbar[6],
+                           const float ebar[6], float Lbar[9], float epsbar[6], float &Ebar, float &phibar) {
+  constexpr int NS = Sym<D>::S, NE = Sym<D>::E;
+  // ---- parameters ----
+  float K, G, eta, eta_bar, kc, p_apex;
+  bool has_apex;
+  float nu = 0.0f, c = 0.0f, sn = 0.0f, cs = 0.0f;
+  if (per_particle) {
+    nu = mt.p[7];
+    c = mt.p[8];
+    const float phi = phip * 0.017453292519943295f;
+    sn = sinf(phi);
+    cs = cosf(phi);
+    const float den = 1.7320508075688772f * (3.0f - sn);
+    eta = 6.0f * sn / den;
+    const float xi = 6.0f * cs / den;
+    K = Ep / (3.0f * (1.0f - 2.0f * nu));
+    G = Ep / (2.0f * (1.0f + nu));
+    eta_bar = mt.p[3];
+    kc = xi * c;
+    p_apex = eta > 0.0f ? kc / eta : 0.0f;
+    has_apex = eta > 0.0f;
+  } else {
+    K = mt.p[0];
+    G = mt.p[1];
+    eta = mt.p[2];
+    eta_bar = mt.p[3];
+    kc = mt.p[4];
+    p_apex = mt.p[5];
+    has_apex = mt.p[6] != 0.0f;
+  }
+  // ---- primal ----
+  float eps[9], Wm[9], deps[9];
+#pragma unroll
+  for (int k = 0; k < NE; k++) {
+    int a, b;
+    eps_entry<D>(k, a, b);
+    eps[a * D + b] = eps_s[k];
+    eps[b * D + a] = eps_s[k];
+  }
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      deps[a * D + b] = (0.5f * (L[a * D + b] + L[b * D + a])) * dt;
+      Wm[a * D + b] = (0.5f * (L[a * D + b] - L[b * D + a])) * dt;
+    }
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int k = 0; k < D; k++) acc += -Wm[a * D + k] * eps[k * D + b] + eps[a * D + k] * Wm[k * D + b];
+      deps[a * D + b] += acc;
+    }
+  const float p_ref = (1.0f / 3.0f) * ((sref[0] + sref[4]) + sref[8]);
+  float s_ref[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] -= p_ref;
+  s_ref[4] -= p_ref;
+  s_ref[8] -= p_ref;
+  float eps_tr[9];
+#pragma unroll
+  for (int k = 0; k < D * D; k++) eps_tr[k] = eps[k] + deps[k];
+  float ev = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++) ev += eps_tr[a * D + a];
+  const float p_tr = p_ref + K * ev;
+  float edev[9], s_tr[9];
+  float ss = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      float e = (a < D && b < D) ? eps_tr[a * D + b] : 0.0f;
+      if (a == b) e -= (1.0f / 3.0f) * ev;
+      if (D < 3 && a == 2 && b == 2) e = 0.0f;
+      edev[3 * a + b] = e;
+      s_tr[3 * a + b] = s_ref[3 * a + b] + 2.0f * G * e;
+      ss += s_tr[3 * a + b] * s_tr[3 * a + b];
+    }
+  const float q = sqrtf(0.5f * ss);
+  const float Phi = (q + eta * p_tr) - kc;
+  // ---- output adjoints in full form ----
+  float Sb[9], Eb[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) Sb[k] = Eb[k] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < NS; k++) Sb[sig_entry<D>(k)] = sbar[k];
+#pragma unroll
+  for (int k = 0; k < NE; k++) {
+    int a, b;
+    eps_entry<D>(k, a, b);
+    Eb[a * D + b] = ebar[k];
+  }
+  float str_b[9], ptr_b = 0.0f, epstr_b[9];
+  float Kb = 0.0f, Gb = 0.0f, etab = 0.0f, kcb = 0.0f, papb = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) str_b[k] = epstr_b[k] = 0.0f;
+  if (Phi <= 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) str_b[k] = Sb[k];
+    ptr_b = Sb[0] + Sb[4] + Sb[8];
+#pragma unroll
+    for (int k = 0; k < D * D; k++) epstr_b[k] = Eb[k];
+  } else {
+    const float den = K * eta * eta_bar + G;
+    const float dgamma = Phi / den;
+    const bool apex = has_apex && (q - G * dgamma < 0.0f);
+    float p = p_tr - K * eta_bar * dgamma;
+    const float cfac = apex ? 0.0f : 1.0f - G * dgamma / q;
+    if (apex) p = p_apex;
+    float sv[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) sv[k] = cfac * s_tr[k];
+    // eps' = (s - s_ref) / 2G + (p - p_ref) / 3K I
+    float sb_[9], pb = 0.0f, trEb = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 9; k++) sb_[k] = Sb[k];
+    pb = Sb[0] + Sb[4] + Sb[8];
+    const float inv2g = 1.0f / (2.0f * G);
+#pragma unroll
+    for (int a = 0; a < D; a++)
+#pragma unroll
+      for (int b = 0; b < D; b++) {
+        const float e = Eb[a * D + b];
+        sb_[3 * a + b] += e * inv2g;
+        Gb -= e * (sv[3 * a + b] - s_ref[3 * a + b]) * inv2g / G;
+      }
+#pragma unroll
+    for (int a = 0; a < D; a++) trEb += Eb[a * D + a];
+    pb += trEb / (3.0f * K);
+    Kb -= trEb * (p - p_ref) / (3.0f * K * K);
+    float dgb = 0.0f;
+    if (apex) {
+      papb += pb;
+    } else {
+      // s = cfac s_tr
+      float cb = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        str_b[k] += cfac * sb_[k];
+        cb += sb_[k] * s_tr[k];
+      }
+      // cfac = 1 - G dgamma / q
+      Gb -= cb * dgamma / q;
+      dgb -= cb * G / q;
+      const float qb_c = cb * G * dgamma / (q * q);
+      // p = p_tr - K eta_bar dgamma
+      ptr_b += pb;
+      Kb -= pb * eta_bar * dgamma;
+      dgb -= pb * K * eta_bar;
+      // q -> s_tr (from cfac)
+#pragma unroll
+      for (int k = 0; k < 9; k++) str_b[k] += qb_c * s_tr[k] / (2.0f * q);
+    }
+    // dgamma = Phi / den
+    const float Phib = dgb / den;
+    const float denb = -dgb * dgamma / den;
+    Kb += denb * eta * eta_bar;
+    etab += denb * K * eta_bar;
+    Gb += denb;
+    // Phi = q + eta p_tr - kc
+    const float qb = Phib;
+    etab += Phib * p_tr;
+    ptr_b += Phib * eta;
+    kcb -= Phib;
+    if (q > 0.0f) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) str_b[k] += qb * s_tr[k] / (2.0f * q);
+    }
+  }
+  // s_tr = s_ref + 2G edev
+  float edev_b[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    edev_b[k] = 2.0f * G * str_b[k];
+    Gb += 2.0f * str_b[k] * edev[k];
+  }
+  float evb = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      if (D < 3 && a == 2 && b == 2) continue;
+      const float e = edev_b[3 * a + b];
+      if (a < D && b < D) epstr_b[a * D + b] += e;
+      if (a == b) evb -= (1.0f / 3.0f) * e;
+    }
+  // p_tr = p_ref + K ev
+  evb += K * ptr_b;
+  Kb += ev * ptr_b;
+#pragma unroll
+  for (int a = 0; a < D; a++) epstr_b[a * D + a] += evb;
+  // eps_tr = eps + deps; deps = sym dt - W eps + eps W
+  float epsb[9], Wb[9];
+#pragma unroll
+  for (int k = 0; k < D * D; k++) {
+    epsb[k] = epstr_b[k];
+    Wb[k] = 0.0f;
+  }
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      const float g = epstr_b[a * D + b];
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        // -W_ak eps_kb
+        Wb[a * D + k] -= g * eps[k * D + b];
+        epsb[k * D + b] -= g * Wm[a * D + k];
+        // eps_ak W_kb
+        epsb[a * D + k] += g * Wm[k * D + b];
+        Wb[k * D + b] += g * eps[a * D + k];
+      }
+    }
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++)
+      Lbar[a * D + b] += 0.5f * dt * (epstr_b[a * D + b] + epstr_b[b * D + a]) +
+                         0.5f * dt * (Wb[a * D + b] - Wb[b * D + a]);
+#pragma unroll
+  for (int k = 0; k < NE; k++) {
+    int a, b;
+    eps_entry<D>(k, a, b);
+    epsbar[k] = a == b ? epsb[a * D + a] : epsb[a * D + b] + epsb[b * D + a];
+  }
+  Ebar = 0.0f;
+  phibar = 0.0f;
+  if (per_particle) {
+    Ebar = Kb / (3.0f * (1.0f - 2.0f * nu)) + Gb / (2.0f * (1.0f + nu));
+    const float s3 = 1.7320508075688772f;
+    const float t = 3.0f - sn;
+    const float deta = (6.0f / s3) * 3.0f / (t * t) * cs;          // d eta / d phi
+    const float dxi = (6.0f / s3) * (1.0f - 3.0f * sn) / (t * t);  // d xi / d phi
+    float g = etab * deta + kcb * c * dxi;
+    if (eta > 0.0f) g += papb * (c * dxi / eta - kc * deta / (eta * eta));
+    phibar = g * 0.017453292519943295f;
+  }
+}
+
 // --------------------------------------------------------------------------
 // quadratic weights with first and second derivatives
 // --------------------------------------------------------------------------
@@ -555,7 +812,7 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
       }
       const bool pp = P.pE && mt.p[7] >= 0.0f;
       float Ebar = 0.0f, phibar = 0.0f;
-      dp_vjp<D>(mt, pp, pp ? P.pE[s] : 0.0f, pp ? P.pphi[s] : 0.0f, L, a.dt, eps_s, sref, sb, eb, Lb, eo, Ebar,
+      dp_vjp_rev<D>(mt, pp, pp ? P.pE[s] : 0.0f, pp ? P.pphi[s] : 0.0f, L, a.dt, eps_s, sref, sb, eb, Lb, eo, Ebar,
                 phibar);
       if (pp) {
         A.gE[s] += Ebar;
@@ -826,6 +1083,59 @@ __global__ void __launch_bounds__(128) kadj_p2g(StepArgs a, AdjState A) {
     const int r = e / 3, c = e % 3;
     A.sig[k * st + s] = r == c ? Sb[e] : Sb[3 * r + c] + Sb[3 * c + r];
   }
+}
+
+// Vector-Jacobian product of the single-point Drucker-Prager update, by
+// reverse mode (method 0) or forward-mode dual numbers (method 1).  Host
+// layouts: L, eps, grad_eps_out, grad_L, grad_eps_in [n][D][D]; sref,
+// grad_S [n][3][3]; E, phi (may be null), grad_E, grad_phi [n].  Output
+// adjoints of the symmetric results count both entries of a pair; the
+// symmetric input eps gets one gradient per independent component, written
+// to both of its entries.
+template <int D>
+__global__ void __launch_bounds__(128) k_point_vjp(DevMaterial mt, int n, float dt, const float *L, const float *eps,
+                                                   const float *sref, const float *E, const float *phi,
+                                                   const float *gS, const float *gE_out, float *gL, float *geps,
+                                                   float *gE, float *gphi, int method) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  constexpr int NS = Sym<D>::S, NE = Sym<D>::E;
+  float Li[9], es[6] = {0, 0, 0, 0, 0, 0}, sr[9], sb[6] = {0, 0, 0, 0, 0, 0}, eb[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < D * D; k++) Li[k] = L[(size_t)i * D * D + k];
+#pragma unroll
+  for (int k = 0; k < 9; k++) sr[k] = sref[(size_t)i * 9 + k];
+#pragma unroll
+  for (int k = 0; k < NE; k++) {
+    int a, b;
+    eps_entry<D>(k, a, b);
+    es[k] = eps[(size_t)i * D * D + a * D + b];
+    eb[k] = gE_out[(size_t)i * D * D + a * D + b] + (a != b ? gE_out[(size_t)i * D * D + b * D + a] : 0.0f);
+  }
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    const int e = sig_entry<D>(k), r = e / 3, c = e % 3;
+    sb[k] = gS[(size_t)i * 9 + e] + (r != c ? gS[(size_t)i * 9 + 3 * c + r] : 0.0f);
+  }
+  const bool pp = E != nullptr && mt.p[7] >= 0.0f;
+  float Lb[9], epsb[6], Eb = 0.0f, pb = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) Lb[k] = 0.0f;
+  if (method == 0)
+    dp_vjp_rev<D>(mt, pp, pp ? E[i] : 0.0f, pp ? phi[i] : 0.0f, Li, dt, es, sr, sb, eb, Lb, epsb, Eb, pb);
+  else
+    dp_vjp<D>(mt, pp, pp ? E[i] : 0.0f, pp ? phi[i] : 0.0f, Li, dt, es, sr, sb, eb, Lb, epsb, Eb, pb);
+#pragma unroll
+  for (int k = 0; k < D * D; k++) gL[(size_t)i * D * D + k] = Lb[k];
+#pragma unroll
+  for (int k = 0; k < NE; k++) {
+    int a, b;
+    eps_entry<D>(k, a, b);
+    geps[(size_t)i * D * D + a * D + b] = epsb[k];
+    geps[(size_t)i * D * D + b * D + a] = epsb[k];
+  }
+  gE[i] = Eb;
+  gphi[i] = pb;
 }
 
 }  // namespace pmpm

@@ -2507,3 +2507,70 @@ int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_devic
 }
 
 }  // extern "C"
+
+extern "C" int pmpm_material_point_vjp(const pmpm_material *mat, int dim, int n, float dt, const float *L,
+                                       const float *eps_e, const float *stress_ref, const float *youngs,
+                                       const float *friction, const float *grad_stress, const float *grad_eps_e,
+                                       float *grad_L, float *grad_eps_e_in, float *grad_youngs, float *grad_friction,
+                                       int method, int device) {
+  if (!mat || (dim != 2 && dim != 3) || n < 0 || !L || !eps_e || !stress_ref || !grad_stress || !grad_eps_e ||
+      !grad_L || !grad_eps_e_in || !grad_youngs || !grad_friction || (method != 0 && method != 1) ||
+      (!youngs != !friction))
+    return PMPM_ERR_INVALID_ARGUMENT;
+  if (mat->type != PMPM_MAT_DRUCKER_PRAGER) return PMPM_ERR_NOT_SUPPORTED;
+  if (n == 0) return PMPM_OK;
+  PMPM_CUDA(cudaSetDevice(device));
+  pmpm_sim tmp;
+  pmpm_desc d{};
+  d.dim = dim;
+  d.cell_size = 1.0f;
+  d.particles_per_cell = 1;
+  d.num_materials = 1;
+  d.materials = mat;
+  d.end[0] = d.end[1] = d.end[2] = 1.0f;
+  PMPM_TRY(setup_handle(&d, &tmp));  // material constants as a simulation holds them
+  const DevMaterial dm = tmp.mats[0];
+  const size_t dd = (size_t)dim * dim;
+  std::vector<void *> bufs;
+  int st = PMPM_OK;
+  auto up = [&](const float *h, size_t count) -> float * {
+    float *p = nullptr;
+    if (!h || st != PMPM_OK) return nullptr;
+    if (cudaMalloc(&p, count * 4) != cudaSuccess) {
+      st = PMPM_ERR_OUT_OF_MEMORY;
+      return nullptr;
+    }
+    bufs.push_back(p);
+    if (cudaMemcpy(p, h, count * 4, cudaMemcpyHostToDevice) != cudaSuccess) st = PMPM_ERR_CUDA;
+    return p;
+  };
+  auto out = [&](size_t count) -> float * {
+    float *p = nullptr;
+    if (st != PMPM_OK) return nullptr;
+    if (cudaMalloc(&p, count * 4) != cudaSuccess) {
+      st = PMPM_ERR_OUT_OF_MEMORY;
+      return nullptr;
+    }
+    bufs.push_back(p);
+    return p;
+  };
+  float *dL = up(L, n * dd), *dE = up(eps_e, n * dd), *dR = up(stress_ref, (size_t)n * 9);
+  float *dY = up(youngs, n), *dF = up(friction, n), *dgS = up(grad_stress, (size_t)n * 9);
+  float *dgEo = up(grad_eps_e, n * dd);
+  float *ogL = out(n * dd), *ogE = out(n * dd), *ogY = out(n), *ogF = out(n);
+  if (st == PMPM_OK) {
+    if (dim == 2)
+      k_point_vjp<2><<<blocks_for(n, 128), 128>>>(dm, n, dt, dL, dE, dR, dY, dF, dgS, dgEo, ogL, ogE, ogY, ogF, method);
+    else
+      k_point_vjp<3><<<blocks_for(n, 128), 128>>>(dm, n, dt, dL, dE, dR, dY, dF, dgS, dgEo, ogL, ogE, ogY, ogF, method);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = PMPM_ERR_CUDA;
+  }
+  if (st == PMPM_OK && (cudaMemcpy(grad_L, ogL, n * dd * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(grad_eps_e_in, ogE, n * dd * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(grad_youngs, ogY, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(grad_friction, ogF, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess))
+    st = PMPM_ERR_CUDA;
+  for (void *p : bufs) cudaFree(p);
+  for (float *p : tmp.bc_values) cudaFree(p);
+  return st;
+}

@@ -155,3 +155,37 @@ def test_autograd_function_matches_direct_backward():
     gE, gphi, _, _ = sim2.rollout_backward(2.0 * (x2 - target.cpu().numpy()) / n)
     np.testing.assert_allclose(Et.grad.cpu().numpy(), gE, rtol=1e-3, atol=1e-3 * np.abs(gE).max())
     np.testing.assert_allclose(pt.grad.cpu().numpy(), gphi, rtol=1e-3, atol=1e-3 * np.abs(gphi).max())
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("cohesion", [0.0, 2e3])
+def test_return_mapping_vjp_reverse_equals_dual_numbers(dim, cohesion):
+    """The reverse-mode VJP of the Drucker-Prager update (used by the rollout
+    adjoint) against forward-mode dual numbers, over states in the elastic,
+    cone and apex branches."""
+    from pyroclastmpm_b200._capi import material_point_vjp
+
+    rng = np.random.default_rng(11 + dim)
+    n = 6000
+    mat = {"type": "DruckerPrager", "density": 1500.0, "E": 1e7, "pois": 0.3, "friction_angle": 30.0,
+           "dilatancy_angle": 5.0, "cohesion": cohesion}
+    L = rng.normal(0, 40.0, (n, dim, dim))
+    L[: n // 3] *= 0.02                                   # mostly elastic
+    L[n // 3: n // 2] += 60.0 * np.eye(dim)               # tension: apex
+    eps = rng.normal(0, 2e-4, (n, dim, dim))
+    eps = 0.5 * (eps + eps.transpose(0, 2, 1))
+    sref = rng.normal(0, 2e3, (n, 3, 3))
+    sref = 0.5 * (sref + sref.transpose(0, 2, 1)) - 1e4 * np.eye(3)
+    if dim == 2:
+        sref[:, 2, :2] = sref[:, :2, 2] = 0
+    E = rng.uniform(2e6, 2e7, n)
+    phi = rng.uniform(20.0, 40.0, n)
+    gS = rng.normal(0, 1, (n, 3, 3))
+    gEo = rng.normal(0, 1e4, (n, dim, dim))
+    out = [material_point_vjp(mat, dim, 1e-4, L, eps, sref, gS, gEo, E, phi, method=m) for m in (0, 1)]
+    for k, name in enumerate(("L", "eps_e", "E", "phi")):
+        a, b = out[0][k].astype(np.float64), out[1][k].astype(np.float64)
+        scale = np.abs(b).max()
+        assert scale > 0
+        err = np.abs(a - b).max() / scale
+        assert err < 2e-4, f"{name}: {err:.2e}"
