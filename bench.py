@@ -388,6 +388,11 @@ def run_calibration(args, world, rank, local, pg):
     if sim.synchronize() != 0:
         raise RuntimeError("device fault in the timed region")
     gE, gphi = out[0], out[1]
+    # the same rollout with checkpoints alone (every segment recomputed)
+    sim.rollout_set_memory(0)
+    ms_fwd0, _ = timed(lambda: sim.rollout_forward(nsteps, every))
+    ms_bwd0, _ = timed(lambda: sim.rollout_backward(grad))
+    sim.rollout_set_memory(-1)
     ms_total = allreduce_max(pg, ms_fwd + ms_bwd)
     value = world * n * nsteps / (ms_total / 1000.0)
     # G2P-side adjoint traffic per particle-step: state in, adjoints in and out
@@ -412,6 +417,11 @@ def run_calibration(args, world, rank, local, pg):
                        "rollout_forward_ms_per_step": ms_fwd / nsteps,
                        "adjoint_ms_per_step": ms_bwd / nsteps,
                        "fwd_plus_adjoint_over_plain_forward": (ms_fwd + ms_bwd) / ms_plain,
+                       "segments": "kept whole from the forward pass where device memory allows (default "
+                                   "budget: 60 % of free memory); checkpoints every 25 steps regardless",
+                       "checkpoints_only": {"rollout_forward_ms_per_step": ms_fwd0 / nsteps,
+                                            "adjoint_ms_per_step": ms_bwd0 / nsteps,
+                                            "fwd_plus_adjoint_over_plain_forward": (ms_fwd0 + ms_bwd0) / ms_plain},
                        "loss": loss, "grad_norm_E": float(np.linalg.norm(gE)),
                        "grad_norm_phi": float(np.linalg.norm(gphi))},
             "roofline": {"bound": "hbm", "kernel": "adjoint step (3 kernels + recomputed P2G)",

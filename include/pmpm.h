@@ -395,6 +395,12 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
  * is off while a rollout is held.
  * ------------------------------------------------------------------------- */
 int pmpm_rollout_forward(pmpm_sim *s, int nsteps, int checkpoint_every);
+/* Device memory for segments kept whole from the forward pass (every step's
+ * state and P2G node data), so the backward pass recomputes none of them:
+ * the last segments are kept while they fit.  bytes < 0 (default): 60 % of
+ * the free device memory at the start of each rollout; 0: checkpoints only.
+ * Gradients do not depend on it. */
+int pmpm_rollout_set_memory(pmpm_sim *s, long long bytes);
 /* Back to the state the last rollout started from (step counter included). */
 int pmpm_rollout_reset(pmpm_sim *s);
 /* grad_positions: dLoss/dx of the final positions [n][dim] (id order).

@@ -83,6 +83,7 @@ EXPORTS = [
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
+    "pmpm_rollout_set_memory",
 ]
 
 EXPORTS += [
@@ -123,6 +124,7 @@ def lib():
     L.pmpm_bc_rigid_sdf.argtypes = [i, i, fp, fp, f, f, fp, f, f, i, ctypes.POINTER(BC)]
     L.pmpm_calculate_timestep.argtypes = [f, f, f, f, f, fp]
     L.pmpm_rollout_forward.argtypes = [vp, i, i]
+    L.pmpm_rollout_set_memory.argtypes = [vp, ctypes.c_longlong]
     L.pmpm_material_point_vjp.argtypes = [ctypes.POINTER(Material), i, i, f] + [vp] * 11 + [i, i]
     L.pmpm_rollout_reset.argtypes = [vp]
     L.pmpm_rollout_backward.argtypes = [vp, vp, i, vp, vp, vp, vp]
@@ -501,6 +503,11 @@ class Simulation:
     # ---- differentiable rollouts ----
     def rollout_forward(self, nsteps, checkpoint_every=25):
         check(lib().pmpm_rollout_forward(self._h, int(nsteps), int(checkpoint_every)), "pmpm_rollout_forward")
+        return self
+
+    def rollout_set_memory(self, nbytes):
+        """Memory for segments kept whole from the forward pass (< 0 automatic, 0 checkpoints only)."""
+        check(lib().pmpm_rollout_set_memory(self._h, int(nbytes)), "pmpm_rollout_set_memory")
         return self
 
     def rollout_reset(self):

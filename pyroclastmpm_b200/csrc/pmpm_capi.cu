@@ -115,6 +115,13 @@ struct pmpm_sim {
     int seg_states = 0;
     char *seg_nodes = nullptr;  // node data of each segment step's P2G
     std::vector<int> seg_epoch;
+    // segments kept whole from the forward pass (no recompute), as memory allows
+    long long budget = -1;  // bytes for kept segments; < 0: 60 % of free device memory
+    std::vector<float *> keep_state;
+    std::vector<char *> keep_nodes;
+    std::vector<std::vector<int>> keep_epoch;
+    size_t keep_per = 0, keep_nodeb = 0;
+    int keep_every = 0;
     AdjState A{};
     bool held = false;
   } ro;
@@ -2305,6 +2312,13 @@ void free_rollout(pmpm_sim *s) {
   if (s->ro.seg_nodes) cudaFree(s->ro.seg_nodes);
   s->ro.seg_nodes = nullptr;
   s->ro.seg = nullptr;
+  for (float *p : s->ro.keep_state)
+    if (p) cudaFree(p);
+  for (char *p : s->ro.keep_nodes)
+    if (p) cudaFree(p);
+  s->ro.keep_state.clear();
+  s->ro.keep_nodes.clear();
+  s->ro.keep_epoch.clear();
   s->ro.seg_states = 0;
   s->ro.A = AdjState{};
   s->ro.held = false;
@@ -2384,16 +2398,29 @@ int to_id_order(pmpm_sim *s, int kind, const float *src, void *dst, size_t bytes
 
 extern "C" {
 
+int pmpm_rollout_set_memory(pmpm_sim *s, long long bytes) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  s->ro.budget = bytes;
+  return PMPM_OK;
+}
+
 int pmpm_rollout_forward(pmpm_sim *s, int nsteps, int checkpoint_every) {
   if (!s || nsteps < 1 || checkpoint_every < 1) return PMPM_ERR_INVALID_ARGUMENT;
   if (s->n == 0) return PMPM_ERR_STATE;
   PMPM_TRY(rollout_supported(s));
   PMPM_CUDA(cudaSetDevice(s->device));
-  free_rollout(s);
   PMPM_TRY(ensure_particle_params(s));
   const size_t per = (size_t)state_floats(s) * s->stride;
-  const int ncp = (nsteps + checkpoint_every - 1) / checkpoint_every;
-  for (int c = 0; c < ncp; c++) {
+  const size_t nodeb = node_snapshot_bytes(s);
+  const int every = checkpoint_every;
+  const int ncp = (nsteps + every - 1) / every;
+  if (s->ro.keep_per != per || s->ro.keep_nodeb != nodeb || s->ro.keep_every != every) {
+    free_rollout(s);  // buffers sized for another layout
+    s->ro.keep_per = per;
+    s->ro.keep_nodeb = nodeb;
+    s->ro.keep_every = every;
+  }
+  while ((int)s->ro.ckpt.size() < ncp) {
     float *buf = nullptr;
     if (cudaMalloc(&buf, per * sizeof(float)) != cudaSuccess) {
       free_rollout(s);
@@ -2401,13 +2428,53 @@ int pmpm_rollout_forward(pmpm_sim *s, int nsteps, int checkpoint_every) {
     }
     s->ro.ckpt.push_back(buf);
   }
-  s->ro.every = checkpoint_every;
+  // keep the last segments whole, as the memory budget allows
+  const size_t segbytes = (size_t)every * (per * sizeof(float) + nodeb);
+  size_t kept_now = 0;
+  for (float *p : s->ro.keep_state)
+    if (p) kept_now += segbytes;
+  size_t budget;
+  if (s->ro.budget < 0) {
+    size_t free_b = 0, total_b = 0;
+    PMPM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    budget = (size_t)(0.6 * (double)(free_b + kept_now));
+  } else {
+    budget = (size_t)s->ro.budget;
+  }
+  const int nkeep = (int)std::min<size_t>((size_t)ncp, budget / segbytes);
+  s->ro.keep_state.resize(std::max<size_t>(s->ro.keep_state.size(), (size_t)ncp), nullptr);
+  s->ro.keep_nodes.resize(std::max<size_t>(s->ro.keep_nodes.size(), (size_t)ncp), nullptr);
+  s->ro.keep_epoch.resize(std::max<size_t>(s->ro.keep_epoch.size(), (size_t)ncp));
+  for (int c = 0; c < (int)s->ro.keep_state.size(); c++) {
+    const bool want = c < ncp && c >= ncp - nkeep;
+    if (want && !s->ro.keep_state[c]) {
+      if (cudaMalloc(&s->ro.keep_state[c], per * every * sizeof(float)) != cudaSuccess ||
+          cudaMalloc(&s->ro.keep_nodes[c], nodeb * every) != cudaSuccess) {
+        free_rollout(s);
+        return PMPM_ERR_OUT_OF_MEMORY;
+      }
+    } else if (!want && s->ro.keep_state[c]) {
+      cudaFree(s->ro.keep_state[c]);
+      cudaFree(s->ro.keep_nodes[c]);
+      s->ro.keep_state[c] = nullptr;
+      s->ro.keep_nodes[c] = nullptr;
+    }
+    if (want) s->ro.keep_epoch[c].assign(every, 0);
+  }
+  s->ro.every = every;
   s->ro.nsteps = nsteps;
   s->ro.start_step = s->step;
   s->ro.held = true;
   for (int k = 0; k < nsteps; k++) {
-    if (k % checkpoint_every == 0) PMPM_TRY(copy_state(s, s->ro.ckpt[k / checkpoint_every], true));
+    const int c = k / every, j = k % every;
+    if (j == 0) PMPM_TRY(copy_state(s, s->ro.ckpt[c], true));
+    const bool keep = s->ro.keep_state[c] != nullptr;
+    if (keep) PMPM_TRY(copy_state(s, s->ro.keep_state[c] + per * j, true));
     PMPM_TRY(PMPM_DISPATCH(s, step_once, s));
+    if (keep) {
+      PMPM_TRY(copy_nodes(s, s->ro.keep_nodes[c] + nodeb * j, true));
+      s->ro.keep_epoch[c][j] = s->epoch;
+    }
   }
   return PMPM_OK;
 }
@@ -2443,7 +2510,9 @@ int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_devic
     PMPM_TRY(dalloc(&A.node, (size_t)8 * s->g.ntotal));
   }
   const size_t nodeb = node_snapshot_bytes(s);
-  if (s->ro.seg_states < every) {
+  bool need_seg = false;
+  for (int c = 0; c * every < nsteps; c++) need_seg = need_seg || !s->ro.keep_state[c];
+  if (need_seg && s->ro.seg_states < every) {
     if (s->ro.seg) cudaFree(s->ro.seg);
     if (s->ro.seg_nodes) cudaFree(s->ro.seg_nodes);
     s->ro.seg = nullptr;
@@ -2474,9 +2543,19 @@ int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_devic
     k_set_particles<<<blocks_for(s->n), kTPB, 0, s->stream>>>(P, D, 0, src, A.x);
     PMPM_LAUNCHED();
   }
-  const int ncp = (int)s->ro.ckpt.size();
+  const int ncp = (nsteps + every - 1) / every;
   for (int c = ncp - 1; c >= 0; c--) {
     const int k0 = c * every, k1 = std::min(k0 + every, nsteps);
+    if (s->ro.keep_state[c]) {
+      // kept from the forward pass: states and node data of every step
+      for (int j = k1 - 1; j >= k0; j--) {
+        PMPM_TRY(copy_state(s, s->ro.keep_state[c] + per * (j - k0), false));
+        PMPM_TRY(copy_nodes(s, s->ro.keep_nodes[c] + nodeb * (j - k0), false));
+        s->step = s->ro.start_step + j;
+        PMPM_TRY(adjoint_step_dispatch(s, s->ro.keep_epoch[c][j - k0]));
+      }
+      continue;
+    }
     PMPM_TRY(copy_state(s, s->ro.ckpt[c], false));
     s->step = s->ro.start_step + k0;
     // forward over the segment, keeping each step's state and P2G node data
