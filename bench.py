@@ -376,7 +376,13 @@ def run_calibration(args, world, rank, local, pg):
     plain.solve(args.warmup)
     ms_plain, _ = timed(lambda: plain.solve(nsteps))
     plain.close()
-    # the warm-up's backward left `sim` at the initial state
+    # a full-length rollout and adjoint in each memory mode first (the kept
+    # segments are allocated once and reused); each backward leaves `sim` at
+    # the initial state
+    for budget in (0, -1):
+        sim.rollout_set_memory(budget)
+        sim.rollout_forward(nsteps, every)
+        sim.rollout_backward(np.zeros((n, 3), np.float32))
     l0 = sim.launch_count()
     ms_fwd, _ = timed(lambda: sim.rollout_forward(nsteps, every))
     x = sim.get("positions").astype(np.float64)
@@ -390,6 +396,8 @@ def run_calibration(args, world, rank, local, pg):
     gE, gphi = out[0], out[1]
     # the same rollout with checkpoints alone (every segment recomputed)
     sim.rollout_set_memory(0)
+    sim.rollout_forward(nsteps, every)  # frees the kept segments outside the timing
+    sim.rollout_backward(grad)
     ms_fwd0, _ = timed(lambda: sim.rollout_forward(nsteps, every))
     ms_bwd0, _ = timed(lambda: sim.rollout_backward(grad))
     sim.rollout_set_memory(-1)

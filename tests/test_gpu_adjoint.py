@@ -33,8 +33,8 @@ def oracle_final(scene, E, phi, steps, precision="f64", x0=None, v0=None):
     return np.array(o["positions"], np.float64)
 
 
-def make_sim(scene, E, phi):
-    sim = Simulation(**scenes.sim_kwargs(scene))
+def make_sim(scene, E, phi, flags=0):
+    sim = Simulation(**scenes.sim_kwargs(scene), flags=flags)
     sim.set_particles(scene["positions"], scene["velocities"]).initialize()
     sim.set("youngs_modulus", E)
     sim.set("friction_angle", phi)
@@ -193,13 +193,16 @@ def test_return_mapping_vjp_reverse_equals_dual_numbers(dim, cohesion):
 
 def test_kept_segments_and_checkpoints_give_the_same_gradients():
     """Backward from segments kept whole, from checkpoints alone (recomputed
-    segments) and from a mix: the same gradients up to FP32 summation order."""
+    segments) and from a mix: the same gradients up to FP32 summation order.
+    Deterministic P2G, so a recomputed segment repeats the forward bit for
+    bit (otherwise summation order can move a particle across the yield
+    surface and change its local Jacobian)."""
     scene, E, phi, _ = impact_cube()
     n = len(scene["positions"])
     w = np.random.default_rng(2).normal(0, 1, (n, 3))
     grads = []
     for budget in (-1, 0, None):
-        sim = make_sim(scene, E, phi)
+        sim = make_sim(scene, E, phi, flags=2)
         if budget is None:  # room for one segment of 5 steps
             nodes = sim.num_nodes
             per_step = 4 * (sim.n + 63) // 64 * 64 * 28 + 4 * nodes * (1 + 6 + 8) + 4 * 1024
