@@ -204,7 +204,7 @@ def workload_name(config):
             }[config]
 
 
-def run_ensemble(args, world, rank, local, pg):
+def run_ensemble(args, world, rank, local, pg, emit=True):
     """Batched ensemble: all instances stepped by one launch per phase, timed
     against one simulation handle per instance stepped one after another."""
     import torch
@@ -322,11 +322,13 @@ def run_ensemble(args, world, rank, local, pg):
                             "one batched step, read back (host wall clock around synchronised calls)"},
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     b.close()
+    return line if rank == 0 else None
 
 
-def run_calibration(args, world, rank, local, pg):
+def run_calibration(args, world, rank, local, pg, emit=True):
     """Differentiable calibration rollout: forward with checkpoints plus the
     adjoint, against the plain forward of the same rollout."""
     import torch
@@ -443,8 +445,10 @@ def run_calibration(args, world, rank, local, pg):
                             "and final positions read back; per-step share of those bytes"},
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     sim.close()
+    return line if rank == 0 else None
 
 
 def sc_nodes(sc):
@@ -467,6 +471,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-sample-scale", type=float, default=0.45)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-companions", dest="companions", action="store_false",
+                    help="skip the batched-ensemble and calibration legs in the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -588,6 +594,27 @@ def main():
         cpu = cpu_reference(args.config, args.cpu_steps, 0, 1.0)
         cpu.pop("seconds", None)
 
+    # the metric's other two legs, measured by their own configurations
+    companions = None
+    if args.companions and args.config == "column":
+        sim.close()
+        sub = argparse.Namespace(**vars(args))
+        sub.no_cpu_baseline = True
+        sub.steps = 10
+        ens = run_ensemble(sub, world, rank, local, pg, emit=False)
+        cal = run_calibration(sub, world, rank, local, pg, emit=False)
+        if rank == 0:
+            companions = {
+                "batched": {"value": ens["value"], "unit": "particle-steps/s", "workload": ens["config"]["workload"],
+                            "ms_per_step": ens["ms_per_step"],
+                            "over_one_sim_per_launch": ens["config"]["batched_over_one_sim_per_launch"]},
+                "fwd_adjoint": {"value": cal["value"], "unit": "particle-steps/s",
+                                "workload": cal["config"]["workload"], "ms_per_step": cal["ms_per_step"],
+                                "over_plain_forward": cal["config"]["fwd_plus_adjoint_over_plain_forward"],
+                                "checkpoints_only_over_plain_forward":
+                                    cal["config"]["checkpoints_only"]["fwd_plus_adjoint_over_plain_forward"]},
+            }
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
@@ -611,6 +638,8 @@ def main():
                             "positions + velocities read back"},
             "cpu_baseline": cpu,
         }
+        if companions:
+            line["companions"] = companions
         print(json.dumps(line), flush=True)
     sim.close()
     if pg is not None:
