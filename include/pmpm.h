@@ -88,7 +88,14 @@ enum {
    * reference's fixed order (slot, then cell-sorted particle), so repeated
    * runs are bitwise identical; the default P2G accumulates in shared memory
    * in whatever order the threads arrive */
-  PMPM_FLAG_DETERMINISTIC = 1u << 1
+  PMPM_FLAG_DETERMINISTIC = 1u << 1,
+  /* MUSL (modified update stress last; the reference declares the solver,
+   * include/pyroclastmpm/solver/musl/musl.cuh, but does not build it): after
+   * the USL grid update and a first G2P of velocities and positions, the new
+   * particle momenta are mapped to the grid again (velocity conditions only)
+   * and the velocity gradient for F and the stress update is taken from
+   * that remapped field; all mappings of a step use its start-of-step weights */
+  PMPM_FLAG_MUSL = 1u << 2
 };
 
 /* Material parameters; fill with the pmpm_material_* helpers.
@@ -316,6 +323,12 @@ int pmpm_g2p(pmpm_sim *sim, int stress_update);
 
 /* Solver::stress_update alone, from the stored velocity gradient. */
 int pmpm_stress_update(pmpm_sim *sim);
+/* The MUSL stages after USL's P2G (a handle created with PMPM_FLAG_MUSL):
+ * 1 MUSL::G2P_double_mapping (velocities, positions set aside),
+ * 2 MUSL::P2G_double_mapping (momentum remap, velocity conditions),
+ * 3 MUSL::G2P (velocity gradient, F, V, positions, stress update)
+ * (include/pyroclastmpm/solver/musl/musl.cuh). */
+int pmpm_musl_stage(pmpm_sim *sim, int stage);
 
 /* USL::solve (src/solver/usl/usl.cpp:69-115) followed by increment_global
  * (src/common/global_settings.cpp:220-227), nsteps times: Solver::solve_nsteps

@@ -85,7 +85,7 @@ def _structs(precision):
                     ("node_ids", P), ("node_types", P),
                     ("num_materials", ctypes.c_int), ("materials", P),
                     ("num_bcs", ctypes.c_int), ("bcs", P),
-                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P)]
+                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P), ("musl", ctypes.c_int)]
 
     return Grid, Material, BC, Sim
 
@@ -156,7 +156,7 @@ class OracleSim:
                  materials=(), bcs=(), precision="f32", global_step=0,
                  stresses=None, volumes=None, masses=None, volumes_original=None,
                  rigid_positions=None, rigid_velocities=None, rigid_colors=None,
-                 youngs_modulus=None, friction_angle=None):
+                 youngs_modulus=None, friction_angle=None, musl=False):
         self.precision = precision
         self.lib = _lib(precision)
         Grid, Material, BC, Sim = _structs(precision)
@@ -258,6 +258,7 @@ class OracleSim:
         s.materials = ctypes.cast(mats, ctypes.c_void_p)
         s.num_bcs = len(self.bc_list)
         s.bcs = ctypes.cast(bcarr, ctypes.c_void_p)
+        s.musl = 1 if musl else 0
         self.s = s
 
     def _fill_bc(self, c, bc, d, nn, npr):

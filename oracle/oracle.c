@@ -1144,6 +1144,147 @@ void or_stress_update(or_sim *s) {
 /* USL::solve (src/solver/usl/usl.cpp:69-115).  apply_on_nodes_f_ext has no
  * override in any boundary condition on this path, and the second
  * apply_on_particles call only writes f_ext, which the next reset clears. */
+/* ------------------------------------------------------------------------ */
+/* MUSL                                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* MUSL (declared by the reference, include/pyroclastmpm/solver/musl/musl.cuh
+ * and musl_kernels.cuh, not built there): G2P_double_mapping updates the
+ * velocities (FLIP/PIC blend as USL G2P) and positions; P2G_double_mapping
+ * maps the new momenta to the nodes (masses and moments; no forces), where
+ * the velocity conditions apply again (NodeDomain, BodyForce "fixed", the
+ * analytic rigid body); G2P then takes the velocity gradient from that field
+ * for F, V and the stress update.  All three use the step's start-of-step
+ * shape functions and bins. */
+static void musl_g2p_velocities(or_sim *s, real *xnew) {
+  const or_grid *g = &s->grid;
+  int d = g->dim, nsn = s->nsn;
+  real one_minus_alpha = (real)(1.0 - (double)s->alpha);
+  for (int i = 0; i < s->num_particles; i++) {
+    int b[3] = {0, 0, 0};
+    for (int a = 0; a < d; a++) b[a] = s->bins[i * d + a];
+    real vinc[3] = {0, 0, 0}, dvinc[3] = {0, 0, 0};
+    for (int sid = 0; sid < nsn; sid++) {
+      int w[3], sel[3];
+      window_offset(d, s->shape_function, sid, w);
+      int node = slot_target(s, b, w, sel);
+      if (s->shape_function != OR_QUADRATIC) {
+        int invalid = 0;
+        for (int a = 0; a < d; a++)
+          if (sel[a] < 0 || sel[a] >= g->num_cells[a]) invalid = 1;
+        if (invalid) continue;
+      }
+      if (node < 0) continue;
+      real m = s->node_masses[node];
+      if (m <= s->small_mass_cutoff) continue;
+      real psi = s->psi[(size_t)i * nsn + sid];
+      for (int a = 0; a < d; a++) {
+        real vn = (real)(s->node_moments[(size_t)node * d + a] / m);
+        real vnt = (real)(s->node_moments_nt[(size_t)node * d + a] / m);
+        dvinc[a] = (real)(dvinc[a] + (real)(psi * (real)(vnt - vn)));
+        vinc[a] = (real)(vinc[a] + (real)(psi * vnt));
+      }
+    }
+    real *v = s->velocities + (size_t)i * d;
+    for (int a = 0; a < d; a++) {
+      v[a] = (real)((real)(one_minus_alpha * vinc[a]) + (real)(s->alpha * (real)(v[a] + dvinc[a])));
+      xnew[(size_t)i * d + a] = (real)(s->positions[(size_t)i * d + a] + (real)(s->dt * vinc[a]));
+    }
+  }
+}
+
+static void musl_remap(or_sim *s) {
+  const or_grid *g = &s->grid;
+  int d = g->dim, nsn = s->nsn;
+  size_t nn = (size_t)g->num_cells_total;
+  real *mass = (real *)calloc(nn, sizeof(real));
+  real *mom = (real *)calloc(nn * d, sizeof(real));
+  for (int sid = 0; sid < nsn; sid++) {
+    int w[3];
+    window_offset(d, s->shape_function, sid, w);
+    for (int k = 0; k < s->num_particles; k++) {
+      int j = s->sorted_index[k];
+      if (s->hash_sorted[k] >= (unsigned int)g->num_cells_total) continue;
+      int b[3] = {0, 0, 0}, sel[3];
+      for (int a = 0; a < d; a++) b[a] = s->bins[j * d + a];
+      if (s->shape_function == OR_QUADRATIC) {
+        int out = 0;
+        for (int a = 0; a < d; a++)
+          if (b[a] < 0 || b[a] >= g->num_cells[a]) out = 1;
+        if (out) continue;
+      }
+      int node = slot_target(s, b, w, sel);
+      if (node < 0) continue;
+      real sm = (real)(s->psi[(size_t)j * nsn + sid] * s->masses[j]);
+      mass[node] = (real)(mass[node] + sm);
+      for (int a = 0; a < d; a++)
+        mom[node * d + a] = (real)(mom[node * d + a] + (real)(sm * s->velocities[(size_t)j * d + a]));
+    }
+  }
+  memset(s->node_masses, 0, sizeof(real) * nn);
+  memset(s->node_moments, 0, sizeof(real) * nn * d);
+  memset(s->node_moments_nt, 0, sizeof(real) * nn * d);
+  for (size_t n = 0; n < nn; n++) {
+    if (mass[n] <= s->small_mass_cutoff) continue;
+    s->node_masses[n] = mass[n];
+    for (int a = 0; a < d; a++) {
+      s->node_moments[n * d + a] = mom[n * d + a];
+      s->node_moments_nt[n * d + a] = mom[n * d + a];
+    }
+  }
+  free(mass);
+  free(mom);
+  for (int k = 0; k < s->num_bcs; k++) {
+    or_bc *bc = &s->bcs[k];
+    if (bc->type == OR_BC_NODEDOMAIN) nodedomain(s, bc);
+    else if (bc->type == OR_BC_BODYFORCE && bc->i[0] == 2) bodyforce(s, bc);
+    else if (bc->type == OR_BC_RIGID_SDF) rigid_sdf(s, bc);
+  }
+}
+
+static void musl_g2p_gradient(or_sim *s, const real *xnew) {
+  const or_grid *g = &s->grid;
+  int d = g->dim, nsn = s->nsn;
+  for (int i = 0; i < s->num_particles; i++) {
+    int b[3] = {0, 0, 0};
+    for (int a = 0; a < d; a++) b[a] = s->bins[i * d + a];
+    real L[9] = {0};
+    for (int sid = 0; sid < nsn; sid++) {
+      int w[3], sel[3];
+      window_offset(d, s->shape_function, sid, w);
+      int node = slot_target(s, b, w, sel);
+      if (s->shape_function != OR_QUADRATIC) {
+        int invalid = 0;
+        for (int a = 0; a < d; a++)
+          if (sel[a] < 0 || sel[a] >= g->num_cells[a]) invalid = 1;
+        if (invalid) continue;
+      }
+      if (node < 0) continue;
+      real m = s->node_masses[node];
+      if (m <= s->small_mass_cutoff) continue;
+      const real *dpsi = s->dpsi + ((size_t)i * nsn + sid) * d;
+      real vnt[3];
+      for (int a = 0; a < d; a++) vnt[a] = (real)(s->node_moments_nt[(size_t)node * d + a] / m);
+      for (int a = 0; a < d; a++)
+        for (int c = 0; c < d; c++) L[a * d + c] = (real)(L[a * d + c] + (real)(dpsi[a] * vnt[c]));
+    }
+    memcpy(s->velocity_gradient + (size_t)i * d * d, L, sizeof(real) * d * d);
+    for (int a = 0; a < d; a++) s->positions[(size_t)i * d + a] = xnew[(size_t)i * d + a];
+    real A[9], Fn[9];
+    real *F = s->F + (size_t)i * d * d;
+    for (int a = 0; a < d; a++)
+      for (int c = 0; c < d; c++) A[a * d + c] = (real)((a == c ? (real)1.0 : (real)0.0) + (real)(L[a * d + c] * s->dt));
+    for (int a = 0; a < d; a++)
+      for (int c = 0; c < d; c++) {
+        real acc = (real)(A[a * d + 0] * F[0 * d + c]);
+        for (int k = 1; k < d; k++) acc = (real)(acc + (real)(A[a * d + k] * F[k * d + c]));
+        Fn[a * d + c] = acc;
+      }
+    memcpy(F, Fn, sizeof(real) * d * d);
+    s->volumes[i] = (real)(det(d, F) * s->volumes_original[i]);
+  }
+}
+
 void or_solve(or_sim *s) {
   or_reset(s);
   or_partition(s);
@@ -1151,7 +1292,15 @@ void or_solve(or_sim *s) {
   or_apply_on_particles(s);
   or_p2g(s);
   or_apply_on_nodes_moments(s);
-  or_g2p(s);
+  if (s->musl) {
+    real *xnew = (real *)malloc(sizeof(real) * (size_t)s->num_particles * s->grid.dim);
+    musl_g2p_velocities(s, xnew);
+    musl_remap(s);
+    musl_g2p_gradient(s, xnew);
+    free(xnew);
+  } else {
+    or_g2p(s);
+  }
   or_stress_update(s);
 }
 

@@ -137,6 +137,9 @@ typedef struct {
    * (degrees) [n], or NULL: replace the material's K, G, eta, kc (friction
    * form of the material only, p[7] = Poisson ratio >= 0) */
   REAL *youngs, *friction;
+
+  /* 1: MUSL step (second momentum mapping, velocity gradient from it) */
+  int musl;
 } or_sim;
 
 void or_grid_init(or_grid *g, int dim, const REAL *origin, const REAL *end, REAL cell_size);

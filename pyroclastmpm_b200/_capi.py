@@ -24,6 +24,7 @@ MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER = 0, 1, 2, 3
 BC_GRAVITY, BC_NODEDOMAIN, BC_BODYFORCE, BC_PLANARDOMAIN = 1, 2, 3, 4
 FLAG_KEEP_VELOCITY_GRADIENT = 1
 FLAG_DETERMINISTIC = 2
+FLAG_MUSL = 4
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not supported",
@@ -83,7 +84,7 @@ EXPORTS = [
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
-    "pmpm_rollout_set_memory",
+    "pmpm_rollout_set_memory", "pmpm_musl_stage",
 ]
 
 EXPORTS += [
@@ -125,6 +126,7 @@ def lib():
     L.pmpm_calculate_timestep.argtypes = [f, f, f, f, f, fp]
     L.pmpm_rollout_forward.argtypes = [vp, i, i]
     L.pmpm_rollout_set_memory.argtypes = [vp, ctypes.c_longlong]
+    L.pmpm_musl_stage.argtypes = [vp, i]
     L.pmpm_material_point_vjp.argtypes = [ctypes.POINTER(Material), i, i, f] + [vp] * 11 + [i, i]
     L.pmpm_rollout_reset.argtypes = [vp]
     L.pmpm_rollout_backward.argtypes = [vp, vp, i, vp, vp, vp, vp]

@@ -220,4 +220,13 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def("P2G", &USL::P2G)
       .def("G2P", &USL::G2P)
       .def_readonly("alpha", &USL::alpha);
+  py::class_<MUSL, USL>(m, "MUSL")
+      .def(py::init<ParticlesContainer, NodesContainer, std::vector<MaterialType>, std::vector<BoundaryConditionType>,
+                    float, unsigned>(),
+           py::arg("particles"), py::arg("nodes"), py::arg("materials") = std::vector<MaterialType>(),
+           py::arg("boundaryconditions") = std::vector<BoundaryConditionType>(), py::arg("alpha") = 0.99f,
+           py::arg("flags") = 0u)
+      .def("G2P_double_mapping", &MUSL::G2P_double_mapping)
+      .def("P2G_double_mapping", &MUSL::P2G_double_mapping)
+      .def("G2P", &MUSL::G2P);
 }

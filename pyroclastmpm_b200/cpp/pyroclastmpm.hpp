@@ -458,5 +458,18 @@ class USL : public Solver {
   Real alpha;
 };
 
+// MUSL (include/pyroclastmpm/solver/musl/musl.cuh: declared by the reference,
+// not built there): USL's P2G and grid update, then G2P_double_mapping,
+// P2G_double_mapping and G2P (velocity gradient from the remapped momenta).
+class MUSL : public USL {
+ public:
+  MUSL(const ParticlesContainer &p, const NodesContainer &n, const std::vector<MaterialType> &mats,
+       const std::vector<BoundaryConditionType> &bcs, Real alpha = 0.99f, unsigned flags = 0)
+      : USL(p, n, mats, bcs, alpha, flags | PMPM_FLAG_MUSL) {}
+  void G2P_double_mapping() { check(pmpm_musl_stage(handle->sim, 1), "G2P_double_mapping"); }
+  void P2G_double_mapping() { check(pmpm_musl_stage(handle->sim, 2), "P2G_double_mapping"); }
+  void G2P() { check(pmpm_musl_stage(handle->sim, 3), "G2P"); }
+};
+
 }  // namespace dim2 / dim3
 }  // namespace pyroclastmpm

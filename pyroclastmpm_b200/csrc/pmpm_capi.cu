@@ -106,6 +106,8 @@ struct pmpm_sim {
   RigidState rigid;
   std::vector<SdfState> sdf;
   bool rigid_shift_pending = false;  // the next G2P moves rigid particles by their set velocity
+  float *musl_x = nullptr;           // MUSL: new positions between the two G2P passes
+  int remap_now = 0, musl_pass_now = 0;
   // differentiable rollout: checkpoints of the particle state (storage-slot
   // order, so the physical re-sort is off while a rollout is held)
   struct Rollout {
@@ -198,6 +200,7 @@ void free_particles(pmpm_sim *s) {
   dfree(s->slot);
   dfree(s->key);
   dfree(s->B.order);
+  dfree(s->musl_x);
   s->n = 0;
   s->stride = 0;
 }
@@ -251,6 +254,9 @@ StepArgs make_args(pmpm_sim *s) {
   a.nbc = (int)s->bcs.size();
   a.nbc_epi = s->rbls_index >= 0 ? s->rbls_index : a.nbc;
   a.rigid_shift = s->rigid_shift_pending ? 1 : 0;
+  a.remap = s->remap_now;
+  a.musl_pass = s->musl_pass_now;
+  a.musl_x = s->musl_x;
   a.has_planar = s->has_planar ? 1 : 0;
   a.has_sref = s->has_sref ? 1 : 0;
   for (int k = 0; k < a.nmat; k++) a.mat[k] = s->mats[k];
@@ -392,7 +398,7 @@ int launch_reorder(pmpm_sim *s) {
 
 template <int D, int SF>
 int launch_p2g(pmpm_sim *s, int apply_bcs) {
-  if (apply_bcs) {
+  if (apply_bcs && !s->remap_now) {
     update_gravity(s);
     update_bodies(s);
   }
@@ -423,7 +429,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   PMPM_LAUNCHED();
   s->launches += 1;
   s->p2g_epoch = s->epoch;
-  if (apply_bcs) PMPM_TRY(launch_rigid<D>(s));
+  if (apply_bcs && !s->remap_now) PMPM_TRY(launch_rigid<D>(s));
   return PMPM_OK;
 }
 
@@ -437,6 +443,27 @@ int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
   return PMPM_OK;
 }
 
+// MUSL after the first P2G: G2P of velocities and positions, momentum
+// remap, G2P of the velocity gradient with F, V and the stress update.
+template <int D, int SF>
+int musl_tail(pmpm_sim *s, int store_L) {
+  s->musl_pass_now = 1;
+  int st = launch_g2p<D, SF>(s, 0, 0);
+  if (st == PMPM_OK) {
+    s->musl_pass_now = 0;
+    s->remap_now = 1;  // node conditions on velocities only (node_bcs)
+    st = launch_p2g<D, SF>(s, 1);
+  }
+  if (st == PMPM_OK) {
+    s->remap_now = 0;
+    s->musl_pass_now = 2;
+    st = launch_g2p<D, SF>(s, 1, store_L);
+  }
+  s->remap_now = 0;
+  s->musl_pass_now = 0;
+  return st;
+}
+
 template <int D, int SF>
 int step_once(pmpm_sim *s) {
   PMPM_TRY((launch_partition<D, SF>(s)));
@@ -447,7 +474,10 @@ int step_once(pmpm_sim *s) {
   }
   PMPM_TRY((launch_p2g<D, SF>(s, 1)));
   const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
-  PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
+  if (s->flags & PMPM_FLAG_MUSL)
+    PMPM_TRY((musl_tail<D, SF>(s, store_L)));
+  else
+    PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
   s->step += 1;
   return PMPM_OK;
 }
@@ -1045,7 +1075,7 @@ static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
       s->has_planar = true;
     } else if (b.type == PMPM_BC_RIGIDBODY_LEVELSET) {
       // the reference hard-codes the linear window (rigidbodylevelset_inline.h:88-101)
-      if (s->rbls_index >= 0 || s->shape != PMPM_SHAPE_LINEAR) {
+      if (s->rbls_index >= 0 || s->shape != PMPM_SHAPE_LINEAR || (s->flags & PMPM_FLAG_MUSL)) {
         st = PMPM_ERR_NOT_SUPPORTED;
         break;
       }
@@ -1218,6 +1248,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   PMPM_TRY(dalloc(&s->slot, (size_t)s->stride));
   PMPM_TRY(dalloc(&s->key, (size_t)s->stride));
   PMPM_TRY(dalloc(&s->B.order, (size_t)s->stride));
+  if (s->flags & PMPM_FLAG_MUSL) PMPM_TRY(dalloc(&s->musl_x, (size_t)s->dim * s->stride));
   const int st = s->stride;
   const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6;
   // ParticlesContainer ctor (src/particles/particles.cpp:51-149): rigid particles appended
@@ -1525,6 +1556,38 @@ int pmpm_g2p(pmpm_sim *s, int stress_update) {
   return PMPM_DISPATCH(s, launch_g2p, s, stress_update ? 1 : 0, 1);
 }
 
+}  // extern "C"
+
+namespace {
+template <int D, int SF>
+int musl_stage(pmpm_sim *s, int stage) {
+  int st = PMPM_OK;
+  if (stage == 1) {
+    s->musl_pass_now = 1;
+    st = launch_g2p<D, SF>(s, 0, 0);
+  } else if (stage == 2) {
+    s->remap_now = 1;
+    st = launch_p2g<D, SF>(s, 1);
+  } else {
+    s->musl_pass_now = 2;
+    st = launch_g2p<D, SF>(s, 1, 1);
+  }
+  s->musl_pass_now = 0;
+  s->remap_now = 0;
+  return st;
+}
+}  // namespace
+
+extern "C" {
+
+int pmpm_musl_stage(pmpm_sim *s, int stage) {
+  if (!s || stage < 1 || stage > 3) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!(s->flags & PMPM_FLAG_MUSL)) return PMPM_ERR_STATE;
+  if (s->n == 0 || !s->partitioned) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  return PMPM_DISPATCH(s, musl_stage, s, stage);
+}
+
 int pmpm_stress_update(pmpm_sim *s) {
   if (!s) return PMPM_ERR_INVALID_ARGUMENT;
   if (s->n == 0) return PMPM_ERR_STATE;
@@ -1568,8 +1631,13 @@ int profile_step(pmpm_sim *s, float *ms, int *launches) {
   n_launch += s->rbls_index >= 0 ? 3 : 1;
   PMPM_CUDA(cudaEventRecord(ev[2], s->stream));
   const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
-  PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
-  n_launch += 1;
+  if (s->flags & PMPM_FLAG_MUSL) {
+    PMPM_TRY((musl_tail<D, SF>(s, store_L)));
+    n_launch += 3;
+  } else {
+    PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
+    n_launch += 1;
+  }
   PMPM_CUDA(cudaEventRecord(ev[3], s->stream));
   s->step += 1;
   PMPM_CUDA(cudaEventSynchronize(ev[3]));
@@ -2017,7 +2085,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
       st = PMPM_ERR_INVALID_ARGUMENT;  // one kernel instantiation serves the batch
       break;
     }
-    if (h->rbls_index >= 0) {
+    if (h->rbls_index >= 0 || (h->flags & PMPM_FLAG_MUSL)) {
       st = PMPM_ERR_NOT_SUPPORTED;
       break;
     }
@@ -2325,7 +2393,8 @@ void free_rollout(pmpm_sim *s) {
 }
 
 int rollout_supported(const pmpm_sim *s) {
-  if (s->shape != PMPM_SHAPE_QUADRATIC || s->has_planar || s->rbls_index >= 0) return PMPM_ERR_NOT_SUPPORTED;
+  if (s->shape != PMPM_SHAPE_QUADRATIC || s->has_planar || s->rbls_index >= 0 || (s->flags & PMPM_FLAG_MUSL))
+    return PMPM_ERR_NOT_SUPPORTED;
   for (const DevMaterial &m : s->mats)
     if (m.type != PMPM_MAT_DRUCKER_PRAGER && m.type != PMPM_MAT_NONE) return PMPM_ERR_NOT_SUPPORTED;
   for (const DevBC &b : s->bcs)

@@ -127,6 +127,9 @@ struct StepArgs {
   int nbc;
   int nbc_epi;      // node BCs [0, nbc_epi) run in the P2G epilogue, the rest after the rigid pass
   int rigid_shift;  // G2P also moves rigid particles by their set velocity (RigidBodyLevelSet)
+  int remap;        // MUSL momentum remap: P2G without forces, velocity conditions only
+  int musl_pass;    // G2P: 0 USL; MUSL 1 velocities (+ positions aside), 2 gradient, F, V, stress
+  float *musl_x;    // MUSL: new positions between the two G2P passes
   int has_planar;
   int has_sref;
   DevMaterial mat[kMaxMat];
@@ -672,6 +675,8 @@ __device__ __forceinline__ void node_bcs_range(const StepArgs &a, int node, cons
                                                float pnt[3], int k0, int k1) {
   for (int k = k0; k < k1; k++) {
     const DevBC &bc = a.bc[k];
+    // the MUSL remap carries no forces: only conditions on velocities apply
+    if (a.remap && (bc.type == PMPM_BC_GRAVITY || (bc.type == PMPM_BC_BODYFORCE && bc.i[0] != 2))) continue;
     if (bc.type == PMPM_BC_GRAVITY) {
       if (m > 0.000000001f) {
 #pragma unroll

@@ -475,11 +475,11 @@ __device__ __forceinline__ void p2g_range(const StepArgs &a, int k0, int k1, con
     mass += sm;
 #pragma unroll
     for (int c = 0; c < D; c++) mom[c] += sm * P.v[c * st + s];
-    if (a.has_planar) {
+    if (a.has_planar && !a.remap) {
 #pragma unroll
       for (int c = 0; c < D; c++) force[c] += psi * P.fext[c * st + s];
     }
-    const float mv = -P.V[s];
+    const float mv = a.remap ? 0.0f : -P.V[s];
     float S[9];
     load_sig3<D>(P, s, S);
 #pragma unroll
@@ -898,12 +898,12 @@ __device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int a
     float mv[3], fx[3] = {0, 0, 0}, S[9];
 #pragma unroll
     for (int c = 0; c < D; c++) mv[c] = m * P.v[c * st + s];
-    if (a.has_planar) {
+    if (a.has_planar && !a.remap) {
 #pragma unroll
       for (int c = 0; c < D; c++) fx[c] = P.fext[c * st + s];
     }
     load_sig3<D>(P, s, S);
-    const float nvol = -P.V[s];
+    const float nvol = a.remap ? 0.0f : -P.V[s];
 #pragma unroll
     for (int k = 0; k < 9; k++) S[k] *= nvol;
     const unsigned hu = P.hash[s];
@@ -1193,7 +1193,7 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
           }
           float m = P.m[s];
           if (SF == PMPM_SHAPE_QUADRATIC && !inside) m = 0.0f;  // takes no part in P2G
-          const float nv = (SF == PMPM_SHAPE_QUADRATIC && !inside) ? 0.0f : -P.V[s];
+          const float nv = ((SF == PMPM_SHAPE_QUADRATIC && !inside) || a.remap) ? 0.0f : -P.V[s];
           st_u[0][jj] = u[0];
           st_u[1][jj] = u[1];
           st_b[0][jj] = b[0];
@@ -1202,7 +1202,7 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             st_mv[c][jj] = m * P.v[c * st + s];
-            st_f[c][jj] = (a.has_planar && m != 0.0f) ? P.fext[c * st + s] : 0.0f;
+            st_f[c][jj] = (a.has_planar && m != 0.0f && !a.remap) ? P.fext[c * st + s] : 0.0f;
           }
           // -V sigma, symmetric: xx yy zz xy xz yz
 #pragma unroll
@@ -1487,14 +1487,14 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
           const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
           const float uz = scaled_coord(P.x[2 * st + s], g.origin[2], g.inv_h);
           const float m = P.m[s];
-          const float nv = -P.V[s];
+          const float nv = a.remap ? 0.0f : -P.V[s];
           st_u[0][jj] = ux;
           st_u[1][jj] = uy;
           st_m[jj] = m;
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             st_mv[c][jj] = m * P.v[c * st + s];
-            st_f[c][jj] = a.has_planar ? P.fext[c * st + s] : 0.0f;
+            st_f[c][jj] = (a.has_planar && !a.remap) ? P.fext[c * st + s] : 0.0f;
           }
 #pragma unroll
           for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
@@ -1747,6 +1747,26 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
         }
       }
     }
+    // RigidBodyLevelSet::set_position (rigidbodylevelset.cpp:222-243) moved
+    // rigid particles by their set velocity before G2P; their weights above
+    // are those of the unmoved position, as the reference's stored psi
+    const bool shift = a.rigid_shift && P.rigid[s];
+    if (a.musl_pass == 1) {
+      // MUSL first mapping: velocities and the new positions (kept aside:
+      // the second mappings use this step's start-of-step weights)
+      bool finite = true;
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        const float vnew = a.one_minus_alpha * vinc[c] + a.alpha * (v[c] + dvinc[c]);
+        const float x0 = shift ? __fadd_rn(x[c], __fmul_rn(v[c], a.dt)) : x[c];
+        const float xnew = x0 + a.dt * vinc[c];
+        P.v[c * st + s] = vnew;
+        a.musl_x[c * st + s] = xnew;
+        finite = finite && isfinite(xnew);
+      }
+      if (!finite) atomicOr(a.fault, kFaultNonFinite);
+      return;
+    }
     // v <- (1 - alpha) v_pic + alpha (v + dv); x += dt v_pic; F <- (I + L dt) F; V = det(F) V0
     float F[9], A[9], Fn[9];
 #pragma unroll
@@ -1765,18 +1785,20 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
         Fn[r * D + c] = acc;
       }
     bool finite = true;
-    // RigidBodyLevelSet::set_position (rigidbodylevelset.cpp:222-243) moved
-    // rigid particles by their set velocity before G2P; their weights above
-    // are those of the unmoved position, as the reference's stored psi
-    const bool shift = a.rigid_shift && P.rigid[s];
+    if (a.musl_pass == 2) {
+      // MUSL second G2P: L from the remapped velocities; positions from the first mapping
 #pragma unroll
-    for (int c = 0; c < D; c++) {
-      const float vnew = a.one_minus_alpha * vinc[c] + a.alpha * (v[c] + dvinc[c]);
-      const float x0 = shift ? __fadd_rn(x[c], __fmul_rn(v[c], a.dt)) : x[c];
-      const float xnew = x0 + a.dt * vinc[c];
-      P.v[c * st + s] = vnew;
-      P.x[c * st + s] = xnew;
-      finite = finite && isfinite(xnew);
+      for (int c = 0; c < D; c++) P.x[c * st + s] = a.musl_x[c * st + s];
+    } else {
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        const float vnew = a.one_minus_alpha * vinc[c] + a.alpha * (v[c] + dvinc[c]);
+        const float x0 = shift ? __fadd_rn(x[c], __fmul_rn(v[c], a.dt)) : x[c];
+        const float xnew = x0 + a.dt * vinc[c];
+        P.v[c * st + s] = vnew;
+        P.x[c * st + s] = xnew;
+        finite = finite && isfinite(xnew);
+      }
     }
 #pragma unroll
     for (int k = 0; k < D * D; k++) P.F[k * st + s] = Fn[k];

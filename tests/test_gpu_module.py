@@ -115,3 +115,25 @@ def test_scoop_through_module_matches_capi():
     sim.solve(5)
     for name in ("positions", "velocities", "stresses"):
         assert rel(getattr(mpm.particles, name), sim.get(name)) < 1e-6, name
+
+
+def test_musl_through_module_matches_capi():
+    """The MUSL class (declared by the reference, built here) against a C ABI
+    handle with the MUSL flag, deterministic reduction: bit for bit."""
+    import pyroclastmpm_b200.MPM2D as pm
+    from pyroclastmpm_b200 import Simulation
+
+    sc = scenes.two_discs()
+    rng = np.random.default_rng(5)
+    sc["velocities"] = sc["velocities"] * (1.0 + 0.01 * rng.uniform(-1, 1, sc["velocities"].shape))
+    pm.set_globals(sc["dt"], sc["particles_per_cell"], "linear", "output")
+    pm.set_global_step(0)
+    nodes = pm.NodesContainer([0.0, 0.0], [1.0, 1.0], sc["cell_size"])
+    particles = pm.ParticlesContainer(sc["positions"], sc["velocities"])
+    mpm = pm.MUSL(particles, nodes, [pm.LinearElastic(1000.0, 1000.0, 0.3)], alpha=0.99, flags=2)
+    mpm.solve_nsteps(5)
+    sim = Simulation(**scenes.sim_kwargs(sc), flags=2 | 4)
+    sim.set_particles(sc["positions"], sc["velocities"]).initialize()
+    sim.solve(5)
+    for name in ("positions", "velocities", "stresses"):
+        np.testing.assert_array_equal(getattr(mpm.particles, name), sim.get(name))

@@ -464,3 +464,71 @@ def test_out_of_domain_is_reported_not_fatal():
     sim.solve(1)
     assert sim.synchronize() == 16
     assert np.isfinite(sim.get("positions")[1:]).all()
+
+
+# ----------------------------------------------------------------------------
+# MUSL (second momentum mapping)
+# ----------------------------------------------------------------------------
+
+MUSL_CASES = ["discs_2d_linear_le", "column_3d_quadratic_dp", "random_2d_quadratic_nf", "random_3d_cubic_le_gravity",
+              "sdf_3d_quadratic_shell"]
+
+
+def musl_pair(scene, precision, flags):
+    kw = scenes.sim_kwargs(scene)
+    sim = Simulation(**kw, flags=flags | 4)
+    sim.set_particles(**particle_kwargs(scene))
+    ref = oracle.OracleSim(**kw, **particle_kwargs(scene), precision=precision, musl=True)
+    return sim, ref
+
+
+@pytest.mark.parametrize("case", MUSL_CASES)
+@pytest.mark.parametrize("flags", [1, 3])
+def test_musl_one_step_matches_oracle(case, flags):
+    scene = STEP_CASES[case]()
+    sim, ref = musl_pair(scene, "f32", flags)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(1)
+    ref.solve(1)
+    names = FIELDS + ("velocity_gradient",)
+    refs = [oracle.OracleSim(**scenes.sim_kwargs(scene), **particle_kwargs(scene), precision=p,
+                             musl=True).initialize() for p in ("f32", "f64")]
+    for r in refs:
+        r.solve(1)
+    for name in names:
+        tol = max(STEP_TOL, 3.0 * rel(refs[0][name], refs[1][name]))
+        err = rel(sim.get(name), ref[name])
+        assert err <= tol, f"{case} {name}: {err:.3e} > {tol:.1e}"
+
+
+@pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp"])
+def test_musl_drift_vs_fp64(case):
+    scene = STEP_CASES[case]()
+    sim, ref = musl_pair(scene, "f64", 0)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(20)
+    ref.solve(20)
+    assert sim.synchronize() == 0
+    for name in ("positions", "velocities", "stresses"):
+        err = rel(sim.get(name), ref[name])
+        assert err <= 1e-4, f"{case} {name}: {err:.3e}"
+
+
+def test_musl_stages_equal_solve():
+    """partition, P2G, the three MUSL stages and the step counter by hand give
+    what one solve gives (deterministic reduction, so bit for bit)."""
+    scene = STEP_CASES["column_3d_quadratic_dp"]()
+    a, _ = musl_pair(scene, "f32", 3)
+    b, _ = musl_pair(scene, "f32", 3)
+    a.initialize()
+    b.initialize()
+    a.solve(1)
+    from pyroclastmpm_b200._capi import check, lib
+    b.partition()
+    b.p2g(apply_bcs=True)
+    for stage in (1, 2, 3):
+        check(lib().pmpm_musl_stage(b.handle, stage), "musl stage")
+    for name in ("positions", "velocities", "stresses", "F"):
+        np.testing.assert_array_equal(a.get(name), b.get(name))

@@ -5,7 +5,8 @@ import pytest
 NAMES = ["set_globals", "set_global_shapefunction", "set_global_timestep", "set_global_step",
          "set_global_output_directory", "NodesContainer", "ParticlesContainer", "Solver", "USL",
          "Material", "LinearElastic", "NewtonFluid", "DruckerPrager", "BoundaryCondition", "Gravity",
-         "NodeDomain", "BodyForce", "PlanarDomain", "RigidBodyLevelSet", "calculate_timestep", "global_dimension"]
+         "NodeDomain", "BodyForce", "PlanarDomain", "RigidBodyLevelSet", "calculate_timestep", "MUSL",
+         "global_dimension"]
 
 
 @pytest.mark.parametrize("dim", [2, 3])
