@@ -79,7 +79,11 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def_property_readonly("moments_nt", [](const NodesContainer &n) {
         return to_array(n.moments_nt(), {n.num_cells_total, DIM});
       })
-      .def("set_output_formats", [](NodesContainer &, const std::vector<std::string> &) {}, py::arg("output_formats"));
+      .def(
+          "set_output_formats",
+          [](NodesContainer &n, const std::vector<std::string> &f) { n.output_formats = f; },
+          py::arg("output_formats"))
+      .def_readwrite("output_formats", &NodesContainer::output_formats);
 
   auto P = py::class_<ParticlesContainer>(m, "ParticlesContainer", py::dynamic_attr());
   P.def(py::init([](py::object pos, py::object vel, py::object col, py::object rpos, py::object rvel, py::object rcol) {
@@ -90,7 +94,99 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
         py::arg("rigid_positions") = py::none(), py::arg("rigid_velocities") = py::none(),
         py::arg("rigid_colors") = py::none());
   P.def_readonly("num_particles", &ParticlesContainer::num_particles);
-  P.def("set_output_formats", [](ParticlesContainer &, const std::vector<std::string> &) {}, py::arg("output_formats"));
+  P.def(
+      "set_output_formats", [](ParticlesContainer &p, const std::vector<std::string> &f) { p.output_formats = f; },
+      py::arg("output_formats"));
+  P.def_readwrite("output_formats", &ParticlesContainer::output_formats);
+  P.def_readwrite("exclude_rigid_from_output", &ParticlesContainer::exclude_rigid_from_output);
+  // pickle_save_particles / pickle_load_particles (python/pybind/particles/
+  // particles_bind.cpp:39-83): the same 13-entry tuple; psi and dpsi are not
+  // kept between steps here (they are recomputed in registers), so entries
+  // 10 and 12 are empty
+  P.def(py::pickle(
+      [](ParticlesContainer &p) {
+        const bool bound = (bool)p.handle;
+        auto getf = [&](int id, int nc, const std::vector<Real> &host) -> py::array_t<float> {
+          if (bound) return to_array(p.get<float>(id, nc), {p.num_particles, nc});
+          if (!host.empty()) return to_array(host, {(py::ssize_t)(host.size() / nc), nc});
+          return py::array_t<float>(std::vector<py::ssize_t>{0, nc});
+        };
+        std::vector<Real> pos = p.positions_, vel = p.velocities_;
+        pos.insert(pos.end(), p.rigid_positions_.begin(), p.rigid_positions_.end());
+        py::array_t<float> x = getf(PMPM_FIELD_POSITIONS, DIM, pos);
+        py::array_t<float> v = bound ? getf(PMPM_FIELD_VELOCITIES, DIM, {}) : py::array_t<float>();
+        if (!bound) {
+          std::vector<Real> vv = p.velocities_;
+          const size_t nn = p.positions_.size() / DIM, nr = p.rigid_positions_.size() / DIM;
+          if (vv.empty()) vv.assign(nn * DIM, 0.0f);
+          if (p.rigid_velocities_.empty())
+            vv.insert(vv.end(), nr * DIM, 0.0f);
+          else
+            vv.insert(vv.end(), p.rigid_velocities_.begin(), p.rigid_velocities_.end());
+          v = to_array(vv, {(py::ssize_t)(nn + nr), DIM});
+        }
+        std::vector<int> col, rig;
+        if (bound) {
+          for (auto c : p.get<unsigned char>(PMPM_FIELD_COLORS, 1)) col.push_back(c);
+          for (auto r : p.get<unsigned char>(PMPM_FIELD_IS_RIGID, 1)) rig.push_back(r);
+        } else {
+          const size_t nn = p.positions_.size() / DIM, nr = p.rigid_positions_.size() / DIM;
+          for (size_t i = 0; i < nn; i++) col.push_back(i < p.colors_.size() ? p.colors_[i] : 0);
+          for (size_t i = 0; i < nr; i++) col.push_back(i < p.rigid_colors_.size() ? p.rigid_colors_[i] : 0);
+          rig.assign(nn, 0);
+          rig.insert(rig.end(), nr, 1);
+        }
+        auto opt = [&](int id, int nc) -> py::object {
+          if (!bound) return py::list();
+          return getf(id, nc, {});
+        };
+        return py::make_tuple(x, v, col, rig, opt(PMPM_FIELD_STRESSES, 9), opt(PMPM_FIELD_MASSES, 1),
+                              opt(PMPM_FIELD_VOLUMES, 1), p.output_formats, opt(PMPM_FIELD_F, DIM * DIM),
+                              opt(PMPM_FIELD_VELOCITY_GRADIENT, DIM * DIM), py::list(),
+                              opt(PMPM_FIELD_VOLUMES_ORIGINAL, 1), py::list());
+      },
+      [](py::tuple t) {
+        if (t.size() != 13) throw std::runtime_error("a ParticlesContainer pickle is a 13-entry tuple");
+        auto x = flat(t[0], DIM), v = flat(t[1], DIM);
+        auto col = t[2].cast<std::vector<int>>();
+        auto rig = t[3].cast<std::vector<int>>();
+        const size_t n = x.size() / DIM;
+        std::vector<Real> xp, vp, xr, vr;
+        std::vector<int> cp, cr;
+        for (size_t i = 0; i < n; i++) {
+          const bool r = i < rig.size() && rig[i];
+          auto &X = r ? xr : xp;
+          auto &Vv = r ? vr : vp;
+          for (int a = 0; a < DIM; a++) {
+            X.push_back(x[i * DIM + a]);
+            Vv.push_back(v.empty() ? 0.0f : v[i * DIM + a]);
+          }
+          (r ? cr : cp).push_back(i < col.size() ? col[i] : 0);
+        }
+        ParticlesContainer p(xp, vp, cp, xr, vr, cr);
+        // stored fields are in input order: non-rigid first, then rigid
+        std::vector<size_t> order;
+        for (size_t i = 0; i < n; i++)
+          if (!(i < rig.size() && rig[i])) order.push_back(i);
+        for (size_t i = 0; i < n; i++)
+          if (i < rig.size() && rig[i]) order.push_back(i);
+        auto put = [&](int id, int nc, py::handle h) {
+          auto f = flat(py::reinterpret_borrow<py::object>(h), 1);
+          if (f.size() != n * nc) return;  // not stored
+          std::vector<float> o(n * nc);
+          for (size_t j = 0; j < n; j++)
+            for (int k = 0; k < nc; k++) o[j * nc + k] = f[order[j] * nc + k];
+          p.set<float>(id, o, nc);
+        };
+        put(PMPM_FIELD_STRESSES, 9, t[4]);
+        put(PMPM_FIELD_MASSES, 1, t[5]);
+        put(PMPM_FIELD_VOLUMES, 1, t[6]);
+        p.output_formats = t[7].cast<std::vector<std::string>>();
+        put(PMPM_FIELD_F, DIM * DIM, t[8]);
+        put(PMPM_FIELD_VELOCITY_GRADIENT, DIM * DIM, t[9]);
+        put(PMPM_FIELD_VOLUMES_ORIGINAL, 1, t[11]);
+        return p;
+      }));
 #define PMPM_PROP(NAME, ID, NCOMP, ...)                                                              \
   P.def_property(                                                                                   \
       NAME,                                                                                         \

@@ -16,7 +16,11 @@
 
 #include <array>
 #include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
 #include <memory>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <variant>
@@ -79,6 +83,73 @@ inline void set_globals(Real dt, int ppc, const std::string &shape, const std::s
   set_global_particles_per_cell(ppc);
 }
 
+// ---------------------------------------------------------------------------
+// output (write_vtk_polydata, src/common/output.cpp:132-191): point sets with
+// named point arrays, written without VTK: "vtk" -> <stem><step>.vtp (XML
+// PolyData, ASCII), "csv" -> <stem><step>.csv (one column per component,
+// "Name:k", as vtkDelimitedTextWriter), "obj" -> <stem><step>.obj (vertices)
+// ---------------------------------------------------------------------------
+struct OutputArray {
+  std::string name;
+  int ncomp;
+  std::vector<double> data;  // [n][ncomp]
+};
+
+inline void write_point_set(const std::string &directory, const std::string &stem, int step, double time,
+                            const std::vector<double> &points3, const std::vector<OutputArray> &arrays,
+                            const std::vector<std::string> &formats) {
+  const size_t n = points3.size() / 3;
+  std::string base = directory;
+  if (!base.empty() && base.back() != '/') base += "/";
+  base += stem + std::to_string(step);
+  for (const std::string &fmt : formats) {
+    std::ostringstream o;
+    o << std::setprecision(9);
+    if (fmt == "vtk") {
+      o << "<?xml version=\"1.0\"?>\n<VTKFile type=\"PolyData\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
+        << "<PolyData>\n<FieldData>\n<DataArray type=\"Float64\" Name=\"Time\" NumberOfTuples=\"1\" "
+        << "format=\"ascii\">" << time << "</DataArray>\n</FieldData>\n"
+        << "<Piece NumberOfPoints=\"" << n << "\" NumberOfVerts=\"0\" NumberOfLines=\"0\" NumberOfStrips=\"0\" "
+        << "NumberOfPolys=\"0\">\n<PointData>\n";
+      for (const OutputArray &a : arrays) {
+        o << "<DataArray type=\"Float64\" Name=\"" << a.name << "\" NumberOfComponents=\"" << a.ncomp
+          << "\" format=\"ascii\">\n";
+        for (double v : a.data) o << v << " ";
+        o << "\n</DataArray>\n";
+      }
+      o << "</PointData>\n<Points>\n<DataArray type=\"Float32\" Name=\"Points\" NumberOfComponents=\"3\" "
+        << "format=\"ascii\">\n";
+      for (double v : points3) o << v << " ";
+      o << "\n</DataArray>\n</Points>\n</Piece>\n</PolyData>\n</VTKFile>\n";
+    } else if (fmt == "csv") {
+      bool first = true;
+      for (const OutputArray &a : arrays)
+        for (int k = 0; k < a.ncomp; k++) {
+          o << (first ? "" : ",") << "\"" << a.name << (a.ncomp > 1 ? ":" + std::to_string(k) : "") << "\"";
+          first = false;
+        }
+      o << "\n";
+      for (size_t i = 0; i < n; i++) {
+        first = true;
+        for (const OutputArray &a : arrays)
+          for (int k = 0; k < a.ncomp; k++) {
+            o << (first ? "" : ",") << a.data[i * a.ncomp + k];
+            first = false;
+          }
+        o << "\n";
+      }
+    } else if (fmt == "obj") {
+      for (size_t i = 0; i < n; i++) o << "v " << points3[3 * i] << " " << points3[3 * i + 1] << " " << points3[3 * i + 2] << "\n";
+    } else {
+      throw std::invalid_argument("output format must be \"vtk\", \"csv\" or \"obj\" (no glTF writer here)");
+    }
+    const std::string ext = fmt == "vtk" ? ".vtp" : "." + fmt;
+    std::ofstream f(base + ext);
+    if (!f) throw std::runtime_error("cannot write " + base + ext);
+    f << o.str();
+  }
+}
+
 // the simulation handle shared by a solver and the containers bound to it
 struct SimHandle {
   pmpm_sim *sim = nullptr;
@@ -112,6 +183,22 @@ class NodesContainer {
     std::vector<Real> out((size_t)num_cells_total * ncomp, 0.0f);
     if (handle) check(pmpm_get_field(handle->sim, id, out.data(), out.size() * sizeof(Real), 0), "nodes field");
     return out;
+  }
+  std::vector<std::string> output_formats;
+  // NodesContainer::output_vtk (src/nodes/nodes.cpp:215-250): the reference
+  // writes nodes only while the global step is at most 1
+  void output_vtk(int step, double time, const std::string &directory) const {
+    if (output_formats.empty() || step > 1) return;
+    const std::vector<Real> xyz = give_coords();
+    std::vector<double> pts((size_t)num_cells_total * 3, 0.0);
+    for (int i = 0; i < num_cells_total; i++)
+      for (int a = 0; a < DIM; a++) pts[(size_t)i * 3 + a] = xyz[(size_t)i * DIM + a];
+    auto arr = [](const std::string &name, int nc, const std::vector<Real> &v) {
+      return OutputArray{name, nc, std::vector<double>(v.begin(), v.end())};
+    };
+    write_point_set(directory, "nodes", step, time, pts,
+                    {arr("Moments", DIM, moments()), arr("MomentsNT", DIM, moments_nt()), arr("Mass", 1, masses())},
+                    output_formats);
   }
   std::vector<Real> masses() const { return field(PMPM_FIELD_NODE_MASSES, 1); }
   std::vector<Real> moments() const { return field(PMPM_FIELD_NODE_MOMENTS, DIM); }
@@ -174,6 +261,80 @@ class ParticlesContainer {
   void apply_pending() {
     for (auto &kv : pending) check(pmpm_set_field(handle->sim, kv.first, kv.second.data(), kv.second.size(), 0), "set");
     pending.clear();
+  }
+
+  std::vector<std::string> output_formats;
+  bool exclude_rigid_from_output = true;
+  // ParticlesContainer::output_vtk (src/particles/particles.cpp:209-318): the
+  // state plus pressure p = tr(sigma_DIM)/3, q = sqrt(3/2 s:s), |q|/p as
+  // |q|/(-p), volumetric strain -tr(eps) and deviatoric strain
+  // sqrt(1/2 e:e) of eps = (F + F^T)/2 - I; rigid particles left out
+  void output_vtk(int step, double time, const std::string &directory) const {
+    if (output_formats.empty() || !handle) return;
+    const size_t n = (size_t)num_particles;
+    const auto x = get<Real>(PMPM_FIELD_POSITIONS, DIM), v = get<Real>(PMPM_FIELD_VELOCITIES, DIM);
+    const auto S = get<Real>(PMPM_FIELD_STRESSES, 9), L = get<Real>(PMPM_FIELD_VELOCITY_GRADIENT, DIM * DIM);
+    const auto F = get<Real>(PMPM_FIELD_F, DIM * DIM), m = get<Real>(PMPM_FIELD_MASSES, 1);
+    const auto V = get<Real>(PMPM_FIELD_VOLUMES, 1), V0 = get<Real>(PMPM_FIELD_VOLUMES_ORIGINAL, 1);
+    const auto col = get<unsigned char>(PMPM_FIELD_COLORS, 1), rig = get<unsigned char>(PMPM_FIELD_IS_RIGID, 1);
+    std::vector<size_t> keep;
+    for (size_t i = 0; i < n; i++)
+      if (!(exclude_rigid_from_output && rig[i])) keep.push_back(i);
+    std::vector<double> pts(keep.size() * 3, 0.0);
+    std::vector<OutputArray> arrays;
+    auto add = [&](const std::string &name, int nc, auto &&value) {
+      OutputArray a{name, nc, std::vector<double>(keep.size() * nc)};
+      for (size_t j = 0; j < keep.size(); j++)
+        for (int k = 0; k < nc; k++) a.data[j * nc + k] = value(keep[j], k);
+      arrays.push_back(std::move(a));
+    };
+    for (size_t j = 0; j < keep.size(); j++)
+      for (int a = 0; a < DIM; a++) pts[j * 3 + a] = x[keep[j] * DIM + a];
+    std::vector<double> p(n), q(n), mu(n), dev(n), vol(n);
+    for (size_t i = 0; i < n; i++) {
+      const Real *s = &S[i * 9];
+      double tr = 0.0;
+      for (int a = 0; a < DIM; a++) tr += s[4 * a];
+      p[i] = tr / 3.0;
+      double ss = 0.0;
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+          const double d = s[3 * a + b] - (a == b ? p[i] : 0.0);
+          ss += d * d;
+        }
+      q[i] = std::sqrt(1.5 * ss);
+      mu[i] = std::fabs(q[i]) / (-p[i]);
+      double e[DIM * DIM], etr = 0.0;
+      for (int a = 0; a < DIM; a++)
+        for (int b = 0; b < DIM; b++) {
+          e[a * DIM + b] = 0.5 * (F[i * DIM * DIM + a * DIM + b] + F[i * DIM * DIM + b * DIM + a]) - (a == b ? 1.0 : 0.0);
+          if (a == b) etr += e[a * DIM + b];
+        }
+      vol[i] = -etr;
+      double es = 0.0;
+      for (int a = 0; a < DIM; a++)
+        for (int b = 0; b < DIM; b++) {
+          const double d = e[a * DIM + b] + (a == b ? vol[i] / 3.0 : 0.0);
+          es += d * d;
+        }
+      dev[i] = std::sqrt(0.5 * es);
+    }
+    add("isRigid", 1, [&](size_t i, int) { return (double)rig[i]; });
+    add("Positions", DIM, [&](size_t i, int k) { return (double)x[i * DIM + k]; });
+    add("Velocity", DIM, [&](size_t i, int k) { return (double)v[i * DIM + k]; });
+    add("Stress", 9, [&](size_t i, int k) { return (double)S[i * 9 + k]; });
+    add("VelocityGradient", DIM * DIM, [&](size_t i, int k) { return (double)L[i * DIM * DIM + k]; });
+    add("DeformationMatrix", DIM * DIM, [&](size_t i, int k) { return (double)F[i * DIM * DIM + k]; });
+    add("Mass", 1, [&](size_t i, int) { return (double)m[i]; });
+    add("Volume", 1, [&](size_t i, int) { return (double)V[i]; });
+    add("VolumeOriginal", 1, [&](size_t i, int) { return (double)V0[i]; });
+    add("Color", 1, [&](size_t i, int) { return (double)col[i]; });
+    add("Pressure", 1, [&](size_t i, int) { return p[i]; });
+    add("q", 1, [&](size_t i, int) { return q[i]; });
+    add("|q|/p", 1, [&](size_t i, int) { return mu[i]; });
+    add("dev strain", 1, [&](size_t i, int) { return dev[i]; });
+    add("vol strain", 1, [&](size_t i, int) { return vol[i]; });
+    write_point_set(directory, "particles", step, time, pts, arrays, output_formats);
   }
 };
 
@@ -405,6 +566,7 @@ class Solver {
     particles.apply_pending();
     check(pmpm_set_step(handle->sim, globals().step), "pmpm_set_step");
     check(pmpm_initialize(handle->sim), "pmpm_initialize");
+    output();
   }
   virtual ~Solver() = default;
 
@@ -417,13 +579,32 @@ class Solver {
   void solve_nsteps(int n) {
     check(pmpm_solve(handle->sim, n), "solve_nsteps");
     sync_step();
+    output();
   }
-  // Solver::run (src/solver/solver.cpp:140-174): total_steps + 1 solves
+  // Solver::run (src/solver/solver.cpp:140-174): output, solve, then
+  // total_steps solves with output every output_frequency
   void run(int total_steps, int output_frequency) {
-    (void)output_frequency;  // output writers are outside this path
-    check(pmpm_solve(handle->sim, total_steps + 1), "run");
+    output();
+    const bool any = !particles.output_formats.empty() || !nodes.output_formats.empty();
+    if (!any || output_frequency <= 0) {
+      check(pmpm_solve(handle->sim, total_steps + 1), "run");
+      sync_step();
+      return;
+    }
+    check(pmpm_solve(handle->sim, 1), "run");
+    for (int step = 1; step < total_steps + 1; step++) {
+      // the reference writes after solve() and before the step increment
+      check(pmpm_solve(handle->sim, 1), "run");
+      if (step % output_frequency == 0) {
+        int st = 0;
+        check(pmpm_get_step(handle->sim, &st), "step");
+        write_output(st - 1);
+      }
+    }
     sync_step();
   }
+  // Solver::output (src/solver/solver.cpp:177-197)
+  void output() { write_output(current_step()); }
   void stress_update() { check(pmpm_stress_update(handle->sim), "stress_update"); }
   int status() { return pmpm_synchronize(handle->sim); }
   int current_step() const {
@@ -435,6 +616,12 @@ class Solver {
   NodesContainer nodes;
   ParticlesContainer particles;
   std::vector<MaterialType> materials;
+
+  void write_output(int step) {
+    const double time = (double)((Real)step * globals().dt);
+    particles.output_vtk(step, time, globals().output_directory);
+    nodes.output_vtk(step, time, globals().output_directory);
+  }
   std::vector<BoundaryConditionType> boundaryconditions;
   std::shared_ptr<SimHandle> handle;
 

@@ -137,3 +137,59 @@ def test_musl_through_module_matches_capi():
     sim.solve(5)
     for name in ("positions", "velocities", "stresses"):
         np.testing.assert_array_equal(getattr(mpm.particles, name), sim.get(name))
+
+
+def test_output_writers_and_run_schedule(tmp_path):
+    """Solver.run(total, frequency) writes particles<step>.vtp/.csv/.obj at
+    step 0 and every `frequency` steps, nodes at steps 0 and 1 only (the
+    reference's rule); the files hold the state the getters return."""
+    import xml.etree.ElementTree as ET
+
+    import pyroclastmpm_b200.MPM2D as pm
+
+    sc = scenes.two_discs()
+    pm.set_globals(sc["dt"], sc["particles_per_cell"], "linear", str(tmp_path))
+    pm.set_global_step(0)
+    nodes = pm.NodesContainer([0.0, 0.0], [1.0, 1.0], sc["cell_size"])
+    nodes.set_output_formats(["vtk"])
+    particles = pm.ParticlesContainer(sc["positions"], sc["velocities"])
+    particles.set_output_formats(["vtk", "csv", "obj"])
+    mpm = pm.USL(particles, nodes, [pm.LinearElastic(1000.0, 1000.0, 0.3)])
+    mpm.run(10, 5)
+    names = sorted(f.name for f in tmp_path.iterdir())
+    for step in (0, 5, 10):
+        for ext in ("vtp", "csv", "obj"):
+            assert f"particles{step}.{ext}" in names
+    assert "nodes0.vtp" in names and "nodes5.vtp" not in names
+    root = ET.parse(tmp_path / "particles10.vtp").getroot()
+    arrays = {a.get("Name"): a for a in root.iter("DataArray")}
+    for key in ("Positions", "Velocity", "Stress", "Pressure", "q", "dev strain", "vol strain"):
+        assert key in arrays, key
+    pos10 = np.array(arrays["Positions"].text.split(), np.float64).reshape(-1, 2)
+    assert float(arrays["Time"].text) == pytest.approx(10 * sc["dt"], rel=1e-6)
+    # run(10) made 11 solves; the last file was written after the 11th solve
+    np.testing.assert_allclose(pos10, mpm.particles.positions, rtol=0, atol=1e-6)
+    header = (tmp_path / "particles0.csv").read_text().splitlines()[0]
+    assert header.startswith('"isRigid","Positions:0","Positions:1","Velocity:0"')
+
+
+def test_particles_pickle_restart():
+    """A bound container pickled after some steps restarts a new solver with
+    the same state (stress, F, masses, volumes)."""
+    import pickle
+
+    import pyroclastmpm_b200.MPM2D as pm
+
+    sc = scenes.two_discs()
+    pm.set_globals(sc["dt"], sc["particles_per_cell"], "linear", "output")
+    pm.set_global_step(0)
+    nodes = pm.NodesContainer([0.0, 0.0], [1.0, 1.0], sc["cell_size"])
+    particles = pm.ParticlesContainer(sc["positions"], sc["velocities"])
+    mpm = pm.USL(particles, nodes, [pm.LinearElastic(1000.0, 1000.0, 0.3)])
+    mpm.solve_nsteps(20)
+    saved = pickle.dumps(mpm.particles)
+    restored = pickle.loads(saved)
+    mpm2 = pm.USL(restored, pm.NodesContainer([0.0, 0.0], [1.0, 1.0], sc["cell_size"]),
+                  [pm.LinearElastic(1000.0, 1000.0, 0.3)])
+    for name in ("positions", "velocities", "stresses", "F", "masses", "volumes"):
+        np.testing.assert_array_equal(getattr(mpm2.particles, name), getattr(mpm.particles, name), err_msg=name)

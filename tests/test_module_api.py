@@ -72,3 +72,32 @@ def test_calculate_timestep_and_rigid_body_api():
     scoop.set_motion([0.5, 0.0, 0.0], 1.0)
     scoop.friction = 0.3
     assert scoop.friction == pytest.approx(0.3)
+
+
+def test_particles_pickle_round_trip_unbound():
+    """pickle_save_particles / pickle_load_particles layout (13 entries) for a
+    container not yet bound to a solver (no GPU needed)."""
+    import pickle
+
+    import pyroclastmpm_b200.MPM2D as pm
+
+    rng = np.random.default_rng(0)
+    x = rng.uniform(0.2, 0.8, (20, 2))
+    v = rng.normal(0, 1, (20, 2))
+    rx = rng.uniform(0.2, 0.8, (5, 2))
+    p = pm.ParticlesContainer(x, v, colors=np.arange(20) % 2, rigid_positions=rx, rigid_colors=[3] * 5)
+    p.set_output_formats(["vtk", "csv"])
+    t = p.__getstate__()
+    assert len(t) == 13
+    np.testing.assert_allclose(t[0], np.concatenate([x, rx]).astype(np.float32))
+    assert list(t[3]) == [0] * 20 + [1] * 5
+    assert list(t[2]) == list(np.arange(20) % 2) + [3] * 5
+    q = pickle.loads(pickle.dumps(p))
+    assert q.num_particles == 25
+    assert q.output_formats == ["vtk", "csv"]
+    t2 = q.__getstate__()
+    for a, b in zip(t, t2):
+        if isinstance(a, np.ndarray):
+            np.testing.assert_array_equal(a, b)
+        else:
+            assert list(a) == list(b)
