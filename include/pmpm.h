@@ -54,7 +54,10 @@ enum {
   PMPM_MAT_NONE = 0,            /* Material base: stress untouched            */
   PMPM_MAT_LINEAR_ELASTIC = 1,  /* src/materials/linearelastic_inline.h:40-107 */
   PMPM_MAT_NEWTON_FLUID = 2,    /* src/materials/newtonfluid_inline.h:49-96    */
-  PMPM_MAT_DRUCKER_PRAGER = 3   /* src/materials/dp_rheo_inline.h:123-246      */
+  PMPM_MAT_DRUCKER_PRAGER = 3,  /* src/materials/dp_rheo_inline.h:123-246      */
+  /* J2 plasticity with linear hardening, 3D (src/materials/vonmises_inline.h:
+   * 36-120; like Drucker-Prager, not a member of the reference's MaterialType) */
+  PMPM_MAT_VON_MISES = 4
 };
 
 /* Boundary conditions: the reference BoundaryConditionType members on this
@@ -104,7 +107,8 @@ enum {
  *   DRUCKER_PRAGER: {K, G, eta, eta_bar, kc, p_apex, has_apex, pois}
  *                   (pois = -1 for the dp_rheo form, which takes no
  *                   per-particle E / friction angle)
- *                   yield sqrt(J2) + eta p - kc (p = tr(sigma)/3) */
+ *                   yield sqrt(J2) + eta p - kc (p = tr(sigma)/3)
+ *   VON_MISES:      {K, G, yield_stress, H} */
 typedef struct {
   int type;
   float density;
@@ -183,6 +187,7 @@ typedef enum {
   PMPM_FIELD_YOUNGS_MODULUS = 14,    /* float [n]  per-particle Drucker-Prager E (no reference
                                         counterpart); first use fills it from the materials    */
   PMPM_FIELD_FRICTION_ANGLE = 15,    /* float [n]  per-particle Drucker-Prager friction angle (deg) */
+  PMPM_FIELD_ACC_EPS_P = 16,         /* float [n]  VonMises accumulated plastic strain (acc_eps_p_gpu) */
   PMPM_FIELD_NODE_MASSES = 20,       /* float [nodes]     NodesContainer::masses_gpu               */
   PMPM_FIELD_NODE_MOMENTS = 21,      /* float [nodes][dim] ::moments_gpu                           */
   PMPM_FIELD_NODE_MOMENTS_NT = 22,   /* float [nodes][dim] ::moments_nt_gpu                        */
@@ -218,6 +223,8 @@ int pmpm_material_drucker_prager(float density, float E, float pois, float frict
                                  float dilatancy_deg, float cohesion, pmpm_material *out);
 /* The reference DP_rheo parameters M (CSL slope), Pt (tensile pressure) and
  * dilatancy angle (degrees): DP_rheo::DP_rheo (src/materials/dp_rheo.cpp:45-70). */
+/* VonMises::VonMises (src/materials/vonmises.cpp:31-44): 3D only */
+int pmpm_material_von_mises(float density, float E, float pois, float yield_stress, float H, pmpm_material *out);
 int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
                           pmpm_material *out);
 

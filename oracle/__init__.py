@@ -28,7 +28,7 @@ _LIBS = {}
 LINEAR, QUADRATIC, CUBIC = 0, 1, 2
 SHAPE_FUNCTIONS = {"linear": LINEAR, "quadratic": QUADRATIC, "cubic": CUBIC}
 
-MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER = 0, 1, 2, 3
+MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER, MAT_VON_MISES = 0, 1, 2, 3, 4
 BC_GRAVITY, BC_NODEDOMAIN, BC_BODYFORCE, BC_PLANARDOMAIN = 1, 2, 3, 4
 BC_RIGIDBODY_LEVELSET, BC_RIGID_SDF = 5, 6
 RIGID_MODES = {"static": 0, "loop_rotate": 1}
@@ -85,7 +85,7 @@ def _structs(precision):
                     ("node_ids", P), ("node_types", P),
                     ("num_materials", ctypes.c_int), ("materials", P),
                     ("num_bcs", ctypes.c_int), ("bcs", P),
-                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P), ("musl", ctypes.c_int)]
+                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P), ("musl", ctypes.c_int), ("acc_eps_p", P)]
 
     return Grid, Material, BC, Sim
 
@@ -134,6 +134,12 @@ def material_params(mat: dict, precision: str = "f32"):
         p_apex = kc / eta if eta > 0 else 0.0
         return MAT_DRUCKER_PRAGER, dens, [bulk, shear, npr(eta), npr(eta_bar), npr(kc), npr(p_apex), has_apex,
                                           float(nu)]
+    if t == "VonMises":
+        E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
+        one, two, three = npr(1), npr(2), npr(3)
+        bulk = E / (three * (one - two * nu))
+        shear = E / (two * (one + nu))
+        return MAT_VON_MISES, dens, [bulk, shear, npr(mat["yield_stress"]), npr(mat.get("H", 0.0)), 0, 0, 0, 0]
     if t == "DP_rheo":
         # the reference's DP_rheo parameters (src/materials/dp_rheo.cpp:45-70)
         E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
@@ -219,6 +225,7 @@ class OracleSim:
         a["node_types"] = np.zeros((nn, 3), np.int32)
         a["eps_e"] = z(n, d, d)
         a["stress_ref"] = z(n, 3, 3)
+        a["acc_eps_p"] = z(n)
         if youngs_modulus is not None:
             a["youngs"] = np.array(youngs_modulus, npr, copy=True).reshape(n)
             a["friction"] = np.array(friction_angle, npr, copy=True).reshape(n)

@@ -1110,6 +1110,54 @@ static void dp_particle_params(const REAL *mp, REAL E, REAL phi_deg, REAL *out) 
   out[7] = (REAL)nu;
 }
 
+/* update_vonmises (src/materials/vonmises_inline.h:36-120), 3D: trial
+ * elastic strain eps + sym(L) dt, p = K tr, s = 2G dev, q = sqrt(3/2 s:s);
+ * Phi = q - (sigma_y + H acc); Newton on dgamma in double until |Phi| <= 1e-7
+ * (acc from the iterate before the last update); s *= 1 - 3G dgamma / q;
+ * eps = s / 2G + tr/3 I. */
+static void vm_point(const real *L, real *sig, real *eps, real *acc, real dt, const or_material *m) {
+  real K = m->p[0], G = m->p[1], sy0 = m->p[2], H = m->p[3];
+  real et[9];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++)
+      et[3 * a + b] = (real)(eps[3 * a + b] + (real)((real)((real)0.5 * (real)(L[3 * a + b] + L[3 * b + a])) * dt));
+  real ev = (real)((real)(et[0] + et[4]) + et[8]);
+  real p = (real)(K * ev);
+  real sv[9], ss = 0;
+  for (int k = 0; k < 9; k++) {
+    real e = et[k];
+    if (k == 0 || k == 4 || k == 8) e = (real)(e - (real)((real)(1.0 / 3.0) * ev));
+    sv[k] = (real)((real)(2.0 * G) * e);
+    ss = (real)(ss + (real)(sv[k] * sv[k]));
+  }
+  real sy = (real)(sy0 + (real)(H * *acc));
+  real q = (real)sqrt((double)(real)(1.5 * ss));
+  real Phi = (real)(q - sy);
+  if (Phi <= 0) {
+    for (int k = 0; k < 9; k++) {
+      sig[k] = (real)(sv[k] + ((k == 0 || k == 4 || k == 8) ? p : (real)0));
+      eps[k] = et[k];
+    }
+    return;
+  }
+  double dgamma = 0.0, acc_eps = *acc;
+  for (int it = 0; it < 100; it++) {
+    acc_eps = (double)*acc + dgamma;
+    double syi = (double)sy0 + (double)H * acc_eps;
+    double phi = (double)q - 3.0 * (double)G * dgamma - syi;
+    dgamma = dgamma - phi / (-3.0 * (double)G - (double)H);
+    if (!(fabs(phi) > 1e-7)) break;
+  }
+  double fac = 1.0 - (3.0 * (double)G * dgamma) / (double)q;
+  for (int k = 0; k < 9; k++) {
+    real sc = (real)(fac * (double)sv[k]);
+    int diag = k == 0 || k == 4 || k == 8;
+    sig[k] = (real)(sc + (diag ? p : (real)0));
+    eps[k] = (real)((double)sc / (2.0 * (double)G) + (diag ? (1.0 / 3.0) * (double)ev : 0.0));
+  }
+  *acc = (real)acc_eps;
+}
+
 void or_stress_update(or_sim *s) {
   int d = s->grid.dim;
   for (int mid = 0; mid < s->num_materials; mid++) {
@@ -1132,6 +1180,8 @@ void or_stress_update(or_sim *s) {
           prm = pp;
         }
         or_dp_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->dt, prm, 0);
+      } else if (m->type == OR_MAT_VON_MISES && d == 3) {
+        vm_point(L, sig, s->eps_e + (size_t)i * 9, s->acc_eps_p + i, s->dt, m);
       }
     }
   }

@@ -37,7 +37,8 @@ enum {
   OR_MAT_NONE = 0,          /* Material base class: stress untouched      */
   OR_MAT_LINEAR_ELASTIC = 1,
   OR_MAT_NEWTON_FLUID = 2,
-  OR_MAT_DRUCKER_PRAGER = 3
+  OR_MAT_DRUCKER_PRAGER = 3,
+  OR_MAT_VON_MISES = 4       /* p = {K, G, yield_stress, H}; 3D only */
 };
 
 /* Boundary-condition ids. */
@@ -140,6 +141,9 @@ typedef struct {
 
   /* 1: MUSL step (second momentum mapping, velocity gradient from it) */
   int musl;
+
+  /* VonMises accumulated plastic strain [n] (elastic strain in eps_e) */
+  REAL *acc_eps_p;
 } or_sim;
 
 void or_grid_init(or_grid *g, int dim, const REAL *origin, const REAL *end, REAL cell_size);

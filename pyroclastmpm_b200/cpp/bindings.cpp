@@ -237,6 +237,18 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def_readwrite("density", &DruckerPrager::density)
       .def("calculate_timestep", &DruckerPrager::calculate_timestep, py::arg("cell_size"), py::arg("factor"));
 
+  py::class_<VonMises>(m, "VonMises", py::dynamic_attr())
+      .def(py::init<float, float, float, float, float>(), py::arg("density"), py::arg("E"), py::arg("pois"),
+           py::arg("yield_stress"), py::arg("H"))
+      .def_readwrite("density", &VonMises::density)
+      .def_readonly("E", &VonMises::E)
+      .def_readonly("pois", &VonMises::pois)
+      .def_readonly("yield_stress", &VonMises::yield_stress)
+      .def_readonly("H", &VonMises::H)
+      .def_readonly("bulk_modulus", &VonMises::bulk_modulus)
+      .def_readonly("shear_modulus", &VonMises::shear_modulus)
+      .def("calculate_timestep", &VonMises::calculate_timestep, py::arg("cell_size"), py::arg("factor"));
+
   py::class_<BoundaryCondition>(m, "BoundaryCondition").def(py::init<>());
   py::class_<Gravity>(m, "Gravity", py::dynamic_attr())
       .def(py::init([](py::object g, bool is_ramp, int ramp_step, py::object ge) {

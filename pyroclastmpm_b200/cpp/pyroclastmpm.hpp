@@ -402,7 +402,27 @@ struct DruckerPrager {
     return dt;
   }
 };
-using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager>;
+// VonMises (src/materials/vonmises.cpp:31-44), 3D only
+struct VonMises {
+  VonMises(Real density, Real E, Real pois, Real yield_stress, Real H)
+      : density(density), E(E), pois(pois), yield_stress(yield_stress), H(H) {
+    bulk_modulus = E / (3.0f * (1.0f - 2.0f * pois));
+    shear_modulus = E / (2.0f * (1.0f + pois));
+  }
+  Real density, E, pois, yield_stress, H, bulk_modulus, shear_modulus;
+  pmpm_material desc() const {
+    pmpm_material m;
+    check(pmpm_material_von_mises(density, E, pois, yield_stress, H, &m), "VonMises");
+    return m;
+  }
+  // VonMises::calculate_timestep (src/materials/vonmises.cpp:96-104)
+  Real calculate_timestep(Real cell_size, Real factor) const {
+    Real dt;
+    check(pmpm_calculate_timestep(cell_size, factor, bulk_modulus, shear_modulus, density, &dt), "calculate_timestep");
+    return dt;
+  }
+};
+using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager, VonMises>;
 
 struct BoundaryCondition {
   bool isActive = true;

@@ -128,6 +128,7 @@ struct pmpm_sim {
     bool held = false;
   } ro;
   bool has_planar = false, has_dp = false, has_sref = false;
+  bool has_vm = false;  // a VonMises material: elastic strain and accumulated plastic strain
 
   // particles (two storage sets, swapped by the physical re-sort)
   int n = 0, stride = 0;
@@ -195,6 +196,7 @@ void free_particles(pmpm_sim *s) {
     dfree(P.hash);
     dfree(P.pE);
     dfree(P.pphi);
+    dfree(P.acc);
     P = DevParticles{};
   }
   dfree(s->slot);
@@ -223,6 +225,7 @@ int alloc_particle_set(pmpm_sim *s, DevParticles &P) {
     PMPM_TRY(dalloc(&P.eps, (size_t)E * st));
     PMPM_TRY(dalloc(&P.sref, (size_t)S * st));
   }
+  if (s->has_vm) PMPM_TRY(dalloc(&P.acc, (size_t)st));
   PMPM_TRY(dalloc(&P.color, (size_t)st));
   PMPM_TRY(dalloc(&P.active, (size_t)st));
   PMPM_TRY(dalloc(&P.rigid, (size_t)st));
@@ -662,6 +665,7 @@ int field_info(const pmpm_sim *s, int field, size_t *bytes) {
     case PMPM_FIELD_VOLUMES_ORIGINAL:
     case PMPM_FIELD_YOUNGS_MODULUS:
     case PMPM_FIELD_FRICTION_ANGLE:
+    case PMPM_FIELD_ACC_EPS_P:
     case PMPM_FIELD_HASH_UNSORTED:
     case PMPM_FIELD_HASH_SORTED:
     case PMPM_FIELD_SORTED_INDEX:
@@ -844,6 +848,18 @@ int pmpm_material_drucker_prager(float density, float E, float pois, float frict
   return PMPM_OK;
 }
 
+int pmpm_material_von_mises(float density, float E, float pois, float yield_stress, float H, pmpm_material *out) {
+  if (!out) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_MAT_VON_MISES;
+  out->density = density;
+  out->params[0] = E / (3.0f * (1.0f - 2.0f * pois));
+  out->params[1] = E / (2.0f * (1.0f + pois));
+  out->params[2] = yield_stress;
+  out->params[3] = H;
+  return PMPM_OK;
+}
+
 int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
                           pmpm_material *out) {
   if (!out) return PMPM_ERR_INVALID_ARGUMENT;
@@ -1023,11 +1039,17 @@ static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
   // materials
   for (int k = 0; k < desc->num_materials; k++) {
     const pmpm_material &m = desc->materials[k];
-    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_DRUCKER_PRAGER) return PMPM_ERR_INVALID_ARGUMENT;
+    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_VON_MISES) return PMPM_ERR_INVALID_ARGUMENT;
+    if (m.type == PMPM_MAT_VON_MISES) {
+      if (desc->dim != 3) return PMPM_ERR_NOT_SUPPORTED;  // the reference's VonMises is 3D only
+      s->has_vm = true;
+      s->has_dp = true;  // elastic-strain history arrays
+    }
     DevMaterial dm;
+    memset(&dm, 0, sizeof(dm));
     dm.type = m.type;
     dm.density = m.density;
-    memcpy(dm.p, m.params, sizeof(dm.p));
+    memcpy(dm.p, m.params, sizeof(m.params));
     if (m.type == PMPM_MAT_NEWTON_FLUID) dm.p[3] = (float)(2.0 * (double)m.params[0] / 3.0);
     if (m.type == PMPM_MAT_DRUCKER_PRAGER) {
       s->has_dp = true;
@@ -1284,6 +1306,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   if (P.fext) PMPM_CUDA(cudaMemset(P.fext, 0, sizeof(float) * D * st));
   if (P.eps) PMPM_CUDA(cudaMemset(P.eps, 0, sizeof(float) * E * st));
   if (P.sref) PMPM_CUDA(cudaMemset(P.sref, 0, sizeof(float) * S * st));
+  if (P.acc) PMPM_CUDA(cudaMemset(P.acc, 0, sizeof(float) * st));
   PMPM_CUDA(cudaMemcpy(P.color, color.data(), st, cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemcpy(P.rigid, rigid.data(), st, cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemcpy(P.active, active.data(), st, cudaMemcpyHostToDevice));
@@ -1442,6 +1465,14 @@ int pmpm_get_field(pmpm_sim *s, int field, void *dst, size_t bytes, int on_devic
     case PMPM_FIELD_MASSES: kind = 4; src = P.m; break;
     case PMPM_FIELD_VOLUMES: kind = 4; src = P.V; break;
     case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; src = P.V0; break;
+    case PMPM_FIELD_ACC_EPS_P:
+      if (!P.acc) {
+        PMPM_CUDA(cudaMemsetAsync(s->staging, 0, need, s->stream));
+        return copy_out(s, s->staging, dst, need, on_device);
+      }
+      kind = 4;
+      src = P.acc;
+      break;
     case PMPM_FIELD_YOUNGS_MODULUS:
     case PMPM_FIELD_FRICTION_ANGLE:
       PMPM_TRY(ensure_particle_params(s));
@@ -1488,6 +1519,7 @@ int pmpm_set_field(pmpm_sim *s, int field, const void *src, size_t bytes, int on
     case PMPM_FIELD_MASSES: kind = 4; dstp = P.m; break;
     case PMPM_FIELD_VOLUMES: kind = 4; dstp = P.V; break;
     case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; dstp = P.V0; break;
+    case PMPM_FIELD_ACC_EPS_P: kind = 4; dstp = P.acc; break;
     case PMPM_FIELD_YOUNGS_MODULUS:
     case PMPM_FIELD_FRICTION_ANGLE:
       PMPM_TRY(ensure_particle_params(s));
@@ -1724,7 +1756,8 @@ int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float d
   DevMaterial dm;
   dm.type = mat->type;
   dm.density = mat->density;
-  memcpy(dm.p, mat->params, sizeof(dm.p));
+  memset(dm.p, 0, sizeof(dm.p));
+  memcpy(dm.p, mat->params, sizeof(mat->params));
   if (mat->type == PMPM_MAT_NEWTON_FLUID) dm.p[3] = (float)(2.0 * (double)mat->params[0] / 3.0);
   const size_t dd = (size_t)dim * dim;
   std::vector<void *> bufs;
@@ -2085,7 +2118,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
       st = PMPM_ERR_INVALID_ARGUMENT;  // one kernel instantiation serves the batch
       break;
     }
-    if (h->rbls_index >= 0 || (h->flags & PMPM_FLAG_MUSL)) {
+    if (h->rbls_index >= 0 || (h->flags & PMPM_FLAG_MUSL) || h->has_vm) {
       st = PMPM_ERR_NOT_SUPPORTED;
       break;
     }

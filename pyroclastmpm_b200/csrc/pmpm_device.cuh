@@ -58,6 +58,7 @@ struct DevParticles {
   int stride;
   float *x, *v, *F, *sig, *L, *m, *V, *V0, *fext, *eps, *sref;
   float *pE, *pphi;  // per-particle Young's modulus and friction angle (deg) of Drucker-Prager, or null
+  float *acc;        // VonMises accumulated plastic strain, or null
   uint8_t *color, *active, *rigid;
   int *id;             // original particle id of each storage slot
   unsigned int *hash;  // reference cell hash of the last partition
@@ -523,6 +524,59 @@ __device__ __forceinline__ void dp_particle_params(const DevMaterial &mt, float 
   prm[5] = eta > 0.0f ? prm[4] / eta : 0.0f;
   prm[6] = eta > 0.0f ? 1.0f : 0.0f;
   prm[7] = nu;
+}
+
+// update_vonmises (src/materials/vonmises_inline.h:36-120), 3D: elastic
+// strain eps (3x3, updated), accumulated plastic strain acc (updated), stress
+// S (written).  deps = sym(L) dt; trial p = K tr(eps_tr), s = 2G dev(eps_tr);
+// Phi = sqrt(3/2 s:s) - (sigma_y + H acc); the reference's Newton iteration
+// on dgamma (in double, |Phi| <= 1e-7) with acc taken before the last update.
+__device__ __forceinline__ void vm_update(const float *prm, const float *L, float dt, float eps[9], float &acc,
+                                          float S[9]) {
+  const float K = prm[0], G = prm[1], sy0 = prm[2], H = prm[3];
+  float eps_tr[9];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) eps_tr[3 * a + b] = eps[3 * a + b] + (0.5f * (L[3 * a + b] + L[3 * b + a])) * (float)dt;
+  const float ev = (eps_tr[0] + eps_tr[4]) + eps_tr[8];
+  const float p = K * ev;
+  float s[9], ss = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    float e = eps_tr[k];
+    if (k == 0 || k == 4 || k == 8) e -= (1.0f / 3.0f) * ev;
+    s[k] = 2.0f * G * e;
+    ss += s[k] * s[k];
+  }
+  const float sy = sy0 + H * acc;
+  const float q = sqrtf(1.5f * ss);
+  const float Phi = q - sy;
+  if (Phi <= 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      S[k] = s[k] + ((k == 0 || k == 4 || k == 8) ? p : 0.0f);
+      eps[k] = eps_tr[k];
+    }
+    return;
+  }
+  double dgamma = 0.0, acc_eps = acc;
+  for (int it = 0; it < 100; it++) {
+    acc_eps = (double)acc + dgamma;
+    const double syi = (double)sy0 + (double)H * acc_eps;
+    const double phi = (double)q - 3.0 * (double)G * dgamma - syi;
+    dgamma = dgamma - phi / (-3.0 * (double)G - (double)H);
+    if (!(fabs(phi) > 1e-7)) break;
+  }
+  const double fac = 1.0 - (3.0 * (double)G * dgamma) / (double)q;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const float sc = (float)(fac * (double)s[k]);
+    const bool diag = k == 0 || k == 4 || k == 8;
+    S[k] = sc + (diag ? p : 0.0f);
+    eps[k] = (float)((double)sc / (2.0 * (double)G) + (diag ? (1.0 / 3.0) * (double)ev : 0.0));
+  }
+  acc = (float)acc_eps;
 }
 
 // --------------------------------------------------------------------------

@@ -418,6 +418,7 @@ __global__ void __launch_bounds__(256) k_reorder(StepArgs a, DevParticles dst, i
     move_comps(S.pE, dst.pE, 1, st, s, k);
     move_comps(S.pphi, dst.pphi, 1, st, s, k);
   }
+  if (S.acc) move_comps(S.acc, dst.acc, 1, st, s, k);
   move_comps(S.hash, dst.hash, 1, st, s, k);
   a.B.order[k] = k;  // storage is now in cell order
 }
@@ -1614,6 +1615,20 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
     le_update<D>(mt, L, a.dt, S);
   } else if (mt.type == PMPM_MAT_NEWTON_FLUID) {
     nf_update<D>(mt, L, P.m[s], P.V[s], P.V0[s], S);
+  } else if (mt.type == PMPM_MAT_VON_MISES) {
+    if (D != 3) return;  // 3D only (rejected at create)
+    float eps[9];
+#pragma unroll
+    for (int x = 0; x < 3; x++)
+#pragma unroll
+      for (int y = 0; y < 3; y++) eps[3 * x + y] = P.eps[eps_index<3>(x, y) * st + s];
+    float acc = P.acc[s];
+    vm_update(mt.p, L, a.dt, eps, acc, S);
+#pragma unroll
+    for (int x = 0; x < 3; x++)
+#pragma unroll
+      for (int y = x; y < 3; y++) P.eps[eps_index<3>(x, y) * st + s] = eps[3 * x + y];
+    P.acc[s] = acc;
   } else {
     float eps[9], sref[9];
 #pragma unroll

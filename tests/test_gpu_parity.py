@@ -317,6 +317,13 @@ def scoop_scene(dim, shape_function, shape="half_cylinder_shell", friction=0.3, 
 
 
 STEP_CASES.update({
+    "random_3d_quadratic_vm": lambda: random_scene(
+        3, 4000, "quadratic", 13, margin=0.0, cell=0.1,
+        mats=[{"type": "VonMises", "density": 1000.0, "E": 1e5, "pois": 0.3, "yield_stress": 200.0, "H": 1e3},
+              {"type": "VonMises", "density": 2000.0, "E": 3e5, "pois": 0.25, "yield_stress": 50.0, "H": 0.0}],
+        bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]},
+             {"type": "NodeDomain", "face0_mode": [1, 1, 1], "face1_mode": [1, 1, 1]}]) | {
+        "colors": np.random.default_rng(13).integers(0, 2, 4000)},
     "rigid_nn_2d_static": lambda: rigid_block_scene(2),
     "rigid_nn_2d_rotate": lambda: rigid_block_scene(2, "loop_rotate", [2.0, 0.0]),
     "rigid_nn_3d_static": lambda: rigid_block_scene(3),
@@ -348,7 +355,8 @@ def test_one_step_matches_oracle(case):
 
 
 @pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "water_2d_quadratic_nf",
-                                  "sdf_3d_quadratic_shell", "sdf_2d_quadratic_shell", "rigid_nn_2d_rotate"])
+                                  "sdf_3d_quadratic_shell", "sdf_2d_quadratic_shell", "rigid_nn_2d_rotate",
+                                  "random_3d_quadratic_vm"])
 def test_multi_step_drift_vs_fp64(case):
     """20 steps: FP32 GPU against the FP64 oracle (drift bound 1e-4)."""
     scene = STEP_CASES[case]()
@@ -532,3 +540,19 @@ def test_musl_stages_equal_solve():
         check(lib().pmpm_musl_stage(b.handle, stage), "musl stage")
     for name in ("positions", "velocities", "stresses", "F"):
         np.testing.assert_array_equal(a.get(name), b.get(name))
+
+
+def test_von_mises_history_matches_oracle():
+    """The VonMises history (elastic strain, accumulated plastic strain)
+    against the oracle after 5 steps; some particles must have yielded."""
+    scene = STEP_CASES["random_3d_quadratic_vm"]()
+    sim, ref = make_pair(scene)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(5)
+    ref.solve(5)
+    acc = sim.get("acc_eps_p")
+    assert (ref["acc_eps_p"] > 0).sum() > 100
+    tol = cond_tol(scene, 5, ("eps_e", "acc_eps_p"), 1e-4)
+    assert rel(sim.get("eps_e"), ref["eps_e"]) <= tol["eps_e"]
+    assert rel(acc, ref["acc_eps_p"]) <= tol["acc_eps_p"]
