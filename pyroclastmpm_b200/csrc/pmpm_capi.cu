@@ -378,10 +378,18 @@ int launch_partition(pmpm_sim *s) {
   PMPM_LAUNCHED();
   k_scatter<<<blocks_for(s->n), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
-  k_sort_cells<<<blocks_for(s->nkeys), kTPB, 0, st>>>(a);
-  PMPM_LAUNCHED();
-  k_sort_big<<<148, 1024, 0, st>>>(a);
-  PMPM_LAUNCHED();
+  // ids in order inside each bin: needed by the deterministic gather and by
+  // the nearest-rigid-particle search (the reference's first minimum); the
+  // other P2G paths accumulate in any order, and the reference partition
+  // views are built from the stored hashes
+  if ((s->flags & PMPM_FLAG_DETERMINISTIC) || s->rbls_index >= 0) {
+    k_sort_cells<<<blocks_for(s->nkeys), kTPB, 0, st>>>(a);
+    PMPM_LAUNCHED();
+    k_sort_big<<<148, 1024, 0, st>>>(a);
+    PMPM_LAUNCHED();
+  } else {
+    s->launches -= 2;
+  }
   s->partitioned = true;
   return PMPM_OK;
 }
@@ -733,13 +741,12 @@ int copy_out(pmpm_sim *s, const void *dev_src, void *dst, size_t bytes, int on_d
 // >= num_cells_total) by (hash, id), as a stable sort of all hashes gives.
 int sorted_views(pmpm_sim *s, std::vector<int> &sorted_index, std::vector<unsigned> &hash_sorted) {
   const int n = s->n;
-  std::vector<int> order(n), id(n);
+  std::vector<int> id(n);
   std::vector<unsigned> hash(n);
-  int nb = 0;
   const DevParticles &P = s->P[s->cur];
-  if (s->dual) {
-    // the step bins by dual cell; the reference permutation is the stable
-    // sort of the stored reference hashes
+  {
+    // the reference permutation is the stable sort of the stored reference
+    // hashes (the step's own bins may be dual cells, in any order inside)
     PMPM_CUDA(cudaMemcpyAsync(id.data(), P.id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
     PMPM_CUDA(cudaMemcpyAsync(hash.data(), P.hash, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s->stream));
     PMPM_CUDA(cudaStreamSynchronize(s->stream));
@@ -752,24 +759,6 @@ int sorted_views(pmpm_sim *s, std::vector<int> &sorted_index, std::vector<unsign
                      [&](int x, int y) { return by_id[x] < by_id[y]; });
     for (int k = 0; k < n; k++) hash_sorted[k] = by_id[sorted_index[k]];
     return PMPM_OK;
-  }
-  PMPM_CUDA(cudaMemcpyAsync(order.data(), s->B.order, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
-  PMPM_CUDA(cudaMemcpyAsync(id.data(), P.id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
-  PMPM_CUDA(cudaMemcpyAsync(hash.data(), P.hash, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, s->stream));
-  PMPM_CUDA(cudaMemcpyAsync(&nb, s->B.scalars, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-  PMPM_CUDA(cudaStreamSynchronize(s->stream));
-  sorted_index.resize(n);
-  hash_sorted.resize(n);
-  for (int k = 0; k < n; k++) {
-    sorted_index[k] = id[order[k]];
-    hash_sorted[k] = hash[order[k]];
-  }
-  std::vector<std::pair<unsigned, int>> tail;
-  for (int k = nb; k < n; k++) tail.emplace_back(hash_sorted[k], sorted_index[k]);
-  std::sort(tail.begin(), tail.end());
-  for (int k = nb; k < n; k++) {
-    hash_sorted[k] = tail[k - nb].first;
-    sorted_index[k] = tail[k - nb].second;
   }
   return PMPM_OK;
 }
@@ -1651,7 +1640,7 @@ int profile_step(pmpm_sim *s, float *ms, int *launches) {
   int n_launch = 0;
   PMPM_CUDA(cudaEventRecord(ev[0], s->stream));
   PMPM_TRY((launch_partition<D, SF>(s)));
-  n_launch += 7;
+  n_launch += ((s->flags & PMPM_FLAG_DETERMINISTIC) || s->rbls_index >= 0) ? 7 : 5;
   if (!s->ro.held && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
     PMPM_TRY(launch_reorder<D>(s));
     n_launch += 1;
@@ -1985,11 +1974,14 @@ int batch_partition(pmpm_batch *b) {
   PMPM_LAUNCHED();
   k_scatter<<<blocks_for(b->n), kTPB, 0, st>>>(ga);
   PMPM_LAUNCHED();
-  k_sort_cells<<<blocks_for(b->nkeys), kTPB, 0, st>>>(ga);
-  PMPM_LAUNCHED();
-  k_sort_big<<<148, 1024, 0, st>>>(ga);
-  PMPM_LAUNCHED();
-  b->launches += 7;
+  b->launches += 5;
+  if (b->flags & PMPM_FLAG_DETERMINISTIC) {  // ids in order inside each bin for the gather
+    k_sort_cells<<<blocks_for(b->nkeys), kTPB, 0, st>>>(ga);
+    PMPM_LAUNCHED();
+    k_sort_big<<<148, 1024, 0, st>>>(ga);
+    PMPM_LAUNCHED();
+    b->launches += 2;
+  }
   return PMPM_OK;
 }
 

@@ -153,45 +153,67 @@ __device__ __forceinline__ void planar_force(const StepArgs &a, int s, const flo
 // chosen with the same comparison as the G2P window (frac < 1/2 -> b - 1).
 __device__ __forceinline__ int dual_coord(float u, int b) { return (u - (float)(b - 1)) < 1.5f ? b : b + 1; }
 
+// Called by every lane of a warp (valid = the lane has a particle): lanes
+// of the warp that share a key add to its count with one atomic (particles
+// stored in cell order after a re-sort mostly share keys with neighbours).
+__device__ __forceinline__ int warp_bin_slot(int *count, unsigned key, bool add) {
+  const unsigned kk = add ? key : 0xffffffffu;
+  const unsigned peers = __match_any_sync(0xffffffffu, kk);
+  int slot = -1;
+  if (add) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&count[key], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    slot = base + __popc(peers & ((1u << lane) - 1u));
+  }
+  return slot;
+}
+
 template <int D, int SF>
-__device__ __forceinline__ void hash_count_body(const StepArgs &a, int s) {
+__device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool valid) {
   const DevGrid &g = a.g;
   float x[3] = {0.0f, 0.0f, 0.0f}, u[3] = {0.0f, 0.0f, 0.0f};
   int b[3] = {0, 0, 0};
   bool in_axes = true;
+  bool binned = false, sorted = false;
+  unsigned key = 0;
+  if (valid) {
 #pragma unroll
-  for (int c = 0; c < D; c++) {
-    x[c] = a.P.x[c * a.P.stride + s];
-    u[c] = scaled_coord(x[c], g.origin[c], g.inv_h);
-    b[c] = (int)u[c];
-    in_axes = in_axes && b[c] >= 0 && b[c] < g.n[c];
-  }
-  const unsigned hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
-  a.P.hash[s] = hu;
-  bool binned;
-  unsigned key;
-  if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual) {
-    int d[3] = {0, 0, 0};
+    for (int c = 0; c < D; c++) {
+      x[c] = a.P.x[c * a.P.stride + s];
+      u[c] = scaled_coord(x[c], g.origin[c], g.inv_h);
+      b[c] = (int)u[c];
+      in_axes = in_axes && b[c] >= 0 && b[c] < g.n[c];
+    }
+    const unsigned hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
+    a.P.hash[s] = hu;
+    if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual) {
+      int d[3] = {0, 0, 0};
 #pragma unroll
-    for (int c = 0; c < D; c++) d[c] = dual_coord(u[c], b[c]);
-    key = (unsigned)(d[0] + d[1] * a.B.kd[0] + d[2] * a.B.kd[0] * a.B.kd[1]);
-    binned = in_axes;
-    if (in_axes) mark_tiles_dual<D>(a, d);
-  } else {
-    key = hu;
-    binned = hu < (unsigned)g.ntotal;
-    mark_tiles<D, SF>(a, b, hu, binned, in_axes);
+      for (int c = 0; c < D; c++) d[c] = dual_coord(u[c], b[c]);
+      key = (unsigned)(d[0] + d[1] * a.B.kd[0] + d[2] * a.B.kd[0] * a.B.kd[1]);
+      binned = in_axes;
+      if (in_axes) mark_tiles_dual<D>(a, d);
+    } else {
+      key = hu;
+      binned = hu < (unsigned)g.ntotal;
+      mark_tiles<D, SF>(a, b, hu, binned, in_axes);
+    }
+    // with a sentinel key (batched ensembles) a particle outside the grid is
+    // sorted into its instance's extra last key, so instances keep their
+    // storage ranges; it is reported as a fault either way
+    sorted = binned;
+    if (!binned && a.B.sentinel) {
+      key = (unsigned)g.ntotal;
+      sorted = true;
+    }
   }
-  // with a sentinel key (batched ensembles) a particle outside the grid is
-  // sorted into its instance's extra last key, so instances keep their
-  // storage ranges; it is reported as a fault either way
-  bool sorted = binned;
-  if (!binned && a.B.sentinel) {
-    key = (unsigned)g.ntotal;
-    sorted = true;
-  }
+  const int slot = warp_bin_slot(a.B.count, key, sorted);
+  if (!valid) return;
   a.P.key[s] = (unsigned)a.B.key_base + key;
-  a.P.slot[s] = sorted ? atomicAdd(&a.B.count[key], 1) : -1;
+  a.P.slot[s] = slot;
   if (!binned || (SF == PMPM_SHAPE_QUADRATIC && !in_axes)) atomicOr(a.fault, kFaultOutOfDomain);
   if (a.has_planar) planar_force<D>(a, s, x);
 }
@@ -199,7 +221,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s) {
 template <int D, int SF>
 __global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < a.P.n) hash_count_body<D, SF>(a, s);
+  hash_count_body<D, SF>(a, s, s < a.P.n);
 }
 
 constexpr int kScanThreads = 1024;
@@ -1337,7 +1359,8 @@ struct Dual3 {
   static constexpr int NS = T::X + 2;   // dual sources per axis
   static constexpr int MAXPAIR = NS * 3;
   static constexpr int NCELL = NS * NS;
-  static constexpr int CAP = 1024;
+  static constexpr int NL = T::Z + 2;   // dual layers a tile reads
+  static constexpr int CAP = 960;
   static constexpr int SLOTS = CAP + NCELL;
   static constexpr int NT = 320;        // threads (10 warps)
   static constexpr int IPT = 2;         // items per thread per round
@@ -1399,7 +1422,8 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
   __shared__ int npair[2];
-  __shared__ int cell_k0[W::NCELL], cell_pref[W::NCELL + 1];
+  // every layer's source cells: first sorted position and running prefix
+  __shared__ int cell_k0[W::NL * W::NCELL], cell_pref[W::NL * W::NCELL + 1];
   __shared__ int warp_tmp[33];
   extern __shared__ __align__(16) float dyn_smem[];
   constexpr int SL = W::SLOTS;
@@ -1432,6 +1456,41 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
   const int kd0 = a.B.kd[0];
   const long long kd01 = (long long)a.B.kd[0] * a.B.kd[1];
 
+  // ---- all layers' dual source cells -> sorted ranges, one prefix ----
+  const int ntab = (dz_hi - dz_lo + 1) * W::NCELL;
+  {
+    constexpr int PER = (W::NL * W::NCELL + NT - 1) / NT;
+    int cnt[PER];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int idx = tid * PER + k;
+      cnt[k] = 0;
+      if (idx < ntab) {
+        const int layer = idx / W::NCELL, vc = idx % W::NCELL;
+        const int sx = t0[0] - 1 + vc % W::NS, sy = t0[1] - 1 + vc / W::NS;
+        int k0 = 0;
+        if (sx >= 0 && sx <= g.n[0] && sy >= 0 && sy <= g.n[1]) {
+          const long long f = sx + (long long)sy * kd0 + (long long)(dz_lo + layer) * kd01;
+          k0 = a.B.offset[f];
+          cnt[k] = a.B.offset[f + 1] - k0;
+        }
+        cell_k0[idx] = k0;
+        sum += cnt[k];
+      }
+    }
+    int total;
+    int ex = block_exclusive_scan(sum, warp_tmp, total);
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int idx = tid * PER + k;
+      if (idx < ntab) cell_pref[idx] = ex;
+      ex += cnt[k];
+    }
+    if (tid == 0) cell_pref[ntab] = total;
+  }
+  __syncthreads();
+
   for (int round = 0; round < nrounds; round++) {
     int item_cell[W::IPT], item_tl[W::IPT];
     float item_xn[W::IPT], item_yn[W::IPT];  // virtual target node coordinates
@@ -1453,36 +1512,20 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
         for (int c = 0; c < 7; c++) win[q][k][c] = 0.0f;
     }
     for (int dz = dz_lo; dz <= dz_hi; dz++) {
-      // ---- the layer's dual source cells -> sorted ranges, prefix ----
-      {
-        const int vc = tid;
-        int cnt = 0, k0 = 0;
-        if (vc < W::NCELL) {
-          const int sx = t0[0] - 1 + vc % W::NS, sy = t0[1] - 1 + vc / W::NS;
-          if (sx >= 0 && sx <= g.n[0] && sy >= 0 && sy <= g.n[1]) {
-            const long long f = sx + (long long)sy * kd0 + (long long)dz * kd01;
-            k0 = a.B.offset[f];
-            cnt = a.B.offset[f + 1] - k0;
-          }
-          cell_k0[vc] = k0;
-        }
-        int total;
-        const int ex = block_exclusive_scan(cnt, warp_tmp, total);
-        if (vc < W::NCELL) cell_pref[vc] = ex;
-        if (tid == 0) cell_pref[W::NCELL] = total;
-      }
-      __syncthreads();
-      const int layer_n = cell_pref[W::NCELL];
+      const int *pref = cell_pref + (dz - dz_lo) * W::NCELL;
+      const int *k0s = cell_k0 + (dz - dz_lo) * W::NCELL;
+      const int base = pref[0];
+      const int layer_n = pref[W::NCELL] - base;
       for (int c0 = 0; c0 < layer_n; c0 += W::CAP) {
         const int c1 = min(c0 + W::CAP, layer_n);
-        // ---- stage particles [c0, c1) ----
+        // ---- stage particles [c0, c1) of the layer ----
         for (int j = c0 + tid; j < c1; j += NT) {
           int lo = 0, hi = W::NCELL;
           while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (cell_pref[mid] <= j) lo = mid; else hi = mid;
+            if (pref[mid] - base <= j) lo = mid; else hi = mid;
           }
-          const int s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+          const int s = a.B.order[k0s[lo] + (j - (pref[lo] - base))];
           const int jj = j - c0 + lo;  // skewed slot: neighbouring cells start in different banks
           const float ux = scaled_coord(P.x[s], g.origin[0], g.inv_h);
           const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
@@ -1513,7 +1556,7 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
         for (int q = 0; q < W::IPT; q++) {
           if (!item_ok[q]) continue;
           const int vc = item_cell[q];
-          const int j0 = max(cell_pref[vc], c0) - c0 + vc, j1 = min(cell_pref[vc + 1], c1) - c0 + vc;
+          const int j0 = max(pref[vc] - base, c0) - c0 + vc, j1 = min(pref[vc + 1] - base, c1) - c0 + vc;
           const float xn = item_xn[q], yn = item_yn[q];
           for (int j = j0; j < j1; j++) {
             float Nx, dNx, Ny, dNy;
@@ -1564,7 +1607,6 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
           win[q][2][c] = 0.0f;
         }
       }
-      __syncthreads();  // cell tables are rebuilt for the next layer
     }
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
@@ -1968,7 +2010,7 @@ __global__ void __launch_bounds__(256) kb_hash_count(const StepArgs *views, cons
   const BatchBlock b = blocks[blockIdx.x];
   load_view(sa, views, b.inst, P, epoch);
   const int s = b.first + (int)threadIdx.x;
-  if (s < b.end) hash_count_body<D, SF>(sa, s);
+  hash_count_body<D, SF>(sa, s, s < b.end);
 }
 
 template <int D, int SF>
