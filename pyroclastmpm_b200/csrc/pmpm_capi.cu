@@ -144,6 +144,8 @@ struct pmpm_sim {
   bool dual = false;  // quadratic 3D fast path bins by dual cell
   int kd[3] = {1, 1, 1};
   int nkeys = 0;
+  int nbricks = 0;     // dual-cell bricks (cell-scatter P2G)
+  int p2g_variant = 0; // 3D quadratic: 0 cell scatter, 1 dual sweep
   int *key = nullptr;  // binning key scratch
   int *fault = nullptr;
   // staging for field conversion
@@ -424,7 +426,20 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
       PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
       attr_set[dev] = true;
     }
-    k_p2g_dual3<<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+    if (s->p2g_variant == 1) {
+      k_p2g_dual3<<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+    } else {
+      constexpr int cbytes = cells3_smem_bytes();
+      static bool cattr_set[64] = {false};  // per device
+      if (!cattr_set[dev]) {
+        PMPM_CUDA(cudaFuncSetAttribute(k_p2g_cells3, cudaFuncAttributeMaxDynamicSharedMemorySize, cbytes));
+        cattr_set[dev] = true;
+      }
+      k_p2g_cells3<<<s->nbricks, Cells3::NT, cbytes, s->stream>>>(a);
+      PMPM_LAUNCHED();
+      k_node_epilogue<3><<<s->g.ntiles, TileDims<3>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
+      s->launches += 1;
+    }
   } else if (D == 3) {
     constexpr int bytes = sweep3_smem_bytes<SF>();
     static bool attr_set[64] = {false};  // per device
@@ -1172,6 +1187,18 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK) st = dalloc(&s->B.block_sums, (size_t)s->nscan_blocks);
   if (st == PMPM_OK) st = dalloc(&s->B.scalars, 4);
   if (st == PMPM_OK) st = dalloc(&s->B.big_cells, nk);
+  if (st == PMPM_OK && s->dual) {
+    s->nbricks = 1;
+    for (int c = 0; c < 3; c++) {
+      s->B.kb[c] = (s->kd[c] + Cells3::B - 1) / Cells3::B;
+      s->nbricks *= s->B.kb[c];
+    }
+    st = dalloc(&s->B.brick_epoch, (size_t)s->nbricks);
+    if (st == PMPM_OK) st = dalloc(&s->N.acc, 8 * nn);
+    if (st == PMPM_OK && (cudaMemset(s->B.brick_epoch, 0xff, sizeof(int) * s->nbricks) != cudaSuccess ||
+                          cudaMemset(s->N.acc, 0, sizeof(float) * 8 * nn) != cudaSuccess))
+      st = PMPM_ERR_CUDA;
+  }
   if (st == PMPM_OK) st = dalloc(&s->fault, 1);
   if (st == PMPM_OK) {
     if (cudaMemset(s->B.count, 0, nk * sizeof(int)) != cudaSuccess ||
@@ -1206,6 +1233,8 @@ int pmpm_destroy(pmpm_sim *s) {
   dfree(s->B.block_sums);
   dfree(s->B.scalars);
   dfree(s->B.big_cells);
+  dfree(s->B.brick_epoch);
+  dfree(s->N.acc);
   dfree(s->fault);
   for (float *p : s->bc_values) dfree(p);
   for (uint8_t *p : s->bc_masks) dfree(p);
@@ -1648,8 +1677,9 @@ int profile_step(pmpm_sim *s, float *ms, int *launches) {
     s->steps_since_sort += 1;
   }
   PMPM_CUDA(cudaEventRecord(ev[1], s->stream));
+  const long long lp0 = s->launches;
   PMPM_TRY((launch_p2g<D, SF>(s, 1)));
-  n_launch += s->rbls_index >= 0 ? 3 : 1;
+  n_launch += (int)(s->launches - lp0);
   PMPM_CUDA(cudaEventRecord(ev[2], s->stream));
   const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
   if (s->flags & PMPM_FLAG_MUSL) {

@@ -72,6 +72,8 @@ struct DevNodes {
   // 3D: vx vy vz - | vntx vnty vntz -  (two float4), 2D: vx vy vntx vnty
   float *vel;
   int *tile_epoch;  // tile active in the partition whose epoch it holds
+  // cell-scatter P2G: per node [m, p0 p1 p2, f0 f1 f2, -], zero outside P2G
+  float *acc;
 };
 
 template <int D>
@@ -88,6 +90,8 @@ struct DevBins {
   int kd[3];
   int nkeys;
   int key_base;     // added to the stored particle keys (an instance's first key in a batch)
+  int kb[3];        // dual-cell bricks per axis (8^3 dual cells each)
+  int *brick_epoch; // brick holds particles in the partition whose epoch it holds (or null)
   int sentinel;     // particles outside the grid take key ntotal (batched ensembles)
   int *count;       // per key, zero between steps
   int *offset;      // exclusive prefix, nkeys + 1 entries

@@ -195,7 +195,13 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
       for (int c = 0; c < D; c++) d[c] = dual_coord(u[c], b[c]);
       key = (unsigned)(d[0] + d[1] * a.B.kd[0] + d[2] * a.B.kd[0] * a.B.kd[1]);
       binned = in_axes;
-      if (in_axes) mark_tiles_dual<D>(a, d);
+      if (in_axes) {
+        mark_tiles_dual<D>(a, d);
+        if (a.B.brick_epoch) {
+          const int bi = d[0] / 8 + (d[1] / 8) * a.B.kb[0] + (d[2] / 8) * a.B.kb[0] * a.B.kb[1];
+          if (a.B.brick_epoch[bi] != a.epoch) a.B.brick_epoch[bi] = a.epoch;
+        }
+      }
     } else {
       key = hu;
       binned = hu < (unsigned)g.ntotal;
@@ -1625,6 +1631,160 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
   }
   __syncthreads();
   tile_epilogue3(a, apply_bcs, t0, acc, tid, NT);
+}
+
+// --------------------------------------------------------------------------
+// P2G, 3D quadratic: warp per dual cell, scatter into brick boxes
+// --------------------------------------------------------------------------
+//
+// All particles of dual cell d reach the same 27 nodes d-1 .. d+1 (clamped
+// onto the grid).  One CTA per brick of 8^3 dual cells that holds particles;
+// each warp takes cells of the brick in turn, stages up to 32 of the cell's
+// particles (per-axis weights and derivatives, m, m v, -V sigma, f_ext) in
+// its own shared-memory area, and lane (i, j, k) < 27 sums the cell's
+// contributions to node d - 1 + (i, j, k) in registers (the staged values
+// are read as broadcasts).  The 27 sums go into the brick's shared 10^3-node
+// box, which is added once per node to the global accumulators; the node
+// epilogue (k_node_epilogue) finishes the nodes and clears the accumulators.
+// No block barrier inside the cell loop.
+struct Cells3 {
+  static constexpr int NW = 8;      // warps per CTA
+  static constexpr int NT = NW * 32;
+  static constexpr int B = 8;       // brick edge (dual cells)
+  static constexpr int BOX = B + 2; // node box edge
+  static constexpr int NBOX = BOX * BOX * BOX;
+  static constexpr int NF = 31;     // staged floats per particle
+};
+
+constexpr int cells3_smem_bytes() { return (7 * Cells3::NBOX + Cells3::NW * Cells3::NF * 32) * 4; }
+
+__global__ void __launch_bounds__(Cells3::NT, 3) k_p2g_cells3(StepArgs a) {
+  using W = Cells3;
+  const DevGrid &g = a.g;
+  const int brick = blockIdx.x;
+  if (a.B.brick_epoch[brick] != a.epoch) return;
+  extern __shared__ __align__(16) float csm[];
+  float *box = csm;                          // [7][NBOX]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float(*stg)[32] = (float(*)[32])(box + 7 * W::NBOX + warp * W::NF * 32);  // [NF][32]
+  for (int k = threadIdx.x; k < 7 * W::NBOX; k += W::NT) box[k] = 0.0f;
+  const int kb0 = a.B.kb[0], kb1 = a.B.kb[1];
+  const int b0[3] = {(brick % kb0) * W::B, ((brick / kb0) % kb1) * W::B, (brick / (kb0 * kb1)) * W::B};
+  __syncthreads();
+  const DevParticles &P = a.P;
+  const int st = P.stride;
+  const int kd0 = a.B.kd[0];
+  const long long kd01 = (long long)a.B.kd[0] * a.B.kd[1];
+  const int li = lane % 3, lj = (lane / 3) % 3, lk = lane / 9;
+  for (int cl = warp; cl < W::B * W::B * W::B; cl += W::NW) {
+    const int d[3] = {b0[0] + cl % W::B, b0[1] + (cl / W::B) % W::B, b0[2] + cl / (W::B * W::B)};
+    if (d[0] >= a.B.kd[0] || d[1] >= a.B.kd[1] || d[2] >= a.B.kd[2]) continue;
+    const long long key = d[0] + (long long)d[1] * kd0 + (long long)d[2] * kd01;
+    const int k0 = a.B.offset[key], cnt = a.B.offset[key + 1] - k0;
+    if (cnt == 0) continue;
+    float acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int p0 = 0; p0 < cnt; p0 += 32) {
+      const int m = min(32, cnt - p0);
+      if (lane < m) {
+        const int s = a.B.order[k0 + p0 + lane];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float u = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+#pragma unroll
+          for (int i = 0; i < 3; i++) {
+            float N, dN;
+            axis_weight<PMPM_SHAPE_QUADRATIC>(u - (float)(d[c] - 1 + i), g.inv_h, 0, N, dN);
+            stg[c * 3 + i][lane] = N;
+            stg[9 + c * 3 + i][lane] = dN;
+          }
+        }
+        const float pm = P.m[s];
+        stg[18][lane] = pm;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          stg[19 + c][lane] = pm * P.v[c * st + s];
+          stg[22 + c][lane] = (a.has_planar && !a.remap) ? P.fext[c * st + s] : 0.0f;
+        }
+        const float nv = a.remap ? 0.0f : -P.V[s];
+#pragma unroll
+        for (int k = 0; k < 6; k++) stg[25 + k][lane] = nv * P.sig[k * st + s];
+      }
+      __syncwarp();
+      if (lane < 27) {
+        for (int q = 0; q < m; q++) {
+          const float nx = stg[li][q], ny = stg[3 + lj][q], nz = stg[6 + lk][q];
+          const float dx = stg[9 + li][q], dy = stg[12 + lj][q], dz = stg[15 + lk][q];
+          const float w = nx * ny * nz;
+          const float gx = dx * ny * nz, gy = nx * dy * nz, gz = nx * ny * dz;
+          acc[0] += stg[18][q] * w;
+          acc[1] += stg[19][q] * w;
+          acc[2] += stg[20][q] * w;
+          acc[3] += stg[21][q] * w;
+          const float Sxx = stg[25][q], Syy = stg[26][q], Szz = stg[27][q];
+          const float Sxy = stg[28][q], Sxz = stg[29][q], Syz = stg[30][q];
+          acc[4] += stg[22][q] * w + Sxx * gx + Sxy * gy + Sxz * gz;
+          acc[5] += stg[23][q] * w + Sxy * gx + Syy * gy + Syz * gz;
+          acc[6] += stg[24][q] * w + Sxz * gx + Syz * gy + Szz * gz;
+        }
+      }
+      __syncwarp();
+    }
+    if (lane < 27) {
+      const int nx = min(max(d[0] - 1 + li, 0), g.n[0] - 1) - (b0[0] - 1);
+      const int ny = min(max(d[1] - 1 + lj, 0), g.n[1] - 1) - (b0[1] - 1);
+      const int nz = min(max(d[2] - 1 + lk, 0), g.n[2] - 1) - (b0[2] - 1);
+      const int bl = nx + W::BOX * (ny + W::BOX * nz);
+#pragma unroll
+      for (int c = 0; c < 7; c++) atomicAdd(&box[c * W::NBOX + bl], acc[c]);
+    }
+  }
+  __syncthreads();
+  for (int bl = threadIdx.x; bl < W::NBOX; bl += W::NT) {
+    const float m = box[bl];
+    if (m == 0.0f) continue;
+    const int x = b0[0] - 1 + bl % W::BOX, y = b0[1] - 1 + (bl / W::BOX) % W::BOX,
+              z = b0[2] - 1 + bl / (W::BOX * W::BOX);
+    if (x < 0 || y < 0 || z < 0 || x >= g.n[0] || y >= g.n[1] || z >= g.n[2]) continue;
+    float *dst = a.N.acc + 8 * (size_t)flat_index(g, x, y, z);
+#pragma unroll
+    for (int c = 0; c < 7; c++) atomicAdd(dst + c, box[c * W::NBOX + bl]);
+  }
+}
+
+// Node epilogue of the scatter P2G, one thread per node of the active tiles:
+// p_nt = p + f dt for m above the cutoff (the reference leaves lighter nodes
+// at 0), the node conditions, v = p/m; the accumulators are cleared.
+template <int D>
+__global__ void __launch_bounds__(TileDims<D>::N) k_node_epilogue(StepArgs a, int apply_bcs, int *node_epoch) {
+  using T = TileDims<D>;
+  const DevGrid &g = a.g;
+  const int tile = blockIdx.x;
+  if (a.N.tile_epoch[tile] != a.epoch) return;
+  if (threadIdx.x == 0) node_epoch[tile] = a.epoch;
+  const int tx = tile % g.tdim[0], ty = (tile / g.tdim[0]) % g.tdim[1], tz = tile / (g.tdim[0] * g.tdim[1]);
+  const int lx = threadIdx.x % T::X, ly = (threadIdx.x / T::X) % T::Y, lz = threadIdx.x / (T::X * T::Y);
+  const int nc[3] = {tx * T::X + lx, ty * T::Y + ly, D == 3 ? tz * T::Z + lz : 0};
+  if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) return;
+  const int node = flat_index(g, nc[0], nc[1], nc[2]);
+  float4 *ac = reinterpret_cast<float4 *>(a.N.acc + 8 * (size_t)node);
+  const float4 q0 = ac[0], q1 = ac[1];
+  ac[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  ac[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float mass = q0.x;
+  const float mom[3] = {q0.y, q0.z, q0.w}, force[3] = {q1.x, q1.y, q1.z};
+  float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+  const bool live = mass > a.cutoff;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      p[c] = mom[c];
+      pnt[c] = mom[c] + force[c] * a.dt;
+    }
+  } else {
+    mass = 0.0f;
+  }
+  if (apply_bcs) node_bcs<D>(a, node, nc, mass, p, pnt);
+  write_node<D>(a, node, mass, p, pnt, live);
 }
 
 // --------------------------------------------------------------------------
