@@ -1634,19 +1634,21 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
 }
 
 // --------------------------------------------------------------------------
-// P2G, 3D quadratic: warp per dual cell, scatter into brick boxes
+// P2G, 3D quadratic: warp per row of dual cells, scatter into brick boxes
 // --------------------------------------------------------------------------
 //
 // All particles of dual cell d reach the same 27 nodes d-1 .. d+1 (clamped
-// onto the grid).  One CTA per brick of 8^3 dual cells that holds particles;
-// each warp takes cells of the brick in turn, stages up to 32 of the cell's
-// particles (per-axis weights and derivatives, m, m v, -V sigma, f_ext) in
-// its own shared-memory area, and lane (i, j, k) < 27 sums the cell's
-// contributions to node d - 1 + (i, j, k) in registers (the staged values
-// are read as broadcasts).  The 27 sums go into the brick's shared 10^3-node
-// box, which is added once per node to the global accumulators; the node
-// epilogue (k_node_epilogue) finishes the nodes and clears the accumulators.
-// No block barrier inside the cell loop.
+// onto the grid).  One CTA per brick of 8^3 dual cells that holds particles.
+// A warp takes a row of 8 cells along x (consecutive keys, so the row's
+// particles are one contiguous sorted range), stages them in its own
+// shared-memory area (per-axis weights and derivatives, m, m v, -V sigma,
+// f_ext; up to 64 at a time), then sums three cells at a time: lane
+// (cell, i, j) adds the cell's particles to the three nodes
+// d - 1 + (i, j, 0..2) in registers, reading the staged values as
+// near-broadcasts.  The sums go into the brick's shared 10^3-node box, which
+// is added once per node to the global accumulators; the node epilogue
+// (k_node_epilogue) finishes the nodes and clears the accumulators.  No
+// block barrier inside the row loop.
 struct Cells3 {
   static constexpr int NW = 8;      // warps per CTA
   static constexpr int NT = NW * 32;
@@ -1654,19 +1656,20 @@ struct Cells3 {
   static constexpr int BOX = B + 2; // node box edge
   static constexpr int NBOX = BOX * BOX * BOX;
   static constexpr int NF = 31;     // staged floats per particle
+  static constexpr int CAPW = 64;   // staged particles per warp
 };
 
-constexpr int cells3_smem_bytes() { return (7 * Cells3::NBOX + Cells3::NW * Cells3::NF * 32) * 4; }
+constexpr int cells3_smem_bytes() { return (7 * Cells3::NBOX + Cells3::NW * Cells3::NF * Cells3::CAPW) * 4; }
 
-__global__ void __launch_bounds__(Cells3::NT, 3) k_p2g_cells3(StepArgs a) {
+__global__ void __launch_bounds__(Cells3::NT, 2) k_p2g_cells3(StepArgs a) {
   using W = Cells3;
   const DevGrid &g = a.g;
   const int brick = blockIdx.x;
   if (a.B.brick_epoch[brick] != a.epoch) return;
   extern __shared__ __align__(16) float csm[];
-  float *box = csm;                          // [7][NBOX]
+  float *box = csm;  // [7][NBOX]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float(*stg)[32] = (float(*)[32])(box + 7 * W::NBOX + warp * W::NF * 32);  // [NF][32]
+  float(*stg)[W::CAPW] = (float(*)[W::CAPW])(box + 7 * W::NBOX + warp * W::NF * W::CAPW);  // [NF][CAPW]
   for (int k = threadIdx.x; k < 7 * W::NBOX; k += W::NT) box[k] = 0.0f;
   const int kb0 = a.B.kb[0], kb1 = a.B.kb[1];
   const int b0[3] = {(brick % kb0) * W::B, ((brick / kb0) % kb1) * W::B, (brick / (kb0 * kb1)) * W::B};
@@ -1675,67 +1678,98 @@ __global__ void __launch_bounds__(Cells3::NT, 3) k_p2g_cells3(StepArgs a) {
   const int st = P.stride;
   const int kd0 = a.B.kd[0];
   const long long kd01 = (long long)a.B.kd[0] * a.B.kd[1];
-  const int li = lane % 3, lj = (lane / 3) % 3, lk = lane / 9;
-  for (int cl = warp; cl < W::B * W::B * W::B; cl += W::NW) {
-    const int d[3] = {b0[0] + cl % W::B, b0[1] + (cl / W::B) % W::B, b0[2] + cl / (W::B * W::B)};
-    if (d[0] >= a.B.kd[0] || d[1] >= a.B.kd[1] || d[2] >= a.B.kd[2]) continue;
-    const long long key = d[0] + (long long)d[1] * kd0 + (long long)d[2] * kd01;
-    const int k0 = a.B.offset[key], cnt = a.B.offset[key + 1] - k0;
-    if (cnt == 0) continue;
-    float acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int p0 = 0; p0 < cnt; p0 += 32) {
-      const int m = min(32, cnt - p0);
-      if (lane < m) {
-        const int s = a.B.order[k0 + p0 + lane];
+  const int ncx = min(W::B, kd0 - b0[0]);  // cells of the brick along x
+  const int lc = lane / 9, lij = lane % 9, li = lij % 3, lj = lij / 3;
+  const bool has_f = a.has_planar && !a.remap;
+  for (int row = warp; row < W::B * W::B; row += W::NW) {
+    const int dy = b0[1] + row % W::B, dz = b0[2] + row / W::B;
+    if (dy >= a.B.kd[1] || dz >= a.B.kd[2]) continue;
+    const long long key0 = b0[0] + (long long)dy * kd0 + (long long)dz * kd01;
+    const int offv = lane <= ncx ? a.B.offset[key0 + lane] : 0;  // lane c: start of cell c
+    const int rs = __shfl_sync(0xffffffffu, offv, 0), re = __shfl_sync(0xffffffffu, offv, ncx);
+    if (rs == re) continue;
+    for (int c0 = rs; c0 < re; c0 += W::CAPW) {
+      const int c1 = min(c0 + W::CAPW, re);
+      // ---- stage the chunk's particles ----
+      for (int j = lane; j < c1 - c0; j += 32) {
+        const int s = a.B.order[c0 + j];
+        float u[3];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          const float u = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+        for (int c = 0; c < 3; c++) u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+        const int dxc = dual_coord(u[0], (int)u[0]);
+        const int dd[3] = {dxc, dy, dz};
+#pragma unroll
+        for (int c = 0; c < 3; c++)
 #pragma unroll
           for (int i = 0; i < 3; i++) {
             float N, dN;
-            axis_weight<PMPM_SHAPE_QUADRATIC>(u - (float)(d[c] - 1 + i), g.inv_h, 0, N, dN);
-            stg[c * 3 + i][lane] = N;
-            stg[9 + c * 3 + i][lane] = dN;
+            axis_weight<PMPM_SHAPE_QUADRATIC>(u[c] - (float)(dd[c] - 1 + i), g.inv_h, 0, N, dN);
+            stg[c * 3 + i][j] = N;
+            stg[9 + c * 3 + i][j] = dN;
           }
-        }
         const float pm = P.m[s];
-        stg[18][lane] = pm;
+        stg[18][j] = pm;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          stg[19 + c][lane] = pm * P.v[c * st + s];
-          stg[22 + c][lane] = (a.has_planar && !a.remap) ? P.fext[c * st + s] : 0.0f;
+          stg[19 + c][j] = pm * P.v[c * st + s];
+          stg[22 + c][j] = has_f ? P.fext[c * st + s] : 0.0f;
         }
         const float nv = a.remap ? 0.0f : -P.V[s];
 #pragma unroll
-        for (int k = 0; k < 6; k++) stg[25 + k][lane] = nv * P.sig[k * st + s];
+        for (int k = 0; k < 6; k++) stg[25 + k][j] = nv * P.sig[k * st + s];
       }
       __syncwarp();
-      if (lane < 27) {
-        for (int q = 0; q < m; q++) {
-          const float nx = stg[li][q], ny = stg[3 + lj][q], nz = stg[6 + lk][q];
-          const float dx = stg[9 + li][q], dy = stg[12 + lj][q], dz = stg[15 + lk][q];
-          const float w = nx * ny * nz;
-          const float gx = dx * ny * nz, gy = nx * dy * nz, gz = nx * ny * dz;
-          acc[0] += stg[18][q] * w;
-          acc[1] += stg[19][q] * w;
-          acc[2] += stg[20][q] * w;
-          acc[3] += stg[21][q] * w;
+      // ---- three cells at a time: lane (cell, i, j) sums nodes (i, j, 0..2) ----
+      for (int pass = 0; pass < ncx; pass += 3) {
+        const int cell = pass + lc;
+        const int cs_ = __shfl_sync(0xffffffffu, offv, min(cell, ncx));
+        const int ce_ = __shfl_sync(0xffffffffu, offv, min(cell + 1, ncx));
+        if (lane >= 27 || cell >= ncx) continue;
+        const int q0 = max(cs_, c0) - c0, q1 = min(ce_, c1) - c0;
+        if (q0 >= q1) continue;
+        float acc[3][7];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+          for (int c = 0; c < 7; c++) acc[k][c] = 0.0f;
+        for (int q = q0; q < q1; q++) {
+          const float nx = stg[li][q], ny = stg[3 + lj][q];
+          const float dnx = stg[9 + li][q], dny = stg[12 + lj][q];
+          const float nn = nx * ny, gx = dnx * ny, gy = nx * dny;
           const float Sxx = stg[25][q], Syy = stg[26][q], Szz = stg[27][q];
           const float Sxy = stg[28][q], Sxz = stg[29][q], Syz = stg[30][q];
-          acc[4] += stg[22][q] * w + Sxx * gx + Sxy * gy + Sxz * gz;
-          acc[5] += stg[23][q] * w + Sxy * gx + Syy * gy + Syz * gz;
-          acc[6] += stg[24][q] * w + Sxz * gx + Syz * gy + Szz * gz;
+          float Ax = Sxx * gx + Sxy * gy, Ay = Sxy * gx + Syy * gy, Az = Sxz * gx + Syz * gy;
+          if (has_f) {
+            Ax += stg[22][q] * nn;
+            Ay += stg[23][q] * nn;
+            Az += stg[24][q] * nn;
+          }
+          const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
+          const float mn = stg[18][q] * nn, mvx = stg[19][q] * nn, mvy = stg[20][q] * nn, mvz = stg[21][q] * nn;
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const float Nz = stg[6 + k][q], dNz = stg[15 + k][q];
+            acc[k][0] += mn * Nz;
+            acc[k][1] += mvx * Nz;
+            acc[k][2] += mvy * Nz;
+            acc[k][3] += mvz * Nz;
+            acc[k][4] += Ax * Nz + Bx * dNz;
+            acc[k][5] += Ay * Nz + By * dNz;
+            acc[k][6] += Az * Nz + Bz * dNz;
+          }
+        }
+        const int d0 = b0[0] + cell;
+        const int nx = min(max(d0 - 1 + li, 0), g.n[0] - 1) - (b0[0] - 1);
+        const int ny = min(max(dy - 1 + lj, 0), g.n[1] - 1) - (b0[1] - 1);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const int nz = min(max(dz - 1 + k, 0), g.n[2] - 1) - (b0[2] - 1);
+          const int bl = nx + W::BOX * (ny + W::BOX * nz);
+#pragma unroll
+          for (int c = 0; c < 7; c++) atomicAdd(&box[c * W::NBOX + bl], acc[k][c]);
         }
       }
       __syncwarp();
-    }
-    if (lane < 27) {
-      const int nx = min(max(d[0] - 1 + li, 0), g.n[0] - 1) - (b0[0] - 1);
-      const int ny = min(max(d[1] - 1 + lj, 0), g.n[1] - 1) - (b0[1] - 1);
-      const int nz = min(max(d[2] - 1 + lk, 0), g.n[2] - 1) - (b0[2] - 1);
-      const int bl = nx + W::BOX * (ny + W::BOX * nz);
-#pragma unroll
-      for (int c = 0; c < 7; c++) atomicAdd(&box[c * W::NBOX + bl], acc[c]);
     }
   }
   __syncthreads();
