@@ -499,6 +499,7 @@ def main():
     sim = Simulation(**kw, device=local, resort_interval=args.resort_interval)
     sim.set_particles(scene["positions"], scene["velocities"])
     sim.initialize()
+    p2g_variant = sim.autotune(3)  # the P2G kernel this configuration runs fastest with
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream, device=local)
 
@@ -622,6 +623,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, numpy PCG64)",
             "config": {"workload": workload_name(args.config), "particles_per_gpu": n, "grid_nodes": sim.num_nodes,
                        "active_nodes": active, "resort_interval": args.resort_interval,
+                       "p2g_kernel": {1: "dual-cell z-sweep", 0: "cell-row scatter"}.get(p2g_variant, "tile"),
                        "l2": "state larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",

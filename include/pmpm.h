@@ -402,6 +402,13 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
                            const float *positions, int num_particles, unsigned *hash_unsorted,
                            int *sorted_index, int *cell_start, int *cell_end, void *stream);
 
+/* Autotuner (no reference counterpart): where a configuration has more than
+ * one P2G kernel (3D quadratic: dual-cell z-sweep per node tile, or a warp
+ * per row of dual cells scattering into brick boxes), time each on `steps`
+ * steps from the current state, keep the fastest for this handle and put
+ * the state (and step counter) back.  *chosen: 1 sweep, 0 cell scatter. */
+int pmpm_autotune(pmpm_sim *s, int steps, int *chosen);
+
 /* ---------------------------------------------------------------------------
  * Differentiable rollouts (no counterpart in the reference).  A rollout of
  * nsteps USL steps from the current state keeps the particle state every

@@ -85,7 +85,7 @@ EXPORTS = [
     "pmpm_profile_step", "pmpm_active_nodes", "pmpm_launch_count", "pmpm_partition_noalloc",
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
-    "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises",
+    "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
 ]
 
 EXPORTS += [
@@ -128,6 +128,7 @@ def lib():
     L.pmpm_rollout_forward.argtypes = [vp, i, i]
     L.pmpm_rollout_set_memory.argtypes = [vp, ctypes.c_longlong]
     L.pmpm_musl_stage.argtypes = [vp, i]
+    L.pmpm_autotune.argtypes = [vp, i, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_material_von_mises.argtypes = [f, f, f, f, f, ctypes.POINTER(Material)]
     L.pmpm_material_point_vjp.argtypes = [ctypes.POINTER(Material), i, i, f] + [vp] * 11 + [i, i]
     L.pmpm_rollout_reset.argtypes = [vp]
@@ -505,6 +506,13 @@ class Simulation:
     def launch_count(self):
         c = ctypes.c_longlong()
         check(lib().pmpm_launch_count(self._h, ctypes.byref(c)), "pmpm_launch_count")
+        return c.value
+
+    def autotune(self, steps=5):
+        """Time each P2G kernel this configuration has on `steps` steps, keep
+        the fastest, restore the state; returns the chosen variant."""
+        c = ctypes.c_int()
+        check(lib().pmpm_autotune(self._h, int(steps), ctypes.byref(c)), "pmpm_autotune")
         return c.value
 
     # ---- differentiable rollouts ----

@@ -145,7 +145,8 @@ struct pmpm_sim {
   int kd[3] = {1, 1, 1};
   int nkeys = 0;
   int nbricks = 0;     // dual-cell bricks (cell-scatter P2G)
-  int p2g_variant = 0; // 3D quadratic: 0 cell scatter, 1 dual sweep
+  int p2g_variant = 1; // 3D quadratic: 0 cell scatter, 1 dual sweep (pmpm_autotune picks)
+  bool tuning = false; // no physical re-sort while the autotuner times variants
   int *key = nullptr;  // binning key scratch
   int *fault = nullptr;
   // staging for field conversion
@@ -493,7 +494,7 @@ int musl_tail(pmpm_sim *s, int store_L) {
 template <int D, int SF>
 int step_once(pmpm_sim *s) {
   PMPM_TRY((launch_partition<D, SF>(s)));
-  if (!s->ro.held && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
+  if (!s->ro.held && !s->tuning && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
     PMPM_TRY(launch_reorder<D>(s));
   } else {
     s->steps_since_sort += 1;
@@ -1670,7 +1671,7 @@ int profile_step(pmpm_sim *s, float *ms, int *launches) {
   PMPM_CUDA(cudaEventRecord(ev[0], s->stream));
   PMPM_TRY((launch_partition<D, SF>(s)));
   n_launch += ((s->flags & PMPM_FLAG_DETERMINISTIC) || s->rbls_index >= 0) ? 7 : 5;
-  if (!s->ro.held && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
+  if (!s->ro.held && !s->tuning && s->resort_interval > 0 && s->steps_since_sort + 1 >= s->resort_interval) {
     PMPM_TRY(launch_reorder<D>(s));
     n_launch += 1;
   } else {
@@ -2775,5 +2776,66 @@ extern "C" int pmpm_material_point_vjp(const pmpm_material *mat, int dim, int n,
     st = PMPM_ERR_CUDA;
   for (void *p : bufs) cudaFree(p);
   for (float *p : tmp.bc_values) cudaFree(p);
+  return st;
+}
+
+extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
+  if (!s || steps < 1) return PMPM_ERR_INVALID_ARGUMENT;
+  if (s->n == 0) return PMPM_ERR_STATE;
+  PMPM_CUDA(cudaSetDevice(s->device));
+  std::vector<int> cands;
+  if (s->dual) cands = {1, 0};
+  if (cands.size() < 2) {
+    if (chosen) *chosen = s->p2g_variant;
+    return PMPM_OK;
+  }
+  // time each variant on the same state: save, step, restore (no re-sort meanwhile)
+  const size_t per = (size_t)state_floats(s) * s->stride;
+  const size_t extra = (size_t)(s->dim * s->dim + 1) * s->stride;  // L and the VonMises history
+  float *saved = nullptr;
+  if (cudaMalloc(&saved, (per + extra) * sizeof(float)) != cudaSuccess) return PMPM_ERR_OUT_OF_MEMORY;
+  const int step0 = s->step;
+  auto copy_extra = [&](bool save) -> int {
+    const DevParticles &P = s->P[s->cur];
+    const size_t nL = (size_t)s->dim * s->dim * s->stride;
+    float *bL = saved + per, *bA = saved + per + nL;
+    const cudaMemcpyKind kd = cudaMemcpyDeviceToDevice;
+    if (P.L) PMPM_CUDA(cudaMemcpyAsync(save ? bL : P.L, save ? P.L : bL, nL * 4, kd, s->stream));
+    if (P.acc) PMPM_CUDA(cudaMemcpyAsync(save ? bA : P.acc, save ? P.acc : bA, (size_t)s->stride * 4, kd, s->stream));
+    return PMPM_OK;
+  };
+  int st = copy_state(s, saved, true);
+  if (st == PMPM_OK) st = copy_extra(true);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_v = s->p2g_variant;
+  s->tuning = true;
+  for (size_t k = 0; k < cands.size() && st == PMPM_OK; k++) {
+    s->p2g_variant = cands[k];
+    st = PMPM_DISPATCH(s, step_once, s);  // warm-up (and first-launch set-up) of the variant
+    if (st != PMPM_OK) break;
+    cudaEventRecord(e0, s->stream);
+    for (int i = 0; i < steps && st == PMPM_OK; i++) st = PMPM_DISPATCH(s, step_once, s);
+    cudaEventRecord(e1, s->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      best_v = cands[k];
+    }
+    if (st == PMPM_OK) st = copy_state(s, saved, false);
+    if (st == PMPM_OK) st = copy_extra(false);
+    s->step = step0;
+  }
+  s->tuning = false;
+  s->p2g_variant = best_v;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s->stream);
+  cudaFree(saved);
+  if (chosen) *chosen = best_v;
   return st;
 }

@@ -556,3 +556,24 @@ def test_von_mises_history_matches_oracle():
     tol = cond_tol(scene, 5, ("eps_e", "acc_eps_p"), 1e-4)
     assert rel(sim.get("eps_e"), ref["eps_e"]) <= tol["eps_e"]
     assert rel(acc, ref["acc_eps_p"]) <= tol["acc_eps_p"]
+
+
+def test_autotune_keeps_state_and_both_variants_match_oracle():
+    """The autotuner times both 3D quadratic P2G kernels from the same state
+    and puts the state back; the simulation then matches the oracle."""
+    from pyroclastmpm_b200._capi import check, lib
+    scene = STEP_CASES["column_3d_quadratic_dp"]()
+    sim, ref = make_pair(scene)
+    sim.initialize()
+    before = {n: sim.get(n) for n in ("positions", "velocities", "stresses", "F")}
+    v = sim.autotune(3)
+    assert v in (0, 1)
+    for n, a in before.items():
+        np.testing.assert_array_equal(sim.get(n), a)
+    assert sim.step == 0
+    ref.initialize()
+    ref.solve(2)
+    sim.solve(2)
+    tol = cond_tol(scene, 2, FIELDS, STEP_TOL)
+    for name in FIELDS:
+        assert rel(sim.get(name), ref[name]) <= tol[name], name
