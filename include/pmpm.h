@@ -57,7 +57,13 @@ enum {
   PMPM_MAT_DRUCKER_PRAGER = 3,  /* src/materials/dp_rheo_inline.h:123-246      */
   /* J2 plasticity with linear hardening, 3D (src/materials/vonmises_inline.h:
    * 36-120; like Drucker-Prager, not a member of the reference's MaterialType) */
-  PMPM_MAT_VON_MISES = 4
+  PMPM_MAT_VON_MISES = 4,
+  /* Modified Cam Clay with the reference's nonlinear (pressure-dependent)
+   * elasticity: update_modifiedcamclay_nonlinear
+   * (src/materials/modifiedcamclay_inline.h:321-511), the update the reference's
+   * ModifiedCamClay::stress_update runs (src/materials/modifiedcamclay.cpp:
+   * 148-178); a member of the reference's MaterialType */
+  PMPM_MAT_MODIFIED_CAM_CLAY = 5
 };
 
 /* Boundary conditions: the reference BoundaryConditionType members on this
@@ -108,7 +114,9 @@ enum {
  *                   (pois = -1 for the dp_rheo form, which takes no
  *                   per-particle E / friction angle)
  *                   yield sqrt(J2) + eta p - kc (p = tr(sigma)/3)
- *   VON_MISES:      {K, G, yield_stress, H} */
+ *   VON_MISES:      {K, G, yield_stress, H}
+ *   MODIFIED_CAM_CLAY: {K, G, M, lam, kap, Vs, Pt, R}
+ *                   (R: preconsolidation ratio, pc = R p0 at initialize) */
 typedef struct {
   int type;
   float density;
@@ -187,7 +195,9 @@ typedef enum {
   PMPM_FIELD_YOUNGS_MODULUS = 14,    /* float [n]  per-particle Drucker-Prager E (no reference
                                         counterpart); first use fills it from the materials    */
   PMPM_FIELD_FRICTION_ANGLE = 15,    /* float [n]  per-particle Drucker-Prager friction angle (deg) */
-  PMPM_FIELD_ACC_EPS_P = 16,         /* float [n]  VonMises accumulated plastic strain (acc_eps_p_gpu) */
+  PMPM_FIELD_ACC_EPS_P = 16,         /* float [n]  VonMises accumulated plastic strain (acc_eps_p_gpu);
+                                        Modified Cam Clay volumetric plastic strain (alpha_gpu) */
+  PMPM_FIELD_PRECONSOLIDATION = 17,  /* float [n]  Modified Cam Clay preconsolidation pressure (pc_gpu) */
   PMPM_FIELD_NODE_MASSES = 20,       /* float [nodes]     NodesContainer::masses_gpu               */
   PMPM_FIELD_NODE_MOMENTS = 21,      /* float [nodes][dim] ::moments_gpu                           */
   PMPM_FIELD_NODE_MOMENTS_NT = 22,   /* float [nodes][dim] ::moments_nt_gpu                        */
@@ -223,10 +233,19 @@ int pmpm_material_drucker_prager(float density, float E, float pois, float frict
                                  float dilatancy_deg, float cohesion, pmpm_material *out);
 /* The reference DP_rheo parameters M (CSL slope), Pt (tensile pressure) and
  * dilatancy angle (degrees): DP_rheo::DP_rheo (src/materials/dp_rheo.cpp:45-70). */
-/* VonMises::VonMises (src/materials/vonmises.cpp:31-44): 3D only */
-int pmpm_material_von_mises(float density, float E, float pois, float yield_stress, float H, pmpm_material *out);
 int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
                           pmpm_material *out);
+/* VonMises::VonMises (src/materials/vonmises.cpp:31-44): 3D only */
+int pmpm_material_von_mises(float density, float E, float pois, float yield_stress, float H, pmpm_material *out);
+/* ModifiedCamClay::ModifiedCamClay (src/materials/modifiedcamclay.cpp:47-63):
+ * M slope of the critical state line, lam / kap slopes of the virgin
+ * consolidation and swelling lines, Vs solid volume (specific volume =
+ * particle volume / Vs), R preconsolidation ratio, Pt tensile yield pressure;
+ * beta is accepted and unused, as in the reference's update.  pmpm_initialize
+ * then does ModifiedCamClay::initialize (:68-108): reference stress = current
+ * stress, elastic strain and alpha = 0, pc = R p0 with p0 = -tr(sigma)/3. */
+int pmpm_material_modified_cam_clay(float density, float E, float pois, float M, float lam, float kap, float Vs,
+                                    float R, float Pt, float beta, pmpm_material *out);
 
 /* Boundary-condition helpers (reference constructors). */
 /* Gravity::Gravity (src/boundaryconditions/gravity.cpp:52-60) */

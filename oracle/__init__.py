@@ -29,6 +29,7 @@ LINEAR, QUADRATIC, CUBIC = 0, 1, 2
 SHAPE_FUNCTIONS = {"linear": LINEAR, "quadratic": QUADRATIC, "cubic": CUBIC}
 
 MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER, MAT_VON_MISES = 0, 1, 2, 3, 4
+MAT_MODIFIED_CAM_CLAY = 5
 BC_GRAVITY, BC_NODEDOMAIN, BC_BODYFORCE, BC_PLANARDOMAIN = 1, 2, 3, 4
 BC_RIGIDBODY_LEVELSET, BC_RIGID_SDF = 5, 6
 RIGID_MODES = {"static": 0, "loop_rotate": 1}
@@ -85,7 +86,8 @@ def _structs(precision):
                     ("node_ids", P), ("node_types", P),
                     ("num_materials", ctypes.c_int), ("materials", P),
                     ("num_bcs", ctypes.c_int), ("bcs", P),
-                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P), ("musl", ctypes.c_int), ("acc_eps_p", P)]
+                    ("eps_e", P), ("stress_ref", P), ("youngs", P), ("friction", P), ("musl", ctypes.c_int), ("acc_eps_p", P),
+                    ("pc", P)]
 
     return Grid, Material, BC, Sim
 
@@ -140,6 +142,14 @@ def material_params(mat: dict, precision: str = "f32"):
         bulk = E / (three * (one - two * nu))
         shear = E / (two * (one + nu))
         return MAT_VON_MISES, dens, [bulk, shear, npr(mat["yield_stress"]), npr(mat.get("H", 0.0)), 0, 0, 0, 0]
+    if t == "ModifiedCamClay":
+        # ModifiedCamClay::ModifiedCamClay (src/materials/modifiedcamclay.cpp:47-63)
+        E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
+        one, two, three = npr(1), npr(2), npr(3)
+        bulk = E / (three * (one - two * nu))
+        shear = E / (two * (one + nu))
+        return MAT_MODIFIED_CAM_CLAY, dens, [bulk, shear, npr(mat["M"]), npr(mat["lam"]), npr(mat["kap"]),
+                                             npr(mat["Vs"]), npr(mat.get("Pt", 0.0)), npr(mat["R"])]
     if t == "DP_rheo":
         # the reference's DP_rheo parameters (src/materials/dp_rheo.cpp:45-70)
         E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
@@ -226,6 +236,7 @@ class OracleSim:
         a["eps_e"] = z(n, d, d)
         a["stress_ref"] = z(n, 3, 3)
         a["acc_eps_p"] = z(n)
+        a["pc"] = z(n)
         if youngs_modulus is not None:
             a["youngs"] = np.array(youngs_modulus, npr, copy=True).reshape(n)
             a["friction"] = np.array(friction_angle, npr, copy=True).reshape(n)
@@ -341,6 +352,17 @@ class OracleSim:
         # Drucker-Prager history starts from the current stresses
         self.a["stress_ref"][:] = self.a["stresses"]
         self.a["eps_e"][:] = 0
+        # ModifiedCamClay::initialize (src/materials/modifiedcamclay.cpp:68-108):
+        # alpha = 0, pc = R p0 with p0 = -tr(sigma)/3, per particle of the colour
+        npr = self.npr
+        self.a["acc_eps_p"][:] = 0
+        for k, m in enumerate(self.materials):
+            if m["type"] != "ModifiedCamClay":
+                continue
+            sel = self.a["colors"] == k
+            tr = np.trace(self.a["stresses"][sel], axis1=1, axis2=2).astype(np.float64)
+            p0 = (-tr / 3.0).astype(npr)
+            self.a["pc"][sel] = p0 * npr(m["R"])
         return self
 
     def _creal(self, v):
@@ -362,6 +384,31 @@ class OracleSim:
 
     def __getitem__(self, k):
         return self.a[k]
+
+
+def mcc_point(dim, L, stress, eps_e, stress_ref, alpha, pc, volume, dt, mat, precision="f32"):
+    """One Modified Cam Clay update of a single material point: returns the
+    new (stress, eps_e, alpha, pc)."""
+    lib = _lib(precision)
+    creal, npr = _real(precision)
+    _, Material, _, _ = _structs(precision)
+    t, dens, p = material_params(mat, precision)
+    m = Material()
+    m.type = t
+    m.density = float(dens)
+    for j in range(8):
+        m.p[j] = float(p[j])
+    Lc = np.ascontiguousarray(np.asarray(L, npr).reshape(dim, dim))
+    sig = np.ascontiguousarray(np.asarray(stress, npr).reshape(3, 3).copy())
+    eps = np.ascontiguousarray(np.asarray(eps_e, npr).reshape(dim, dim).copy())
+    sref = np.ascontiguousarray(np.asarray(stress_ref, npr).reshape(3, 3))
+    a = np.array([alpha], npr)
+    c = np.array([pc], npr)
+    vp = ctypes.c_void_p
+    lib.or_mcc_point(dim, Lc.ctypes.data_as(vp), sig.ctypes.data_as(vp), eps.ctypes.data_as(vp),
+                     sref.ctypes.data_as(vp), a.ctypes.data_as(vp), c.ctypes.data_as(vp), creal(volume), creal(dt),
+                     ctypes.byref(m))
+    return sig, eps, a[0], c[0]
 
 
 def dp_point(dim, L, stress, eps_e, stress_ref, dt, mat, precision="f32", velgrad_is_strain_increment=False):

@@ -1158,6 +1158,134 @@ static void vm_point(const real *L, real *sig, real *eps, real *acc, real dt, co
   *acc = (real)acc_eps;
 }
 
+/* update_modifiedcamclay_nonlinear (src/materials/modifiedcamclay_inline.h:
+ * 321-511) and compute_yield_function (:57-63), pressures positive in
+ * compression, in the reference's types: real for the trial state, the
+ * volumetric increments and the yield function of the residual; double for
+ * the Newton unknowns (lambda, alpha), p, q, p_s, the hardening slope H and
+ * the 2 x 2 iteration matrix, inverted as its adjugate over the determinant.
+ * The iteration stops at |R| <= 1e-2, the bound growing tenfold per
+ * iteration after 1000 (in FP32 the residual's noise lies above 1e-2, so the
+ * bound is what stops it).  Stress, elastic strain and pc take the last
+ * evaluated iterate; alpha the updated unknowns.  V: current particle volume
+ * (specific volume V / Vs).  p = {K, G, M, lam, kap, Vs, Pt, R}. */
+static real mcc_yield(real p, real Pt, real ps, real q, real M) {
+  real a = (real)((real)(ps - p) - Pt), b = (real)(q / M);
+  return (real)((real)((real)(a * a) + (real)(b * b)) - (real)(ps * ps));
+}
+
+void or_mcc_point(int d, const REAL *L, REAL *sig, REAL *eps_e, const REAL *sref, REAL *alpha, REAL *pc, REAL V,
+                  REAL dt, const or_material *m) {
+  real K = m->p[0], G = m->p[1], M = m->p[2], lam = m->p[3], kap = m->p[4], Vs = m->p[5], Pt = m->p[6];
+  real deps[9], W[9];
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      deps[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] + L[b * d + a])) * dt);
+      W[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] - L[b * d + a])) * dt);
+    }
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real we = 0, ew = 0;
+      for (int k = 0; k < d; k++) {
+        we = (real)(we + (real)(W[a * d + k] * eps_e[k * d + b]));
+        ew = (real)(ew + (real)(eps_e[a * d + k] * W[k * d + b]));
+      }
+      deps[a * d + b] = (real)(deps[a * d + b] + (real)(-we + ew));
+    }
+  real p_ref = (real)(-(real)(1.0 / 3.0) * (real)((real)(sref[0] + sref[4]) + sref[8]));
+  real s_ref[9];
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] = (real)(s_ref[0] + p_ref);
+  s_ref[4] = (real)(s_ref[4] + p_ref);
+  s_ref[8] = (real)(s_ref[8] + p_ref);
+  real eps_tr[9], tr_prev = 0, tr_inc = 0, tr_tr = 0;
+  for (int k = 0; k < d * d; k++) eps_tr[k] = (real)(eps_e[k] + deps[k]);
+  for (int a = 0; a < d; a++) {
+    tr_prev = (real)(tr_prev + eps_e[a * d + a]);
+    tr_inc = (real)(tr_inc + deps[a * d + a]);
+    tr_tr = (real)(tr_tr + eps_tr[a * d + a]);
+  }
+  real ev_tr = -tr_tr;
+  real edev[9] = {0};
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) edev[3 * a + b] = eps_tr[a * d + b];
+  real third = (real)((1.0 / 3.0) * (double)ev_tr);
+  for (int a = 0; a < 3; a++) edev[3 * a + a] = (real)(edev[3 * a + a] + third);
+  if (d < 3) edev[8] = 0;
+  real v_spec = (real)(V / Vs);
+  real p_prev = (real)(-(double)(real)((real)(sig[0] + sig[4]) + sig[8]) / 3.0);
+  real v_kap = (real)(v_spec / kap);
+  real dev_tr = -tr_inc;
+  real p_tr = (real)((double)p_prev / (1.0 - (double)(real)(v_kap * dev_tr)));
+  real two_g = (real)(2.0 * (double)G);
+  real s_tr[9];
+  for (int k = 0; k < 9; k++) s_tr[k] = (real)(s_ref[k] + (real)(two_g * edev[k]));
+  real ss = 0;
+  for (int a = 0; a < 3; a++) {
+    real row = 0;
+    for (int k = 0; k < 3; k++) row = (real)(row + (real)(s_tr[3 * a + k] * s_tr[3 * a + k]));
+    ss = (real)(ss + row);
+  }
+  real q_tr = (real)sqrt(1.5 * (double)ss);
+  real pc_prev = *pc;
+  real ps_tr = (real)(0.5 * (double)(real)(pc_prev + Pt));
+  if (mcc_yield(p_tr, Pt, ps_tr, q_tr, M) <= (real)0.0) {
+    for (int k = 0; k < 9; k++) sig[k] = s_tr[k];
+    sig[0] = (real)(sig[0] - p_tr);
+    sig[4] = (real)(sig[4] - p_tr);
+    sig[8] = (real)(sig[8] - p_tr);
+    for (int k = 0; k < d * d; k++) eps_e[k] = eps_tr[k];
+    return;
+  }
+  real a_prev = *alpha;
+  double lamb = 0.0, a_next = (double)a_prev, tol = 1e-2, conv;
+  double p_next = 0.0, q_next = 0.0, ps_next = 0.0;
+  real s_next[9], dev_e = 0;
+  double vlt = (double)(real)(v_spec / (real)(lam - kap));
+  double MM = (double)(real)(M * M), six_g = (double)(real)(6 * G), m12g = (double)(real)(-12 * G);
+  int counter = 0;
+  do {
+    double lm = lamb, an = a_next;
+    real dpv = (real)(an - (double)a_prev);
+    dev_e = (real)(dev_tr - dpv);
+    p_next = (double)p_prev / (1.0 - (double)(real)(v_kap * dev_e));
+    q_next = (MM / (MM + six_g * lm)) * (double)q_tr;
+    ps_next = 0.5 * ((double)pc_prev * (1.0 + vlt * (double)dpv) + (double)Pt);
+    real cs = (real)(MM / (MM + 6.0 * (double)G * lm));
+    for (int k = 0; k < 9; k++) s_next[k] = (real)(cs * s_tr[k]);
+    double R0 = (double)mcc_yield((real)p_next, Pt, (real)ps_next, (real)q_next, M);
+    double R1 = an - (double)a_prev + 2.0 * lm * (ps_next - p_next - (double)Pt);
+    double omv = 1.0 - vlt * (double)dpv;
+    double H = 0.5 * vlt * ((double)pc_prev / (omv * omv));
+    double pbar = ps_next - p_next - (double)Pt;
+    double d00 = (m12g / (MM + six_g * lm)) * (q_next / (double)M) * (q_next / (double)M);
+    double d01 = (2.0 * pbar) * ((double)K + H) - 2.0 * ps_next * H;
+    double d10 = 2.0 * pbar;
+    double d11 = 1.0 + (2.0 * lm) * ((double)K + H);
+    double inv_det = 1.0 / (d00 * d11 - d01 * d10);
+    double i00 = d11 * inv_det, i01 = -d01 * inv_det, i10 = -d10 * inv_det, i11 = d00 * inv_det;
+    lamb = lm - (i00 * R0 + i01 * R1);
+    a_next = an - (i10 * R0 + i11 * R1);
+    conv = sqrt(R0 * R0 + R1 * R1);
+    if (counter > 1000) tol *= 10.0;
+    counter += 1;
+  } while (fabs(conv) > tol && counter < 1400);
+  real pn = (real)p_next;
+  for (int k = 0; k < 9; k++) sig[k] = s_next[k];
+  sig[0] = (real)(sig[0] - pn);
+  sig[4] = (real)(sig[4] - pn);
+  sig[8] = (real)(sig[8] - pn);
+  real evol = (real)((1.0 / 3.0) * (double)(real)(tr_prev + dev_e));
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real e = (real)((real)(s_next[3 * a + b] - s_ref[3 * a + b]) / two_g);
+      if (a == b) e = (real)(e - evol);
+      eps_e[a * d + b] = e;
+    }
+  *alpha = (real)a_next;
+  *pc = (real)(2.0 * ps_next - (double)Pt);
+}
+
 void or_stress_update(or_sim *s) {
   int d = s->grid.dim;
   for (int mid = 0; mid < s->num_materials; mid++) {
@@ -1182,6 +1310,9 @@ void or_stress_update(or_sim *s) {
         or_dp_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->dt, prm, 0);
       } else if (m->type == OR_MAT_VON_MISES && d == 3) {
         vm_point(L, sig, s->eps_e + (size_t)i * 9, s->acc_eps_p + i, s->dt, m);
+      } else if (m->type == OR_MAT_MODIFIED_CAM_CLAY) {
+        or_mcc_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->acc_eps_p + i,
+                  s->pc + i, s->volumes[i], s->dt, m);
       }
     }
   }

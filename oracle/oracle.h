@@ -38,7 +38,8 @@ enum {
   OR_MAT_LINEAR_ELASTIC = 1,
   OR_MAT_NEWTON_FLUID = 2,
   OR_MAT_DRUCKER_PRAGER = 3,
-  OR_MAT_VON_MISES = 4       /* p = {K, G, yield_stress, H}; 3D only */
+  OR_MAT_VON_MISES = 4,      /* p = {K, G, yield_stress, H}; 3D only */
+  OR_MAT_MODIFIED_CAM_CLAY = 5 /* p = {K, G, M, lam, kap, Vs, Pt, R} */
 };
 
 /* Boundary-condition ids. */
@@ -142,8 +143,12 @@ typedef struct {
   /* 1: MUSL step (second momentum mapping, velocity gradient from it) */
   int musl;
 
-  /* VonMises accumulated plastic strain [n] (elastic strain in eps_e) */
+  /* VonMises accumulated plastic strain [n] (elastic strain in eps_e);
+   * Modified Cam Clay volumetric plastic strain alpha [n] */
   REAL *acc_eps_p;
+
+  /* Modified Cam Clay preconsolidation pressure [n] */
+  REAL *pc;
 } or_sim;
 
 void or_grid_init(or_grid *g, int dim, const REAL *origin, const REAL *end, REAL cell_size);
@@ -169,6 +174,11 @@ void or_solve(or_sim *s);
 void or_solve_nsteps(or_sim *s, int nsteps);
 void or_dp_point(int dim, const REAL *L, REAL *stress, REAL *eps_e, const REAL *stress_ref,
                  REAL dt, const REAL *p, int velgrad_is_strain_increment);
+/* One Modified Cam Clay update of a single material point (stress [3][3],
+ * elastic strain [dim][dim], reference stress [3][3], alpha, pc; V the
+ * particle's current volume). */
+void or_mcc_point(int dim, const REAL *L, REAL *stress, REAL *eps_e, const REAL *stress_ref, REAL *alpha, REAL *pc,
+                  REAL V, REAL dt, const or_material *m);
 
 #ifdef __cplusplus
 }

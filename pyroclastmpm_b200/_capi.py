@@ -36,7 +36,7 @@ FIELDS = {
     "positions": 0, "velocities": 1, "stresses": 2, "F": 3, "velocity_gradient": 4, "masses": 5,
     "volumes": 6, "volumes_original": 7, "colors": 8, "is_rigid": 9, "is_active": 10,
     "forces_external": 11, "eps_e": 12, "stress_ref": 13, "youngs_modulus": 14, "friction_angle": 15,
-    "acc_eps_p": 16,
+    "acc_eps_p": 16, "alpha": 16, "pc": 17,
     "node_masses": 20, "node_moments": 21, "node_moments_nt": 22, "node_ids": 23, "node_types": 24,
     "bins": 30, "hash_unsorted": 31, "hash_sorted": 32, "sorted_index": 33, "cell_start": 34, "cell_end": 35,
 }
@@ -86,6 +86,7 @@ EXPORTS = [
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
     "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
+    "pmpm_material_modified_cam_clay",
 ]
 
 EXPORTS += [
@@ -130,6 +131,7 @@ def lib():
     L.pmpm_musl_stage.argtypes = [vp, i]
     L.pmpm_autotune.argtypes = [vp, i, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_material_von_mises.argtypes = [f, f, f, f, f, ctypes.POINTER(Material)]
+    L.pmpm_material_modified_cam_clay.argtypes = [f] * 10 + [ctypes.POINTER(Material)]
     L.pmpm_material_point_vjp.argtypes = [ctypes.POINTER(Material), i, i, f] + [vp] * 11 + [i, i]
     L.pmpm_rollout_reset.argtypes = [vp]
     L.pmpm_rollout_backward.argtypes = [vp, vp, i, vp, vp, vp, vp]
@@ -210,6 +212,10 @@ def make_material(m: dict) -> Material:
     elif t == "VonMises":
         check(L.pmpm_material_von_mises(m["density"], m["E"], m.get("pois", 0.0), m["yield_stress"], m.get("H", 0.0),
                                         ctypes.byref(out)), "material")
+    elif t == "ModifiedCamClay":
+        check(L.pmpm_material_modified_cam_clay(m["density"], m["E"], m.get("pois", 0.0), m["M"], m["lam"], m["kap"],
+                                                m["Vs"], m["R"], m.get("Pt", 0.0), m.get("beta", 1.0),
+                                                ctypes.byref(out)), "material")
     elif t == "DP_rheo":
         check(L.pmpm_material_dp_rheo(m["density"], m["E"], m.get("pois", 0.0), m["M"], m.get("Pt", 0.0),
                                       m.get("dilatancy_angle", 0.0), ctypes.byref(out)), "material")
@@ -309,7 +315,7 @@ def field_shape(name, dim, n, num_nodes, nsn=None):
         "stresses": (n, 3, 3), "stress_ref": (n, 3, 3), "F": (n, dim, dim), "velocity_gradient": (n, dim, dim),
         "eps_e": (n, dim, dim), "masses": (n,), "volumes": (n,), "volumes_original": (n,),
         "youngs_modulus": (n,), "friction_angle": (n,), "acc_eps_p": (n,),
-        "colors": (n,), "is_rigid": (n,), "is_active": (n,),
+        "alpha": (n,), "pc": (n,), "colors": (n,), "is_rigid": (n,), "is_active": (n,),
         "node_masses": (num_nodes,), "node_moments": (num_nodes, dim), "node_moments_nt": (num_nodes, dim),
         "node_ids": (num_nodes, 3), "node_types": (num_nodes, 3), "bins": (n, dim),
         "hash_unsorted": (n,), "hash_sorted": (n,), "sorted_index": (n,),

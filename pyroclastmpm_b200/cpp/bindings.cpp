@@ -249,6 +249,31 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def_readonly("shear_modulus", &VonMises::shear_modulus)
       .def("calculate_timestep", &VonMises::calculate_timestep, py::arg("cell_size"), py::arg("factor"));
 
+  py::class_<ModifiedCamClay>(m, "ModifiedCamClay", py::dynamic_attr())
+      .def(py::init<float, float, float, float, float, float, float, float, float, float>(), py::arg("density"),
+           py::arg("E"), py::arg("pois"), py::arg("M"), py::arg("lam"), py::arg("kap"), py::arg("Vs"), py::arg("R"),
+           py::arg("Pt"), py::arg("beta"))
+      // ModifiedCamClay::initialize (modified_camclay_bind.cpp): the history is
+      // set up when the solver is built from the particles' current stresses
+      .def("initialize",
+           [](ModifiedCamClay &, ParticlesContainer particles, int mat_id) { return py::make_tuple(particles, mat_id); },
+           py::arg("particles"), py::arg("mat_id") = 0)
+      .def_readwrite("density", &ModifiedCamClay::density)
+      .def_readonly("E", &ModifiedCamClay::E)
+      .def_readonly("pois", &ModifiedCamClay::pois)
+      .def_readonly("M", &ModifiedCamClay::M)
+      .def_readonly("lam", &ModifiedCamClay::lam)
+      .def_readonly("kap", &ModifiedCamClay::kap)
+      .def_readonly("Vs", &ModifiedCamClay::Vs)
+      .def_readonly("R", &ModifiedCamClay::R)
+      .def_readonly("Pt", &ModifiedCamClay::Pt)
+      .def_readonly("beta", &ModifiedCamClay::beta)
+      .def_readonly("bulk_modulus", &ModifiedCamClay::bulk_modulus)
+      .def_readonly("shear_modulus", &ModifiedCamClay::shear_modulus)
+      .def_readonly("lame_modulus", &ModifiedCamClay::lame_modulus)
+      .def_static("calculate_timestep", &ModifiedCamClay::calculate_timestep, py::arg("cell_size"), py::arg("factor"),
+                  py::arg("bulk_modulus"), py::arg("shear_modulus"), py::arg("density"));
+
   py::class_<BoundaryCondition>(m, "BoundaryCondition").def(py::init<>());
   py::class_<Gravity>(m, "Gravity", py::dynamic_attr())
       .def(py::init([](py::object g, bool is_ramp, int ramp_step, py::object ge) {

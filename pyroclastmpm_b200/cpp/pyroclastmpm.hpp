@@ -422,7 +422,32 @@ struct VonMises {
     return dt;
   }
 };
-using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager, VonMises>;
+// ModifiedCamClay (src/materials/modifiedcamclay.cpp:47-63): the
+// constructor's R is the preconsolidation ratio (pc = R p0 at the solver's
+// initialize, from the particles' stresses); beta is kept and unused, as in
+// the reference's stress update.
+struct ModifiedCamClay {
+  ModifiedCamClay(Real density, Real E, Real pois, Real M, Real lam, Real kap, Real Vs, Real R, Real Pt, Real beta)
+      : density(density), E(E), pois(pois), M(M), lam(lam), kap(kap), Vs(Vs), R(R), Pt(Pt), beta(beta) {
+    bulk_modulus = E / (3.0f * (1.0f - 2.0f * pois));
+    shear_modulus = E / (2.0f * (1.0f + pois));
+    lame_modulus = E * pois / ((1.0f + pois) * (1.0f - 2.0f * pois));
+  }
+  Real density, E, pois, M, lam, kap, Vs, R, Pt, beta, bulk_modulus, shear_modulus, lame_modulus;
+  pmpm_material desc() const {
+    pmpm_material m;
+    check(pmpm_material_modified_cam_clay(density, E, pois, M, lam, kap, Vs, R, Pt, beta, &m), "ModifiedCamClay");
+    return m;
+  }
+  // ModifiedCamClay::calculate_timestep (src/materials/modifiedcamclay.cpp:
+  // 184-195): the moduli and density are arguments
+  static Real calculate_timestep(Real cell_size, Real factor, Real bulk_modulus, Real shear_modulus, Real density) {
+    Real dt;
+    check(pmpm_calculate_timestep(cell_size, factor, bulk_modulus, shear_modulus, density, &dt), "calculate_timestep");
+    return dt;
+  }
+};
+using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager, VonMises, ModifiedCamClay>;
 
 struct BoundaryCondition {
   bool isActive = true;

@@ -129,6 +129,7 @@ struct pmpm_sim {
   } ro;
   bool has_planar = false, has_dp = false, has_sref = false;
   bool has_vm = false;  // a VonMises material: elastic strain and accumulated plastic strain
+  bool has_mcc = false; // a Modified Cam Clay material: elastic strain, alpha and pc
 
   // particles (two storage sets, swapped by the physical re-sort)
   int n = 0, stride = 0;
@@ -200,6 +201,7 @@ void free_particles(pmpm_sim *s) {
     dfree(P.pE);
     dfree(P.pphi);
     dfree(P.acc);
+    dfree(P.pc);
     P = DevParticles{};
   }
   dfree(s->slot);
@@ -228,7 +230,8 @@ int alloc_particle_set(pmpm_sim *s, DevParticles &P) {
     PMPM_TRY(dalloc(&P.eps, (size_t)E * st));
     PMPM_TRY(dalloc(&P.sref, (size_t)S * st));
   }
-  if (s->has_vm) PMPM_TRY(dalloc(&P.acc, (size_t)st));
+  if (s->has_vm || s->has_mcc) PMPM_TRY(dalloc(&P.acc, (size_t)st));
+  if (s->has_mcc) PMPM_TRY(dalloc(&P.pc, (size_t)st));
   PMPM_TRY(dalloc(&P.color, (size_t)st));
   PMPM_TRY(dalloc(&P.active, (size_t)st));
   PMPM_TRY(dalloc(&P.rigid, (size_t)st));
@@ -667,6 +670,27 @@ __global__ void k_dp_init(DevParticles P, int D, int *nonzero_ref) {
   if (nz) atomicOr(nonzero_ref, 1);
 }
 
+// ModifiedCamClay::initialize (src/materials/modifiedcamclay.cpp:68-108), the
+// part that is not the shared history reset of k_dp_init: per particle of a
+// Modified Cam Clay colour, alpha = 0 and pc = R p0 with p0 = -tr(sigma)/3
+// (the reference applies one material's R to every particle; here each
+// particle takes its own material's).
+__global__ void k_mcc_init(StepArgs a, int D) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.P.n) return;
+  const int st = a.P.stride;
+  const int c = a.P.color[s];
+  float pc = 0.0f;
+  if (c < a.nmat && a.mat[c].type == PMPM_MAT_MODIFIED_CAM_CLAY) {
+    const float sxx = a.P.sig[0 * st + s], syy = a.P.sig[1 * st + s];
+    const float szz = a.P.sig[(D == 2 ? 3 : 2) * st + s];
+    const float p0 = (float)(-(double)((sxx + syy) + szz) / 3.0);
+    pc = p0 * a.mat[c].p[7];
+  }
+  a.P.acc[s] = 0.0f;
+  a.P.pc[s] = pc;
+}
+
 int field_info(const pmpm_sim *s, int field, size_t *bytes) {
   const size_t n = (size_t)s->n, D = (size_t)s->dim, nn = (size_t)s->g.ntotal;
   switch (field) {
@@ -690,6 +714,7 @@ int field_info(const pmpm_sim *s, int field, size_t *bytes) {
     case PMPM_FIELD_YOUNGS_MODULUS:
     case PMPM_FIELD_FRICTION_ANGLE:
     case PMPM_FIELD_ACC_EPS_P:
+    case PMPM_FIELD_PRECONSOLIDATION:
     case PMPM_FIELD_HASH_UNSORTED:
     case PMPM_FIELD_HASH_SORTED:
     case PMPM_FIELD_SORTED_INDEX:
@@ -865,6 +890,25 @@ int pmpm_material_von_mises(float density, float E, float pois, float yield_stre
   return PMPM_OK;
 }
 
+int pmpm_material_modified_cam_clay(float density, float E, float pois, float M, float lam, float kap, float Vs,
+                                    float R, float Pt, float beta, pmpm_material *out) {
+  (void)beta;  // not used by the reference's update either
+  if (!out) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!(lam != kap) || !(kap != 0.0f) || !(Vs != 0.0f) || !(M != 0.0f)) return PMPM_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  out->type = PMPM_MAT_MODIFIED_CAM_CLAY;
+  out->density = density;
+  out->params[0] = E / (3.0f * (1.0f - 2.0f * pois));
+  out->params[1] = E / (2.0f * (1.0f + pois));
+  out->params[2] = M;
+  out->params[3] = lam;
+  out->params[4] = kap;
+  out->params[5] = Vs;
+  out->params[6] = Pt;
+  out->params[7] = R;
+  return PMPM_OK;
+}
+
 int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
                           pmpm_material *out) {
   if (!out) return PMPM_ERR_INVALID_ARGUMENT;
@@ -992,6 +1036,8 @@ int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float fact
     case PMPM_MAT_NEWTON_FLUID:
       return pmpm_calculate_timestep(cell_size, factor, mat->params[1], 0.0f, mat->density, dt);
     case PMPM_MAT_DRUCKER_PRAGER:
+    case PMPM_MAT_VON_MISES:
+    case PMPM_MAT_MODIFIED_CAM_CLAY:
       return pmpm_calculate_timestep(cell_size, factor, mat->params[0], mat->params[1], mat->density, dt);
     default:
       return PMPM_ERR_NOT_SUPPORTED;
@@ -1044,7 +1090,11 @@ static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
   // materials
   for (int k = 0; k < desc->num_materials; k++) {
     const pmpm_material &m = desc->materials[k];
-    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_VON_MISES) return PMPM_ERR_INVALID_ARGUMENT;
+    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_MODIFIED_CAM_CLAY) return PMPM_ERR_INVALID_ARGUMENT;
+    if (m.type == PMPM_MAT_MODIFIED_CAM_CLAY) {
+      s->has_mcc = true;
+      s->has_dp = true;  // elastic strain and reference stress
+    }
     if (m.type == PMPM_MAT_VON_MISES) {
       if (desc->dim != 3) return PMPM_ERR_NOT_SUPPORTED;  // the reference's VonMises is 3D only
       s->has_vm = true;
@@ -1326,6 +1376,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   if (P.eps) PMPM_CUDA(cudaMemset(P.eps, 0, sizeof(float) * E * st));
   if (P.sref) PMPM_CUDA(cudaMemset(P.sref, 0, sizeof(float) * S * st));
   if (P.acc) PMPM_CUDA(cudaMemset(P.acc, 0, sizeof(float) * st));
+  if (P.pc) PMPM_CUDA(cudaMemset(P.pc, 0, sizeof(float) * st));
   PMPM_CUDA(cudaMemcpy(P.color, color.data(), st, cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemcpy(P.rigid, rigid.data(), st, cudaMemcpyHostToDevice));
   PMPM_CUDA(cudaMemcpy(P.active, active.data(), st, cudaMemcpyHostToDevice));
@@ -1368,6 +1419,10 @@ int pmpm_initialize(pmpm_sim *s) {
     PMPM_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     PMPM_CUDA(cudaStreamSynchronize(s->stream));
     s->has_sref = h != 0;
+  }
+  if (s->has_mcc) {
+    k_mcc_init<<<blocks_for(s->n), kTPB, 0, s->stream>>>(make_args(s), s->dim);
+    PMPM_LAUNCHED();
   }
   PMPM_CUDA(cudaStreamSynchronize(s->stream));
   return PMPM_OK;
@@ -1485,12 +1540,13 @@ int pmpm_get_field(pmpm_sim *s, int field, void *dst, size_t bytes, int on_devic
     case PMPM_FIELD_VOLUMES: kind = 4; src = P.V; break;
     case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; src = P.V0; break;
     case PMPM_FIELD_ACC_EPS_P:
-      if (!P.acc) {
+    case PMPM_FIELD_PRECONSOLIDATION:
+      src = field == PMPM_FIELD_ACC_EPS_P ? P.acc : P.pc;
+      if (!src) {
         PMPM_CUDA(cudaMemsetAsync(s->staging, 0, need, s->stream));
         return copy_out(s, s->staging, dst, need, on_device);
       }
       kind = 4;
-      src = P.acc;
       break;
     case PMPM_FIELD_YOUNGS_MODULUS:
     case PMPM_FIELD_FRICTION_ANGLE:
@@ -1539,6 +1595,7 @@ int pmpm_set_field(pmpm_sim *s, int field, const void *src, size_t bytes, int on
     case PMPM_FIELD_VOLUMES: kind = 4; dstp = P.V; break;
     case PMPM_FIELD_VOLUMES_ORIGINAL: kind = 4; dstp = P.V0; break;
     case PMPM_FIELD_ACC_EPS_P: kind = 4; dstp = P.acc; break;
+    case PMPM_FIELD_PRECONSOLIDATION: kind = 4; dstp = P.pc; break;
     case PMPM_FIELD_YOUNGS_MODULUS:
     case PMPM_FIELD_FRICTION_ANGLE:
       PMPM_TRY(ensure_particle_params(s));
@@ -2141,7 +2198,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
       st = PMPM_ERR_INVALID_ARGUMENT;  // one kernel instantiation serves the batch
       break;
     }
-    if (h->rbls_index >= 0 || (h->flags & PMPM_FLAG_MUSL) || h->has_vm) {
+    if (h->rbls_index >= 0 || (h->flags & PMPM_FLAG_MUSL) || h->has_vm || h->has_mcc) {
       st = PMPM_ERR_NOT_SUPPORTED;
       break;
     }
@@ -2791,7 +2848,7 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   }
   // time each variant on the same state: save, step, restore (no re-sort meanwhile)
   const size_t per = (size_t)state_floats(s) * s->stride;
-  const size_t extra = (size_t)(s->dim * s->dim + 1) * s->stride;  // L and the VonMises history
+  const size_t extra = (size_t)(s->dim * s->dim + 2) * s->stride;  // L, alpha (or VonMises history) and pc
   float *saved = nullptr;
   if (cudaMalloc(&saved, (per + extra) * sizeof(float)) != cudaSuccess) return PMPM_ERR_OUT_OF_MEMORY;
   const int step0 = s->step;
@@ -2802,6 +2859,8 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
     const cudaMemcpyKind kd = cudaMemcpyDeviceToDevice;
     if (P.L) PMPM_CUDA(cudaMemcpyAsync(save ? bL : P.L, save ? P.L : bL, nL * 4, kd, s->stream));
     if (P.acc) PMPM_CUDA(cudaMemcpyAsync(save ? bA : P.acc, save ? P.acc : bA, (size_t)s->stride * 4, kd, s->stream));
+    float *bP = bA + s->stride;
+    if (P.pc) PMPM_CUDA(cudaMemcpyAsync(save ? bP : P.pc, save ? P.pc : bP, (size_t)s->stride * 4, kd, s->stream));
     return PMPM_OK;
   };
   int st = copy_state(s, saved, true);

@@ -58,7 +58,8 @@ struct DevParticles {
   int stride;
   float *x, *v, *F, *sig, *L, *m, *V, *V0, *fext, *eps, *sref;
   float *pE, *pphi;  // per-particle Young's modulus and friction angle (deg) of Drucker-Prager, or null
-  float *acc;        // VonMises accumulated plastic strain, or null
+  float *acc;        // VonMises accumulated plastic strain / Modified Cam Clay alpha, or null
+  float *pc;         // Modified Cam Clay preconsolidation pressure, or null
   uint8_t *color, *active, *rigid;
   int *id;             // original particle id of each storage slot
   unsigned int *hash;  // reference cell hash of the last partition
@@ -581,6 +582,151 @@ __device__ __forceinline__ void vm_update(const float *prm, const float *L, floa
     eps[k] = (float)((double)sc / (2.0 * (double)G) + (diag ? (1.0 / 3.0) * (double)ev : 0.0));
   }
   acc = (float)acc_eps;
+}
+
+// Small-strain increment of the co-rotational stress updates
+// (src/materials/modifiedcamclay_inline.h:350-362, dp_rheo_inline.h:155-161):
+// deps = sym(L) dt - W eps + eps W with W = skew(L) dt (D x D).
+template <int D>
+__device__ __forceinline__ void corotational_increment(const float *L, float dt, const float eps[9], float deps[9]) {
+  float W[9];
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      deps[a * D + b] = (0.5f * (L[a * D + b] + L[b * D + a])) * dt;
+      W[a * D + b] = (0.5f * (L[a * D + b] - L[b * D + a])) * dt;
+    }
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) {
+      float we = 0.0f, ew = 0.0f;
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        we += W[a * D + k] * eps[k * D + b];
+        ew += eps[a * D + k] * W[k * D + b];
+      }
+      deps[a * D + b] += -we + ew;
+    }
+}
+
+// Modified Cam Clay with pressure-dependent elasticity:
+// update_modifiedcamclay_nonlinear (src/materials/modifiedcamclay_inline.h:
+// 321-511), yield function compute_yield_function (:57-63).  Pressures are
+// positive in compression.  V is the particle's current volume (specific
+// volume V / Vs), S holds the previous stress on entry and the new one on
+// exit, eps the D x D elastic strain, alpha the volumetric plastic strain,
+// pc the preconsolidation pressure.
+//   trial: p = p_prev / (1 - (v/kap) dev_e), s = dev(sref) + 2G dev(eps + deps)
+//   (zz deviator zeroed in 2D), q = sqrt(3/2 s:s);
+//   yield f = (p_s - p - Pt)^2 + (q/M)^2 - p_s^2 with p_s = (pc + Pt)/2;
+//   plastic: Newton on (lambda, alpha) with the reference's residuals and
+//   its 2 x 2 iteration matrix (which takes dp/dalpha as -K), until
+//   |R| <= 1e-2, the bound growing tenfold per iteration after 1000.  The
+//   iteration runs in FP64 (the reference mixes FP32 and FP64 there; with
+//   FP32 residuals it needs the growing bound to stop); stress, strain and
+//   pc come from the last evaluated iterate, alpha from the updated one.
+__device__ __forceinline__ float mcc_yield(float p, float Pt, float ps, float q, float M) {
+  return (ps - p - Pt) * (ps - p - Pt) + (q / M) * (q / M) - ps * ps;
+}
+
+template <int D>
+__device__ __forceinline__ void mcc_update(const float *prm, const float *L, float dt, float V, float eps[9],
+                                           const float sref[9], float S[9], float &alpha, float &pc) {
+  const float K = prm[0], G = prm[1], M = prm[2], lam = prm[3], kap = prm[4], Vs = prm[5], Pt = prm[6];
+  float deps[9];
+  corotational_increment<D>(L, dt, eps, deps);
+  const float p_ref = -(1.0f / 3.0f) * ((sref[0] + sref[4]) + sref[8]);
+  float s_ref[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] += p_ref;
+  s_ref[4] += p_ref;
+  s_ref[8] += p_ref;
+  float eps_tr[9], tr_prev = 0.0f, tr_inc = 0.0f, tr_tr = 0.0f;
+#pragma unroll
+  for (int k = 0; k < D * D; k++) eps_tr[k] = eps[k] + deps[k];
+#pragma unroll
+  for (int a = 0; a < D; a++) {
+    tr_prev += eps[a * D + a];
+    tr_inc += deps[a * D + a];
+    tr_tr += eps_tr[a * D + a];
+  }
+  const float ev_tr = -tr_tr;
+  float edev[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) edev[k] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) edev[3 * a + b] = eps_tr[a * D + b];
+#pragma unroll
+  for (int a = 0; a < 3; a++) edev[3 * a + a] += (1.0f / 3.0f) * ev_tr;
+  if (D < 3) edev[8] = 0.0f;
+  const float v_spec = V / Vs;
+  const float p_prev = -((S[0] + S[4]) + S[8]) / 3.0f;
+  const float v_kap = v_spec / kap;
+  const float dev_tr = -tr_inc;
+  const float p_tr = p_prev / (1.0f - v_kap * dev_tr);
+  float s_tr[9], ss = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    s_tr[k] = s_ref[k] + 2.0f * G * edev[k];
+    ss += s_tr[k] * s_tr[k];
+  }
+  const float q_tr = sqrtf(1.5f * ss);
+  const float pc_prev = pc;
+  const float f_tr = mcc_yield(p_tr, Pt, 0.5f * (pc_prev + Pt), q_tr, M);
+  if (f_tr <= 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) S[k] = s_tr[k] - ((k == 0 || k == 4 || k == 8) ? p_tr : 0.0f);
+#pragma unroll
+    for (int k = 0; k < D * D; k++) eps[k] = eps_tr[k];
+    return;
+  }
+  const double Kd = K, Gd = G, Md = M, MM = Md * Md, Ptd = Pt, pcd = pc_prev, a_prev = alpha;
+  const double vlt = (double)v_spec / ((double)lam - (double)kap);
+  double lamb = 0.0, a_next = a_prev, tol = 1e-2;
+  double p = p_tr, c = 1.0, ps = 0.5 * (pcd + Ptd), dev_e = dev_tr;
+  for (int it = 0; it < 1400; it++) {
+    const double dpv = a_next - a_prev;
+    dev_e = (double)dev_tr - dpv;
+    p = (double)p_prev / (1.0 - (double)v_kap * dev_e);
+    c = MM / (MM + 6.0 * Gd * lamb);
+    const double q = c * (double)q_tr;
+    ps = 0.5 * (pcd * (1.0 + vlt * dpv) + Ptd);
+    const double pbar = ps - p - Ptd;
+    const double R0 = pbar * pbar + (q / Md) * (q / Md) - ps * ps;
+    const double R1 = dpv + 2.0 * lamb * pbar;
+    const double omv = 1.0 - vlt * dpv;
+    const double H = 0.5 * vlt * (pcd / (omv * omv));
+    const double d00 = (-12.0 * Gd / (MM + 6.0 * Gd * lamb)) * (q / Md) * (q / Md);
+    const double d01 = 2.0 * pbar * (Kd + H) - 2.0 * ps * H;
+    const double d10 = 2.0 * pbar;
+    const double d11 = 1.0 + 2.0 * lamb * (Kd + H);
+    const double det = d00 * d11 - d01 * d10;
+    lamb -= (d11 * R0 - d01 * R1) / det;
+    a_next -= (d00 * R1 - d10 * R0) / det;
+    const double conv = sqrt(R0 * R0 + R1 * R1);
+    if (it > 1000) tol *= 10.0;
+    if (!(conv > tol)) break;
+  }
+  const float cf = (float)c, pn = (float)p;
+  const float two_g = (float)(2.0 * Gd);
+  const float evol = (float)((1.0 / 3.0) * ((double)tr_prev + dev_e));
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const float sk = cf * s_tr[k];
+    S[k] = sk - ((k == 0 || k == 4 || k == 8) ? pn : 0.0f);
+    s_tr[k] = sk;
+  }
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) eps[a * D + b] = (s_tr[3 * a + b] - s_ref[3 * a + b]) / two_g - (a == b ? evol : 0.0f);
+  alpha = (float)a_next;
+  pc = (float)(2.0 * ps - Ptd);
 }
 
 // --------------------------------------------------------------------------

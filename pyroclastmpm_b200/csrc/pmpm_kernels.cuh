@@ -447,6 +447,7 @@ __global__ void __launch_bounds__(256) k_reorder(StepArgs a, DevParticles dst, i
     move_comps(S.pphi, dst.pphi, 1, st, s, k);
   }
   if (S.acc) move_comps(S.acc, dst.acc, 1, st, s, k);
+  if (S.pc) move_comps(S.pc, dst.pc, 1, st, s, k);
   move_comps(S.hash, dst.hash, 1, st, s, k);
   a.B.order[k] = k;  // storage is now in cell order
 }
@@ -1865,6 +1866,28 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
 #pragma unroll
       for (int y = x; y < 3; y++) P.eps[eps_index<3>(x, y) * st + s] = eps[3 * x + y];
     P.acc[s] = acc;
+  } else if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY) {
+    float eps[9], sref[9];
+#pragma unroll
+    for (int x = 0; x < D; x++)
+#pragma unroll
+      for (int y = 0; y < D; y++) eps[x * D + y] = P.eps[eps_index<D>(x, y) * st + s];
+#pragma unroll
+    for (int x = 0; x < 3; x++)
+#pragma unroll
+      for (int y = 0; y < 3; y++) {
+        const int k = sig_index<D>(x, y);
+        sref[3 * x + y] = (k < 0 || !a.has_sref) ? 0.0f : P.sref[k * st + s];
+      }
+    load_sig3<D>(P, s, S);
+    float alpha = P.acc[s], pc = P.pc[s];
+    mcc_update<D>(mt.p, L, a.dt, P.V[s], eps, sref, S, alpha, pc);
+#pragma unroll
+    for (int x = 0; x < D; x++)
+#pragma unroll
+      for (int y = x; y < D; y++) P.eps[eps_index<D>(x, y) * st + s] = eps[x * D + y];
+    P.acc[s] = alpha;
+    P.pc[s] = pc;
   } else {
     float eps[9], sref[9];
 #pragma unroll

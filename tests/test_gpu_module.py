@@ -193,3 +193,39 @@ def test_particles_pickle_restart():
                   [pm.LinearElastic(1000.0, 1000.0, 0.3)])
     for name in ("positions", "velocities", "stresses", "F", "masses", "volumes"):
         np.testing.assert_array_equal(getattr(mpm2.particles, name), getattr(mpm.particles, name), err_msg=name)
+
+
+def test_modified_cam_clay_through_module_matches_capi():
+    """The reference's Modified Cam Clay workflow: prestressed particles,
+    material.initialize(particles, 0), then a USL solver; the same steps as
+    the C ABI run of the same scene."""
+    import pyroclastmpm_b200.MPM3D as pm
+    from pyroclastmpm_b200 import Simulation
+
+    rng = np.random.default_rng(9)
+    n, h = 2000, 0.1
+    x = rng.uniform(0.15, 0.85, (n, 3))
+    v = rng.normal(0, 0.2, (n, 3))
+    S = np.broadcast_to(-5e3 * np.eye(3), (n, 3, 3)).copy()
+    Vs = h ** 3 / 8 / 1.8
+    args = (1000.0, 1e6, 0.2, 1.05, 0.13, 0.033, Vs, 1.0, 0.0, 1.0)
+    pm.set_globals(1e-4, 8, "quadratic", "output")
+    pm.set_global_step(0)
+    particles = pm.ParticlesContainer(x, v)
+    particles.stresses = S
+    mat = pm.ModifiedCamClay(*args)
+    particles, _ = mat.initialize(particles, 0)
+    nodes = pm.NodesContainer([0.0] * 3, [1.0] * 3, h)
+    usl = pm.USL(particles, nodes, [mat], [pm.Gravity([0.0, 0.0, -9.81])], alpha=0.99)
+    usl.solve_nsteps(3)
+    m = dict(zip(("density", "E", "pois", "M", "lam", "kap", "Vs", "R", "Pt", "beta"), args))
+    sim = Simulation(3, [0.0] * 3, [1.0] * 3, h, shape_function="quadratic", dt=1e-4, particles_per_cell=8,
+                     alpha=0.99, materials=[dict(m, type="ModifiedCamClay")],
+                     bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]}])
+    sim.set_particles(x, v)
+    sim.set("stresses", S)
+    sim.initialize()
+    sim.solve(3)
+    for name in ("positions", "stresses"):
+        assert rel(getattr(usl.particles, name), sim.get(name)) < 1e-5, name
+    assert mat.calculate_timestep(h, 0.3, mat.bulk_modulus, mat.shear_modulus, 1000.0) > 0
