@@ -62,9 +62,14 @@ def make_oracle(scene, precision):
 
 
 def point_loads(n, dim, seed):
-    """Velocity gradients of compression, extension and shear (1/s)."""
+    """Velocity gradients (1/s): shear with some compression.  Sustained
+    extension drives the pressure to zero, where the ellipse (no tensile
+    strength, Pt = 0) degenerates and the reference's iteration stops
+    converging; those states are left out."""
     rng = np.random.default_rng(seed)
     L = rng.normal(0, 0.3, (n, dim, dim))
+    L -= (np.trace(L, axis1=1, axis2=2) / dim)[:, None, None] * np.eye(dim)
+    L -= rng.uniform(0.02, 0.3, n)[:, None, None] * np.eye(dim)
     L[: n // 3] -= 0.5 * np.eye(dim)  # compression: on to the cap
     L[n // 3: n // 2] *= 0.05         # nearly elastic
     return L
