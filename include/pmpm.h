@@ -63,7 +63,11 @@ enum {
    * (src/materials/modifiedcamclay_inline.h:321-511), the update the reference's
    * ModifiedCamClay::stress_update runs (src/materials/modifiedcamclay.cpp:
    * 148-178); a member of the reference's MaterialType */
-  PMPM_MAT_MODIFIED_CAM_CLAY = 5
+  PMPM_MAT_MODIFIED_CAM_CLAY = 5,
+  /* Drucker-Prager cone with a Cam-Clay-type cap and exponential hardening:
+   * update_druckerpragercap (src/materials/druckerprager_cap_inline.h:370-554;
+   * like Drucker-Prager, not a member of the reference's MaterialType) */
+  PMPM_MAT_DRUCKER_PRAGER_CAP = 6
 };
 
 /* Boundary conditions: the reference BoundaryConditionType members on this
@@ -116,11 +120,12 @@ enum {
  *                   yield sqrt(J2) + eta p - kc (p = tr(sigma)/3)
  *   VON_MISES:      {K, G, yield_stress, H}
  *   MODIFIED_CAM_CLAY: {K, G, M, lam, kap, Vs, Pt, R}
- *                   (R: preconsolidation ratio, pc = R p0 at initialize) */
+ *                   (R: preconsolidation ratio, pc = R p0 at initialize)
+ *   DRUCKER_PRAGER_CAP: {K, G, M, lam, kap, Vs, Pt, R, beta, eta_bar} */
 typedef struct {
   int type;
   float density;
-  float params[8];
+  float params[12];
 } pmpm_material;
 
 /* Boundary-condition parameters; fill with the pmpm_bc_* helpers.
@@ -246,6 +251,13 @@ int pmpm_material_von_mises(float density, float E, float pois, float yield_stre
  * stress, elastic strain and alpha = 0, pc = R p0 with p0 = -tr(sigma)/3. */
 int pmpm_material_modified_cam_clay(float density, float E, float pois, float M, float lam, float kap, float Vs,
                                     float R, float Pt, float beta, pmpm_material *out);
+/* DruckerPragerCap::DruckerPragerCap (src/materials/druckerprager_cap.cpp:
+ * 43-67): as ModifiedCamClay, plus beta (cap ellipse ratio on its compressive
+ * side) and the dilatancy angle in degrees (eta_bar = 6 sin(psi) /
+ * (sqrt(3) (3 + sin(psi)))); the cone slope is eta = M / sqrt(3).  Initialize
+ * as ModifiedCamClay (DruckerPragerCap::initialize, :72-108). */
+int pmpm_material_drucker_prager_cap(float density, float E, float pois, float M, float lam, float kap, float Vs,
+                                     float R, float Pt, float beta, float dilatancy_deg, pmpm_material *out);
 
 /* Boundary-condition helpers (reference constructors). */
 /* Gravity::Gravity (src/boundaryconditions/gravity.cpp:52-60) */

@@ -29,7 +29,7 @@ LINEAR, QUADRATIC, CUBIC = 0, 1, 2
 SHAPE_FUNCTIONS = {"linear": LINEAR, "quadratic": QUADRATIC, "cubic": CUBIC}
 
 MAT_NONE, MAT_LINEAR_ELASTIC, MAT_NEWTON_FLUID, MAT_DRUCKER_PRAGER, MAT_VON_MISES = 0, 1, 2, 3, 4
-MAT_MODIFIED_CAM_CLAY = 5
+MAT_MODIFIED_CAM_CLAY, MAT_DRUCKER_PRAGER_CAP = 5, 6
 BC_GRAVITY, BC_NODEDOMAIN, BC_BODYFORCE, BC_PLANARDOMAIN = 1, 2, 3, 4
 BC_RIGIDBODY_LEVELSET, BC_RIGID_SDF = 5, 6
 RIGID_MODES = {"static": 0, "loop_rotate": 1}
@@ -63,7 +63,7 @@ def _structs(precision):
                     ("num_cells", ctypes.c_int * 3), ("num_cells_total", ctypes.c_int)]
 
     class Material(ctypes.Structure):
-        _fields_ = [("type", ctypes.c_int), ("density", creal), ("p", creal * 8)]
+        _fields_ = [("type", ctypes.c_int), ("density", creal), ("p", creal * 12)]
 
     class BC(ctypes.Structure):
         _fields_ = [("type", ctypes.c_int), ("i", ctypes.c_int * 8), ("r", creal * 16),
@@ -150,6 +150,17 @@ def material_params(mat: dict, precision: str = "f32"):
         shear = E / (two * (one + nu))
         return MAT_MODIFIED_CAM_CLAY, dens, [bulk, shear, npr(mat["M"]), npr(mat["lam"]), npr(mat["kap"]),
                                              npr(mat["Vs"]), npr(mat.get("Pt", 0.0)), npr(mat["R"])]
+    if t == "DruckerPragerCap":
+        # DruckerPragerCap::DruckerPragerCap (src/materials/druckerprager_cap.cpp:43-67)
+        E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
+        one, two, three = npr(1), npr(2), npr(3)
+        bulk = E / (three * (one - two * nu))
+        shear = E / (two * (one + nu))
+        psi = math.radians(float(mat.get("dilatancy_angle", 0.0)))
+        eta_bar = 6.0 * math.sin(psi) / (math.sqrt(3.0) * (3.0 + math.sin(psi)))
+        return MAT_DRUCKER_PRAGER_CAP, dens, [bulk, shear, npr(mat["M"]), npr(mat["lam"]), npr(mat["kap"]),
+                                              npr(mat["Vs"]), npr(mat.get("Pt", 0.0)), npr(mat["R"]),
+                                              npr(mat.get("beta", 1.0)), npr(eta_bar)]
     if t == "DP_rheo":
         # the reference's DP_rheo parameters (src/materials/dp_rheo.cpp:45-70)
         E, nu = npr(mat["E"]), npr(mat.get("pois", 0.0))
@@ -250,7 +261,7 @@ class OracleSim:
             t, dens, p = material_params(m, precision)
             mats[k].type = t
             mats[k].density = float(dens)
-            for j in range(8):
+            for j in range(len(p)):
                 mats[k].p[j] = float(p[j])
         self._mats = mats
         self.bc_list = list(bcs)
@@ -352,12 +363,13 @@ class OracleSim:
         # Drucker-Prager history starts from the current stresses
         self.a["stress_ref"][:] = self.a["stresses"]
         self.a["eps_e"][:] = 0
-        # ModifiedCamClay::initialize (src/materials/modifiedcamclay.cpp:68-108):
+        # ModifiedCamClay::initialize (src/materials/modifiedcamclay.cpp:68-108),
+        # DruckerPragerCap::initialize (src/materials/druckerprager_cap.cpp:72-108):
         # alpha = 0, pc = R p0 with p0 = -tr(sigma)/3, per particle of the colour
         npr = self.npr
         self.a["acc_eps_p"][:] = 0
         for k, m in enumerate(self.materials):
-            if m["type"] != "ModifiedCamClay":
+            if m["type"] not in ("ModifiedCamClay", "DruckerPragerCap"):
                 continue
             sel = self.a["colors"] == k
             tr = np.trace(self.a["stresses"][sel], axis1=1, axis2=2).astype(np.float64)
@@ -387,8 +399,9 @@ class OracleSim:
 
 
 def mcc_point(dim, L, stress, eps_e, stress_ref, alpha, pc, volume, dt, mat, precision="f32"):
-    """One Modified Cam Clay update of a single material point: returns the
-    new (stress, eps_e, alpha, pc)."""
+    """One Modified Cam Clay (or, for a DruckerPragerCap material, Drucker-
+    Prager cap, volume = the original volume) update of a single material
+    point: returns the new (stress, eps_e, alpha, pc)."""
     lib = _lib(precision)
     creal, npr = _real(precision)
     _, Material, _, _ = _structs(precision)
@@ -396,7 +409,7 @@ def mcc_point(dim, L, stress, eps_e, stress_ref, alpha, pc, volume, dt, mat, pre
     m = Material()
     m.type = t
     m.density = float(dens)
-    for j in range(8):
+    for j in range(len(p)):
         m.p[j] = float(p[j])
     Lc = np.ascontiguousarray(np.asarray(L, npr).reshape(dim, dim))
     sig = np.ascontiguousarray(np.asarray(stress, npr).reshape(3, 3).copy())
@@ -405,9 +418,9 @@ def mcc_point(dim, L, stress, eps_e, stress_ref, alpha, pc, volume, dt, mat, pre
     a = np.array([alpha], npr)
     c = np.array([pc], npr)
     vp = ctypes.c_void_p
-    lib.or_mcc_point(dim, Lc.ctypes.data_as(vp), sig.ctypes.data_as(vp), eps.ctypes.data_as(vp),
-                     sref.ctypes.data_as(vp), a.ctypes.data_as(vp), c.ctypes.data_as(vp), creal(volume), creal(dt),
-                     ctypes.byref(m))
+    fn = lib.or_dpc_point if mat["type"] == "DruckerPragerCap" else lib.or_mcc_point
+    fn(dim, Lc.ctypes.data_as(vp), sig.ctypes.data_as(vp), eps.ctypes.data_as(vp), sref.ctypes.data_as(vp),
+       a.ctypes.data_as(vp), c.ctypes.data_as(vp), creal(volume), creal(dt), ctypes.byref(m))
     return sig, eps, a[0], c[0]
 
 

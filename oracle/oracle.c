@@ -1286,6 +1286,161 @@ void or_mcc_point(int d, const REAL *L, REAL *sig, REAL *eps_e, const REAL *sref
   *pc = (real)(2.0 * ps_next - (double)Pt);
 }
 
+/* update_druckerpragercap (src/materials/druckerprager_cap_inline.h:370-554)
+ * with return_mapping_cone (:124-141), return_mapping_apex (:143-156),
+ * return_mapping_cap (:159-235), compute_pc / compute_a / compute_b (:56-84),
+ * the yield functions (:94-111) and update_plasticity (:328-346), p =
+ * tr(sigma)/3 (tension positive), in the reference's types: real for the
+ * trial state, the yield functions' arguments, pc and a; double for the
+ * return mappings.  Past the apex the return takes eta_bar dgamma =
+ * (p_tr - Pt) / K directly (the reference divides by eta_bar and multiplies
+ * back, 0/0 for eta_bar = 0).  The cap's Newton iteration stops at
+ * |R| <= 0.1, the bound growing tenfold per iteration after 1000; its
+ * results are the last evaluated iterate's.  V0: the particle's original
+ * volume.  p = {K, G, M, lam, kap, Vs, Pt, R, beta, eta_bar}. */
+static real dpc_pc(real v0, real pc_prev, real lam, real kap, real a_next, real a_prev) {
+  real C = (real)(v0 / (real)(lam - kap));
+  return (real)((real)exp((double)(real)(C * (real)(a_next - a_prev))) * pc_prev);
+}
+
+static real dpc_cap_yield(real p, real Pt, real a, real q, real b, real M) {
+  real pa = (real)((real)(p - Pt) + a), qm = (real)(q / M);
+  return (real)((1.0 / (double)(real)(b * b)) * (double)pa * (double)pa + (double)(real)(qm * qm) -
+                (double)(real)(a * a));
+}
+
+void or_dpc_point(int d, const REAL *L, REAL *sig, REAL *eps_e, const REAL *sref, REAL *alpha, REAL *pc, REAL V0,
+                  REAL dt, const or_material *m) {
+  real K = m->p[0], G = m->p[1], M = m->p[2], lam = m->p[3], kap = m->p[4], Vs = m->p[5], Pt = m->p[6];
+  real beta = m->p[8], eta_bar = m->p[9];
+  real deps[9], W[9];
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      deps[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] + L[b * d + a])) * dt);
+      W[a * d + b] = (real)((real)((real)0.5 * (real)(L[a * d + b] - L[b * d + a])) * dt);
+    }
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real we = 0, ew = 0;
+      for (int k = 0; k < d; k++) {
+        we = (real)(we + (real)(W[a * d + k] * eps_e[k * d + b]));
+        ew = (real)(ew + (real)(eps_e[a * d + k] * W[k * d + b]));
+      }
+      deps[a * d + b] = (real)(deps[a * d + b] + (real)(-we + ew));
+    }
+  real p_ref = (real)((real)(1.0 / 3.0) * (real)((real)(sref[0] + sref[4]) + sref[8]));
+  real s_ref[9];
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] = (real)(s_ref[0] - p_ref);
+  s_ref[4] = (real)(s_ref[4] - p_ref);
+  s_ref[8] = (real)(s_ref[8] - p_ref);
+  real eps_tr[9], ev = 0;
+  for (int k = 0; k < d * d; k++) eps_tr[k] = (real)(eps_e[k] + deps[k]);
+  for (int a = 0; a < d; a++) ev = (real)(ev + eps_tr[a * d + a]);
+  real p_tr = (real)(p_ref + (real)(K * ev));
+  real edev[9] = {0};
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) edev[3 * a + b] = eps_tr[a * d + b];
+  real third = (real)((1.0 / 3.0) * (double)ev);
+  for (int a = 0; a < 3; a++) edev[3 * a + a] = (real)(edev[3 * a + a] - third);
+  if (d < 3) edev[8] = 0;
+  real two_g = (real)(2.0 * (double)G);
+  real s_tr[9];
+  for (int k = 0; k < 9; k++) s_tr[k] = (real)(s_ref[k] + (real)(two_g * edev[k]));
+  real ss = 0;
+  for (int a = 0; a < 3; a++) {
+    real row = 0;
+    for (int k = 0; k < 3; k++) row = (real)(row + (real)(s_tr[3 * a + k] * s_tr[3 * a + k]));
+    ss = (real)(ss + row);
+  }
+  real J2 = (real)(0.5 * (double)ss);
+  real q_tr = (real)sqrt(3.0 * (double)J2);
+  real sqrtJ2 = (real)sqrt((double)J2);
+  real eta = (real)(sqrt(1.0 / 3.0) * (double)M);
+  real phi_cone = (real)(sqrtJ2 + (real)(eta * (real)(p_tr - Pt)));
+  real v0 = (real)(V0 / Vs);
+  real a_prev = *alpha, pc_prev = *pc;
+  real a_tr = (real)((real)(pc_prev + Pt) / (real)(1 + beta));
+  real b_tr = p_tr < (real)(Pt - a_tr) ? beta : (real)1;
+  real phi_cap = dpc_cap_yield(p_tr, Pt, a_tr, q_tr, b_tr, M);
+  if (phi_cone <= (real)0.0 && phi_cap <= (real)0.0) {
+    for (int k = 0; k < 9; k++) sig[k] = s_tr[k];
+    sig[0] = (real)(sig[0] + p_tr);
+    sig[4] = (real)(sig[4] + p_tr);
+    sig[8] = (real)(sig[8] + p_tr);
+    for (int k = 0; k < d * d; k++) eps_e[k] = eps_tr[k];
+    return;
+  }
+  double p_next = p_tr, pc_next = pc_prev, a_next = a_tr, al = a_prev;
+  real s_next[9];
+  for (int k = 0; k < 9; k++) s_next[k] = s_tr[k];
+  int done = 0;
+  if (phi_cone > (real)0.0) {
+    double dg = (double)phi_cone / ((double)K * (double)eta * (double)eta_bar + (double)G);
+    if ((double)sqrtJ2 - (double)G * dg < 0.0) {
+      double edg = ((double)p_tr - (double)Pt) / (double)K;
+      al = (double)a_prev - edg;
+      p_next = (double)p_tr - (double)K * edg;
+      for (int k = 0; k < 9; k++) s_next[k] = 0;
+      pc_next = dpc_pc(v0, pc_prev, lam, kap, (real)al, a_prev);
+      done = 1;
+    } else {
+      al = (double)a_prev - (double)eta_bar * dg;
+      p_next = (double)p_tr - (double)K * (double)eta_bar * dg;
+      real sc = (real)(1.0 - ((double)G * dg) / (double)sqrtJ2);
+      for (int k = 0; k < 9; k++) s_next[k] = (real)(sc * s_tr[k]);
+      pc_next = dpc_pc(v0, pc_prev, lam, kap, (real)al, a_prev);
+      a_next = (real)((real)((real)pc_next + Pt) / (real)(1 + beta));
+    }
+  }
+  if (!done && phi_cap > (real)0.0 && p_next < a_next) {
+    double dgam = 0.0, alv = a_prev, tol = 1e-1, conv;
+    double MM = (double)(real)(M * M), six_g = (double)(real)(6 * G), m12g = (double)(real)(-12 * G);
+    int counter = 0;
+    do {
+      double dgn = dgam;
+      al = alv;
+      p_next = (double)p_tr + (double)K * (al - (double)a_prev);
+      double q_next = (MM / (MM + six_g * dgn)) * (double)q_tr;
+      pc_next = dpc_pc(v0, pc_prev, lam, kap, (real)al, a_prev);
+      a_next = (real)((real)((real)pc_next + Pt) / (real)(1 + beta));
+      double b_next = (real)p_next < (real)(Pt - (real)a_next) ? (double)beta : 1.0;
+      real cs = (real)(MM / (MM + six_g * dgn));
+      for (int k = 0; k < 9; k++) s_next[k] = (real)(cs * s_tr[k]);
+      double R0 = (double)dpc_cap_yield((real)p_next, Pt, (real)a_next, (real)q_next, (real)b_next, M);
+      double R1 = al - (double)a_prev + dgn * (2.0 / (b_next * b_next)) * (p_next - (double)Pt + a_next);
+      double dPc = pc_next * ((double)v0 / ((double)lam - (double)kap));
+      double H = dPc / (1.0 + (double)beta);
+      double pbar = p_next - (double)Pt + a_next;
+      double d00 = (m12g / (MM + six_g * dgn)) * (q_next / (double)M) * (q_next / (double)M);
+      double d01 = ((2.0 * pbar) / (b_next * b_next)) * ((double)K + H) - 2.0 * a_next * H;
+      double d10 = (2.0 * pbar) / (b_next * b_next);
+      double d11 = 1.0 + ((2.0 * dgn) / (b_next * b_next)) * ((double)K + H);
+      double inv_det = 1.0 / (d00 * d11 - d01 * d10);
+      double i00 = d11 * inv_det, i01 = -d01 * inv_det, i10 = -d10 * inv_det, i11 = d00 * inv_det;
+      dgam = dgn - (i00 * R0 + i01 * R1);
+      alv = al - (i10 * R0 + i11 * R1);
+      conv = sqrt(R0 * R0 + R1 * R1);
+      counter++;
+      if (counter > 1000) tol *= 10.0;
+    } while (conv > tol && counter < 1400);
+  }
+  real pn = (real)p_next;
+  for (int k = 0; k < 9; k++) sig[k] = s_next[k];
+  sig[0] = (real)(sig[0] + pn);
+  sig[4] = (real)(sig[4] + pn);
+  sig[8] = (real)(sig[8] + pn);
+  real dpk = (real)((p_next - (double)p_ref) / (3.0 * (double)K));
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) {
+      real e = (real)((real)(s_next[3 * a + b] - s_ref[3 * a + b]) / two_g);
+      if (a == b) e = (real)(e + dpk);
+      eps_e[a * d + b] = e;
+    }
+  *alpha = (real)al;
+  *pc = (real)pc_next;
+}
+
 void or_stress_update(or_sim *s) {
   int d = s->grid.dim;
   for (int mid = 0; mid < s->num_materials; mid++) {
@@ -1312,7 +1467,10 @@ void or_stress_update(or_sim *s) {
         vm_point(L, sig, s->eps_e + (size_t)i * 9, s->acc_eps_p + i, s->dt, m);
       } else if (m->type == OR_MAT_MODIFIED_CAM_CLAY) {
         or_mcc_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->acc_eps_p + i,
-                  s->pc + i, s->volumes[i], s->dt, m);
+                     s->pc + i, s->volumes[i], s->dt, m);
+      } else if (m->type == OR_MAT_DRUCKER_PRAGER_CAP) {
+        or_dpc_point(d, L, sig, s->eps_e + (size_t)i * d * d, s->stress_ref + (size_t)i * 9, s->acc_eps_p + i,
+                     s->pc + i, s->volumes_original[i], s->dt, m);
       }
     }
   }

@@ -39,7 +39,8 @@ enum {
   OR_MAT_NEWTON_FLUID = 2,
   OR_MAT_DRUCKER_PRAGER = 3,
   OR_MAT_VON_MISES = 4,      /* p = {K, G, yield_stress, H}; 3D only */
-  OR_MAT_MODIFIED_CAM_CLAY = 5 /* p = {K, G, M, lam, kap, Vs, Pt, R} */
+  OR_MAT_MODIFIED_CAM_CLAY = 5, /* p = {K, G, M, lam, kap, Vs, Pt, R} */
+  OR_MAT_DRUCKER_PRAGER_CAP = 6 /* p = {K, G, M, lam, kap, Vs, Pt, R, beta, eta_bar} */
 };
 
 /* Boundary-condition ids. */
@@ -74,7 +75,7 @@ typedef struct {
 typedef struct {
   int type;
   REAL density;
-  REAL p[8];
+  REAL p[12];
 } or_material;
 
 /* Boundary-condition parameters (state that the reference mutates, the
@@ -179,6 +180,9 @@ void or_dp_point(int dim, const REAL *L, REAL *stress, REAL *eps_e, const REAL *
  * particle's current volume). */
 void or_mcc_point(int dim, const REAL *L, REAL *stress, REAL *eps_e, const REAL *stress_ref, REAL *alpha, REAL *pc,
                   REAL V, REAL dt, const or_material *m);
+/* One Drucker-Prager cap update of a single material point (V0: original volume). */
+void or_dpc_point(int dim, const REAL *L, REAL *stress, REAL *eps_e, const REAL *stress_ref, REAL *alpha, REAL *pc,
+                  REAL V0, REAL dt, const or_material *m);
 
 #ifdef __cplusplus
 }

@@ -52,7 +52,7 @@ class PmpmError(RuntimeError):
 
 
 class Material(ctypes.Structure):
-    _fields_ = [("type", ctypes.c_int), ("density", ctypes.c_float), ("params", ctypes.c_float * 8)]
+    _fields_ = [("type", ctypes.c_int), ("density", ctypes.c_float), ("params", ctypes.c_float * 12)]
 
 
 class BC(ctypes.Structure):
@@ -86,7 +86,7 @@ EXPORTS = [
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
     "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
-    "pmpm_material_modified_cam_clay",
+    "pmpm_material_modified_cam_clay", "pmpm_material_drucker_prager_cap",
 ]
 
 EXPORTS += [
@@ -132,6 +132,7 @@ def lib():
     L.pmpm_autotune.argtypes = [vp, i, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_material_von_mises.argtypes = [f, f, f, f, f, ctypes.POINTER(Material)]
     L.pmpm_material_modified_cam_clay.argtypes = [f] * 10 + [ctypes.POINTER(Material)]
+    L.pmpm_material_drucker_prager_cap.argtypes = [f] * 11 + [ctypes.POINTER(Material)]
     L.pmpm_material_point_vjp.argtypes = [ctypes.POINTER(Material), i, i, f] + [vp] * 11 + [i, i]
     L.pmpm_rollout_reset.argtypes = [vp]
     L.pmpm_rollout_backward.argtypes = [vp, vp, i, vp, vp, vp, vp]
@@ -216,6 +217,10 @@ def make_material(m: dict) -> Material:
         check(L.pmpm_material_modified_cam_clay(m["density"], m["E"], m.get("pois", 0.0), m["M"], m["lam"], m["kap"],
                                                 m["Vs"], m["R"], m.get("Pt", 0.0), m.get("beta", 1.0),
                                                 ctypes.byref(out)), "material")
+    elif t == "DruckerPragerCap":
+        check(L.pmpm_material_drucker_prager_cap(m["density"], m["E"], m.get("pois", 0.0), m["M"], m["lam"],
+                                                 m["kap"], m["Vs"], m["R"], m.get("Pt", 0.0), m.get("beta", 1.0),
+                                                 m.get("dilatancy_angle", 0.0), ctypes.byref(out)), "material")
     elif t == "DP_rheo":
         check(L.pmpm_material_dp_rheo(m["density"], m["E"], m.get("pois", 0.0), m["M"], m.get("Pt", 0.0),
                                       m.get("dilatancy_angle", 0.0), ctypes.byref(out)), "material")

@@ -274,6 +274,27 @@ PYBIND11_MODULE(PMPM_MODULE, m) {
       .def_static("calculate_timestep", &ModifiedCamClay::calculate_timestep, py::arg("cell_size"), py::arg("factor"),
                   py::arg("bulk_modulus"), py::arg("shear_modulus"), py::arg("density"));
 
+  py::class_<DruckerPragerCap>(m, "DruckerPragerCap", py::dynamic_attr())
+      .def(py::init<float, float, float, float, float, float, float, float, float, float, float>(), py::arg("density"),
+           py::arg("E"), py::arg("pois"), py::arg("M"), py::arg("lam"), py::arg("kap"), py::arg("Vs"), py::arg("R"),
+           py::arg("Pt"), py::arg("beta"), py::arg("dilatancy_angle") = 0.0f)
+      .def("initialize",
+           [](DruckerPragerCap &, ParticlesContainer particles, int mat_id) { return py::make_tuple(particles, mat_id); },
+           py::arg("particles"), py::arg("mat_id") = 0)
+      .def_readwrite("density", &DruckerPragerCap::density)
+      .def_readonly("E", &DruckerPragerCap::E)
+      .def_readonly("pois", &DruckerPragerCap::pois)
+      .def_readonly("M", &DruckerPragerCap::M)
+      .def_readonly("lam", &DruckerPragerCap::lam)
+      .def_readonly("kap", &DruckerPragerCap::kap)
+      .def_readonly("Vs", &DruckerPragerCap::Vs)
+      .def_readonly("R", &DruckerPragerCap::R)
+      .def_readonly("Pt", &DruckerPragerCap::Pt)
+      .def_readonly("beta", &DruckerPragerCap::beta)
+      .def_readonly("dilatancy_angle", &DruckerPragerCap::dilatancy_angle)
+      .def_readonly("bulk_modulus", &DruckerPragerCap::bulk_modulus)
+      .def_readonly("shear_modulus", &DruckerPragerCap::shear_modulus);
+
   py::class_<BoundaryCondition>(m, "BoundaryCondition").def(py::init<>());
   py::class_<Gravity>(m, "Gravity", py::dynamic_attr())
       .def(py::init([](py::object g, bool is_ramp, int ramp_step, py::object ge) {

@@ -447,7 +447,22 @@ struct ModifiedCamClay {
     return dt;
   }
 };
-using MaterialType = std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager, VonMises, ModifiedCamClay>;
+// DruckerPragerCap (src/materials/druckerprager_cap.cpp:43-67): the
+// ModifiedCamClay parameters plus the dilatancy angle in degrees
+struct DruckerPragerCap : ModifiedCamClay {
+  DruckerPragerCap(Real density, Real E, Real pois, Real M, Real lam, Real kap, Real Vs, Real R, Real Pt, Real beta,
+                   Real dilatancy_angle)
+      : ModifiedCamClay(density, E, pois, M, lam, kap, Vs, R, Pt, beta), dilatancy_angle(dilatancy_angle) {}
+  Real dilatancy_angle;
+  pmpm_material desc() const {
+    pmpm_material m;
+    check(pmpm_material_drucker_prager_cap(density, E, pois, M, lam, kap, Vs, R, Pt, beta, dilatancy_angle, &m),
+          "DruckerPragerCap");
+    return m;
+  }
+};
+using MaterialType =
+    std::variant<Material, LinearElastic, NewtonFluid, DruckerPrager, VonMises, ModifiedCamClay, DruckerPragerCap>;
 
 struct BoundaryCondition {
   bool isActive = true;

@@ -129,7 +129,7 @@ struct pmpm_sim {
   } ro;
   bool has_planar = false, has_dp = false, has_sref = false;
   bool has_vm = false;  // a VonMises material: elastic strain and accumulated plastic strain
-  bool has_mcc = false; // a Modified Cam Clay material: elastic strain, alpha and pc
+  bool has_mcc = false; // a Modified Cam Clay or Drucker-Prager cap material: elastic strain, alpha, pc
 
   // particles (two storage sets, swapped by the physical re-sort)
   int n = 0, stride = 0;
@@ -670,9 +670,10 @@ __global__ void k_dp_init(DevParticles P, int D, int *nonzero_ref) {
   if (nz) atomicOr(nonzero_ref, 1);
 }
 
-// ModifiedCamClay::initialize (src/materials/modifiedcamclay.cpp:68-108), the
-// part that is not the shared history reset of k_dp_init: per particle of a
-// Modified Cam Clay colour, alpha = 0 and pc = R p0 with p0 = -tr(sigma)/3
+// ModifiedCamClay::initialize (src/materials/modifiedcamclay.cpp:68-108) and
+// DruckerPragerCap::initialize (src/materials/druckerprager_cap.cpp:72-108),
+// the part that is not the shared history reset of k_dp_init: per particle of
+// a Modified Cam Clay or Drucker-Prager cap colour, alpha = 0 and pc = R p0 with p0 = -tr(sigma)/3
 // (the reference applies one material's R to every particle; here each
 // particle takes its own material's).
 __global__ void k_mcc_init(StepArgs a, int D) {
@@ -681,7 +682,7 @@ __global__ void k_mcc_init(StepArgs a, int D) {
   const int st = a.P.stride;
   const int c = a.P.color[s];
   float pc = 0.0f;
-  if (c < a.nmat && a.mat[c].type == PMPM_MAT_MODIFIED_CAM_CLAY) {
+  if (c < a.nmat && (a.mat[c].type == PMPM_MAT_MODIFIED_CAM_CLAY || a.mat[c].type == PMPM_MAT_DRUCKER_PRAGER_CAP)) {
     const float sxx = a.P.sig[0 * st + s], syy = a.P.sig[1 * st + s];
     const float szz = a.P.sig[(D == 2 ? 3 : 2) * st + s];
     const float p0 = (float)(-(double)((sxx + syy) + szz) / 3.0);
@@ -909,6 +910,17 @@ int pmpm_material_modified_cam_clay(float density, float E, float pois, float M,
   return PMPM_OK;
 }
 
+int pmpm_material_drucker_prager_cap(float density, float E, float pois, float M, float lam, float kap, float Vs,
+                                     float R, float Pt, float beta, float dilatancy_deg, pmpm_material *out) {
+  PMPM_TRY(pmpm_material_modified_cam_clay(density, E, pois, M, lam, kap, Vs, R, Pt, beta, out));
+  if (!(1.0f + beta != 0.0f)) return PMPM_ERR_INVALID_ARGUMENT;
+  out->type = PMPM_MAT_DRUCKER_PRAGER_CAP;
+  const double psi = (double)dilatancy_deg * 3.14159265358979323846 / 180.0;
+  out->params[8] = beta;
+  out->params[9] = (float)(6.0 * std::sin(psi) / (std::sqrt(3.0) * (3.0 + std::sin(psi))));
+  return PMPM_OK;
+}
+
 int pmpm_material_dp_rheo(float density, float E, float pois, float M, float Pt, float dilatancy_deg,
                           pmpm_material *out) {
   if (!out) return PMPM_ERR_INVALID_ARGUMENT;
@@ -1038,6 +1050,7 @@ int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float fact
     case PMPM_MAT_DRUCKER_PRAGER:
     case PMPM_MAT_VON_MISES:
     case PMPM_MAT_MODIFIED_CAM_CLAY:
+    case PMPM_MAT_DRUCKER_PRAGER_CAP:
       return pmpm_calculate_timestep(cell_size, factor, mat->params[0], mat->params[1], mat->density, dt);
     default:
       return PMPM_ERR_NOT_SUPPORTED;
@@ -1090,8 +1103,8 @@ static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
   // materials
   for (int k = 0; k < desc->num_materials; k++) {
     const pmpm_material &m = desc->materials[k];
-    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_MODIFIED_CAM_CLAY) return PMPM_ERR_INVALID_ARGUMENT;
-    if (m.type == PMPM_MAT_MODIFIED_CAM_CLAY) {
+    if (m.type < PMPM_MAT_NONE || m.type > PMPM_MAT_DRUCKER_PRAGER_CAP) return PMPM_ERR_INVALID_ARGUMENT;
+    if (m.type == PMPM_MAT_MODIFIED_CAM_CLAY || m.type == PMPM_MAT_DRUCKER_PRAGER_CAP) {
       s->has_mcc = true;
       s->has_dp = true;  // elastic strain and reference stress
     }

@@ -105,9 +105,10 @@ struct DevBins {
 struct DevMaterial {
   int type;
   float density;
-  // p[0..7]: the pmpm_material parameters; Drucker-Prager (friction-angle
-  // form) also p[8] = cohesion, for per-particle parameters
-  float p[10];
+  // p[0..11]: the pmpm_material parameters; Drucker-Prager (friction-angle
+  // form, which uses p[0..7]) also p[8] = cohesion, p[9] = friction angle,
+  // for per-particle parameters
+  float p[12];
 };
 
 struct DevBC {
@@ -727,6 +728,144 @@ __device__ __forceinline__ void mcc_update(const float *prm, const float *L, flo
     for (int b = 0; b < D; b++) eps[a * D + b] = (s_tr[3 * a + b] - s_ref[3 * a + b]) / two_g - (a == b ? evol : 0.0f);
   alpha = (float)a_next;
   pc = (float)(2.0 * ps - Ptd);
+}
+
+// Drucker-Prager cone with a cap: update_druckerpragercap
+// (src/materials/druckerprager_cap_inline.h:370-554) with return_mapping_cone
+// (:124-141), return_mapping_apex (:143-156), return_mapping_cap (:159-235),
+// compute_pc / compute_a / compute_b (:56-84), the yield functions (:94-111)
+// and update_plasticity (:328-346).  Pressure p = tr(sigma)/3 (tension
+// positive).  Cone: sqrt(J2) + eta (p - Pt), eta = M / sqrt(3); cap:
+// (p - Pt + a)^2 / b^2 + (q/M)^2 - a^2 with a = (pc + Pt) / (1 + beta) and
+// b = beta beyond the cap's centre (p < Pt - a), else 1; hardening
+// pc = pc_prev exp(v0 / (lam - kap) (alpha - alpha_prev)), v0 = V0 / Vs.
+// The cone return is closed form; past the apex the stress goes to p = Pt,
+// s = 0 (the apex's eta_bar dgamma is (p_tr - Pt) / K; the reference divides
+// by eta_bar and multiplies back, which is 0/0 for eta_bar = 0, where this
+// keeps the limit).  The cap return is the reference's Newton iteration on
+// (dgamma, alpha) from the trial state, in FP64, until |R| <= 0.1 with the
+// bound growing tenfold per iteration after 1000; its results are the last
+// evaluated iterate's.  V0: the particle's original volume.
+template <int D>
+__device__ __forceinline__ void dpc_update(const float *prm, const float *L, float dt, float V0, float eps[9],
+                                           const float sref[9], float S[9], float &alpha, float &pc) {
+  const float K = prm[0], G = prm[1], M = prm[2], lam = prm[3], kap = prm[4], Vs = prm[5], Pt = prm[6];
+  const float beta = prm[8], eta_bar = prm[9];
+  float deps[9];
+  corotational_increment<D>(L, dt, eps, deps);
+  const float p_ref = (1.0f / 3.0f) * ((sref[0] + sref[4]) + sref[8]);
+  float s_ref[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) s_ref[k] = sref[k];
+  s_ref[0] -= p_ref;
+  s_ref[4] -= p_ref;
+  s_ref[8] -= p_ref;
+  float eps_tr[9], ev = 0.0f;
+#pragma unroll
+  for (int k = 0; k < D * D; k++) eps_tr[k] = eps[k] + deps[k];
+#pragma unroll
+  for (int a = 0; a < D; a++) ev += eps_tr[a * D + a];
+  const float p_tr = p_ref + K * ev;
+  float edev[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) edev[k] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) edev[3 * a + b] = eps_tr[a * D + b];
+#pragma unroll
+  for (int a = 0; a < 3; a++) edev[3 * a + a] -= (1.0f / 3.0f) * ev;
+  if (D < 3) edev[8] = 0.0f;
+  float s_tr[9], ss = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    s_tr[k] = s_ref[k] + 2.0f * G * edev[k];
+    ss += s_tr[k] * s_tr[k];
+  }
+  const float J2 = 0.5f * ss;
+  const float q_tr = sqrtf(3.0f * J2);
+  const float sqrtJ2 = sqrtf(J2);
+  const float eta = 0.57735026918962576f * M;
+  const float phi_cone = sqrtJ2 + eta * (p_tr - Pt);
+  const double C = ((double)V0 / (double)Vs) / ((double)lam - (double)kap);
+  const float a_tr = (pc + Pt) / (1.0f + beta);
+  const float b_tr = p_tr < Pt - a_tr ? beta : 1.0f;
+  const float phi_cap =
+      (float)((1.0 / ((double)b_tr * b_tr)) * (double)(p_tr - Pt + a_tr) * (double)(p_tr - Pt + a_tr) +
+              (double)((q_tr / M) * (q_tr / M)) - (double)(a_tr * a_tr));
+  if (phi_cone <= 0.0f && phi_cap <= 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) S[k] = s_tr[k] + ((k == 0 || k == 4 || k == 8) ? p_tr : 0.0f);
+#pragma unroll
+    for (int k = 0; k < D * D; k++) eps[k] = eps_tr[k];
+    return;
+  }
+  const double Kd = K, Gd = G, Md = M, MM = Md * Md, Ptd = Pt, a_prev = alpha, pc_prev = pc;
+  double p = p_tr, pcn = pc_prev, an = a_tr, al = a_prev;
+  float s[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) s[k] = s_tr[k];
+  bool done = false;
+  if (phi_cone > 0.0f) {
+    const double dg = (double)phi_cone / (Kd * (double)eta * (double)eta_bar + Gd);
+    if ((double)sqrtJ2 - Gd * dg < 0.0) {
+      const double edg = ((double)p_tr - Ptd) / Kd;
+      al = a_prev - edg;
+      p = (double)p_tr - Kd * edg;
+#pragma unroll
+      for (int k = 0; k < 9; k++) s[k] = 0.0f;
+      pcn = exp(C * (al - a_prev)) * pc_prev;
+      done = true;
+    } else {
+      al = a_prev - (double)eta_bar * dg;
+      p = (double)p_tr - Kd * (double)eta_bar * dg;
+      const float sc = (float)(1.0 - (Gd * dg) / (double)sqrtJ2);
+#pragma unroll
+      for (int k = 0; k < 9; k++) s[k] = sc * s_tr[k];
+      pcn = exp(C * (al - a_prev)) * pc_prev;
+      an = (pcn + Ptd) / (1.0 + (double)beta);
+    }
+  }
+  if (!done && phi_cap > 0.0f && p < an) {
+    double dgam = 0.0, alv = a_prev, tol = 0.1;
+    for (int it = 1; it <= 1400; it++) {
+      al = alv;
+      p = (double)p_tr + Kd * (al - a_prev);
+      const double c = MM / (MM + 6.0 * Gd * dgam);
+      const double q = c * (double)q_tr;
+      pcn = exp(C * (al - a_prev)) * pc_prev;
+      an = (pcn + Ptd) / (1.0 + (double)beta);
+      const double b = p < Ptd - an ? (double)beta : 1.0;
+      const float cf = (float)c;
+#pragma unroll
+      for (int k = 0; k < 9; k++) s[k] = cf * s_tr[k];
+      const double pbar = p - Ptd + an;
+      const double R0 = pbar * pbar / (b * b) + (q / Md) * (q / Md) - an * an;
+      const double R1 = al - a_prev + dgam * (2.0 / (b * b)) * pbar;
+      const double H = pcn * C / (1.0 + (double)beta);
+      const double d00 = (-12.0 * Gd / (MM + 6.0 * Gd * dgam)) * (q / Md) * (q / Md);
+      const double d01 = (2.0 * pbar / (b * b)) * (Kd + H) - 2.0 * an * H;
+      const double d10 = 2.0 * pbar / (b * b);
+      const double d11 = 1.0 + (2.0 * dgam / (b * b)) * (Kd + H);
+      const double det = d00 * d11 - d01 * d10;
+      dgam -= (d11 * R0 - d01 * R1) / det;
+      alv -= (d00 * R1 - d10 * R0) / det;
+      const double conv = sqrt(R0 * R0 + R1 * R1);
+      if (it > 1000) tol *= 10.0;
+      if (!(conv > tol)) break;
+    }
+  }
+  const float pn = (float)p;
+  const float dpk = (float)((p - (double)p_ref) / (3.0 * Kd));
+  const float two_g = (float)(2.0 * Gd);
+#pragma unroll
+  for (int k = 0; k < 9; k++) S[k] = s[k] + ((k == 0 || k == 4 || k == 8) ? pn : 0.0f);
+#pragma unroll
+  for (int a = 0; a < D; a++)
+#pragma unroll
+    for (int b = 0; b < D; b++) eps[a * D + b] = (s[3 * a + b] - s_ref[3 * a + b]) / two_g + (a == b ? dpk : 0.0f);
+  alpha = (float)al;
+  pc = (float)pcn;
 }
 
 // --------------------------------------------------------------------------

@@ -1866,7 +1866,7 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
 #pragma unroll
       for (int y = x; y < 3; y++) P.eps[eps_index<3>(x, y) * st + s] = eps[3 * x + y];
     P.acc[s] = acc;
-  } else if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY) {
+  } else if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY || mt.type == PMPM_MAT_DRUCKER_PRAGER_CAP) {
     float eps[9], sref[9];
 #pragma unroll
     for (int x = 0; x < D; x++)
@@ -1881,7 +1881,10 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
       }
     load_sig3<D>(P, s, S);
     float alpha = P.acc[s], pc = P.pc[s];
-    mcc_update<D>(mt.p, L, a.dt, P.V[s], eps, sref, S, alpha, pc);
+    if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY)
+      mcc_update<D>(mt.p, L, a.dt, P.V[s], eps, sref, S, alpha, pc);
+    else
+      dpc_update<D>(mt.p, L, a.dt, P.V0[s], eps, sref, S, alpha, pc);
 #pragma unroll
     for (int x = 0; x < D; x++)
 #pragma unroll

@@ -1,4 +1,5 @@
-"""Modified Cam Clay on the sm_100a path against the CPU oracle.
+"""Modified Cam Clay and Drucker-Prager cap on the sm_100a path against the
+CPU oracle.
 
 Two levels, as the reference's constitutive analyses and its USL solver use
 the material: repeated stress updates of material points under fixed
@@ -15,7 +16,10 @@ import pytest
 import oracle
 from pyroclastmpm_b200 import Simulation
 
+from test_dpc_oracle import DPC
 from test_mcc_oracle import MCC, assert_strain_close
+
+MATERIALS = {"mcc": MCC, "dpc": DPC}
 
 pytestmark = pytest.mark.gpu
 
@@ -28,7 +32,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
 
 
-def block(dim, shape_function, seed=3, R=1.0, n=None):
+def block(dim, shape_function, seed=3, R=1.0, n=None, material="mcc"):
     rng = np.random.default_rng(seed)
     n = n or (4000 if dim == 3 else 2000)
     h = 0.1
@@ -37,7 +41,7 @@ def block(dim, shape_function, seed=3, R=1.0, n=None):
     g[-1] = -9.81
     return dict(dim=dim, origin=[0.0] * dim, end=[1.0] * dim, cell_size=h, shape_function=shape_function,
                 dt=1e-4, particles_per_cell=2 ** dim, alpha=0.99,
-                materials=[dict(MCC, Vs=V / 1.8, R=R)],
+                materials=[dict(MATERIALS[material], Vs=V / 1.8, R=R)],
                 bcs=[{"type": "Gravity", "gravity": g},
                      {"type": "NodeDomain", "face0_mode": [1] * dim, "face1_mode": [1] * dim}],
                 positions=rng.uniform(0.15, 0.85, (n, dim)), velocities=rng.normal(0, 0.2, (n, dim)),
@@ -93,9 +97,10 @@ def oracle_fields(o):
             "positions": o["positions"], "velocities": o["velocities"], "F": o["F"], "volumes": o["volumes"]}
 
 
+@pytest.mark.parametrize("material", ["mcc", "dpc"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_material_point_updates_match_oracle(dim):
-    scene = block(dim, "linear", seed=5 + dim, R=1.1)
+def test_material_point_updates_match_oracle(dim, material):
+    scene = block(dim, "linear", seed=5 + dim, R=1.1, material=material)
     n = len(scene["positions"])
     L = point_loads(n, dim, seed=dim)
     sim = make_gpu(scene)
@@ -115,9 +120,10 @@ def test_material_point_updates_match_oracle(dim):
     assert_strain_close(sim.get("eps_e"), f64["eps_e"], max(1e-4, 3.0 * rel(f32["eps_e"], f64["eps_e"])))
 
 
+@pytest.mark.parametrize("material", ["mcc", "dpc"])
 @pytest.mark.parametrize("dim,shape_function", [(2, "linear"), (2, "quadratic"), (3, "quadratic"), (3, "linear")])
-def test_usl_steps_match_oracle(dim, shape_function):
-    scene = block(dim, shape_function)
+def test_usl_steps_match_oracle(dim, shape_function, material):
+    scene = block(dim, shape_function, material=material)
     steps = 4
     sim = make_gpu(scene)
     refs = {p: make_oracle(scene, p) for p in ("f32", "f64")}
@@ -134,11 +140,12 @@ def test_usl_steps_match_oracle(dim, shape_function):
     assert_strain_close(sim.get("eps_e"), f64["eps_e"], max(1e-4, 3.0 * rel(f32["eps_e"], f64["eps_e"])))
 
 
-def test_rejected_where_unsupported():
-    """Batched ensembles and differentiable rollouts take no Modified Cam Clay."""
+@pytest.mark.parametrize("material", ["mcc", "dpc"])
+def test_rejected_where_unsupported(material):
+    """Differentiable rollouts take neither material."""
     from pyroclastmpm_b200._capi import PmpmError
 
-    scene = block(3, "quadratic", n=500)
+    scene = block(3, "quadratic", n=500, material=material)
     sim = make_gpu(scene)
     with pytest.raises(PmpmError):
         sim.rollout_forward(4, 2)

@@ -6,7 +6,7 @@ NAMES = ["set_globals", "set_global_shapefunction", "set_global_timestep", "set_
          "set_global_output_directory", "NodesContainer", "ParticlesContainer", "Solver", "USL",
          "Material", "LinearElastic", "NewtonFluid", "DruckerPrager", "BoundaryCondition", "Gravity",
          "NodeDomain", "BodyForce", "PlanarDomain", "RigidBodyLevelSet", "calculate_timestep", "MUSL",
-         "VonMises", "ModifiedCamClay", "global_dimension"]
+         "VonMises", "ModifiedCamClay", "DruckerPragerCap", "global_dimension"]
 
 
 @pytest.mark.parametrize("dim", [2, 3])
