@@ -427,11 +427,15 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
     static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
     if (!attr_set[dev]) {
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
       attr_set[dev] = true;
     }
     if (s->p2g_variant == 1) {
-      k_p2g_dual3<<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+      if (s->has_planar)
+        k_p2g_dual3<true><<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+      else
+        k_p2g_dual3<false><<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
     } else {
       constexpr int cbytes = cells3_smem_bytes();
       static bool cattr_set[64] = {false};  // per device
@@ -466,7 +470,10 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
 template <int D, int SF>
 int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
   StepArgs a = make_args(s);
-  k_g2p<D, SF><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
+  if (s->has_vm || s->has_mcc)
+    k_g2p<D, SF, true><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
+  else
+    k_g2p<D, SF, false><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
   PMPM_LAUNCHED();
   s->launches += 1;
   s->rigid_shift_pending = false;

@@ -1418,6 +1418,8 @@ __device__ __forceinline__ void tile_epilogue3(const StepArgs &a, int apply_bcs,
   }
 }
 
+// PLANAR: the handle has a PlanarDomain (per-particle external forces to map)
+template <bool PLANAR>
 __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
   using W = Dual3;
   using T = TileDims<3>;
@@ -1545,7 +1547,7 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             st_mv[c][jj] = m * P.v[c * st + s];
-            st_f[c][jj] = (a.has_planar && !a.remap) ? P.fext[c * st + s] : 0.0f;
+            if (PLANAR) st_f[c][jj] = a.remap ? 0.0f : P.fext[c * st + s];
           }
 #pragma unroll
           for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
@@ -1565,7 +1567,7 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
           const int vc = item_cell[q];
           const int j0 = max(pref[vc] - base, c0) - c0 + vc, j1 = min(pref[vc + 1] - base, c1) - c0 + vc;
           const float xn = item_xn[q], yn = item_yn[q];
-          for (int j = j0; j < j1; j++) {
+          auto add = [&](int j) {
             float Nx, dNx, Ny, dNy;
             axis_weight<PMPM_SHAPE_QUADRATIC>(st_u[0][j] - xn, g.inv_h, 0, Nx, dNx);
             axis_weight<PMPM_SHAPE_QUADRATIC>(st_u[1][j] - yn, g.inv_h, 0, Ny, dNy);
@@ -1575,9 +1577,14 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
             const float nn = Nx * Ny;
             const float gx = dNx * Ny, gy = Nx * dNy;
             // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
-            const float Ax = st_f[0][j] * nn + Sxx * gx + Sxy * gy;
-            const float Ay = st_f[1][j] * nn + Sxy * gx + Syy * gy;
-            const float Az = st_f[2][j] * nn + Sxz * gx + Syz * gy;
+            float Ax = Sxx * gx + Sxy * gy;
+            float Ay = Sxy * gx + Syy * gy;
+            float Az = Sxz * gx + Syz * gy;
+            if (PLANAR) {
+              Ax += st_f[0][j] * nn;
+              Ay += st_f[1][j] * nn;
+              Az += st_f[2][j] * nn;
+            }
             const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
             const float mn = m * nn, mvxn = st_mv[0][j] * nn, mvyn = st_mv[1][j] * nn, mvzn = st_mv[2][j] * nn;
 #pragma unroll
@@ -1591,7 +1598,14 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
               win[q][k][5] += Ay * Nz + By * dNz;
               win[q][k][6] += Az * Nz + Bz * dNz;
             }
+          };
+          // two particles per pass: the second's shared-memory loads overlap the first's arithmetic
+          int j = j0;
+          for (; j + 1 < j1; j += 2) {
+            add(j);
+            add(j + 1);
           }
+          if (j < j1) add(j);
         }
         __syncthreads();
       }
@@ -1837,7 +1851,11 @@ __device__ __forceinline__ float det_rows(const float *A) {
 
 // Material update of storage slot s from velocity gradient L
 // (Solver::stress_update, src/solver/solver.cpp:110-121; materials by colour).
-template <int D>
+// FULL = false leaves out the iterative materials (VonMises, Modified Cam
+// Clay, Drucker-Prager cap): launches whose handle holds none of them use it,
+// so their FP64 Newton code does not raise the register count of the common
+// kernels.
+template <int D, bool FULL = true>
 __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, const float *L) {
   const DevParticles &P = a.P;
   const int color = P.color[s];
@@ -1853,44 +1871,51 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
   } else if (mt.type == PMPM_MAT_NEWTON_FLUID) {
     nf_update<D>(mt, L, P.m[s], P.V[s], P.V0[s], S);
   } else if (mt.type == PMPM_MAT_VON_MISES) {
-    if (D != 3) return;  // 3D only (rejected at create)
-    float eps[9];
+    if constexpr (D == 3 && FULL) {  // 3D only (rejected at create)
+      float eps[9];
 #pragma unroll
-    for (int x = 0; x < 3; x++)
+      for (int x = 0; x < 3; x++)
 #pragma unroll
-      for (int y = 0; y < 3; y++) eps[3 * x + y] = P.eps[eps_index<3>(x, y) * st + s];
-    float acc = P.acc[s];
-    vm_update(mt.p, L, a.dt, eps, acc, S);
+        for (int y = 0; y < 3; y++) eps[3 * x + y] = P.eps[eps_index<3>(x, y) * st + s];
+      float acc = P.acc[s];
+      vm_update(mt.p, L, a.dt, eps, acc, S);
 #pragma unroll
-    for (int x = 0; x < 3; x++)
+      for (int x = 0; x < 3; x++)
 #pragma unroll
-      for (int y = x; y < 3; y++) P.eps[eps_index<3>(x, y) * st + s] = eps[3 * x + y];
-    P.acc[s] = acc;
+        for (int y = x; y < 3; y++) P.eps[eps_index<3>(x, y) * st + s] = eps[3 * x + y];
+      P.acc[s] = acc;
+    } else {
+      return;
+    }
   } else if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY || mt.type == PMPM_MAT_DRUCKER_PRAGER_CAP) {
-    float eps[9], sref[9];
+    if constexpr (FULL) {
+      float eps[9], sref[9];
 #pragma unroll
-    for (int x = 0; x < D; x++)
+      for (int x = 0; x < D; x++)
 #pragma unroll
-      for (int y = 0; y < D; y++) eps[x * D + y] = P.eps[eps_index<D>(x, y) * st + s];
+        for (int y = 0; y < D; y++) eps[x * D + y] = P.eps[eps_index<D>(x, y) * st + s];
 #pragma unroll
-    for (int x = 0; x < 3; x++)
+      for (int x = 0; x < 3; x++)
 #pragma unroll
-      for (int y = 0; y < 3; y++) {
-        const int k = sig_index<D>(x, y);
-        sref[3 * x + y] = (k < 0 || !a.has_sref) ? 0.0f : P.sref[k * st + s];
-      }
-    load_sig3<D>(P, s, S);
-    float alpha = P.acc[s], pc = P.pc[s];
-    if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY)
-      mcc_update<D>(mt.p, L, a.dt, P.V[s], eps, sref, S, alpha, pc);
-    else
-      dpc_update<D>(mt.p, L, a.dt, P.V0[s], eps, sref, S, alpha, pc);
+        for (int y = 0; y < 3; y++) {
+          const int k = sig_index<D>(x, y);
+          sref[3 * x + y] = (k < 0 || !a.has_sref) ? 0.0f : P.sref[k * st + s];
+        }
+      load_sig3<D>(P, s, S);
+      float alpha = P.acc[s], pc = P.pc[s];
+      if (mt.type == PMPM_MAT_MODIFIED_CAM_CLAY)
+        mcc_update<D>(mt.p, L, a.dt, P.V[s], eps, sref, S, alpha, pc);
+      else
+        dpc_update<D>(mt.p, L, a.dt, P.V0[s], eps, sref, S, alpha, pc);
 #pragma unroll
-    for (int x = 0; x < D; x++)
+      for (int x = 0; x < D; x++)
 #pragma unroll
-      for (int y = x; y < D; y++) P.eps[eps_index<D>(x, y) * st + s] = eps[x * D + y];
-    P.acc[s] = alpha;
-    P.pc[s] = pc;
+        for (int y = x; y < D; y++) P.eps[eps_index<D>(x, y) * st + s] = eps[x * D + y];
+      P.acc[s] = alpha;
+      P.pc[s] = pc;
+    } else {
+      return;
+    }
   } else {
     float eps[9], sref[9];
 #pragma unroll
@@ -1925,7 +1950,7 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
   store_sig3<D>(P, s, S);
 }
 
-template <int D, int SF>
+template <int D, int SF, bool FULL = true>
 __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress, int store_L) {
   const DevParticles &P = a.P;
   const DevGrid &g = a.g;
@@ -1980,29 +2005,24 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
         }
       }
     }
+    // Separable sums: along x first (per (y, z) row of the stencil), then
+    // weighted by the row's y/z factors.  v_pic = sum psi v_nt,
+    // dv = sum psi (v_nt - v), L = sum grad(psi) v_nt^T.
     float vinc[3] = {0, 0, 0}, dvinc[3] = {0, 0, 0};
     constexpr int KZ = D == 3 ? K : 1;
+    const float4 *vel = reinterpret_cast<const float4 *>(a.N.vel);
 #pragma unroll
-    for (int ky = 0; ky < K; ky++) {
+    for (int kz = 0; kz < KZ; kz++) {
 #pragma unroll
-      for (int kx = 0; kx < K; kx++) {
+      for (int ky = 0; ky < K; ky++) {
+        if (!ok[1][ky] || (D == 3 && !ok[2][kz])) continue;
+        const int row = idx[1][ky] * g.n[0] + (D == 3 ? idx[2][kz] * g.n[0] * g.n[1] : 0);
+        float sv[3] = {0, 0, 0}, sd[3] = {0, 0, 0}, sg[3] = {0, 0, 0};
 #pragma unroll
-        for (int kz = 0; kz < KZ; kz++) {
-          if (!ok[0][kx] || !ok[1][ky] || (D == 3 && !ok[2][kz])) continue;
-          const int node = idx[0][kx] + idx[1][ky] * g.n[0] + (D == 3 ? idx[2][kz] * g.n[0] * g.n[1] : 0);
-          float psi, dpsi[3];
-          if (D == 2) {
-            psi = N[0][kx] * N[1][ky];
-            dpsi[0] = dN[0][kx] * N[1][ky];
-            dpsi[1] = dN[1][ky] * N[0][kx];
-          } else {
-            psi = N[0][kx] * N[1][ky] * N[2][kz];
-            dpsi[0] = dN[0][kx] * N[1][ky] * N[2][kz];
-            dpsi[1] = dN[1][ky] * N[0][kx] * N[2][kz];
-            dpsi[2] = dN[2][kz] * N[0][kx] * N[1][ky];
-          }
+        for (int kx = 0; kx < K; kx++) {
+          if (!ok[0][kx]) continue;
+          const int node = idx[0][kx] + row;
           float vn[3], vnt[3];
-          const float4 *vel = reinterpret_cast<const float4 *>(a.N.vel);
           if (D == 3) {
             const float4 q0 = __ldg(vel + 2 * (size_t)node), q1 = __ldg(vel + 2 * (size_t)node + 1);
             vn[0] = q0.x; vn[1] = q0.y; vn[2] = q0.z;
@@ -2014,13 +2034,21 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
           }
 #pragma unroll
           for (int c = 0; c < D; c++) {
-            dvinc[c] += psi * (vnt[c] - vn[c]);
-            vinc[c] += psi * vnt[c];
+            sv[c] += N[0][kx] * vnt[c];
+            sd[c] += N[0][kx] * (vnt[c] - vn[c]);
+            sg[c] += dN[0][kx] * vnt[c];
           }
+        }
+        const float wyz = D == 3 ? N[1][ky] * N[2][kz] : N[1][ky];
+        const float gyz = D == 3 ? dN[1][ky] * N[2][kz] : dN[1][ky];
+        const float wgz = D == 3 ? N[1][ky] * dN[2][kz] : 0.0f;
 #pragma unroll
-          for (int r = 0; r < D; r++)
-#pragma unroll
-            for (int c = 0; c < D; c++) L[r * D + c] += dpsi[r] * vnt[c];
+        for (int c = 0; c < D; c++) {
+          vinc[c] += wyz * sv[c];
+          dvinc[c] += wyz * sd[c];
+          L[0 * D + c] += wyz * sg[c];
+          L[1 * D + c] += gyz * sv[c];
+          if (D == 3) L[2 * D + c] += wgz * sv[c];
         }
       }
     }
@@ -2086,13 +2114,13 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 #pragma unroll
     for (int k = 0; k < D * D; k++) P.L[k * st + s] = L[k];
   }
-  if (do_stress) stress_update_point<D>(a, s, L);
+  if (do_stress) stress_update_point<D, FULL>(a, s, L);
 }
 
-template <int D, int SF>
-__global__ void __launch_bounds__(256) k_g2p(StepArgs a, int do_stress, int store_L) {
+template <int D, int SF, bool FULL>
+__global__ void __launch_bounds__(256, (SF == PMPM_SHAPE_CUBIC || FULL) ? 2 : 3) k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < a.P.n) g2p_body<D, SF>(a, s, do_stress, store_L);
+  if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
 }
 
 // Stress update alone from the stored velocity gradient.
@@ -2255,7 +2283,7 @@ __global__ void __launch_bounds__(256) kb_g2p(const StepArgs *views, const Batch
   const BatchBlock b = blocks[blockIdx.x];
   load_view(sa, views, b.inst, P, epoch);
   const int s = b.first + (int)threadIdx.x;
-  if (s < b.end) g2p_body<D, SF>(sa, s, do_stress, store_L);
+  if (s < b.end) g2p_body<D, SF, false>(sa, s, do_stress, store_L);  // batches hold no iterative material
 }
 
 }  // namespace pmpm
