@@ -215,18 +215,15 @@ __device__ __forceinline__ void axis_weight(float r, float inv_h, int type, floa
     else
       dN = r > 0.0f ? -inv_h : inv_h;
   } else if (SF == PMPM_SHAPE_QUADRATIC) {
-    float ar = fabsf(r);
-    if (ar < 0.5f) {
-      N = 0.75f - r * r;
-      dN = inv_h * (-2.0f * r);
-    } else if (ar < 1.5f) {
-      float t = 1.5f - ar;
-      N = 0.5f * t * t;
-      dN = inv_h * (r > 0.0f ? -t : t);
-    } else {
-      N = 0.0f;
-      dN = 0.0f;
-    }
+    // both pieces evaluated and selected: no divergence between lanes whose
+    // nodes sit at different stencil offsets
+    const float ar = fabsf(r);
+    const float t = 1.5f - ar;
+    const float n_in = 0.75f - r * r, dn_in = inv_h * (-2.0f * r);
+    const float n_out = 0.5f * t * t, dn_out = inv_h * (r > 0.0f ? -t : t);
+    const bool inner = ar < 0.5f, outer = ar < 1.5f;
+    N = inner ? n_in : (outer ? n_out : 0.0f);
+    dN = inner ? dn_in : (outer ? dn_out : 0.0f);
   } else {
     int k = -1;
     if (r >= -2.0f && r < -1.0f)

@@ -1601,11 +1601,13 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
           };
           // two particles per pass: the second's shared-memory loads overlap the first's arithmetic
           int j = j0;
-          for (; j + 1 < j1; j += 2) {
+          for (; j + 3 < j1; j += 4) {
             add(j);
             add(j + 1);
+            add(j + 2);
+            add(j + 3);
           }
-          if (j < j1) add(j);
+          for (; j < j1; j++) add(j);
         }
         __syncthreads();
       }
