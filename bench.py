@@ -32,6 +32,15 @@ METRIC = "particle-steps/s on 1xB200: plain vs batched vs fwd+adjoint, <=1e-4 re
 STEP_BYTES = {("3d", "dp"): 224, ("2d", "le"): 96, ("2d", "dp"): 120}
 
 
+def p2g_kernel_name(kw, variant):
+    """The P2G kernel a configuration runs (3D quadratic: the autotuner's pick)."""
+    if kw["dim"] == 2:
+        return "tile scatter (2D)"
+    if kw["shape_function"] == "quadratic":
+        return {1: "dual-cell z-sweep", 0: "cell-row scatter"}[variant]
+    return "z-sweep (3D %s)" % kw["shape_function"]
+
+
 def load_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -623,7 +632,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, numpy PCG64)",
             "config": {"workload": workload_name(args.config), "particles_per_gpu": n, "grid_nodes": sim.num_nodes,
                        "active_nodes": active, "resort_interval": args.resort_interval,
-                       "p2g_kernel": {1: "dual-cell z-sweep", 0: "cell-row scatter"}.get(p2g_variant, "tile"),
+                       "p2g_kernel": p2g_kernel_name(kw, p2g_variant),
                        "l2": "state larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",

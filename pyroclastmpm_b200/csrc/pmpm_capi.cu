@@ -147,6 +147,8 @@ struct pmpm_sim {
   int nkeys = 0;
   int nbricks = 0;     // dual-cell bricks (cell-scatter P2G)
   int p2g_variant = 1; // 3D quadratic: 0 cell scatter, 1 dual sweep (pmpm_autotune picks)
+  int num_sms = 1;       // persistent P2G grids: CTAs per SM x this
+  unsigned p2g_seq = 0;  // queue-driven P2G launches so far (fetch counter parity)
   bool tuning = false; // no physical re-sort while the autotuner times variants
   int *key = nullptr;  // binning key scratch
   int *fault = nullptr;
@@ -376,6 +378,12 @@ int launch_partition(pmpm_sim *s) {
   k_hash_count<D, SF><<<blocks_for(s->n), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
   s->launches += 7;
+  if (D == 3 && !(s->flags & PMPM_FLAG_DETERMINISTIC)) {
+    // active-tile queue of the persistent 3D sweep P2G kernels
+    k_tile_list<<<(s->g.ntiles + 255) / 256, 256, 0, st>>>(a);
+    PMPM_LAUNCHED();
+    s->launches += 1;
+  }
   k_scan_reduce<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->nkeys, s->B.block_sums);
   PMPM_LAUNCHED();
   k_scan_top<<<1, kScanThreads, 0, st>>>(s->B.block_sums, s->nscan_blocks, s->B.scalars);
@@ -432,10 +440,13 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
       attr_set[dev] = true;
     }
     if (s->p2g_variant == 1) {
+      // persistent CTAs over the active-tile queue of this partition
+      a.p2g_par = (int)(s->p2g_seq++ & 1u);
+      const int grid = std::min(s->g.ntiles, 2 * s->num_sms);
       if (s->has_planar)
-        k_p2g_dual3<true><<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+        k_p2g_dual3<true><<<grid, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
       else
-        k_p2g_dual3<false><<<s->g.ntiles, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+        k_p2g_dual3<false><<<grid, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
     } else {
       constexpr int cbytes = cells3_smem_bytes();
       static bool cattr_set[64] = {false};  // per device
@@ -456,7 +467,9 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
       PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
       attr_set[dev] = true;
     }
-    k_p2g_sweep3<SF><<<s->g.ntiles, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+    a.p2g_par = (int)(s->p2g_seq++ & 1u);
+    const int grid = std::min(s->g.ntiles, s->num_sms);
+    k_p2g_sweep3<SF><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
   } else {
     k_p2g_tile<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
   }
@@ -1244,6 +1257,11 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK) st = dalloc(&s->N.vel, nn * (s->dim == 3 ? NodeVel<3>::F : NodeVel<2>::F));
   if (st == PMPM_OK) st = dalloc(&s->N.tile_epoch, (size_t)g.ntiles);
   if (st == PMPM_OK) st = dalloc(&s->node_epoch, (size_t)g.ntiles);
+  if (st == PMPM_OK) st = dalloc(&s->N.tile_list, (size_t)g.ntiles);
+  if (st == PMPM_OK) st = dalloc(&s->N.tile_queue, 4);
+  if (st == PMPM_OK && cudaMemset(s->N.tile_queue, 0, 4 * sizeof(int)) != cudaSuccess) st = PMPM_ERR_CUDA;
+  if (st == PMPM_OK && cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess)
+    st = PMPM_ERR_CUDA;
   // binning key space (reference cells, or dual cells for the 3D quadratic fast path)
   s->dual = s->dim == 3 && s->shape == PMPM_SHAPE_QUADRATIC && !(s->flags & PMPM_FLAG_DETERMINISTIC);
   s->nkeys = 1;
@@ -1298,6 +1316,8 @@ int pmpm_destroy(pmpm_sim *s) {
   dfree(s->N.pnt);
   dfree(s->N.vel);
   dfree(s->N.tile_epoch);
+  dfree(s->N.tile_list);
+  dfree(s->N.tile_queue);
   dfree(s->node_epoch);
   dfree(s->B.count);
   dfree(s->B.offset);

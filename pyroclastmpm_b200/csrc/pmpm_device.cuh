@@ -73,6 +73,11 @@ struct DevNodes {
   // 3D: vx vy vz - | vntx vnty vntz -  (two float4), 2D: vx vy vntx vnty
   float *vel;
   int *tile_epoch;  // tile active in the partition whose epoch it holds
+  // active-tile queue of the 3D sweep P2G kernels (null where not used):
+  // tile_list[0 .. tile_queue[epoch & 1]) are the tiles the binning pass of
+  // that epoch marked; tile_queue[2 + parity] is a launch's fetch counter
+  int *tile_list;
+  int *tile_queue;
   // cell-scatter P2G: per node [m, p0 p1 p2, f0 f1 f2, -], zero outside P2G
   float *acc;
 };
@@ -139,6 +144,7 @@ struct StepArgs {
   float *musl_x;    // MUSL: new positions between the two G2P passes
   int has_planar;
   int has_sref;
+  int p2g_par;      // fetch counter of this P2G launch (tile queue)
   DevMaterial mat[kMaxMat];
   DevBC bc[kMaxBC];
 };

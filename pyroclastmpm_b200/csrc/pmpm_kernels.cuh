@@ -44,6 +44,41 @@ __device__ __forceinline__ int tile_of(const DevGrid &g, const int c[3]) {
 // binning
 // --------------------------------------------------------------------------
 
+// Marks tile t active in this partition (plain stores: every writer stores
+// the same value).
+__device__ __forceinline__ void mark_tile(const StepArgs &a, int t) {
+  if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+}
+
+// Active-tile queue of this partition: the tiles marked with its epoch, in
+// tile order within each warp (one atomic per warp).  Runs after the binning
+// pass; clears the next partition's count.
+__global__ void __launch_bounds__(256) k_tile_list(StepArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int *count = &a.N.tile_queue[a.epoch & 1];
+  if (t == 0) a.N.tile_queue[(a.epoch + 1) & 1] = 0;
+  const bool on = t < a.g.ntiles && a.N.tile_epoch[t] == a.epoch;
+  const unsigned m = __ballot_sync(0xffffffffu, on);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == __ffs(m) - 1) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  if (on) {
+    const int i = base + __popc(m & ((1u << lane) - 1u));
+    if (i < a.g.ntiles) a.N.tile_list[i] = t;
+  }
+}
+
+// Next tile of the active-tile queue for the whole CTA, or -1.
+__device__ __forceinline__ int next_tile(const StepArgs &a, int *cur) {
+  if (threadIdx.x == 0) *cur = atomicAdd(&a.N.tile_queue[2 + a.p2g_par], 1);
+  __syncthreads();
+  const int idx = *cur;
+  __syncthreads();
+  return idx < min(a.N.tile_queue[a.epoch & 1], a.g.ntiles) ? a.N.tile_list[idx] : -1;
+}
+
 // Marks every node tile the particle's P2G contributions or G2P reads touch.
 template <int D, int SF>
 __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], unsigned hu, bool binned,
@@ -75,7 +110,7 @@ __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], un
       for (int ty = tlo[1]; ty <= thi[1]; ty++)
         for (int tx = tlo[0]; tx <= thi[0]; tx++) {
           int t = tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
-          if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+          mark_tile(a, t);
         }
   }
   if (SF != PMPM_SHAPE_QUADRATIC && clipped && binned) {
@@ -89,7 +124,7 @@ __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], un
       if ((unsigned)f >= (unsigned)g.ntotal) continue;
       int c[3] = {f % g.n[0], (f / g.n[0]) % g.n[1], f / (g.n[0] * g.n[1])};
       int t = tile_of<D>(g, c);
-      if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+      mark_tile(a, t);
     }
   }
 }
@@ -110,7 +145,7 @@ __device__ __forceinline__ void mark_tiles_dual(const StepArgs &a, const int d[3
     for (int ty = tlo[1]; ty <= thi[1]; ty++)
       for (int tx = tlo[0]; tx <= thi[0]; tx++) {
         const int t = tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
-        if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+        mark_tile(a, t);
       }
 }
 
@@ -1093,14 +1128,12 @@ __device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
 }
 
 template <int SF>
-__global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
+__device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile) {
   using W = Sweep3<SF>;
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int WIN = W::WIN;
   const DevGrid &g = a.g;
-  const int tile = blockIdx.x;
-  if (a.N.tile_epoch[tile] != a.epoch) return;
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
   __shared__ int npair[2];
@@ -1349,6 +1382,15 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
   write_node<3>(a, node, mass, p, pnt, live);
 }
 
+// One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
+template <int SF>
+__global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
+  __shared__ int cur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
+  for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
+    sweep3_tile<SF>(a, apply_bcs, node_epoch, tile);
+}
+
 // --------------------------------------------------------------------------
 // P2G, 3D quadratic fast path: dual-cell z-sweep
 // --------------------------------------------------------------------------
@@ -1420,14 +1462,12 @@ __device__ __forceinline__ void tile_epilogue3(const StepArgs &a, int apply_bcs,
 
 // PLANAR: the handle has a PlanarDomain (per-particle external forces to map)
 template <bool PLANAR>
-__global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
+__device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile) {
   using W = Dual3;
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int NN = T::N;  // nodes per tile
   const DevGrid &g = a.g;
-  const int tile = blockIdx.x;
-  if (a.N.tile_epoch[tile] != a.epoch) return;
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
   __shared__ int npair[2];
@@ -1648,6 +1688,15 @@ __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int appl
   }
   __syncthreads();
   tile_epilogue3(a, apply_bcs, t0, acc, tid, NT);
+}
+
+// One persistent CTA pass over the active-tile queue (grid: 2 CTAs per SM).
+template <bool PLANAR>
+__global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
+  __shared__ int cur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
+  for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
+    dual3_tile<PLANAR>(a, apply_bcs, node_epoch, tile);
 }
 
 // --------------------------------------------------------------------------
