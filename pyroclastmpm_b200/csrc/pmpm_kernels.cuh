@@ -1290,10 +1290,36 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
           const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
           const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
           const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
-          for (int j = j0; j < j1; j++) {
+          // cubic: a particle at u >= 0 in cell b = (int)u meets node b + w
+          // at r in [-w, 1 - w), on spline piece 2 - w, so the item's pieces
+          // are fixed: their coefficients are loaded once (particles at u < 0
+          // take the general evaluation)
+          float cx[4] = {0, 0, 0, 0}, dx[3] = {0, 0, 0}, cy[4] = {0, 0, 0, 0}, dy[3] = {0, 0, 0};
+          if (SF == PMPM_SHAPE_CUBIC) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              cx[k] = kCubicW[typex][2 - wx][k];
+              cy[k] = kCubicW[typey][2 - wy][k];
+            }
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              dx[k] = kCubicD[typex][2 - wx][k];
+              dy[k] = kCubicD[typey][2 - wy][k];
+            }
+          }
+          auto add = [&](int j) {
             float Nx, dNx, Ny, dNy;
-            axis_weight<SF>(st_u[0][j] - (float)(st_b[0][j] + wx), g.inv_h, typex, Nx, dNx);
-            axis_weight<SF>(st_u[1][j] - (float)(st_b[1][j] + wy), g.inv_h, typey, Ny, dNy);
+            const float ux = st_u[0][j], uy = st_u[1][j];
+            const float rx = ux - (float)(st_b[0][j] + wx), ry = uy - (float)(st_b[1][j] + wy);
+            if (SF == PMPM_SHAPE_CUBIC && ux >= 0.0f && uy >= 0.0f) {
+              Nx = ((cx[0] * rx + cx[1]) * rx + cx[2]) * rx + cx[3];
+              dNx = g.inv_h * ((dx[0] * rx + dx[1]) * rx + dx[2]);
+              Ny = ((cy[0] * ry + cy[1]) * ry + cy[2]) * ry + cy[3];
+              dNy = g.inv_h * ((dy[0] * ry + dy[1]) * ry + dy[2]);
+            } else {
+              axis_weight<SF>(rx, g.inv_h, typex, Nx, dNx);
+              axis_weight<SF>(ry, g.inv_h, typey, Ny, dNy);
+            }
             const float m = st_m[j];
             const float mvx = st_mv[0][j], mvy = st_mv[1][j], mvz = st_mv[2][j];
             const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
@@ -1317,7 +1343,13 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
               win[q][k][5] += Ay * Nz + By * dNz;
               win[q][k][6] += Az * Nz + Bz * dNz;
             }
+          };
+          int j = j0;
+          for (; j + 1 < j1; j += 2) {
+            add(j);
+            add(j + 1);
           }
+          if (j < j1) add(j);
         }
         __syncthreads();
       }
