@@ -214,6 +214,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
   bool in_axes = true;
   bool binned = false, sorted = false;
   unsigned key = 0;
+  int dcell[3] = {0, 0, 0};
   if (valid) {
 #pragma unroll
     for (int c = 0; c < D; c++) {
@@ -230,13 +231,8 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
       for (int c = 0; c < D; c++) d[c] = dual_coord(u[c], b[c]);
       key = (unsigned)(d[0] + d[1] * a.B.kd[0] + d[2] * a.B.kd[0] * a.B.kd[1]);
       binned = in_axes;
-      if (in_axes) {
-        mark_tiles_dual<D>(a, d);
-        if (a.B.brick_epoch) {
-          const int bi = d[0] / 8 + (d[1] / 8) * a.B.kb[0] + (d[2] / 8) * a.B.kb[0] * a.B.kb[1];
-          if (a.B.brick_epoch[bi] != a.epoch) a.B.brick_epoch[bi] = a.epoch;
-        }
-      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) dcell[c] = d[c];
     } else {
       key = hu;
       binned = hu < (unsigned)g.ntotal;
@@ -253,6 +249,15 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
   }
   const int slot = warp_bin_slot(a.B.count, key, sorted);
   if (!valid) return;
+  if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual && binned && slot == 0) {
+    // all particles of a dual cell share its tiles and brick: the cell's
+    // first arrival marks them
+    mark_tiles_dual<D>(a, dcell);
+    if (a.B.brick_epoch) {
+      const int bi = dcell[0] / 8 + (dcell[1] / 8) * a.B.kb[0] + (dcell[2] / 8) * a.B.kb[0] * a.B.kb[1];
+      if (a.B.brick_epoch[bi] != a.epoch) a.B.brick_epoch[bi] = a.epoch;
+    }
+  }
   a.P.key[s] = (unsigned)a.B.key_base + key;
   a.P.slot[s] = slot;
   if (!binned || (SF == PMPM_SHAPE_QUADRATIC && !in_axes)) atomicOr(a.fault, kFaultOutOfDomain);
@@ -297,13 +302,26 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *smem_warp, int &
   return r;
 }
 
+// kScanPer consecutive keys per thread: one 16-byte access when all are in range
+__device__ __forceinline__ void load_keys4(const int *p, int base, int n, int v[kScanPer]) {
+  static_assert(kScanPer == 4, "vector width");
+  if (base + kScanPer <= n) {
+    const int4 q = *reinterpret_cast<const int4 *>(p + base);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) v[k] = base + k < n ? p[base + k] : 0;
+  }
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int *count, int n, int *block_sums) {
   __shared__ int sw[33];
   const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
+  int v[kScanPer];
+  load_keys4(count, base, n, v);
   int sum = 0;
 #pragma unroll
-  for (int k = 0; k < kScanPer; k++)
-    if (base + k < n) sum += count[base + k];
+  for (int k = 0; k < kScanPer; k++) sum += v[k];
   int total;
   block_exclusive_scan(sum, sw, total);
   if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
@@ -333,21 +351,26 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(int *count, int n, 
   __shared__ int sw[33];
   const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
   int v[kScanPer];
+  load_keys4(count, base, n, v);
   int sum = 0;
 #pragma unroll
-  for (int k = 0; k < kScanPer; k++) {
-    v[k] = base + k < n ? count[base + k] : 0;
-    sum += v[k];
-  }
+  for (int k = 0; k < kScanPer; k++) sum += v[k];
   int total;
   int ex = block_exclusive_scan(sum, sw, total) + block_sums[blockIdx.x];
+  if (base + kScanPer <= n) {
+    const int4 o = make_int4(ex, ex + v[0], ex + v[0] + v[1], ex + v[0] + v[1] + v[2]);
+    *reinterpret_cast<int4 *>(offset + base) = o;
+    *reinterpret_cast<int4 *>(count + base) = make_int4(0, 0, 0, 0);
+    ex = o.w + v[3];
+  } else {
 #pragma unroll
-  for (int k = 0; k < kScanPer; k++) {
-    if (base + k < n) {
-      offset[base + k] = ex;
-      count[base + k] = 0;
+    for (int k = 0; k < kScanPer; k++) {
+      if (base + k < n) {
+        offset[base + k] = ex;
+        count[base + k] = 0;
+      }
+      ex += v[k];
     }
-    ex += v[k];
   }
   if (base <= n - 1 && n - 1 < base + kScanPer) offset[n] = ex;
 }
