@@ -2224,7 +2224,7 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 }
 
 template <int D, int SF, bool FULL>
-__global__ void __launch_bounds__(256, (SF == PMPM_SHAPE_CUBIC || FULL) ? 2 : 3) k_g2p(StepArgs a, int do_stress, int store_L) {
+__global__ void __launch_bounds__(256, (SF == PMPM_SHAPE_CUBIC || FULL) ? 2 : 4) k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
 }
