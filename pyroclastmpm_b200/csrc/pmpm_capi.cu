@@ -464,12 +464,16 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
     static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
     if (!attr_set[dev]) {
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
       attr_set[dev] = true;
     }
     a.p2g_par = (int)(s->p2g_seq++ & 1u);
     const int grid = std::min(s->g.ntiles, s->num_sms);
-    k_p2g_sweep3<SF><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+    if (s->has_planar)
+      k_p2g_sweep3<SF, true><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+    else
+      k_p2g_sweep3<SF, false><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
   } else {
     k_p2g_tile<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
   }

@@ -1150,7 +1150,7 @@ __device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
   return cnt;
 }
 
-template <int SF>
+template <int SF, bool PLANAR>
 __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile) {
   using W = Sweep3<SF>;
   using T = TileDims<3>;
@@ -1288,7 +1288,7 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             st_mv[c][jj] = m * P.v[c * st + s];
-            st_f[c][jj] = (a.has_planar && m != 0.0f && !a.remap) ? P.fext[c * st + s] : 0.0f;
+            if (PLANAR) st_f[c][jj] = (m != 0.0f && !a.remap) ? P.fext[c * st + s] : 0.0f;
           }
           // -V sigma, symmetric: xx yy zz xy xz yz
 #pragma unroll
@@ -1350,9 +1350,14 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
             const float nn = Nx * Ny;
             const float gx = dNx * Ny, gy = Nx * dNy;
             // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
-            const float Ax = st_f[0][j] * nn + Sxx * gx + Sxy * gy;
-            const float Ay = st_f[1][j] * nn + Sxy * gx + Syy * gy;
-            const float Az = st_f[2][j] * nn + Sxz * gx + Syz * gy;
+            float Ax = Sxx * gx + Sxy * gy;
+            float Ay = Sxy * gx + Syy * gy;
+            float Az = Sxz * gx + Syz * gy;
+            if (PLANAR) {
+              Ax += st_f[0][j] * nn;
+              Ay += st_f[1][j] * nn;
+              Az += st_f[2][j] * nn;
+            }
             const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
             const float mn = m * nn, mvxn = mvx * nn, mvyn = mvy * nn, mvzn = mvz * nn;
 #pragma unroll
@@ -1438,12 +1443,12 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 }
 
 // One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
-template <int SF>
+template <int SF, bool PLANAR>
 __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
   for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
-    sweep3_tile<SF>(a, apply_bcs, node_epoch, tile);
+    sweep3_tile<SF, PLANAR>(a, apply_bcs, node_epoch, tile);
 }
 
 // --------------------------------------------------------------------------
@@ -2224,7 +2229,7 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 }
 
 template <int D, int SF, bool FULL>
-__global__ void __launch_bounds__(256, (SF == PMPM_SHAPE_CUBIC || FULL) ? 2 : 4) k_g2p(StepArgs a, int do_stress, int store_L) {
+__global__ void __launch_bounds__(256, FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 3 : 4)) k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
 }
