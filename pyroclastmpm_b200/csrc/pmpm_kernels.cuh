@@ -1122,7 +1122,11 @@ struct Sweep3 {
 
 template <int SF>
 constexpr int sweep3_smem_bytes() {
-  return (7 * Sweep3<SF>::NT + Sweep3<SF>::SLOTS * (2 + 2 + 1 + 3 + 3 + 6 + 2 * Sweep3<SF>::WIN)) * 4;
+  // cubic also stages the x and y weights of all four offsets (one CTA per
+  // SM either way, so the space is free)
+  return (7 * Sweep3<SF>::NT +
+          Sweep3<SF>::SLOTS * (2 + 2 + 1 + 3 + 3 + 6 + 2 * Sweep3<SF>::WIN +
+                               (SF == PMPM_SHAPE_CUBIC ? 4 * Sweep3<SF>::WIN : 0))) * 4;
 }
 
 // pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
@@ -1175,6 +1179,10 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   float(*st_S)[SL] = st_f + 3;                      // [6] -V sigma
   float(*st_nz)[SL] = st_S + 6;                     // [WIN]
   float(*st_dnz)[SL] = st_nz + WIN;                 // [WIN]
+  float(*st_wx)[SL] = st_dnz + WIN;                 // cubic: [WIN] x weights per offset
+  float(*st_dwx)[SL] = st_wx + WIN;                 // [WIN]
+  float(*st_wy)[SL] = st_dwx + WIN;                 // [WIN]
+  float(*st_dwy)[SL] = st_wy + WIN;                 // [WIN]
 
   const int tid = threadIdx.x;
   const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
@@ -1302,6 +1310,36 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
             st_nz[k][jj] = N;
             st_dnz[k][jj] = dN;
           }
+          if (SF == PMPM_SHAPE_CUBIC) {
+            // x and y weights of the four offsets: r from the particle's own
+            // bin, the node type of the target the offset reaches from the
+            // (possibly aliased) source cell it is staged for.  At u >= 0
+            // offset w sits on spline piece 2 - w (r in [-w, 1 - w)), so its
+            // coefficients are the same for neighbouring lanes; u < 0 takes
+            // the general form
+            const int src[2] = {t0[0] - W::HI + lo % W::NS, t0[1] - W::HI + lo / W::NS};
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+              float(*wN)[SL] = c == 0 ? st_wx : st_wy;
+              float(*wD)[SL] = c == 0 ? st_dwx : st_dwy;
+#pragma unroll
+              for (int k = 0; k < WIN; k++) {
+                const int tgt = src[c] + k + W::LO;
+                const int type = cubic_node_type(min(max(tgt, 0), g.n[c] - 1), g.n[c]);
+                const float r = u[c] - (float)(b[c] + k + W::LO);
+                float N, dN;
+                if (u[c] >= 0.0f) {
+                  const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
+                  N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
+                  dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
+                } else {
+                  axis_weight<SF>(r, g.inv_h, type, N, dN);
+                }
+                wN[k][jj] = N;
+                wD[k][jj] = dN;
+              }
+            }
+          }
         }
         __syncthreads();
         // ---- items: add their source cell's staged particles ----
@@ -1313,35 +1351,17 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
           const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
           const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
           const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
-          // cubic: a particle at u >= 0 in cell b = (int)u meets node b + w
-          // at r in [-w, 1 - w), on spline piece 2 - w, so the item's pieces
-          // are fixed: their coefficients are loaded once (particles at u < 0
-          // take the general evaluation)
-          float cx[4] = {0, 0, 0, 0}, dx[3] = {0, 0, 0}, cy[4] = {0, 0, 0, 0}, dy[3] = {0, 0, 0};
-          if (SF == PMPM_SHAPE_CUBIC) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-              cx[k] = kCubicW[typex][2 - wx][k];
-              cy[k] = kCubicW[typey][2 - wy][k];
-            }
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-              dx[k] = kCubicD[typex][2 - wx][k];
-              dy[k] = kCubicD[typey][2 - wy][k];
-            }
-          }
+          const int ix = item_ix[q], iy = item_iy[q];
           auto add = [&](int j) {
             float Nx, dNx, Ny, dNy;
-            const float ux = st_u[0][j], uy = st_u[1][j];
-            const float rx = ux - (float)(st_b[0][j] + wx), ry = uy - (float)(st_b[1][j] + wy);
-            if (SF == PMPM_SHAPE_CUBIC && ux >= 0.0f && uy >= 0.0f) {
-              Nx = ((cx[0] * rx + cx[1]) * rx + cx[2]) * rx + cx[3];
-              dNx = g.inv_h * ((dx[0] * rx + dx[1]) * rx + dx[2]);
-              Ny = ((cy[0] * ry + cy[1]) * ry + cy[2]) * ry + cy[3];
-              dNy = g.inv_h * ((dy[0] * ry + dy[1]) * ry + dy[2]);
+            if (SF == PMPM_SHAPE_CUBIC) {
+              Nx = st_wx[ix][j];
+              dNx = st_dwx[ix][j];
+              Ny = st_wy[iy][j];
+              dNy = st_dwy[iy][j];
             } else {
-              axis_weight<SF>(rx, g.inv_h, typex, Nx, dNx);
-              axis_weight<SF>(ry, g.inv_h, typey, Ny, dNy);
+              axis_weight<SF>(st_u[0][j] - (float)(st_b[0][j] + wx), g.inv_h, typex, Nx, dNx);
+              axis_weight<SF>(st_u[1][j] - (float)(st_b[1][j] + wy), g.inv_h, typey, Ny, dNy);
             }
             const float m = st_m[j];
             const float mvx = st_mv[0][j], mvy = st_mv[1][j], mvz = st_mv[2][j];
