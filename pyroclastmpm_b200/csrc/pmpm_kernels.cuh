@@ -1305,8 +1305,16 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
           for (int k = 0; k < WIN; k++) {
             const int tz = cz + k + W::LO;
             const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(min(max(tz, 0), g.n[2] - 1), g.n[2]) : 0;
+            const float r = u[2] - (float)(b[2] + k + W::LO);
             float N, dN;
-            axis_weight<SF>(u[2] - (float)(b[2] + k + W::LO), g.inv_h, type, N, dN);
+            if (SF == PMPM_SHAPE_CUBIC && u[2] >= 0.0f) {
+              // fixed spline piece of offset k (see the x / y weights below)
+              const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
+              N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
+              dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
+            } else {
+              axis_weight<SF>(r, g.inv_h, type, N, dN);
+            }
             st_nz[k][jj] = N;
             st_dnz[k][jj] = dN;
           }
