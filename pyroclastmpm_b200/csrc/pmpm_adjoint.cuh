@@ -663,6 +663,7 @@ struct AdjState {
   float *x, *v, *F, *sig, *eps;  // adjoints of the particle state
   float *gE, *gphi;              // accumulated parameter gradients
   float *node;                   // per node: [0..2] vbar / pbar, [3..5] vntbar / fbar, [6] mbar
+  float *Lb;                     // velocity-gradient adjoint between the two G2P backward kernels
 };
 
 template <int D>
@@ -687,73 +688,40 @@ __device__ __forceinline__ void load_node_vel(const StepArgs &a, int node, float
 // memory once per node; a CTA whose box exceeds kAdjBoxNodes adds directly.
 constexpr int kAdjBoxNodes = 1536;
 
+// First half: the F update and the stress update of one particle.  L is
+// recomputed from the step's node velocities; the velocity-gradient adjoint
+// goes to A.Lb for the scatter, the F and elastic-strain adjoints are
+// replaced in place, the stress adjoint is cleared and the parameter
+// gradients are added.  (Split from the scatter so that neither kernel
+// carries the other's registers: the return-mapping VJP needs many, the
+// scatter its shared-memory node box.)
 template <int D>
-__global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
-  __shared__ int box[6];
-  __shared__ float acc[kAdjBoxNodes * 6];
-  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) kadj_g2p_mat(StepArgs a, AdjState A) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const DevParticles &P = a.P;
-  const bool valid = s0 < P.n;
-  const int s = valid ? s0 : P.n - 1;
+  if (s >= P.n) return;
   const DevGrid &g = a.g;
   const int st = P.stride;
   constexpr int NE = Sym<D>::E, NS = Sym<D>::S;
-  float x[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+  float x[3] = {0, 0, 0};
 #pragma unroll
-  for (int c = 0; c < D; c++) {
-    x[c] = P.x[c * st + s];
-    v[c] = P.v[c * st + s];
-  }
+  for (int c = 0; c < D; c++) x[c] = P.x[c * st + s];
   QuadStencil<D> Q;
   Q.build(g, x);
-  // ---- node box of the CTA ----
-  if (threadIdx.x < 3) {
-    box[threadIdx.x] = INT_MAX;
-    box[3 + threadIdx.x] = -1;
-  }
-  __syncthreads();
-  const bool contributes = valid && Q.inside;
-  if (contributes) {
-#pragma unroll
-    for (int c = 0; c < D; c++) {
-      atomicMin(&box[c], Q.idx[c][0]);
-      atomicMax(&box[3 + c], Q.idx[c][2]);
-    }
-  }
-  __syncthreads();
-  int bx = 1, by = 1, bz = 1, b0x = 0, b0y = 0, b0z = 0;
-  if (box[3] >= 0) {
-    b0x = box[0];
-    b0y = box[1];
-    bx = box[3] - box[0] + 1;
-    by = box[4] - box[1] + 1;
-    if (D == 3) {
-      b0z = box[2];
-      bz = box[5] - box[2] + 1;
-    }
-  }
-  const bool use_smem = box[3] >= 0 && bx * by * bz <= kAdjBoxNodes;
-  const int nbox = use_smem ? bx * by * bz : 0;
-  for (int k = threadIdx.x; k < nbox * 6; k += blockDim.x) acc[k] = 0.0f;
-  __syncthreads();
-  // incoming adjoints (of the step's outputs)
-  float xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, Fb[9], sb[6] = {0, 0, 0, 0, 0, 0}, eb[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-  for (int c = 0; c < D; c++) {
-    xb[c] = A.x[c * st + s];
-    vb[c] = A.v[c * st + s];
-  }
+  float Fb[9], sb[6] = {0, 0, 0, 0, 0, 0}, eb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int k = 0; k < D * D; k++) Fb[k] = A.F[k * st + s];
 #pragma unroll
   for (int k = 0; k < NS; k++) sb[k] = A.sig[k * st + s];
 #pragma unroll
   for (int k = 0; k < NE; k++) eb[k] = A.eps[k * st + s];
-  float xo[3] = {xb[0], xb[1], xb[2]};  // position adjoint: identity part
-  float vo[3] = {0, 0, 0}, Fo[9], eo[6] = {0, 0, 0, 0, 0, 0};
+  float Fo[9], eo[6] = {0, 0, 0, 0, 0, 0}, Lb[9];
 #pragma unroll
-  for (int k = 0; k < 9; k++) Fo[k] = 0.0f;
-  if (contributes) {
+  for (int k = 0; k < 9; k++) {
+    Fo[k] = 0.0f;
+    Lb[k] = 0.0f;
+  }
+  if (Q.inside) {
     // recompute L
     float L[9];
 #pragma unroll
@@ -777,7 +745,6 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
 #pragma unroll
     for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
     // F' = (I + dt L) F: Lbar = dt Fbar' F^T, Fbar = (I + dt L)^T Fbar'
-    float Lb[9];
 #pragma unroll
     for (int r = 0; r < D; r++)
 #pragma unroll
@@ -823,6 +790,86 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
 #pragma unroll
       for (int k = 0; k < NE; k++) eo[k] = eb[k];
     }
+  } else {
+    // outside the grid: the particle's state is kept
+#pragma unroll
+    for (int k = 0; k < D * D; k++) Fo[k] = Fb[k];
+#pragma unroll
+    for (int k = 0; k < NE; k++) eo[k] = eb[k];
+  }
+#pragma unroll
+  for (int k = 0; k < D * D; k++) {
+    A.Lb[k * st + s] = Lb[k];
+    A.F[k * st + s] = Fo[k];
+  }
+#pragma unroll
+  for (int k = 0; k < NE; k++) A.eps[k * st + s] = eo[k];
+#pragma unroll
+  for (int k = 0; k < NS; k++) A.sig[k * st + s] = 0.0f;
+}
+
+// Second half: the transposed G2P scatter of one particle (velocity and
+// position adjoints; node adjoints summed over the CTA's node box in shared
+// memory), with the velocity-gradient adjoint from kadj_g2p_mat.
+template <int D>
+__global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
+  __shared__ int box[6];
+  __shared__ float acc[kAdjBoxNodes * 6];
+  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const DevParticles &P = a.P;
+  const bool valid = s0 < P.n;
+  const int s = valid ? s0 : P.n - 1;
+  const DevGrid &g = a.g;
+  const int st = P.stride;
+  float x[3] = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < D; c++) x[c] = P.x[c * st + s];
+  QuadStencil<D> Q;
+  Q.build(g, x);
+  // ---- node box of the CTA ----
+  if (threadIdx.x < 3) {
+    box[threadIdx.x] = INT_MAX;
+    box[3 + threadIdx.x] = -1;
+  }
+  __syncthreads();
+  const bool contributes = valid && Q.inside;
+  if (contributes) {
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      atomicMin(&box[c], Q.idx[c][0]);
+      atomicMax(&box[3 + c], Q.idx[c][2]);
+    }
+  }
+  __syncthreads();
+  int bx = 1, by = 1, bz = 1, b0x = 0, b0y = 0, b0z = 0;
+  if (box[3] >= 0) {
+    b0x = box[0];
+    b0y = box[1];
+    bx = box[3] - box[0] + 1;
+    by = box[4] - box[1] + 1;
+    if (D == 3) {
+      b0z = box[2];
+      bz = box[5] - box[2] + 1;
+    }
+  }
+  const bool use_smem = box[3] >= 0 && bx * by * bz <= kAdjBoxNodes;
+  const int nbox = use_smem ? bx * by * bz : 0;
+  for (int k = threadIdx.x; k < nbox * 6; k += blockDim.x) acc[k] = 0.0f;
+  __syncthreads();
+  // incoming adjoints (of the step's outputs)
+  float xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < D; c++) {
+    xb[c] = A.x[c * st + s];
+    vb[c] = A.v[c * st + s];
+  }
+  float xo[3] = {xb[0], xb[1], xb[2]};  // position adjoint: identity part
+  float vo[3] = {0, 0, 0};
+  if (contributes) {
+    float Lb[9];
+#pragma unroll
+    for (int k = 0; k < D * D; k++) Lb[k] = A.Lb[k * st + s];
+    constexpr int KZ = D == 3 ? 3 : 1;
     // G2P transposed
     const float alpha = a.alpha, oma = a.one_minus_alpha;
     float pic[3], dv[3];
@@ -874,13 +921,9 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
           }
         }
   } else {
-    // outside the grid: the particle does not move and its state is kept
+    // outside the grid: the particle does not move
 #pragma unroll
     for (int c = 0; c < D; c++) vo[c] = vb[c];
-#pragma unroll
-    for (int k = 0; k < D * D; k++) Fo[k] = Fb[k];
-#pragma unroll
-    for (int k = 0; k < NE; k++) eo[k] = eb[k];
   }
   // ---- box sums -> global node adjoints ----
   __syncthreads();
@@ -898,12 +941,6 @@ __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
     A.x[c * st + s] = xo[c];
     A.v[c * st + s] = vo[c];
   }
-#pragma unroll
-  for (int k = 0; k < D * D; k++) A.F[k * st + s] = Fo[k];
-#pragma unroll
-  for (int k = 0; k < NE; k++) A.eps[k * st + s] = eo[k];
-#pragma unroll
-  for (int k = 0; k < NS; k++) A.sig[k * st + s] = 0.0f;
 }
 
 // Backward of the node update for the nodes of the active tiles:

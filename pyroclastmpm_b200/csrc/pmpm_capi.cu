@@ -2532,7 +2532,7 @@ void free_rollout(pmpm_sim *s) {
   for (float *p : s->ro.ckpt) cudaFree(p);
   s->ro.ckpt.clear();
   for (float *p : {s->ro.seg, s->ro.A.x, s->ro.A.v, s->ro.A.F, s->ro.A.sig, s->ro.A.eps, s->ro.A.gE, s->ro.A.gphi,
-                   s->ro.A.node})
+                   s->ro.A.node, s->ro.A.Lb})
     if (p) cudaFree(p);
   if (s->ro.seg_nodes) cudaFree(s->ro.seg_nodes);
   s->ro.seg_nodes = nullptr;
@@ -2598,13 +2598,15 @@ int adjoint_step(pmpm_sim *s, int epoch) {
   PMPM_CUDA(cudaMemsetAsync(A.node, 0, sizeof(float) * 8 * (size_t)s->g.ntotal, s->stream));
   StepArgs a = make_args(s);
   a.epoch = epoch;  // the epoch the restored tile marks carry
+  kadj_g2p_mat<D><<<blocks_for(s->n, 128), 128, 0, s->stream>>>(a, A);
+  PMPM_LAUNCHED();
   kadj_g2p<D><<<blocks_for(s->n, 128), 128, 0, s->stream>>>(a, A);
   PMPM_LAUNCHED();
   kadj_grid<D><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, A);
   PMPM_LAUNCHED();
   kadj_p2g<D><<<blocks_for(s->n, 128), 128, 0, s->stream>>>(a, A);
   PMPM_LAUNCHED();
-  s->launches += 3;
+  s->launches += 4;
   return PMPM_OK;
 }
 
@@ -2734,6 +2736,7 @@ int pmpm_rollout_backward(pmpm_sim *s, const float *grad_positions, int on_devic
     PMPM_TRY(dalloc(&A.gE, (size_t)st));
     PMPM_TRY(dalloc(&A.gphi, (size_t)st));
     PMPM_TRY(dalloc(&A.node, (size_t)8 * s->g.ntotal));
+    PMPM_TRY(dalloc(&A.Lb, (size_t)D * D * st));
   }
   const size_t nodeb = node_snapshot_bytes(s);
   bool need_seg = false;
