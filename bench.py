@@ -443,7 +443,7 @@ def run_calibration(args, world, rank, local, pg, emit=True):
                                             "fwd_plus_adjoint_over_plain_forward": (ms_fwd0 + ms_bwd0) / ms_plain},
                        "loss": loss, "grad_norm_E": float(np.linalg.norm(gE)),
                        "grad_norm_phi": float(np.linalg.norm(gphi))},
-            "roofline": {"bound": "hbm", "kernel": "adjoint step (3 kernels + recomputed P2G)",
+            "roofline": {"bound": "hbm", "kernel": "adjoint step (4 kernels + recomputed P2G)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
                          "algorithmic_bytes_per_launch": adj_bytes, "ms_per_launch": ms_adj_step},
