@@ -925,9 +925,13 @@ __device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int a
   __syncthreads();
   const int ntot = row_pref[Sh::ROWS];
 
-  // ---- particles: each thread takes one contiguous chunk of the list ----
+  // ---- particles: each thread takes one contiguous chunk of the list; the
+  // lanes of a warp take chunks NT/32 apart, so their stencils rarely share
+  // nodes (neighbouring chunks lie in neighbouring cells, whose stencils
+  // overlap and would serialise the shared-memory atomics) ----
   const int chunk = (ntot + NT - 1) / NT;
-  const int j0 = tid * chunk, j1 = min(j0 + chunk, ntot);
+  const int slot = (tid & 31) * (NT / 32) + (tid >> 5);
+  const int j0 = slot * chunk, j1 = min(j0 + chunk, ntot);
   int row = 0;
   if (j0 < j1) {
     int lo = 0, hi = Sh::ROWS;  // last row with row_pref <= j0
