@@ -39,7 +39,8 @@ typedef enum {
   PMPM_ERR_STATE = 5,          /* call order: e.g. a step before particles exist */
   PMPM_ERR_OUT_OF_DOMAIN = 16, /* a particle's cell lies outside the grid        */
   PMPM_ERR_NONFINITE = 17,     /* NaN or Inf appeared in particle positions      */
-  PMPM_ERR_CELL_OVERFLOW = 18  /* more particles in one cell than the sort holds */
+  PMPM_ERR_CELL_OVERFLOW = 18, /* more particles in one cell than the sort holds */
+  PMPM_ERR_TIMEOUT = 19        /* a bounded wait inside a kernel ran out: the step's results are invalid */
 } pmpm_status;
 
 /* Shape functions: numbering of the reference SFType

@@ -29,7 +29,7 @@ FLAG_MUSL = 4
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not supported",
     5: "call out of order", 16: "a particle left the background grid", 17: "non-finite particle position",
-    18: "too many particles in one cell",
+    18: "too many particles in one cell", 19: "a bounded wait inside a kernel ran out",
 }
 
 FIELDS = {

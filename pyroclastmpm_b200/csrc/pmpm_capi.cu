@@ -65,6 +65,38 @@ void dfree(T *&p) {
   p = nullptr;
 }
 
+// Single-pass key scan state: per-chunk tagged status words and the ticket
+// counters of alternate launches (both zeroed once at allocation).
+struct ScanState {
+  unsigned long long *status = nullptr;
+  int *ticket = nullptr;
+  unsigned launches = 0;
+};
+
+int alloc_scan(ScanState &sc, int nblocks) {
+  PMPM_TRY(dalloc(&sc.status, (size_t)nblocks));
+  PMPM_TRY(dalloc(&sc.ticket, 2));
+  PMPM_CUDA(cudaMemset(sc.status, 0, sizeof(unsigned long long) * nblocks));
+  PMPM_CUDA(cudaMemset(sc.ticket, 0, 2 * sizeof(int)));
+  return PMPM_OK;
+}
+
+void free_scan(ScanState &sc) {
+  dfree(sc.status);
+  dfree(sc.ticket);
+}
+
+// count -> offset (exclusive), counts cleared, scalars reset; one launch
+int launch_scan(ScanState &sc, int *count, int nkeys, int *offset, int *scalars, int *fault, int nblocks,
+                cudaStream_t st) {
+  const unsigned tag = sc.launches % 0x3fffffffu + 1u;  // never 0: zeroed status words carry no tag
+  sc.launches += 1;
+  k_scan_onepass<<<nblocks, kScanThreads, 0, st>>>(count, nkeys, offset, sc.status, sc.ticket, scalars, fault, tag,
+                                                   nblocks);
+  PMPM_LAUNCHED();
+  return PMPM_OK;
+}
+
 struct GravityState {
   int bc_index;
   float current[3];
@@ -142,6 +174,7 @@ struct pmpm_sim {
   // bins
   DevBins B{};
   int nscan_blocks = 0;
+  ScanState scan;
   bool dual = false;  // quadratic 3D fast path bins by dual cell
   int kd[3] = {1, 1, 1};
   int nkeys = 0;
@@ -384,12 +417,8 @@ int launch_partition(pmpm_sim *s) {
     PMPM_LAUNCHED();
     s->launches += 1;
   }
-  k_scan_reduce<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->nkeys, s->B.block_sums);
-  PMPM_LAUNCHED();
-  k_scan_top<<<1, kScanThreads, 0, st>>>(s->B.block_sums, s->nscan_blocks, s->B.scalars);
-  PMPM_LAUNCHED();
-  k_scan_apply<<<s->nscan_blocks, kScanThreads, 0, st>>>(s->B.count, s->nkeys, s->B.block_sums, s->B.offset);
-  PMPM_LAUNCHED();
+  PMPM_TRY(launch_scan(s->scan, s->B.count, s->nkeys, s->B.offset, s->B.scalars, s->fault, s->nscan_blocks, st));
+  s->launches -= 2;  // one scan launch instead of three
   k_scatter<<<blocks_for(s->n), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
   // ids in order inside each bin: needed by the deterministic gather and by
@@ -1278,6 +1307,7 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK) st = dalloc(&s->B.count, nk);
   if (st == PMPM_OK) st = dalloc(&s->B.offset, nk + 1);
   if (st == PMPM_OK) st = dalloc(&s->B.block_sums, (size_t)s->nscan_blocks);
+  if (st == PMPM_OK) st = alloc_scan(s->scan, s->nscan_blocks);
   if (st == PMPM_OK) st = dalloc(&s->B.scalars, 4);
   if (st == PMPM_OK) st = dalloc(&s->B.big_cells, nk);
   if (st == PMPM_OK && s->dual) {
@@ -1326,6 +1356,7 @@ int pmpm_destroy(pmpm_sim *s) {
   dfree(s->B.count);
   dfree(s->B.offset);
   dfree(s->B.block_sums);
+  free_scan(s->scan);
   dfree(s->B.scalars);
   dfree(s->B.big_cells);
   dfree(s->B.brick_epoch);
@@ -1862,6 +1893,7 @@ int pmpm_synchronize(pmpm_sim *s) {
   if (f & kFaultNonFinite) return PMPM_ERR_NONFINITE;
   if (f & kFaultOutOfDomain) return PMPM_ERR_OUT_OF_DOMAIN;
   if (f & kFaultCellOverflow) return PMPM_ERR_CELL_OVERFLOW;
+  if (f & kFaultWaitTimeout) return PMPM_ERR_TIMEOUT;
   return PMPM_OK;
 }
 
@@ -1947,6 +1979,7 @@ struct pmpm_batch {
   int *node_epoch = nullptr;
   DevBins B{};
   int nscan_blocks = 0;
+  ScanState scan;
   int *fault = nullptr;
   std::vector<StepArgs> views;
   StepArgs *d_views = nullptr;
@@ -2098,15 +2131,10 @@ int batch_partition(pmpm_batch *b) {
   kb_hash_count<D, SF><<<b->nblocks, kTPB, 0, st>>>(b->d_views, b->d_blocks, P, b->epoch);
   PMPM_LAUNCHED();
   const StepArgs ga = batch_global_args(b);
-  k_scan_reduce<<<b->nscan_blocks, kScanThreads, 0, st>>>(b->B.count, b->nkeys, b->B.block_sums);
-  PMPM_LAUNCHED();
-  k_scan_top<<<1, kScanThreads, 0, st>>>(b->B.block_sums, b->nscan_blocks, b->B.scalars);
-  PMPM_LAUNCHED();
-  k_scan_apply<<<b->nscan_blocks, kScanThreads, 0, st>>>(b->B.count, b->nkeys, b->B.block_sums, b->B.offset);
-  PMPM_LAUNCHED();
+  PMPM_TRY(launch_scan(b->scan, b->B.count, b->nkeys, b->B.offset, b->B.scalars, b->fault, b->nscan_blocks, st));
   k_scatter<<<blocks_for(b->n), kTPB, 0, st>>>(ga);
   PMPM_LAUNCHED();
-  b->launches += 5;
+  b->launches += 3;
   if (b->flags & PMPM_FLAG_DETERMINISTIC) {  // ids in order inside each bin for the gather
     k_sort_cells<<<blocks_for(b->nkeys), kTPB, 0, st>>>(ga);
     PMPM_LAUNCHED();
@@ -2208,6 +2236,7 @@ int pmpm_batch_destroy(pmpm_batch *b) {
                   (void *)b->B.order, (void *)b->B.block_sums, (void *)b->B.scalars, (void *)b->B.big_cells,
                   (void *)b->fault, (void *)b->d_views, (void *)b->d_blocks, (void *)b->d_tiles, b->staging})
     if (p) cudaFree(p);
+  free_scan(b->scan);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return PMPM_OK;
@@ -2305,6 +2334,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
   if (st == PMPM_OK) st = dalloc(&b->B.count, (size_t)b->nkeys);
   if (st == PMPM_OK) st = dalloc(&b->B.offset, (size_t)b->nkeys + 1);
   if (st == PMPM_OK) st = dalloc(&b->B.block_sums, (size_t)b->nscan_blocks);
+  if (st == PMPM_OK) st = alloc_scan(b->scan, b->nscan_blocks);
   if (st == PMPM_OK) st = dalloc(&b->B.scalars, 4);
   if (st == PMPM_OK) st = dalloc(&b->B.big_cells, (size_t)b->nkeys);
   if (st == PMPM_OK) st = dalloc(&b->fault, 1);
@@ -2485,6 +2515,7 @@ int pmpm_batch_synchronize(pmpm_batch *b) {
   if (f & kFaultNonFinite) return PMPM_ERR_NONFINITE;
   if (f & kFaultOutOfDomain) return PMPM_ERR_OUT_OF_DOMAIN;
   if (f & kFaultCellOverflow) return PMPM_ERR_CELL_OVERFLOW;
+  if (f & kFaultWaitTimeout) return PMPM_ERR_TIMEOUT;
   return PMPM_OK;
 }
 

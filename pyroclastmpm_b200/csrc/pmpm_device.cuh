@@ -23,7 +23,7 @@ constexpr int kMaxMat = PMPM_MAX_MATERIALS;
 constexpr int kMaxBC = PMPM_MAX_BCS;
 
 // fault word bits (first fault wins the status)
-enum : int { kFaultOutOfDomain = 1, kFaultNonFinite = 2, kFaultCellOverflow = 4 };
+enum : int { kFaultOutOfDomain = 1, kFaultNonFinite = 2, kFaultCellOverflow = 4, kFaultWaitTimeout = 8 };
 
 struct DevGrid {
   float origin[3];

@@ -327,6 +327,83 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int *count, 
   if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
+// Single-pass exclusive scan of the per-key counts into offsets (decoupled
+// look-back): each CTA takes a ticket in launch order, scans its chunk,
+// publishes the chunk total and then the inclusive prefix in status[ticket]
+// (tagged with the launch, so nothing is cleared between launches), and
+// sums its predecessors' published values back to the first inclusive one.
+// A CTA only waits on CTAs with smaller tickets, which are already running;
+// the wait is bounded (kFaultWaitTimeout).  Clears the counts it consumed;
+// the last CTA writes offset[n], the binned total and resets the per-step
+// counters and the next launch's ticket counter.
+constexpr unsigned long long kScanAggregate = 1ull << 32, kScanInclusive = 2ull << 32;
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n, int *offset,
+                                                                unsigned long long *status, int *ticket,
+                                                                int *scalars, int *fault, unsigned tag,
+                                                                int nblocks) {
+  __shared__ int sw[33];
+  __shared__ int sh_block, sh_prefix;
+  if (threadIdx.x == 0) sh_block = atomicAdd(&ticket[tag & 1u], 1);
+  __syncthreads();
+  const int blk = sh_block;
+  const int base = blk * kScanChunk + threadIdx.x * kScanPer;
+  int v[kScanPer];
+  load_keys4(count, base, n, v);
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; k++) sum += v[k];
+  int total;
+  const int ex_local = block_exclusive_scan(sum, sw, total);
+  if (threadIdx.x == 0) {
+    const unsigned long long t = (unsigned long long)tag << 34;
+    int prefix = 0;
+    if (blk > 0) {
+      atomicExch(&status[blk], t | kScanAggregate | (unsigned)total);
+      int j = blk - 1;
+      long long spins = 0;
+      while (j >= 0) {
+        const unsigned long long w = atomicAdd(&status[j], 0ull);
+        if ((w >> 34) != (unsigned long long)tag) {
+          if (++spins > (1ll << 22)) {
+            atomicOr(fault, kFaultWaitTimeout);
+            break;
+          }
+          continue;
+        }
+        prefix += (int)(unsigned)(w & 0xffffffffull);
+        if (w & kScanInclusive) break;
+        j--;
+      }
+    }
+    atomicExch(&status[blk], t | kScanInclusive | (unsigned)(prefix + total));
+    sh_prefix = prefix;
+    if (blk == nblocks - 1) {
+      offset[n] = prefix + total;
+      scalars[0] = prefix + total;  // binned particles
+      scalars[1] = 0;               // unbinned counter
+      scalars[2] = 0;               // big-cell counter
+      ticket[(tag + 1u) & 1u] = 0;
+    }
+  }
+  __syncthreads();
+  int ex = ex_local + sh_prefix;
+  if (base + kScanPer <= n) {
+    const int4 o = make_int4(ex, ex + v[0], ex + v[0] + v[1], ex + v[0] + v[1] + v[2]);
+    *reinterpret_cast<int4 *>(offset + base) = o;
+    *reinterpret_cast<int4 *>(count + base) = make_int4(0, 0, 0, 0);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+      if (base + k < n) {
+        offset[base + k] = ex;
+        count[base + k] = 0;
+      }
+      ex += v[k];
+    }
+  }
+}
+
 // Scans the block sums in place (single CTA) and resets the per-step counters.
 __global__ void __launch_bounds__(kScanThreads) k_scan_top(int *block_sums, int nblocks, int *scalars) {
   __shared__ int sw[33];
