@@ -181,6 +181,10 @@ struct pmpm_sim {
   int nbricks = 0;     // dual-cell bricks (cell-scatter P2G)
   int p2g_variant = 1; // 3D quadratic: 0 cell scatter, 1 dual sweep (pmpm_autotune picks)
   int num_sms = 1;       // persistent P2G grids: CTAs per SM x this
+  // the last step's G2P binned the current positions for the next partition
+  // (3D quadratic): counts, slots, keys and marks are in place
+  bool keys_fresh = false;
+  unsigned *hash_next = nullptr;  // reference hashes binned ahead [stride]
   unsigned p2g_seq = 0;  // queue-driven P2G launches so far (fetch counter parity)
   bool tuning = false; // no physical re-sort while the autotuner times variants
   int *key = nullptr;  // binning key scratch
@@ -241,6 +245,7 @@ void free_particles(pmpm_sim *s) {
   }
   dfree(s->slot);
   dfree(s->key);
+  dfree(s->hash_next);
   dfree(s->B.order);
   dfree(s->musl_x);
   s->n = 0;
@@ -408,8 +413,14 @@ int launch_partition(pmpm_sim *s) {
   s->epoch += 1;
   StepArgs a = make_args(s);
   cudaStream_t st = s->stream;
-  k_hash_count<D, SF><<<blocks_for(s->n), kTPB, 0, st>>>(a);
-  PMPM_LAUNCHED();
+  if (!s->keys_fresh) {
+    k_hash_count<D, SF><<<blocks_for(s->n), kTPB, 0, st>>>(a);
+    PMPM_LAUNCHED();
+  } else {
+    s->launches -= 1;  // binned by the last step's G2P
+    std::swap(s->P[s->cur].hash, s->hash_next);
+  }
+  s->keys_fresh = false;
   s->launches += 7;
   if (D == 3 && !(s->flags & PMPM_FLAG_DETERMINISTIC)) {
     // active-tile queue of the persistent 3D sweep P2G kernels
@@ -513,9 +524,23 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   return PMPM_OK;
 }
 
+// Invalidates binning done ahead by a step's G2P (particle state is about to
+// change outside a step): its counts are cleared, its marks are harmless.
+int drop_fresh_keys(pmpm_sim *s) {
+  if (!s->keys_fresh) return PMPM_OK;
+  s->keys_fresh = false;
+  PMPM_CUDA(cudaMemsetAsync(s->B.count, 0, sizeof(int) * (size_t)s->nkeys, s->stream));
+  return PMPM_OK;
+}
+
+// bin_next: the step loop's final G2P also bins the new positions (see
+// k_g2p); any other G2P changes positions, so earlier binning is dropped.
 template <int D, int SF>
-int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
+int launch_g2p(pmpm_sim *s, int do_stress, int store_L, bool bin_next = false) {
+  PMPM_TRY(drop_fresh_keys(s));
   StepArgs a = make_args(s);
+  a.bin_next = bin_next ? 1 : 0;
+  a.hash_next = s->hash_next;
   if (s->has_vm || s->has_mcc)
     k_g2p<D, SF, true><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
   else
@@ -523,6 +548,7 @@ int launch_g2p(pmpm_sim *s, int do_stress, int store_L) {
   PMPM_LAUNCHED();
   s->launches += 1;
   s->rigid_shift_pending = false;
+  s->keys_fresh = bin_next;
   return PMPM_OK;
 }
 
@@ -557,10 +583,15 @@ int step_once(pmpm_sim *s) {
   }
   PMPM_TRY((launch_p2g<D, SF>(s, 1)));
   const int store_L = (s->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
-  if (s->flags & PMPM_FLAG_MUSL)
+  if (s->flags & PMPM_FLAG_MUSL) {
     PMPM_TRY((musl_tail<D, SF>(s, store_L)));
-  else
-    PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L)));
+  } else {
+    // 3D quadratic: the next partition's binning rides on this G2P (not
+    // while a rollout or the autotuner saves and restores states, nor with
+    // a PlanarDomain, whose particle forces the binning pass computes)
+    const bool bin_next = s->dual && !s->tuning && !s->ro.held && s->rbls_index < 0 && !s->has_planar;
+    PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L, bin_next)));
+  }
   s->step += 1;
   return PMPM_OK;
 }
@@ -1402,6 +1433,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
       (num_rigid > 0 && !rigid_positions) || num_particles + num_rigid < 1)
     return PMPM_ERR_INVALID_ARGUMENT;
   PMPM_CUDA(cudaSetDevice(s->device));
+  PMPM_TRY(drop_fresh_keys(s));
   PMPM_CUDA(cudaStreamSynchronize(s->stream));
   free_particles(s);
   const int D = s->dim;
@@ -1413,6 +1445,7 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   PMPM_TRY(alloc_particle_set(s, s->P[1]));
   PMPM_TRY(dalloc(&s->slot, (size_t)s->stride));
   PMPM_TRY(dalloc(&s->key, (size_t)s->stride));
+  if (s->dual) PMPM_TRY(dalloc(&s->hash_next, (size_t)s->stride));
   PMPM_TRY(dalloc(&s->B.order, (size_t)s->stride));
   if (s->flags & PMPM_FLAG_MUSL) PMPM_TRY(dalloc(&s->musl_x, (size_t)s->dim * s->stride));
   const int st = s->stride;
@@ -1655,6 +1688,7 @@ int pmpm_set_field(pmpm_sim *s, int field, const void *src, size_t bytes, int on
   if (bytes != need) return PMPM_ERR_INVALID_ARGUMENT;
   if (s->n == 0) return PMPM_ERR_STATE;
   PMPM_CUDA(cudaSetDevice(s->device));
+  PMPM_TRY(drop_fresh_keys(s));
   const DevParticles &P = s->P[s->cur];
   int kind = -1;
   void *dstp = nullptr;
@@ -2541,6 +2575,7 @@ int state_floats(const pmpm_sim *s) {
 }
 
 int copy_state(pmpm_sim *s, float *buf, bool save) {
+  if (!save) PMPM_TRY(drop_fresh_keys(s));
   const int D = s->dim, st = s->stride;
   const DevParticles &P = s->P[s->cur];
   float *arrays[6] = {P.x, P.v, P.F, P.sig, P.eps, P.V};

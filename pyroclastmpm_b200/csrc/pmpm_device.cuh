@@ -145,6 +145,8 @@ struct StepArgs {
   int has_planar;
   int has_sref;
   int p2g_par;      // fetch counter of this P2G launch (tile queue)
+  int bin_next;     // G2P: bin the new positions for the next partition
+  unsigned *hash_next;  // their reference hashes (swapped in by that partition)
   DevMaterial mat[kMaxMat];
   DevBC bc[kMaxBC];
 };

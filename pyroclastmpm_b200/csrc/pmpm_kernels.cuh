@@ -46,8 +46,8 @@ __device__ __forceinline__ int tile_of(const DevGrid &g, const int c[3]) {
 
 // Marks tile t active in this partition (plain stores: every writer stores
 // the same value).
-__device__ __forceinline__ void mark_tile(const StepArgs &a, int t) {
-  if (a.N.tile_epoch[t] != a.epoch) a.N.tile_epoch[t] = a.epoch;
+__device__ __forceinline__ void mark_tile(const StepArgs &a, int t, int epoch) {
+  if (a.N.tile_epoch[t] != epoch) a.N.tile_epoch[t] = epoch;
 }
 
 // Active-tile queue of this partition: the tiles marked with its epoch, in
@@ -82,7 +82,7 @@ __device__ __forceinline__ int next_tile(const StepArgs &a, int *cur) {
 // Marks every node tile the particle's P2G contributions or G2P reads touch.
 template <int D, int SF>
 __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], unsigned hu, bool binned,
-                                           bool in_axes) {
+                                           bool in_axes, int epoch) {
   using T = TileDims<D>;
   constexpr int LO = Stencil<SF>::WLO, HI = Stencil<SF>::WLO + Stencil<SF>::WIN - 1;
   const DevGrid &g = a.g;
@@ -110,7 +110,7 @@ __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], un
       for (int ty = tlo[1]; ty <= thi[1]; ty++)
         for (int tx = tlo[0]; tx <= thi[0]; tx++) {
           int t = tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
-          mark_tile(a, t);
+          mark_tile(a, t, epoch);
         }
   }
   if (SF != PMPM_SHAPE_QUADRATIC && clipped && binned) {
@@ -124,14 +124,14 @@ __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], un
       if ((unsigned)f >= (unsigned)g.ntotal) continue;
       int c[3] = {f % g.n[0], (f / g.n[0]) % g.n[1], f / (g.n[0] * g.n[1])};
       int t = tile_of<D>(g, c);
-      mark_tile(a, t);
+      mark_tile(a, t, epoch);
     }
   }
 }
 
 // Dual binning: the particle's nodes are d - 1 .. d + 1 (clamped) per axis.
 template <int D>
-__device__ __forceinline__ void mark_tiles_dual(const StepArgs &a, const int d[3]) {
+__device__ __forceinline__ void mark_tiles_dual(const StepArgs &a, const int d[3], int epoch) {
   using T = TileDims<D>;
   const DevGrid &g = a.g;
   const int tsz[3] = {T::X, T::Y, T::Z};
@@ -145,7 +145,7 @@ __device__ __forceinline__ void mark_tiles_dual(const StepArgs &a, const int d[3
     for (int ty = tlo[1]; ty <= thi[1]; ty++)
       for (int tx = tlo[0]; tx <= thi[0]; tx++) {
         const int t = tx + ty * g.tdim[0] + tz * g.tdim[0] * g.tdim[1];
-        mark_tile(a, t);
+        mark_tile(a, t, epoch);
       }
 }
 
@@ -207,7 +207,9 @@ __device__ __forceinline__ int warp_bin_slot(int *count, unsigned key, bool add)
 }
 
 template <int D, int SF>
-__device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool valid) {
+// epoch: the partition the marks are for (the G2P of a step bins for the
+// next); hash_out: where the reference cell hashes go
+__device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool valid, int epoch, unsigned *hash_out) {
   const DevGrid &g = a.g;
   float x[3] = {0.0f, 0.0f, 0.0f}, u[3] = {0.0f, 0.0f, 0.0f};
   int b[3] = {0, 0, 0};
@@ -224,7 +226,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
       in_axes = in_axes && b[c] >= 0 && b[c] < g.n[c];
     }
     const unsigned hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
-    a.P.hash[s] = hu;
+    hash_out[s] = hu;
     if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual) {
       int d[3] = {0, 0, 0};
 #pragma unroll
@@ -236,7 +238,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
     } else {
       key = hu;
       binned = hu < (unsigned)g.ntotal;
-      mark_tiles<D, SF>(a, b, hu, binned, in_axes);
+      mark_tiles<D, SF>(a, b, hu, binned, in_axes, epoch);
     }
     // with a sentinel key (batched ensembles) a particle outside the grid is
     // sorted into its instance's extra last key, so instances keep their
@@ -252,10 +254,10 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
   if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual && binned && slot == 0) {
     // all particles of a dual cell share its tiles and brick: the cell's
     // first arrival marks them
-    mark_tiles_dual<D>(a, dcell);
+    mark_tiles_dual<D>(a, dcell, epoch);
     if (a.B.brick_epoch) {
       const int bi = dcell[0] / 8 + (dcell[1] / 8) * a.B.kb[0] + (dcell[2] / 8) * a.B.kb[0] * a.B.kb[1];
-      if (a.B.brick_epoch[bi] != a.epoch) a.B.brick_epoch[bi] = a.epoch;
+      if (a.B.brick_epoch[bi] != epoch) a.B.brick_epoch[bi] = epoch;
     }
   }
   a.P.key[s] = (unsigned)a.B.key_base + key;
@@ -267,7 +269,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
 template <int D, int SF>
 __global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  hash_count_body<D, SF>(a, s, s < a.P.n);
+  hash_count_body<D, SF>(a, s, s < a.P.n, a.epoch, a.P.hash);
 }
 
 constexpr int kScanThreads = 1024;
@@ -2337,10 +2339,18 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
   if (do_stress) stress_update_point<D, FULL>(a, s, L);
 }
 
+// bin_next (3D quadratic, dual binning): the step's last G2P also bins the
+// new positions for the next partition (counts, slots, keys, tile and brick
+// marks of epoch + 1), which then skips its binning pass.
 template <int D, int SF, bool FULL>
 __global__ void __launch_bounds__(256, FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 3 : 4)) k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
+  if constexpr (D == 3 && SF == PMPM_SHAPE_QUADRATIC) {
+    // the reference hashes of the new positions wait in hash_next until
+    // the next partition: the views of this step's partition stay readable
+    if (a.bin_next) hash_count_body<D, SF>(a, s, s < a.P.n, a.epoch + 1, a.hash_next);
+  }
 }
 
 // Stress update alone from the stored velocity gradient.
@@ -2478,7 +2488,7 @@ __global__ void __launch_bounds__(256) kb_hash_count(const StepArgs *views, cons
   const BatchBlock b = blocks[blockIdx.x];
   load_view(sa, views, b.inst, P, epoch);
   const int s = b.first + (int)threadIdx.x;
-  hash_count_body<D, SF>(sa, s, s < b.end);
+  hash_count_body<D, SF>(sa, s, s < b.end, sa.epoch, sa.P.hash);
 }
 
 template <int D, int SF>

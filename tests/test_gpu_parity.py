@@ -577,3 +577,31 @@ def test_autotune_keeps_state_and_both_variants_match_oracle():
     tol = cond_tol(scene, 2, FIELDS, STEP_TOL)
     for name in FIELDS:
         assert rel(sim.get(name), ref[name]) <= tol[name], name
+
+
+def test_binning_ahead_keeps_reference_views_and_survives_edits():
+    """3D quadratic steps bin the next partition inside their G2P: after a
+    step the reference partition views still describe that step's own
+    partition, and positions edited between steps are binned afresh."""
+    scene = STEP_CASES["column_3d_quadratic_dp"]()
+    sim, ref = make_pair(scene)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(2)
+    ref.solve(2)
+    for name in ("hash_unsorted", "hash_sorted", "sorted_index", "cell_start", "cell_end"):
+        np.testing.assert_array_equal(sim.get(name), ref[name], err_msg=name)
+    rng = np.random.default_rng(8)
+    x = ref["positions"].astype(np.float64)
+    x = (x + rng.uniform(-0.3, 0.3, x.shape) * scene["cell_size"]).astype(np.float32)
+    lo = np.array(scene["origin"]) + 1.5 * scene["cell_size"]
+    hi = np.array(scene["end"]) - 1.5 * scene["cell_size"]
+    x = np.clip(x, lo, hi).astype(np.float32)
+    sim.set("positions", x)
+    ref["positions"][:] = x
+    sim.solve(1)
+    ref.solve(1)
+    assert sim.synchronize() == 0
+    np.testing.assert_array_equal(sim.get("hash_unsorted"), ref["hash_unsorted"])
+    for name in ("positions", "velocities"):
+        assert rel(sim.get(name), ref[name]) <= 1e-4, name
