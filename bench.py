@@ -611,8 +611,8 @@ def main():
         sub = argparse.Namespace(**vars(args))
         sub.no_cpu_baseline = True
         sub.steps = 10
-        ens = run_ensemble(sub, world, rank, local, pg, emit=False)
         cal = run_calibration(sub, world, rank, local, pg, emit=False)
+        ens = run_ensemble(sub, world, rank, local, pg, emit=False)
         if rank == 0:
             companions = {
                 "batched": {"value": ens["value"], "unit": "particle-steps/s", "workload": ens["config"]["workload"],
@@ -620,9 +620,13 @@ def main():
                             "over_one_sim_per_launch": ens["config"]["batched_over_one_sim_per_launch"]},
                 "fwd_adjoint": {"value": cal["value"], "unit": "particle-steps/s",
                                 "workload": cal["config"]["workload"], "ms_per_step": cal["ms_per_step"],
+                                "plain_forward_ms_per_step": cal["config"]["plain_forward_ms_per_step"],
+                                "rollout_forward_ms_per_step": cal["config"]["rollout_forward_ms_per_step"],
+                                "adjoint_ms_per_step": cal["config"]["adjoint_ms_per_step"],
                                 "over_plain_forward": cal["config"]["fwd_plus_adjoint_over_plain_forward"],
                                 "checkpoints_only_over_plain_forward":
-                                    cal["config"]["checkpoints_only"]["fwd_plus_adjoint_over_plain_forward"]},
+                                    cal["config"]["checkpoints_only"]["fwd_plus_adjoint_over_plain_forward"],
+                                "clocks": cal.get("clocks")},
             }
 
     if rank == 0:
