@@ -480,6 +480,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-sample-scale", type=float, default=0.45)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--p2g-kernel", default="auto", choices=["auto", "dual", "cells"],
+                    help="3D quadratic P2G kernel: autotuned (default) or fixed (fixed for profiling runs, "
+                         "whose serialised launches make the autotuner's timings meaningless)")
     ap.add_argument("--no-companions", dest="companions", action="store_false",
                     help="skip the batched-ensemble and calibration legs in the default line")
     args = ap.parse_args()
@@ -508,7 +511,11 @@ def main():
     sim = Simulation(**kw, device=local, resort_interval=args.resort_interval)
     sim.set_particles(scene["positions"], scene["velocities"])
     sim.initialize()
-    p2g_variant = sim.autotune(3)  # the P2G kernel this configuration runs fastest with
+    if args.p2g_kernel == "auto":
+        p2g_variant = sim.autotune(3)  # the P2G kernel this configuration runs fastest with
+    else:
+        p2g_variant = {"dual": 1, "cells": 0}[args.p2g_kernel]
+        sim.set_p2g_kernel(p2g_variant)
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream, device=local)
 

@@ -440,6 +440,9 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
  * steps from the current state, keep the fastest for this handle and put
  * the state (and step counter) back.  *chosen: 1 sweep, 0 cell scatter. */
 int pmpm_autotune(pmpm_sim *s, int steps, int *chosen);
+/* Selects the P2G kernel directly (the autotuner's choices: 1 sweep, 0 cell
+ * scatter); PMPM_ERR_NOT_SUPPORTED where the configuration has only one. */
+int pmpm_set_p2g_kernel(pmpm_sim *s, int variant);
 
 /* ---------------------------------------------------------------------------
  * Differentiable rollouts (no counterpart in the reference).  A rollout of

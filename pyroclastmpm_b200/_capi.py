@@ -86,7 +86,7 @@ EXPORTS = [
     "pmpm_bc_rigidbodylevelset", "pmpm_bc_rigid_sdf", "pmpm_calculate_timestep", "pmpm_material_timestep",
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
     "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
-    "pmpm_material_modified_cam_clay", "pmpm_material_drucker_prager_cap",
+    "pmpm_material_modified_cam_clay", "pmpm_material_drucker_prager_cap", "pmpm_set_p2g_kernel",
 ]
 
 EXPORTS += [
@@ -130,6 +130,7 @@ def lib():
     L.pmpm_rollout_set_memory.argtypes = [vp, ctypes.c_longlong]
     L.pmpm_musl_stage.argtypes = [vp, i]
     L.pmpm_autotune.argtypes = [vp, i, ctypes.POINTER(ctypes.c_int)]
+    L.pmpm_set_p2g_kernel.argtypes = [vp, i]
     L.pmpm_material_von_mises.argtypes = [f, f, f, f, f, ctypes.POINTER(Material)]
     L.pmpm_material_modified_cam_clay.argtypes = [f] * 10 + [ctypes.POINTER(Material)]
     L.pmpm_material_drucker_prager_cap.argtypes = [f] * 11 + [ctypes.POINTER(Material)]
@@ -525,6 +526,10 @@ class Simulation:
         c = ctypes.c_int()
         check(lib().pmpm_autotune(self._h, int(steps), ctypes.byref(c)), "pmpm_autotune")
         return c.value
+
+    def set_p2g_kernel(self, variant):
+        """Select the P2G kernel (1 sweep, 0 cell scatter; 3D quadratic)."""
+        check(lib().pmpm_set_p2g_kernel(self._h, int(variant)), "pmpm_set_p2g_kernel")
 
     # ---- differentiable rollouts ----
     def rollout_forward(self, nsteps, checkpoint_every=25):

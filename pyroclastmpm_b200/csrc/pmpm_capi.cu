@@ -2949,6 +2949,13 @@ extern "C" int pmpm_material_point_vjp(const pmpm_material *mat, int dim, int n,
   return st;
 }
 
+extern "C" int pmpm_set_p2g_kernel(pmpm_sim *s, int variant) {
+  if (!s || (variant != 0 && variant != 1)) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!s->dual) return PMPM_ERR_NOT_SUPPORTED;
+  s->p2g_variant = variant;
+  return PMPM_OK;
+}
+
 extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   if (!s || steps < 1) return PMPM_ERR_INVALID_ARGUMENT;
   if (s->n == 0) return PMPM_ERR_STATE;

@@ -357,35 +357,49 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n
   for (int k = 0; k < kScanPer; k++) sum += v[k];
   int total;
   const int ex_local = block_exclusive_scan(sum, sw, total);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    // warp 0 looks back over 32 predecessors at a time: the nearest one with
+    // an inclusive prefix ends the walk, the aggregates before it add up
+    const int lane = threadIdx.x;
     const unsigned long long t = (unsigned long long)tag << 34;
     int prefix = 0;
     if (blk > 0) {
-      atomicExch(&status[blk], t | kScanAggregate | (unsigned)total);
-      int j = blk - 1;
+      if (lane == 0) atomicExch(&status[blk], t | kScanAggregate | (unsigned)total);
+      int top = blk - 1;
       long long spins = 0;
-      while (j >= 0) {
-        const unsigned long long w = atomicAdd(&status[j], 0ull);
-        if ((w >> 34) != (unsigned long long)tag) {
+      for (;;) {
+        const int idx = top - lane;
+        unsigned long long w = idx >= 0 ? atomicAdd(&status[idx], 0ull) : (t | kScanInclusive);
+        const bool ready = (w >> 34) == (unsigned long long)tag;
+        const unsigned incl = __ballot_sync(0xffffffffu, ready && (w & kScanInclusive));
+        const unsigned rdy = __ballot_sync(0xffffffffu, ready);
+        const int first = incl ? __ffs(incl) - 1 : 31;  // lanes 0..first are needed
+        const unsigned need = first == 31 ? 0xffffffffu : ((1u << (first + 1)) - 1u);
+        if ((rdy & need) != need) {
           if (++spins > (1ll << 22)) {
-            atomicOr(fault, kFaultWaitTimeout);
+            if (lane == 0) atomicOr(fault, kFaultWaitTimeout);
             break;
           }
           continue;
         }
-        prefix += (int)(unsigned)(w & 0xffffffffull);
-        if (w & kScanInclusive) break;
-        j--;
+        int val = lane <= first ? (int)(unsigned)(w & 0xffffffffull) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+        prefix += val;
+        if (incl) break;
+        top -= 32;
       }
     }
-    atomicExch(&status[blk], t | kScanInclusive | (unsigned)(prefix + total));
-    sh_prefix = prefix;
-    if (blk == nblocks - 1) {
-      offset[n] = prefix + total;
-      scalars[0] = prefix + total;  // binned particles
-      scalars[1] = 0;               // unbinned counter
-      scalars[2] = 0;               // big-cell counter
-      ticket[(tag + 1u) & 1u] = 0;
+    if (lane == 0) {
+      atomicExch(&status[blk], t | kScanInclusive | (unsigned)(prefix + total));
+      sh_prefix = prefix;
+      if (blk == nblocks - 1) {
+        offset[n] = prefix + total;
+        scalars[0] = prefix + total;  // binned particles
+        scalars[1] = 0;               // unbinned counter
+        scalars[2] = 0;               // big-cell counter
+        ticket[(tag + 1u) & 1u] = 0;
+      }
     }
   }
   __syncthreads();

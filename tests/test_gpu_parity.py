@@ -605,3 +605,19 @@ def test_binning_ahead_keeps_reference_views_and_survives_edits():
     np.testing.assert_array_equal(sim.get("hash_unsorted"), ref["hash_unsorted"])
     for name in ("positions", "velocities"):
         assert rel(sim.get(name), ref[name]) <= 1e-4, name
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_each_3d_quadratic_p2g_kernel_matches_oracle(variant):
+    """Both 3D quadratic P2G kernels (cell-row scatter 0, dual sweep 1),
+    selected directly, against the oracle over two steps."""
+    scene = STEP_CASES["column_3d_quadratic_dp"]()
+    sim, ref = make_pair(scene)
+    sim.set_p2g_kernel(variant)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(2)
+    ref.solve(2)
+    tol = cond_tol(scene, 2, FIELDS, STEP_TOL)
+    for name in FIELDS:
+        assert rel(sim.get(name), ref[name]) <= tol[name], name
