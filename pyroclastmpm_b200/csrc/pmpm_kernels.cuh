@@ -2206,6 +2206,11 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
   float L[9];
 #pragma unroll
   for (int k = 0; k < 9; k++) L[k] = 0.0f;
+  // F is loaded before the stencil gather so that its DRAM latency overlaps
+  // the node loads
+  float F[9];
+#pragma unroll
+  for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
   if (SF != PMPM_SHAPE_QUADRATIC || inside) {
     // per-axis weights, node indices and validity
     float N[3][K], dN[3][K];
@@ -2309,9 +2314,7 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
       return;
     }
     // v <- (1 - alpha) v_pic + alpha (v + dv); x += dt v_pic; F <- (I + L dt) F; V = det(F) V0
-    float F[9], A[9], Fn[9];
-#pragma unroll
-    for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
+    float A[9], Fn[9];
 #pragma unroll
     for (int r = 0; r < D; r++)
 #pragma unroll
