@@ -424,7 +424,8 @@ int launch_partition(pmpm_sim *s) {
   s->launches += 7;
   if (D == 3 && !(s->flags & PMPM_FLAG_DETERMINISTIC)) {
     // active-tile queue of the persistent 3D sweep P2G kernels
-    k_tile_list<<<(s->g.ntiles + 255) / 256, 256, 0, st>>>(a);
+    k_tile_list<<<(s->g.ntiles + 255) / 256, 256, 0, st>>>(s->N.tile_epoch, s->g.ntiles, s->epoch, s->N.tile_list,
+                                                          s->N.tile_queue);
     PMPM_LAUNCHED();
     s->launches += 1;
   }
@@ -2020,6 +2021,8 @@ struct pmpm_batch {
   std::vector<int> dynamic_bcs;  // instances whose BC state changes per step (gravity ramp, moving bodies)
   BatchBlock *d_blocks = nullptr;
   int nblocks = 0;
+  int num_sms = 1;       // persistent P2G grid: 8 CTAs per SM x this
+  unsigned p2g_seq = 0;  // P2G launches so far (fetch counter parity)
   BatchTile *d_tiles = nullptr;
   bool has_dp = false, has_sref = false, has_planar = false;
   void *staging = nullptr;
@@ -2164,6 +2167,10 @@ int batch_partition(pmpm_batch *b) {
   cudaStream_t st = b->stream;
   kb_hash_count<D, SF><<<b->nblocks, kTPB, 0, st>>>(b->d_views, b->d_blocks, P, b->epoch);
   PMPM_LAUNCHED();
+  k_tile_list<<<(b->ntiles + 255) / 256, 256, 0, st>>>(b->N.tile_epoch, b->ntiles, b->epoch, b->N.tile_list,
+                                                        b->N.tile_queue);
+  PMPM_LAUNCHED();
+  b->launches += 1;
   const StepArgs ga = batch_global_args(b);
   PMPM_TRY(launch_scan(b->scan, b->B.count, b->nkeys, b->B.offset, b->B.scalars, b->fault, b->nscan_blocks, st));
   k_scatter<<<blocks_for(b->n), kTPB, 0, st>>>(ga);
@@ -2208,8 +2215,13 @@ int batch_step(pmpm_batch *b, float *ms) {
   if (!b->dynamic_bcs.empty()) PMPM_TRY(upload_views(b, true));
   const DevParticles P = batch_particles(b);
   const int gather = (b->flags & PMPM_FLAG_DETERMINISTIC) ? 1 : 0;
-  kb_p2g<D, SF><<<b->ntiles, TileDims<D>::N, 0, b->stream>>>(b->d_views, b->d_tiles, b->N.tile_epoch, P, b->epoch,
-                                                              1, b->node_epoch, gather);
+  {
+    // persistent CTAs over the active-tile queue of this partition
+    const int par = (int)(b->p2g_seq++ & 1u);
+    const int grid = std::min(b->ntiles, 8 * b->num_sms);
+    kb_p2g<D, SF><<<grid, TileDims<D>::N, 0, b->stream>>>(b->d_views, b->d_tiles, b->N.tile_list, b->N.tile_queue, par,
+                                                           b->ntiles, P, b->epoch, 1, b->node_epoch, gather);
+  }
   PMPM_LAUNCHED();
   b->p2g_epoch = b->epoch;
   if (ms) PMPM_CUDA(cudaEventRecord(ev[2], b->stream));
@@ -2266,7 +2278,8 @@ int pmpm_batch_destroy(pmpm_batch *b) {
       if (p) cudaFree(p);
   }
   for (void *p : {(void *)b->slot, (void *)b->key, (void *)b->N.m, (void *)b->N.p, (void *)b->N.pnt, (void *)b->N.vel,
-                  (void *)b->N.tile_epoch, (void *)b->node_epoch, (void *)b->B.count, (void *)b->B.offset,
+                  (void *)b->N.tile_epoch, (void *)b->N.tile_list, (void *)b->N.tile_queue, (void *)b->node_epoch,
+                  (void *)b->B.count, (void *)b->B.offset,
                   (void *)b->B.order, (void *)b->B.block_sums, (void *)b->B.scalars, (void *)b->B.big_cells,
                   (void *)b->fault, (void *)b->d_views, (void *)b->d_blocks, (void *)b->d_tiles, b->staging})
     if (p) cudaFree(p);
@@ -2363,6 +2376,11 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
   if (st == PMPM_OK) st = dalloc(&b->N.pnt, (size_t)b->nn * D);
   if (st == PMPM_OK) st = dalloc(&b->N.vel, (size_t)b->nn * F);
   if (st == PMPM_OK) st = dalloc(&b->N.tile_epoch, (size_t)b->ntiles);
+  if (st == PMPM_OK) st = dalloc(&b->N.tile_list, (size_t)b->ntiles);
+  if (st == PMPM_OK) st = dalloc(&b->N.tile_queue, 4);
+  if (st == PMPM_OK && cudaMemset(b->N.tile_queue, 0, 4 * sizeof(int)) != cudaSuccess) st = PMPM_ERR_CUDA;
+  if (st == PMPM_OK && cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    st = PMPM_ERR_CUDA;
   if (st == PMPM_OK) st = dalloc(&b->node_epoch, (size_t)b->ntiles);
   b->nscan_blocks = (b->nkeys + kScanChunk - 1) / kScanChunk;
   if (st == PMPM_OK) st = dalloc(&b->B.count, (size_t)b->nkeys);

@@ -53,11 +53,12 @@ __device__ __forceinline__ void mark_tile(const StepArgs &a, int t, int epoch) {
 // Active-tile queue of this partition: the tiles marked with its epoch, in
 // tile order within each warp (one atomic per warp).  Runs after the binning
 // pass; clears the next partition's count.
-__global__ void __launch_bounds__(256) k_tile_list(StepArgs a) {
+__global__ void __launch_bounds__(256) k_tile_list(const int *tile_epoch, int ntiles, int epoch, int *tile_list,
+                                                   int *tile_queue) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int *count = &a.N.tile_queue[a.epoch & 1];
-  if (t == 0) a.N.tile_queue[(a.epoch + 1) & 1] = 0;
-  const bool on = t < a.g.ntiles && a.N.tile_epoch[t] == a.epoch;
+  int *count = &tile_queue[epoch & 1];
+  if (t == 0) tile_queue[(epoch + 1) & 1] = 0;
+  const bool on = t < ntiles && tile_epoch[t] == epoch;
   const unsigned m = __ballot_sync(0xffffffffu, on);
   if (!m) return;
   const int lane = threadIdx.x & 31;
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(256) k_tile_list(StepArgs a) {
   base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
   if (on) {
     const int i = base + __popc(m & ((1u << lane) - 1u));
-    if (i < a.g.ntiles) a.N.tile_list[i] = t;
+    if (i < ntiles) tile_list[i] = t;
   }
 }
 
@@ -2508,19 +2509,32 @@ __global__ void __launch_bounds__(256) kb_hash_count(const StepArgs *views, cons
   hash_count_body<D, SF>(sa, s, s < b.end, sa.epoch, sa.P.hash);
 }
 
+// Persistent CTAs over the batch's active-tile queue (tile_list[0 ..
+// tile_queue[epoch & 1]) are global tile indices; tile_queue[2 + par] is this
+// launch's fetch counter, the other one is reset for the next launch).
 template <int D, int SF>
 __global__ void __launch_bounds__(TileDims<D>::N) kb_p2g(const StepArgs *views, const BatchTile *tiles,
-                                                         const int *tile_epoch, DevParticles P, int epoch,
-                                                         int apply_bcs, int *node_epoch, int gather) {
+                                                         const int *tile_list, int *tile_queue, int par,
+                                                         int ntiles, DevParticles P, int epoch, int apply_bcs,
+                                                         int *node_epoch, int gather) {
   __shared__ StepArgs sa;
-  const BatchTile t = tiles[blockIdx.x];
-  if (tile_epoch[t.global_tile] != epoch) return;  // inactive: skip the view copy
-  load_view(sa, views, t.inst, P, epoch);
-  int *ne = node_epoch + (t.global_tile - t.tile);
-  if (gather)
-    p2g_gather_body<D, SF>(sa, t.tile, apply_bcs, ne);
-  else
-    p2g_tile_body<D, SF>(sa, t.tile, apply_bcs, ne);
+  __shared__ int cur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) tile_queue[2 + (par ^ 1)] = 0;
+  const int count = min(tile_queue[epoch & 1], ntiles);
+  for (;;) {
+    if (threadIdx.x == 0) cur = atomicAdd(&tile_queue[2 + par], 1);
+    __syncthreads();
+    const int idx = cur;
+    __syncthreads();
+    if (idx >= count) break;
+    const BatchTile t = tiles[tile_list[idx]];
+    load_view(sa, views, t.inst, P, epoch);
+    int *ne = node_epoch + (t.global_tile - t.tile);
+    if (gather)
+      p2g_gather_body<D, SF>(sa, t.tile, apply_bcs, ne);
+    else
+      p2g_tile_body<D, SF>(sa, t.tile, apply_bcs, ne);
+  }
 }
 
 template <int D, int SF>
