@@ -471,7 +471,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   StepArgs a = make_args(s);
   if (s->flags & PMPM_FLAG_DETERMINISTIC) {
     k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
-  } else if (s->dual) {
+  } else if (D == 3 && s->dual) {
     constexpr int bytes = dual3_smem_bytes();
     static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
@@ -1142,6 +1142,17 @@ int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float fact
   }
 }
 
+// Binning key space: reference cells, or dual cells (floor(x/h + 1/2), one
+// more per axis) for quadratic shape functions outside the deterministic mode.
+static void set_key_space(pmpm_sim *s) {
+  s->dual = s->shape == PMPM_SHAPE_QUADRATIC && !(s->flags & PMPM_FLAG_DETERMINISTIC);
+  s->nkeys = 1;
+  for (int c = 0; c < 3; c++) {
+    s->kd[c] = (s->dual && c < s->dim) ? s->g.n[c] + 1 : s->g.n[c];
+    s->nkeys *= s->kd[c];
+  }
+}
+
 // Descriptor -> handle parameters: grid, materials and boundary conditions
 // (BodyForce arrays are copied to the device; nothing else is allocated).
 static int setup_handle(const pmpm_desc *desc, pmpm_sim *s) {
@@ -1327,13 +1338,7 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK && cudaMemset(s->N.tile_queue, 0, 4 * sizeof(int)) != cudaSuccess) st = PMPM_ERR_CUDA;
   if (st == PMPM_OK && cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess)
     st = PMPM_ERR_CUDA;
-  // binning key space (reference cells, or dual cells for the 3D quadratic fast path)
-  s->dual = s->dim == 3 && s->shape == PMPM_SHAPE_QUADRATIC && !(s->flags & PMPM_FLAG_DETERMINISTIC);
-  s->nkeys = 1;
-  for (int c = 0; c < 3; c++) {
-    s->kd[c] = (s->dual && c < s->dim) ? g.n[c] + 1 : g.n[c];
-    s->nkeys *= s->kd[c];
-  }
+  set_key_space(s);
   const size_t nk = (size_t)s->nkeys;
   s->nscan_blocks = (s->nkeys + kScanChunk - 1) / kScanChunk;
   if (st == PMPM_OK) st = dalloc(&s->B.count, nk);
@@ -1342,7 +1347,7 @@ int pmpm_create(const pmpm_desc *desc, pmpm_sim **out) {
   if (st == PMPM_OK) st = alloc_scan(s->scan, s->nscan_blocks);
   if (st == PMPM_OK) st = dalloc(&s->B.scalars, 4);
   if (st == PMPM_OK) st = dalloc(&s->B.big_cells, nk);
-  if (st == PMPM_OK && s->dual) {
+  if (st == PMPM_OK && s->dual && s->dim == 3) {
     s->nbricks = 1;
     for (int c = 0; c < 3; c++) {
       s->B.kb[c] = (s->kd[c] + Cells3::B - 1) / Cells3::B;
@@ -2047,8 +2052,9 @@ StepArgs batch_view(pmpm_batch *b, int i) {
   a.N.vel = b->N.vel + (size_t)F * b->noff[i];
   a.N.tile_epoch = b->N.tile_epoch + b->toff[i];
   a.B = b->B;
-  a.B.dual = 0;
-  a.B.nkeys = h->g.ntotal + 1;
+  a.B.dual = h->dual ? 1 : 0;
+  for (int c = 0; c < 3; c++) a.B.kd[c] = h->kd[c];
+  a.B.nkeys = h->nkeys + 1;  // the instance's keys and its sentinel
   a.B.key_base = b->koff[i];
   a.B.sentinel = 1;
   a.B.count = b->B.count + b->koff[i];
@@ -2309,6 +2315,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
     b->inst.push_back(h);
     st = setup_handle(in.desc, h);
     if (st != PMPM_OK) break;
+    set_key_space(h);
     h->device = device;
     if (i == 0) {
       b->dim = h->dim;
@@ -2335,7 +2342,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
     n += in.num_particles;
     nn += h->g.ntotal;
     nt += h->g.ntiles;
-    nk += h->g.ntotal + 1;
+    nk += (long long)h->nkeys + 1;
   }
   if (st == PMPM_OK && (n > INT32_MAX / 2 || nn > INT32_MAX / 8 || nk > INT32_MAX / 2)) st = PMPM_ERR_NOT_SUPPORTED;
   if (st != PMPM_OK) {
@@ -2969,7 +2976,7 @@ extern "C" int pmpm_material_point_vjp(const pmpm_material *mat, int dim, int n,
 
 extern "C" int pmpm_set_p2g_kernel(pmpm_sim *s, int variant) {
   if (!s || (variant != 0 && variant != 1)) return PMPM_ERR_INVALID_ARGUMENT;
-  if (!s->dual) return PMPM_ERR_NOT_SUPPORTED;
+  if (!s->dual || s->dim != 3) return PMPM_ERR_NOT_SUPPORTED;
   s->p2g_variant = variant;
   return PMPM_OK;
 }
@@ -2979,7 +2986,7 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   if (s->n == 0) return PMPM_ERR_STATE;
   PMPM_CUDA(cudaSetDevice(s->device));
   std::vector<int> cands;
-  if (s->dual) cands = {1, 0};
+  if (s->dual && s->dim == 3) cands = {1, 0};
   if (cands.size() < 2) {
     if (chosen) *chosen = s->p2g_variant;
     return PMPM_OK;

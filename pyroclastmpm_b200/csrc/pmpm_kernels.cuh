@@ -246,7 +246,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
     // storage ranges; it is reported as a fault either way
     sorted = binned;
     if (!binned && a.B.sentinel) {
-      key = (unsigned)g.ntotal;
+      key = (unsigned)(a.B.nkeys - 1);  // the instance's last key
       sorted = true;
     }
   }
@@ -917,6 +917,167 @@ struct P2GTileShape {
   static constexpr int NACC = 1 + 2 * D;
 };
 
+// Particle phase of the tile P2G under dual-cell binning (quadratic): the
+// source cells are the dual cells d in [t0 - 1, t0 + T] per axis, whose
+// particles all reach the same nodes d - 1 .. d + 1 (clamped onto the grid).
+// Each thread takes a contiguous chunk of the cell-sorted list; with RUN,
+// consecutive particles of one dual cell are summed in registers and the
+// cell's window is added to the shared accumulators once per run.
+template <int D, bool RUN>
+__device__ __forceinline__ void p2g_dual_particles(const StepArgs &a, const int t0[3], float *acc, int *row_k0,
+                                                   int *row_pref, int *warp_tmp) {
+  using T = TileDims<D>;
+  constexpr int NT = T::N;
+  constexpr int RY = T::Y + 2, RZ = D == 3 ? T::Z + 2 : 1;
+  constexpr int ROWS = RY * RZ;
+  constexpr int NW = D == 3 ? 27 : 9;  // window nodes
+  constexpr int NV = 1 + 2 * D;        // mass, momentum, force
+  const DevGrid &g = a.g;
+  const DevParticles &P = a.P;
+  const int st = P.stride;
+  const int tid = threadIdx.x;
+  const long long kd0 = a.B.kd[0], kd01 = (long long)a.B.kd[0] * a.B.kd[1];
+  // ---- source rows (along x) -> sorted-order ranges ----
+  int carry = 0;
+  for (int it = 0; it < (ROWS + NT - 1) / NT; it++) {
+    const int r = it * NT + tid;
+    int cnt = 0, k0 = 0;
+    if (r < ROWS) {
+      const int dy = t0[1] - 1 + r % RY, dz = D == 3 ? t0[2] - 1 + r / RY : 0;
+      const int dx0 = max(t0[0] - 1, 0), dx1 = min(t0[0] + T::X, g.n[0]);  // dual coordinates run 0 .. n
+      const bool row_in = dy >= 0 && dy <= g.n[1] && (D == 2 || (dz >= 0 && dz <= g.n[2]));
+      if (row_in && dx0 <= dx1) {
+        const long long base = (long long)dy * kd0 + (long long)dz * kd01;
+        k0 = a.B.offset[base + dx0];
+        cnt = a.B.offset[base + dx1 + 1] - k0;
+      }
+    }
+    int total;
+    const int ex = block_exclusive_scan(cnt, warp_tmp, total);
+    if (r < ROWS) {
+      row_k0[r] = k0;
+      row_pref[r] = carry + ex;
+    }
+    carry += total;
+  }
+  if (tid == 0) row_pref[ROWS] = carry;
+  __syncthreads();
+  const int ntot = row_pref[ROWS];
+  // contiguous chunks; the lanes of a warp take chunks NT/32 apart
+  const int chunk = (ntot + NT - 1) / NT;
+  const int slot = (tid & 31) * (NT / 32) + (tid >> 5);
+  const int j0 = slot * chunk, j1 = min(j0 + chunk, ntot);
+  int row = 0;
+  if (j0 < j1) {
+    int lo = 0, hi = ROWS;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (row_pref[mid] <= j0) lo = mid; else hi = mid;
+    }
+    row = lo;
+  }
+  float run[RUN ? NW : 1][NV];
+#pragma unroll
+  for (int w = 0; w < (RUN ? NW : 1); w++)
+#pragma unroll
+    for (int v = 0; v < NV; v++) run[w][v] = 0.0f;
+  int run_d[3] = {0, 0, 0};
+  bool have_run = false;
+  // adds a window's values (node k of each axis at d - 1 + k, clamped) to
+  // the shared accumulators of the tile nodes it reaches
+  auto add_window = [&](const int d[3], int w, const float *val) {
+    const int kx = w % 3, ky = (w / 3) % 3, kz = D == 3 ? w / 9 : 0;
+    const int nx = min(max(d[0] - 1 + kx, 0), g.n[0] - 1) - t0[0];
+    const int ny = min(max(d[1] - 1 + ky, 0), g.n[1] - 1) - t0[1];
+    const int nz = D == 3 ? min(max(d[2] - 1 + kz, 0), g.n[2] - 1) - t0[2] : 0;
+    if (nx < 0 || nx >= T::X || ny < 0 || ny >= T::Y || nz < 0 || nz >= T::Z) return;
+    const int ln = nx + T::X * (ny + T::Y * nz);
+#pragma unroll
+    for (int v = 0; v < NV; v++) atomicAdd(&acc[v * NT + ln], val[v]);
+  };
+  for (int j = j0; j < j1; j++) {
+    while (row_pref[row + 1] <= j) row++;
+    const int s = a.B.order[row_k0[row] + (j - row_pref[row])];
+    float u[3] = {0, 0, 0};
+    int d[3] = {0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+      d[c] = dual_coord(u[c], (int)u[c]);
+    }
+    if (RUN) {
+      const bool same = have_run && d[0] == run_d[0] && d[1] == run_d[1] && (D == 2 || d[2] == run_d[2]);
+      if (have_run && !same) {
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+          add_window(run_d, w, run[w]);
+#pragma unroll
+          for (int v = 0; v < NV; v++) run[w][v] = 0.0f;
+        }
+      }
+      have_run = true;
+#pragma unroll
+      for (int c = 0; c < 3; c++) run_d[c] = d[c];
+    }
+    float N[3][3], dN[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        N[c][k] = 1.0f;
+        dN[c][k] = 0.0f;
+        if (c < D) axis_weight<PMPM_SHAPE_QUADRATIC>(u[c] - (float)(d[c] - 1 + k), g.inv_h, 0, N[c][k], dN[c][k]);
+      }
+    const float m = P.m[s];
+    float mv[3] = {0, 0, 0}, fx[3] = {0, 0, 0}, S[9];
+#pragma unroll
+    for (int c = 0; c < D; c++) mv[c] = m * P.v[c * st + s];
+    if (a.has_planar && !a.remap) {
+#pragma unroll
+      for (int c = 0; c < D; c++) fx[c] = P.fext[c * st + s];
+    }
+    load_sig3<D>(P, s, S);
+    const float nvol = a.remap ? 0.0f : -P.V[s];
+#pragma unroll
+    for (int k = 0; k < 9; k++) S[k] *= nvol;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+      const int kx = w % 3, ky = (w / 3) % 3, kz = D == 3 ? w / 9 : 0;
+      float psi, dpsi[3];
+      if (D == 2) {
+        psi = N[0][kx] * N[1][ky];
+        dpsi[0] = dN[0][kx] * N[1][ky];
+        dpsi[1] = dN[1][ky] * N[0][kx];
+        dpsi[2] = 0.0f;
+      } else {
+        psi = N[0][kx] * N[1][ky] * N[2][kz];
+        dpsi[0] = dN[0][kx] * N[1][ky] * N[2][kz];
+        dpsi[1] = dN[1][ky] * N[0][kx] * N[2][kz];
+        dpsi[2] = dN[2][kz] * N[0][kx] * N[1][ky];
+      }
+      float val[NV];
+      val[0] = psi * m;
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        float f = psi * fx[c] + S[3 * c + 0] * dpsi[0] + S[3 * c + 1] * dpsi[1];
+        if (D == 3) f += S[3 * c + 2] * dpsi[2];
+        val[1 + c] = psi * mv[c];
+        val[1 + D + c] = f;
+      }
+      if (RUN) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) run[w][v] += val[v];
+      } else {
+        add_window(d, w, val);
+      }
+    }
+  }
+  if (RUN && have_run) {
+#pragma unroll
+    for (int w = 0; w < NW; w++) add_window(run_d, w, run[w]);
+  }
+}
+
 template <int D, int SF>
 __device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int apply_bcs, int *node_epoch) {
   using T = TileDims<D>;
@@ -939,213 +1100,225 @@ __device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int a
   for (int k = 0; k < Sh::NACC; k++) acc[k * NT + tid] = 0.0f;
   if (tid == 0) node_epoch[tile] = a.epoch;
 
-  // ---- halo rows -> flat cell intervals -> sorted-order ranges ----
-  // Interior tiles (halo inside the grid) have disjoint, increasing row
-  // intervals.  Near the grid boundary the reference's flat arithmetic can
-  // make virtual rows overlap, so there the intervals are sorted and merged
-  // (each particle must be visited once).
-  bool interior = true;
-  {
-    const int tsz[3] = {T::X, T::Y, T::Z};
-#pragma unroll
-    for (int c = 0; c < D; c++)
-      interior = interior && t0[c] - Sh::HI >= 0 && t0[c] + tsz[c] - 1 - Sh::LO <= g.n[c] - 1;
-  }
-  const bool merge = SF != PMPM_SHAPE_QUADRATIC && !interior;
-  for (int r = tid; r < Sh::ROWS; r += NT) {
-    const int cy = t0[1] - Sh::HI + r % Sh::HY;
-    const int cz = D == 3 ? t0[2] - Sh::HI + r / Sh::HY : 0;
-    int x0 = t0[0] - Sh::HI, x1 = t0[0] + T::X - 1 - Sh::LO;
-    long long lo, hi;
-    if (SF == PMPM_SHAPE_QUADRATIC) {
-      const bool row_in = cy >= 0 && cy < g.n[1] && cz >= 0 && cz < g.n[2];
-      x0 = max(x0, 0);
-      x1 = min(x1, g.n[0] - 1);
-      lo = flat_index(g, x0, cy, cz);
-      hi = row_in ? (long long)flat_index(g, x1, cy, cz) : lo - 1;
-    } else {
-      const long long base = (long long)cy * g.n[0] + (long long)cz * g.n[0] * g.n[1];
-      lo = max(base + x0, 0ll);
-      hi = min(base + x1, (long long)g.ntotal - 1);
+  bool dual_done = false;
+  if constexpr (SF == PMPM_SHAPE_QUADRATIC) {
+    static_assert(Sh::ROWS >= (TileDims<D>::Y + 2) * (D == 3 ? TileDims<D>::Z + 2 : 1), "dual source rows");
+    if (a.B.dual) {
+      // dual-cell binning: the source cells are the dual cells whose
+      // windows reach the tile
+      p2g_dual_particles<D, D == 2>(a, t0, acc, row_k0, row_pref, warp_tmp);
+      dual_done = true;
     }
-    // keep 0 <= lo and hi <= ntotal - 1; lo > hi marks an empty row
-    row_lo[r] = (int)min(max(lo, 0ll), (long long)g.ntotal);
-    row_hi[r] = (int)max(min(hi, (long long)g.ntotal - 1), -1ll);
   }
-  __syncthreads();
-  if (merge && tid == 0) {
-    // insertion sort by interval start, then clip each start past the
-    // furthest end seen so far
-    for (int i = 1; i < Sh::ROWS; i++) {
-      const int l = row_lo[i], h = row_hi[i];
-      int j = i - 1;
-      while (j >= 0 && row_lo[j] > l) {
-        row_lo[j + 1] = row_lo[j];
-        row_hi[j + 1] = row_hi[j];
-        j--;
+  if (!dual_done) {
+    // ---- halo rows -> flat cell intervals -> sorted-order ranges ----
+    // Interior tiles (halo inside the grid) have disjoint, increasing row
+    // intervals.  Near the grid boundary the reference's flat arithmetic can
+    // make virtual rows overlap, so there the intervals are sorted and merged
+    // (each particle must be visited once).
+    bool interior = true;
+    {
+      const int tsz[3] = {T::X, T::Y, T::Z};
+  #pragma unroll
+      for (int c = 0; c < D; c++)
+        interior = interior && t0[c] - Sh::HI >= 0 && t0[c] + tsz[c] - 1 - Sh::LO <= g.n[c] - 1;
+    }
+    const bool merge = SF != PMPM_SHAPE_QUADRATIC && !interior;
+    for (int r = tid; r < Sh::ROWS; r += NT) {
+      const int cy = t0[1] - Sh::HI + r % Sh::HY;
+      const int cz = D == 3 ? t0[2] - Sh::HI + r / Sh::HY : 0;
+      int x0 = t0[0] - Sh::HI, x1 = t0[0] + T::X - 1 - Sh::LO;
+      long long lo, hi;
+      if (SF == PMPM_SHAPE_QUADRATIC) {
+        const bool row_in = cy >= 0 && cy < g.n[1] && cz >= 0 && cz < g.n[2];
+        x0 = max(x0, 0);
+        x1 = min(x1, g.n[0] - 1);
+        lo = flat_index(g, x0, cy, cz);
+        hi = row_in ? (long long)flat_index(g, x1, cy, cz) : lo - 1;
+      } else {
+        const long long base = (long long)cy * g.n[0] + (long long)cz * g.n[0] * g.n[1];
+        lo = max(base + x0, 0ll);
+        hi = min(base + x1, (long long)g.ntotal - 1);
       }
-      row_lo[j + 1] = l;
-      row_hi[j + 1] = h;
+      // keep 0 <= lo and hi <= ntotal - 1; lo > hi marks an empty row
+      row_lo[r] = (int)min(max(lo, 0ll), (long long)g.ntotal);
+      row_hi[r] = (int)max(min(hi, (long long)g.ntotal - 1), -1ll);
     }
-    int maxend = -1;
-    for (int i = 0; i < Sh::ROWS; i++) {
-      if (row_lo[i] > row_hi[i]) continue;
-      if (row_lo[i] <= maxend) row_lo[i] = maxend + 1;
-      if (row_hi[i] > maxend) maxend = row_hi[i];
-    }
-  }
-  __syncthreads();
-  const int nrow_iter = (Sh::ROWS + NT - 1) / NT;
-  int carry = 0;
-  for (int it = 0; it < nrow_iter; it++) {
-    const int r = it * NT + tid;
-    int cnt = 0, k0 = 0;
-    if (r < Sh::ROWS) {
-      const int lo = row_lo[r], hi = row_hi[r];
-      if (lo <= hi) {
-        k0 = a.B.offset[lo];
-        cnt = a.B.offset[hi + 1] - k0;
+    __syncthreads();
+    if (merge && tid == 0) {
+      // insertion sort by interval start, then clip each start past the
+      // furthest end seen so far
+      for (int i = 1; i < Sh::ROWS; i++) {
+        const int l = row_lo[i], h = row_hi[i];
+        int j = i - 1;
+        while (j >= 0 && row_lo[j] > l) {
+          row_lo[j + 1] = row_lo[j];
+          row_hi[j + 1] = row_hi[j];
+          j--;
+        }
+        row_lo[j + 1] = l;
+        row_hi[j + 1] = h;
+      }
+      int maxend = -1;
+      for (int i = 0; i < Sh::ROWS; i++) {
+        if (row_lo[i] > row_hi[i]) continue;
+        if (row_lo[i] <= maxend) row_lo[i] = maxend + 1;
+        if (row_hi[i] > maxend) maxend = row_hi[i];
       }
     }
-    int total;
-    const int ex = block_exclusive_scan(cnt, warp_tmp, total);
-    if (r < Sh::ROWS) {
-      row_k0[r] = k0;
-      row_pref[r] = carry + ex;
+    __syncthreads();
+    const int nrow_iter = (Sh::ROWS + NT - 1) / NT;
+    int carry = 0;
+    for (int it = 0; it < nrow_iter; it++) {
+      const int r = it * NT + tid;
+      int cnt = 0, k0 = 0;
+      if (r < Sh::ROWS) {
+        const int lo = row_lo[r], hi = row_hi[r];
+        if (lo <= hi) {
+          k0 = a.B.offset[lo];
+          cnt = a.B.offset[hi + 1] - k0;
+        }
+      }
+      int total;
+      const int ex = block_exclusive_scan(cnt, warp_tmp, total);
+      if (r < Sh::ROWS) {
+        row_k0[r] = k0;
+        row_pref[r] = carry + ex;
+      }
+      carry += total;
     }
-    carry += total;
-  }
-  if (tid == 0) row_pref[Sh::ROWS] = carry;
-  __syncthreads();
-  const int ntot = row_pref[Sh::ROWS];
+    if (tid == 0) row_pref[Sh::ROWS] = carry;
+    __syncthreads();
+    const int ntot = row_pref[Sh::ROWS];
 
-  // ---- particles: each thread takes one contiguous chunk of the list; the
-  // lanes of a warp take chunks NT/32 apart, so their stencils rarely share
-  // nodes (neighbouring chunks lie in neighbouring cells, whose stencils
-  // overlap and would serialise the shared-memory atomics) ----
-  const int chunk = (ntot + NT - 1) / NT;
-  const int slot = (tid & 31) * (NT / 32) + (tid >> 5);
-  const int j0 = slot * chunk, j1 = min(j0 + chunk, ntot);
-  int row = 0;
-  if (j0 < j1) {
-    int lo = 0, hi = Sh::ROWS;  // last row with row_pref <= j0
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (row_pref[mid] <= j0) lo = mid; else hi = mid;
-    }
-    row = lo;
-  }
-  const DevParticles &P = a.P;
-  const int st = P.stride;
-  for (int j = j0; j < j1; j++) {
-    while (row_pref[row + 1] <= j) row++;
-    const int s = a.B.order[row_k0[row] + (j - row_pref[row])];
-    float u[3] = {0, 0, 0};
-    int b[3] = {0, 0, 0};
-    bool inside = true;
-#pragma unroll
-    for (int c = 0; c < D; c++) {
-      u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
-      b[c] = (int)u[c];
-      inside = inside && b[c] >= 0 && b[c] < g.n[c];
-    }
-    if (SF == PMPM_SHAPE_QUADRATIC && !inside) continue;
-    // per-axis weights, target node coordinates and tile-local coordinates
-    float N[3][K], dN[3][K];
-    int loc[3][K];   // tile-local coordinate, or -1 outside the tile
-    bool inrange[3][K];
-    int woff[3] = {Stencil<SF>::WLO, Stencil<SF>::WLO, Stencil<SF>::WLO};
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        N[c][k] = 1.0f;
-        dN[c][k] = 0.0f;
-        loc[c][k] = 0;
-        inrange[c][k] = true;
+    // ---- particles: each thread takes one contiguous chunk of the list; the
+    // lanes of a warp take chunks NT/32 apart, so their stencils rarely share
+    // nodes (neighbouring chunks lie in neighbouring cells, whose stencils
+    // overlap and would serialise the shared-memory atomics) ----
+    const int chunk = (ntot + NT - 1) / NT;
+    const int slot = (tid & 31) * (NT / 32) + (tid >> 5);
+    const int j0 = slot * chunk, j1 = min(j0 + chunk, ntot);
+    int row = 0;
+    if (j0 < j1) {
+      int lo = 0, hi = Sh::ROWS;  // last row with row_pref <= j0
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (row_pref[mid] <= j0) lo = mid; else hi = mid;
       }
-    const int tsz[3] = {T::X, T::Y, T::Z};
-#pragma unroll
-    for (int c = 0; c < D; c++) {
-      if (SF == PMPM_SHAPE_QUADRATIC) woff[c] = (u[c] - (float)(b[c] - 1)) < 1.5f ? -1 : 0;
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        const int sel = b[c] + woff[c] + k;
-        const bool in = sel >= 0 && sel < g.n[c];
-        const int node_c = SF == PMPM_SHAPE_QUADRATIC ? min(max(sel, 0), g.n[c] - 1) : sel;
-        const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(in ? sel : 0, g.n[c]) : 0;
-        axis_weight<SF>(u[c] - (float)sel, g.inv_h, type, N[c][k], dN[c][k]);
-        inrange[c][k] = SF == PMPM_SHAPE_QUADRATIC ? true : in;
-        const int l = node_c - t0[c];
-        loc[c][k] = (l >= 0 && l < tsz[c]) ? l : -1;
+      row = lo;
+    }
+    const DevParticles &P = a.P;
+    const int st = P.stride;
+    for (int j = j0; j < j1; j++) {
+      while (row_pref[row + 1] <= j) row++;
+      const int s = a.B.order[row_k0[row] + (j - row_pref[row])];
+      float u[3] = {0, 0, 0};
+      int b[3] = {0, 0, 0};
+      bool inside = true;
+  #pragma unroll
+      for (int c = 0; c < D; c++) {
+        u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+        b[c] = (int)u[c];
+        inside = inside && b[c] >= 0 && b[c] < g.n[c];
       }
-    }
-    const float m = P.m[s];
-    float mv[3], fx[3] = {0, 0, 0}, S[9];
-#pragma unroll
-    for (int c = 0; c < D; c++) mv[c] = m * P.v[c * st + s];
-    if (a.has_planar && !a.remap) {
-#pragma unroll
-      for (int c = 0; c < D; c++) fx[c] = P.fext[c * st + s];
-    }
-    load_sig3<D>(P, s, S);
-    const float nvol = a.remap ? 0.0f : -P.V[s];
-#pragma unroll
-    for (int k = 0; k < 9; k++) S[k] *= nvol;
-    const unsigned hu = P.hash[s];
-    constexpr int KZ = D == 3 ? K : 1;
-#pragma unroll
-    for (int ky = 0; ky < K; ky++) {
-#pragma unroll
-      for (int kx = 0; kx < K; kx++) {
-#pragma unroll
-        for (int kz = 0; kz < KZ; kz++) {
-          int lx = loc[0][kx], ly = loc[1][ky], lz = D == 3 ? loc[2][kz] : 0;
-          const bool all_in = inrange[0][kx] && inrange[1][ky] && (D == 2 || inrange[2][kz]);
-          float tN[3] = {N[0][kx], N[1][ky], D == 3 ? N[2][kz] : 1.0f};
-          float tdN[3] = {dN[0][kx], dN[1][ky], D == 3 ? dN[2][kz] : 0.0f};
-          if (!all_in) {
-            // reference aliasing: the slot leaves the grid on an axis; its
-            // node is the flat index hash + flat(window offset)
-            const int w[3] = {woff[0] + kx, woff[1] + ky, D == 3 ? woff[2] + kz : 0};
-            const long long f = (long long)hu + w[0] + (long long)w[1] * g.n[0] +
-                                (long long)w[2] * g.n[0] * g.n[1];
-            if (f < 0 || f >= g.ntotal) continue;
-            const int fc[3] = {(int)(f % g.n[0]), (int)((f / g.n[0]) % g.n[1]),
-                               (int)(f / ((long long)g.n[0] * g.n[1]))};
-            lx = fc[0] - t0[0];
-            ly = fc[1] - t0[1];
-            lz = D == 3 ? fc[2] - t0[2] : 0;
-            if (lx < 0 || lx >= T::X || ly < 0 || ly >= T::Y || lz < 0 || lz >= T::Z) continue;
-            if (SF == PMPM_SHAPE_CUBIC) {
-              // node types of the aliased node (src/shapefunction/shapefunction.cpp:104-110)
-#pragma unroll
-              for (int c = 0; c < D; c++)
-                axis_weight<SF>(u[c] - (float)(b[c] + w[c]), g.inv_h, cubic_node_type(fc[c], g.n[c]), tN[c], tdN[c]);
+      if (SF == PMPM_SHAPE_QUADRATIC && !inside) continue;
+      // per-axis weights, target node coordinates and tile-local coordinates
+      float N[3][K], dN[3][K];
+      int loc[3][K];   // tile-local coordinate, or -1 outside the tile
+      bool inrange[3][K];
+      int woff[3] = {Stencil<SF>::WLO, Stencil<SF>::WLO, Stencil<SF>::WLO};
+  #pragma unroll
+      for (int c = 0; c < 3; c++)
+  #pragma unroll
+        for (int k = 0; k < K; k++) {
+          N[c][k] = 1.0f;
+          dN[c][k] = 0.0f;
+          loc[c][k] = 0;
+          inrange[c][k] = true;
+        }
+      const int tsz[3] = {T::X, T::Y, T::Z};
+  #pragma unroll
+      for (int c = 0; c < D; c++) {
+        if (SF == PMPM_SHAPE_QUADRATIC) woff[c] = (u[c] - (float)(b[c] - 1)) < 1.5f ? -1 : 0;
+  #pragma unroll
+        for (int k = 0; k < K; k++) {
+          const int sel = b[c] + woff[c] + k;
+          const bool in = sel >= 0 && sel < g.n[c];
+          const int node_c = SF == PMPM_SHAPE_QUADRATIC ? min(max(sel, 0), g.n[c] - 1) : sel;
+          const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(in ? sel : 0, g.n[c]) : 0;
+          axis_weight<SF>(u[c] - (float)sel, g.inv_h, type, N[c][k], dN[c][k]);
+          inrange[c][k] = SF == PMPM_SHAPE_QUADRATIC ? true : in;
+          const int l = node_c - t0[c];
+          loc[c][k] = (l >= 0 && l < tsz[c]) ? l : -1;
+        }
+      }
+      const float m = P.m[s];
+      float mv[3], fx[3] = {0, 0, 0}, S[9];
+  #pragma unroll
+      for (int c = 0; c < D; c++) mv[c] = m * P.v[c * st + s];
+      if (a.has_planar && !a.remap) {
+  #pragma unroll
+        for (int c = 0; c < D; c++) fx[c] = P.fext[c * st + s];
+      }
+      load_sig3<D>(P, s, S);
+      const float nvol = a.remap ? 0.0f : -P.V[s];
+  #pragma unroll
+      for (int k = 0; k < 9; k++) S[k] *= nvol;
+      const unsigned hu = P.hash[s];
+      constexpr int KZ = D == 3 ? K : 1;
+  #pragma unroll
+      for (int ky = 0; ky < K; ky++) {
+  #pragma unroll
+        for (int kx = 0; kx < K; kx++) {
+  #pragma unroll
+          for (int kz = 0; kz < KZ; kz++) {
+            int lx = loc[0][kx], ly = loc[1][ky], lz = D == 3 ? loc[2][kz] : 0;
+            const bool all_in = inrange[0][kx] && inrange[1][ky] && (D == 2 || inrange[2][kz]);
+            float tN[3] = {N[0][kx], N[1][ky], D == 3 ? N[2][kz] : 1.0f};
+            float tdN[3] = {dN[0][kx], dN[1][ky], D == 3 ? dN[2][kz] : 0.0f};
+            if (!all_in) {
+              // reference aliasing: the slot leaves the grid on an axis; its
+              // node is the flat index hash + flat(window offset)
+              const int w[3] = {woff[0] + kx, woff[1] + ky, D == 3 ? woff[2] + kz : 0};
+              const long long f = (long long)hu + w[0] + (long long)w[1] * g.n[0] +
+                                  (long long)w[2] * g.n[0] * g.n[1];
+              if (f < 0 || f >= g.ntotal) continue;
+              const int fc[3] = {(int)(f % g.n[0]), (int)((f / g.n[0]) % g.n[1]),
+                                 (int)(f / ((long long)g.n[0] * g.n[1]))};
+              lx = fc[0] - t0[0];
+              ly = fc[1] - t0[1];
+              lz = D == 3 ? fc[2] - t0[2] : 0;
+              if (lx < 0 || lx >= T::X || ly < 0 || ly >= T::Y || lz < 0 || lz >= T::Z) continue;
+              if (SF == PMPM_SHAPE_CUBIC) {
+                // node types of the aliased node (src/shapefunction/shapefunction.cpp:104-110)
+  #pragma unroll
+                for (int c = 0; c < D; c++)
+                  axis_weight<SF>(u[c] - (float)(b[c] + w[c]), g.inv_h, cubic_node_type(fc[c], g.n[c]), tN[c], tdN[c]);
+              }
+            } else if (lx < 0 || ly < 0 || lz < 0) {
+              continue;
             }
-          } else if (lx < 0 || ly < 0 || lz < 0) {
-            continue;
-          }
-          float psi, dpsi[3];
-          if (D == 2) {
-            psi = tN[0] * tN[1];
-            dpsi[0] = tdN[0] * tN[1];
-            dpsi[1] = tdN[1] * tN[0];
-            dpsi[2] = 0.0f;
-          } else {
-            psi = tN[0] * tN[1] * tN[2];
-            dpsi[0] = tdN[0] * tN[1] * tN[2];
-            dpsi[1] = tdN[1] * tN[0] * tN[2];
-            dpsi[2] = tdN[2] * tN[0] * tN[1];
-          }
-          const int ln = lx + T::X * (ly + T::Y * lz);
-          atomicAdd(&acc[ln], psi * m);
-#pragma unroll
-          for (int c = 0; c < D; c++) {
-            float f = psi * fx[c] + S[3 * c + 0] * dpsi[0] + S[3 * c + 1] * dpsi[1];
-            if (D == 3) f += S[3 * c + 2] * dpsi[2];
-            atomicAdd(&acc[(1 + c) * NT + ln], psi * mv[c]);
-            atomicAdd(&acc[(1 + D + c) * NT + ln], f);
+            float psi, dpsi[3];
+            if (D == 2) {
+              psi = tN[0] * tN[1];
+              dpsi[0] = tdN[0] * tN[1];
+              dpsi[1] = tdN[1] * tN[0];
+              dpsi[2] = 0.0f;
+            } else {
+              psi = tN[0] * tN[1] * tN[2];
+              dpsi[0] = tdN[0] * tN[1] * tN[2];
+              dpsi[1] = tdN[1] * tN[0] * tN[2];
+              dpsi[2] = tdN[2] * tN[0] * tN[1];
+            }
+            const int ln = lx + T::X * (ly + T::Y * lz);
+            atomicAdd(&acc[ln], psi * m);
+  #pragma unroll
+            for (int c = 0; c < D; c++) {
+              float f = psi * fx[c] + S[3 * c + 0] * dpsi[0] + S[3 * c + 1] * dpsi[1];
+              if (D == 3) f += S[3 * c + 2] * dpsi[2];
+              atomicAdd(&acc[(1 + c) * NT + ln], psi * mv[c]);
+              atomicAdd(&acc[(1 + D + c) * NT + ln], f);
+            }
           }
         }
       }
@@ -2357,14 +2530,14 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
   if (do_stress) stress_update_point<D, FULL>(a, s, L);
 }
 
-// bin_next (3D quadratic, dual binning): the step's last G2P also bins the
+// bin_next (quadratic, dual binning): the step's last G2P also bins the
 // new positions for the next partition (counts, slots, keys, tile and brick
 // marks of epoch + 1), which then skips its binning pass.
 template <int D, int SF, bool FULL>
 __global__ void __launch_bounds__(256, FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 3 : 4)) k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
-  if constexpr (D == 3 && SF == PMPM_SHAPE_QUADRATIC) {
+  if constexpr (SF == PMPM_SHAPE_QUADRATIC) {
     // the reference hashes of the new positions wait in hash_next until
     // the next partition: the views of this step's partition stay readable
     if (a.bin_next) hash_count_body<D, SF>(a, s, s < a.P.n, a.epoch + 1, a.hash_next);
