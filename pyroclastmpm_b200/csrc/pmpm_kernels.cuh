@@ -1348,7 +1348,7 @@ __device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int a
 }
 
 template <int D, int SF>
-__global__ void __launch_bounds__(TileDims<D>::N) k_p2g_tile(StepArgs a, int apply_bcs, int *node_epoch) {
+__global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) k_p2g_tile(StepArgs a, int apply_bcs, int *node_epoch) {
   p2g_tile_body<D, SF>(a, blockIdx.x, apply_bcs, node_epoch);
 }
 
@@ -2686,7 +2686,7 @@ __global__ void __launch_bounds__(256) kb_hash_count(const StepArgs *views, cons
 // tile_queue[epoch & 1]) are global tile indices; tile_queue[2 + par] is this
 // launch's fetch counter, the other one is reset for the next launch).
 template <int D, int SF>
-__global__ void __launch_bounds__(TileDims<D>::N) kb_p2g(const StepArgs *views, const BatchTile *tiles,
+__global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) kb_p2g(const StepArgs *views, const BatchTile *tiles,
                                                          const int *tile_list, int *tile_queue, int par,
                                                          int ntiles, DevParticles P, int epoch, int apply_bcs,
                                                          int *node_epoch, int gather) {
