@@ -2028,6 +2028,8 @@ struct pmpm_batch {
   int nblocks = 0;
   int num_sms = 1;       // persistent P2G grid: 8 CTAs per SM x this
   unsigned p2g_seq = 0;  // P2G launches so far (fetch counter parity)
+  bool keys_fresh = false;         // the last step's G2P binned the current positions
+  unsigned *hash_next = nullptr;   // their reference hashes [stride]
   BatchTile *d_tiles = nullptr;
   bool has_dp = false, has_sref = false, has_planar = false;
   void *staging = nullptr;
@@ -2169,10 +2171,16 @@ int upload_views(pmpm_batch *b, bool only_dynamic) {
 template <int D, int SF>
 int batch_partition(pmpm_batch *b) {
   b->epoch += 1;
-  const DevParticles P = batch_particles(b);
   cudaStream_t st = b->stream;
-  kb_hash_count<D, SF><<<b->nblocks, kTPB, 0, st>>>(b->d_views, b->d_blocks, P, b->epoch);
-  PMPM_LAUNCHED();
+  if (b->keys_fresh) {
+    std::swap(b->P[b->cur].hash, b->hash_next);  // binned by the last step's G2P
+  } else {
+    const DevParticles P = batch_particles(b);
+    kb_hash_count<D, SF><<<b->nblocks, kTPB, 0, st>>>(b->d_views, b->d_blocks, P, b->epoch);
+    PMPM_LAUNCHED();
+    b->launches += 1;
+  }
+  b->keys_fresh = false;
   k_tile_list<<<(b->ntiles + 255) / 256, 256, 0, st>>>(b->N.tile_epoch, b->ntiles, b->epoch, b->N.tile_list,
                                                         b->N.tile_queue);
   PMPM_LAUNCHED();
@@ -2181,7 +2189,7 @@ int batch_partition(pmpm_batch *b) {
   PMPM_TRY(launch_scan(b->scan, b->B.count, b->nkeys, b->B.offset, b->B.scalars, b->fault, b->nscan_blocks, st));
   k_scatter<<<blocks_for(b->n), kTPB, 0, st>>>(ga);
   PMPM_LAUNCHED();
-  b->launches += 3;
+  b->launches += 2;
   if (b->flags & PMPM_FLAG_DETERMINISTIC) {  // ids in order inside each bin for the gather
     k_sort_cells<<<blocks_for(b->nkeys), kTPB, 0, st>>>(ga);
     PMPM_LAUNCHED();
@@ -2232,8 +2240,13 @@ int batch_step(pmpm_batch *b, float *ms) {
   b->p2g_epoch = b->epoch;
   if (ms) PMPM_CUDA(cudaEventRecord(ev[2], b->stream));
   const int store_L = (b->flags & PMPM_FLAG_KEEP_VELOCITY_GRADIENT) ? 1 : 0;
-  kb_g2p<D, SF><<<b->nblocks, kTPB, 0, b->stream>>>(b->d_views, b->d_blocks, P, b->epoch, 1, store_L);
+  // the next partition's binning rides on this G2P (not with a PlanarDomain,
+  // whose particle forces the binning pass computes)
+  const bool bin_next = !b->has_planar;
+  kb_g2p<D, SF><<<b->nblocks, kTPB, 0, b->stream>>>(b->d_views, b->d_blocks, P, b->epoch, 1, store_L,
+                                                     bin_next ? 1 : 0, b->hash_next);
   PMPM_LAUNCHED();
+  b->keys_fresh = bin_next;
   b->launches += 2;
   b->step += 1;
   if (ms) {
@@ -2283,7 +2296,7 @@ int pmpm_batch_destroy(pmpm_batch *b) {
                     (void *)P.rigid, (void *)P.id, (void *)P.hash})
       if (p) cudaFree(p);
   }
-  for (void *p : {(void *)b->slot, (void *)b->key, (void *)b->N.m, (void *)b->N.p, (void *)b->N.pnt, (void *)b->N.vel,
+  for (void *p : {(void *)b->slot, (void *)b->key, (void *)b->hash_next, (void *)b->N.m, (void *)b->N.p, (void *)b->N.pnt, (void *)b->N.vel,
                   (void *)b->N.tile_epoch, (void *)b->N.tile_list, (void *)b->N.tile_queue, (void *)b->node_epoch,
                   (void *)b->B.count, (void *)b->B.offset,
                   (void *)b->B.order, (void *)b->B.block_sums, (void *)b->B.scalars, (void *)b->B.big_cells,
@@ -2376,6 +2389,7 @@ int pmpm_batch_create(int num_instances, const pmpm_instance *instances, int dev
   const size_t stv = (size_t)b->stride;
   if (st == PMPM_OK) st = dalloc(&b->slot, stv);
   if (st == PMPM_OK) st = dalloc(&b->key, stv);
+  if (st == PMPM_OK) st = dalloc(&b->hash_next, stv);
   if (st == PMPM_OK) st = dalloc(&b->B.order, stv);
   const int F = D == 3 ? NodeVel<3>::F : NodeVel<2>::F;
   if (st == PMPM_OK) st = dalloc(&b->N.m, (size_t)b->nn);
@@ -2557,6 +2571,11 @@ int pmpm_batch_get_field(pmpm_batch *b, int instance, int field, void *dst, size
 int pmpm_batch_set_field(pmpm_batch *b, int instance, int field, const void *src, size_t bytes, int on_device) {
   if (!b || instance < 0 || instance >= (int)b->inst.size()) return PMPM_ERR_INVALID_ARGUMENT;
   if (!batch_field_ok(field) || field >= PMPM_FIELD_NODE_MASSES) return PMPM_ERR_NOT_SUPPORTED;
+  PMPM_CUDA(cudaSetDevice(b->device));
+  if (b->keys_fresh) {  // particle state changes outside a step: redo the binning
+    b->keys_fresh = false;
+    PMPM_CUDA(cudaMemsetAsync(b->B.count, 0, sizeof(int) * (size_t)b->nkeys, b->stream));
+  }
   pmpm_sim v;
   batch_instance_handle(b, instance, v);
   const int st = pmpm_set_field(&v, field, src, bytes, on_device);

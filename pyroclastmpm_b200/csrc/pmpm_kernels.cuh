@@ -2710,14 +2710,18 @@ __global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) kb_p2g(const S
   }
 }
 
+// bin_next: also bin the new positions for the next partition (as k_g2p),
+// their reference hashes into hash_next
 template <int D, int SF>
 __global__ void __launch_bounds__(256) kb_g2p(const StepArgs *views, const BatchBlock *blocks, DevParticles P,
-                                              int epoch, int do_stress, int store_L) {
+                                              int epoch, int do_stress, int store_L, int bin_next,
+                                              unsigned *hash_next) {
   __shared__ StepArgs sa;
   const BatchBlock b = blocks[blockIdx.x];
   load_view(sa, views, b.inst, P, epoch);
   const int s = b.first + (int)threadIdx.x;
   if (s < b.end) g2p_body<D, SF, false>(sa, s, do_stress, store_L);  // batches hold no iterative material
+  if (bin_next) hash_count_body<D, SF>(sa, s, s < b.end, epoch + 1, hash_next);
 }
 
 }  // namespace pmpm
