@@ -89,9 +89,9 @@ struct NodeVel {
 
 struct DevBins {
   // Binning key space.  Reference mode: the reference cell hash (key grid =
-  // node grid).  Dual mode (quadratic fast path): the dual cell
-  // floor(x/h + 1/2), whose particles share one 3x3x3 node window; key grid =
-  // node grid + 1 per axis.
+  // node grid).  Dual mode (quadratic, outside the deterministic mode): the
+  // dual cell floor(x/h + 1/2), whose particles share one 3x3 (3x3x3) node
+  // window; key grid = node grid + 1 per axis.
   int dual;
   int kd[3];
   int nkeys;
