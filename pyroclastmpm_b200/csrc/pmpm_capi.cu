@@ -472,12 +472,12 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   if (s->flags & PMPM_FLAG_DETERMINISTIC) {
     k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
   } else if (D == 3 && s->dual) {
-    constexpr int bytes = dual3_smem_bytes();
+    constexpr int bytes = dual3_smem_bytes<false>(), pbytes = dual3_smem_bytes<true>();
     static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
     if (!attr_set[dev]) {
       PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
       attr_set[dev] = true;
     }
     if (s->p2g_variant == 1) {
@@ -485,7 +485,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
       a.p2g_par = (int)(s->p2g_seq++ & 1u);
       const int grid = std::min(s->g.ntiles, 2 * s->num_sms);
       if (s->has_planar)
-        k_p2g_dual3<true><<<grid, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+        k_p2g_dual3<true><<<grid, Dual3::NT, pbytes, s->stream>>>(a, apply_bcs, s->node_epoch);
       else
         k_p2g_dual3<false><<<grid, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
     } else {

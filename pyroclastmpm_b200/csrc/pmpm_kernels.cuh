@@ -1768,13 +1768,28 @@ struct Dual3 {
   static constexpr int MAXPAIR = NS * 3;
   static constexpr int NCELL = NS * NS;
   static constexpr int NL = T::Z + 2;   // dual layers a tile reads
-  static constexpr int CAP = 960;
-  static constexpr int SLOTS = CAP + NCELL;
   static constexpr int NT = 320;        // threads (10 warps)
   static constexpr int IPT = 2;         // items per thread per round
+  // staged bytes per particle: the x and y weights of the three offsets
+  // (float2 N, dN each), float4 (m, m vx, m vy, m vz), float4 (Sxx, Sxy,
+  // Sxy, Syy), float4 (Sxz, Syz, Szz, Nz2), float4 (Nz0, Nz1, dNz0, dNz1),
+  // with a PlanarDomain float4 (f, 0); S = -V sigma
+  __host__ __device__ static constexpr int slot_bytes(bool planar) { return 6 * 8 + 4 * 16 + (planar ? 16 : 0); }
+  // two CTAs per SM: 116,736 B of shared memory each, less the 1 KB the
+  // runtime reserves, the static tables and the node accumulators
+  static constexpr int STATIC_BYTES = 8448;
+  __host__ __device__ static constexpr int cap(bool planar) {
+    return ((116736 - 1024 - STATIC_BYTES - 7 * T::N * 4) / slot_bytes(planar)) & ~7;
+  }
 };
 
-constexpr int dual3_smem_bytes() { return (7 * TileDims<3>::N + Dual3::SLOTS * (2 + 1 + 3 + 3 + 6 + 6)) * 4; }
+template <bool PLANAR>
+constexpr int dual3_smem_bytes() { return 7 * TileDims<3>::N * 4 + Dual3::cap(PLANAR) * Dual3::slot_bytes(PLANAR); }
+
+// Staged slot of chunk position j: an XOR swizzle inside aligned groups of
+// eight, so lanes reading the same position of neighbouring cells (runs of
+// about eight) hit different shared-memory banks with 8- and 16-byte loads.
+__device__ __forceinline__ int dual_slot(int j) { return j ^ ((j >> 3) & 7); }
 
 __device__ __forceinline__ int build_dual_pairs(int t0, int n, int *pairs) {
   int cnt = 0;
@@ -1826,6 +1841,7 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int NN = T::N;  // nodes per tile
+  constexpr int CAP = W::cap(PLANAR);
   const DevGrid &g = a.g;
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
@@ -1834,15 +1850,14 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   __shared__ int cell_k0[W::NL * W::NCELL], cell_pref[W::NL * W::NCELL + 1];
   __shared__ int warp_tmp[33];
   extern __shared__ __align__(16) float dyn_smem[];
-  constexpr int SL = W::SLOTS;
-  float *acc = dyn_smem;                            // [7][NN]
-  float(*st_u)[SL] = (float(*)[SL])(acc + 7 * NN);  // [2] scaled x, y
-  float *st_m = (float *)(st_u + 2);                // [SL]
-  float(*st_mv)[SL] = (float(*)[SL])(st_m + SL);    // [3] m v
-  float(*st_f)[SL] = st_mv + 3;                     // [3] external force
-  float(*st_S)[SL] = st_f + 3;                      // [6] -V sigma
-  float(*st_nz)[SL] = st_S + 6;                     // [3] z weights of the layer's nodes
-  float(*st_dnz)[SL] = st_nz + 3;                   // [3]
+  float *acc = dyn_smem;                                           // [7][NN]
+  float2(*st_wx)[CAP] = (float2(*)[CAP])(acc + 7 * NN);            // [3] x weights (N, dN) per offset
+  float2(*st_wy)[CAP] = st_wx + 3;                                 // [3]
+  float4 *st_p = (float4 *)(st_wy + 3);                            // (m, m v)
+  float4 *st_s0 = st_p + CAP;                                      // (Sxx, Sxy, Sxy, Syy)
+  float4 *st_s1 = st_s0 + CAP;                                     // (Sxz, Syz, Szz, Nz2)
+  float4 *st_z = st_s1 + CAP;                                      // (Nz0, Nz1, dNz0, dNz1)
+  float4 *st_f = st_z + CAP;                                       // PLANAR: (f, 0)
 
   const int tid = threadIdx.x;
   const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
@@ -1900,10 +1915,11 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   __syncthreads();
 
   for (int round = 0; round < nrounds; round++) {
-    int item_cell[W::IPT], item_tl[W::IPT];
-    float item_xn[W::IPT], item_yn[W::IPT];  // virtual target node coordinates
+    int item_cell[W::IPT], item_tl[W::IPT], item_ix[W::IPT], item_iy[W::IPT];
     bool item_ok[W::IPT];
-    float win[W::IPT][3][7];
+    // window of three z nodes per item: (m, m vx), (m vy, m vz), (fx, fy), fz
+    float2 wa[W::IPT][3], wb[W::IPT][3], wc[W::IPT][3];
+    float wz[W::IPT][3];
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
       const int it = (round * W::IPT + q) * NT + tid;
@@ -1912,20 +1928,21 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
       const int py = item_ok[q] ? pairs_y[it / nx] : 0;
       item_cell[q] = pair_src(py) * W::NS + pair_src(px);
       item_tl[q] = pair_tgt(px) + T::X * pair_tgt(py);
-      item_xn[q] = (float)(t0[0] - 1 + pair_src(px) - 1 + pair_off(px));
-      item_yn[q] = (float)(t0[1] - 1 + pair_src(py) - 1 + pair_off(py));
+      item_ix[q] = pair_off(px);
+      item_iy[q] = pair_off(py);
 #pragma unroll
-      for (int k = 0; k < 3; k++)
-#pragma unroll
-        for (int c = 0; c < 7; c++) win[q][k][c] = 0.0f;
+      for (int k = 0; k < 3; k++) {
+        wa[q][k] = wb[q][k] = wc[q][k] = make_float2(0.0f, 0.0f);
+        wz[q][k] = 0.0f;
+      }
     }
     for (int dz = dz_lo; dz <= dz_hi; dz++) {
       const int *pref = cell_pref + (dz - dz_lo) * W::NCELL;
       const int *k0s = cell_k0 + (dz - dz_lo) * W::NCELL;
       const int base = pref[0];
       const int layer_n = pref[W::NCELL] - base;
-      for (int c0 = 0; c0 < layer_n; c0 += W::CAP) {
-        const int c1 = min(c0 + W::CAP, layer_n);
+      for (int c0 = 0; c0 < layer_n; c0 += CAP) {
+        const int c1 = min(c0 + CAP, layer_n);
         // ---- stage particles [c0, c1) of the layer ----
         for (int j = c0 + tid; j < c1; j += NT) {
           int lo = 0, hi = W::NCELL;
@@ -1934,28 +1951,35 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
             if (pref[mid] - base <= j) lo = mid; else hi = mid;
           }
           const int s = a.B.order[k0s[lo] + (j - (pref[lo] - base))];
-          const int jj = j - c0 + lo;  // skewed slot: neighbouring cells start in different banks
+          const int jj = dual_slot(j - c0);
+          // the particle's dual cell: its nodes are d - 1 .. d + 1 per axis
+          const int sx = t0[0] - 1 + lo % W::NS, sy = t0[1] - 1 + lo / W::NS;
           const float ux = scaled_coord(P.x[s], g.origin[0], g.inv_h);
           const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
           const float uz = scaled_coord(P.x[2 * st + s], g.origin[2], g.inv_h);
+#pragma unroll
+          for (int i = 0; i < 3; i++) {
+            float N, dN;
+            axis_weight<PMPM_SHAPE_QUADRATIC>(ux - (float)(sx - 1 + i), g.inv_h, 0, N, dN);
+            st_wx[i][jj] = make_float2(N, dN);
+            axis_weight<PMPM_SHAPE_QUADRATIC>(uy - (float)(sy - 1 + i), g.inv_h, 0, N, dN);
+            st_wy[i][jj] = make_float2(N, dN);
+          }
+          float Nz[3], dNz[3];
+#pragma unroll
+          for (int k = 0; k < 3; k++) axis_weight<PMPM_SHAPE_QUADRATIC>(uz - (float)(dz - 1 + k), g.inv_h, 0, Nz[k], dNz[k]);
           const float m = P.m[s];
           const float nv = a.remap ? 0.0f : -P.V[s];
-          st_u[0][jj] = ux;
-          st_u[1][jj] = uy;
-          st_m[jj] = m;
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            st_mv[c][jj] = m * P.v[c * st + s];
-            if (PLANAR) st_f[c][jj] = a.remap ? 0.0f : P.fext[c * st + s];
-          }
-#pragma unroll
-          for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
-#pragma unroll
-          for (int k = 0; k < 3; k++) {
-            float N, dN;
-            axis_weight<PMPM_SHAPE_QUADRATIC>(uz - (float)(dz - 1 + k), g.inv_h, 0, N, dN);
-            st_nz[k][jj] = N;
-            st_dnz[k][jj] = dN;
+          st_p[jj] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
+          const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
+          const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
+          st_s0[jj] = make_float4(Sxx, Sxy, Sxy, Syy);
+          st_s1[jj] = make_float4(Sxz, Syz, Szz, Nz[2]);
+          st_z[jj] = make_float4(Nz[0], Nz[1], dNz[0], dNz[1]);
+          if (PLANAR) {
+            const bool use = !a.remap;
+            st_f[jj] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f,
+                                   use ? P.fext[2 * st + s] : 0.0f, 0.0f);
           }
         }
         __syncthreads();
@@ -1964,41 +1988,38 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
         for (int q = 0; q < W::IPT; q++) {
           if (!item_ok[q]) continue;
           const int vc = item_cell[q];
-          const int j0 = max(pref[vc] - base, c0) - c0 + vc, j1 = min(pref[vc + 1] - base, c1) - c0 + vc;
-          const float xn = item_xn[q], yn = item_yn[q];
-          auto add = [&](int j) {
-            float Nx, dNx, Ny, dNy;
-            axis_weight<PMPM_SHAPE_QUADRATIC>(st_u[0][j] - xn, g.inv_h, 0, Nx, dNx);
-            axis_weight<PMPM_SHAPE_QUADRATIC>(st_u[1][j] - yn, g.inv_h, 0, Ny, dNy);
-            const float m = st_m[j];
-            const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
-            const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
-            const float nn = Nx * Ny;
-            const float gx = dNx * Ny, gy = Nx * dNy;
-            // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
-            float Ax = Sxx * gx + Sxy * gy;
-            float Ay = Sxy * gx + Syy * gy;
-            float Az = Sxz * gx + Syz * gy;
+          const int j0 = max(pref[vc] - base, c0) - c0, j1 = min(pref[vc + 1] - base, c1) - c0;
+          const float2 *wxp = st_wx[item_ix[q]], *wyp = st_wy[item_iy[q]];
+          auto add = [&](int jp) {
+            const int j = dual_slot(jp);
+            const float2 wx = wxp[j], wy = wyp[j];
+            const float4 pm = st_p[j], s0 = st_s0[j], s1 = st_s1[j], zw = st_z[j];
+            const float nn = wx.x * wy.x, gx = wx.y * wy.x, gy = wx.x * wy.y;
+            const float2 nn2 = make_float2(nn, nn), gx2 = make_float2(gx, gx), gy2 = make_float2(gy, gy);
+            const float2 mm = __fmul2_rn(make_float2(pm.x, pm.y), nn2);
+            const float2 mv = __fmul2_rn(make_float2(pm.z, pm.w), nn2);
+            // f = Nz (f_ext nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
+            float2 A = __ffma2_rn(make_float2(s0.z, s0.w), gy2, __fmul2_rn(make_float2(s0.x, s0.y), gx2));
+            float Az = fmaf(s1.y, gy, s1.x * gx);
             if (PLANAR) {
-              Ax += st_f[0][j] * nn;
-              Ay += st_f[1][j] * nn;
-              Az += st_f[2][j] * nn;
+              const float4 fe = st_f[j];
+              A = __ffma2_rn(make_float2(fe.x, fe.y), nn2, A);
+              Az = fmaf(fe.z, nn, Az);
             }
-            const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
-            const float mn = m * nn, mvxn = st_mv[0][j] * nn, mvyn = st_mv[1][j] * nn, mvzn = st_mv[2][j] * nn;
+            const float2 B = __fmul2_rn(make_float2(s1.x, s1.y), nn2);
+            const float Bz = s1.z * nn;
+            const float Nz[3] = {zw.x, zw.y, s1.w};
+            const float dNz[3] = {zw.z, zw.w, -zw.z - zw.w};  // the three derivatives sum to zero
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-              const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
-              win[q][k][0] += mn * Nz;
-              win[q][k][1] += mvxn * Nz;
-              win[q][k][2] += mvyn * Nz;
-              win[q][k][3] += mvzn * Nz;
-              win[q][k][4] += Ax * Nz + Bx * dNz;
-              win[q][k][5] += Ay * Nz + By * dNz;
-              win[q][k][6] += Az * Nz + Bz * dNz;
+              const float2 n2 = make_float2(Nz[k], Nz[k]), d2 = make_float2(dNz[k], dNz[k]);
+              wa[q][k] = __ffma2_rn(mm, n2, wa[q][k]);
+              wb[q][k] = __ffma2_rn(mv, n2, wb[q][k]);
+              wc[q][k] = __ffma2_rn(B, d2, __ffma2_rn(A, n2, wc[q][k]));
+              wz[q][k] = fmaf(Bz, dNz[k], fmaf(Az, Nz[k], wz[q][k]));
             }
           };
-          // two particles per pass: the second's shared-memory loads overlap the first's arithmetic
+          // four particles per pass: their shared-memory loads overlap the arithmetic
           int j = j0;
           for (; j + 3 < j1; j += 4) {
             add(j);
@@ -2018,16 +2039,24 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
           const int lz = tz - t0[2];
           if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
             const int ln = item_tl[q] + T::X * T::Y * lz;
-#pragma unroll
-            for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NN + ln], win[q][0][c]);
+            atomicAdd(&acc[ln], wa[q][0].x);
+            atomicAdd(&acc[NN + ln], wa[q][0].y);
+            atomicAdd(&acc[2 * NN + ln], wb[q][0].x);
+            atomicAdd(&acc[3 * NN + ln], wb[q][0].y);
+            atomicAdd(&acc[4 * NN + ln], wc[q][0].x);
+            atomicAdd(&acc[5 * NN + ln], wc[q][0].y);
+            atomicAdd(&acc[6 * NN + ln], wz[q][0]);
           }
         }
 #pragma unroll
-        for (int c = 0; c < 7; c++) {
-          win[q][0][c] = win[q][1][c];
-          win[q][1][c] = win[q][2][c];
-          win[q][2][c] = 0.0f;
+        for (int k = 0; k < 2; k++) {
+          wa[q][k] = wa[q][k + 1];
+          wb[q][k] = wb[q][k + 1];
+          wc[q][k] = wc[q][k + 1];
+          wz[q][k] = wz[q][k + 1];
         }
+        wa[q][2] = wb[q][2] = wc[q][2] = make_float2(0.0f, 0.0f);
+        wz[q][2] = 0.0f;
       }
     }
 #pragma unroll
@@ -2039,8 +2068,13 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
         const int lz = tz - t0[2];
         if (lz >= 0 && lz < T::Z) {
           const int ln = item_tl[q] + T::X * T::Y * lz;
-#pragma unroll
-          for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NN + ln], win[q][k][c]);
+          atomicAdd(&acc[ln], wa[q][k].x);
+          atomicAdd(&acc[NN + ln], wa[q][k].y);
+          atomicAdd(&acc[2 * NN + ln], wb[q][k].x);
+          atomicAdd(&acc[3 * NN + ln], wb[q][k].y);
+          atomicAdd(&acc[4 * NN + ln], wc[q][k].x);
+          atomicAdd(&acc[5 * NN + ln], wc[q][k].y);
+          atomicAdd(&acc[6 * NN + ln], wz[q][k]);
         }
       }
     }
@@ -2048,7 +2082,6 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   __syncthreads();
   tile_epilogue3(a, apply_bcs, t0, acc, tid, NT);
 }
-
 // One persistent CTA pass over the active-tile queue (grid: 2 CTAs per SM).
 template <bool PLANAR>
 __global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
