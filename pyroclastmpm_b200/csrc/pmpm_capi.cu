@@ -483,7 +483,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
     if (s->p2g_variant == 1) {
       // persistent CTAs over the active-tile queue of this partition
       a.p2g_par = (int)(s->p2g_seq++ & 1u);
-      const int grid = std::min(s->g.ntiles, 2 * s->num_sms);
+      const int grid = std::min(s->g.ntiles, s->num_sms);
       if (s->has_planar)
         k_p2g_dual3<true><<<grid, Dual3::NT, pbytes, s->stream>>>(a, apply_bcs, s->node_epoch);
       else

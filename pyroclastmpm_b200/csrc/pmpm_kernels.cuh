@@ -1760,7 +1760,10 @@ __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs
 // (particle, node) pair the sweep visits carries weight.  Work item = (x
 // pair, y pair), a pair being (dual source column, node offset 0..2) whose
 // target lies in the tile; items sweep the dual layers along z with a
-// three-node register window, as k_p2g_sweep3.
+// three-node register window, as k_p2g_sweep3.  One CTA of 20 warps per SM
+// (one item per thread) stages the tile's particles, all layers in z order,
+// in pieces of up to 1,872 regardless of layer boundaries (two barriers per
+// piece), and finds the next piece's storage slots while the items run.
 
 struct Dual3 {
   using T = TileDims<3>;
@@ -1768,18 +1771,18 @@ struct Dual3 {
   static constexpr int MAXPAIR = NS * 3;
   static constexpr int NCELL = NS * NS;
   static constexpr int NL = T::Z + 2;   // dual layers a tile reads
-  static constexpr int NT = 320;        // threads (10 warps)
-  static constexpr int IPT = 2;         // items per thread per round
+  static constexpr int NT = 640;        // threads (20 warps), one CTA per SM
+  static constexpr int IPT = 1;         // items per thread
   // staged bytes per particle: the x and y weights of the three offsets
   // (float2 N, dN each), float4 (m, m vx, m vy, m vz), float4 (Sxx, Sxy,
   // Sxy, Syy), float4 (Sxz, Syz, Szz, Nz2), float4 (Nz0, Nz1, dNz0, dNz1),
   // with a PlanarDomain float4 (f, 0); S = -V sigma
   __host__ __device__ static constexpr int slot_bytes(bool planar) { return 6 * 8 + 4 * 16 + (planar ? 16 : 0); }
-  // two CTAs per SM: 116,736 B of shared memory each, less the 1 KB the
-  // runtime reserves, the static tables and the node accumulators
+  // staged particles: 227 KB of shared memory per CTA, less the static
+  // tables and the node accumulators
   static constexpr int STATIC_BYTES = 8448;
   __host__ __device__ static constexpr int cap(bool planar) {
-    return ((116736 - 1024 - STATIC_BYTES - 7 * T::N * 4) / slot_bytes(planar)) & ~7;
+    return ((232448 - STATIC_BYTES - 7 * T::N * 4) / slot_bytes(planar)) & ~7;
   }
 };
 
@@ -1872,7 +1875,6 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   __syncthreads();
   const int nx = npair[0], ny = npair[1];
   const int nitems = nx * ny;
-  const int nrounds = (nitems + NT * W::IPT - 1) / (NT * W::IPT);
   const int dz_lo = max(t0[2] - 1, 0), dz_hi = min(t0[2] + T::Z, g.n[2]);
   const DevParticles &P = a.P;
   const int st = P.stride;
@@ -1914,81 +1916,147 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   }
   __syncthreads();
 
-  for (int round = 0; round < nrounds; round++) {
-    int item_cell[W::IPT], item_tl[W::IPT], item_ix[W::IPT], item_iy[W::IPT];
-    bool item_ok[W::IPT];
-    // window of three z nodes per item: (m, m vx), (m vy, m vz), (fx, fy), fz
-    float2 wa[W::IPT][3], wb[W::IPT][3], wc[W::IPT][3];
-    float wz[W::IPT][3];
+  static_assert(T::X * 3 * T::Y * 3 <= NT * W::IPT, "one round of items covers a tile");
+  int item_cell[W::IPT], item_tl[W::IPT], item_ix[W::IPT], item_iy[W::IPT];
+  bool item_ok[W::IPT];
+  // window of three z nodes per item: (m, m vx), (m vy, m vz), (fx, fy), fz
+  float2 wa[W::IPT][3], wb[W::IPT][3], wc[W::IPT][3];
+  float wz[W::IPT][3];
+#pragma unroll
+  for (int q = 0; q < W::IPT; q++) {
+    const int it = q * NT + tid;
+    item_ok[q] = it < nitems;
+    const int px = item_ok[q] ? pairs_x[it % nx] : 0;
+    const int py = item_ok[q] ? pairs_y[it / nx] : 0;
+    item_cell[q] = pair_src(py) * W::NS + pair_src(px);
+    item_tl[q] = pair_tgt(px) + T::X * pair_tgt(py);
+    item_ix[q] = pair_off(px);
+    item_iy[q] = pair_off(py);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      wa[q][k] = wb[q][k] = wc[q][k] = make_float2(0.0f, 0.0f);
+      wz[q][k] = 0.0f;
+    }
+  }
+
+  // The tile's particles, all layers in z order, are positions
+  // 0 .. cell_pref[ntab] of the table; they are staged in pieces of CAP
+  // positions regardless of layer boundaries.  Table cell and storage slot
+  // of position j:
+  auto locate = [&](int j, int &lo, int &s) {
+    lo = 0;
+    int hi = ntab;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (cell_pref[mid] <= j) lo = mid; else hi = mid;
+    }
+    s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+  };
+  // ---- node dz_lo + L - 1 gets nothing from layers after L: flush, shift ----
+  auto flush_shift = [&](int L) {
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
-      const int it = (round * W::IPT + q) * NT + tid;
-      item_ok[q] = it < nitems;
-      const int px = item_ok[q] ? pairs_x[it % nx] : 0;
-      const int py = item_ok[q] ? pairs_y[it / nx] : 0;
-      item_cell[q] = pair_src(py) * W::NS + pair_src(px);
-      item_tl[q] = pair_tgt(px) + T::X * pair_tgt(py);
-      item_ix[q] = pair_off(px);
-      item_iy[q] = pair_off(py);
+      if (item_ok[q]) {
+        const int tz = max(dz_lo + L - 1, 0);
+        const int lz = tz - t0[2];
+        if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
+          const int ln = item_tl[q] + T::X * T::Y * lz;
+          atomicAdd(&acc[ln], wa[q][0].x);
+          atomicAdd(&acc[NN + ln], wa[q][0].y);
+          atomicAdd(&acc[2 * NN + ln], wb[q][0].x);
+          atomicAdd(&acc[3 * NN + ln], wb[q][0].y);
+          atomicAdd(&acc[4 * NN + ln], wc[q][0].x);
+          atomicAdd(&acc[5 * NN + ln], wc[q][0].y);
+          atomicAdd(&acc[6 * NN + ln], wz[q][0]);
+        }
+      }
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        wa[q][k] = wb[q][k] = wc[q][k] = make_float2(0.0f, 0.0f);
-        wz[q][k] = 0.0f;
+      for (int k = 0; k < 2; k++) {
+        wa[q][k] = wa[q][k + 1];
+        wb[q][k] = wb[q][k + 1];
+        wc[q][k] = wc[q][k + 1];
+        wz[q][k] = wz[q][k + 1];
+      }
+      wa[q][2] = wb[q][2] = wc[q][2] = make_float2(0.0f, 0.0f);
+      wz[q][2] = 0.0f;
+    }
+  };
+
+  const int nlayers = dz_hi - dz_lo + 1;
+  const int total = cell_pref[ntab];
+  // positions tid + r NT of the next piece, found (cell search and the
+  // sorted-order gather) while the current piece's items run
+  constexpr int R = (CAP + NT - 1) / NT;
+  int pf_lo[R], pf_s[R];
+  int L = 0;  // layer whose particles the items add next
+  for (int p0 = 0; p0 < total; p0 += CAP) {
+    const int p1 = min(p0 + CAP, total);
+    // ---- stage positions [p0, p1) ----
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int j = p0 + tid + r * NT;
+      if (j < p1) {
+        int lo, s;
+        if (p0 > 0) {
+          lo = pf_lo[r];
+          s = pf_s[r];
+        } else {
+          locate(j, lo, s);
+        }
+        const int jj = dual_slot(j - p0);
+        // the particle's dual cell: its nodes are d - 1 .. d + 1 per axis
+        const int layer = lo / W::NCELL, vc = lo - layer * W::NCELL;
+        const int dz = dz_lo + layer;
+        const int sx = t0[0] - 1 + vc % W::NS, sy = t0[1] - 1 + vc / W::NS;
+        const float ux = scaled_coord(P.x[s], g.origin[0], g.inv_h);
+        const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
+        const float uz = scaled_coord(P.x[2 * st + s], g.origin[2], g.inv_h);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          float N, dN;
+          axis_weight<PMPM_SHAPE_QUADRATIC>(ux - (float)(sx - 1 + i), g.inv_h, 0, N, dN);
+          st_wx[i][jj] = make_float2(N, dN);
+          axis_weight<PMPM_SHAPE_QUADRATIC>(uy - (float)(sy - 1 + i), g.inv_h, 0, N, dN);
+          st_wy[i][jj] = make_float2(N, dN);
+        }
+        float Nz[3], dNz[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) axis_weight<PMPM_SHAPE_QUADRATIC>(uz - (float)(dz - 1 + k), g.inv_h, 0, Nz[k], dNz[k]);
+        const float m = P.m[s];
+        const float nv = a.remap ? 0.0f : -P.V[s];
+        st_p[jj] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
+        const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
+        const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
+        st_s0[jj] = make_float4(Sxx, Sxy, Sxy, Syy);
+        st_s1[jj] = make_float4(Sxz, Syz, Szz, Nz[2]);
+        st_z[jj] = make_float4(Nz[0], Nz[1], dNz[0], dNz[1]);
+        if (PLANAR) {
+          const bool use = !a.remap;
+          st_f[jj] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f,
+                                 use ? P.fext[2 * st + s] : 0.0f, 0.0f);
+        }
       }
     }
-    for (int dz = dz_lo; dz <= dz_hi; dz++) {
-      const int *pref = cell_pref + (dz - dz_lo) * W::NCELL;
-      const int *k0s = cell_k0 + (dz - dz_lo) * W::NCELL;
-      const int base = pref[0];
-      const int layer_n = pref[W::NCELL] - base;
-      for (int c0 = 0; c0 < layer_n; c0 += CAP) {
-        const int c1 = min(c0 + CAP, layer_n);
-        // ---- stage particles [c0, c1) of the layer ----
-        for (int j = c0 + tid; j < c1; j += NT) {
-          int lo = 0, hi = W::NCELL;
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (pref[mid] - base <= j) lo = mid; else hi = mid;
-          }
-          const int s = a.B.order[k0s[lo] + (j - (pref[lo] - base))];
-          const int jj = dual_slot(j - c0);
-          // the particle's dual cell: its nodes are d - 1 .. d + 1 per axis
-          const int sx = t0[0] - 1 + lo % W::NS, sy = t0[1] - 1 + lo / W::NS;
-          const float ux = scaled_coord(P.x[s], g.origin[0], g.inv_h);
-          const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
-          const float uz = scaled_coord(P.x[2 * st + s], g.origin[2], g.inv_h);
+    __syncthreads();
+    if (p1 < total) {
+      const int n1 = min(p1 + CAP, total);
 #pragma unroll
-          for (int i = 0; i < 3; i++) {
-            float N, dN;
-            axis_weight<PMPM_SHAPE_QUADRATIC>(ux - (float)(sx - 1 + i), g.inv_h, 0, N, dN);
-            st_wx[i][jj] = make_float2(N, dN);
-            axis_weight<PMPM_SHAPE_QUADRATIC>(uy - (float)(sy - 1 + i), g.inv_h, 0, N, dN);
-            st_wy[i][jj] = make_float2(N, dN);
-          }
-          float Nz[3], dNz[3];
-#pragma unroll
-          for (int k = 0; k < 3; k++) axis_weight<PMPM_SHAPE_QUADRATIC>(uz - (float)(dz - 1 + k), g.inv_h, 0, Nz[k], dNz[k]);
-          const float m = P.m[s];
-          const float nv = a.remap ? 0.0f : -P.V[s];
-          st_p[jj] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
-          const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
-          const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
-          st_s0[jj] = make_float4(Sxx, Sxy, Sxy, Syy);
-          st_s1[jj] = make_float4(Sxz, Syz, Szz, Nz[2]);
-          st_z[jj] = make_float4(Nz[0], Nz[1], dNz[0], dNz[1]);
-          if (PLANAR) {
-            const bool use = !a.remap;
-            st_f[jj] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f,
-                                   use ? P.fext[2 * st + s] : 0.0f, 0.0f);
-          }
-        }
-        __syncthreads();
-        // ---- items: add their source cell's staged particles ----
+      for (int r = 0; r < R; r++) {
+        const int j = p1 + tid + r * NT;
+        if (j < n1) locate(j, pf_lo[r], pf_s[r]);
+      }
+    }
+    // ---- items: layers with particles before p1 add their part of the piece;
+    // layers that end in it (empty ones included) are complete ----
+    while (L < nlayers) {
+      const int ls = cell_pref[L * W::NCELL], le = cell_pref[(L + 1) * W::NCELL];
+      if (ls < p1) {
+        const int *pref = cell_pref + L * W::NCELL;
 #pragma unroll
         for (int q = 0; q < W::IPT; q++) {
           if (!item_ok[q]) continue;
           const int vc = item_cell[q];
-          const int j0 = max(pref[vc] - base, c0) - c0, j1 = min(pref[vc + 1] - base, c1) - c0;
+          const int j0 = max(pref[vc], p0) - p0, j1 = min(pref[vc + 1], p1) - p0;
           const float2 *wxp = st_wx[item_ix[q]], *wyp = st_wy[item_iy[q]];
           auto add = [&](int jp) {
             const int j = dual_slot(jp);
@@ -2029,62 +2097,39 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
           }
           for (; j < j1; j++) add(j);
         }
-        __syncthreads();
       }
-      // ---- node dz - 1 gets nothing from later layers: flush, shift ----
-#pragma unroll
-      for (int q = 0; q < W::IPT; q++) {
-        if (item_ok[q]) {
-          const int tz = max(dz - 1, 0);
-          const int lz = tz - t0[2];
-          if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
-            const int ln = item_tl[q] + T::X * T::Y * lz;
-            atomicAdd(&acc[ln], wa[q][0].x);
-            atomicAdd(&acc[NN + ln], wa[q][0].y);
-            atomicAdd(&acc[2 * NN + ln], wb[q][0].x);
-            atomicAdd(&acc[3 * NN + ln], wb[q][0].y);
-            atomicAdd(&acc[4 * NN + ln], wc[q][0].x);
-            atomicAdd(&acc[5 * NN + ln], wc[q][0].y);
-            atomicAdd(&acc[6 * NN + ln], wz[q][0]);
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-          wa[q][k] = wa[q][k + 1];
-          wb[q][k] = wb[q][k + 1];
-          wc[q][k] = wc[q][k + 1];
-          wz[q][k] = wz[q][k + 1];
-        }
-        wa[q][2] = wb[q][2] = wc[q][2] = make_float2(0.0f, 0.0f);
-        wz[q][2] = 0.0f;
-      }
+      if (le > p1) break;  // the layer goes on in the next piece
+      flush_shift(L);
+      L++;
     }
+    __syncthreads();
+  }
+  for (; L < nlayers; L++) flush_shift(L);  // layers after the last particle
 #pragma unroll
-    for (int q = 0; q < W::IPT; q++) {
-      if (!item_ok[q]) continue;
+  for (int q = 0; q < W::IPT; q++) {
+    if (!item_ok[q]) continue;
 #pragma unroll
-      for (int k = 0; k < 2; k++) {
-        const int tz = min(dz_hi + k, g.n[2] - 1);
-        const int lz = tz - t0[2];
-        if (lz >= 0 && lz < T::Z) {
-          const int ln = item_tl[q] + T::X * T::Y * lz;
-          atomicAdd(&acc[ln], wa[q][k].x);
-          atomicAdd(&acc[NN + ln], wa[q][k].y);
-          atomicAdd(&acc[2 * NN + ln], wb[q][k].x);
-          atomicAdd(&acc[3 * NN + ln], wb[q][k].y);
-          atomicAdd(&acc[4 * NN + ln], wc[q][k].x);
-          atomicAdd(&acc[5 * NN + ln], wc[q][k].y);
-          atomicAdd(&acc[6 * NN + ln], wz[q][k]);
-        }
+    for (int k = 0; k < 2; k++) {
+      const int tz = min(dz_hi + k, g.n[2] - 1);
+      const int lz = tz - t0[2];
+      if (lz >= 0 && lz < T::Z) {
+        const int ln = item_tl[q] + T::X * T::Y * lz;
+        atomicAdd(&acc[ln], wa[q][k].x);
+        atomicAdd(&acc[NN + ln], wa[q][k].y);
+        atomicAdd(&acc[2 * NN + ln], wb[q][k].x);
+        atomicAdd(&acc[3 * NN + ln], wb[q][k].y);
+        atomicAdd(&acc[4 * NN + ln], wc[q][k].x);
+        atomicAdd(&acc[5 * NN + ln], wc[q][k].y);
+        atomicAdd(&acc[6 * NN + ln], wz[q][k]);
       }
     }
   }
   __syncthreads();
   tile_epilogue3(a, apply_bcs, t0, acc, tid, NT);
 }
-// One persistent CTA pass over the active-tile queue (grid: 2 CTAs per SM).
+// One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
 template <bool PLANAR>
-__global__ void __launch_bounds__(Dual3::NT, 2) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
+__global__ void __launch_bounds__(Dual3::NT, 1) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
   for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
