@@ -587,10 +587,10 @@ int step_once(pmpm_sim *s) {
   if (s->flags & PMPM_FLAG_MUSL) {
     PMPM_TRY((musl_tail<D, SF>(s, store_L)));
   } else {
-    // 3D quadratic: the next partition's binning rides on this G2P (not
-    // while a rollout or the autotuner saves and restores states, nor with
-    // a PlanarDomain, whose particle forces the binning pass computes)
-    const bool bin_next = s->dual && !s->tuning && !s->ro.held && s->rbls_index < 0 && !s->has_planar;
+    // quadratic: the next partition's binning rides on this G2P (not while
+    // the autotuner times kernels, nor with a PlanarDomain, whose particle
+    // forces the binning pass computes; state restores drop the binning)
+    const bool bin_next = s->dual && !s->tuning && s->rbls_index < 0 && !s->has_planar;
     PMPM_TRY((launch_g2p<D, SF>(s, 1, store_L, bin_next)));
   }
   s->step += 1;
@@ -2618,6 +2618,54 @@ int state_floats(const pmpm_sim *s) {
   return D + D + D * D + (D == 2 ? 4 : 6) + (D == 2 ? 3 : 6) + 1;
 }
 
+// Up to eight device-to-device copies of 4-byte words in one launch (the
+// rollout's state and node snapshots): blockIdx.y picks the copy.
+struct CopyList {
+  const void *src[8];
+  void *dst[8];
+  long long nbytes[8];
+  int count = 0;
+  void add(const void *from, void *to, size_t bytes) {
+    src[count] = from;
+    dst[count] = to;
+    nbytes[count] = (long long)bytes;
+    count++;
+  }
+};
+
+__global__ void k_copy_list(CopyList c) {
+  const int e = blockIdx.y;
+  const char *src = (const char *)c.src[e];
+  char *dst = (char *)c.dst[e];
+  const long long nb = c.nbytes[e];
+  const long long step = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+    const long long n4 = nb >> 4;
+    for (long long i = t0; i < n4; i += step) reinterpret_cast<float4 *>(dst)[i] = reinterpret_cast<const float4 *>(src)[i];
+    for (long long i = (n4 << 2) + t0; i < (nb >> 2); i += step)
+      reinterpret_cast<float *>(dst)[i] = reinterpret_cast<const float *>(src)[i];
+  } else {
+    for (long long i = t0; i < (nb >> 2); i += step)
+      reinterpret_cast<float *>(dst)[i] = reinterpret_cast<const float *>(src)[i];
+  }
+}
+
+int launch_copy_list(pmpm_sim *s, const CopyList &c) {
+  if (c.count == 0) return PMPM_OK;
+  long long most = 0;
+  for (int k = 0; k < c.count; k++) {
+    if ((c.nbytes[k] & 3) || ((reinterpret_cast<uintptr_t>(c.src[k]) | reinterpret_cast<uintptr_t>(c.dst[k])) & 3))
+      return PMPM_ERR_INVALID_ARGUMENT;
+    most = std::max(most, c.nbytes[k]);
+  }
+  const long long blocks = std::min<long long>((most / 16 + 255) / 256 + 1, 8LL * s->num_sms);
+  k_copy_list<<<dim3((unsigned)blocks, (unsigned)c.count), 256, 0, s->stream>>>(c);
+  PMPM_LAUNCHED();
+  s->launches += 1;
+  return PMPM_OK;
+}
+
 int copy_state(pmpm_sim *s, float *buf, bool save) {
   if (!save) PMPM_TRY(drop_fresh_keys(s));
   const int D = s->dim, st = s->stride;
@@ -2625,17 +2673,18 @@ int copy_state(pmpm_sim *s, float *buf, bool save) {
   float *arrays[6] = {P.x, P.v, P.F, P.sig, P.eps, P.V};
   const int ncomp[6] = {D, D, D * D, D == 2 ? 4 : 6, D == 2 ? 3 : 6, 1};
   size_t off = 0;
+  CopyList c;
   for (int k = 0; k < 6; k++) {
     const size_t bytes = sizeof(float) * (size_t)ncomp[k] * st;
     if (arrays[k]) {
       if (save)
-        PMPM_CUDA(cudaMemcpyAsync(buf + off, arrays[k], bytes, cudaMemcpyDeviceToDevice, s->stream));
+        c.add(arrays[k], buf + off, bytes);
       else
-        PMPM_CUDA(cudaMemcpyAsync(arrays[k], buf + off, bytes, cudaMemcpyDeviceToDevice, s->stream));
+        c.add(buf + off, arrays[k], bytes);
     }
     off += (size_t)ncomp[k] * st;
   }
-  return PMPM_OK;
+  return launch_copy_list(s, c);
 }
 
 void free_rollout(pmpm_sim *s) {
@@ -2677,20 +2726,24 @@ size_t node_snapshot_bytes(const pmpm_sim *s) {
   return sizeof(float) * nn * (1 + 2 * D + F) + sizeof(int) * (size_t)s->g.ntiles;
 }
 
+// The tile activity saved is the epoch of the P2G that wrote each tile (not
+// the binning marks, which the step's G2P has already advanced to the next
+// partition's tiles); restored into the marks the adjoint kernels read.
 int copy_nodes(pmpm_sim *s, char *buf, bool save) {
   const size_t nn = (size_t)s->g.ntotal, D = (size_t)s->dim;
   const size_t F = s->dim == 3 ? NodeVel<3>::F : NodeVel<2>::F;
-  void *arrays[5] = {s->N.m, s->N.p, s->N.pnt, s->N.vel, s->N.tile_epoch};
+  void *arrays[5] = {s->N.m, s->N.p, s->N.pnt, s->N.vel, save ? s->node_epoch : s->N.tile_epoch};
   const size_t bytes[5] = {4 * nn, 4 * D * nn, 4 * D * nn, 4 * F * nn, 4 * (size_t)s->g.ntiles};
   size_t off = 0;
+  CopyList c;
   for (int k = 0; k < 5; k++) {
     if (save)
-      PMPM_CUDA(cudaMemcpyAsync(buf + off, arrays[k], bytes[k], cudaMemcpyDeviceToDevice, s->stream));
+      c.add(arrays[k], buf + off, bytes[k]);
     else
-      PMPM_CUDA(cudaMemcpyAsync(arrays[k], buf + off, bytes[k], cudaMemcpyDeviceToDevice, s->stream));
+      c.add(buf + off, arrays[k], bytes[k]);
     off += bytes[k];
   }
-  return PMPM_OK;
+  return launch_copy_list(s, c);
 }
 
 // The step's P2G alone (partition and P2G with the node conditions).
