@@ -501,18 +501,18 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
       s->launches += 1;
     }
   } else if (D == 3) {
-    constexpr int bytes = sweep3_smem_bytes<SF>();
+    constexpr int bytes = sweep3_smem_bytes<SF, false>(), pbytes = sweep3_smem_bytes<SF, true>();
     static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
     if (!attr_set[dev]) {
       PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
       attr_set[dev] = true;
     }
     a.p2g_par = (int)(s->p2g_seq++ & 1u);
     const int grid = std::min(s->g.ntiles, s->num_sms);
     if (s->has_planar)
-      k_p2g_sweep3<SF, true><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+      k_p2g_sweep3<SF, true><<<grid, TileDims<3>::N, pbytes, s->stream>>>(a, apply_bcs, s->node_epoch);
     else
       k_p2g_sweep3<SF, false><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
   } else {

@@ -1382,22 +1382,28 @@ struct Sweep3 {
   static constexpr int NS = T::X + WIN - 1;          // source cells per axis
   static constexpr int MAXPAIR = NS * WIN;           // (source, offset) pairs per axis
   static constexpr int NCELL = NS * NS;              // source cells per layer
-  static constexpr int CAP = 1024;                   // staged particles per chunk
-  // each cell's staged run starts one slot later than packing would put it,
-  // so runs of neighbouring cells (read by neighbouring lanes) start in
-  // different shared-memory banks
-  static constexpr int SLOTS = CAP + NS * NS;
+  static constexpr int NL = T::Z + WIN - 1;          // source layers a tile reads
   static constexpr int NT = T::N;
   static constexpr int IPT = 2;                      // items per thread per round
+  // staged floats per particle: m, m v (3), -V sigma (6), the z weights and
+  // derivatives of the layer's WIN nodes; cubic adds the x and y weights and
+  // derivatives of the WIN offsets, linear the scaled x, y and bins; a
+  // PlanarDomain the external force (3)
+  __host__ __device__ static constexpr int floats(bool planar) {
+    return 10 + 2 * WIN + (SF == PMPM_SHAPE_CUBIC ? 4 * WIN : 4) + (planar ? 3 : 0);
+  }
+  // static shared memory: pair lists, the all-layer cell table, scan scratch
+  static constexpr int STATIC_BYTES = (4 * (2 * MAXPAIR + 2 + 2 * NL * NCELL + 1 + 33 + 1) + 255) / 256 * 256 + 256;
+  // staged particles: 227 KB per CTA less the static part and the node
+  // accumulators
+  __host__ __device__ static constexpr int cap(bool planar) {
+    return ((232448 - STATIC_BYTES - 7 * NT * 4) / (4 * floats(planar))) & ~7;
+  }
 };
 
-template <int SF>
+template <int SF, bool PLANAR>
 constexpr int sweep3_smem_bytes() {
-  // cubic also stages the x and y weights of all four offsets (one CTA per
-  // SM either way, so the space is free)
-  return (7 * Sweep3<SF>::NT +
-          Sweep3<SF>::SLOTS * (2 + 2 + 1 + 3 + 3 + 6 + 2 * Sweep3<SF>::WIN +
-                               (SF == PMPM_SHAPE_CUBIC ? 4 * Sweep3<SF>::WIN : 0))) * 4;
+  return (7 * Sweep3<SF>::NT + Sweep3<SF>::cap(PLANAR) * Sweep3<SF>::floats(PLANAR)) * 4;
 }
 
 // pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
@@ -1425,35 +1431,41 @@ __device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
   return cnt;
 }
 
+// Staged slot of piece position j: an XOR swizzle inside aligned groups of
+// eight, so lanes reading the same position of neighbouring cells (runs of
+// about eight) hit different shared-memory banks.
+__device__ __forceinline__ int sweep_slot(int j) { return j ^ ((j >> 3) & 7); }
+
 template <int SF, bool PLANAR>
 __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile) {
   using W = Sweep3<SF>;
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int WIN = W::WIN;
+  constexpr int SL = W::cap(PLANAR);
   const DevGrid &g = a.g;
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
   __shared__ int npair[2];
-  __shared__ int cell_k0[W::NCELL], cell_pref[W::NCELL + 1];
+  // every layer's source cells: first sorted position and running prefix
+  __shared__ int cell_k0[W::NL * W::NCELL], cell_pref[W::NL * W::NCELL + 1];
   __shared__ int warp_tmp[33];
   // dynamic shared memory: tile accumulators, then the staged particles
-  // (structure of arrays, W::CAP entries each); size sweep3_smem_bytes<SF>()
+  // (structure of arrays, SL entries each); size sweep3_smem_bytes<SF, PLANAR>()
   extern __shared__ __align__(16) float dyn_smem[];
-  float *acc = dyn_smem;                                   // [7][NT]
-  constexpr int SL = W::SLOTS;
-  float(*st_u)[SL] = (float(*)[SL])(acc + 7 * NT);  // [2] scaled x, y
-  int(*st_b)[SL] = (int(*)[SL])(st_u + 2);          // [2] bins x, y
-  float *st_m = (float *)(st_b + 2);                // [SL]
+  float *acc = dyn_smem;                            // [7][NT]
+  float *st_m = acc + 7 * NT;                       // [SL]
   float(*st_mv)[SL] = (float(*)[SL])(st_m + SL);    // [3] m v
-  float(*st_f)[SL] = st_mv + 3;                     // [3] external force
-  float(*st_S)[SL] = st_f + 3;                      // [6] -V sigma
+  float(*st_S)[SL] = st_mv + 3;                     // [6] -V sigma
   float(*st_nz)[SL] = st_S + 6;                     // [WIN]
   float(*st_dnz)[SL] = st_nz + WIN;                 // [WIN]
   float(*st_wx)[SL] = st_dnz + WIN;                 // cubic: [WIN] x weights per offset
   float(*st_dwx)[SL] = st_wx + WIN;                 // [WIN]
   float(*st_wy)[SL] = st_dwx + WIN;                 // [WIN]
   float(*st_dwy)[SL] = st_wy + WIN;                 // [WIN]
+  float(*st_u)[SL] = st_dnz + WIN;                  // linear / quadratic: [2] scaled x, y
+  int(*st_b)[SL] = (int(*)[SL])(st_u + 2);          // [2] bins x, y
+  float(*st_f)[SL] = SF == PMPM_SHAPE_CUBIC ? st_dwy + WIN : (float(*)[SL])(st_b + 2);  // [3] external force
 
   const int tid = threadIdx.x;
   const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
@@ -1477,10 +1489,140 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     cz_lo = max(cz_lo, 0);
     cz_hi = min(cz_hi, g.n[2] - 1);
   }
+  const int nlayers = cz_hi - cz_lo + 1;
   const DevParticles &P = a.P;
   const int st = P.stride;
   const long long nxny = (long long)g.n[0] * g.n[1];
 
+  // ---- all layers' source cells -> sorted ranges, one prefix ----
+  const int ntab = nlayers * W::NCELL;
+  {
+    constexpr int PER = (W::NL * W::NCELL + NT - 1) / NT;
+    int cnt[PER];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int idx = tid * PER + k;
+      cnt[k] = 0;
+      if (idx < ntab) {
+        const int layer = idx / W::NCELL, vc = idx % W::NCELL;
+        const int sx = t0[0] - W::HI + vc % W::NS, sy = t0[1] - W::HI + vc / W::NS;
+        const long long f = sx + (long long)sy * g.n[0] + (long long)(cz_lo + layer) * nxny;
+        const bool valid = SF == PMPM_SHAPE_QUADRATIC ? (sx >= 0 && sx < g.n[0] && sy >= 0 && sy < g.n[1])
+                                                      : (f >= 0 && f < g.ntotal);
+        int k0 = 0;
+        if (valid) {
+          k0 = a.B.offset[f];
+          cnt[k] = a.B.offset[f + 1] - k0;
+        }
+        cell_k0[idx] = k0;
+        sum += cnt[k];
+      }
+    }
+    int total;
+    int ex = block_exclusive_scan(sum, warp_tmp, total);
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int idx = tid * PER + k;
+      if (idx < ntab) cell_pref[idx] = ex;
+      ex += cnt[k];
+    }
+    if (tid == 0) cell_pref[ntab] = total;
+  }
+  __syncthreads();
+  const int total = cell_pref[ntab];
+
+  // table cell and storage slot of position j of the tile's particle list
+  auto locate = [&](int j, int &lo, int &s) {
+    lo = 0;
+    int hi = ntab;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (cell_pref[mid] <= j) lo = mid; else hi = mid;
+    }
+    s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+  };
+  // ---- stage particle list position j into slot jj ----
+  auto stage_one = [&](int lo, int s, int jj) {
+    const int layer = lo / W::NCELL, vc = lo - layer * W::NCELL;
+    const int cz = cz_lo + layer;
+    float u[3];
+    int b[3];
+    bool inside = true;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+      b[c] = (int)u[c];
+      inside = inside && b[c] >= 0 && b[c] < g.n[c];
+    }
+    float m = P.m[s];
+    if (SF == PMPM_SHAPE_QUADRATIC && !inside) m = 0.0f;  // takes no part in P2G
+    const float nv = ((SF == PMPM_SHAPE_QUADRATIC && !inside) || a.remap) ? 0.0f : -P.V[s];
+    if (SF != PMPM_SHAPE_CUBIC) {
+      st_u[0][jj] = u[0];
+      st_u[1][jj] = u[1];
+      st_b[0][jj] = b[0];
+      st_b[1][jj] = b[1];
+    }
+    st_m[jj] = m;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      st_mv[c][jj] = m * P.v[c * st + s];
+      if (PLANAR) st_f[c][jj] = (m != 0.0f && !a.remap) ? P.fext[c * st + s] : 0.0f;
+    }
+    // -V sigma, symmetric: xx yy zz xy xz yz
+#pragma unroll
+    for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
+#pragma unroll
+    for (int k = 0; k < WIN; k++) {
+      const int tz = cz + k + W::LO;
+      const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(min(max(tz, 0), g.n[2] - 1), g.n[2]) : 0;
+      const float r = u[2] - (float)(b[2] + k + W::LO);
+      float N, dN;
+      if (SF == PMPM_SHAPE_CUBIC && u[2] >= 0.0f) {
+        // fixed spline piece of offset k (see the x / y weights below)
+        const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
+        N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
+        dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
+      } else {
+        axis_weight<SF>(r, g.inv_h, type, N, dN);
+      }
+      st_nz[k][jj] = N;
+      st_dnz[k][jj] = dN;
+    }
+    if (SF == PMPM_SHAPE_CUBIC) {
+      // x and y weights of the four offsets: r from the particle's own
+      // bin, the node type of the target the offset reaches from the
+      // (possibly aliased) source cell it is staged for.  At u >= 0
+      // offset w sits on spline piece 2 - w (r in [-w, 1 - w)), so its
+      // coefficients are the same for neighbouring lanes; u < 0 takes
+      // the general form
+      const int src[2] = {t0[0] - W::HI + vc % W::NS, t0[1] - W::HI + vc / W::NS};
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        float(*wN)[SL] = c == 0 ? st_wx : st_wy;
+        float(*wD)[SL] = c == 0 ? st_dwx : st_dwy;
+#pragma unroll
+        for (int k = 0; k < WIN; k++) {
+          const int tgt = src[c] + k + W::LO;
+          const int type = cubic_node_type(min(max(tgt, 0), g.n[c] - 1), g.n[c]);
+          const float r = u[c] - (float)(b[c] + k + W::LO);
+          float N, dN;
+          if (u[c] >= 0.0f) {
+            const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
+            N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
+            dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
+          } else {
+            axis_weight<SF>(r, g.inv_h, type, N, dN);
+          }
+          wN[k][jj] = N;
+          wD[k][jj] = dN;
+        }
+      }
+    }
+  };
+
+  constexpr int R = (SL + NT - 1) / NT;
   for (int round = 0; round < nrounds; round++) {
     // this thread's items
     int item_cell[W::IPT], item_ix[W::IPT], item_iy[W::IPT], item_tl[W::IPT];
@@ -1504,187 +1646,12 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 #pragma unroll
         for (int c = 0; c < 7; c++) win[q][k][c] = 0.0f;
     }
-    for (int cz = cz_lo; cz <= cz_hi; cz++) {
-      // ---- the layer's source cells -> sorted ranges, prefix ----
-      int carry = 0;
-      for (int it = 0; it < (W::NCELL + NT - 1) / NT; it++) {
-        const int vc = it * NT + tid;
-        int cnt = 0, k0 = 0;
-        if (vc < W::NCELL) {
-          const int sx = t0[0] - W::HI + vc % W::NS, sy = t0[1] - W::HI + vc / W::NS;
-          bool valid;
-          long long f;
-          if (SF == PMPM_SHAPE_QUADRATIC) {
-            valid = sx >= 0 && sx < g.n[0] && sy >= 0 && sy < g.n[1];
-            f = sx + (long long)sy * g.n[0] + (long long)cz * nxny;
-          } else {
-            f = sx + (long long)sy * g.n[0] + (long long)cz * nxny;
-            valid = f >= 0 && f < g.ntotal;
-          }
-          if (valid) {
-            k0 = a.B.offset[f];
-            cnt = a.B.offset[f + 1] - k0;
-          }
-          cell_k0[vc] = k0;
-        }
-        int total;
-        const int ex = block_exclusive_scan(cnt, warp_tmp, total);
-        if (vc < W::NCELL) cell_pref[vc] = carry + ex;
-        carry += total;
-      }
-      if (tid == 0) cell_pref[W::NCELL] = carry;
-      __syncthreads();
-      const int layer_n = cell_pref[W::NCELL];
-      // cubic z node types of this layer's targets cz + LO .. cz + HI
-      for (int c0 = 0; c0 < layer_n; c0 += W::CAP) {
-        const int c1 = min(c0 + W::CAP, layer_n);
-        // ---- stage particles [c0, c1) ----
-        for (int j = c0 + tid; j < c1; j += NT) {
-          int lo = 0, hi = W::NCELL;
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (cell_pref[mid] <= j) lo = mid; else hi = mid;
-          }
-          const int s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
-          const int jj = j - c0 + lo;  // skewed slot
-          float u[3];
-          int b[3];
-          bool inside = true;
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
-            b[c] = (int)u[c];
-            inside = inside && b[c] >= 0 && b[c] < g.n[c];
-          }
-          float m = P.m[s];
-          if (SF == PMPM_SHAPE_QUADRATIC && !inside) m = 0.0f;  // takes no part in P2G
-          const float nv = ((SF == PMPM_SHAPE_QUADRATIC && !inside) || a.remap) ? 0.0f : -P.V[s];
-          st_u[0][jj] = u[0];
-          st_u[1][jj] = u[1];
-          st_b[0][jj] = b[0];
-          st_b[1][jj] = b[1];
-          st_m[jj] = m;
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            st_mv[c][jj] = m * P.v[c * st + s];
-            if (PLANAR) st_f[c][jj] = (m != 0.0f && !a.remap) ? P.fext[c * st + s] : 0.0f;
-          }
-          // -V sigma, symmetric: xx yy zz xy xz yz
-#pragma unroll
-          for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
-#pragma unroll
-          for (int k = 0; k < WIN; k++) {
-            const int tz = cz + k + W::LO;
-            const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(min(max(tz, 0), g.n[2] - 1), g.n[2]) : 0;
-            const float r = u[2] - (float)(b[2] + k + W::LO);
-            float N, dN;
-            if (SF == PMPM_SHAPE_CUBIC && u[2] >= 0.0f) {
-              // fixed spline piece of offset k (see the x / y weights below)
-              const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
-              N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
-              dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
-            } else {
-              axis_weight<SF>(r, g.inv_h, type, N, dN);
-            }
-            st_nz[k][jj] = N;
-            st_dnz[k][jj] = dN;
-          }
-          if (SF == PMPM_SHAPE_CUBIC) {
-            // x and y weights of the four offsets: r from the particle's own
-            // bin, the node type of the target the offset reaches from the
-            // (possibly aliased) source cell it is staged for.  At u >= 0
-            // offset w sits on spline piece 2 - w (r in [-w, 1 - w)), so its
-            // coefficients are the same for neighbouring lanes; u < 0 takes
-            // the general form
-            const int src[2] = {t0[0] - W::HI + lo % W::NS, t0[1] - W::HI + lo / W::NS};
-#pragma unroll
-            for (int c = 0; c < 2; c++) {
-              float(*wN)[SL] = c == 0 ? st_wx : st_wy;
-              float(*wD)[SL] = c == 0 ? st_dwx : st_dwy;
-#pragma unroll
-              for (int k = 0; k < WIN; k++) {
-                const int tgt = src[c] + k + W::LO;
-                const int type = cubic_node_type(min(max(tgt, 0), g.n[c] - 1), g.n[c]);
-                const float r = u[c] - (float)(b[c] + k + W::LO);
-                float N, dN;
-                if (u[c] >= 0.0f) {
-                  const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
-                  N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
-                  dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
-                } else {
-                  axis_weight<SF>(r, g.inv_h, type, N, dN);
-                }
-                wN[k][jj] = N;
-                wD[k][jj] = dN;
-              }
-            }
-          }
-        }
-        __syncthreads();
-        // ---- items: add their source cell's staged particles ----
-#pragma unroll
-        for (int q = 0; q < W::IPT; q++) {
-          if (!item_ok[q]) continue;
-          const int vc = item_cell[q];
-          const int j0 = max(cell_pref[vc], c0) - c0 + vc, j1 = min(cell_pref[vc + 1], c1) - c0 + vc;
-          const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
-          const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
-          const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
-          const int ix = item_ix[q], iy = item_iy[q];
-          auto add = [&](int j) {
-            float Nx, dNx, Ny, dNy;
-            if (SF == PMPM_SHAPE_CUBIC) {
-              Nx = st_wx[ix][j];
-              dNx = st_dwx[ix][j];
-              Ny = st_wy[iy][j];
-              dNy = st_dwy[iy][j];
-            } else {
-              axis_weight<SF>(st_u[0][j] - (float)(st_b[0][j] + wx), g.inv_h, typex, Nx, dNx);
-              axis_weight<SF>(st_u[1][j] - (float)(st_b[1][j] + wy), g.inv_h, typey, Ny, dNy);
-            }
-            const float m = st_m[j];
-            const float mvx = st_mv[0][j], mvy = st_mv[1][j], mvz = st_mv[2][j];
-            const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
-            const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
-            const float nn = Nx * Ny;
-            const float gx = dNx * Ny, gy = Nx * dNy;
-            // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
-            float Ax = Sxx * gx + Sxy * gy;
-            float Ay = Sxy * gx + Syy * gy;
-            float Az = Sxz * gx + Syz * gy;
-            if (PLANAR) {
-              Ax += st_f[0][j] * nn;
-              Ay += st_f[1][j] * nn;
-              Az += st_f[2][j] * nn;
-            }
-            const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
-            const float mn = m * nn, mvxn = mvx * nn, mvyn = mvy * nn, mvzn = mvz * nn;
-#pragma unroll
-            for (int k = 0; k < WIN; k++) {
-              const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
-              win[q][k][0] += mn * Nz;
-              win[q][k][1] += mvxn * Nz;
-              win[q][k][2] += mvyn * Nz;
-              win[q][k][3] += mvzn * Nz;
-              win[q][k][4] += Ax * Nz + Bx * dNz;
-              win[q][k][5] += Ay * Nz + By * dNz;
-              win[q][k][6] += Az * Nz + Bz * dNz;
-            }
-          };
-          int j = j0;
-          for (; j + 1 < j1; j += 2) {
-            add(j);
-            add(j + 1);
-          }
-          if (j < j1) add(j);
-        }
-        __syncthreads();
-      }
-      // ---- the lowest window node is complete: flush and shift ----
+    // ---- the lowest window node of layer L is complete: flush, shift ----
+    auto flush_shift = [&](int L) {
 #pragma unroll
       for (int q = 0; q < W::IPT; q++) {
         if (item_ok[q]) {
-          int tz = cz + W::LO;
+          int tz = cz_lo + L + W::LO;
           if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
           const int lz = tz - t0[2];
           if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
@@ -1700,7 +1667,109 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 #pragma unroll
         for (int c = 0; c < 7; c++) win[q][WIN - 1][c] = 0.0f;
       }
+    };
+    // The tile's particles, all layers in z order, are positions
+    // 0 .. total of the table; they are staged in pieces of SL positions
+    // regardless of layer boundaries, and the next piece's storage slots
+    // are found while the current piece's items run.
+    int pf_lo[R], pf_s[R];
+    int L = 0;  // layer whose particles the items add next
+    for (int p0 = 0; p0 < total; p0 += SL) {
+      const int p1 = min(p0 + SL, total);
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const int j = p0 + tid + r * NT;
+        if (j < p1) {
+          int lo, s;
+          if (p0 > 0) {
+            lo = pf_lo[r];
+            s = pf_s[r];
+          } else {
+            locate(j, lo, s);
+          }
+          stage_one(lo, s, sweep_slot(j - p0));
+        }
+      }
+      __syncthreads();
+      if (p1 < total) {
+        const int n1 = min(p1 + SL, total);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const int j = p1 + tid + r * NT;
+          if (j < n1) locate(j, pf_lo[r], pf_s[r]);
+        }
+      }
+      // ---- items: layers with particles before p1 add their part of the
+      // piece; layers that end in it (empty ones included) are complete ----
+      while (L < nlayers) {
+        const int ls = cell_pref[L * W::NCELL], le = cell_pref[(L + 1) * W::NCELL];
+        if (ls < p1) {
+          const int *pref = cell_pref + L * W::NCELL;
+#pragma unroll
+          for (int q = 0; q < W::IPT; q++) {
+            if (!item_ok[q]) continue;
+            const int vc = item_cell[q];
+            const int j0 = max(pref[vc], p0) - p0, j1 = min(pref[vc + 1], p1) - p0;
+            const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
+            const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
+            const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
+            const int ix = item_ix[q], iy = item_iy[q];
+            auto add = [&](int jp) {
+              const int j = sweep_slot(jp);
+              float Nx, dNx, Ny, dNy;
+              if (SF == PMPM_SHAPE_CUBIC) {
+                Nx = st_wx[ix][j];
+                dNx = st_dwx[ix][j];
+                Ny = st_wy[iy][j];
+                dNy = st_dwy[iy][j];
+              } else {
+                axis_weight<SF>(st_u[0][j] - (float)(st_b[0][j] + wx), g.inv_h, typex, Nx, dNx);
+                axis_weight<SF>(st_u[1][j] - (float)(st_b[1][j] + wy), g.inv_h, typey, Ny, dNy);
+              }
+              const float m = st_m[j];
+              const float mvx = st_mv[0][j], mvy = st_mv[1][j], mvz = st_mv[2][j];
+              const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
+              const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
+              const float nn = Nx * Ny;
+              const float gx = dNx * Ny, gy = Nx * dNy;
+              // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
+              float Ax = Sxx * gx + Sxy * gy;
+              float Ay = Sxy * gx + Syy * gy;
+              float Az = Sxz * gx + Syz * gy;
+              if (PLANAR) {
+                Ax += st_f[0][j] * nn;
+                Ay += st_f[1][j] * nn;
+                Az += st_f[2][j] * nn;
+              }
+              const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
+              const float mn = m * nn, mvxn = mvx * nn, mvyn = mvy * nn, mvzn = mvz * nn;
+#pragma unroll
+              for (int k = 0; k < WIN; k++) {
+                const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
+                win[q][k][0] = fmaf(mn, Nz, win[q][k][0]);
+                win[q][k][1] = fmaf(mvxn, Nz, win[q][k][1]);
+                win[q][k][2] = fmaf(mvyn, Nz, win[q][k][2]);
+                win[q][k][3] = fmaf(mvzn, Nz, win[q][k][3]);
+                win[q][k][4] = fmaf(Bx, dNz, fmaf(Ax, Nz, win[q][k][4]));
+                win[q][k][5] = fmaf(By, dNz, fmaf(Ay, Nz, win[q][k][5]));
+                win[q][k][6] = fmaf(Bz, dNz, fmaf(Az, Nz, win[q][k][6]));
+              }
+            };
+            int j = j0;
+            for (; j + 1 < j1; j += 2) {
+              add(j);
+              add(j + 1);
+            }
+            if (j < j1) add(j);
+          }
+        }
+        if (le > p1) break;  // the layer goes on in the next piece
+        flush_shift(L);
+        L++;
+      }
+      __syncthreads();
     }
+    for (; L < nlayers; L++) flush_shift(L);  // layers after the last particle
     // ---- remaining window nodes after the last layer ----
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
