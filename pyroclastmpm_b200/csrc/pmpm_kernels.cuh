@@ -2569,8 +2569,14 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
     }
     // Separable sums: along x first (per (y, z) row of the stencil), then
     // weighted by the row's y/z factors.  v_pic = sum psi v_nt,
-    // dv = sum psi (v_nt - v), L = sum grad(psi) v_nt^T.
-    float vinc[3] = {0, 0, 0}, dvinc[3] = {0, 0, 0};
+    // dv = sum psi (v_nt - v), L = sum grad(psi) v_nt^T.  The x and y
+    // components go in packed FP32 pairs (the same roundings as one FMA per
+    // component), z alone.
+    float2 vinc2 = make_float2(0.0f, 0.0f), dvinc2 = make_float2(0.0f, 0.0f);
+    float vincz = 0.0f, dvincz = 0.0f;
+    float2 Lr2[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};  // L[r][0..1]
+    float Lrz[3] = {0.0f, 0.0f, 0.0f};                                                               // L[r][2]
+    const float2 minus1 = make_float2(-1.0f, -1.0f);
     constexpr int KZ = D == 3 ? K : 1;
     const float4 *vel = reinterpret_cast<const float4 *>(a.N.vel);
 #pragma unroll
@@ -2579,40 +2585,55 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
       for (int ky = 0; ky < K; ky++) {
         if (!ok[1][ky] || (D == 3 && !ok[2][kz])) continue;
         const int row = idx[1][ky] * g.n[0] + (D == 3 ? idx[2][kz] * g.n[0] * g.n[1] : 0);
-        float sv[3] = {0, 0, 0}, sd[3] = {0, 0, 0}, sg[3] = {0, 0, 0};
+        float2 sv2 = make_float2(0.0f, 0.0f), sd2 = make_float2(0.0f, 0.0f), sg2 = make_float2(0.0f, 0.0f);
+        float svz = 0.0f, sdz = 0.0f, sgz = 0.0f;
 #pragma unroll
         for (int kx = 0; kx < K; kx++) {
           if (!ok[0][kx]) continue;
           const int node = idx[0][kx] + row;
-          float vn[3], vnt[3];
+          const float n = N[0][kx], dn = dN[0][kx];
+          const float2 n2 = make_float2(n, n), dn2 = make_float2(dn, dn);
+          float2 vn2, vnt2;
           if (D == 3) {
             const float4 q0 = __ldg(vel + 2 * (size_t)node), q1 = __ldg(vel + 2 * (size_t)node + 1);
-            vn[0] = q0.x; vn[1] = q0.y; vn[2] = q0.z;
-            vnt[0] = q1.x; vnt[1] = q1.y; vnt[2] = q1.z;
+            vn2 = make_float2(q0.x, q0.y);
+            vnt2 = make_float2(q1.x, q1.y);
+            svz = fmaf(n, q1.z, svz);
+            sdz = fmaf(n, q1.z - q0.z, sdz);
+            sgz = fmaf(dn, q1.z, sgz);
           } else {
             const float4 q = __ldg(vel + node);
-            vn[0] = q.x; vn[1] = q.y; vn[2] = 0.0f;
-            vnt[0] = q.z; vnt[1] = q.w; vnt[2] = 0.0f;
+            vn2 = make_float2(q.x, q.y);
+            vnt2 = make_float2(q.z, q.w);
           }
-#pragma unroll
-          for (int c = 0; c < D; c++) {
-            sv[c] += N[0][kx] * vnt[c];
-            sd[c] += N[0][kx] * (vnt[c] - vn[c]);
-            sg[c] += dN[0][kx] * vnt[c];
-          }
+          sv2 = __ffma2_rn(n2, vnt2, sv2);
+          sd2 = __ffma2_rn(n2, __ffma2_rn(vn2, minus1, vnt2), sd2);  // v_nt - v, rounded once
+          sg2 = __ffma2_rn(dn2, vnt2, sg2);
         }
         const float wyz = D == 3 ? N[1][ky] * N[2][kz] : N[1][ky];
         const float gyz = D == 3 ? dN[1][ky] * N[2][kz] : dN[1][ky];
         const float wgz = D == 3 ? N[1][ky] * dN[2][kz] : 0.0f;
-#pragma unroll
-        for (int c = 0; c < D; c++) {
-          vinc[c] += wyz * sv[c];
-          dvinc[c] += wyz * sd[c];
-          L[0 * D + c] += wyz * sg[c];
-          L[1 * D + c] += gyz * sv[c];
-          if (D == 3) L[2 * D + c] += wgz * sv[c];
+        const float2 wyz2 = make_float2(wyz, wyz), gyz2 = make_float2(gyz, gyz);
+        vinc2 = __ffma2_rn(wyz2, sv2, vinc2);
+        dvinc2 = __ffma2_rn(wyz2, sd2, dvinc2);
+        Lr2[0] = __ffma2_rn(wyz2, sg2, Lr2[0]);
+        Lr2[1] = __ffma2_rn(gyz2, sv2, Lr2[1]);
+        if (D == 3) {
+          Lr2[2] = __ffma2_rn(make_float2(wgz, wgz), sv2, Lr2[2]);
+          vincz = fmaf(wyz, svz, vincz);
+          dvincz = fmaf(wyz, sdz, dvincz);
+          Lrz[0] = fmaf(wyz, sgz, Lrz[0]);
+          Lrz[1] = fmaf(gyz, svz, Lrz[1]);
+          Lrz[2] = fmaf(wgz, svz, Lrz[2]);
         }
       }
+    }
+    const float vinc[3] = {vinc2.x, vinc2.y, vincz}, dvinc[3] = {dvinc2.x, dvinc2.y, dvincz};
+#pragma unroll
+    for (int r = 0; r < D; r++) {
+      L[r * D + 0] = Lr2[r].x;
+      L[r * D + 1] = Lr2[r].y;
+      if (D == 3) L[r * D + 2] = Lrz[r];
     }
     // RigidBodyLevelSet::set_position (rigidbodylevelset.cpp:222-243) moved
     // rigid particles by their set velocity before G2P; their weights above
