@@ -1628,7 +1628,9 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     int item_cell[W::IPT], item_ix[W::IPT], item_iy[W::IPT], item_tl[W::IPT];
     int item_tx[W::IPT], item_ty[W::IPT];
     bool item_ok[W::IPT];
-    float win[W::IPT][WIN][7];
+    // window of WIN z nodes per item: (m, m vx), (m vy, m vz), (fx, fy), fz
+    float2 wa[W::IPT][WIN], wb[W::IPT][WIN], wc[W::IPT][WIN];
+    float wz[W::IPT][WIN];
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
       const int it = (round * W::IPT + q) * NT + tid;
@@ -1642,10 +1644,20 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
       item_ty[q] = pair_tgt(py);
       item_tl[q] = item_tx[q] + T::X * item_ty[q];
 #pragma unroll
-      for (int k = 0; k < WIN; k++)
-#pragma unroll
-        for (int c = 0; c < 7; c++) win[q][k][c] = 0.0f;
+      for (int k = 0; k < WIN; k++) {
+        wa[q][k] = wb[q][k] = wc[q][k] = make_float2(0.0f, 0.0f);
+        wz[q][k] = 0.0f;
+      }
     }
+    auto add_node = [&](int q, int k, int ln) {
+      atomicAdd(&acc[ln], wa[q][k].x);
+      atomicAdd(&acc[NT + ln], wa[q][k].y);
+      atomicAdd(&acc[2 * NT + ln], wb[q][k].x);
+      atomicAdd(&acc[3 * NT + ln], wb[q][k].y);
+      atomicAdd(&acc[4 * NT + ln], wc[q][k].x);
+      atomicAdd(&acc[5 * NT + ln], wc[q][k].y);
+      atomicAdd(&acc[6 * NT + ln], wz[q][k]);
+    };
     // ---- the lowest window node of layer L is complete: flush, shift ----
     auto flush_shift = [&](int L) {
 #pragma unroll
@@ -1654,18 +1666,17 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
           int tz = cz_lo + L + W::LO;
           if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
           const int lz = tz - t0[2];
-          if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
-            const int ln = item_tl[q] + T::X * T::Y * lz;
-#pragma unroll
-            for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NT + ln], win[q][0][c]);
-          }
+          if (lz >= 0 && lz < T::Z && tz < g.n[2]) add_node(q, 0, item_tl[q] + T::X * T::Y * lz);
         }
 #pragma unroll
-        for (int k = 0; k < WIN - 1; k++)
-#pragma unroll
-          for (int c = 0; c < 7; c++) win[q][k][c] = win[q][k + 1][c];
-#pragma unroll
-        for (int c = 0; c < 7; c++) win[q][WIN - 1][c] = 0.0f;
+        for (int k = 0; k < WIN - 1; k++) {
+          wa[q][k] = wa[q][k + 1];
+          wb[q][k] = wb[q][k + 1];
+          wc[q][k] = wc[q][k + 1];
+          wz[q][k] = wz[q][k + 1];
+        }
+        wa[q][WIN - 1] = wb[q][WIN - 1] = wc[q][WIN - 1] = make_float2(0.0f, 0.0f);
+        wz[q][WIN - 1] = 0.0f;
       }
     };
     // The tile's particles, all layers in z order, are positions
@@ -1732,27 +1743,27 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
               const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
               const float nn = Nx * Ny;
               const float gx = dNx * Ny, gy = Nx * dNy;
-              // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn)
-              float Ax = Sxx * gx + Sxy * gy;
-              float Ay = Sxy * gx + Syy * gy;
-              float Az = Sxz * gx + Syz * gy;
+              const float2 nn2 = make_float2(nn, nn);
+              // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn); x and
+              // y components in packed FP32 pairs
+              float2 A = __ffma2_rn(make_float2(Sxy, Syy), make_float2(gy, gy),
+                                    __fmul2_rn(make_float2(Sxx, Sxy), make_float2(gx, gx)));
+              float Az = fmaf(Syz, gy, Sxz * gx);
               if (PLANAR) {
-                Ax += st_f[0][j] * nn;
-                Ay += st_f[1][j] * nn;
-                Az += st_f[2][j] * nn;
+                A = __ffma2_rn(make_float2(st_f[0][j], st_f[1][j]), nn2, A);
+                Az = fmaf(st_f[2][j], nn, Az);
               }
-              const float Bx = Sxz * nn, By = Syz * nn, Bz = Szz * nn;
-              const float mn = m * nn, mvxn = mvx * nn, mvyn = mvy * nn, mvzn = mvz * nn;
+              const float2 B = __fmul2_rn(make_float2(Sxz, Syz), nn2);
+              const float Bz = Szz * nn;
+              const float2 mm = __fmul2_rn(make_float2(m, mvx), nn2), mv = __fmul2_rn(make_float2(mvy, mvz), nn2);
 #pragma unroll
               for (int k = 0; k < WIN; k++) {
                 const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
-                win[q][k][0] = fmaf(mn, Nz, win[q][k][0]);
-                win[q][k][1] = fmaf(mvxn, Nz, win[q][k][1]);
-                win[q][k][2] = fmaf(mvyn, Nz, win[q][k][2]);
-                win[q][k][3] = fmaf(mvzn, Nz, win[q][k][3]);
-                win[q][k][4] = fmaf(Bx, dNz, fmaf(Ax, Nz, win[q][k][4]));
-                win[q][k][5] = fmaf(By, dNz, fmaf(Ay, Nz, win[q][k][5]));
-                win[q][k][6] = fmaf(Bz, dNz, fmaf(Az, Nz, win[q][k][6]));
+                const float2 n2 = make_float2(Nz, Nz), d2 = make_float2(dNz, dNz);
+                wa[q][k] = __ffma2_rn(mm, n2, wa[q][k]);
+                wb[q][k] = __ffma2_rn(mv, n2, wb[q][k]);
+                wc[q][k] = __ffma2_rn(B, d2, __ffma2_rn(A, n2, wc[q][k]));
+                wz[q][k] = fmaf(Bz, dNz, fmaf(Az, Nz, wz[q][k]));
               }
             };
             int j = j0;
@@ -1779,11 +1790,7 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
         int tz = cz_hi + 1 + k + W::LO;
         if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
         const int lz = tz - t0[2];
-        if (lz >= 0 && lz < T::Z && tz < g.n[2]) {
-          const int ln = item_tl[q] + T::X * T::Y * lz;
-#pragma unroll
-          for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NT + ln], win[q][k][c]);
-        }
+        if (lz >= 0 && lz < T::Z && tz < g.n[2]) add_node(q, k, item_tl[q] + T::X * T::Y * lz);
       }
     }
   }
