@@ -1385,12 +1385,14 @@ struct Sweep3 {
   static constexpr int NL = T::Z + WIN - 1;          // source layers a tile reads
   static constexpr int NT = T::N;
   static constexpr int IPT = 2;                      // items per thread per round
-  // staged floats per particle: m, m v (3), -V sigma (6), the z weights and
-  // derivatives of the layer's WIN nodes; cubic adds the x and y weights and
-  // derivatives of the WIN offsets, linear the scaled x, y and bins; a
-  // PlanarDomain the external force (3)
+  static constexpr int NZ4 = (2 * WIN + 3) / 4;     // float4s of z weights
+  // staged floats per particle: the x and y weights of the WIN offsets
+  // (float2 N, dN each), float4 (m, m vx, m vy, m vz), float4 (Sxx, Sxy, Sxy,
+  // Syy), float4 (Sxz, Syz, Szz, 0), the z weights then derivatives of the
+  // layer's WIN nodes (NZ4 float4s); a PlanarDomain adds float4 (f, 0);
+  // S = -V sigma
   __host__ __device__ static constexpr int floats(bool planar) {
-    return 10 + 2 * WIN + (SF == PMPM_SHAPE_CUBIC ? 4 * WIN : 4) + (planar ? 3 : 0);
+    return 4 * WIN + 12 + 4 * NZ4 + (planar ? 4 : 0);
   }
   // static shared memory: pair lists, the all-layer cell table, scan scratch
   static constexpr int STATIC_BYTES = (4 * (2 * MAXPAIR + 2 + 2 * NL * NCELL + 1 + 33 + 1) + 255) / 256 * 256 + 256;
@@ -1451,21 +1453,16 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   __shared__ int cell_k0[W::NL * W::NCELL], cell_pref[W::NL * W::NCELL + 1];
   __shared__ int warp_tmp[33];
   // dynamic shared memory: tile accumulators, then the staged particles
-  // (structure of arrays, SL entries each); size sweep3_smem_bytes<SF, PLANAR>()
+  // (arrays of SL slots, see Sweep3::floats); size sweep3_smem_bytes<SF, PLANAR>()
   extern __shared__ __align__(16) float dyn_smem[];
-  float *acc = dyn_smem;                            // [7][NT]
-  float *st_m = acc + 7 * NT;                       // [SL]
-  float(*st_mv)[SL] = (float(*)[SL])(st_m + SL);    // [3] m v
-  float(*st_S)[SL] = st_mv + 3;                     // [6] -V sigma
-  float(*st_nz)[SL] = st_S + 6;                     // [WIN]
-  float(*st_dnz)[SL] = st_nz + WIN;                 // [WIN]
-  float(*st_wx)[SL] = st_dnz + WIN;                 // cubic: [WIN] x weights per offset
-  float(*st_dwx)[SL] = st_wx + WIN;                 // [WIN]
-  float(*st_wy)[SL] = st_dwx + WIN;                 // [WIN]
-  float(*st_dwy)[SL] = st_wy + WIN;                 // [WIN]
-  float(*st_u)[SL] = st_dnz + WIN;                  // linear / quadratic: [2] scaled x, y
-  int(*st_b)[SL] = (int(*)[SL])(st_u + 2);          // [2] bins x, y
-  float(*st_f)[SL] = SF == PMPM_SHAPE_CUBIC ? st_dwy + WIN : (float(*)[SL])(st_b + 2);  // [3] external force
+  float *acc = dyn_smem;                                    // [7][NT]
+  float2(*st_wx)[SL] = (float2(*)[SL])(acc + 7 * NT);       // [WIN] x weights (N, dN) per offset
+  float2(*st_wy)[SL] = st_wx + WIN;                         // [WIN]
+  float4 *st_p = (float4 *)(st_wy + WIN);                   // (m, m v)
+  float4 *st_s0 = st_p + SL;                                // (Sxx, Sxy, Sxy, Syy)
+  float4 *st_s1 = st_s0 + SL;                               // (Sxz, Syz, Szz, 0)
+  float4(*st_z)[SL] = (float4(*)[SL])(st_s1 + SL);          // [NZ4] z N[0..WIN), dN[0..WIN)
+  float4 *st_f = (float4 *)(st_z + W::NZ4);                 // PLANAR: (f, 0)
 
   const int tid = threadIdx.x;
   const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
@@ -1558,68 +1555,52 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     float m = P.m[s];
     if (SF == PMPM_SHAPE_QUADRATIC && !inside) m = 0.0f;  // takes no part in P2G
     const float nv = ((SF == PMPM_SHAPE_QUADRATIC && !inside) || a.remap) ? 0.0f : -P.V[s];
-    if (SF != PMPM_SHAPE_CUBIC) {
-      st_u[0][jj] = u[0];
-      st_u[1][jj] = u[1];
-      st_b[0][jj] = b[0];
-      st_b[1][jj] = b[1];
-    }
-    st_m[jj] = m;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      st_mv[c][jj] = m * P.v[c * st + s];
-      if (PLANAR) st_f[c][jj] = (m != 0.0f && !a.remap) ? P.fext[c * st + s] : 0.0f;
+    st_p[jj] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
+    if (PLANAR) {
+      const bool use = m != 0.0f && !a.remap;
+      st_f[jj] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f, use ? P.fext[2 * st + s] : 0.0f,
+                             0.0f);
     }
     // -V sigma, symmetric: xx yy zz xy xz yz
+    const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
+    const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
+    st_s0[jj] = make_float4(Sxx, Sxy, Sxy, Syy);
+    st_s1[jj] = make_float4(Sxz, Syz, Szz, 0.0f);
+    // weights of the WIN offsets per axis: r from the particle's own bin
+    // (the reference psi), the cubic node type of the target the offset
+    // reaches from the (possibly aliased) source cell the particle is
+    // staged for.  Cubic at u >= 0: offset w sits on spline piece 2 - w
+    // (r in [-w, 1 - w)), so its coefficients are the same for neighbouring
+    // lanes; u < 0 takes the general form
+    const int src[3] = {t0[0] - W::HI + vc % W::NS, t0[1] - W::HI + vc / W::NS, cz};
+    float zf[4 * W::NZ4];
 #pragma unroll
-    for (int k = 0; k < 6; k++) st_S[k][jj] = nv * P.sig[k * st + s];
+    for (int k = 0; k < 4 * W::NZ4; k++) zf[k] = 0.0f;
 #pragma unroll
-    for (int k = 0; k < WIN; k++) {
-      const int tz = cz + k + W::LO;
-      const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(min(max(tz, 0), g.n[2] - 1), g.n[2]) : 0;
-      const float r = u[2] - (float)(b[2] + k + W::LO);
-      float N, dN;
-      if (SF == PMPM_SHAPE_CUBIC && u[2] >= 0.0f) {
-        // fixed spline piece of offset k (see the x / y weights below)
-        const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
-        N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
-        dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
-      } else {
-        axis_weight<SF>(r, g.inv_h, type, N, dN);
-      }
-      st_nz[k][jj] = N;
-      st_dnz[k][jj] = dN;
-    }
-    if (SF == PMPM_SHAPE_CUBIC) {
-      // x and y weights of the four offsets: r from the particle's own
-      // bin, the node type of the target the offset reaches from the
-      // (possibly aliased) source cell it is staged for.  At u >= 0
-      // offset w sits on spline piece 2 - w (r in [-w, 1 - w)), so its
-      // coefficients are the same for neighbouring lanes; u < 0 takes
-      // the general form
-      const int src[2] = {t0[0] - W::HI + vc % W::NS, t0[1] - W::HI + vc / W::NS};
+    for (int c = 0; c < 3; c++) {
 #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        float(*wN)[SL] = c == 0 ? st_wx : st_wy;
-        float(*wD)[SL] = c == 0 ? st_dwx : st_dwy;
-#pragma unroll
-        for (int k = 0; k < WIN; k++) {
-          const int tgt = src[c] + k + W::LO;
-          const int type = cubic_node_type(min(max(tgt, 0), g.n[c] - 1), g.n[c]);
-          const float r = u[c] - (float)(b[c] + k + W::LO);
-          float N, dN;
-          if (u[c] >= 0.0f) {
-            const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
-            N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
-            dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
-          } else {
-            axis_weight<SF>(r, g.inv_h, type, N, dN);
-          }
-          wN[k][jj] = N;
-          wD[k][jj] = dN;
+      for (int k = 0; k < WIN; k++) {
+        const int tgt = src[c] + k + W::LO;
+        const int type = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(min(max(tgt, 0), g.n[c] - 1), g.n[c]) : 0;
+        const float r = u[c] - (float)(b[c] + k + W::LO);
+        float N, dN;
+        if (SF == PMPM_SHAPE_CUBIC && u[c] >= 0.0f) {
+          const float *cw = kCubicW[type][WIN - 1 - k], *cd = kCubicD[type][WIN - 1 - k];
+          N = ((cw[0] * r + cw[1]) * r + cw[2]) * r + cw[3];
+          dN = g.inv_h * ((cd[0] * r + cd[1]) * r + cd[2]);
+        } else {
+          axis_weight<SF>(r, g.inv_h, type, N, dN);
+        }
+        if (c == 0) st_wx[k][jj] = make_float2(N, dN);
+        else if (c == 1) st_wy[k][jj] = make_float2(N, dN);
+        else {
+          zf[k] = N;
+          zf[WIN + k] = dN;
         }
       }
     }
+#pragma unroll
+    for (int k = 0; k < W::NZ4; k++) st_z[k][jj] = make_float4(zf[4 * k], zf[4 * k + 1], zf[4 * k + 2], zf[4 * k + 3]);
   };
 
   constexpr int R = (SL + NT - 1) / NT;
@@ -1721,44 +1702,39 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
             if (!item_ok[q]) continue;
             const int vc = item_cell[q];
             const int j0 = max(pref[vc], p0) - p0, j1 = min(pref[vc + 1], p1) - p0;
-            const int wx = item_ix[q] + W::LO, wy = item_iy[q] + W::LO;
-            const int typex = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[0] + item_tx[q], g.n[0]) : 0;
-            const int typey = SF == PMPM_SHAPE_CUBIC ? cubic_node_type(t0[1] + item_ty[q], g.n[1]) : 0;
-            const int ix = item_ix[q], iy = item_iy[q];
+            const float2 *wxp = st_wx[item_ix[q]], *wyp = st_wy[item_iy[q]];
             auto add = [&](int jp) {
               const int j = sweep_slot(jp);
-              float Nx, dNx, Ny, dNy;
-              if (SF == PMPM_SHAPE_CUBIC) {
-                Nx = st_wx[ix][j];
-                dNx = st_dwx[ix][j];
-                Ny = st_wy[iy][j];
-                dNy = st_dwy[iy][j];
-              } else {
-                axis_weight<SF>(st_u[0][j] - (float)(st_b[0][j] + wx), g.inv_h, typex, Nx, dNx);
-                axis_weight<SF>(st_u[1][j] - (float)(st_b[1][j] + wy), g.inv_h, typey, Ny, dNy);
+              const float2 wx = wxp[j], wy = wyp[j];
+              const float4 pm = st_p[j], s0 = st_s0[j], s1 = st_s1[j];
+              float zf[4 * W::NZ4];
+#pragma unroll
+              for (int k = 0; k < W::NZ4; k++) {
+                const float4 z4 = st_z[k][j];
+                zf[4 * k] = z4.x;
+                zf[4 * k + 1] = z4.y;
+                zf[4 * k + 2] = z4.z;
+                zf[4 * k + 3] = z4.w;
               }
-              const float m = st_m[j];
-              const float mvx = st_mv[0][j], mvy = st_mv[1][j], mvz = st_mv[2][j];
-              const float Sxx = st_S[0][j], Syy = st_S[1][j], Szz = st_S[2][j];
-              const float Sxy = st_S[3][j], Sxz = st_S[4][j], Syz = st_S[5][j];
-              const float nn = Nx * Ny;
-              const float gx = dNx * Ny, gy = Nx * dNy;
+              const float nn = wx.x * wy.x;
+              const float gx = wx.y * wy.x, gy = wx.x * wy.y;
               const float2 nn2 = make_float2(nn, nn);
               // f_c = Nz (f_ext,c nn + S_c0 gx + S_c1 gy) + dNz (S_c2 nn); x and
               // y components in packed FP32 pairs
-              float2 A = __ffma2_rn(make_float2(Sxy, Syy), make_float2(gy, gy),
-                                    __fmul2_rn(make_float2(Sxx, Sxy), make_float2(gx, gx)));
-              float Az = fmaf(Syz, gy, Sxz * gx);
+              float2 A = __ffma2_rn(make_float2(s0.z, s0.w), make_float2(gy, gy),
+                                    __fmul2_rn(make_float2(s0.x, s0.y), make_float2(gx, gx)));
+              float Az = fmaf(s1.y, gy, s1.x * gx);
               if (PLANAR) {
-                A = __ffma2_rn(make_float2(st_f[0][j], st_f[1][j]), nn2, A);
-                Az = fmaf(st_f[2][j], nn, Az);
+                const float4 fe = st_f[j];
+                A = __ffma2_rn(make_float2(fe.x, fe.y), nn2, A);
+                Az = fmaf(fe.z, nn, Az);
               }
-              const float2 B = __fmul2_rn(make_float2(Sxz, Syz), nn2);
-              const float Bz = Szz * nn;
-              const float2 mm = __fmul2_rn(make_float2(m, mvx), nn2), mv = __fmul2_rn(make_float2(mvy, mvz), nn2);
+              const float2 B = __fmul2_rn(make_float2(s1.x, s1.y), nn2);
+              const float Bz = s1.z * nn;
+              const float2 mm = __fmul2_rn(make_float2(pm.x, pm.y), nn2), mv = __fmul2_rn(make_float2(pm.z, pm.w), nn2);
 #pragma unroll
               for (int k = 0; k < WIN; k++) {
-                const float Nz = st_nz[k][j], dNz = st_dnz[k][j];
+                const float Nz = zf[k], dNz = zf[WIN + k];
                 const float2 n2 = make_float2(Nz, Nz), d2 = make_float2(dNz, dNz);
                 wa[q][k] = __ffma2_rn(mm, n2, wa[q][k]);
                 wb[q][k] = __ffma2_rn(mv, n2, wb[q][k]);
