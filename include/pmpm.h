@@ -416,9 +416,9 @@ int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float d
 /* Spatial partition that allocates no device memory.  No counterpart in the
  * reference; it gives the results of pmpm_partition (reference hashing,
  * stable sort, cell ranges) to callers that cannot allocate device memory at
- * the point they need them, for example code running while a CUDA graph is
- * being captured, code inside an allocator callback, or plug-ins held to a
- * fixed memory budget.  The caller passes device pointers: positions
+ * the point they need them, for example code inside a memory pool's or a
+ * framework's allocation callback, or plug-ins held to a fixed device-memory
+ * budget by their host application.  The caller passes device pointers: positions
  * [n][dim] (the particles in index order) in, and hash_unsorted [n],
  * sorted_index [n] (binned particles), cell_start and cell_end [cells] out,
  * with cells = num_cells[0] * num_cells[1] (* num_cells[2]).  Temporaries

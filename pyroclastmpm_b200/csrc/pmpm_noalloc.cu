@@ -1,10 +1,9 @@
 // Spatial partition without any device allocation (pmpm_partition_noalloc).
 //
 // Some callers cannot allocate device memory at the point where they need a
-// partition: code that runs while a CUDA graph is being captured (cudaMalloc
-// is not allowed during stream capture), host code that runs inside a memory
-// pool's or framework's allocation callback, or plug-ins that live under a
-// fixed device-memory budget handed to them by a host application.  This
+// partition: host code that runs inside a memory pool's or a framework's
+// allocation callback, or plug-ins that live under a fixed device-memory
+// budget handed to them by a host application.  This
 // entry point serves them: the caller provides the inputs and the outputs,
 // and the temporary arrays live in one file-scope device array of fixed size
 // that every GPU which loads this library holds until the process exits.

@@ -1,8 +1,8 @@
 """The allocation-free partition entry point (pmpm_partition_noalloc).
 
-Callers that cannot allocate device memory where they need a partition (a
-CUDA graph being captured, an allocator callback, a plug-in on a fixed memory
-budget) use this entry point: they pass the inputs and outputs, and the
+Callers that cannot allocate device memory where they need a partition (an
+allocator callback, a plug-in on a fixed device-memory budget) use this entry
+point: they pass the inputs and outputs, and the
 library's temporaries live in a fixed array inside the library.  This test
 calls it through the C ABI twice in a row (the second call must not see
 leftovers of the first) and checks it against the regular partition entry
