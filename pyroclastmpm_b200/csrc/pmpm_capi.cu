@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -2243,8 +2244,9 @@ int batch_step(pmpm_batch *b, float *ms) {
   // the next partition's binning rides on this G2P (not with a PlanarDomain,
   // whose particle forces the binning pass computes)
   const bool bin_next = !b->has_planar;
+  const int view_words = (int)((b->has_planar ? sizeof(StepArgs) : offsetof(StepArgs, bc)) / sizeof(int));
   kb_g2p<D, SF><<<b->nblocks, kTPB, 0, b->stream>>>(b->d_views, b->d_blocks, P, b->epoch, 1, store_L,
-                                                     bin_next ? 1 : 0, b->hash_next);
+                                                     bin_next ? 1 : 0, b->hash_next, view_words);
   PMPM_LAUNCHED();
   b->keys_fresh = bin_next;
   b->launches += 2;

@@ -2888,12 +2888,13 @@ struct BatchTile {
   int inst, tile, global_tile;  // node tile `tile` of instance inst
 };
 
+// nwords: how much of the view to copy (the whole of it unless the kernel
+// reads nothing past a known member)
 __device__ __forceinline__ void load_view(StepArgs &sa, const StepArgs *views, int inst, const DevParticles &P,
-                                          int epoch) {
+                                          int epoch, int nwords = (int)(sizeof(StepArgs) / sizeof(int))) {
   const int *src = reinterpret_cast<const int *>(views + inst);
   int *dst = reinterpret_cast<int *>(&sa);
-  constexpr int W = (int)(sizeof(StepArgs) / sizeof(int));
-  for (int k = threadIdx.x; k < W; k += blockDim.x) dst[k] = __ldg(src + k);
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) dst[k] = __ldg(src + k);
   __syncthreads();
   if (threadIdx.x == 0) {
     sa.P = P;
@@ -2941,14 +2942,16 @@ __global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) kb_p2g(const S
 }
 
 // bin_next: also bin the new positions for the next partition (as k_g2p),
-// their reference hashes into hash_next
+// their reference hashes into hash_next.  view_words: the part of the
+// instance view to copy (G2P and the stress update read nothing of the node
+// conditions; the binning reads them only for a PlanarDomain)
 template <int D, int SF>
 __global__ void __launch_bounds__(256) kb_g2p(const StepArgs *views, const BatchBlock *blocks, DevParticles P,
                                               int epoch, int do_stress, int store_L, int bin_next,
-                                              unsigned *hash_next) {
+                                              unsigned *hash_next, int view_words) {
   __shared__ StepArgs sa;
   const BatchBlock b = blocks[blockIdx.x];
-  load_view(sa, views, b.inst, P, epoch);
+  load_view(sa, views, b.inst, P, epoch, view_words);
   const int s = b.first + (int)threadIdx.x;
   if (s < b.end) g2p_body<D, SF, false>(sa, s, do_stress, store_L);  // batches hold no iterative material
   if (bin_next) hash_count_body<D, SF>(sa, s, s < b.end, epoch + 1, hash_next);
