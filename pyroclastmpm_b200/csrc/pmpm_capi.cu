@@ -424,9 +424,17 @@ int launch_partition(pmpm_sim *s) {
   s->keys_fresh = false;
   s->launches += 7;
   if (D == 3 && !(s->flags & PMPM_FLAG_DETERMINISTIC)) {
-    // active-tile queue of the persistent 3D sweep P2G kernels
-    k_tile_list<<<(s->g.ntiles + 255) / 256, 256, 0, st>>>(s->N.tile_epoch, s->g.ntiles, s->epoch, s->N.tile_list,
-                                                          s->N.tile_queue);
+    // active queue of the persistent 3D sweep P2G kernels: tiles (dual
+    // sweep) or pairs of tiles stacked in z (linear and cubic sweeps)
+    if (SF == PMPM_SHAPE_QUADRATIC) {
+      k_tile_list<<<(s->g.ntiles + 255) / 256, 256, 0, st>>>(s->N.tile_epoch, s->g.ntiles, s->epoch,
+                                                            s->N.tile_list, s->N.tile_queue);
+    } else {
+      const int plane = s->g.tdim[0] * s->g.tdim[1];
+      const int nunits = plane * ((s->g.tdim[2] + 1) / 2);
+      k_pair_list<<<(nunits + 255) / 256, 256, 0, st>>>(s->N.tile_epoch, plane, s->g.tdim[2], s->epoch,
+                                                        s->N.tile_list, s->N.tile_queue);
+    }
     PMPM_LAUNCHED();
     s->launches += 1;
   }

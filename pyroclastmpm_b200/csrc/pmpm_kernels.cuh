@@ -71,6 +71,32 @@ __global__ void __launch_bounds__(256) k_tile_list(const int *tile_epoch, int nt
   }
 }
 
+// Active queue of tile pairs stacked in z (tiles tz = 2k and 2k + 1 of one
+// column; unit u = column + k * columns), for the linear and cubic sweeps:
+// a pair is active when either tile is marked with this partition's epoch.
+__global__ void __launch_bounds__(256) k_pair_list(const int *tile_epoch, int plane, int tdim2, int epoch,
+                                                   int *list, int *queue) {
+  const int nunits = plane * ((tdim2 + 1) / 2);
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  int *count = &queue[epoch & 1];
+  if (u == 0) queue[(epoch + 1) & 1] = 0;
+  bool on = false;
+  if (u < nunits) {
+    const int col = u % plane, tz = 2 * (u / plane);
+    on = tile_epoch[col + tz * plane] == epoch || (tz + 1 < tdim2 && tile_epoch[col + (tz + 1) * plane] == epoch);
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, on);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == __ffs(m) - 1) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  if (on) {
+    const int i = base + __popc(m & ((1u << lane) - 1u));
+    if (i < nunits) list[i] = u;
+  }
+}
+
 // Next tile of the active-tile queue for the whole CTA, or -1.
 __device__ __forceinline__ int next_tile(const StepArgs &a, int *cur) {
   if (threadIdx.x == 0) *cur = atomicAdd(&a.N.tile_queue[2 + a.p2g_par], 1);
@@ -1356,9 +1382,10 @@ __global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) k_p2g_tile(Ste
 // P2G, 3D fast path: z-sweep with register windows
 // --------------------------------------------------------------------------
 //
-// One CTA per active 8x8x8 node tile.  Work item = (x pair, y pair), a pair
-// being (source cell column, stencil offset) whose target node column lies in
-// the tile.  Each item sweeps the source cell layers along z.  For every
+// One CTA per active work unit of two 8x8x8 node tiles stacked in z (8x8x16
+// nodes, so a cubic unit reads 19 source layers for 16 node layers instead
+// of 11 for 8).  Work item = (x pair, y pair), a pair being (source cell
+// column, stencil offset) whose target node column lies in the unit.  Each item sweeps the source cell layers along z.  For every
 // layer the CTA stages the particles of the layer's halo cells in shared
 // memory (with their z weights, which every item needs), then each item adds
 // its source cell's particles into a register window of the WIN z nodes
@@ -1382,7 +1409,9 @@ struct Sweep3 {
   static constexpr int NS = T::X + WIN - 1;          // source cells per axis
   static constexpr int MAXPAIR = NS * WIN;           // (source, offset) pairs per axis
   static constexpr int NCELL = NS * NS;              // source cells per layer
-  static constexpr int NL = T::Z + WIN - 1;          // source layers a tile reads
+  static constexpr int TZ = 2 * T::Z;                // nodes along z of a work unit (two tiles)
+  static constexpr int NN = T::X * T::Y * TZ;        // nodes of a work unit
+  static constexpr int NL = TZ + WIN - 1;            // source layers a unit reads
   static constexpr int NT = T::N;
   static constexpr int IPT = 2;                      // items per thread per round
   static constexpr int NZ4 = (2 * WIN + 3) / 4;     // float4s of z weights
@@ -1399,13 +1428,13 @@ struct Sweep3 {
   // staged particles: 227 KB per CTA less the static part and the node
   // accumulators
   __host__ __device__ static constexpr int cap(bool planar) {
-    return ((232448 - STATIC_BYTES - 7 * NT * 4) / (4 * floats(planar))) & ~7;
+    return ((232448 - STATIC_BYTES - 7 * NN * 4) / (4 * floats(planar))) & ~7;
   }
 };
 
 template <int SF, bool PLANAR>
 constexpr int sweep3_smem_bytes() {
-  return (7 * Sweep3<SF>::NT + Sweep3<SF>::cap(PLANAR) * Sweep3<SF>::floats(PLANAR)) * 4;
+  return (7 * Sweep3<SF>::NN + Sweep3<SF>::cap(PLANAR) * Sweep3<SF>::floats(PLANAR)) * 4;
 }
 
 // pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
@@ -1439,12 +1468,13 @@ __device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
 __device__ __forceinline__ int sweep_slot(int j) { return j ^ ((j >> 3) & 7); }
 
 template <int SF, bool PLANAR>
-__device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile) {
+__device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int unit) {
   using W = Sweep3<SF>;
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int WIN = W::WIN;
   constexpr int SL = W::cap(PLANAR);
+  constexpr int TZ = W::TZ, NN = W::NN;
   const DevGrid &g = a.g;
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
@@ -1455,8 +1485,8 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   // dynamic shared memory: tile accumulators, then the staged particles
   // (arrays of SL slots, see Sweep3::floats); size sweep3_smem_bytes<SF, PLANAR>()
   extern __shared__ __align__(16) float dyn_smem[];
-  float *acc = dyn_smem;                                    // [7][NT]
-  float2(*st_wx)[SL] = (float2(*)[SL])(acc + 7 * NT);       // [WIN] x weights (N, dN) per offset
+  float *acc = dyn_smem;                                    // [7][NN]
+  float2(*st_wx)[SL] = (float2(*)[SL])(acc + 7 * NN);       // [WIN] x weights (N, dN) per offset
   float2(*st_wy)[SL] = st_wx + WIN;                         // [WIN]
   float4 *st_p = (float4 *)(st_wy + WIN);                   // (m, m v)
   float4 *st_s0 = st_p + SL;                                // (Sxx, Sxy, Sxy, Syy)
@@ -1464,13 +1494,15 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   float4(*st_z)[SL] = (float4(*)[SL])(st_s1 + SL);          // [NZ4] z N[0..WIN), dN[0..WIN)
   float4 *st_f = (float4 *)(st_z + W::NZ4);                 // PLANAR: (f, 0)
 
+  // work unit `unit`: the two tiles 2k, 2k + 1 along z of one tile column
   const int tid = threadIdx.x;
-  const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
-                     (tile / (g.tdim[0] * g.tdim[1])) * T::Z};
-#pragma unroll
-  for (int k = 0; k < 7; k++) acc[k * NT + tid] = 0.0f;
+  const int plane = g.tdim[0] * g.tdim[1];
+  const int col = unit % plane, tz0 = 2 * (unit / plane);
+  const int t0[3] = {(col % g.tdim[0]) * T::X, (col / g.tdim[0]) * T::Y, tz0 * T::Z};
+  for (int k = tid; k < 7 * NN; k += NT) acc[k] = 0.0f;
   if (tid == 0) {
-    node_epoch[tile] = a.epoch;
+    node_epoch[col + tz0 * plane] = a.epoch;
+    if (tz0 + 1 < g.tdim[2]) node_epoch[col + (tz0 + 1) * plane] = a.epoch;
     npair[0] = build_pairs<SF>(t0[0], g.n[0], pairs_x);
   } else if (tid == 32) {
     npair[1] = build_pairs<SF>(t0[1], g.n[1], pairs_y);
@@ -1481,7 +1513,7 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   const int nrounds = (nitems + NT * W::IPT - 1) / (NT * W::IPT);
 
   // z range of source layers
-  int cz_lo = t0[2] - W::HI, cz_hi = t0[2] + T::Z - 1 - W::LO;
+  int cz_lo = t0[2] - W::HI, cz_hi = t0[2] + TZ - 1 - W::LO;
   if (SF == PMPM_SHAPE_QUADRATIC) {
     cz_lo = max(cz_lo, 0);
     cz_hi = min(cz_hi, g.n[2] - 1);
@@ -1632,12 +1664,12 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     }
     auto add_node = [&](int q, int k, int ln) {
       atomicAdd(&acc[ln], wa[q][k].x);
-      atomicAdd(&acc[NT + ln], wa[q][k].y);
-      atomicAdd(&acc[2 * NT + ln], wb[q][k].x);
-      atomicAdd(&acc[3 * NT + ln], wb[q][k].y);
-      atomicAdd(&acc[4 * NT + ln], wc[q][k].x);
-      atomicAdd(&acc[5 * NT + ln], wc[q][k].y);
-      atomicAdd(&acc[6 * NT + ln], wz[q][k]);
+      atomicAdd(&acc[NN + ln], wa[q][k].y);
+      atomicAdd(&acc[2 * NN + ln], wb[q][k].x);
+      atomicAdd(&acc[3 * NN + ln], wb[q][k].y);
+      atomicAdd(&acc[4 * NN + ln], wc[q][k].x);
+      atomicAdd(&acc[5 * NN + ln], wc[q][k].y);
+      atomicAdd(&acc[6 * NN + ln], wz[q][k]);
     };
     // ---- the lowest window node of layer L is complete: flush, shift ----
     auto flush_shift = [&](int L) {
@@ -1647,7 +1679,7 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
           int tz = cz_lo + L + W::LO;
           if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
           const int lz = tz - t0[2];
-          if (lz >= 0 && lz < T::Z && tz < g.n[2]) add_node(q, 0, item_tl[q] + T::X * T::Y * lz);
+          if (lz >= 0 && lz < TZ && tz < g.n[2]) add_node(q, 0, item_tl[q] + T::X * T::Y * lz);
         }
 #pragma unroll
         for (int k = 0; k < WIN - 1; k++) {
@@ -1766,31 +1798,33 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
         int tz = cz_hi + 1 + k + W::LO;
         if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
         const int lz = tz - t0[2];
-        if (lz >= 0 && lz < T::Z && tz < g.n[2]) add_node(q, k, item_tl[q] + T::X * T::Y * lz);
+        if (lz >= 0 && lz < TZ && tz < g.n[2]) add_node(q, k, item_tl[q] + T::X * T::Y * lz);
       }
     }
   }
   __syncthreads();
 
-  // ---- node epilogue (one node per thread) ----
-  const int lx = tid % T::X, ly = (tid / T::X) % T::Y, lz = tid / (T::X * T::Y);
-  const int nc[3] = {t0[0] + lx, t0[1] + ly, t0[2] + lz};
-  if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) return;
-  const int node = flat_index(g, nc[0], nc[1], nc[2]);
-  float mass = acc[tid];
-  float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
-  const bool live = mass > a.cutoff;
-  if (live) {
+  // ---- node epilogue (two nodes per thread) ----
+  for (int ln = tid; ln < NN; ln += NT) {
+    const int lx = ln % T::X, ly = (ln / T::X) % T::Y, lz = ln / (T::X * T::Y);
+    const int nc[3] = {t0[0] + lx, t0[1] + ly, t0[2] + lz};
+    if (nc[0] >= g.n[0] || nc[1] >= g.n[1] || nc[2] >= g.n[2]) continue;
+    const int node = flat_index(g, nc[0], nc[1], nc[2]);
+    float mass = acc[ln];
+    float p[3] = {0.0f, 0.0f, 0.0f}, pnt[3] = {0.0f, 0.0f, 0.0f};
+    const bool live = mass > a.cutoff;
+    if (live) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      p[c] = acc[(1 + c) * NT + tid];
-      pnt[c] = p[c] + acc[(4 + c) * NT + tid] * a.dt;
+      for (int c = 0; c < 3; c++) {
+        p[c] = acc[(1 + c) * NN + ln];
+        pnt[c] = p[c] + acc[(4 + c) * NN + ln] * a.dt;
+      }
+    } else {
+      mass = 0.0f;
     }
-  } else {
-    mass = 0.0f;
+    if (apply_bcs) node_bcs<3>(a, node, nc, mass, p, pnt);
+    write_node<3>(a, node, mass, p, pnt, live);
   }
-  if (apply_bcs) node_bcs<3>(a, node, nc, mass, p, pnt);
-  write_node<3>(a, node, mass, p, pnt, live);
 }
 
 // One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
@@ -1798,8 +1832,8 @@ template <int SF, bool PLANAR>
 __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
-  for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
-    sweep3_tile<SF, PLANAR>(a, apply_bcs, node_epoch, tile);
+  for (int unit = next_tile(a, &cur); unit >= 0; unit = next_tile(a, &cur))
+    sweep3_tile<SF, PLANAR>(a, apply_bcs, node_epoch, unit);
 }
 
 // --------------------------------------------------------------------------
