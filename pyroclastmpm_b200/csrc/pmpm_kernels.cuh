@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(256) k_hash_count(StepArgs a) {
 }
 
 constexpr int kScanThreads = 1024;
-constexpr int kScanPer = 4;
+constexpr int kScanPer = 16;
 constexpr int kScanChunk = kScanThreads * kScanPer;
 
 __device__ __forceinline__ int block_exclusive_scan(int v, int *smem_warp, int &total) {
@@ -331,29 +331,22 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *smem_warp, int &
   return r;
 }
 
-// kScanPer consecutive keys per thread: one 16-byte access when all are in range
-__device__ __forceinline__ void load_keys4(const int *p, int base, int n, int v[kScanPer]) {
-  static_assert(kScanPer == 4, "vector width");
+// kScanPer consecutive keys per thread: 16-byte accesses when all are in range
+__device__ __forceinline__ void load_keys(const int *p, int base, int n, int v[kScanPer]) {
+  static_assert(kScanPer % 4 == 0, "vector width");
   if (base + kScanPer <= n) {
-    const int4 q = *reinterpret_cast<const int4 *>(p + base);
-    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+#pragma unroll
+    for (int q = 0; q < kScanPer / 4; q++) {
+      const int4 w = *reinterpret_cast<const int4 *>(p + base + 4 * q);
+      v[4 * q] = w.x;
+      v[4 * q + 1] = w.y;
+      v[4 * q + 2] = w.z;
+      v[4 * q + 3] = w.w;
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) v[k] = base + k < n ? p[base + k] : 0;
   }
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int *count, int n, int *block_sums) {
-  __shared__ int sw[33];
-  const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
-  int v[kScanPer];
-  load_keys4(count, base, n, v);
-  int sum = 0;
-#pragma unroll
-  for (int k = 0; k < kScanPer; k++) sum += v[k];
-  int total;
-  block_exclusive_scan(sum, sw, total);
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
 // Single-pass exclusive scan of the per-key counts into offsets (decoupled
@@ -378,7 +371,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n
   const int blk = sh_block;
   const int base = blk * kScanChunk + threadIdx.x * kScanPer;
   int v[kScanPer];
-  load_keys4(count, base, n, v);
+  load_keys(count, base, n, v);
   int sum = 0;
 #pragma unroll
   for (int k = 0; k < kScanPer; k++) sum += v[k];
@@ -432,9 +425,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n
   __syncthreads();
   int ex = ex_local + sh_prefix;
   if (base + kScanPer <= n) {
-    const int4 o = make_int4(ex, ex + v[0], ex + v[0] + v[1], ex + v[0] + v[1] + v[2]);
-    *reinterpret_cast<int4 *>(offset + base) = o;
-    *reinterpret_cast<int4 *>(count + base) = make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int q = 0; q < kScanPer / 4; q++) {
+      int4 o;
+      o.x = ex;
+      o.y = o.x + v[4 * q];
+      o.z = o.y + v[4 * q + 1];
+      o.w = o.z + v[4 * q + 2];
+      ex = o.w + v[4 * q + 3];
+      *reinterpret_cast<int4 *>(offset + base + 4 * q) = o;
+      *reinterpret_cast<int4 *>(count + base + 4 * q) = make_int4(0, 0, 0, 0);
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
@@ -445,54 +446,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n
       ex += v[k];
     }
   }
-}
-
-// Scans the block sums in place (single CTA) and resets the per-step counters.
-__global__ void __launch_bounds__(kScanThreads) k_scan_top(int *block_sums, int nblocks, int *scalars) {
-  __shared__ int sw[33];
-  int carry = 0;
-  for (int base = 0; base < nblocks; base += kScanThreads) {
-    int i = base + threadIdx.x;
-    int v = i < nblocks ? block_sums[i] : 0;
-    int total;
-    int ex = block_exclusive_scan(v, sw, total);
-    if (i < nblocks) block_sums[i] = carry + ex;
-    carry += total;
-  }
-  if (threadIdx.x == 0) {
-    scalars[0] = carry;  // binned particles
-    scalars[1] = 0;      // unbinned counter
-    scalars[2] = 0;      // big-cell counter
-  }
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(int *count, int n, const int *block_sums,
-                                                               int *offset) {
-  __shared__ int sw[33];
-  const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
-  int v[kScanPer];
-  load_keys4(count, base, n, v);
-  int sum = 0;
-#pragma unroll
-  for (int k = 0; k < kScanPer; k++) sum += v[k];
-  int total;
-  int ex = block_exclusive_scan(sum, sw, total) + block_sums[blockIdx.x];
-  if (base + kScanPer <= n) {
-    const int4 o = make_int4(ex, ex + v[0], ex + v[0] + v[1], ex + v[0] + v[1] + v[2]);
-    *reinterpret_cast<int4 *>(offset + base) = o;
-    *reinterpret_cast<int4 *>(count + base) = make_int4(0, 0, 0, 0);
-    ex = o.w + v[3];
-  } else {
-#pragma unroll
-    for (int k = 0; k < kScanPer; k++) {
-      if (base + k < n) {
-        offset[base + k] = ex;
-        count[base + k] = 0;
-      }
-      ex += v[k];
-    }
-  }
-  if (base <= n - 1 && n - 1 < base + kScanPer) offset[n] = ex;
 }
 
 __global__ void __launch_bounds__(256) k_scatter(StepArgs a) {
