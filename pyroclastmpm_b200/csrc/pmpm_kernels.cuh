@@ -242,8 +242,9 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
   int b[3] = {0, 0, 0};
   bool in_axes = true;
   bool binned = false, sorted = false;
-  unsigned key = 0;
+  unsigned key = 0, hu = 0;
   int dcell[3] = {0, 0, 0};
+  bool ref_cells = false;
   if (valid) {
 #pragma unroll
     for (int c = 0; c < D; c++) {
@@ -252,7 +253,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
       b[c] = (int)u[c];
       in_axes = in_axes && b[c] >= 0 && b[c] < g.n[c];
     }
-    const unsigned hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
+    hu = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
     hash_out[s] = hu;
     if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual) {
       int d[3] = {0, 0, 0};
@@ -265,7 +266,7 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
     } else {
       key = hu;
       binned = hu < (unsigned)g.ntotal;
-      mark_tiles<D, SF>(a, b, hu, binned, in_axes, epoch);
+      ref_cells = true;
     }
     // with a sentinel key (batched ensembles) a particle outside the grid is
     // sorted into its instance's extra last key, so instances keep their
@@ -278,6 +279,9 @@ __device__ __forceinline__ void hash_count_body(const StepArgs &a, int s, bool v
   }
   const int slot = warp_bin_slot(a.B.count, key, sorted);
   if (!valid) return;
+  // reference cells: all particles of a cell mark the same tiles, so the
+  // cell's first arrival marks them (a particle outside the grid marks its own)
+  if (ref_cells && (slot == 0 || !binned)) mark_tiles<D, SF>(a, b, hu, binned, in_axes, epoch);
   if (SF == PMPM_SHAPE_QUADRATIC && a.B.dual && binned && slot == 0) {
     // all particles of a dual cell share its tiles and brick: the cell's
     // first arrival marks them
