@@ -2755,7 +2755,7 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 // new positions for the next partition (counts, slots, keys, tile and brick
 // marks of epoch + 1), which then skips its binning pass.
 template <int D, int SF, bool FULL>
-__global__ void __launch_bounds__(256, FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 3 : 4)) k_g2p(StepArgs a, int do_stress, int store_L) {
+__global__ void __launch_bounds__(256, FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4)) k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
   if constexpr (SF == PMPM_SHAPE_QUADRATIC) {
