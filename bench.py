@@ -1,10 +1,13 @@
 """Benchmark of the USL MPM step: particle-steps/s on B200.
 
-Default workload: the 3D granular column collapse (1,331,712 particles,
-Drucker-Prager, quadratic B-splines, gravity, slip walls, 257x65x129 nodes,
-dt 1e-5), the configuration the headline metric is quoted on.  Synthetic,
-seeded particle set (numpy PCG64 seed 0).  The particle state (~154 MB) is
-larger than the 126 MB L2, so no flush is needed between timed steps.
+Default workload: the 3D granular bed dug by a rigid scoop (4,915,200
+particles, cubic B-splines, Drucker-Prager, half-cylinder shell contact with
+Coulomb friction, gravity, slip walls, 241x97x129 nodes, dt 8e-6), the
+largest configuration and the one the plain-step roofline target is stated
+on; the granular column (1,331,712 particles, quadratic), the batched
+ensemble and the forward + adjoint rollout follow as companion legs.
+Synthetic, seeded particle sets (numpy PCG64).  The particle state is larger
+than the 126 MB L2, so no flush is needed between timed steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -160,9 +163,9 @@ def cpu_reference_ensemble(steps, num):
 
 
 def cpu_reference(config, steps, warmup, sample_scale):
-    """The oracle (C restatement of the reference step, one thread) on a
-    bounded sample of the workload: the same grid, the particle region scaled
-    by sample_scale per axis."""
+    """The oracle (C restatement of the reference step, one thread) on the
+    workload, or with sample_scale < 1 on a bounded sample of it: the same
+    grid, the particle region scaled by sample_scale per axis."""
     import oracle
     from pyroclastmpm_b200 import scenes
 
@@ -177,40 +180,163 @@ def cpu_reference(config, steps, warmup, sample_scale):
     ref.solve(steps)
     dt = time.perf_counter() - t0
     n = len(scene["positions"])
+    what = "the full workload" if sample_scale == 1.0 else \
+        f"{config} particle region scaled {sample_scale:g} per axis, same grid"
     return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{n} particles ({config} particle region scaled {sample_scale:g} per axis, same grid), "
-                      f"{steps} steps after {warmup} warm-up, serial C oracle (FP32)",
+            "sample": f"{n} particles ({what}), {steps} steps after {warmup} warm-up, serial C oracle (FP32)",
             "seconds": dt}
-
-
-def run_reference(args, world, rank, pg):
-    line = None
-    if rank == 0:
-        cb = cpu_reference(args.config, args.steps, args.warmup, args.ref_sample_scale)
-        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "particle-steps/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1000.0 * cb["seconds"] / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_name(args.config), "sample": cb["sample"]},
-                "cpu_baseline": cb,
-                "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-    return line
 
 
 def workload_name(config):
     return {"column": "granular column collapse 3D, Drucker-Prager, quadratic B-spline, 1,331,712 particles, "
                       "257x65x129 nodes, gravity + slip walls, dt 1e-5",
             "discs": "two-disc elastic impact 2D, linear, 2,528 particles, 51x51 nodes, dt 1e-3",
-            "bed": "granular bed 3D with a translating, turning half-cylinder scoop (SDF contact, Coulomb 0.3), "
-                   "Drucker-Prager, cubic B-spline, 4,915,200 particles, 241x97x129 nodes, dt 8e-6",
+            "bed": "granular bed 3D dug by a translating, turning half-cylinder scoop (R 0.15, t 0.01, L 0.4; "
+                   "SDF contact, Coulomb 0.3), Drucker-Prager, cubic B-spline, 4,915,200 particles, "
+                   "241x97x129 nodes, gravity + slip walls, dt 8e-6",
             "calibration": "differentiable calibration rollout: 3D Drucker-Prager cube, 262,144 particles "
                            "(64^3 lattice, h 1/128), quadratic, per-particle E and friction angle, 500 steps of "
                            "dt 2e-5, checkpoints every 25, forward + adjoint",
             "ensemble": "batched ensemble of 256 2D instances (column collapses and disc impacts, 2k-64k particles, "
                         "64^2-512^2 grids, LE / NF / DP cycled, per-instance CFL 0.3 dt), quadratic B-spline"
             }[config]
+
+
+def static_config(config, world):
+    """The workload's description: the same for both arms (nothing measured)."""
+    from pyroclastmpm_b200 import scenes
+
+    if config in ("ensemble", "calibration"):
+        return {"workload": workload_name(config), "parallelism": f"replicas x{world}"}
+    scene = scene_for(config)
+    return {"workload": workload_name(config), "particles_per_gpu": int(len(scene["positions"])),
+            "grid_nodes": int(sc_nodes(scene)), "l2": "state larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}"}
+
+
+def run_reference(args, world, rank, pg):
+    """The reference arm: the reference step (the oracle's C restatement, one
+    thread as the reference's CPU build) on the same workload and particle
+    count as the B200 arm, for a few steps (about 50 s per step of the bed)."""
+    line = None
+    if rank == 0:
+        steps, warmup = max(1, min(args.steps, args.ref_steps)), max(0, min(args.warmup, args.ref_warmup))
+        cb = cpu_reference(args.config, steps, warmup, 1.0)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "particle-steps/s",
+                "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+                "ms_per_step": 1000.0 * cb["seconds"] / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": static_config(args.config, world),
+                "cpu_baseline": {k: v for k, v in cb.items() if k != "seconds"},
+                "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "note": f"timed {steps} steps after {warmup} warm-up (the --steps/--warmup asked for, capped at "
+                        f"--ref-steps {args.ref_steps} / --ref-warmup {args.ref_warmup}: one serial step of this "
+                        "workload takes tens of seconds)"}
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def rel_err_fields(gpu_get, ref, names):
+    out = {}
+    for name in names:
+        a = np.asarray(gpu_get(name), np.float64)
+        b = np.asarray(ref[name], np.float64)
+        out[name] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+    return out
+
+
+def plain_rel_err(config, local, steps=5, scale=None):
+    """Error of the GPU step against the FP64 oracle on a bounded sample of
+    the workload (same grid and physics, the particle region scaled), after
+    `steps` steps: max |a - b| / max |b| per field; the FP32 oracle's own
+    distance from FP64 beside it (what the reference's FP32 arithmetic
+    reaches).  Outside any timed region."""
+    import oracle
+    from pyroclastmpm_b200 import Simulation, scenes
+
+    scale = scale if scale is not None else {"bed": 0.35, "column": 0.5, "discs": 1.0}[config]
+    scene = scene_for(config, scale=scale)
+    kw = scenes.sim_kwargs(scene)
+    sim = Simulation(**kw, device=local)
+    sim.set_particles(scene["positions"], scene["velocities"]).initialize()
+    sim.solve(steps)
+    if sim.synchronize() != 0:
+        raise RuntimeError("device fault in the error check")
+    names = ("positions", "velocities", "stresses")
+    refs = {p: oracle.OracleSim(**kw, positions=scene["positions"], velocities=scene["velocities"],
+                                precision=p).initialize() for p in ("f64", "f32")}
+    for r in refs.values():
+        r.solve(steps)
+    err = rel_err_fields(sim.get, refs["f64"], names)
+    floor = rel_err_fields(lambda nm: refs["f32"][nm], refs["f64"], names)
+    sim.close()
+    return {"value": max(err.values()), "per_field": err, "fp32_oracle_vs_fp64": floor, "steps": steps,
+            "sample": f"{len(scene['positions'])} particles ({config} particle region scaled {scale:g} per axis, "
+                      f"same grid), {steps} steps, FP64 C oracle",
+            "measure": "max |gpu - fp64| / max |fp64| per field (positions, velocities, stresses)"}
+
+
+# FP32 flops per particle-step, counted from the algorithm (not the
+# instruction stream): per (particle, node) pair of P2G the weight and its
+# gradient (D - 1 + D (D - 1) products), mass and momentum (2 + 2D), the
+# stress force -V sigma grad N (2 D^2 + D); per pair of G2P the weight and
+# gradient again, the FLIP increment (3D), the PIC velocity (2D) and the
+# velocity gradient (2 D^2); per particle the spline pieces of both maps
+# (2 D WIN evaluations of N and dN), and the particle-local update (FLIP/PIC
+# blend, position, F = (I + L dt) F, det F, the return mapping) as a lump.
+SPLINE_FLOPS = {"linear": 3, "quadratic": 6, "cubic": 11}
+WIN = {"linear": 2, "quadratic": 3, "cubic": 4}
+LOCAL_FLOPS = {2: 100, 3: 330}
+NODE_FLOPS = 18  # per active node: p_nt = p + f dt, v = p / m, v_nt, conditions
+
+
+def flops_per_particle(dim, sf):
+    nsn = WIN[sf] ** dim
+    p2g_pair = (dim - 1) + dim * (dim - 1) + 2 + 2 * dim + 2 * dim * dim + dim
+    g2p_pair = (dim - 1) + dim * (dim - 1) + 3 * dim + 2 * dim + 2 * dim * dim
+    weights = dim * WIN[sf] * SPLINE_FLOPS[sf]
+    return {"p2g": nsn * p2g_pair + weights, "g2p_stress": nsn * g2p_pair + weights + LOCAL_FLOPS[dim],
+            "step": nsn * (p2g_pair + g2p_pair) + 2 * weights + LOCAL_FLOPS[dim]}
+
+
+def fp32_peak_tflops(sm_mhz):
+    """148 SMs x 128 FP32 lanes x 2 flops (FMA) per clock."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def ensemble_rel_err(local, picks=(0, 1, 2, 3, 4, 5), steps=20):
+    """Error of batched instances against the FP64 oracle: one instance of
+    each scene and material kind stepped in a batch of their own (the same
+    kernels) for `steps` steps; max over instances and fields, the FP32
+    oracle's own distance beside it."""
+    import oracle
+    from pyroclastmpm_b200 import Batch, scenes
+
+    insts = scenes.ensemble()
+    sel = [insts[i] for i in picks]
+    b = Batch(sel, device=local).initialize()
+    b.solve(steps)
+    if b.synchronize() != 0:
+        raise RuntimeError("device fault in the error check")
+    names = ("positions", "velocities", "stresses")
+    err, floor = {}, {}
+    for k, sc in enumerate(sel):
+        kw = scenes.sim_kwargs(sc)
+        refs = {p: oracle.OracleSim(**kw, positions=sc["positions"], velocities=sc["velocities"],
+                                    precision=p).initialize() for p in ("f64", "f32")}
+        for r in refs.values():
+            r.solve(steps)
+        e = rel_err_fields(lambda nm: b.get(k, nm), refs["f64"], names)
+        f = rel_err_fields(lambda nm: refs["f32"][nm], refs["f64"], names)
+        for nm in names:
+            err[nm] = max(err.get(nm, 0.0), e[nm])
+            floor[nm] = max(floor.get(nm, 0.0), f[nm])
+    b.close()
+    return {"value": max(err.values()), "per_field": err, "fp32_oracle_vs_fp64": floor, "steps": steps,
+            "sample": f"ensemble instances {list(picks)} (LE / NF / DP, columns and discs) in one batch, "
+                      f"{steps} steps, FP64 C oracle per instance",
+            "measure": "max over instances of max |gpu - fp64| / max |fp64| per field"}
 
 
 def run_ensemble(args, world, rank, local, pg, emit=True):
@@ -308,6 +434,7 @@ def run_ensemble(args, world, rank, local, pg, emit=True):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_ensemble(1, 16)
         cpu.pop("seconds", None)
+    err = ensemble_rel_err(local) if rank == 0 and args.error_check else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
@@ -329,12 +456,65 @@ def run_ensemble(args, world, rank, local, pg, emit=True):
                     "d2h_bytes_per_step": nbytes // 2,
                     "note": "per step: every instance's positions + velocities uploaded from pinned host memory, "
                             "one batched step, read back (host wall clock around synchronised calls)"},
+            "rel_err_vs_fp64": err,
             "cpu_baseline": cpu,
         }
         if emit:
             print(json.dumps(line), flush=True)
     b.close()
     return line if rank == 0 else None
+
+
+def calibration_rel_err(local, steps=50, every=10, eps=1e-4):
+    """Errors of the differentiable rollout on the 4,096-particle copy of the
+    calibration cube (16^3 lattice): final positions of the forward rollout
+    against the FP64 oracle, and the adjoint's directional derivatives of
+    the loss w . x_final (fixed random w) along random perturbations of the
+    per-particle E and friction angle against FP64 central differences."""
+    import oracle
+    from pyroclastmpm_b200 import Simulation, scenes
+
+    scene, E, phi, _ = scenes.calibration_cube(n_side=16, cell_size=1.0 / 32, domain=0.5, dt=1e-4)
+    n = len(scene["positions"])
+    kw = scenes.sim_kwargs(scene)
+    sim = Simulation(**kw, device=local)
+    sim.set_particles(scene["positions"], scene["velocities"]).initialize()
+    sim.set("youngs_modulus", E)
+    sim.set("friction_angle", phi)
+    sim.rollout_forward(steps, every)
+    x_gpu = sim.get("positions")
+    w = np.random.default_rng(7).normal(0, 1, (n, 3))
+    gE, gphi, _gx, _gv = sim.rollout_backward(w)
+    if sim.synchronize() != 0:
+        raise RuntimeError("device fault in the error check")
+    sim.close()
+
+    def final(Ep, phip, precision="f64"):
+        o = oracle.OracleSim(**kw, positions=scene["positions"], velocities=scene["velocities"],
+                             youngs_modulus=Ep, friction_angle=phip, precision=precision).initialize()
+        o.solve(steps)
+        return np.array(o["positions"], np.float64)
+
+    x64 = final(E, phi)
+    x32 = final(E, phi, "f32")
+    fwd = float(np.abs(x_gpu - x64).max() / np.abs(x64).max())
+    fwd_floor = float(np.abs(x32 - x64).max() / np.abs(x64).max())
+    rng = np.random.default_rng(0)
+    dE = E * rng.normal(0, 1, n)
+    dphi = rng.normal(0, 1, n)
+    grads = {}
+    for name, adj, run in (("E", float(np.dot(gE.astype(np.float64), dE)),
+                            lambda e: final(E + e * dE, phi)),
+                           ("friction_angle", float(np.dot(gphi.astype(np.float64), dphi)),
+                            lambda e: final(E, phi + e * dphi))):
+        fd = (float((w * run(eps)).sum()) - float((w * run(-eps)).sum())) / (2 * eps)
+        grads[name] = abs(adj - fd) / max(abs(fd), 1e-30)
+    return {"value": max([fwd] + list(grads.values())), "forward_positions": fwd,
+            "fp32_oracle_forward_positions": fwd_floor, "gradient_directional": grads,
+            "sample": f"4,096-particle copy of the cube (16^3 lattice, h 1/32, dt 1e-4), {steps} steps, "
+                      f"checkpoints every {every}; FP64 C oracle, central differences with step {eps:g}",
+            "measure": "forward: max |gpu - fp64| / max |fp64| of final positions; gradients: |adjoint - FD| / "
+                       "|FD| of directional derivatives"}
 
 
 def run_calibration(args, world, rank, local, pg, emit=True):
@@ -421,9 +601,10 @@ def run_calibration(args, world, rank, local, pg, emit=True):
     achieved = adj_bytes / (ms_adj_step / 1000.0) / 1e9
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference("column", 1, 0, 0.3)
+        cpu = cpu_reference("column", 3, 1, 0.3)
         cpu.pop("seconds", None)
         cpu["sample"] += " (forward only: the reference has no adjoint)"
+    err = calibration_rel_err(local) if rank == 0 and args.error_check else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": nsteps,
@@ -452,6 +633,7 @@ def run_calibration(args, world, rank, local, pg, emit=True):
                     "d2h_bytes_per_step": int((gE.nbytes + gphi.nbytes + 4 * 3 * n) // nsteps),
                     "note": "rollout through the C ABI: loss gradient uploaded from host, parameter gradients "
                             "and final positions read back; per-step share of those bytes"},
+            "rel_err_vs_fp64": err,
             "cpu_baseline": cpu,
         }
         if emit:
@@ -467,46 +649,15 @@ def sc_nodes(sc):
     return n
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="column", choices=["column", "discs", "bed", "ensemble", "calibration"])
-    ap.add_argument("--rollout-steps", type=int, default=500)
-    ap.add_argument("--resort-interval", type=int, default=32)
-    ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--cpu-steps", type=int, default=1)
-    ap.add_argument("--ref-sample-scale", type=float, default=0.45)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--p2g-kernel", default="auto", choices=["auto", "dual", "cells"],
-                    help="3D quadratic P2G kernel: autotuned (default) or fixed (fixed for profiling runs, "
-                         "whose serialised launches make the autotuner's timings meaningless)")
-    ap.add_argument("--no-companions", dest="companions", action="store_false",
-                    help="skip the batched-ensemble and calibration legs in the default line")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-
-    world, rank, local, pg = dist_setup()
-    if args.impl == "reference":
-        run_reference(args, world, rank, pg)
-        if pg is not None:
-            pg.destroy_process_group()
-        return
-
-    if args.config in ("ensemble", "calibration"):
-        (run_ensemble if args.config == "ensemble" else run_calibration)(args, world, rank, local, pg)
-        if pg is not None:
-            pg.destroy_process_group()
-        return
-
+def run_plain(args, config, world, rank, local, pg, steps, with_cpu, with_err=True):
+    """One simulation per GPU: K device-timed steps, phase split, rooflines,
+    end to end through the C ABI, error against FP64, CPU baseline."""
     import torch
 
     from pyroclastmpm_b200 import Simulation, scenes
 
     torch.cuda.set_device(local)
-    scene = scene_for(args.config)
+    scene = scene_for(config)
     kw = scenes.sim_kwargs(scene)
     sim = Simulation(**kw, device=local, resort_interval=args.resort_interval)
     sim.set_particles(scene["positions"], scene["velocities"])
@@ -517,6 +668,8 @@ def main():
         p2g_variant = {"dual": 1, "cells": 0}[args.p2g_kernel]
         sim.set_p2g_kernel(p2g_variant)
     n = sim.n
+    dim = scene["dim"]
+    sf = scene["shape_function"]
     stream = torch.cuda.ExternalStream(sim.stream, device=local)
 
     for _ in range(args.warmup):
@@ -535,7 +688,7 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    sim.solve(args.steps)
+    sim.solve(steps)
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
@@ -547,7 +700,7 @@ def main():
     status = sim.synchronize()
     if status != 0:
         raise RuntimeError(f"device fault in the timed region: {status}")
-    value = world * n * args.steps / (ms_max / 1000.0)
+    value = world * n * steps / (ms_max / 1000.0)
 
     # ---- per-phase times (CUDA events inside the library, same stream) ----
     phases = np.zeros(3)
@@ -557,7 +710,6 @@ def main():
         phases += np.array(p)
     phases /= nprof
     active = sim.active_nodes()
-    dim = scene["dim"]
     peak, peak_kind = load_peak()
     step_bytes = STEP_BYTES[("3d", "dp")] if dim == 3 else STEP_BYTES[("2d", "le")]
     grid_bytes = 16 * dim * active
@@ -579,61 +731,147 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(args.config, {}).get(dom_name)
+            traffic = json.load(open(tpath)).get(config, {}).get(dom_name)
         except Exception:
             traffic = None
-    step_ms = ms_max / args.steps
+    step_ms = ms_max / steps
     step_achieved = (step_bytes * n + grid_bytes) / (step_ms / 1000.0) / 1e9
+    # FP32 flops against the SIMT peak at the sampled clock
+    fl = flops_per_particle(dim, sf)
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    fpeak = fp32_peak_tflops(sm_mhz)
+    dom_flops = n * fl.get(dom_name, 0) + (active * NODE_FLOPS if dom_name == "p2g" else 0)
+    dom_tflops = dom_flops / (phases[dom] / 1000.0) / 1e12
+    step_tflops = (n * fl["step"] + active * NODE_FLOPS) / (step_ms / 1000.0) / 1e12
 
-    # ---- end to end through the C ABI with host buffers ----
+    # ---- end to end through the C ABI with host buffers (host wall clock) ----
     pin_x = torch.empty((n, dim), dtype=torch.float32, pin_memory=True)
     pin_v = torch.empty((n, dim), dtype=torch.float32, pin_memory=True)
     pin_x.copy_(torch.from_numpy(sim.get("positions")))
     pin_v.copy_(torch.from_numpy(sim.get("velocities")))
     nbytes = n * dim * 4
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+
     def e2e_step():
         sim.set_ptr("positions", pin_x.data_ptr(), nbytes)
         sim.set_ptr("velocities", pin_v.data_ptr(), nbytes)
         sim.solve(1)
-        sim.get_ptr("positions", pin_x.data_ptr(), nbytes)
+        sim.get_ptr("positions", pin_x.data_ptr(), nbytes)   # returns after the copy: synchronous
         sim.get_ptr("velocities", pin_v.data_ptr(), nbytes)
 
     for _ in range(2):  # untimed: first-use staging buffers and transfers
         e2e_step()
     torch.cuda.synchronize()
-    e0.record(stream)
+    barrier(pg)
+    t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        sim.set_ptr("positions", pin_x.data_ptr(), nbytes)
-        sim.set_ptr("velocities", pin_v.data_ptr(), nbytes)
-        sim.solve(1)
-        sim.get_ptr("positions", pin_x.data_ptr(), nbytes)
-        sim.get_ptr("velocities", pin_v.data_ptr(), nbytes)
-    e1.record(stream)
-    e1.synchronize()
-    e2e_ms = allreduce_max(pg, e0.elapsed_time(e1) / args.e2e_steps)
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = allreduce_max(pg, 1000.0 * (time.perf_counter() - t0) / args.e2e_steps)
     e2e_value = world * n / (e2e_ms / 1000.0)
+    sim.close()
 
+    err = None
+    if with_err and rank == 0:
+        err = plain_rel_err(config, local)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference(args.config, args.cpu_steps, 0, 1.0)
+    if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference(config, args.cpu_steps, 1, args.cpu_sample_scale.get(config, 1.0))
         cpu.pop("seconds", None)
 
-    # the metric's other two legs, measured by their own configurations
-    companions = None
-    if args.companions and args.config == "column":
-        sim.close()
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, numpy PCG64)",
+        "config": static_config(config, world),
+        "tuned": {"p2g_kernel": p2g_kernel_name(kw, p2g_variant), "resort_interval": args.resort_interval},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                     "traffic": traffic, "algorithmic_bytes_per_launch": algo[dom_name],
+                     "ms_per_launch": float(phases[dom])},
+        "flop_roofline": {"bound": "fp32", "kernel": dom_name, "achieved": dom_tflops, "peak": fpeak,
+                          "unit": "TFLOP/s", "frac": dom_tflops / fpeak, "flops_per_launch": dom_flops,
+                          "peak_source": f"148 SMs x 128 FP32 lanes x 2 flops x sampled SM clock {sm_mhz:g} MHz"},
+        "step_roofline": {"achieved": step_achieved, "peak": peak, "unit": "GB/s",
+                          "frac": step_achieved / peak, "bytes_per_particle_step": step_bytes,
+                          "grid_bytes_per_step": grid_bytes, "active_nodes": active,
+                          "fp32_tflops": step_tflops, "fp32_frac": step_tflops / fpeak,
+                          "flops_per_particle_step": fl["step"]},
+        "phases_ms": dict(zip(phase_names, [float(x) for x in phases])),
+        "clocks": clocks, "gpu_launches": int(launches),
+        "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 2 * nbytes,
+                "d2h_bytes_per_step": 2 * nbytes,
+                "note": "per step: positions + velocities uploaded from pinned host memory through "
+                        "pmpm_set_field, one step, both read back through pmpm_get_field; host wall clock"},
+        "rel_err_vs_fp64": err,
+        "cpu_baseline": cpu,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="bed", choices=["column", "discs", "bed", "ensemble", "calibration"])
+    ap.add_argument("--rollout-steps", type=int, default=500)
+    ap.add_argument("--resort-interval", type=int, default=32)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--ref-steps", type=int, default=2,
+                    help="most steps the reference arm times (one serial step of the bed takes ~50 s)")
+    ap.add_argument("--ref-warmup", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-error-check", dest="error_check", action="store_false",
+                    help="skip the FP64 error checks (profiling runs)")
+    ap.add_argument("--p2g-kernel", default="auto", choices=["auto", "dual", "cells"],
+                    help="3D quadratic P2G kernel: autotuned (default) or fixed (fixed for profiling runs, "
+                         "whose serialised launches make the autotuner's timings meaningless)")
+    ap.add_argument("--no-companions", dest="companions", action="store_false",
+                    help="skip the column, batched-ensemble and calibration legs in the default line")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    # cpu_baseline samples: the same grid, the particle region scaled per axis
+    # so that one warm-up step and --cpu-steps steps take about half a minute
+    args.cpu_sample_scale = {"bed": 0.5, "column": 0.75, "discs": 1.0}
+
+    world, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    if args.config in ("ensemble", "calibration"):
+        (run_ensemble if args.config == "ensemble" else run_calibration)(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    line = run_plain(args, args.config, world, rank, local, pg, args.steps, with_cpu=True,
+                     with_err=args.error_check)
+    # the metric's other legs, measured by their own configurations
+    if args.companions and args.config == "bed":
         sub = argparse.Namespace(**vars(args))
         sub.no_cpu_baseline = True
+        col = run_plain(sub, "column", world, rank, local, pg, args.steps, with_cpu=False,
+                        with_err=args.error_check)
         sub.steps = 10
         cal = run_calibration(sub, world, rank, local, pg, emit=False)
         ens = run_ensemble(sub, world, rank, local, pg, emit=False)
         if rank == 0:
-            companions = {
+            line["companions"] = {
+                "column": {"value": col["value"], "unit": "particle-steps/s", "workload": col["config"]["workload"],
+                           "ms_per_step": col["ms_per_step"], "phases_ms": col["phases_ms"],
+                           "roofline": col["roofline"], "flop_roofline": col["flop_roofline"],
+                           "step_roofline": col["step_roofline"], "e2e": col["e2e"],
+                           "rel_err_vs_fp64": col["rel_err_vs_fp64"], "tuned": col["tuned"]},
                 "batched": {"value": ens["value"], "unit": "particle-steps/s", "workload": ens["config"]["workload"],
                             "ms_per_step": ens["ms_per_step"],
-                            "over_one_sim_per_launch": ens["config"]["batched_over_one_sim_per_launch"]},
+                            "over_one_sim_per_launch": ens["config"]["batched_over_one_sim_per_launch"],
+                            "rel_err_vs_fp64": ens.get("rel_err_vs_fp64")},
                 "fwd_adjoint": {"value": cal["value"], "unit": "particle-steps/s",
                                 "workload": cal["config"]["workload"], "ms_per_step": cal["ms_per_step"],
                                 "plain_forward_ms_per_step": cal["config"]["plain_forward_ms_per_step"],
@@ -642,37 +880,11 @@ def main():
                                 "over_plain_forward": cal["config"]["fwd_plus_adjoint_over_plain_forward"],
                                 "checkpoints_only_over_plain_forward":
                                     cal["config"]["checkpoints_only"]["fwd_plus_adjoint_over_plain_forward"],
+                                "rel_err_vs_fp64": cal.get("rel_err_vs_fp64"),
                                 "clocks": cal.get("clocks")},
             }
-
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, numpy PCG64)",
-            "config": {"workload": workload_name(args.config), "particles_per_gpu": n, "grid_nodes": sim.num_nodes,
-                       "active_nodes": active, "resort_interval": args.resort_interval,
-                       "p2g_kernel": p2g_kernel_name(kw, p2g_variant),
-                       "l2": "state larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": traffic, "algorithmic_bytes_per_launch": algo[dom_name],
-                         "ms_per_launch": float(phases[dom])},
-            "step_roofline": {"achieved": step_achieved, "peak": peak, "unit": "GB/s",
-                              "frac": step_achieved / peak,
-                              "bytes_per_particle_step": step_bytes, "grid_bytes_per_step": grid_bytes},
-            "phases_ms": dict(zip(phase_names, [float(x) for x in phases])),
-            "clocks": clocks, "gpu_launches": int(launches),
-            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 2 * nbytes,
-                    "d2h_bytes_per_step": 2 * nbytes,
-                    "note": "per step: positions + velocities uploaded from pinned host memory, one step, "
-                            "positions + velocities read back"},
-            "cpu_baseline": cpu,
-        }
-        if companions:
-            line["companions"] = companions
         print(json.dumps(line), flush=True)
-    sim.close()
     if pg is not None:
         pg.destroy_process_group()
 

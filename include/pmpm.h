@@ -386,6 +386,23 @@ int pmpm_profile_step(pmpm_sim *sim, float ms[3], int *launches);
 /* Number of kernels the handle has launched since it was created. */
 int pmpm_launch_count(const pmpm_sim *sim, long long *count);
 
+/* Bound on the key scan's look-back wait (no reference counterpart: the
+ * reference sorts with thrust and calls exit() on a CUDA error,
+ * include/pyroclastmpm/common/types_common.h:170-187).  A CTA of the
+ * one-launch scan polls its predecessors' published sums at most `spins`
+ * times (default 4194304); past that it records PMPM_ERR_TIMEOUT, and the
+ * kernels that index particles through the scan's offsets skip the step's
+ * P2G instead of reading through an invalid prefix.  After PMPM_ERR_TIMEOUT
+ * the particle state is invalid: set it again.  0 gives up at the first
+ * poll that finds a predecessor not yet published. */
+int pmpm_set_wait_limit(pmpm_sim *sim, long long spins);
+
+/* The tag (1 .. 2^30 - 2) that the key scan's launch number `launch` stamps
+ * on its published sums; consecutive launches alternate its parity, which
+ * picks their ticket counters, across the counter's wrap as well.
+ * Diagnostic, no reference counterpart. */
+int pmpm_scan_tag(unsigned launch, unsigned *tag);
+
 /* Number of grid nodes with mass above the cutoff after the last P2G
  * (the nodes the step actually updates). */
 int pmpm_active_nodes(pmpm_sim *sim, int *count);
@@ -425,11 +442,18 @@ int pmpm_material_point_update(const pmpm_material *mat, int dim, int n, float d
  * live in one fixed device array inside the library: at most 131072
  * particles and 131072 cells (larger inputs return
  * PMPM_ERR_INVALID_ARGUMENT).  The first call on a device looks up that
- * array's address; make it before any stream capture.  Calls share the array,
- * so calls that overlap on the GPU race: serialise them.  Waits for `stream`
- * (cudaStream_t, may be NULL) before returning.  Returns
- * PMPM_ERR_OUT_OF_DOMAIN when a particle lies outside the grid (the outputs
- * then cover the particles inside it). */
+ * array's address and, with CUDA's lazy module loading, is when the driver
+ * loads this code and places the array; make that first call (a warm-up
+ * call will do) before any stream capture and outside any allocation
+ * callback.  Calls share the array, so calls that overlap on the GPU race:
+ * serialise them.  Waits for `stream` (cudaStream_t, may be NULL) before
+ * returning.  Returns PMPM_ERR_OUT_OF_DOMAIN when a particle's cell lies
+ * outside the grid on any axis or a coordinate is not finite; the outputs
+ * still follow the reference's flat hash (a particle whose flat index stays
+ * inside the grid is binned where it points, one past it is left out).
+ * Returns PMPM_ERR_CELL_OVERFLOW when one cell holds more than 2048
+ * particles: that cell's entries of sorted_index are then not in ascending
+ * order (the other outputs are complete). */
 int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const int *num_cells,
                            const float *positions, int num_particles, unsigned *hash_unsorted,
                            int *sorted_index, int *cell_start, int *cell_end, void *stream);
@@ -525,6 +549,8 @@ int pmpm_batch_synchronize(pmpm_batch *b);
 /* One step with CUDA-event times: ms[0] partition, ms[1] P2G, ms[2] G2P. */
 int pmpm_batch_profile_step(pmpm_batch *b, float *ms, int *launches);
 int pmpm_batch_launch_count(const pmpm_batch *b, long long *count);
+/* pmpm_set_wait_limit for the batch's key scan. */
+int pmpm_batch_set_wait_limit(pmpm_batch *b, long long spins);
 
 #ifdef __cplusplus
 }

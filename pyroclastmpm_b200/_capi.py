@@ -87,12 +87,14 @@ EXPORTS = [
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
     "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
     "pmpm_material_modified_cam_clay", "pmpm_material_drucker_prager_cap", "pmpm_set_p2g_kernel",
+    "pmpm_set_wait_limit", "pmpm_scan_tag",
 ]
 
 EXPORTS += [
     "pmpm_batch_create", "pmpm_batch_destroy", "pmpm_batch_initialize", "pmpm_batch_solve",
     "pmpm_batch_num_instances", "pmpm_batch_num_particles", "pmpm_batch_get_field", "pmpm_batch_set_field",
     "pmpm_batch_synchronize", "pmpm_batch_profile_step", "pmpm_batch_launch_count",
+    "pmpm_batch_set_wait_limit",
 ]
 
 RIGID_MODES = {"static": 0, "loop_rotate": 1}
@@ -175,10 +177,20 @@ def lib():
     L.pmpm_profile_step.argtypes = [vp, fp, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_active_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.pmpm_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
+    L.pmpm_batch_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
+    L.pmpm_scan_tag.argtypes = [ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)]
     L.pmpm_partition_noalloc.argtypes = [i, fp, f, ctypes.POINTER(ctypes.c_int), vp, i, vp, vp, vp, vp, vp]
     L.pmpm_material_point_update.argtypes = [ctypes.POINTER(Material), i, i, f, vp, vp, vp, vp, vp, vp, vp, i, i]
     _lib = L
     return L
+
+
+def scan_tag(launch):
+    """The key scan's look-back tag for launch number `launch` (diagnostic)."""
+    t = ctypes.c_uint()
+    check(lib().pmpm_scan_tag(ctypes.c_uint(launch & 0xffffffff), ctypes.byref(t)), "pmpm_scan_tag")
+    return t.value
 
 
 def check(status, what):
@@ -520,6 +532,10 @@ class Simulation:
         check(lib().pmpm_launch_count(self._h, ctypes.byref(c)), "pmpm_launch_count")
         return c.value
 
+    def set_wait_limit(self, spins):
+        """Bound on the key scan's look-back polls (default 2**22)."""
+        check(lib().pmpm_set_wait_limit(self._h, int(spins)), "pmpm_set_wait_limit")
+
     def autotune(self, steps=5):
         """Time each P2G kernel this configuration has on `steps` steps, keep
         the fastest, restore the state; returns the chosen variant."""
@@ -696,3 +712,6 @@ class Batch:
         c = ctypes.c_longlong()
         check(lib().pmpm_batch_launch_count(self._h, ctypes.byref(c)), "pmpm_batch_launch_count")
         return c.value
+
+    def set_wait_limit(self, spins):
+        check(lib().pmpm_batch_set_wait_limit(self._h, int(spins)), "pmpm_batch_set_wait_limit")

@@ -72,7 +72,10 @@ struct ScanState {
   unsigned long long *status = nullptr;
   int *ticket = nullptr;
   unsigned launches = 0;
+  long long spin_limit = 1ll << 22;  // look-back polls before a CTA gives up
 };
+
+unsigned scan_tag(unsigned launch) { return launch % 0x3ffffffeu + 1u; }
 
 int alloc_scan(ScanState &sc, int nblocks) {
   PMPM_TRY(dalloc(&sc.status, (size_t)nblocks));
@@ -90,10 +93,13 @@ void free_scan(ScanState &sc) {
 // count -> offset (exclusive), counts cleared, scalars reset; one launch
 int launch_scan(ScanState &sc, int *count, int nkeys, int *offset, int *scalars, int *fault, int nblocks,
                 cudaStream_t st) {
-  const unsigned tag = sc.launches % 0x3fffffffu + 1u;  // never 0: zeroed status words carry no tag
+  // 30-bit tag, never 0 (zeroed status words carry no tag); the modulus is
+  // even so that consecutive launches always alternate the tag's parity,
+  // which selects the ticket counter (each launch resets the other one)
+  const unsigned tag = scan_tag(sc.launches);
   sc.launches += 1;
   k_scan_onepass<<<nblocks, kScanThreads, 0, st>>>(count, nkeys, offset, sc.status, sc.ticket, scalars, fault, tag,
-                                                   nblocks);
+                                                   nblocks, sc.spin_limit);
   PMPM_LAUNCHED();
   return PMPM_OK;
 }
@@ -1897,6 +1903,18 @@ int pmpm_profile_step(pmpm_sim *s, float ms[3], int *launches) {
   return PMPM_DISPATCH(s, profile_step, s, ms, launches);
 }
 
+int pmpm_set_wait_limit(pmpm_sim *s, long long spins) {
+  if (!s || spins < 0) return PMPM_ERR_INVALID_ARGUMENT;
+  s->scan.spin_limit = spins;
+  return PMPM_OK;
+}
+
+int pmpm_scan_tag(unsigned launch, unsigned *tag) {
+  if (!tag) return PMPM_ERR_INVALID_ARGUMENT;
+  *tag = scan_tag(launch);
+  return PMPM_OK;
+}
+
 int pmpm_launch_count(const pmpm_sim *s, long long *count) {
   if (!s || !count) return PMPM_ERR_INVALID_ARGUMENT;
   *count = s->launches;
@@ -1939,10 +1957,10 @@ int pmpm_synchronize(pmpm_sim *s) {
   PMPM_CUDA(cudaMemcpyAsync(&f, s->fault, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   PMPM_CUDA(cudaStreamSynchronize(s->stream));
   if (f) PMPM_CUDA(cudaMemset(s->fault, 0, sizeof(int)));
+  if (f & kFaultWaitTimeout) return PMPM_ERR_TIMEOUT;  // the step's P2G did not run: reported first
   if (f & kFaultNonFinite) return PMPM_ERR_NONFINITE;
   if (f & kFaultOutOfDomain) return PMPM_ERR_OUT_OF_DOMAIN;
   if (f & kFaultCellOverflow) return PMPM_ERR_CELL_OVERFLOW;
-  if (f & kFaultWaitTimeout) return PMPM_ERR_TIMEOUT;
   return PMPM_OK;
 }
 
@@ -2600,10 +2618,16 @@ int pmpm_batch_synchronize(pmpm_batch *b) {
   PMPM_CUDA(cudaMemcpyAsync(&f, b->fault, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   PMPM_CUDA(cudaStreamSynchronize(b->stream));
   if (f) PMPM_CUDA(cudaMemset(b->fault, 0, sizeof(int)));
+  if (f & kFaultWaitTimeout) return PMPM_ERR_TIMEOUT;  // the step's P2G did not run: reported first
   if (f & kFaultNonFinite) return PMPM_ERR_NONFINITE;
   if (f & kFaultOutOfDomain) return PMPM_ERR_OUT_OF_DOMAIN;
   if (f & kFaultCellOverflow) return PMPM_ERR_CELL_OVERFLOW;
-  if (f & kFaultWaitTimeout) return PMPM_ERR_TIMEOUT;
+  return PMPM_OK;
+}
+
+int pmpm_batch_set_wait_limit(pmpm_batch *b, long long spins) {
+  if (!b || spins < 0) return PMPM_ERR_INVALID_ARGUMENT;
+  b->scan.spin_limit = spins;
   return PMPM_OK;
 }
 

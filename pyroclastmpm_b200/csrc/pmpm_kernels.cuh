@@ -367,7 +367,7 @@ constexpr unsigned long long kScanAggregate = 1ull << 32, kScanInclusive = 2ull 
 __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n, int *offset,
                                                                 unsigned long long *status, int *ticket,
                                                                 int *scalars, int *fault, unsigned tag,
-                                                                int nblocks) {
+                                                                int nblocks, long long spin_limit) {
   __shared__ int sw[33];
   __shared__ int sh_block, sh_prefix;
   if (threadIdx.x == 0) sh_block = atomicAdd(&ticket[tag & 1u], 1);
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n
         const int first = incl ? __ffs(incl) - 1 : 31;  // lanes 0..first are needed
         const unsigned need = first == 31 ? 0xffffffffu : ((1u << (first + 1)) - 1u);
         if ((rdy & need) != need) {
-          if (++spins > (1ll << 22)) {
+          if (++spins > spin_limit) {
             if (lane == 0) atomicOr(fault, kFaultWaitTimeout);
             break;
           }
@@ -452,7 +452,15 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_onepass(int *count, int n
   }
 }
 
+// True when this step's key scan gave up a bounded wait: its offsets are
+// then not a valid prefix, so every kernel that indexes particles through
+// them returns without work (the step reports PMPM_ERR_TIMEOUT).
+__device__ __forceinline__ bool binning_failed(const int *fault) {
+  return (*(volatile const int *)fault & kFaultWaitTimeout) != 0;
+}
+
 __global__ void __launch_bounds__(256) k_scatter(StepArgs a) {
+  if (binning_failed(a.fault)) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.P.n) return;
   const int slot = a.P.slot[s];
@@ -469,6 +477,7 @@ constexpr int kBigCell = 2048;
 
 // Orders each cell's particles by id; cells above kSmallCell go to k_sort_big.
 __global__ void __launch_bounds__(256) k_sort_cells(StepArgs a) {
+  if (binning_failed(a.fault)) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.B.nkeys) return;
   const int lo = a.B.offset[c], hi = a.B.offset[c + 1];
@@ -501,6 +510,7 @@ __global__ void __launch_bounds__(256) k_sort_cells(StepArgs a) {
 // Bitonic sort in shared memory of each large cell (up to kBigCell entries).
 __global__ void __launch_bounds__(1024) k_sort_big(StepArgs a) {
   __shared__ int key[kBigCell], val[kBigCell];
+  if (binning_failed(a.fault)) return;
   const int nbig = a.B.scalars[2];
   for (int bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
     const int c = a.B.big_cells[bi];
@@ -718,6 +728,7 @@ __device__ __forceinline__ void p2g_gather_body(const StepArgs &a, int tile, int
 
 template <int D, int SF>
 __global__ void __launch_bounds__(TileDims<D>::N) k_p2g_gather(StepArgs a, int apply_bcs, int *node_epoch) {
+  if (binning_failed(a.fault)) return;
   p2g_gather_body<D, SF>(a, blockIdx.x, apply_bcs, node_epoch);
 }
 
@@ -765,7 +776,7 @@ __global__ void __launch_bounds__(TileDims<D>::N) k_rigid_nodes(StepArgs a, int 
   const DevGrid &g = a.g;
   const DevParticles &P = a.P;
   const int tile = blockIdx.x;
-  if (a.N.tile_epoch[tile] != a.epoch) return;
+  if (a.N.tile_epoch[tile] != a.epoch || binning_failed(a.fault)) return;
   const int tx = tile % g.tdim[0], ty = (tile / g.tdim[0]) % g.tdim[1], tz = tile / (g.tdim[0] * g.tdim[1]);
   const int lx = threadIdx.x % T::X, ly = (threadIdx.x / T::X) % T::Y, lz = threadIdx.x / (T::X * T::Y);
   const int nc[3] = {tx * T::X + lx, ty * T::Y + ly, D == 3 ? tz * T::Z + lz : 0};
@@ -1332,6 +1343,7 @@ __device__ __forceinline__ void p2g_tile_body(const StepArgs &a, int tile, int a
 
 template <int D, int SF>
 __global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) k_p2g_tile(StepArgs a, int apply_bcs, int *node_epoch) {
+  if (binning_failed(a.fault)) return;
   p2g_tile_body<D, SF>(a, blockIdx.x, apply_bcs, node_epoch);
 }
 
@@ -1789,6 +1801,7 @@ template <int SF, bool PLANAR>
 __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
+  if (binning_failed(a.fault)) return;
   for (int unit = next_tile(a, &cur); unit >= 0; unit = next_tile(a, &cur))
     sweep3_tile<SF, PLANAR>(a, apply_bcs, node_epoch, unit);
 }
@@ -2175,6 +2188,7 @@ template <bool PLANAR>
 __global__ void __launch_bounds__(Dual3::NT, 1) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
+  if (binning_failed(a.fault)) return;
   for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
     dual3_tile<PLANAR>(a, apply_bcs, node_epoch, tile);
 }
@@ -2211,7 +2225,7 @@ __global__ void __launch_bounds__(Cells3::NT, 2) k_p2g_cells3(StepArgs a) {
   using W = Cells3;
   const DevGrid &g = a.g;
   const int brick = blockIdx.x;
-  if (a.B.brick_epoch[brick] != a.epoch) return;
+  if (a.B.brick_epoch[brick] != a.epoch || binning_failed(a.fault)) return;
   extern __shared__ __align__(16) float csm[];
   float *box = csm;  // [7][NBOX]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -2915,6 +2929,7 @@ __global__ void __launch_bounds__(TileDims<D>::N, D == 2 ? 3 : 1) kb_p2g(const S
   __shared__ StepArgs sa;
   __shared__ int cur;
   if (blockIdx.x == 0 && threadIdx.x == 0) tile_queue[2 + (par ^ 1)] = 0;
+  if (binning_failed(views[0].fault)) return;
   const int count = min(tile_queue[epoch & 1], ntiles);
   for (;;) {
     if (threadIdx.x == 0) cur = atomicAdd(&tile_queue[2 + par], 1);

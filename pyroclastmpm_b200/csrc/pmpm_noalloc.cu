@@ -47,7 +47,10 @@ constexpr int kScratchInts = kOffFlags + 4;
 
 static __device__ __align__(256) int g_partition_scratch[kScratchInts];
 
-// Device address of g_partition_scratch per device, looked up once.
+// Device address of g_partition_scratch per device, looked up once.  Two
+// host threads making a first call on the same device at once may both
+// look it up; they store the same address, so the unsynchronised write is
+// harmless.
 int *g_scratch_ptr[64] = {nullptr};
 
 struct NaGrid {
@@ -84,20 +87,29 @@ __device__ __forceinline__ int na_block_scan(int v, int *sw, int &total) {
   return r;
 }
 
-// hash = NODE_MEM_INDEX((int)((x - origin) * inv_h)) and per-cell counts
+// hash = NODE_MEM_INDEX((int)((x - origin) * inv_h)) and per-cell counts.
+// Binning follows the reference's flat index (a particle past a face whose
+// flat index stays inside the grid lands in the cell it points at); the
+// out-of-domain flag is raised per axis and for non-finite coordinates.
 __global__ void na_hash_count(NaGrid g, const float *x, int n, unsigned *hash_out, int *scratch) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int b[3] = {0, 0, 0};
-  for (int c = 0; c < g.dim; c++) b[c] = (int)__fmul_rn(__fsub_rn(x[(size_t)i * g.dim + c], g.origin[c]), g.inv_h);
+  bool inside = true;
+  for (int c = 0; c < g.dim; c++) {
+    const float xc = x[(size_t)i * g.dim + c];
+    b[c] = (int)__fmul_rn(__fsub_rn(xc, g.origin[c]), g.inv_h);
+    inside = inside && isfinite(xc) && b[c] >= 0 && b[c] < g.n[c];
+  }
   const unsigned h = (unsigned)(b[0] + b[1] * g.n[0] + b[2] * g.n[0] * g.n[1]);
   hash_out[i] = h;
   if (h < (unsigned)g.ntotal) {
     scratch[kOffSlot + i] = atomicAdd(&scratch[kOffCount + h], 1);
   } else {
     scratch[kOffSlot + i] = -1;
-    atomicOr(&scratch[kOffFlags + 0], 1);
+    inside = false;
   }
+  if (!inside) atomicOr(&scratch[kOffFlags + 0], 1);
 }
 
 __global__ void __launch_bounds__(kNaThreads) na_scan_reduce(int ncells, int *scratch) {

@@ -92,7 +92,10 @@ def granular_bed(domain=(1.5, 0.6, 0.8), cell_size=1.0 / 160, bed=(1.0, 0.5, 0.3
                  seed=1, shape_function="cubic", dt=8e-6, scale=1.0, with_scoop=True, **kw):
     """3D granular bed dug by a translating, turning half-cylinder scoop
     (R 0.15, t 0.01, L 0.4, 0.5 m/s in x, 1 rad/s, Coulomb 0.3); Drucker-Prager,
-    gravity, slip walls."""
+    gravity, slip walls.  The scoop's axis sits at the bed's top, offset from
+    the node lattice by (0.37, 0.21, 0.43) cells: on a node line, nodes would
+    lie exactly on the shell's mid-surface and its end caps' centre lines,
+    where the contact normal flips direction with the last bit of rounding."""
     spacing = cell_size / ppc_1d
     b = np.asarray(bed, np.float64) * scale
     pts = _lattice(np.zeros(3), b, spacing)
@@ -102,7 +105,8 @@ def granular_bed(domain=(1.5, 0.6, 0.8), cell_size=1.0 / 160, bed=(1.0, 0.5, 0.3
     d.update(positions=pts, velocities=np.zeros_like(pts))
     if with_scoop:
         top = float(b[2])
-        body = scoop(center=(0.15 * scale, 0.5 * float(b[1]), top), radius=0.15 * scale,
+        off = np.array([0.37, 0.21, 0.43]) * cell_size
+        body = scoop(center=tuple(np.array([0.15 * scale, 0.5 * float(b[1]), top]) + off), radius=0.15 * scale,
                      thickness=max(0.01 * scale, 1.5 * cell_size), length=0.8 * float(b[1]))
         d["bcs"] = [d["bcs"][0], body, d["bcs"][1]]
     return d

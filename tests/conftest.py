@@ -10,6 +10,7 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the sm_100a kernels")
+    config.addinivalue_line("markers", "fullsize: parity at the benchmark's full sizes (minutes of CPU oracle time)")
 
 
 def gpu_available():

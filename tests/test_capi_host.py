@@ -80,3 +80,21 @@ def test_scene_particle_counts():
     assert scenes.granular_column()["positions"].shape == (1331712, 3)
     s = scenes.granular_column(cell_size=1.0 / 64)
     assert s["positions"].shape == (25 * 32 * 25, 3)
+
+
+def test_scan_tag_parity_alternates_across_the_wrap():
+    """Consecutive key-scan launches alternate the tag's parity (it selects
+    the ticket counter the launch before reset) and never publish tag 0,
+    also where the tag modulus and the 32-bit launch counter wrap."""
+    from pyroclastmpm_b200 import _capi
+
+    starts = [0, 0x3ffffff0, 2 * 0x3ffffffe - 8, 0xfffffff0]
+    for s0 in starts:
+        prev = None
+        for k in range(32):
+            launch = (s0 + k) & 0xffffffff
+            t = _capi.scan_tag(launch)
+            assert 1 <= t <= 0x3ffffffe
+            if prev is not None:
+                assert (t & 1) != (prev & 1), (hex(launch), t, prev)
+            prev = t

@@ -333,6 +333,7 @@ STEP_CASES.update({
     "sdf_2d_linear_sphere_frictionless": lambda: scoop_scene(2, "linear", "sphere", 0.0),
     "sdf_3d_quadratic_shell": lambda: scoop_scene(3, "quadratic"),
     "sdf_3d_cubic_sphere": lambda: scoop_scene(3, "cubic", "sphere", 0.5),
+    "sdf_3d_cubic_shell": lambda: scoop_scene(3, "cubic"),
     "sdf_3d_linear_shell_stick": lambda: scoop_scene(3, "linear", friction=100.0),
 })
 
@@ -356,7 +357,7 @@ def test_one_step_matches_oracle(case):
 
 @pytest.mark.parametrize("case", ["discs_2d_linear_le", "column_3d_quadratic_dp", "water_2d_quadratic_nf",
                                   "sdf_3d_quadratic_shell", "sdf_2d_quadratic_shell", "rigid_nn_2d_rotate",
-                                  "random_3d_quadratic_vm"])
+                                  "random_3d_quadratic_vm", "random_3d_cubic_le_gravity", "sdf_3d_cubic_shell"])
 def test_multi_step_drift_vs_fp64(case):
     """20 steps: FP32 GPU against the FP64 oracle (drift bound 1e-4)."""
     scene = STEP_CASES[case]()

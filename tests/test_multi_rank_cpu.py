@@ -65,6 +65,11 @@ def test_reference_arm_under_torchrun_two_ranks():
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1, r.stdout
     d = json.loads(lines[0])
-    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["steps"] == 2 and d["warmup"] == 3
+    # the reference arm times at most --ref-steps (2) steps after --ref-warmup (1)
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["steps"] == 2 and d["warmup"] == 1
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert d["config"] == bench.static_config("discs", 2)
     assert d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]

@@ -29,7 +29,7 @@ def _regular(dim, x, cell):
     return out
 
 
-def _noalloc(dim, x, cell, num_cells):
+def _noalloc(dim, x, cell, num_cells, expect=0, check_memory=False):
     import torch
 
     from pyroclastmpm_b200 import _capi
@@ -44,10 +44,15 @@ def _noalloc(dim, x, cell, num_cells):
     ce = torch.full((ncells,), -7, dtype=torch.int32, device="cuda")
     origin = (ctypes.c_float * 3)(0.0, 0.0, 0.0)
     nc = (ctypes.c_int * 3)(*num_cells)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     st = L.pmpm_partition_noalloc(dim, origin, ctypes.c_float(cell), nc, ctypes.c_void_p(xs.data_ptr()), n,
                                   ctypes.c_void_p(hash_u.data_ptr()), ctypes.c_void_p(sidx.data_ptr()),
                                   ctypes.c_void_p(cs.data_ptr()), ctypes.c_void_p(ce.data_ptr()), None)
-    assert st == 0, _capi.STATUS.get(st, st)
+    assert st == expect, _capi.STATUS.get(st, st)
+    if check_memory:
+        # a call after the first one on this device takes no device memory
+        assert torch.cuda.mem_get_info()[0] == free0
     return {"hash_unsorted": hash_u.cpu().numpy().view(np.uint32), "sorted_index": sidx.cpu().numpy(),
             "cell_start": cs.cpu().numpy(), "cell_end": ce.cpu().numpy()}
 
@@ -63,7 +68,7 @@ def test_noalloc_partition_matches_regular_twice(dim):
         x[: 1500 + 300 * call] = rng.uniform(0.41, 0.44, size=(1500 + 300 * call, dim))  # cells with > 32 particles
         x[2000:2010] = np.round(x[2000:2010] * 20) / 20  # exact cell faces
         ref = _regular(dim, x, cell)
-        got = _noalloc(dim, x, cell, list(ref["num_cells"]))
+        got = _noalloc(dim, x, cell, list(ref["num_cells"]), check_memory=call == 1)
         for k in ("hash_unsorted", "sorted_index", "cell_start", "cell_end"):
             np.testing.assert_array_equal(got[k], ref[k], err_msg=f"call {call}: {k}")
         results.append(got)
@@ -82,3 +87,44 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     p = ctypes.c_void_p(buf.data_ptr())
     st = L.pmpm_partition_noalloc(2, origin, ctypes.c_float(0.01), nc, p, 1, p, p, p, p, None)
     assert st == 1
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_noalloc_reports_particles_outside_the_grid(dim):
+    """A particle past the +x face whose flat index stays inside the grid and
+    a NaN coordinate: binned as the reference's flat hash puts them (the same
+    outputs as the regular partition), and reported as out of the domain."""
+    rng = np.random.default_rng(31 + dim)
+    cell = 0.05
+    x = rng.uniform(0.0, 1.0, size=(3000, dim))
+    x[7] = [1.07] + [0.5] * (dim - 1)       # column 21 of 21: wraps into the next row
+    x[11] = [np.nan] + [0.3] * (dim - 1)
+    ref = _regular(dim, x, cell)
+    got = _noalloc(dim, x, cell, list(ref["num_cells"]), expect=16)
+    for k in ("hash_unsorted", "sorted_index", "cell_start", "cell_end"):
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    x[11] = [0.3] * dim
+    got = _noalloc(dim, x, cell, list(ref["num_cells"]), expect=16)   # the +x particle alone
+    x[7] = [0.5] * dim
+    _noalloc(dim, x, cell, list(ref["num_cells"]), expect=0)
+
+
+def test_noalloc_reports_cells_beyond_the_sort():
+    """More than 2048 particles in one cell: PMPM_ERR_CELL_OVERFLOW; every
+    output but that cell's order inside sorted_index is still the regular
+    partition's, and that cell holds the right particles."""
+    rng = np.random.default_rng(41)
+    cell = 0.05
+    x = rng.uniform(0.0, 1.0, size=(8000, 3))
+    x[:2100] = rng.uniform(0.4005, 0.4495, size=(2100, 3))
+    ref = _regular(3, x, cell)
+    got = _noalloc(3, x, cell, list(ref["num_cells"]), expect=18)
+    for k in ("hash_unsorted", "cell_start", "cell_end"):
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    c = int(ref["hash_unsorted"][0])
+    lo, hi = int(ref["cell_start"][c]), int(ref["cell_end"][c])
+    assert hi - lo >= 2100  # the uniform particles may add one or two
+    outside = np.ones(len(x), bool)
+    outside[lo:hi] = False
+    np.testing.assert_array_equal(got["sorted_index"][outside], ref["sorted_index"][outside])
+    np.testing.assert_array_equal(np.sort(got["sorted_index"][lo:hi]), ref["sorted_index"][lo:hi])
