@@ -458,15 +458,37 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
                            const float *positions, int num_particles, unsigned *hash_unsorted,
                            int *sorted_index, int *cell_start, int *cell_end, void *stream);
 
-/* Autotuner (no reference counterpart): where a configuration has more than
- * one P2G kernel (3D quadratic: dual-cell z-sweep per node tile, or a warp
- * per row of dual cells scattering into brick boxes), time each on `steps`
- * steps from the current state, keep the fastest for this handle and put
- * the state (and step counter) back.  *chosen: 1 sweep, 0 cell scatter. */
+/* Autotuner (no reference counterpart; the reference launches every kernel
+ * with a fixed block of 64 threads, include/pyroclastmpm/common/types_common.h:
+ * 205-229).  Tunes, from the current state, for this handle:
+ *  - the P2G kernel where a configuration has more than one (3D quadratic:
+ *    dual-cell z-sweep per node tile, or a warp per row of dual cells
+ *    scattering into brick boxes) and the staging of the 3D sweeps (bulk
+ *    copies of sorted records, or a gather through the sorted order): each
+ *    (kernel, staging) pair is timed on `steps` steps;
+ *  - the re-sort interval (when it is not 0): one physical re-sort is timed,
+ *    then the chosen kernels on max(16, 4 steps) steps without re-sorts; the
+ *    interval in {8, 16, 32, 64, 128} minimising t_sort / K + slope K / 2
+ *    (slope: the growth of the step time per step) is kept.
+ * The particle state and the step counter are put back afterwards.
+ * *chosen: the P2G kernel (1 sweep, 0 cell scatter); pmpm_get_tuning reports
+ * all choices. */
 int pmpm_autotune(pmpm_sim *s, int steps, int *chosen);
 /* Selects the P2G kernel directly (the autotuner's choices: 1 sweep, 0 cell
  * scatter); PMPM_ERR_NOT_SUPPORTED where the configuration has only one. */
 int pmpm_set_p2g_kernel(pmpm_sim *s, int variant);
+/* Staging of the 3D sweep P2G kernels: 1 (default) the particles of each
+ * row of source cells arrive in shared memory by one bulk copy
+ * (cp.async.bulk on an mbarrier) from records written in sorted order just
+ * before the P2G; 0 each particle's fields are gathered through the sorted
+ * order.  PMPM_ERR_NOT_SUPPORTED without a 3D sweep (2D, deterministic). */
+int pmpm_set_p2g_staging(pmpm_sim *s, int mode);
+/* Steps between physical re-sorts of particle storage (0: never). */
+int pmpm_set_resort_interval(pmpm_sim *s, int steps);
+/* The handle's current choices: P2G kernel (as pmpm_set_p2g_kernel), staging
+ * (as pmpm_set_p2g_staging, -1 where it does not apply), re-sort interval.
+ * Any pointer may be NULL. */
+int pmpm_get_tuning(const pmpm_sim *s, int *p2g_kernel, int *staging, int *resort_interval);
 
 /* ---------------------------------------------------------------------------
  * Differentiable rollouts (no counterpart in the reference).  A rollout of

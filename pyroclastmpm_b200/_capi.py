@@ -87,7 +87,7 @@ EXPORTS = [
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
     "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
     "pmpm_material_modified_cam_clay", "pmpm_material_drucker_prager_cap", "pmpm_set_p2g_kernel",
-    "pmpm_set_wait_limit", "pmpm_scan_tag",
+    "pmpm_set_wait_limit", "pmpm_scan_tag", "pmpm_set_p2g_staging", "pmpm_set_resort_interval", "pmpm_get_tuning",
 ]
 
 EXPORTS += [
@@ -178,6 +178,10 @@ def lib():
     L.pmpm_active_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.pmpm_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
+    L.pmpm_set_p2g_staging.argtypes = [vp, i]
+    L.pmpm_set_resort_interval.argtypes = [vp, i]
+    L.pmpm_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int)]
     L.pmpm_batch_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
     L.pmpm_scan_tag.argtypes = [ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)]
     L.pmpm_partition_noalloc.argtypes = [i, fp, f, ctypes.POINTER(ctypes.c_int), vp, i, vp, vp, vp, vp, vp]
@@ -535,6 +539,19 @@ class Simulation:
     def set_wait_limit(self, spins):
         """Bound on the key scan's look-back polls (default 2**22)."""
         check(lib().pmpm_set_wait_limit(self._h, int(spins)), "pmpm_set_wait_limit")
+
+    def set_p2g_staging(self, mode):
+        """3D sweeps: 1 bulk copies of sorted records, 0 gather through the sorted order."""
+        check(lib().pmpm_set_p2g_staging(self._h, int(mode)), "pmpm_set_p2g_staging")
+
+    def set_resort_interval(self, steps):
+        check(lib().pmpm_set_resort_interval(self._h, int(steps)), "pmpm_set_resort_interval")
+
+    def tuning(self):
+        """The handle's choices: {"p2g_kernel", "staging", "resort_interval"}."""
+        k, g, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().pmpm_get_tuning(self._h, ctypes.byref(k), ctypes.byref(g), ctypes.byref(r)), "pmpm_get_tuning")
+        return {"p2g_kernel": k.value, "staging": g.value, "resort_interval": r.value}
 
     def autotune(self, steps=5):
         """Time each P2G kernel this configuration has on `steps` steps, keep

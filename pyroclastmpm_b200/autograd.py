@@ -63,3 +63,26 @@ def rollout(sim: Simulation, youngs: torch.Tensor, friction: torch.Tensor, nstep
     """Final positions after `nsteps` steps, differentiable in the per-particle
     Young's modulus and friction angle (degrees)."""
     return _Rollout.apply(youngs, friction, sim, int(nsteps), int(checkpoint_every))
+
+
+def calibrate(sim: Simulation, target: torch.Tensor, youngs0, friction0, nsteps: int, checkpoint_every: int = 25,
+              iterations: int = 40, lr_log_youngs: float = 0.05, lr_friction: float = 0.5):
+    """Per-particle calibration of Young's modulus and friction angle to a
+    target final configuration: Adam on (log E, friction angle in degrees),
+    the loss being the mean squared distance of the final positions from
+    `target` [n, dim] (a CUDA tensor).  Returns (E, friction, losses): the
+    parameters after the last iteration and the loss of every iteration."""
+    dev = target.device
+    logE = torch.log(torch.as_tensor(youngs0, dtype=torch.float32, device=dev)).clone().requires_grad_(True)
+    phi = torch.as_tensor(friction0, dtype=torch.float32, device=dev).clone().requires_grad_(True)
+    opt = torch.optim.Adam([{"params": [logE], "lr": lr_log_youngs}, {"params": [phi], "lr": lr_friction}])
+    losses = []
+    n = target.shape[0]
+    for _ in range(iterations):
+        opt.zero_grad()
+        x = rollout(sim, torch.exp(logE), phi, nsteps, checkpoint_every)
+        loss = ((x.double() - target.double()) ** 2).sum() / n
+        loss.backward()
+        opt.step()
+        losses.append(float(loss.item()))
+    return torch.exp(logE).detach(), phi.detach(), losses

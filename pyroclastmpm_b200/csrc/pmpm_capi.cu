@@ -187,6 +187,7 @@ struct pmpm_sim {
   int nkeys = 0;
   int nbricks = 0;     // dual-cell bricks (cell-scatter P2G)
   int p2g_variant = 1; // 3D quadratic: 0 cell scatter, 1 dual sweep (pmpm_autotune picks)
+  int p2g_staging = 1; // 3D sweeps: 1 bulk copies of sorted records, 0 gather through the order
   int num_sms = 1;       // persistent P2G grids: CTAs per SM x this
   // the last step's G2P binned the current positions for the next partition
   // (3D quadratic): counts, slots, keys and marks are in place
@@ -254,6 +255,7 @@ void free_particles(pmpm_sim *s) {
   dfree(s->key);
   dfree(s->hash_next);
   dfree(s->B.order);
+  dfree(s->B.rec);
   dfree(s->musl_x);
   s->n = 0;
   s->stride = 0;
@@ -487,22 +489,47 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
   if (s->flags & PMPM_FLAG_DETERMINISTIC) {
     k_p2g_gather<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
   } else if (D == 3 && s->dual) {
-    constexpr int bytes = dual3_smem_bytes<false>(), pbytes = dual3_smem_bytes<true>();
-    static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
+    static bool attr_set[64] = {false};  // per device
     if (!attr_set[dev]) {
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     dual3_smem_bytes<false, true>()));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     dual3_smem_bytes<true, true>()));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     dual3_smem_bytes<false, false>()));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_dual3<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     dual3_smem_bytes<true, false>()));
       attr_set[dev] = true;
     }
     if (s->p2g_variant == 1) {
-      // persistent CTAs over the active-tile queue of this partition
+      // (bulk staging: sorted records of this partition's particles first)
+      // persistent CTAs over the active-tile queue
+      if (s->p2g_staging) {
+        if (s->has_planar)
+          k_records<PMPM_SHAPE_QUADRATIC, true, true><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a);
+        else
+          k_records<PMPM_SHAPE_QUADRATIC, true, false><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a);
+        PMPM_LAUNCHED();
+        s->launches += 1;
+      }
       a.p2g_par = (int)(s->p2g_seq++ & 1u);
       const int grid = std::min(s->g.ntiles, s->num_sms);
-      if (s->has_planar)
-        k_p2g_dual3<true><<<grid, Dual3::NT, pbytes, s->stream>>>(a, apply_bcs, s->node_epoch);
-      else
-        k_p2g_dual3<false><<<grid, Dual3::NT, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+      if (s->p2g_staging) {
+        if (s->has_planar)
+          k_p2g_dual3<true, true><<<grid, Dual3::NT, dual3_smem_bytes<true, true>(), s->stream>>>(a, apply_bcs,
+                                                                                                  s->node_epoch);
+        else
+          k_p2g_dual3<false, true><<<grid, Dual3::NT, dual3_smem_bytes<false, true>(), s->stream>>>(a, apply_bcs,
+                                                                                                    s->node_epoch);
+      } else {
+        if (s->has_planar)
+          k_p2g_dual3<true, false><<<grid, Dual3::NT, dual3_smem_bytes<true, false>(), s->stream>>>(a, apply_bcs,
+                                                                                                    s->node_epoch);
+        else
+          k_p2g_dual3<false, false><<<grid, Dual3::NT, dual3_smem_bytes<false, false>(), s->stream>>>(
+              a, apply_bcs, s->node_epoch);
+      }
     } else {
       constexpr int cbytes = cells3_smem_bytes();
       static bool cattr_set[64] = {false};  // per device
@@ -516,20 +543,45 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
       s->launches += 1;
     }
   } else if (D == 3) {
-    constexpr int bytes = sweep3_smem_bytes<SF, false>(), pbytes = sweep3_smem_bytes<SF, true>();
-    static bool attr_set[64] = {false};  // per device
     const int dev = s->device < 64 ? s->device : 63;
+    static bool attr_set[64] = {false};  // per device
     if (!attr_set[dev]) {
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sweep3_smem_bytes<SF, false, true>()));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sweep3_smem_bytes<SF, true, true>()));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sweep3_smem_bytes<SF, false, false>()));
+      PMPM_CUDA(cudaFuncSetAttribute(k_p2g_sweep3<SF, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sweep3_smem_bytes<SF, true, false>()));
       attr_set[dev] = true;
+    }
+    if (s->p2g_staging) {
+      if (s->has_planar)
+        k_records<SF, false, true><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a);
+      else
+        k_records<SF, false, false><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a);
+      PMPM_LAUNCHED();
+      s->launches += 1;
     }
     a.p2g_par = (int)(s->p2g_seq++ & 1u);
     const int grid = std::min(s->g.ntiles, s->num_sms);
-    if (s->has_planar)
-      k_p2g_sweep3<SF, true><<<grid, TileDims<3>::N, pbytes, s->stream>>>(a, apply_bcs, s->node_epoch);
-    else
-      k_p2g_sweep3<SF, false><<<grid, TileDims<3>::N, bytes, s->stream>>>(a, apply_bcs, s->node_epoch);
+    constexpr int NT3 = TileDims<3>::N;
+    if (s->p2g_staging) {
+      if (s->has_planar)
+        k_p2g_sweep3<SF, true, true><<<grid, NT3, sweep3_smem_bytes<SF, true, true>(), s->stream>>>(a, apply_bcs,
+                                                                                                   s->node_epoch);
+      else
+        k_p2g_sweep3<SF, false, true><<<grid, NT3, sweep3_smem_bytes<SF, false, true>(), s->stream>>>(
+            a, apply_bcs, s->node_epoch);
+    } else {
+      if (s->has_planar)
+        k_p2g_sweep3<SF, true, false><<<grid, NT3, sweep3_smem_bytes<SF, true, false>(), s->stream>>>(
+            a, apply_bcs, s->node_epoch);
+      else
+        k_p2g_sweep3<SF, false, false><<<grid, NT3, sweep3_smem_bytes<SF, false, false>(), s->stream>>>(
+            a, apply_bcs, s->node_epoch);
+    }
   } else {
     k_p2g_tile<D, SF><<<s->g.ntiles, TileDims<D>::N, 0, s->stream>>>(a, apply_bcs, s->node_epoch);
   }
@@ -1468,6 +1520,11 @@ int pmpm_set_particles(pmpm_sim *s, int num_particles, const float *positions, c
   PMPM_TRY(dalloc(&s->key, (size_t)s->stride));
   if (s->dual) PMPM_TRY(dalloc(&s->hash_next, (size_t)s->stride));
   PMPM_TRY(dalloc(&s->B.order, (size_t)s->stride));
+  if (s->dim == 3 && !(s->flags & PMPM_FLAG_DETERMINISTIC)) {
+    // sorted P2G records of the 3D sweep kernels (k_records)
+    s->B.rec4 = s->has_planar ? 5 : 4;
+    PMPM_TRY(dalloc(&s->B.rec, (size_t)s->stride * s->B.rec4));
+  }
   if (s->flags & PMPM_FLAG_MUSL) PMPM_TRY(dalloc(&s->musl_x, (size_t)s->dim * s->stride));
   const int st = s->stride;
   const int S = D == 2 ? 4 : 6, E = D == 2 ? 3 : 6;
@@ -1529,6 +1586,8 @@ int pmpm_initialize(pmpm_sim *s) {
   if (s->n == 0) return PMPM_ERR_STATE;
   PMPM_CUDA(cudaSetDevice(s->device));
   PMPM_TRY(pmpm_partition(s));
+  // particle storage starts in cell order (the re-sort interval counts from here)
+  if (s->resort_interval > 0 && !s->ro.held) PMPM_TRY(s->dim == 2 ? launch_reorder<2>(s) : launch_reorder<3>(s));
   DevParticles &P = s->P[s->cur];
   // calculate_initial_volumes: (REAL)pow(h, DIM) / ppc
   float vol = (float)std::pow((double)s->g.h, (double)s->dim);
@@ -3087,17 +3146,72 @@ extern "C" int pmpm_set_p2g_kernel(pmpm_sim *s, int variant) {
   return PMPM_OK;
 }
 
+extern "C" int pmpm_set_p2g_staging(pmpm_sim *s, int mode) {
+  if (!s || (mode != 0 && mode != 1)) return PMPM_ERR_INVALID_ARGUMENT;
+  if (!s->B.rec) return PMPM_ERR_NOT_SUPPORTED;
+  s->p2g_staging = mode;
+  return PMPM_OK;
+}
+
+extern "C" int pmpm_set_resort_interval(pmpm_sim *s, int steps) {
+  if (!s || steps < 0) return PMPM_ERR_INVALID_ARGUMENT;
+  s->resort_interval = steps;
+  return PMPM_OK;
+}
+
+extern "C" int pmpm_get_tuning(const pmpm_sim *s, int *p2g_kernel, int *staging, int *resort_interval) {
+  if (!s) return PMPM_ERR_INVALID_ARGUMENT;
+  if (p2g_kernel) *p2g_kernel = s->p2g_variant;
+  if (staging) *staging = s->B.rec ? s->p2g_staging : -1;
+  if (resort_interval) *resort_interval = s->resort_interval;
+  return PMPM_OK;
+}
+
+namespace {
+
+// Re-sort interval from a cost model: a physical re-sort costs t_sort once;
+// between re-sorts the step slows by about sigma per step as particles leave
+// their sorted storage order (slope of the step times over the sampled
+// steps, none re-sorted).  Steps per interval K cost t_sort / K + sigma K / 2
+// on average; the candidate that minimises it is chosen.
+int pick_resort_interval(float t_sort, const std::vector<float> &step_ms) {
+  const int m = (int)step_ms.size();
+  double sx = 0, sy = 0, sxx = 0, sxy = 0;
+  for (int i = 0; i < m; i++) {
+    sx += i;
+    sy += step_ms[i];
+    sxx += (double)i * i;
+    sxy += (double)i * step_ms[i];
+  }
+  const double den = m * sxx - sx * sx;
+  const double sigma = den > 0 ? std::max(0.0, (m * sxy - sx * sy) / den) : 0.0;
+  const int cands[] = {8, 16, 32, 64, 128};
+  int best = 32;
+  double best_cost = 1e300;
+  for (int k : cands) {
+    const double cost = t_sort / k + sigma * k / 2.0;
+    if (cost < best_cost - 1e-12) {
+      best_cost = cost;
+      best = k;
+    }
+  }
+  return best;
+}
+
+}  // namespace
+
 extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   if (!s || steps < 1) return PMPM_ERR_INVALID_ARGUMENT;
   if (s->n == 0) return PMPM_ERR_STATE;
   PMPM_CUDA(cudaSetDevice(s->device));
-  std::vector<int> cands;
-  if (s->dual && s->dim == 3) cands = {1, 0};
-  if (cands.size() < 2) {
-    if (chosen) *chosen = s->p2g_variant;
-    return PMPM_OK;
-  }
-  // time each variant on the same state: save, step, restore (no re-sort meanwhile)
+  // candidates: (P2G kernel, staging) pairs this configuration has
+  std::vector<std::pair<int, int>> cands;
+  const bool dual3 = s->dual && s->dim == 3;
+  const bool staged = s->B.rec != nullptr;
+  for (int v : dual3 ? std::vector<int>{1, 0} : std::vector<int>{s->p2g_variant})
+    for (int g : staged && v == 1 ? std::vector<int>{1, 0} : std::vector<int>{s->p2g_staging})
+      cands.push_back({v, g});
+  // time each candidate on the same state: save, step, restore (no re-sort meanwhile)
   const size_t per = (size_t)state_floats(s) * s->stride;
   const size_t extra = (size_t)(s->dim * s->dim + 2) * s->stride;  // L, alpha (or VonMises history) and pc
   float *saved = nullptr;
@@ -3120,11 +3234,13 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  int best_v = s->p2g_variant;
+  std::pair<int, int> best_c = {s->p2g_variant, s->p2g_staging};
+  std::vector<float> step_ms;
   s->tuning = true;
   for (size_t k = 0; k < cands.size() && st == PMPM_OK; k++) {
-    s->p2g_variant = cands[k];
-    st = PMPM_DISPATCH(s, step_once, s);  // warm-up (and first-launch set-up) of the variant
+    s->p2g_variant = cands[k].first;
+    s->p2g_staging = cands[k].second;
+    st = PMPM_DISPATCH(s, step_once, s);  // warm-up (and first-launch set-up) of the candidate
     if (st != PMPM_OK) break;
     cudaEventRecord(e0, s->stream);
     for (int i = 0; i < steps && st == PMPM_OK; i++) st = PMPM_DISPATCH(s, step_once, s);
@@ -3134,18 +3250,57 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
     cudaEventElapsedTime(&ms, e0, e1);
     if (ms < best) {
       best = ms;
-      best_v = cands[k];
+      best_c = cands[k];
     }
     if (st == PMPM_OK) st = copy_state(s, saved, false);
     if (st == PMPM_OK) st = copy_extra(false);
     s->step = step0;
   }
+  s->p2g_variant = best_c.first;
+  s->p2g_staging = best_c.second;
+  // re-sort interval: one physical re-sort timed (into the other storage
+  // set), then the chosen kernels stepped on that sorted copy without
+  // re-sorts, each step timed; the state returns to the original set after
+  if (st == PMPM_OK && s->resort_interval > 0 && !s->ro.held) {
+    const int since0 = s->steps_since_sort;
+    float t_sort = 0.0f;
+    st = PMPM_DISPATCH(s, step_once, s);  // fresh partition for the re-sort
+    if (st == PMPM_OK) {
+      cudaEventRecord(e0, s->stream);
+      st = s->dim == 2 ? launch_reorder<2>(s) : launch_reorder<3>(s);
+      cudaEventRecord(e1, s->stream);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(&t_sort, e0, e1);
+    }
+    if (st == PMPM_OK) {
+      const int nsample = std::max(16, 4 * steps);
+      std::vector<cudaEvent_t> ev(nsample + 1);
+      for (auto &e : ev) cudaEventCreate(&e);
+      cudaEventRecord(ev[0], s->stream);
+      for (int i = 0; i < nsample && st == PMPM_OK; i++) {
+        st = PMPM_DISPATCH(s, step_once, s);
+        cudaEventRecord(ev[i + 1], s->stream);
+      }
+      cudaEventSynchronize(ev[nsample]);
+      for (int i = 0; i < nsample && st == PMPM_OK; i++) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        step_ms.push_back(ms);
+      }
+      for (auto &e : ev) cudaEventDestroy(e);
+      s->cur = 1 - s->cur;  // back to the storage set the tuning started from
+    }
+    if (st == PMPM_OK) s->resort_interval = pick_resort_interval(t_sort, step_ms);
+    if (st == PMPM_OK) st = copy_state(s, saved, false);
+    if (st == PMPM_OK) st = copy_extra(false);
+    s->steps_since_sort = since0;
+    s->step = step0;
+  }
   s->tuning = false;
-  s->p2g_variant = best_v;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaStreamSynchronize(s->stream);
   cudaFree(saved);
-  if (chosen) *chosen = best_v;
+  if (chosen) *chosen = best_c.first;
   return st;
 }

@@ -105,6 +105,12 @@ struct DevBins {
   int *block_sums;  // scan scratch
   int *scalars;     // [0] binned count, [1] unbinned counter, [2] big-cell count
   int *big_cells;   // cells too large for the in-register sort
+  // P2G records of the 3D sweep kernels in sorted order (null where not
+  // used): rec4 float4s per particle (4, or 5 with a PlanarDomain), written
+  // by k_records just before each P2G launch, copied into shared memory by
+  // the sweeps' bulk copies one row of source cells at a time
+  float4 *rec;
+  int rec4;
 };
 
 struct DevMaterial {

@@ -33,6 +33,93 @@ struct IPow<B, 0> {
   static constexpr int value = 1;
 };
 
+// --------------------------------------------------------------------------
+// bulk copies into shared memory on an mbarrier (sm_90+ async proxy)
+// --------------------------------------------------------------------------
+//
+// A CTA arms a barrier phase with the bytes it expects, any of its threads
+// issue cp.async.bulk copies global -> shared that complete those bytes on
+// the barrier, and every thread waits for the phase with a bounded poll.
+// Plain per-CTA copies from this GPU's own memory: no cluster multicast.
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// the barrier's initialisation visible to the async proxy (the copy engine)
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// orders this thread's earlier shared-memory accesses before later
+// async-proxy writes to the same memory
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// bytes (a multiple of 16) from 16-byte aligned global src to 16-byte aligned shared dst
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// one poll of the phase of the given parity; suspends the thread for at most
+// about kBulkPollNs nanoseconds while the phase is incomplete
+constexpr unsigned kBulkPollNs = 500;
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kBulkPollNs)
+      : "memory");
+  return ok != 0;
+}
+
+// The copy state of one CTA: its barrier and a flag set once a wait gave up.
+struct BulkState {
+  unsigned long long bar;
+  int failed;
+};
+
+// Waits for the barrier phase of the given parity.  After kBulkWaitPolls
+// polls (about a second) the wait gives up, records kFaultWaitTimeout and
+// marks the CTA's copies failed: later waits return at once and no further
+// copies are issued, so the kernel finishes (its results are then invalid).
+constexpr int kBulkWaitPolls = 1 << 21;
+__device__ __forceinline__ bool mbar_wait(BulkState *bs, unsigned parity, int *fault) {
+  if (*(volatile int *)&bs->failed) return false;
+  for (int k = 0; k < kBulkWaitPolls; k++)
+    if (mbar_try_wait(&bs->bar, parity)) return true;
+  *(volatile int *)&bs->failed = 1;
+  atomicOr(fault, kFaultWaitTimeout);
+  return false;
+}
+
+// Sets up the CTA's copy state (one thread), before the block barrier that
+// publishes it.
+__device__ __forceinline__ void bulk_init(BulkState *bs) {
+  bs->failed = 0;
+  mbar_init(&bs->bar, 1);
+  fence_mbar_init();
+}
+
+// binning_failed() read once per CTA and shared, for kernels whose threads
+// must agree (block barriers follow).
+__device__ __forceinline__ bool binning_failed_cta(const int *fault) {
+  __shared__ int flag;
+  if (threadIdx.x == 0) flag = (*(volatile const int *)fault & kFaultWaitTimeout) != 0;
+  __syncthreads();
+  return flag != 0;
+}
+
 template <int D>
 __device__ __forceinline__ int tile_of(const DevGrid &g, const int c[3]) {
   using T = TileDims<D>;
@@ -553,6 +640,63 @@ __global__ void __launch_bounds__(1024) k_sort_big(StepArgs a) {
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) a.B.order[lo + i] = val[i];
     __syncthreads();
   }
+}
+
+// --------------------------------------------------------------------------
+// P2G records of the 3D sweeps
+// --------------------------------------------------------------------------
+//
+// Sorted position k of the binned particles -> rec[k * R4 ..]:
+//   [0] (m, m vx, m vy, m vz)   [1] (Sxx, Sxy, Sxy, Syy)   [2] (Sxz, Syz, Szz, 0)
+//   [3] (x, y, z, 0)            [4] PlanarDomain only: (f_ext, 0)
+// with S = -V sigma; the MUSL momentum remap maps neither stress nor
+// external force.  The sweeps copy a row of source cells (consecutive keys:
+// one run of records) into shared memory with one bulk copy instead of
+// gathering each particle's fields through the sorted order.  Written just
+// before each P2G from the current particle state, so a P2G after any
+// change of state (stage calls, field setters, MUSL) reads current values.
+// DUAL: the dual-cell sweep (its cells hold only particles inside the grid;
+// f_ext mapped for all); otherwise the linear/cubic sweep conventions (a
+// quadratic particle outside the grid on an axis takes no part; f_ext only
+// with mass).
+template <int SF, bool DUAL, bool PLANAR>
+__device__ __forceinline__ void make_record(const StepArgs &a, int s, float4 r[5]) {
+  const DevParticles &P = a.P;
+  const DevGrid &g = a.g;
+  const int st = P.stride;
+  const float x[3] = {P.x[s], P.x[st + s], P.x[2 * st + s]};
+  bool drop = false;
+  if (!DUAL && SF == PMPM_SHAPE_QUADRATIC) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int b = (int)scaled_coord(x[c], g.origin[c], g.inv_h);
+      drop = drop || b < 0 || b >= g.n[c];
+    }
+  }
+  const float m = drop ? 0.0f : P.m[s];
+  const float nv = (drop || a.remap) ? 0.0f : -P.V[s];
+  const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
+  const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
+  r[0] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
+  r[1] = make_float4(Sxx, Sxy, Sxy, Syy);
+  r[2] = make_float4(Sxz, Syz, Szz, 0.0f);
+  r[3] = make_float4(x[0], x[1], x[2], 0.0f);
+  if (PLANAR) {
+    const bool use = DUAL ? !a.remap : (m != 0.0f && !a.remap);
+    r[4] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f, use ? P.fext[2 * st + s] : 0.0f, 0.0f);
+  }
+}
+
+template <int SF, bool DUAL, bool PLANAR>
+__global__ void __launch_bounds__(256) k_records(StepArgs a) {
+  if (binning_failed(a.fault)) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.B.scalars[0]) return;  // binned particles occupy sorted positions [0, binned)
+  float4 r[5];
+  make_record<SF, DUAL, PLANAR>(a, a.B.order[k], r);
+  float4 *dst = a.B.rec + (size_t)k * (PLANAR ? 5 : 4);
+#pragma unroll
+  for (int q = 0; q < (PLANAR ? 5 : 4); q++) dst[q] = r[q];
 }
 
 // --------------------------------------------------------------------------
@@ -1392,18 +1536,59 @@ struct Sweep3 {
   __host__ __device__ static constexpr int floats(bool planar) {
     return 4 * WIN + 12 + 4 * NZ4 + (planar ? 4 : 0);
   }
-  // static shared memory: pair lists, the all-layer cell table, scan scratch
-  static constexpr int STATIC_BYTES = (4 * (2 * MAXPAIR + 2 + 2 * NL * NCELL + 1 + 33 + 1) + 255) / 256 * 256 + 256;
-  // staged particles: 227 KB per CTA less the static part and the node
-  // accumulators
-  __host__ __device__ static constexpr int cap(bool planar) {
-    return ((232448 - STATIC_BYTES - 7 * NN * 4) / (4 * floats(planar))) & ~7;
+  // float4s of one P2G record (k_records), bulk-copied per row of source cells
+  __host__ __device__ static constexpr int rec4(bool planar) { return planar ? 5 : 4; }
+  static constexpr int NROWS = NL * NS;              // rows of source cells along x
+  // static shared memory: pair lists, the all-layer cell table, scan scratch,
+  // the copy barrier
+  static constexpr int STATIC_BYTES =
+      (4 * (2 * MAXPAIR + 2 + 2 * NL * NCELL + 1 + 33 + 1 + 2) + 255) / 256 * 256 + 256;
+  // staged particles (and with bulk staging their records): 227 KB per CTA
+  // less the static part and the node accumulators
+  __host__ __device__ static constexpr int cap(bool planar, bool bulk) {
+    return ((232448 - STATIC_BYTES - 7 * NN * 4) / (4 * floats(planar) + (bulk ? 16 * rec4(planar) : 0))) & ~7;
   }
 };
 
-template <int SF, bool PLANAR>
+template <int SF, bool PLANAR, bool BULK>
 constexpr int sweep3_smem_bytes() {
-  return (7 * Sweep3<SF>::NN + Sweep3<SF>::cap(PLANAR) * Sweep3<SF>::floats(PLANAR)) * 4;
+  using W = Sweep3<SF>;
+  return (7 * W::NN + W::cap(PLANAR, BULK) * W::floats(PLANAR)) * 4 +
+         (BULK ? W::cap(PLANAR, BULK) * W::rec4(PLANAR) * 16 : 0);
+}
+
+// Issues the bulk copies of positions [p0, p1) of a work unit's particle
+// list into raw[0 .. p1 - p0) (R4 float4s each) and arms the barrier with
+// their bytes.  The list runs through the unit's table of source cells in
+// order; a row of NS cells along x has consecutive binning keys, so its
+// particles are one run of the sorted records: one copy per row that
+// overlaps the piece, issued by the row's thread.  Every copy lies inside
+// the binned records (sorted positions of the row's cells) and inside raw.
+template <int NS, int R4>
+__device__ __forceinline__ void issue_piece(const float4 *rec, const int *cell_k0, const int *cell_pref, int nrows,
+                                            int p0, int p1, float4 *raw, BulkState *bs) {
+  const int tid = threadIdx.x;
+  if (*(volatile int *)&bs->failed) return;  // the CTA's copies stopped after a wait gave up
+  unsigned long long *bar = &bs->bar;
+  if (tid == 0) mbar_arrive_expect_tx(bar, (unsigned)(p1 - p0) * R4 * 16u);
+  if (tid < nrows) {
+    const int c0 = tid * NS;
+    const int a0 = cell_pref[c0], b0 = cell_pref[c0 + NS];
+    const int lo = max(a0, p0), hi = min(b0, p1);
+    if (lo < hi) {
+      // the row's first particle is the first particle of its first non-empty cell
+      int k0 = 0;
+      for (int i = 0; i < NS; i++) {
+        if (cell_pref[c0 + i + 1] > cell_pref[c0 + i]) {
+          k0 = cell_k0[c0 + i];
+          break;
+        }
+      }
+      fence_async_smem();
+      bulk_copy_g2s(raw + (size_t)(lo - p0) * R4, rec + (size_t)(k0 + (lo - a0)) * R4, (unsigned)(hi - lo) * R4 * 16u,
+                    bar);
+    }
+  }
 }
 
 // pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
@@ -1436,13 +1621,18 @@ __device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
 // about eight) hit different shared-memory banks.
 __device__ __forceinline__ int sweep_slot(int j) { return j ^ ((j >> 3) & 7); }
 
-template <int SF, bool PLANAR>
-__device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int unit) {
+// BULK: a piece's particles arrive as sorted records by bulk copy (k_records
+// wrote them); otherwise each is gathered through the sorted order.
+// bs / phase: the CTA's copy state and the parity of its barrier's next phase
+template <int SF, bool PLANAR, bool BULK>
+__device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int unit,
+                                            BulkState *bs, unsigned &phase) {
   using W = Sweep3<SF>;
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int WIN = W::WIN;
-  constexpr int SL = W::cap(PLANAR);
+  constexpr int SL = W::cap(PLANAR, BULK);
+  constexpr int R4 = W::rec4(PLANAR);
   constexpr int TZ = W::TZ, NN = W::NN;
   const DevGrid &g = a.g;
 
@@ -1462,6 +1652,7 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   float4 *st_s1 = st_s0 + SL;                               // (Sxz, Syz, Szz, 0)
   float4(*st_z)[SL] = (float4(*)[SL])(st_s1 + SL);          // [NZ4] z N[0..WIN), dN[0..WIN)
   float4 *st_f = (float4 *)(st_z + W::NZ4);                 // PLANAR: (f, 0)
+  float4 *raw = (float4 *)(acc + 7 * NN + SL * W::floats(PLANAR));  // BULK: [SL][R4] records of the piece
 
   // work unit `unit`: the two tiles 2k, 2k + 1 along z of one tile column
   const int tid = threadIdx.x;
@@ -1488,8 +1679,6 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     cz_hi = min(cz_hi, g.n[2] - 1);
   }
   const int nlayers = cz_hi - cz_lo + 1;
-  const DevParticles &P = a.P;
-  const int st = P.stride;
   const long long nxny = (long long)g.n[0] * g.n[1];
 
   // ---- all layers' source cells -> sorted ranges, one prefix ----
@@ -1530,43 +1719,33 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   __syncthreads();
   const int total = cell_pref[ntab];
 
-  // table cell and storage slot of position j of the tile's particle list
-  auto locate = [&](int j, int &lo, int &s) {
-    lo = 0;
-    int hi = ntab;
+  // table cell of position j of the unit's particle list
+  auto locate = [&](int j) {
+    int lo = 0, hi = ntab;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
       if (cell_pref[mid] <= j) lo = mid; else hi = mid;
     }
-    s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+    return lo;
   };
-  // ---- stage particle list position j into slot jj ----
-  auto stage_one = [&](int lo, int s, int jj) {
+  // ---- stage particle list position j (record r, table cell lo) into slot jj ----
+  auto stage_one = [&](int lo, const float4 *r, int jj) {
     const int layer = lo / W::NCELL, vc = lo - layer * W::NCELL;
     const int cz = cz_lo + layer;
+    const float4 xp = r[3];
+    const float xs[3] = {xp.x, xp.y, xp.z};
     float u[3];
     int b[3];
-    bool inside = true;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      u[c] = scaled_coord(P.x[c * st + s], g.origin[c], g.inv_h);
+      u[c] = scaled_coord(xs[c], g.origin[c], g.inv_h);
       b[c] = (int)u[c];
-      inside = inside && b[c] >= 0 && b[c] < g.n[c];
     }
-    float m = P.m[s];
-    if (SF == PMPM_SHAPE_QUADRATIC && !inside) m = 0.0f;  // takes no part in P2G
-    const float nv = ((SF == PMPM_SHAPE_QUADRATIC && !inside) || a.remap) ? 0.0f : -P.V[s];
-    st_p[jj] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
-    if (PLANAR) {
-      const bool use = m != 0.0f && !a.remap;
-      st_f[jj] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f, use ? P.fext[2 * st + s] : 0.0f,
-                             0.0f);
-    }
-    // -V sigma, symmetric: xx yy zz xy xz yz
-    const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
-    const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
-    st_s0[jj] = make_float4(Sxx, Sxy, Sxy, Syy);
-    st_s1[jj] = make_float4(Sxz, Syz, Szz, 0.0f);
+    // (m, m v), -V sigma as (xx, xy, xy, yy) (xz, yz, zz, 0), f_ext: k_records
+    st_p[jj] = r[0];
+    st_s0[jj] = r[1];
+    st_s1[jj] = r[2];
+    if (PLANAR) st_f[jj] = r[4];
     // weights of the WIN offsets per axis: r from the particle's own bin
     // (the reference psi), the cubic node type of the target the offset
     // reaches from the (possibly aliased) source cell the particle is
@@ -1605,7 +1784,13 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   };
 
   constexpr int R = (SL + NT - 1) / NT;
+  const int nrows = nlayers * W::NS;
+  // storage slot of list position j (table cell lo), for the gathered staging
+  auto slot_of = [&](int j, int lo) { return a.B.order[cell_k0[lo] + (j - cell_pref[lo])]; };
   for (int round = 0; round < nrounds; round++) {
+    // the first piece's records are on their way while the items are set up
+    if (BULK && total > 0)
+      issue_piece<W::NS, R4>(a.B.rec, cell_k0, cell_pref, nrows, 0, min(SL, total), raw, bs);
     // this thread's items
     int item_cell[W::IPT], item_ix[W::IPT], item_iy[W::IPT], item_tl[W::IPT];
     int item_tx[W::IPT], item_ty[W::IPT];
@@ -1661,35 +1846,45 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
         wz[q][WIN - 1] = 0.0f;
       }
     };
-    // The tile's particles, all layers in z order, are positions
+    // The unit's particles, all layers in z order, are positions
     // 0 .. total of the table; they are staged in pieces of SL positions
-    // regardless of layer boundaries, and the next piece's storage slots
-    // are found while the current piece's items run.
+    // regardless of layer boundaries.  A piece's records arrive by bulk copy
+    // (issued while the previous piece's items ran), are turned into
+    // weights here, and the next piece's copies and table cells are started
+    // before this piece's items run.
     int pf_lo[R], pf_s[R];
     int L = 0;  // layer whose particles the items add next
     for (int p0 = 0; p0 < total; p0 += SL) {
       const int p1 = min(p0 + SL, total);
+      if (BULK) {
+        mbar_wait(bs, phase, a.fault);
+        phase ^= 1u;
+      }
 #pragma unroll
       for (int r = 0; r < R; r++) {
         const int j = p0 + tid + r * NT;
         if (j < p1) {
-          int lo, s;
-          if (p0 > 0) {
-            lo = pf_lo[r];
-            s = pf_s[r];
+          const int lo = p0 > 0 ? pf_lo[r] : locate(j);
+          if (BULK) {
+            stage_one(lo, raw + (size_t)(j - p0) * R4, sweep_slot(j - p0));
           } else {
-            locate(j, lo, s);
+            float4 rc[5];
+            make_record<SF, false, PLANAR>(a, p0 > 0 ? pf_s[r] : slot_of(j, lo), rc);
+            stage_one(lo, rc, sweep_slot(j - p0));
           }
-          stage_one(lo, s, sweep_slot(j - p0));
         }
       }
       __syncthreads();
       if (p1 < total) {
         const int n1 = min(p1 + SL, total);
+        if (BULK) issue_piece<W::NS, R4>(a.B.rec, cell_k0, cell_pref, nrows, p1, n1, raw, bs);
 #pragma unroll
         for (int r = 0; r < R; r++) {
           const int j = p1 + tid + r * NT;
-          if (j < n1) locate(j, pf_lo[r], pf_s[r]);
+          if (j < n1) {
+            pf_lo[r] = locate(j);
+            if (!BULK) pf_s[r] = slot_of(j, pf_lo[r]);
+          }
         }
       }
       // ---- items: layers with particles before p1 add their part of the
@@ -1797,13 +1992,17 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 }
 
 // One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
-template <int SF, bool PLANAR>
+template <int SF, bool PLANAR, bool BULK>
 __global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
+  __shared__ BulkState bs;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
-  if (binning_failed(a.fault)) return;
+  if (binning_failed_cta(a.fault)) return;
+  if (threadIdx.x == 0) bulk_init(&bs);
+  __syncthreads();
+  unsigned phase = 0;
   for (int unit = next_tile(a, &cur); unit >= 0; unit = next_tile(a, &cur))
-    sweep3_tile<SF, PLANAR>(a, apply_bcs, node_epoch, unit);
+    sweep3_tile<SF, PLANAR, BULK>(a, apply_bcs, node_epoch, unit, &bs, phase);
 }
 
 // --------------------------------------------------------------------------
@@ -1834,16 +2033,22 @@ struct Dual3 {
   // Sxy, Syy), float4 (Sxz, Syz, Szz, Nz2), float4 (Nz0, Nz1, dNz0, dNz1),
   // with a PlanarDomain float4 (f, 0); S = -V sigma
   __host__ __device__ static constexpr int slot_bytes(bool planar) { return 6 * 8 + 4 * 16 + (planar ? 16 : 0); }
-  // staged particles: 227 KB of shared memory per CTA, less the static
-  // tables and the node accumulators
-  static constexpr int STATIC_BYTES = 8448;
-  __host__ __device__ static constexpr int cap(bool planar) {
-    return ((232448 - STATIC_BYTES - 7 * T::N * 4) / slot_bytes(planar)) & ~7;
+  // float4s of one P2G record (k_records), bulk-copied per row of dual cells
+  __host__ __device__ static constexpr int rec4(bool planar) { return planar ? 5 : 4; }
+  static constexpr int NROWS = NL * NS;  // rows of dual cells along x
+  // staged particles and their records: 227 KB of shared memory per CTA,
+  // less the static tables (with the copy barrier) and the node accumulators
+  static constexpr int STATIC_BYTES = 8704;
+  __host__ __device__ static constexpr int cap(bool planar, bool bulk) {
+    return ((232448 - STATIC_BYTES - 7 * T::N * 4) / (slot_bytes(planar) + (bulk ? 16 * rec4(planar) : 0))) & ~7;
   }
 };
 
-template <bool PLANAR>
-constexpr int dual3_smem_bytes() { return 7 * TileDims<3>::N * 4 + Dual3::cap(PLANAR) * Dual3::slot_bytes(PLANAR); }
+template <bool PLANAR, bool BULK>
+constexpr int dual3_smem_bytes() {
+  return 7 * TileDims<3>::N * 4 +
+         Dual3::cap(PLANAR, BULK) * (Dual3::slot_bytes(PLANAR) + (BULK ? 16 * Dual3::rec4(PLANAR) : 0));
+}
 
 // Staged slot of chunk position j: an XOR swizzle inside aligned groups of
 // eight, so lanes reading the same position of neighbouring cells (runs of
@@ -1894,13 +2099,18 @@ __device__ __forceinline__ void tile_epilogue3(const StepArgs &a, int apply_bcs,
 }
 
 // PLANAR: the handle has a PlanarDomain (per-particle external forces to map)
-template <bool PLANAR>
-__device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile) {
+// BULK: a piece's particles arrive as sorted records by bulk copy (k_records
+// wrote them); otherwise each is gathered through the sorted order.
+// bs / phase: the CTA's copy state and the parity of its barrier's next phase
+template <bool PLANAR, bool BULK>
+__device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int *node_epoch, int tile,
+                                           BulkState *bs, unsigned &phase) {
   using W = Dual3;
   using T = TileDims<3>;
   constexpr int NT = W::NT;
   constexpr int NN = T::N;  // nodes per tile
-  constexpr int CAP = W::cap(PLANAR);
+  constexpr int CAP = W::cap(PLANAR, BULK);
+  constexpr int R4 = W::rec4(PLANAR);
   const DevGrid &g = a.g;
 
   __shared__ int pairs_x[W::MAXPAIR], pairs_y[W::MAXPAIR];
@@ -1917,6 +2127,7 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   float4 *st_s1 = st_s0 + CAP;                                     // (Sxz, Syz, Szz, Nz2)
   float4 *st_z = st_s1 + CAP;                                      // (Nz0, Nz1, dNz0, dNz1)
   float4 *st_f = st_z + CAP;                                       // PLANAR: (f, 0)
+  float4 *raw = (float4 *)((char *)acc + 7 * NN * 4 + CAP * W::slot_bytes(PLANAR));  // BULK: [CAP][R4] records
 
   const int tid = threadIdx.x;
   const int t0[3] = {(tile % g.tdim[0]) * T::X, ((tile / g.tdim[0]) % g.tdim[1]) * T::Y,
@@ -1932,8 +2143,6 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   const int nx = npair[0], ny = npair[1];
   const int nitems = nx * ny;
   const int dz_lo = max(t0[2] - 1, 0), dz_hi = min(t0[2] + T::Z, g.n[2]);
-  const DevParticles &P = a.P;
-  const int st = P.stride;
   const int kd0 = a.B.kd[0];
   const long long kd01 = (long long)a.B.kd[0] * a.B.kd[1];
 
@@ -1997,16 +2206,14 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
 
   // The tile's particles, all layers in z order, are positions
   // 0 .. cell_pref[ntab] of the table; they are staged in pieces of CAP
-  // positions regardless of layer boundaries.  Table cell and storage slot
-  // of position j:
-  auto locate = [&](int j, int &lo, int &s) {
-    lo = 0;
-    int hi = ntab;
+  // positions regardless of layer boundaries.  Table cell of position j:
+  auto locate = [&](int j) {
+    int lo = 0, hi = ntab;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
       if (cell_pref[mid] <= j) lo = mid; else hi = mid;
     }
-    s = a.B.order[cell_k0[lo] + (j - cell_pref[lo])];
+    return lo;
   };
   // ---- node dz_lo + L - 1 gets nothing from layers after L: flush, shift ----
   auto flush_shift = [&](int L) {
@@ -2040,33 +2247,43 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
 
   const int nlayers = dz_hi - dz_lo + 1;
   const int total = cell_pref[ntab];
-  // positions tid + r NT of the next piece, found (cell search and the
-  // sorted-order gather) while the current piece's items run
+  const int nrows = nlayers * W::NS;
+  // table cells of positions tid + r NT of the next piece, found while the
+  // current piece's items run; the next piece's records are copied in then
   constexpr int R = (CAP + NT - 1) / NT;
   int pf_lo[R], pf_s[R];
+  // storage slot of list position j (table cell lo), for the gathered staging
+  auto slot_of = [&](int j, int lo) { return a.B.order[cell_k0[lo] + (j - cell_pref[lo])]; };
   int L = 0;  // layer whose particles the items add next
+  if (BULK && total > 0)
+    issue_piece<W::NS, R4>(a.B.rec, cell_k0, cell_pref, nrows, 0, min(CAP, total), raw, bs);
   for (int p0 = 0; p0 < total; p0 += CAP) {
     const int p1 = min(p0 + CAP, total);
-    // ---- stage positions [p0, p1) ----
+    if (BULK) {
+      mbar_wait(bs, phase, a.fault);
+      phase ^= 1u;
+    }
+    // ---- stage positions [p0, p1) from their records ----
 #pragma unroll
     for (int r = 0; r < R; r++) {
       const int j = p0 + tid + r * NT;
       if (j < p1) {
-        int lo, s;
-        if (p0 > 0) {
-          lo = pf_lo[r];
-          s = pf_s[r];
-        } else {
-          locate(j, lo, s);
-        }
+        const int lo = p0 > 0 ? pf_lo[r] : locate(j);
+        float4 own[5];
+        const float4 *rc = own;
+        if (BULK)
+          rc = raw + (size_t)(j - p0) * R4;
+        else
+          make_record<PMPM_SHAPE_QUADRATIC, true, PLANAR>(a, p0 > 0 ? pf_s[r] : slot_of(j, lo), own);
         const int jj = dual_slot(j - p0);
         // the particle's dual cell: its nodes are d - 1 .. d + 1 per axis
         const int layer = lo / W::NCELL, vc = lo - layer * W::NCELL;
         const int dz = dz_lo + layer;
         const int sx = t0[0] - 1 + vc % W::NS, sy = t0[1] - 1 + vc / W::NS;
-        const float ux = scaled_coord(P.x[s], g.origin[0], g.inv_h);
-        const float uy = scaled_coord(P.x[st + s], g.origin[1], g.inv_h);
-        const float uz = scaled_coord(P.x[2 * st + s], g.origin[2], g.inv_h);
+        const float4 xp = rc[3];
+        const float ux = scaled_coord(xp.x, g.origin[0], g.inv_h);
+        const float uy = scaled_coord(xp.y, g.origin[1], g.inv_h);
+        const float uz = scaled_coord(xp.z, g.origin[2], g.inv_h);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
           float N, dN;
@@ -2078,28 +2295,26 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
         float Nz[3], dNz[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) axis_weight<PMPM_SHAPE_QUADRATIC>(uz - (float)(dz - 1 + k), g.inv_h, 0, Nz[k], dNz[k]);
-        const float m = P.m[s];
-        const float nv = a.remap ? 0.0f : -P.V[s];
-        st_p[jj] = make_float4(m, m * P.v[s], m * P.v[st + s], m * P.v[2 * st + s]);
-        const float Sxx = nv * P.sig[s], Syy = nv * P.sig[st + s], Szz = nv * P.sig[2 * st + s];
-        const float Sxy = nv * P.sig[3 * st + s], Sxz = nv * P.sig[4 * st + s], Syz = nv * P.sig[5 * st + s];
-        st_s0[jj] = make_float4(Sxx, Sxy, Sxy, Syy);
-        st_s1[jj] = make_float4(Sxz, Syz, Szz, Nz[2]);
+        // (m, m v), -V sigma as (xx, xy, xy, yy) (xz, yz, zz, -), f_ext: k_records
+        st_p[jj] = rc[0];
+        st_s0[jj] = rc[1];
+        const float4 s1 = rc[2];
+        st_s1[jj] = make_float4(s1.x, s1.y, s1.z, Nz[2]);
         st_z[jj] = make_float4(Nz[0], Nz[1], dNz[0], dNz[1]);
-        if (PLANAR) {
-          const bool use = !a.remap;
-          st_f[jj] = make_float4(use ? P.fext[s] : 0.0f, use ? P.fext[st + s] : 0.0f,
-                                 use ? P.fext[2 * st + s] : 0.0f, 0.0f);
-        }
+        if (PLANAR) st_f[jj] = rc[4];
       }
     }
     __syncthreads();
     if (p1 < total) {
       const int n1 = min(p1 + CAP, total);
+      if (BULK) issue_piece<W::NS, R4>(a.B.rec, cell_k0, cell_pref, nrows, p1, n1, raw, bs);
 #pragma unroll
       for (int r = 0; r < R; r++) {
         const int j = p1 + tid + r * NT;
-        if (j < n1) locate(j, pf_lo[r], pf_s[r]);
+        if (j < n1) {
+          pf_lo[r] = locate(j);
+          if (!BULK) pf_s[r] = slot_of(j, pf_lo[r]);
+        }
       }
     }
     // ---- items: layers with particles before p1 add their part of the piece;
@@ -2184,13 +2399,17 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   tile_epilogue3(a, apply_bcs, t0, acc, tid, NT);
 }
 // One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
-template <bool PLANAR>
+template <bool PLANAR, bool BULK>
 __global__ void __launch_bounds__(Dual3::NT, 1) k_p2g_dual3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
+  __shared__ BulkState bs;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
-  if (binning_failed(a.fault)) return;
+  if (binning_failed_cta(a.fault)) return;
+  if (threadIdx.x == 0) bulk_init(&bs);
+  __syncthreads();
+  unsigned phase = 0;
   for (int tile = next_tile(a, &cur); tile >= 0; tile = next_tile(a, &cur))
-    dual3_tile<PLANAR>(a, apply_bcs, node_epoch, tile);
+    dual3_tile<PLANAR, BULK>(a, apply_bcs, node_epoch, tile, &bs, phase);
 }
 
 // --------------------------------------------------------------------------

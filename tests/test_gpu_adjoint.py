@@ -120,7 +120,7 @@ def directional_checks(scene, E, phi, steps, every, names, tol, eps=1e-4):
 
 def test_adjoint_smooth_rollout_matches_fp64_finite_differences():
     scene, E, phi, _ = flight_cube()
-    directional_checks(scene, E, phi, 16, 5, ("E", "x0", "v0"), 1e-3)
+    directional_checks(scene, E, phi, 16, 5, ("E", "x0", "v0"), 1e-4)
 
 
 @pytest.mark.parametrize("steps,every", [(4, 1), (16, 5)])

@@ -30,11 +30,11 @@ def bench_scene(config):
     return scenes.granular_column() if config == "column" else scenes.granular_bed()
 
 
-def gpu_run(scene, steps):
+def gpu_run(scene, steps, allowed=(0,)):
     sim = Simulation(**scenes.sim_kwargs(scene))
     sim.set_particles(scene["positions"], scene["velocities"]).initialize()
     sim.solve(steps)
-    assert sim.synchronize() == 0
+    assert sim.synchronize() in allowed
     return sim
 
 
@@ -73,9 +73,12 @@ def test_two_disc_impact_3000_steps_vs_fp64():
     the soft impact with 99 % FLIP amplifies rounding, so the FP32 reference
     arithmetic itself ends far from FP64 (the FP32 oracle: positions ~5e-3,
     velocities O(1)); the GPU must stay within three times that distance
-    per field, and within 1e-3 on positions."""
+    per field, and within 1e-3 on positions.  After the rebound the discs
+    reach the edges of the grid (no walls in this configuration), which the
+    step reports as PMPM_ERR_OUT_OF_DOMAIN while it goes on as the oracle
+    does."""
     scene = scenes.two_discs()
-    sim = gpu_run(scene, 3000)
+    sim = gpu_run(scene, 3000, allowed=(0, 16))
     r64 = oracle_run(scene, 3000, "f64")
     r32 = oracle_run(scene, 3000, "f32")
     for name in DRIFT_FIELDS:

@@ -569,6 +569,8 @@ def test_autotune_keeps_state_and_both_variants_match_oracle():
     before = {n: sim.get(n) for n in ("positions", "velocities", "stresses", "F")}
     v = sim.autotune(3)
     assert v in (0, 1)
+    t = sim.tuning()
+    assert t["p2g_kernel"] == v and t["staging"] in (0, 1) and t["resort_interval"] in (8, 16, 32, 64, 128)
     for n, a in before.items():
         np.testing.assert_array_equal(sim.get(n), a)
     assert sim.step == 0
@@ -620,5 +622,48 @@ def test_each_3d_quadratic_p2g_kernel_matches_oracle(variant):
     sim.solve(2)
     ref.solve(2)
     tol = cond_tol(scene, 2, FIELDS, STEP_TOL)
+    for name in FIELDS:
+        assert rel(sim.get(name), ref[name]) <= tol[name], name
+
+
+@pytest.mark.parametrize("staging", [0, 1])
+@pytest.mark.parametrize("case", ["column_3d_quadratic_dp", "random_3d_cubic_le_gravity", "sdf_3d_cubic_shell",
+                                  "random_3d_linear_nf_planar", "sdf_3d_linear_shell_stick"])
+def test_each_p2g_staging_matches_oracle(case, staging):
+    """The 3D sweeps' two stagings (bulk copies of sorted records 1, gather
+    through the sorted order 0), selected directly, against the oracle over
+    two steps, across re-sorts (interval 1) and with a PlanarDomain."""
+    scene = STEP_CASES[case]()
+    sim, ref = make_pair(scene, resort_interval=1)
+    sim.set_p2g_staging(staging)
+    sim.initialize()
+    ref.initialize()
+    sim.solve(2)
+    ref.solve(2)
+    assert sim.synchronize() == 0
+    tol = cond_tol(scene, 2, FIELDS, STEP_TOL)
+    for name in FIELDS:
+        assert rel(sim.get(name), ref[name]) <= tol[name], name
+
+
+def test_autotune_picks_staging_and_resort_interval_on_cubic():
+    """On a cubic sweep the autotuner chooses the staging and the re-sort
+    interval and leaves the state as it was."""
+    scene = STEP_CASES["random_3d_cubic_le_gravity"]()
+    sim, ref = make_pair(scene)
+    sim.initialize()
+    sim.solve(1)
+    ref.initialize()
+    ref.solve(1)
+    before = {n: sim.get(n) for n in ("positions", "velocities", "stresses", "F")}
+    sim.autotune(2)
+    t = sim.tuning()
+    assert t["staging"] in (0, 1) and t["resort_interval"] in (8, 16, 32, 64, 128)
+    for n, a in before.items():
+        np.testing.assert_array_equal(sim.get(n), a)
+    assert sim.step == 1
+    sim.solve(2)
+    ref.solve(2)
+    tol = cond_tol(scene, 3, FIELDS, STEP_TOL)
     for name in FIELDS:
         assert rel(sim.get(name), ref[name]) <= tol[name], name
