@@ -78,11 +78,16 @@ def calibrate(sim: Simulation, target: torch.Tensor, youngs0, friction0, nsteps:
     opt = torch.optim.Adam([{"params": [logE], "lr": lr_log_youngs}, {"params": [phi], "lr": lr_friction}])
     losses = []
     n = target.shape[0]
+    scale = None
     for _ in range(iterations):
         opt.zero_grad()
         x = rollout(sim, torch.exp(logE), phi, nsteps, checkpoint_every)
         loss = ((x.double() - target.double()) ** 2).sum() / n
-        loss.backward()
+        # the loss (m^2) and its per-particle gradients are tiny; scaled by
+        # the first loss, the gradients stay far above Adam's epsilon
+        if scale is None:
+            scale = 1.0 / max(float(loss.item()), 1e-300)
+        (loss * scale).backward()
         opt.step()
         losses.append(float(loss.item()))
     return torch.exp(logE).detach(), phi.detach(), losses

@@ -815,7 +815,11 @@ template <int D>
 __global__ void __launch_bounds__(128) kadj_g2p(StepArgs a, AdjState A) {
   __shared__ int box[6];
   __shared__ float acc[kAdjBoxNodes * 6];
-  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  // Storage sorted by cell keeps a cell's particles (8 on a 2x2x2 lattice)
+  // together; thread t takes particle (t % 16) * 8 + t / 16 of the CTA's
+  // 128, so a warp's lanes spread over 16 cells and their shared-memory
+  // atomics on the nodes those cells share collide two ways instead of eight.
+  const int s0 = blockIdx.x * 128 + (threadIdx.x & 15) * 8 + (threadIdx.x >> 4);
   const DevParticles &P = a.P;
   const bool valid = s0 < P.n;
   const int s = valid ? s0 : P.n - 1;

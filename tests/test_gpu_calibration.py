@@ -22,13 +22,17 @@ def test_calibration_loss_falls_and_parameters_move_to_target():
     kw = scenes.sim_kwargs(scene)
     tgt = Simulation(**kw)
     tgt.set_particles(scene["positions"], scene["velocities"]).initialize()
-    tgt.solve(nsteps)  # the material's own parameters: E = 10 MPa, 30 deg
+    n = len(scene["positions"])
+    tgt.set("youngs_modulus", np.full(n, tE, np.float32))
+    tgt.set("friction_angle", np.full(n, tphi, np.float32))
+    tgt.rollout_forward(nsteps, every)  # the same stepping as the calibration's rollouts
     assert tgt.synchronize() == 0
     target = torch.tensor(tgt.get("positions"), device="cuda")
     tgt.close()
     sim = Simulation(**kw)
     sim.set_particles(scene["positions"], scene["velocities"]).initialize()
-    E, phi, losses = calibrate(sim, target, E0, phi0, nsteps, every, iterations=40)
+    E, phi, losses = calibrate(sim, target, E0, phi0, nsteps, every, iterations=40, lr_log_youngs=0.1,
+                               lr_friction=1.0)
     assert sim.synchronize() == 0
     hist = ", ".join(f"{v:.3e}" for v in losses[::5])
     assert losses[-1] <= 0.1 * losses[0], hist
