@@ -566,7 +566,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
     }
     a.p2g_par = (int)(s->p2g_seq++ & 1u);
     const int grid = std::min(s->g.ntiles, s->num_sms);
-    constexpr int NT3 = TileDims<3>::N;
+    constexpr int NT3 = Sweep3<SF>::NT;
     if (s->p2g_staging) {
       if (s->has_planar)
         k_p2g_sweep3<SF, true, true><<<grid, NT3, sweep3_smem_bytes<SF, true, true>(), s->stream>>>(a, apply_bcs,

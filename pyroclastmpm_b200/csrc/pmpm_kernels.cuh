@@ -1525,8 +1525,8 @@ struct Sweep3 {
   static constexpr int TZ = 2 * T::Z;                // nodes along z of a work unit (two tiles)
   static constexpr int NN = T::X * T::Y * TZ;        // nodes of a work unit
   static constexpr int NL = TZ + WIN - 1;            // source layers a unit reads
-  static constexpr int NT = T::N;
-  static constexpr int IPT = 2;                      // items per thread per round
+  static constexpr int NT = 1024;
+  static constexpr int IPT = 1;                      // items per thread per round
   static constexpr int NZ4 = (2 * WIN + 3) / 4;     // float4s of z weights
   // staged floats per particle: the x and y weights of the WIN offsets
   // (float2 N, dN each), float4 (m, m vx, m vy, m vz), float4 (Sxx, Sxy, Sxy,
@@ -1993,7 +1993,7 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 
 // One persistent CTA pass over the active-tile queue (grid: 1 CTA per SM).
 template <int SF, bool PLANAR, bool BULK>
-__global__ void __launch_bounds__(512, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
+__global__ void __launch_bounds__(Sweep3<SF>::NT, 1) k_p2g_sweep3(StepArgs a, int apply_bcs, int *node_epoch) {
   __shared__ int cur;
   __shared__ BulkState bs;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.N.tile_queue[2 + (a.p2g_par ^ 1)] = 0;  // the next launch's counter
