@@ -610,9 +610,11 @@ int launch_g2p(pmpm_sim *s, int do_stress, int store_L, bool bin_next = false) {
   a.bin_next = bin_next ? 1 : 0;
   a.hash_next = s->hash_next;
   if (s->has_vm || s->has_mcc)
-    k_g2p<D, SF, true><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
+    k_g2p<D, SF, true><<<blocks_for(s->n, G2PLaunch<D, SF, true>::NT), G2PLaunch<D, SF, true>::NT, 0, s->stream>>>(
+        a, do_stress, store_L);
   else
-    k_g2p<D, SF, false><<<blocks_for(s->n), kTPB, 0, s->stream>>>(a, do_stress, store_L);
+    k_g2p<D, SF, false><<<blocks_for(s->n, G2PLaunch<D, SF, false>::NT), G2PLaunch<D, SF, false>::NT, 0,
+                          s->stream>>>(a, do_stress, store_L);
   PMPM_LAUNCHED();
   s->launches += 1;
   s->rigid_shift_pending = false;

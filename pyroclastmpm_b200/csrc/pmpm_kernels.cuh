@@ -2987,8 +2987,19 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 // bin_next (quadratic, dual binning): the step's last G2P also bins the
 // new positions for the next partition (counts, slots, keys, tile and brick
 // marks of epoch + 1), which then skips its binning pass.
+// Threads per block and blocks per SM of k_g2p: the 3D cubic gather runs
+// 128-thread blocks, five per SM at up to 102 registers (20 warps; 256-thread
+// blocks fit two at 128 registers, 16 warps)
 template <int D, int SF, bool FULL>
-__global__ void __launch_bounds__(256, FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4)) k_g2p(StepArgs a, int do_stress, int store_L) {
+struct G2PLaunch {
+  static constexpr bool SMALL = D == 3 && SF == PMPM_SHAPE_CUBIC && !FULL;
+  static constexpr int NT = SMALL ? 128 : 256;
+  static constexpr int MIN_BLOCKS = SMALL ? 5 : (FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4));
+};
+
+template <int D, int SF, bool FULL>
+__global__ void __launch_bounds__(G2PLaunch<D, SF, FULL>::NT, G2PLaunch<D, SF, FULL>::MIN_BLOCKS)
+    k_g2p(StepArgs a, int do_stress, int store_L) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < a.P.n) g2p_body<D, SF, FULL>(a, s, do_stress, store_L);
   if constexpr (SF == PMPM_SHAPE_QUADRATIC) {
