@@ -2737,10 +2737,18 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 #pragma unroll
   for (int k = 0; k < 9; k++) L[k] = 0.0f;
   // F is loaded before the stencil gather so that its DRAM latency overlaps
-  // the node loads
+  // the node loads; the cubic 3D gather instead requests it into L2 and
+  // loads it after the gather (nine registers fewer while the stencil's
+  // loads are in flight)
+  constexpr bool F_LATE = D == 3 && SF == PMPM_SHAPE_CUBIC;
   float F[9];
+  if constexpr (F_LATE) {
 #pragma unroll
-  for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
+    for (int k = 0; k < D * D; k++) prefetch_l2(P.F + k * st + s);
+  } else {
+#pragma unroll
+    for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
+  }
   // 3D: the state the stress update reads after the gather is requested
   // into L2 now (no registers held), so its DRAM latency overlaps the gather
   // too (column G2P 0.104 -> 0.098 ms; the batched 2D G2P ran 6 % slower
@@ -2942,6 +2950,10 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
       return;
     }
     // v <- (1 - alpha) v_pic + alpha (v + dv); x += dt v_pic; F <- (I + L dt) F; V = det(F) V0
+    if constexpr (F_LATE) {
+#pragma unroll
+      for (int k = 0; k < D * D; k++) F[k] = P.F[k * st + s];
+    }
     float A[9], Fn[9];
 #pragma unroll
     for (int r = 0; r < D; r++)

