@@ -3000,13 +3000,14 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 // new positions for the next partition (counts, slots, keys, tile and brick
 // marks of epoch + 1), which then skips its binning pass.
 // Threads per block and blocks per SM of k_g2p: the 3D cubic gather runs
-// 128-thread blocks, five per SM at up to 102 registers (20 warps; 256-thread
-// blocks fit two at 128 registers, 16 warps)
+// 128-thread blocks, six per SM at up to 80 registers (24 warps; a few bytes
+// spill, and F is loaded after the gather; 256-thread blocks fit two at 128
+// registers, 16 warps)
 template <int D, int SF, bool FULL>
 struct G2PLaunch {
   static constexpr bool SMALL = D == 3 && SF == PMPM_SHAPE_CUBIC && !FULL;
   static constexpr int NT = SMALL ? 128 : 256;
-  static constexpr int MIN_BLOCKS = SMALL ? 5 : (FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4));
+  static constexpr int MIN_BLOCKS = SMALL ? 6 : (FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4));
 };
 
 template <int D, int SF, bool FULL>
