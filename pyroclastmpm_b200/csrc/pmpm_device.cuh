@@ -215,6 +215,28 @@ __constant__ float kCubicD[5][4][3] = {
     {{0.5f, 2.0f, 2.0f}, {-1.5f, -2.0f, 0.0f}, {1.0f, -2.0f, 0.0f}, {0, 0, 0}},
 };
 
+// The four cubic weights of one axis where all four nodes b - 1 .. b + 2 of a
+// particle at u = b + t (t in [0, 1)) are of interior type 3, with their
+// derivatives times inv_h, evaluated together from t and s = 1 - t.  They
+// are the type-3 pieces of the table above (src/shapefunction/cubic.cuh:
+// 28-197) at r = t + 1, t, t - 1, t - 2: (2 - r)^3 / 6 = s^3 / 6,
+// r^3 / 2 - r^2 + 2/3, -r^3 / 2 - r^2 + 2/3 = s^3 / 2 - s^2 + 2/3 and
+// (2 + r)^3 / 6 = t^3 / 6 (derivatives -s^2 / 2, 1.5 t^2 - 2t,
+// 2s - 1.5 s^2, t^2 / 2); the same polynomials, FP32 rounding apart.
+__device__ __forceinline__ void cubic_interior_weights(float t, float inv_h, float N[4], float dN[4]) {
+  const float s = 1.0f - t;
+  const float t2 = t * t, s2 = s * s;
+  const float t3 = t2 * t, s3 = s2 * s;
+  N[0] = s3 * (1.0f / 6.0f);
+  N[1] = fmaf(0.5f, t3, (2.0f / 3.0f) - t2);
+  N[2] = fmaf(0.5f, s3, (2.0f / 3.0f) - s2);
+  N[3] = t3 * (1.0f / 6.0f);
+  dN[0] = (-0.5f * s2) * inv_h;
+  dN[1] = fmaf(1.5f, t2, -2.0f * t) * inv_h;
+  dN[2] = fmaf(-1.5f, s2, 2.0f * s) * inv_h;
+  dN[3] = (0.5f * t2) * inv_h;
+}
+
 // Weight and derivative of one axis for relative coordinate r (in cells).
 // linear: src/shapefunction/linear.cuh:28-52 (derivative 0 at r == 0);
 // quadratic: uniform C1 quadratic B-spline of support 3h;

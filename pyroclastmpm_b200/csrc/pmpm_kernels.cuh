@@ -1758,6 +1758,22 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     for (int k = 0; k < 4 * W::NZ4; k++) zf[k] = 0.0f;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
+      if (SF == PMPM_SHAPE_CUBIC && u[c] >= 0.0f && src[c] + W::LO >= 2 && src[c] + W::LO + 3 <= g.n[c] - 2) {
+        // all four targets are interior nodes (type 3) and the source cell
+        // is the particle's own: the four weights together
+        float N4[4], dN4[4];
+        cubic_interior_weights(u[c] - (float)b[c], g.inv_h, N4, dN4);
+#pragma unroll
+        for (int k = 0; k < WIN; k++) {
+          if (c == 0) st_wx[k][jj] = make_float2(N4[k], dN4[k]);
+          else if (c == 1) st_wy[k][jj] = make_float2(N4[k], dN4[k]);
+          else {
+            zf[k] = N4[k];
+            zf[WIN + k] = dN4[k];
+          }
+        }
+        continue;
+      }
 #pragma unroll
       for (int k = 0; k < WIN; k++) {
         const int tgt = src[c] + k + W::LO;
@@ -2787,6 +2803,16 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
     for (int c = 0; c < D; c++) {
       int w0 = Stencil<SF>::WLO;
       if (SF == PMPM_SHAPE_QUADRATIC) w0 = (u[c] - (float)(b[c] - 1)) < 1.5f ? -1 : 0;
+      if (SF == PMPM_SHAPE_CUBIC && b[c] - 1 >= 2 && b[c] + 2 <= g.n[c] - 2) {
+        // four interior nodes (type 3): the four weights together
+        cubic_interior_weights(u[c] - (float)b[c], g.inv_h, N[c], dN[c]);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          idx[c][k] = b[c] - 1 + k;
+          ok[c][k] = true;
+        }
+        continue;
+      }
 #pragma unroll
       for (int k = 0; k < K; k++) {
         const int sel = b[c] + w0 + k;
