@@ -1610,11 +1610,26 @@ __device__ __forceinline__ int build_pairs(int t0, int n, int *pairs) {
       if (SF == PMPM_SHAPE_QUADRATIC) t = min(max(t, 0), n - 1);
       const int l = t - t0;
       if (l < 0 || l >= TS || t >= n || t < 0) continue;
-      pairs[cnt++] = si | (i << 8) | (l << 12);
+      pairs[cnt++] = si | (i << 8) | (l << 12) | (1 << 16);
     }
   }
   return cnt;
 }
+
+// Linear and cubic: every (target column l, stencil offset i) of the unit in
+// target-major order, 8 WIN entries, so that the WIN pairs adding into one
+// target are neighbouring work items (neighbouring lanes of a warp); the
+// source column is l - i - LO + HI; bit 16 marks a target inside the grid.
+template <int SF>
+__device__ __forceinline__ int build_pairs_by_target(int t0, int n, int *pairs) {
+  using W = Sweep3<SF>;
+  int cnt = 0;
+  for (int l = 0; l < W::T::X; l++)
+    for (int i = 0; i < W::WIN; i++)
+      pairs[cnt++] = (l - i - W::LO + W::HI) | (i << 8) | (l << 12) | (t0 + l < n ? 1 << 16 : 0);
+  return cnt;
+}
+__device__ __forceinline__ bool pair_valid(int p) { return (p >> 16) & 1; }
 
 // Staged slot of piece position j: an XOR swizzle inside aligned groups of
 // eight, so lanes reading the same position of neighbouring cells (runs of
@@ -1663,9 +1678,11 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
   if (tid == 0) {
     node_epoch[col + tz0 * plane] = a.epoch;
     if (tz0 + 1 < g.tdim[2]) node_epoch[col + (tz0 + 1) * plane] = a.epoch;
-    npair[0] = build_pairs<SF>(t0[0], g.n[0], pairs_x);
+    npair[0] = SF == PMPM_SHAPE_QUADRATIC ? build_pairs<SF>(t0[0], g.n[0], pairs_x)
+                                          : build_pairs_by_target<SF>(t0[0], g.n[0], pairs_x);
   } else if (tid == 32) {
-    npair[1] = build_pairs<SF>(t0[1], g.n[1], pairs_y);
+    npair[1] = SF == PMPM_SHAPE_QUADRATIC ? build_pairs<SF>(t0[1], g.n[1], pairs_y)
+                                          : build_pairs_by_target<SF>(t0[1], g.n[1], pairs_y);
   }
   __syncthreads();
   const int nx = npair[0], ny = npair[1];
@@ -1817,9 +1834,10 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
       const int it = (round * W::IPT + q) * NT + tid;
-      item_ok[q] = it < nitems;
-      const int px = item_ok[q] ? pairs_x[it % nx] : 0;
-      const int py = item_ok[q] ? pairs_y[it / nx] : 0;
+      const bool in = it < nitems;
+      const int px = in ? pairs_x[it % nx] : 0;
+      const int py = in ? pairs_y[it / nx] : 0;
+      item_ok[q] = in && pair_valid(px) && pair_valid(py);
       item_cell[q] = pair_src(py) * W::NS + pair_src(px);
       item_ix[q] = pair_off(px);
       item_iy[q] = pair_off(py);
@@ -1832,24 +1850,37 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
         wz[q][k] = 0.0f;
       }
     }
-    auto add_node = [&](int q, int k, int ln) {
-      atomicAdd(&acc[ln], wa[q][k].x);
-      atomicAdd(&acc[NN + ln], wa[q][k].y);
-      atomicAdd(&acc[2 * NN + ln], wb[q][k].x);
-      atomicAdd(&acc[3 * NN + ln], wb[q][k].y);
-      atomicAdd(&acc[4 * NN + ln], wc[q][k].x);
-      atomicAdd(&acc[5 * NN + ln], wc[q][k].y);
-      atomicAdd(&acc[6 * NN + ln], wz[q][k]);
+    // Window node k of item q into the node accumulators at layer lz.  Called
+    // by every thread of the CTA at the same point.  Linear and cubic: the
+    // WIN lanes of one target column (neighbours, target-major pairs) sum
+    // their values with shuffles and one of them adds them: WIN times fewer
+    // shared-memory atomics, none colliding inside a warp.  Quadratic (its
+    // folded pairs are not target-major): one atomic per item.
+    constexpr bool REDUCE = SF != PMPM_SHAPE_QUADRATIC && W::IPT == 1;
+    auto add_node = [&](int q, int k, int lz) {
+      float v[7] = {wa[q][k].x, wa[q][k].y, wb[q][k].x, wb[q][k].y, wc[q][k].x, wc[q][k].y, wz[q][k]};
+      if (REDUCE) {
+#pragma unroll
+        for (int c = 0; c < 7; c++) {
+#pragma unroll
+          for (int o = 1; o < WIN; o <<= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+        }
+        if ((threadIdx.x & (WIN - 1)) != 0) return;
+      }
+      if (!item_ok[q]) return;
+      const int ln = item_tl[q] + T::X * T::Y * lz;
+#pragma unroll
+      for (int c = 0; c < 7; c++) atomicAdd(&acc[c * NN + ln], v[c]);
     };
     // ---- the lowest window node of layer L is complete: flush, shift ----
     auto flush_shift = [&](int L) {
 #pragma unroll
       for (int q = 0; q < W::IPT; q++) {
-        if (item_ok[q]) {
+        {
           int tz = cz_lo + L + W::LO;
           if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
           const int lz = tz - t0[2];
-          if (lz >= 0 && lz < TZ && tz < g.n[2]) add_node(q, 0, item_tl[q] + T::X * T::Y * lz);
+          if (lz >= 0 && lz < TZ && tz < g.n[2]) add_node(q, 0, lz);
         }
 #pragma unroll
         for (int k = 0; k < WIN - 1; k++) {
@@ -1972,13 +2003,12 @@ __device__ __forceinline__ void sweep3_tile(const StepArgs &a, int apply_bcs, in
     // ---- remaining window nodes after the last layer ----
 #pragma unroll
     for (int q = 0; q < W::IPT; q++) {
-      if (!item_ok[q]) continue;
 #pragma unroll
       for (int k = 0; k < WIN - 1; k++) {
         int tz = cz_hi + 1 + k + W::LO;
         if (SF == PMPM_SHAPE_QUADRATIC) tz = min(max(tz, 0), g.n[2] - 1);
         const int lz = tz - t0[2];
-        if (lz >= 0 && lz < TZ && tz < g.n[2]) add_node(q, k, item_tl[q] + T::X * T::Y * lz);
+        if (lz >= 0 && lz < TZ && tz < g.n[2]) add_node(q, k, lz);
       }
     }
   }
