@@ -403,6 +403,13 @@ int pmpm_set_wait_limit(pmpm_sim *sim, long long spins);
  * Diagnostic, no reference counterpart. */
 int pmpm_scan_tag(unsigned launch, unsigned *tag);
 
+/* The autotuner's re-sort interval rule (pmpm_autotune) on given timings:
+ * t_sort the time of one physical re-sort, step_ms[0 .. m) the times of m
+ * consecutive steps after it (ms); *interval gets the K in {8, 16, 32, 64,
+ * 128} minimising t_sort / K + slope K / 2.  Host only, no GPU work; no
+ * reference counterpart. */
+int pmpm_pick_resort_interval(float t_sort, const float *step_ms, int m, int *interval);
+
 /* Number of grid nodes with mass above the cutoff after the last P2G
  * (the nodes the step actually updates). */
 int pmpm_active_nodes(pmpm_sim *sim, int *count);
@@ -467,9 +474,10 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
  *    copies of sorted records, or a gather through the sorted order): each
  *    (kernel, staging) pair is timed on `steps` steps;
  *  - the re-sort interval (when it is not 0): one physical re-sort is timed,
- *    then the chosen kernels on max(16, 4 steps) steps without re-sorts; the
+ *    then the chosen kernels on max(48, 4 steps) steps without re-sorts; the
  *    interval in {8, 16, 32, 64, 128} minimising t_sort / K + slope K / 2
- *    (slope: the growth of the step time per step) is kept.
+ *    is kept (slope: the growth of the step time per step, fitted by least
+ *    squares, less two standard errors of the fit, at least 0).
  * The particle state and the step counter are put back afterwards.
  * *chosen: the P2G kernel (1 sweep, 0 cell scatter); pmpm_get_tuning reports
  * all choices. */

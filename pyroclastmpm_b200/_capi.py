@@ -87,7 +87,7 @@ EXPORTS = [
     "pmpm_rollout_forward", "pmpm_rollout_reset", "pmpm_rollout_backward", "pmpm_material_point_vjp",
     "pmpm_rollout_set_memory", "pmpm_musl_stage", "pmpm_material_von_mises", "pmpm_autotune",
     "pmpm_material_modified_cam_clay", "pmpm_material_drucker_prager_cap", "pmpm_set_p2g_kernel",
-    "pmpm_set_wait_limit", "pmpm_scan_tag", "pmpm_set_p2g_staging", "pmpm_set_resort_interval", "pmpm_get_tuning",
+    "pmpm_set_wait_limit", "pmpm_scan_tag", "pmpm_pick_resort_interval", "pmpm_set_p2g_staging", "pmpm_set_resort_interval", "pmpm_get_tuning",
 ]
 
 EXPORTS += [
@@ -184,6 +184,7 @@ def lib():
                                   ctypes.POINTER(ctypes.c_int)]
     L.pmpm_batch_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
     L.pmpm_scan_tag.argtypes = [ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)]
+    L.pmpm_pick_resort_interval.argtypes = [f, fp, i, ctypes.POINTER(ctypes.c_int)]
     L.pmpm_partition_noalloc.argtypes = [i, fp, f, ctypes.POINTER(ctypes.c_int), vp, i, vp, vp, vp, vp, vp]
     L.pmpm_material_point_update.argtypes = [ctypes.POINTER(Material), i, i, f, vp, vp, vp, vp, vp, vp, vp, i, i]
     _lib = L
@@ -195,6 +196,16 @@ def scan_tag(launch):
     t = ctypes.c_uint()
     check(lib().pmpm_scan_tag(ctypes.c_uint(launch & 0xffffffff), ctypes.byref(t)), "pmpm_scan_tag")
     return t.value
+
+
+def pick_resort_interval(t_sort, step_ms):
+    """The autotuner's re-sort interval for a re-sort time and the step times
+    after it (ms)."""
+    a = np.ascontiguousarray(step_ms, dtype=np.float32)
+    k = ctypes.c_int()
+    check(lib().pmpm_pick_resort_interval(ctypes.c_float(t_sort), a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          len(a), ctypes.byref(k)), "pmpm_pick_resort_interval")
+    return k.value
 
 
 def check(status, what):

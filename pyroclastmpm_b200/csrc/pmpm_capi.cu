@@ -3186,7 +3186,21 @@ int pick_resort_interval(float t_sort, const std::vector<float> &step_ms) {
     sxy += (double)i * step_ms[i];
   }
   const double den = m * sxx - sx * sx;
-  const double sigma = den > 0 ? std::max(0.0, (m * sxy - sx * sy) / den) : 0.0;
+  const double slope = den > 0 ? (m * sxy - sx * sy) / den : 0.0;
+  // the growth counts only beyond two standard errors of the fitted slope:
+  // step-to-step noise of a few microseconds otherwise reads as disorder
+  // growth and picks short intervals whose re-sorts cost more than they save
+  double se = 0.0;
+  if (den > 0 && m > 2) {
+    const double icpt = (sy - slope * sx) / m;
+    double rss = 0.0;
+    for (int i = 0; i < m; i++) {
+      const double r = step_ms[i] - (icpt + slope * i);
+      rss += r * r;
+    }
+    se = std::sqrt(rss / (m - 2) / (sxx - sx * sx / m));
+  }
+  const double sigma = std::max(0.0, slope - 2.0 * se);
   const int cands[] = {8, 16, 32, 64, 128};
   int best = 32;
   double best_cost = 1e300;
@@ -3201,6 +3215,12 @@ int pick_resort_interval(float t_sort, const std::vector<float> &step_ms) {
 }
 
 }  // namespace
+
+extern "C" int pmpm_pick_resort_interval(float t_sort, const float *step_ms, int m, int *interval) {
+  if (!step_ms || !interval || m < 1 || !(t_sort >= 0.0f)) return PMPM_ERR_INVALID_ARGUMENT;
+  *interval = pick_resort_interval(t_sort, std::vector<float>(step_ms, step_ms + m));
+  return PMPM_OK;
+}
 
 extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   if (!s || steps < 1) return PMPM_ERR_INVALID_ARGUMENT;
@@ -3275,7 +3295,7 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
       cudaEventElapsedTime(&t_sort, e0, e1);
     }
     if (st == PMPM_OK) {
-      const int nsample = std::max(16, 4 * steps);
+      const int nsample = std::max(48, 4 * steps);
       std::vector<cudaEvent_t> ev(nsample + 1);
       for (auto &e : ev) cudaEventCreate(&e);
       cudaEventRecord(ev[0], s->stream);

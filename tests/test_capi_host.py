@@ -98,3 +98,28 @@ def test_scan_tag_parity_alternates_across_the_wrap():
             if prev is not None:
                 assert (t & 1) != (prev & 1), (hex(launch), t, prev)
             prev = t
+
+
+def test_resort_interval_rule_ignores_noise_and_follows_real_growth():
+    """The autotuner's re-sort interval rule: step times that only scatter
+    (no growth beyond the noise of the fitted slope) keep the longest
+    interval, whatever the noise draws; a clear growth of the step time
+    after a re-sort picks the interval that balances it against the re-sort,
+    K = sqrt(2 t_sort / slope) rounded to the candidates."""
+    import numpy as np
+    from pyroclastmpm_b200 import _capi
+
+    rng = np.random.default_rng(7)
+    for _ in range(50):
+        flat = 1.71 + rng.normal(0.0, 0.01, 48)
+        assert _capi.pick_resort_interval(0.49, flat) == 128
+    steps = np.arange(48)
+    # slope 2e-3 ms per step: sqrt(2 * 0.49 / 2e-3) = 22 -> 16 or 32 by cost
+    grow = 1.70 + 2e-3 * steps + rng.normal(0.0, 0.002, 48)
+    k = _capi.pick_resort_interval(0.49, grow)
+    costs = {c: 0.49 / c + 2e-3 * c / 2 for c in (8, 16, 32, 64, 128)}
+    assert k == min(costs, key=costs.get)
+    # steep growth: the shortest candidate
+    assert _capi.pick_resort_interval(0.05, 1.7 + 0.05 * steps) == 8
+    with pytest.raises(_capi.PmpmError):
+        _capi.pick_resort_interval(0.49, [])
