@@ -233,22 +233,43 @@ __device__ __forceinline__ void mark_tiles(const StepArgs &a, const int b[3], un
   if (SF != PMPM_SHAPE_QUADRATIC && clipped && binned) {
     // slots leaving the grid on an axis: the reference's flat index check lets
     // them land on a node of a neighbouring row (src/solver/usl/usl_inline.h:114-126)
-    constexpr int NS = IPow<Stencil<SF>::WIN, D>::value;
-    for (int sid = 0; sid < NS; sid++) {
-      int w[3];
-      window_offset<D, SF>(sid, w);
-      // a slot inside the grid on every axis is its own node, whose tile the
-      // loop above marked (skipping them took the bed's binning pass from
-      // 0.23 to 0.19 ms: a warp holding a cell on a grid face walked all 64)
-      bool alias = false;
+    // A slot inside the grid on every axis is its own node, whose tile the
+    // loop above marked (skipping them took the bed's binning pass from 0.23
+    // to 0.19 ms: a warp holding a cell on a grid face walked all 64).  The
+    // node of an aliased slot's flat index: one carry per axis where that
+    // reproduces the index (the particle's own cell in the grid), else
+    // divisions.
+    constexpr int W = Stencil<SF>::WIN;
+    const int nxy = g.n[0] * g.n[1];
+    for (int wz = (D == 3 ? LO : 0); wz <= (D == 3 ? HI : 0); wz++) {
+      const bool zin = D == 2 || (b[2] + wz >= 0 && b[2] + wz < g.n[2]);
+      for (int wy = LO; wy < LO + W; wy++) {
+        const bool yin = b[1] + wy >= 0 && b[1] + wy < g.n[1];
 #pragma unroll
-      for (int c = 0; c < D; c++) alias = alias || b[c] + w[c] < 0 || b[c] + w[c] >= g.n[c];
-      if (!alias) continue;
-      int f = (int)hu + w[0] + w[1] * g.n[0] + w[2] * g.n[0] * g.n[1];
-      if ((unsigned)f >= (unsigned)g.ntotal) continue;
-      int c[3] = {f % g.n[0], (f / g.n[0]) % g.n[1], f / (g.n[0] * g.n[1])};
-      int t = tile_of<D>(g, c);
-      mark_tile(a, t, epoch);
+        for (int wx = LO; wx < LO + W; wx++) {
+          if (zin && yin && b[0] + wx >= 0 && b[0] + wx < g.n[0]) continue;
+          const int f = (int)hu + wx + wy * g.n[0] + wz * nxy;
+          if ((unsigned)f >= (unsigned)g.ntotal) continue;
+          int c[3] = {b[0] + wx, b[1] + wy, D == 3 ? b[2] + wz : 0};
+#pragma unroll
+          for (int k = 0; k < D - 1; k++) {
+            if (c[k] < 0) {
+              c[k] += g.n[k];
+              c[k + 1] -= 1;
+            } else if (c[k] >= g.n[k]) {
+              c[k] -= g.n[k];
+              c[k + 1] += 1;
+            }
+          }
+          if (c[0] < 0 || c[0] >= g.n[0] || c[1] < 0 || c[1] >= g.n[1] || c[2] < 0 ||
+              c[0] + c[1] * g.n[0] + c[2] * nxy != f) {
+            c[0] = f % g.n[0];
+            c[1] = (f / g.n[0]) % g.n[1];
+            c[2] = f / nxy;
+          }
+          mark_tile(a, tile_of<D>(g, c), epoch);
+        }
+      }
     }
   }
 }
