@@ -448,7 +448,7 @@ int launch_partition(pmpm_sim *s) {
   }
   PMPM_TRY(launch_scan(s->scan, s->B.count, s->nkeys, s->B.offset, s->B.scalars, s->fault, s->nscan_blocks, st));
   s->launches -= 2;  // one scan launch instead of three
-  k_scatter<<<blocks_for(s->n), kTPB, 0, st>>>(a);
+  k_scatter<<<blocks_for((s->n + kScatterPer - 1) / kScatterPer), kTPB, 0, st>>>(a);
   PMPM_LAUNCHED();
   // ids in order inside each bin: needed by the deterministic gather and by
   // the nearest-rigid-particle search (the reference's first minimum); the
@@ -2275,7 +2275,7 @@ int batch_partition(pmpm_batch *b) {
   b->launches += 1;
   const StepArgs ga = batch_global_args(b);
   PMPM_TRY(launch_scan(b->scan, b->B.count, b->nkeys, b->B.offset, b->B.scalars, b->fault, b->nscan_blocks, st));
-  k_scatter<<<blocks_for(b->n), kTPB, 0, st>>>(ga);
+  k_scatter<<<blocks_for((b->n + kScatterPer - 1) / kScatterPer), kTPB, 0, st>>>(ga);
   PMPM_LAUNCHED();
   b->launches += 2;
   if (b->flags & PMPM_FLAG_DETERMINISTIC) {  // ids in order inside each bin for the gather

@@ -577,16 +577,41 @@ __device__ __forceinline__ bool binning_failed(const int *fault) {
   return (*(volatile const int *)fault & kFaultWaitTimeout) != 0;
 }
 
+// Four consecutive particles per thread (kScatterPer): their slots and keys
+// in one 16-byte load each where aligned, so four offset gathers are in
+// flight per thread instead of one.
+constexpr int kScatterPer = 4;
 __global__ void __launch_bounds__(256) k_scatter(StepArgs a) {
   if (binning_failed(a.fault)) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.P.n) return;
-  const int slot = a.P.slot[s];
-  if (slot >= 0) {
-    a.B.order[a.B.offset[a.P.key[s]] + slot] = s;
+  const int s0 = (blockIdx.x * blockDim.x + threadIdx.x) * kScatterPer;
+  if (s0 >= a.P.n) return;
+  int slot[kScatterPer], key[kScatterPer];
+  const bool vec = s0 + kScatterPer <= a.P.n && ((reinterpret_cast<uintptr_t>(a.P.slot + s0) |
+                                                  reinterpret_cast<uintptr_t>(a.P.key + s0)) & 15) == 0;
+  if (vec) {
+    const int4 sv = *reinterpret_cast<const int4 *>(a.P.slot + s0);
+    const int4 kv = *reinterpret_cast<const int4 *>(a.P.key + s0);
+    slot[0] = sv.x; slot[1] = sv.y; slot[2] = sv.z; slot[3] = sv.w;
+    key[0] = kv.x; key[1] = kv.y; key[2] = kv.z; key[3] = kv.w;
   } else {
-    int k = atomicAdd(&a.B.scalars[1], 1);
-    a.B.order[a.B.scalars[0] + k] = s;
+#pragma unroll
+    for (int q = 0; q < kScatterPer; q++) {
+      const bool in = s0 + q < a.P.n;
+      slot[q] = in ? a.P.slot[s0 + q] : -2;
+      key[q] = in && slot[q] >= 0 ? (int)a.P.key[s0 + q] : 0;
+    }
+  }
+  int base[kScatterPer];
+#pragma unroll
+  for (int q = 0; q < kScatterPer; q++) base[q] = slot[q] >= 0 ? a.B.offset[key[q]] : 0;
+#pragma unroll
+  for (int q = 0; q < kScatterPer; q++) {
+    if (slot[q] >= 0) {
+      a.B.order[base[q] + slot[q]] = s0 + q;
+    } else if (s0 + q < a.P.n) {  // not binned
+      int k = atomicAdd(&a.B.scalars[1], 1);
+      a.B.order[a.B.scalars[0] + k] = s0 + q;
+    }
   }
 }
 
