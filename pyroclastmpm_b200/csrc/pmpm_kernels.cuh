@@ -2818,6 +2818,15 @@ __device__ __forceinline__ void stress_update_point(const StepArgs &a, int s, co
 
 __device__ __forceinline__ void prefetch_l2(const float *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
+// A 3D node's packed velocities (v, -), (v_nt, -) (32 bytes, 32-byte aligned:
+// two float4 per node from a 256-byte aligned allocation) in one 256-bit
+// read-only load (sm_100), where two 128-bit loads took two instructions.
+__device__ __forceinline__ void ldg_node8(const float4 *p, float4 &q0, float4 &q1) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(q0.x), "=f"(q0.y), "=f"(q0.z), "=f"(q0.w), "=f"(q1.x), "=f"(q1.y), "=f"(q1.z), "=f"(q1.w)
+      : "l"(p));
+}
+
 template <int D, int SF, bool FULL = true>
 __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress, int store_L) {
   const DevParticles &P = a.P;
@@ -2948,7 +2957,8 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
             const float2 n2 = make_float2(n, n), dn2 = make_float2(dn, dn);
             float2 vn2, vnt2;
             if (D == 3) {
-              const float4 q0 = __ldg(vel + 2 * (size_t)node), q1 = __ldg(vel + 2 * (size_t)node + 1);
+              float4 q0, q1;
+              ldg_node8(vel + 2 * (size_t)node, q0, q1);
               vn2 = make_float2(q0.x, q0.y);
               vnt2 = make_float2(q1.x, q1.y);
               svz = fmaf(n, q1.z, svz);
@@ -3012,7 +3022,8 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
             const int node = idx[0][kx] + row;
             float vn[3], vnt[3];
             if (D == 3) {
-              const float4 q0 = __ldg(vel + 2 * (size_t)node), q1 = __ldg(vel + 2 * (size_t)node + 1);
+              float4 q0, q1;
+              ldg_node8(vel + 2 * (size_t)node, q0, q1);
               vn[0] = q0.x; vn[1] = q0.y; vn[2] = q0.z;
               vnt[0] = q1.x; vnt[1] = q1.y; vnt[2] = q1.z;
             } else {
