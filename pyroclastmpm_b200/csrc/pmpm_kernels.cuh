@@ -3123,14 +3123,15 @@ __device__ __forceinline__ void g2p_body(const StepArgs &a, int s, int do_stress
 // new positions for the next partition (counts, slots, keys, tile and brick
 // marks of epoch + 1), which then skips its binning pass.
 // Threads per block and blocks per SM of k_g2p: the 3D cubic gather runs
-// 128-thread blocks, six per SM at up to 80 registers (24 warps; a few bytes
-// spill, and F is loaded after the gather; 256-thread blocks fit two at 128
-// registers, 16 warps)
+// 128-thread blocks, five per SM at up to 96 registers (20 warps, no spills;
+// F is loaded after the gather).  With the 256-bit node loads, six blocks at
+// 80 registers (28 bytes of spills) ran the bed's G2P 1 % slower and seven
+// at 72 (96 bytes) 13 % slower; 256-thread blocks fit two at 128 registers.
 template <int D, int SF, bool FULL>
 struct G2PLaunch {
   static constexpr bool SMALL = D == 3 && SF == PMPM_SHAPE_CUBIC && !FULL;
   static constexpr int NT = SMALL ? 128 : 256;
-  static constexpr int MIN_BLOCKS = SMALL ? 6 : (FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4));
+  static constexpr int MIN_BLOCKS = SMALL ? 5 : (FULL ? 2 : (SF == PMPM_SHAPE_CUBIC ? 2 : 4));
 };
 
 template <int D, int SF, bool FULL>
