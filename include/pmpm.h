@@ -483,7 +483,11 @@ int pmpm_partition_noalloc(int dim, const float *origin, float cell_size, const 
  * all choices. */
 int pmpm_autotune(pmpm_sim *s, int steps, int *chosen);
 /* Selects the P2G kernel directly (the autotuner's choices: 1 sweep, 0 cell
- * scatter); PMPM_ERR_NOT_SUPPORTED where the configuration has only one. */
+ * scatter); PMPM_ERR_NOT_SUPPORTED where the configuration has only one.
+ * The 3D quadratic sweep runs one work item per thread of its CTA (up to 640);
+ * on a grid with a node count divisible by 8 along x or y, the tiles ending at
+ * that face hold 27 (source, offset) pairs along it and more items than that,
+ * so such grids run the cell scatter and selecting the sweep is refused. */
 int pmpm_set_p2g_kernel(pmpm_sim *s, int variant);
 /* Staging of the 3D sweep P2G kernels: 1 (default) the particles of each
  * row of source cells arrive in shared memory by one bulk copy

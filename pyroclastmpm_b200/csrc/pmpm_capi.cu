@@ -187,6 +187,7 @@ struct pmpm_sim {
   int nkeys = 0;
   int nbricks = 0;     // dual-cell bricks (cell-scatter P2G)
   int p2g_variant = 1; // 3D quadratic: 0 cell scatter, 1 dual sweep (pmpm_autotune picks)
+  bool dual3_fits = true;  // every dual-sweep tile's work items fit the CTA's threads
   int p2g_staging = 1; // 3D sweeps: 1 bulk copies of sorted records, 0 gather through the order
   int num_sms = 1;       // persistent P2G grids: CTAs per SM x this
   // the last step's G2P binned the current positions for the next partition
@@ -502,7 +503,7 @@ int launch_p2g(pmpm_sim *s, int apply_bcs) {
                                      dual3_smem_bytes<true, false>()));
       attr_set[dev] = true;
     }
-    if (s->p2g_variant == 1) {
+    if (s->p2g_variant == 1 && s->dual3_fits) {
       // (bulk staging: sorted records of this partition's particles first)
       // persistent CTAs over the active-tile queue
       if (s->p2g_staging) {
@@ -1211,8 +1212,31 @@ int pmpm_material_timestep(const pmpm_material *mat, float cell_size, float fact
   }
 }
 
+// Most (dual source, offset) pairs of any tile along an axis of n nodes, as
+// the dual sweep builds them (build_dual_pairs): 24 inside the grid, 27 in a
+// tile of eight node columns ending at the last node, where the clamped
+// offsets of the face's dual cells fold onto that node (n a multiple of 8).
+static int dual_pairs_max(int n) {
+  int most = 0;
+  for (int t0 = 0; t0 < n; t0 += TileDims<3>::X) {
+    int cnt = 0;
+    for (int si = 0; si < Dual3::NS; si++) {
+      const int src = t0 - 1 + si;
+      if (src < 0 || src > n) continue;
+      for (int i = 0; i < 3; i++) {
+        const int l = std::min(std::max(src - 1 + i, 0), n - 1) - t0;
+        if (l >= 0 && l < TileDims<3>::X) cnt++;
+      }
+    }
+    most = std::max(most, cnt);
+  }
+  return most;
+}
+
 // Binning key space: reference cells, or dual cells (floor(x/h + 1/2), one
 // more per axis) for quadratic shape functions outside the deterministic mode.
+// The dual sweep runs one work item per thread of its CTA: where a tile has
+// more (27 pairs along x or y), the cell-row scatter P2G is used instead.
 static void set_key_space(pmpm_sim *s) {
   s->dual = s->shape == PMPM_SHAPE_QUADRATIC && !(s->flags & PMPM_FLAG_DETERMINISTIC);
   s->nkeys = 1;
@@ -1220,6 +1244,9 @@ static void set_key_space(pmpm_sim *s) {
     s->kd[c] = (s->dual && c < s->dim) ? s->g.n[c] + 1 : s->g.n[c];
     s->nkeys *= s->kd[c];
   }
+  s->dual3_fits = !(s->dual && s->dim == 3) ||
+                  dual_pairs_max(s->g.n[0]) * dual_pairs_max(s->g.n[1]) <= Dual3::NT * Dual3::IPT;
+  if (!s->dual3_fits) s->p2g_variant = 0;
 }
 
 // Descriptor -> handle parameters: grid, materials and boundary conditions
@@ -3144,6 +3171,7 @@ extern "C" int pmpm_material_point_vjp(const pmpm_material *mat, int dim, int n,
 extern "C" int pmpm_set_p2g_kernel(pmpm_sim *s, int variant) {
   if (!s || (variant != 0 && variant != 1)) return PMPM_ERR_INVALID_ARGUMENT;
   if (!s->dual || s->dim != 3) return PMPM_ERR_NOT_SUPPORTED;
+  if (variant == 1 && !s->dual3_fits) return PMPM_ERR_NOT_SUPPORTED;  // tiles with more items than threads
   s->p2g_variant = variant;
   return PMPM_OK;
 }
@@ -3228,7 +3256,7 @@ extern "C" int pmpm_autotune(pmpm_sim *s, int steps, int *chosen) {
   PMPM_CUDA(cudaSetDevice(s->device));
   // candidates: (P2G kernel, staging) pairs this configuration has
   std::vector<std::pair<int, int>> cands;
-  const bool dual3 = s->dual && s->dim == 3;
+  const bool dual3 = s->dual && s->dim == 3 && s->dual3_fits;
   const bool staged = s->B.rec != nullptr;
   for (int v : dual3 ? std::vector<int>{1, 0} : std::vector<int>{s->p2g_variant})
     for (int g : staged && v == 1 ? std::vector<int>{1, 0} : std::vector<int>{s->p2g_staging})

@@ -2283,6 +2283,9 @@ __device__ __forceinline__ void dual3_tile(const StepArgs &a, int apply_bcs, int
   }
   __syncthreads();
 
+  // one round of items covers a tile of up to 24 pairs per axis; grids whose
+  // face tiles have 27 (a node count divisible by 8 along x or y) run the
+  // cell-row scatter instead (the host's dual_pairs_max)
   static_assert(T::X * 3 * T::Y * 3 <= NT * W::IPT, "one round of items covers a tile");
   int item_cell[W::IPT], item_tl[W::IPT], item_ix[W::IPT], item_iy[W::IPT];
   bool item_ok[W::IPT];

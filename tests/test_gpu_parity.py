@@ -243,6 +243,12 @@ STEP_CASES = {
                      bcs=[{"type": "NodeDomain", "face0_mode": [0, 1], "face1_mode": [1, 0]}]),
         colors=np.random.default_rng(3).integers(0, 2, 3000)),
     "column_3d_quadratic_dp": lambda: scenes.granular_column(cell_size=1.0 / 64),
+    # 64 x 32 x 32 nodes, particles up to the upper x and y faces: a tile
+    # whose last node column is the grid's last has 27 dual pairs per axis
+    # (the clamped offsets fold onto the last node), more work items than
+    # the dual sweep's 640 threads, so this grid runs the cell scatter
+    "column_3d_quadratic_dp_face_tiles": lambda: scenes.granular_column(
+        domain=(63 / 64, 31 / 64, 31 / 64), cell_size=1.0 / 64, column=(63 / 64, 31 / 64, 0.2)),
     "random_3d_cubic_le_gravity": lambda: random_scene(
         3, 4000, "cubic", 4, margin=0.05, cell=0.1,
         bcs=[{"type": "Gravity", "gravity": [0.0, 0.0, -9.81]},
@@ -667,3 +673,28 @@ def test_autotune_picks_staging_and_resort_interval_on_cubic():
     tol = cond_tol(scene, 3, FIELDS, STEP_TOL)
     for name in FIELDS:
         assert rel(sim.get(name), ref[name]) <= tol[name], name
+
+
+def test_dual_sweep_refused_where_face_tiles_exceed_its_threads():
+    """On a grid with a node count divisible by 8 along x (64 x 32 x 32
+    nodes) the tiles at the upper face have 27 dual pairs along that axis and
+    more work items than the dual sweep's CTA: the handle runs the cell
+    scatter, refuses the sweep, and the autotuner keeps to the scatter; on
+    the 65 x 17 x 33 column the sweep stays the default."""
+    from pyroclastmpm_b200._capi import PmpmError
+
+    face = STEP_CASES["column_3d_quadratic_dp_face_tiles"]()
+    sim, _ref = make_pair(face)
+    sim.initialize()
+    assert sim.tuning()["p2g_kernel"] == 0
+    with pytest.raises(PmpmError):
+        sim.set_p2g_kernel(1)
+    sim.set_p2g_kernel(0)
+    sim.autotune(1)
+    assert sim.tuning()["p2g_kernel"] == 0
+    sim.close()
+    col = STEP_CASES["column_3d_quadratic_dp"]()
+    sim, _ref = make_pair(col)
+    sim.initialize()
+    assert sim.tuning()["p2g_kernel"] == 1
+    sim.close()
