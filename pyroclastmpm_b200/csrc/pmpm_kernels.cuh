@@ -131,11 +131,10 @@ __device__ __forceinline__ int tile_of(const DevGrid &g, const int c[3]) {
 // binning
 // --------------------------------------------------------------------------
 
-// Marks tile t active in this partition (plain stores: every writer stores
-// the same value).
-// Read before write: the cells of a tile mark it from many SMs, and plain
-// stores of the same word from all of them made the bed's binning pass 0.23
-// -> 0.31 ms.
+// Marks tile t active in this partition.  Writers race harmlessly (all store
+// the same value); the read first skips the store once the mark is set, as
+// the cells of a tile mark it from many SMs (storing unconditionally made
+// the bed's binning pass 0.23 -> 0.31 ms).
 __device__ __forceinline__ void mark_tile(const StepArgs &a, int t, int epoch) {
   if (a.N.tile_epoch[t] != epoch) a.N.tile_epoch[t] = epoch;
 }
@@ -1648,7 +1647,9 @@ __device__ __forceinline__ void issue_piece(const float4 *rec, const int *cell_k
 }
 
 // pair encoding: source (virtual, relative to tile origin - HI) in bits 0..7,
-// stencil offset in bits 8..9, target local coordinate in bits 12..15
+// stencil offset in bits 8..9, target local coordinate in bits 12..15, bit
+// 16 set where the target lies inside the grid (every listed pair, except the
+// padded target-major lists of the linear and cubic sweeps)
 __device__ __forceinline__ int pair_src(int p) { return p & 0xff; }
 __device__ __forceinline__ int pair_off(int p) { return (p >> 8) & 0x3; }
 __device__ __forceinline__ int pair_tgt(int p) { return (p >> 12) & 0xf; }
